@@ -1,0 +1,513 @@
+/*
+ * CPU oracle for the RNS-CKKS evaluator hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker: it is loaded by the
+ * tests, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg, and
+ * never by the product library (shmoai_b200/), which has its own host math
+ * and CUDA kernels.
+ *
+ * It restates, in plain scalar C (OpenMP over limbs), the arithmetic of the
+ * reference evaluator (ShMOAI's vendored PhantomFHE):
+ *
+ *   prime chain        thirdparty/phantom-fhe/src/modulus.cu:79-110 (CoeffModulus::Create,
+ *                      per-bit-size lists assigned from the back) and
+ *                      src/util/numth.cu:209-235 (get_primes: 2^b - 2N + 1 downwards)
+ *   NTT tables         src/util/ntt.cu:11-56 (minimal primitive 2N-th root,
+ *                      root_powers[bitrev(i)] = psi^i)
+ *   forward / inverse  src/ntt/fntt_2d.cu, src/ntt/intt_2d.cu (negacyclic CT/GS,
+ *                      output in bit-reversed order, fully reduced to [0,q))
+ *   ModUp              src/rns_bconv.cu:530-628 and src/rns.cu:138-181 (digit limbs
+ *                      copied unchanged, the rest base-converted without correction)
+ *   inner product      src/eval_key_switch.cu:12-66 (key digit = [b | a] over QP)
+ *   ModDown            src/rns_bconv.cu:776-828 (INTT of P limbs, fast base
+ *                      conversion P->Ql, NTT, (cx - delta) * P^-1)
+ *   key switch         src/eval_key_switch.cu:91-178
+ *   Galois (NTT form)  include/galois.cuh:44-60 and src/galois.cu:8-21
+ *   rescale            src/rns.cu:1125-1181 (floor: c_last mod q_j, no rounding term)
+ *   tensor / add /     src/polymath.cu:17-230, 468-504; src/evaluate.cu:1237-1266
+ *   multiply_plain
+ *   ct-pt matmul       src/include/source/matrix_mul/Ct_pt_matrix_mul.cuh:112-158
+ *                      (multiply_plain by a constant plaintext + add_inplace, summed)
+ *
+ * Layouts: a polynomial is [L][N] uint64 limbs (limb i under prime i of the
+ * chain), a ciphertext is [2][L][N], a key-switching key is
+ * [dnum][2][nq+np][N] with the "b" half first (the half added to c0).
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef unsigned __int128 u128;
+
+static inline uint64_t mulmod(uint64_t a, uint64_t b, uint64_t q) { return (uint64_t)(((u128)a * b) % q); }
+static inline uint64_t addmod(uint64_t a, uint64_t b, uint64_t q) { uint64_t s = a + b; return s >= q ? s - q : s; }
+static inline uint64_t submod(uint64_t a, uint64_t b, uint64_t q) { return a >= b ? a - b : a + q - b; }
+
+static uint64_t powmod(uint64_t a, uint64_t e, uint64_t q) {
+    uint64_t r = 1 % q;
+    a %= q;
+    while (e) {
+        if (e & 1) r = mulmod(r, a, q);
+        a = mulmod(a, a, q);
+        e >>= 1;
+    }
+    return r;
+}
+
+uint64_t orc_invmod(uint64_t a, uint64_t q) { return powmod(a % q, q - 2, q); }
+
+/* Deterministic Miller-Rabin for 64-bit integers (these bases are exact below 2^64). */
+int orc_is_prime(uint64_t n) {
+    static const uint64_t bases[12] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    if (n < 2) return 0;
+    for (int i = 0; i < 12; i++) {
+        if (n == bases[i]) return 1;
+        if (n % bases[i] == 0) return 0;
+    }
+    uint64_t d = n - 1;
+    int r = 0;
+    while ((d & 1) == 0) { d >>= 1; r++; }
+    for (int i = 0; i < 12; i++) {
+        uint64_t x = powmod(bases[i], d, n);
+        if (x == 1 || x == n - 1) continue;
+        int ok = 0;
+        for (int k = 1; k < r; k++) {
+            x = mulmod(x, x, n);
+            if (x == n - 1) { ok = 1; break; }
+        }
+        if (!ok) return 0;
+    }
+    return 1;
+}
+
+/* CoeffModulus::Create restated: for each bit size, primes = 1 mod 2N searched
+ * downwards from 2^b - 2N + 1; the i-th request of a size takes the LAST
+ * remaining prime of that size's list.  Returns 0 on success. */
+int orc_gen_primes(uint32_t log_n, const int *bits, uint32_t count, uint64_t *out) {
+    uint64_t two_n = 2ull << log_n;
+    for (uint32_t i = 0; i < count; i++) {
+        int b = bits[i];
+        uint32_t total = 0, before = 0;
+        for (uint32_t k = 0; k < count; k++) {
+            if (bits[k] == b) {
+                total++;
+                if (k < i) before++;
+            }
+        }
+        /* the (before)-th request takes list[total - 1 - before] */
+        uint32_t want = total - 1 - before;
+        uint64_t v = (1ull << b) - two_n + 1, lower = 1ull << (b - 1);
+        uint32_t found = 0;
+        int got = 0;
+        while (v > lower) {
+            if (orc_is_prime(v)) {
+                if (found == want) { out[i] = v; got = 1; break; }
+                found++;
+            }
+            v -= two_n;
+        }
+        if (!got) return -1;
+    }
+    return 0;
+}
+
+static uint32_t bitrev(uint32_t x, int bits) {
+    uint32_t r = 0;
+    for (int i = 0; i < bits; i++) { r = (r << 1) | (x & 1); x >>= 1; }
+    return r;
+}
+
+/* Smallest primitive 2N-th root of unity mod q (src/util/numth.cu:307-333 picks
+ * a primitive root and scans all of its odd powers for the minimum). */
+uint64_t orc_minimal_root(uint64_t q, uint32_t log_n) {
+    uint64_t two_n = 2ull << log_n, n = 1ull << log_n;
+    uint64_t root = 0;
+    for (uint64_t x = 2; x < q; x++) {
+        uint64_t r = powmod(x, (q - 1) / two_n, q);
+        if (powmod(r, n, q) == q - 1) { root = r; break; }
+    }
+    uint64_t sq = mulmod(root, root, q), cur = root, best = root;
+    for (uint64_t i = 0; i < n; i++) {
+        if (cur < best) best = cur;
+        cur = mulmod(cur, sq, q);
+    }
+    return best;
+}
+
+/* rp[bitrev(i)] = psi^i and irp[bitrev(i)] = psi^-i (no N^-1 folded in). */
+void orc_ntt_tables(uint64_t q, uint32_t log_n, uint64_t *rp, uint64_t *irp) {
+    uint32_t n = 1u << log_n;
+    uint64_t psi = orc_minimal_root(q, log_n), ipsi = orc_invmod(psi, q);
+    uint64_t p = 1, ip = 1;
+    for (uint32_t i = 0; i < n; i++) {
+        rp[bitrev(i, log_n)] = p;
+        irp[bitrev(i, log_n)] = ip;
+        p = mulmod(p, psi, q);
+        ip = mulmod(ip, ipsi, q);
+    }
+}
+
+/* Negacyclic forward NTT, natural order in, bit-reversed order out. */
+void orc_ntt_fwd(uint64_t *a, uint32_t log_n, uint64_t q, const uint64_t *rp) {
+    uint32_t n = 1u << log_n, t = n;
+    for (uint32_t m = 1; m < n; m <<= 1) {
+        t >>= 1;
+        for (uint32_t i = 0; i < m; i++) {
+            uint64_t w = rp[m + i];
+            uint32_t j1 = 2 * i * t;
+            for (uint32_t j = j1; j < j1 + t; j++) {
+                uint64_t x = a[j], y = mulmod(a[j + t], w, q);
+                a[j] = addmod(x, y, q);
+                a[j + t] = submod(x, y, q);
+            }
+        }
+    }
+}
+
+/* Inverse of orc_ntt_fwd (Gentleman-Sande), including the N^-1 scaling. */
+void orc_ntt_inv(uint64_t *a, uint32_t log_n, uint64_t q, const uint64_t *irp) {
+    uint32_t n = 1u << log_n, t = 1;
+    for (uint32_t m = n >> 1; m >= 1; m >>= 1) {
+        for (uint32_t i = 0; i < m; i++) {
+            uint64_t w = irp[m + i];
+            uint32_t j1 = 2 * i * t;
+            for (uint32_t j = j1; j < j1 + t; j++) {
+                uint64_t x = a[j], y = a[j + t];
+                a[j] = addmod(x, y, q);
+                a[j + t] = mulmod(submod(x, y, q), w, q);
+            }
+        }
+        t <<= 1;
+    }
+    uint64_t ninv = orc_invmod(n, q);
+    for (uint32_t j = 0; j < n; j++) a[j] = mulmod(a[j], ninv, q);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Context: prime chain Q (nq primes) followed by special primes P (np).     */
+
+typedef struct {
+    uint32_t log_n, n, nq, np;
+    uint64_t *primes;   /* nq + np */
+    uint64_t *rp, *irp; /* (nq + np) * n */
+} orc_ctx;
+
+orc_ctx *orc_ctx_create(uint32_t log_n, const uint64_t *primes, uint32_t nq, uint32_t np) {
+    orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
+    c->log_n = log_n;
+    c->n = 1u << log_n;
+    c->nq = nq;
+    c->np = np;
+    uint32_t k = nq + np;
+    c->primes = (uint64_t *)malloc(sizeof(uint64_t) * k);
+    memcpy(c->primes, primes, sizeof(uint64_t) * k);
+    c->rp = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)k * c->n);
+    c->irp = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)k * c->n);
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < (int)k; i++)
+        orc_ntt_tables(primes[i], log_n, c->rp + (size_t)i * c->n, c->irp + (size_t)i * c->n);
+    return c;
+}
+
+void orc_ctx_destroy(orc_ctx *c) {
+    if (!c) return;
+    free(c->primes);
+    free(c->rp);
+    free(c->irp);
+    free(c);
+}
+
+void orc_ctx_tables(const orc_ctx *c, uint32_t prime_idx, uint64_t *rp, uint64_t *irp) {
+    memcpy(rp, c->rp + (size_t)prime_idx * c->n, sizeof(uint64_t) * c->n);
+    memcpy(irp, c->irp + (size_t)prime_idx * c->n, sizeof(uint64_t) * c->n);
+}
+
+/* Transform n_polys polynomials of L limbs each (Q chain, limb i -> prime i). */
+void orc_ntt(const orc_ctx *c, uint64_t *a, uint32_t n_polys, uint32_t L, int inverse) {
+    size_t n = c->n;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int p = 0; p < (int)n_polys; p++)
+        for (int i = 0; i < (int)L; i++) {
+            uint64_t *x = a + ((size_t)p * L + i) * n;
+            if (inverse) orc_ntt_inv(x, c->log_n, c->primes[i], c->irp + (size_t)i * n);
+            else orc_ntt_fwd(x, c->log_n, c->primes[i], c->rp + (size_t)i * n);
+        }
+}
+
+/* Prime index (into c->primes) of extended limb j of a QlP polynomial. */
+static inline uint32_t ext_prime(const orc_ctx *c, uint32_t L, uint32_t j) { return j < L ? j : c->nq + (j - L); }
+
+void orc_add(const orc_ctx *c, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys, uint32_t L) {
+    size_t n = c->n;
+#pragma omp parallel for collapse(2)
+    for (int p = 0; p < (int)n_polys; p++)
+        for (int i = 0; i < (int)L; i++) {
+            size_t o = ((size_t)p * L + i) * n;
+            uint64_t q = c->primes[i];
+            for (size_t k = 0; k < n; k++) out[o + k] = addmod(a[o + k], b[o + k], q);
+        }
+}
+
+/* ct (n_polys x [L][N]) times one plaintext [L][N], pointwise (NTT form). */
+void orc_multiply_plain(const orc_ctx *c, const uint64_t *ct, const uint64_t *pt, uint64_t *out, uint32_t n_polys,
+                        uint32_t L) {
+    size_t n = c->n;
+#pragma omp parallel for collapse(2)
+    for (int p = 0; p < (int)n_polys; p++)
+        for (int i = 0; i < (int)L; i++) {
+            size_t o = ((size_t)p * L + i) * n;
+            uint64_t q = c->primes[i];
+            for (size_t k = 0; k < n; k++) out[o + k] = mulmod(ct[o + k], pt[(size_t)i * n + k], q);
+        }
+}
+
+/* (a0,a1) x (b0,b1) -> (a0b0, a0b1 + a1b0, a1b1) */
+void orc_tensor(const orc_ctx *c, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t L) {
+    size_t n = c->n, ln = (size_t)L * n;
+#pragma omp parallel for
+    for (int i = 0; i < (int)L; i++) {
+        uint64_t q = c->primes[i];
+        for (size_t k = 0; k < n; k++) {
+            size_t o = (size_t)i * n + k;
+            uint64_t a0 = a[o], a1 = a[ln + o], b0 = b[o], b1 = b[ln + o];
+            out[o] = mulmod(a0, b0, q);
+            out[ln + o] = addmod(mulmod(a0, b1, q), mulmod(a1, b0, q), q);
+            out[2 * ln + o] = mulmod(a1, b1, q);
+        }
+    }
+}
+
+/* Floor rescale by the last prime: out_j = (c_j - NTT_j(c_last mod q_j)) * q_last^-1. */
+void orc_rescale(const orc_ctx *c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L) {
+    size_t n = c->n;
+    uint64_t ql = c->primes[L - 1];
+    uint64_t *last = (uint64_t *)malloc(sizeof(uint64_t) * n * n_polys);
+    for (uint32_t p = 0; p < n_polys; p++) {
+        memcpy(last + p * n, in + ((size_t)p * L + L - 1) * n, sizeof(uint64_t) * n);
+        orc_ntt_inv(last + p * n, c->log_n, ql, c->irp + (size_t)(L - 1) * n);
+    }
+#pragma omp parallel for collapse(2)
+    for (int p = 0; p < (int)n_polys; p++)
+        for (int j = 0; j < (int)L - 1; j++) {
+            uint64_t qj = c->primes[j], inv = orc_invmod(ql % qj, qj);
+            uint64_t *o = out + ((size_t)p * (L - 1) + j) * n;
+            for (size_t k = 0; k < n; k++) o[k] = last[p * n + k] % qj;
+            orc_ntt_fwd(o, c->log_n, qj, c->rp + (size_t)j * n);
+            const uint64_t *ci = in + ((size_t)p * L + j) * n;
+            for (size_t k = 0; k < n; k++) o[k] = mulmod(submod(ci[k], o[k], qj), inv, qj);
+        }
+    free(last);
+}
+
+/* NTT-domain automorphism X -> X^elt: out[k] = in[perm[k]] with
+ * 2*brv(perm[k]) + 1 = (2*brv(k) + 1) * elt mod 2N. */
+void orc_galois_perm(uint32_t log_n, uint32_t elt, uint32_t *perm) {
+    uint32_t n = 1u << log_n;
+    for (uint32_t k = 0; k < n; k++) {
+        uint64_t e = ((uint64_t)(2 * bitrev(k, log_n) + 1) * elt) & (2ull * n - 1);
+        perm[k] = bitrev((uint32_t)((e - 1) >> 1), log_n);
+    }
+}
+
+void orc_apply_galois(const orc_ctx *c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                      uint32_t elt) {
+    size_t n = c->n;
+    uint32_t *perm = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    orc_galois_perm(c->log_n, elt, perm);
+#pragma omp parallel for
+    for (int r = 0; r < (int)(n_polys * L); r++)
+        for (size_t k = 0; k < n; k++) out[(size_t)r * n + k] = in[(size_t)r * n + perm[k]];
+    free(perm);
+}
+
+/* Galois element of a left rotation by `step` slots (src/galois.cu:47-91). */
+uint32_t orc_galois_elt_from_step(uint32_t log_n, int step) {
+    uint32_t n = 1u << log_n;
+    uint64_t m = 2ull * n;
+    if (step == 0) return (uint32_t)(m - 1);
+    uint32_t pos = (uint32_t)(step < 0 ? -step : step);
+    int s = step < 0 ? (int)(n >> 1) - (int)pos : (int)pos;
+    uint64_t g = 1;
+    while (s--) g = (g * 5) & (m - 1);
+    return (uint32_t)g;
+}
+
+/* ModUp of c (NTT form, L limbs): out[b] is digit b extended to QlP
+ * ([beta][L+np][N]).  Digit b covers limbs [b*np, min((b+1)*np, L)). */
+void orc_modup(const orc_ctx *c, const uint64_t *cin, uint32_t L, uint64_t *out) {
+    size_t n = c->n;
+    uint32_t alpha = c->np, beta = (L + alpha - 1) / alpha, LP = L + c->np;
+    uint64_t *x = (uint64_t *)malloc(sizeof(uint64_t) * L * n);
+    memcpy(x, cin, sizeof(uint64_t) * L * n);
+#pragma omp parallel for
+    for (int i = 0; i < (int)L; i++) orc_ntt_inv(x + (size_t)i * n, c->log_n, c->primes[i], c->irp + (size_t)i * n);
+    for (uint32_t b = 0; b < beta; b++) {
+        uint32_t s = b * alpha, e = s + alpha < L ? s + alpha : L;
+        /* y_i = x_i * (Qhat_i)^-1 mod q_i, Qhat_i = prod_{k in digit, k != i} q_k */
+        for (uint32_t i = s; i < e; i++) {
+            uint64_t qi = c->primes[i], h = 1;
+            for (uint32_t k = s; k < e; k++)
+                if (k != i) h = mulmod(h, c->primes[k] % qi, qi);
+            uint64_t hinv = orc_invmod(h, qi);
+            for (size_t k = 0; k < n; k++) x[(size_t)i * n + k] = mulmod(x[(size_t)i * n + k], hinv, qi);
+        }
+        uint64_t *ob = out + (size_t)b * LP * n;
+#pragma omp parallel for
+        for (int j = 0; j < (int)LP; j++) {
+            uint64_t *o = ob + (size_t)j * n;
+            if (j >= (int)s && j < (int)e) {
+                memcpy(o, cin + (size_t)j * n, sizeof(uint64_t) * n);
+                continue;
+            }
+            uint32_t pj = ext_prime(c, L, j);
+            uint64_t t = c->primes[pj];
+            uint64_t hm[64];
+            for (uint32_t i = s; i < e; i++) {
+                uint64_t h = 1;
+                for (uint32_t k = s; k < e; k++)
+                    if (k != i) h = mulmod(h, c->primes[k] % t, t);
+                hm[i - s] = h;
+            }
+            for (size_t k = 0; k < n; k++) {
+                u128 acc = 0;
+                for (uint32_t i = s; i < e; i++) acc += (u128)x[(size_t)i * n + k] * hm[i - s];
+                o[k] = (uint64_t)(acc % t);
+            }
+            orc_ntt_fwd(o, c->log_n, t, c->rp + (size_t)pj * n);
+        }
+    }
+    free(x);
+}
+
+/* ModDown of one QlP polynomial (NTT form) to Ql: (cx_j - NTT(conv_P->q_j(INTT(cx_P)))) * P^-1. */
+static void moddown_one(const orc_ctx *c, const uint64_t *cx, uint32_t L, uint64_t *out) {
+    size_t n = c->n;
+    uint32_t np = c->np;
+    uint64_t *z = (uint64_t *)malloc(sizeof(uint64_t) * np * n);
+    for (uint32_t k = 0; k < np; k++) {
+        uint32_t pk = c->nq + k;
+        uint64_t p = c->primes[pk], h = 1;
+        memcpy(z + (size_t)k * n, cx + (size_t)(L + k) * n, sizeof(uint64_t) * n);
+        orc_ntt_inv(z + (size_t)k * n, c->log_n, p, c->irp + (size_t)pk * n);
+        for (uint32_t k2 = 0; k2 < np; k2++)
+            if (k2 != k) h = mulmod(h, c->primes[c->nq + k2] % p, p);
+        uint64_t hinv = orc_invmod(h, p);
+        for (size_t t = 0; t < n; t++) z[(size_t)k * n + t] = mulmod(z[(size_t)k * n + t], hinv, p);
+    }
+#pragma omp parallel for
+    for (int j = 0; j < (int)L; j++) {
+        uint64_t q = c->primes[j];
+        uint64_t hm[64], P = 1;
+        for (uint32_t k = 0; k < np; k++) {
+            uint64_t h = 1;
+            for (uint32_t k2 = 0; k2 < np; k2++)
+                if (k2 != k) h = mulmod(h, c->primes[c->nq + k2] % q, q);
+            hm[k] = h;
+            P = mulmod(P, c->primes[c->nq + k] % q, q);
+        }
+        uint64_t pinv = orc_invmod(P, q);
+        uint64_t *o = out + (size_t)j * n;
+        for (size_t t = 0; t < n; t++) {
+            u128 acc = 0;
+            for (uint32_t k = 0; k < np; k++) acc += (u128)z[(size_t)k * n + t] * hm[k];
+            o[t] = (uint64_t)(acc % q);
+        }
+        orc_ntt_fwd(o, c->log_n, q, c->rp + (size_t)j * n);
+        const uint64_t *ci = cx + (size_t)j * n;
+        for (size_t t = 0; t < n; t++) o[t] = mulmod(submod(ci[t], o[t], q), pinv, q);
+    }
+    free(z);
+}
+
+/* Hybrid key switch of one polynomial d (NTT form, L limbs) with a key of
+ * dnum digits over QP: returns (cx0, cx1), each [L][N], not yet added. */
+void orc_keyswitch(const orc_ctx *c, const uint64_t *d, uint32_t L, const uint64_t *key, uint32_t dnum,
+                   uint64_t *out) {
+    size_t n = c->n;
+    uint32_t alpha = c->np, beta = (L + alpha - 1) / alpha, LP = L + c->np, QP = c->nq + c->np;
+    (void)dnum;
+    uint64_t *up = (uint64_t *)malloc(sizeof(uint64_t) * beta * LP * n);
+    orc_modup(c, d, L, up);
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * 2 * LP * n);
+#pragma omp parallel for
+    for (int j = 0; j < (int)LP; j++) {
+        uint32_t pj = ext_prime(c, L, j);
+        uint64_t t = c->primes[pj];
+        for (size_t k = 0; k < n; k++) {
+            u128 a0 = 0, a1 = 0;
+            for (uint32_t b = 0; b < beta; b++) {
+                uint64_t v = up[((size_t)b * LP + j) * n + k];
+                const uint64_t *kb = key + (size_t)b * 2 * QP * n;
+                a0 += (u128)v * kb[(size_t)pj * n + k];
+                a1 += (u128)v * kb[((size_t)QP + pj) * n + k];
+                a0 %= t;
+                a1 %= t;
+            }
+            cx[(size_t)j * n + k] = (uint64_t)a0;
+            cx[((size_t)LP + j) * n + k] = (uint64_t)a1;
+        }
+    }
+    moddown_one(c, cx, L, out);
+    moddown_one(c, cx + (size_t)LP * n, L, out + (size_t)L * n);
+    free(cx);
+    free(up);
+}
+
+/* Relinearize a size-3 ciphertext: (c0 + cx0, c1 + cx1) with cx = KS(c2). */
+void orc_relinearize(const orc_ctx *c, const uint64_t *ct3, uint32_t L, const uint64_t *key, uint32_t dnum,
+                     uint64_t *out) {
+    size_t ln = (size_t)L * c->n;
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * 2 * ln);
+    orc_keyswitch(c, ct3 + 2 * ln, L, key, dnum, cx);
+    orc_add(c, ct3, cx, out, 2, L);
+    free(cx);
+}
+
+/* Rotation / conjugation: (sigma(c0) + cx0, cx1) with cx = KS(sigma(c1)). */
+void orc_apply_galois_ct(const orc_ctx *c, const uint64_t *ct, uint32_t L, uint32_t elt, const uint64_t *key,
+                         uint32_t dnum, uint64_t *out) {
+    size_t ln = (size_t)L * c->n;
+    uint64_t *g = (uint64_t *)malloc(sizeof(uint64_t) * 2 * ln);
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * 2 * ln);
+    orc_apply_galois(c, ct, g, 2, L, elt);
+    orc_keyswitch(c, g + ln, L, key, dnum, cx);
+    orc_add(c, g, cx, out, 1, L);
+    memcpy(out + ln, cx + ln, sizeof(uint64_t) * ln);
+    free(cx);
+    free(g);
+}
+
+/* Signed integer -> residue (the canonical form an NTT-domain constant takes). */
+static inline uint64_t signed_residue(int64_t w, uint64_t q) {
+    if (w >= 0) return (uint64_t)w % q;
+    uint64_t r = (uint64_t)(-(w + 1)) % q; /* |w| - 1 without overflow */
+    r = r + 1 == q ? 0 : r + 1;
+    return r ? q - r : 0;
+}
+
+uint64_t orc_signed_residue(int64_t w, uint64_t q) { return signed_residue(w, q); }
+
+/* Y_o = sum_i X_i * W[i][o] (constant plaintexts, NTT form), no rescale.
+ * X: [n_in][2][L][N]; W: [n_in][n_out] signed integers; Y: [n_out][2][L][N]. */
+void orc_ctpt_matmul(const orc_ctx *c, const uint64_t *X, const int64_t *W, uint32_t n_in, uint32_t n_out,
+                     uint32_t L, uint64_t *Y) {
+    size_t n = c->n, ctw = 2 * (size_t)L * n;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int o = 0; o < (int)n_out; o++)
+        for (int r = 0; r < (int)(2 * L); r++) {
+            uint32_t limb = (uint32_t)r % L;
+            uint64_t q = c->primes[limb];
+            uint64_t *y = Y + (size_t)o * ctw + (size_t)r * n;
+            u128 *acc = (u128 *)calloc(n, sizeof(u128));
+            for (uint32_t i = 0; i < n_in; i++) {
+                uint64_t w = signed_residue(W[(size_t)i * n_out + o], q);
+                const uint64_t *x = X + (size_t)i * ctw + (size_t)r * n;
+                for (size_t k = 0; k < n; k++) {
+                    acc[k] += (u128)x[k] * w;
+                    if ((i & 31) == 31) acc[k] %= q;
+                }
+            }
+            for (size_t k = 0; k < n; k++) y[k] = (uint64_t)(acc[k] % q);
+            free(acc);
+        }
+}

@@ -1,0 +1,90 @@
+// Batched negacyclic NTT / INTT over RNS limbs.
+//
+// Definition (bit-identical to the reference, thirdparty/phantom-fhe/src/ntt/fntt_2d.cu
+// and intt_2d.cu): forward = Cooley-Tukey with root_powers[bitrev(i)] = psi^i, natural
+// order in, bit-reversed order out, fully reduced to [0, q); inverse = Gentleman-Sande
+// with psi^-i, including N^-1.
+//
+// Decomposition: N = M * M (M = 2^(2R)).  The first log M forward stages only
+// combine elements of one "column" {c + M*p : p < M}; the last log M stages only
+// combine elements of one contiguous "block" {b*M + p : p < M}.  Each phase is one
+// kernel in which a CTA owns 16 columns (or 16 blocks) of one limb; a thread owns
+// 2^R elements and runs R radix-2 stages in registers, twice, with one shared-memory
+// exchange in between.  Global loads and stores are 128-byte coalesced (16
+// consecutive words per column row / per block segment).  Values between the two
+// phases are lazy in [0, 4q) (Harvey butterflies; q < 2^62).
+//
+// The inverse's last stage folds a per-limb scale c (N^-1, or N^-1 times the
+// ModUp digit factor) into both outputs: (X+Y)*c and (X-Y)*psi^-(N/2)*c.
+#pragma once
+#include <cstdint>
+
+#include "modarith.cuh"
+
+namespace shm {
+
+constexpr int kNttSubs = 16;  // columns / blocks per CTA
+
+struct LimbMap {
+    uint8_t prime[256];  // limb slot within a polynomial -> prime index; 255 = leave untouched
+};
+
+// scale constants of the inverse's last stage, per limb slot: c, c', c*psi^-(N/2), (c*psi^-(N/2))'
+struct InvScale {
+    const uint64_t *c;  // [slots][4]
+};
+
+__device__ __forceinline__ void ct_bf(uint64_t &x, uint64_t &y, uint64_t w, uint64_t ws, uint64_t q) {
+    uint64_t q2 = 2 * q;
+    uint64_t a = csub(x, q2);
+    uint64_t t = shoup_lazy(y, w, ws, q);
+    x = a + t;
+    y = a - t + q2;
+}
+
+__device__ __forceinline__ void gs_bf(uint64_t &x, uint64_t &y, uint64_t w, uint64_t ws, uint64_t q) {
+    uint64_t q2 = 2 * q;
+    uint64_t a = x + y;
+    uint64_t d = x - y + q2;
+    x = csub(a, q2);
+    y = shoup_lazy(d, w, ws, q);
+}
+
+// R forward stages on E = 2^R registers.  Stage r of the pass is global stage
+// s0 + r; the twiddle of the pair starting at m is tw[(tb << (s0 + r)) + (g << r) + (m >> (R - r))].
+template <int R>
+__device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
+                                         const uint64_t *__restrict__ ws, uint32_t tb, uint32_t s0, uint32_t g,
+                                         uint64_t q) {
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int half = (1 << R) >> (r + 1);
+        const uint32_t base = (tb << (s0 + r)) + (g << r);
+#pragma unroll
+        for (int m = 0; m < (1 << R); m++) {
+            if (m & half) continue;
+            uint32_t idx = base + (m >> (R - r));
+            ct_bf(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
+        }
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void inv_pass(uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
+                                         const uint64_t *__restrict__ ws, uint32_t tb, uint32_t s0, uint32_t g,
+                                         uint64_t q, int skip_stage0) {
+#pragma unroll
+    for (int r = R - 1; r >= 0; r--) {
+        if (r == 0 && skip_stage0) break;
+        const int half = (1 << R) >> (r + 1);
+        const uint32_t base = (tb << (s0 + r)) + (g << r);
+#pragma unroll
+        for (int m = 0; m < (1 << R); m++) {
+            if (m & half) continue;
+            uint32_t idx = base + (m >> (R - r));
+            gs_bf(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
+        }
+    }
+}
+
+}  // namespace shm
