@@ -1,0 +1,130 @@
+/*
+ * shmoai_ckks.h -- C ABI of the B200 CKKS evaluation core.
+ *
+ * Drop-in boundary for ShMOAI's evaluator hot path.  Each entry point replaces
+ * the reference operation cited beside it (paths are inside the ShMOAI tree);
+ * results are bit-identical to the reference's for the same primes, keys and
+ * inputs.
+ *
+ * Conventions
+ *  - All ring data is uint64 residues in DEVICE memory, in NTT form unless a
+ *    function says otherwise.  A polynomial at level L is [L][N] (limb i under
+ *    prime i of the chain); a ciphertext is [2][L][N]; batches of ciphertexts
+ *    are contiguous [n_cts][2][L][N].  This is the reference's own layout
+ *    (thirdparty/phantom-fhe/include/ciphertext.h:274-282).
+ *  - Key-switching keys are [dnum][2][nq+np][N]: per digit the "b" half
+ *    (added into c0) followed by the "a" half (secretkey.cu:328-373 layout).
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  Every call is
+ *    asynchronous on that stream.
+ *  - `workspace` / `workspace_bytes`: device scratch owned by the caller, at
+ *    least shm_*_workspace_bytes(); pass NULL to use the context's internal
+ *    arena (grown on demand; serialise such calls per context).
+ *  - Every function returns SHM_OK or a negative SHM_E* code and never throws;
+ *    shm_last_error() gives the message of the calling thread's last failure.
+ */
+#ifndef SHMOAI_CKKS_H
+#define SHMOAI_CKKS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHM_OK 0
+#define SHM_EINVAL -1   /* bad argument (level, size, shape) */
+#define SHM_ECUDA -2    /* CUDA runtime error */
+#define SHM_ENOMEM -3   /* device allocation failed */
+#define SHM_EINTERNAL -4
+
+typedef struct shm_context shm_context;
+
+/* Context over a prime chain given by bit sizes: n_q ciphertext primes then
+ * n_p special primes, generated exactly like CoeffModulus::Create
+ * (thirdparty/phantom-fhe/src/modulus.cu:79-110).  Replaces PhantomContext(parms)
+ * (thirdparty/phantom-fhe/src/context.cu:141-238).  log_n in {12, 16}. */
+int shm_context_create(shm_context **out, uint32_t log_n, const int *bits, uint32_t n_q, uint32_t n_p, int device);
+/* Same with explicit primes (n_q + n_p values, each 1 mod 2N, < 2^61). */
+int shm_context_create_from_primes(shm_context **out, uint32_t log_n, const uint64_t *primes, uint32_t n_q,
+                                   uint32_t n_p, int device);
+void shm_context_destroy(shm_context *ctx);
+/* log_n, n_q, n_p, dnum = n_q / n_p (secretkey.cu:341) */
+int shm_context_info(const shm_context *ctx, uint32_t *log_n, uint32_t *n_q, uint32_t *n_p, uint32_t *dnum);
+int shm_context_primes(const shm_context *ctx, uint64_t *out);
+const char *shm_last_error(void);
+/* Total kernels launched by this library in this process (no reference
+ * counterpart: instrumentation for the benchmark's launch count). */
+uint64_t shm_kernel_launches(void);
+
+/* Forward / inverse negacyclic NTT of n_polys polynomials of L limbs, in place.
+ * Replaces nwt_2d_radix8_forward_inplace / nwt_2d_radix8_backward_inplace
+ * (thirdparty/phantom-fhe/include/ntt.cuh:47-99) as called by
+ * moai::Evaluator::transform_to_ntt_inplace / transform_from_ntt_inplace
+ * (src/include/source/ckks_evaluator_parallel.cuh:396-442). */
+int shm_ntt_forward(const shm_context *ctx, uint64_t *data, uint32_t n_polys, uint32_t L, void *stream);
+int shm_ntt_inverse(const shm_context *ctx, uint64_t *data, uint32_t n_polys, uint32_t L, void *stream);
+
+/* out = a + b, a - b, -a over n_polys polynomials of L limbs.
+ * Replaces add_inplace / sub_inplace / negate (thirdparty/phantom-fhe/src/evaluate.cu:114-348). */
+int shm_add(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+            uint32_t L, void *stream);
+int shm_sub(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+            uint32_t L, void *stream);
+int shm_negate(const shm_context *ctx, const uint64_t *a, uint64_t *out, uint32_t n_polys, uint32_t L, void *stream);
+
+/* out[c] = ct[c] * pt for n_polys polynomials and one plaintext [L][N].
+ * Replaces multiply_plain_inplace / multiply_plain_ntt (evaluate.cu:1237-1266). */
+int shm_multiply_plain(const shm_context *ctx, const uint64_t *ct, const uint64_t *pt, uint64_t *out,
+                       uint32_t n_polys, uint32_t L, void *stream);
+
+/* Size-3 tensor product of n_cts ciphertext pairs: out [n_cts][3][L][N].
+ * Replaces bgv_ckks_multiply -> tensor_prod_2x2_rns_poly (evaluate.cu:350-402). */
+int shm_multiply(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_cts,
+                 uint32_t L, void *stream);
+
+/* Rescale (floor division by the last prime) of n_polys polynomials, L -> L-1 limbs.
+ * Replaces rescale_to_next / divide_and_round_q_last_ntt (evaluate.cu:1392-1443,
+ * src/rns.cu:1157-1181). */
+size_t shm_rescale_workspace_bytes(const shm_context *ctx, uint32_t n_polys, uint32_t L);
+int shm_rescale(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                void *workspace, size_t workspace_bytes, void *stream);
+
+/* Key switch of n_cts polynomials d [n_cts][L][N]: out (a [n_cts][2][L][N] buffer)
+ * receives (cx0, cx1).  Replaces keyswitch_inplace's modup / inner product /
+ * moddown (src/eval_key_switch.cu:91-178). */
+size_t shm_keyswitch_workspace_bytes(const shm_context *ctx, uint32_t n_cts, uint32_t L);
+int shm_keyswitch(const shm_context *ctx, const uint64_t *d, const uint64_t *key, uint64_t *out, uint32_t n_cts,
+                  uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Relinearize n_cts size-3 ciphertexts [n_cts][3][L][N] into [n_cts][2][L][N].
+ * Replaces relinearize_inplace (evaluate.cu:1358-1390). */
+int shm_relinearize(const shm_context *ctx, const uint64_t *ct3, const uint64_t *relin_key, uint64_t *out,
+                    uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Apply the automorphism X -> X^galois_elt with its key to n_cts ciphertexts.
+ * Replaces apply_galois_inplace (evaluate.cu:1586-1647). */
+int shm_apply_galois(const shm_context *ctx, const uint64_t *ct, uint32_t galois_elt, const uint64_t *galois_key,
+                     uint64_t *out, uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes,
+                     void *stream);
+/* Galois element of a rotation by `step` slots (0 = conjugation).
+ * Replaces PhantomGaloisTool::get_elt_from_step (src/galois.cu:47-91). */
+uint32_t shm_galois_elt_from_step(const shm_context *ctx, int step);
+/* HRotate: shm_apply_galois with shm_galois_elt_from_step(step).
+ * Replaces moai::Evaluator::rotate_vector_inplace (ckks_evaluator_parallel.cuh:341-347). */
+int shm_rotate(const shm_context *ctx, const uint64_t *ct, int step, const uint64_t *galois_key, uint64_t *out,
+               uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Rotation-free ct-pt matmul: Y[o] = sum_i X[i] * W[i][o] over n_in input
+ * ciphertexts X [n_in][2][L][N] and signed integer weights W [n_in][n_out]
+ * (the encoded constants round(w * scale)); Y is [n_out][2][L][N] before the
+ * rescale.  Replaces the multiply_plain + add_inplace loop of
+ * ct_pt_matrix_mul_wo_pre (src/include/source/matrix_mul/Ct_pt_matrix_mul.cuh:112-158). */
+size_t shm_ctpt_matmul_workspace_bytes(const shm_context *ctx, uint32_t n_in, uint32_t n_out, uint32_t L);
+int shm_ctpt_matmul(const shm_context *ctx, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in,
+                    uint32_t n_out, uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SHMOAI_CKKS_H */

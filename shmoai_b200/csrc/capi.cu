@@ -1,0 +1,446 @@
+// Context construction and the extern "C" entry points of include/shmoai_ckks.h.
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/shmoai_ckks.h"
+#include "core.hpp"
+#include "host_math.hpp"
+
+namespace shm {
+
+std::atomic<unsigned long long> g_launches{0};
+
+namespace {
+
+template <typename T>
+T *upload(const std::vector<T> &v) {
+    T *d = nullptr;
+    SHM_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
+    SHM_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+}
+
+void push4(std::vector<uint64_t> &v, uint64_t c, uint64_t psi_half_inv, uint64_t q) {
+    uint64_t c1 = host::mulmod(c, psi_half_inv, q);
+    v.push_back(c);
+    v.push_back(host::shoup_of(c, q));
+    v.push_back(c1);
+    v.push_back(host::shoup_of(c1, q));
+}
+
+}  // namespace
+
+Context::~Context() {
+    cudaSetDevice(device);
+    for (void *p : {(void *)pc, (void *)tw, (void *)inv_scale_plain, (void *)moddown_scale, (void *)moddown_conv,
+                    (void *)p_inv, (void *)rescale_inv, arena})
+        if (p) cudaFree(p);
+    for (auto &l : ks) {
+        if (l.modup_scale) cudaFree(l.modup_scale);
+        if (l.modup_conv) cudaFree(l.modup_conv);
+    }
+    for (auto &kv : galois_perm) cudaFree(kv.second);
+}
+
+const uint32_t *Context::perm(uint32_t elt) {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = galois_perm.find(elt);
+    if (it != galois_perm.end()) return it->second;
+    if (!(elt & 1) || elt >= 2 * n) throw std::invalid_argument("Galois element must be odd and < 2N");
+    // NTT-domain automorphism (src/galois.cu:8-21, include/galois.cuh:44-60):
+    // slot k holds a(psi^(2*brv(k)+1)); X -> X^elt moves slot perm[k] to k with
+    // 2*brv(perm[k]) + 1 = (2*brv(k) + 1) * elt mod 2N.
+    std::vector<uint32_t> p(n);
+    for (uint32_t k = 0; k < n; k++) {
+        uint64_t e = ((uint64_t)(2 * host::bitrev(k, log_n) + 1) * elt) & (2ull * n - 1);
+        p[k] = host::bitrev((uint32_t)((e - 1) >> 1), log_n);
+    }
+    uint32_t *d = upload(p);
+    galois_perm[elt] = d;
+    return d;
+}
+
+void *Context::workspace(size_t bytes) {
+    if (bytes <= arena_bytes) return arena;
+    if (arena) SHM_CUDA(cudaFree(arena));
+    arena = nullptr;
+    arena_bytes = 0;
+    SHM_CUDA(cudaMalloc(&arena, bytes));
+    arena_bytes = bytes;
+    return arena;
+}
+
+Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uint32_t nq, uint32_t np, int device) {
+    if (log_n != 12 && log_n != 16) throw std::invalid_argument("log_n must be 12 or 16");
+    if (nq < 1 || nq + np != primes.size() || nq + np > 250) throw std::invalid_argument("bad prime counts");
+    std::unique_ptr<Context> c(new Context);
+    c->device = device;
+    SHM_CUDA(cudaSetDevice(device));
+    c->log_n = log_n;
+    c->n = 1u << log_n;
+    c->nq = nq;
+    c->np = np;
+    c->dnum = np ? nq / np : 0;
+    c->primes = primes;
+    const uint32_t QP = nq + np, n = c->n;
+    for (uint64_t q : primes) {
+        if (q >= (1ull << 61) || (q - 1) % (2ull * n) || !host::is_prime(q))
+            throw std::invalid_argument("every prime must be < 2^61 and 1 mod 2N");
+        if (np && (uint64_t)np * q >= (1ull << 63))
+            throw std::invalid_argument("alpha * q must stay below 2^63 for the lazy base conversion");
+    }
+    // per-prime constants and twiddles
+    std::vector<uint64_t> tw((size_t)QP * 4 * n), psi_half_inv(QP), sc_plain;
+    for (uint32_t i = 0; i < QP; i++) {
+        uint64_t q = primes[i], *t = tw.data() + (size_t)i * 4 * n;
+        host::ntt_tables(q, log_n, t, t + n, t + 2 * n, t + 3 * n);
+        psi_half_inv[i] = t[2 * n + 1];
+        PrimeConst p{};
+        p.q = q;
+        p.mu = host::barrett_mu(q);
+        p.shift = host::bit_length(q) - 1;
+        p.n_inv = host::invmod(n, q);
+        p.n_inv_shoup = host::shoup_of(p.n_inv, q);
+        c->h_pc.push_back(p);
+        push4(sc_plain, p.n_inv, psi_half_inv[i], q);
+    }
+    c->pc = upload(c->h_pc);
+    c->tw = upload(tw);
+    c->inv_scale_plain = upload(sc_plain);
+
+    // rescale: row L-1 holds q_{L-1}^-1 mod q_j
+    std::vector<uint64_t> rinv((size_t)nq * nq * 2, 0);
+    for (uint32_t L = 2; L <= nq; L++)
+        for (uint32_t j = 0; j + 1 < L; j++) {
+            uint64_t q = primes[j], v = host::invmod(primes[L - 1] % q, q);
+            rinv[((size_t)(L - 1) * nq + j) * 2] = v;
+            rinv[((size_t)(L - 1) * nq + j) * 2 + 1] = host::shoup_of(v, q);
+        }
+    c->rescale_inv = upload(rinv);
+
+    c->ks.resize(nq + 1);
+    if (np) {
+        std::vector<uint64_t> P(primes.begin() + nq, primes.end());
+        // ModDown constants
+        std::vector<uint64_t> mds, mdc((size_t)nq * np), pinv((size_t)nq * 2);
+        for (uint32_t k = 0; k < np; k++) {
+            uint64_t p = P[k], h = host::partial_product(P, k, p);
+            push4(mds, host::mulmod(host::invmod(h, p), c->h_pc[nq + k].n_inv, p), psi_half_inv[nq + k], p);
+        }
+        for (uint32_t j = 0; j < nq; j++) {
+            uint64_t q = primes[j], prod = 1;
+            for (uint32_t k = 0; k < np; k++) {
+                mdc[(size_t)j * np + k] = host::partial_product(P, k, q);
+                prod = host::mulmod(prod, P[k] % q, q);
+            }
+            uint64_t v = host::invmod(prod, q);
+            pinv[2 * j] = v;
+            pinv[2 * j + 1] = host::shoup_of(v, q);
+        }
+        c->moddown_scale = upload(mds);
+        c->moddown_conv = upload(mdc);
+        c->p_inv = upload(pinv);
+        // ModUp constants per level
+        for (uint32_t L = 1; L <= nq; L++) {
+            LevelKS &ks = c->ks[L];
+            ks.L = L;
+            ks.beta = (L + np - 1) / np;
+            const uint32_t LP = L + np;
+            std::vector<uint64_t> msc, conv((size_t)ks.beta * LP * np, 0);
+            for (uint32_t b = 0; b < ks.beta; b++) {
+                uint32_t s = b * np, e = std::min(s + np, L);
+                std::vector<uint64_t> D(primes.begin() + s, primes.begin() + e);
+                for (uint32_t i = s; i < e; i++) {
+                    uint64_t q = primes[i], h = host::partial_product(D, i - s, q);
+                    push4(msc, host::mulmod(host::invmod(h, q), c->h_pc[i].n_inv, q), psi_half_inv[i], q);
+                }
+                for (uint32_t j = 0; j < LP; j++) {
+                    if (j >= s && j < e) continue;
+                    uint64_t t = primes[j < L ? j : nq + (j - L)];
+                    for (uint32_t i = 0; i < e - s; i++)
+                        conv[((size_t)b * LP + j) * np + i] = host::partial_product(D, i, t);
+                }
+            }
+            ks.modup_scale = upload(msc);
+            ks.modup_conv = upload(conv);
+        }
+    }
+    SHM_CUDA(cudaDeviceSynchronize());
+    return c.release();
+}
+
+}  // namespace shm
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+struct shm_context {
+    shm::Context *c;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <typename F>
+int guard(F &&f) {
+    try {
+        f();
+        return SHM_OK;
+    } catch (const std::invalid_argument &e) {
+        g_err = e.what();
+        return SHM_EINVAL;
+    } catch (const shm::CudaError &e) {
+        g_err = e.what();
+        return std::strstr(e.what(), "out of memory") ? SHM_ENOMEM : SHM_ECUDA;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return SHM_EINTERNAL;
+    } catch (...) {
+        g_err = "unknown error";
+        return SHM_EINTERNAL;
+    }
+}
+
+shm::Context &ctx_of(const shm_context *h) {
+    if (!h || !h->c) throw std::invalid_argument("null context");
+    return *h->c;
+}
+
+cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+void check_level(const shm::Context &c, uint32_t L) {
+    if (L < 1 || L > c.nq) throw std::invalid_argument("level (limb count) out of range");
+}
+
+uint64_t *ws_of(shm::Context &c, void *ws, size_t have, size_t need_words) {
+    size_t need = need_words * 8;
+    if (ws) {
+        if (have < need) throw std::invalid_argument("workspace too small");
+        return static_cast<uint64_t *>(ws);
+    }
+    return static_cast<uint64_t *>(c.workspace(need));
+}
+
+void set_device(const shm::Context &c) { SHM_CUDA(cudaSetDevice(c.device)); }
+
+}  // namespace
+
+extern "C" {
+
+const char *shm_last_error(void) { return g_err.c_str(); }
+
+uint64_t shm_kernel_launches(void) { return shm::g_launches.load(std::memory_order_relaxed); }
+
+int shm_context_create_from_primes(shm_context **out, uint32_t log_n, const uint64_t *primes, uint32_t n_q,
+                                   uint32_t n_p, int device) {
+    return guard([&] {
+        if (!out || !primes) throw std::invalid_argument("null argument");
+        std::vector<uint64_t> p(primes, primes + n_q + n_p);
+        *out = new shm_context{shm::create_context(log_n, p, n_q, n_p, device)};
+    });
+}
+
+int shm_context_create(shm_context **out, uint32_t log_n, const int *bits, uint32_t n_q, uint32_t n_p, int device) {
+    return guard([&] {
+        if (!out || !bits) throw std::invalid_argument("null argument");
+        std::vector<int> b(bits, bits + n_q + n_p);
+        auto p = shm::host::create_primes((int)log_n, b);
+        *out = new shm_context{shm::create_context(log_n, p, n_q, n_p, device)};
+    });
+}
+
+void shm_context_destroy(shm_context *ctx) {
+    if (!ctx) return;
+    delete ctx->c;
+    delete ctx;
+}
+
+int shm_context_info(const shm_context *ctx, uint32_t *log_n, uint32_t *n_q, uint32_t *n_p, uint32_t *dnum) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        if (log_n) *log_n = c.log_n;
+        if (n_q) *n_q = c.nq;
+        if (n_p) *n_p = c.np;
+        if (dnum) *dnum = c.dnum;
+    });
+}
+
+int shm_context_primes(const shm_context *ctx, uint64_t *out) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        std::memcpy(out, c.primes.data(), c.primes.size() * sizeof(uint64_t));
+    });
+}
+
+int shm_ntt_forward(const shm_context *ctx, uint64_t *data, uint32_t n_polys, uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::ntt_forward(c, data, n_polys * L, L, shm::q_map(L), S(stream));
+    });
+}
+
+int shm_ntt_inverse(const shm_context *ctx, uint64_t *data, uint32_t n_polys, uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::ntt_inverse(c, data, n_polys * L, L, shm::q_map(L), nullptr, S(stream));
+    });
+}
+
+static int ew(const shm_context *ctx, shm::EwOp op, const uint64_t *a, const uint64_t *b, uint64_t *out,
+              uint32_t n_polys, uint32_t L, uint32_t b_polys, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::elementwise(c, op, a, b, out, n_polys, L, b_polys, S(stream));
+    });
+}
+
+int shm_add(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+            uint32_t L, void *stream) {
+    return ew(ctx, shm::EwOp::Add, a, b, out, n_polys, L, n_polys, stream);
+}
+
+int shm_sub(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+            uint32_t L, void *stream) {
+    return ew(ctx, shm::EwOp::Sub, a, b, out, n_polys, L, n_polys, stream);
+}
+
+int shm_negate(const shm_context *ctx, const uint64_t *a, uint64_t *out, uint32_t n_polys, uint32_t L, void *stream) {
+    return ew(ctx, shm::EwOp::Negate, a, nullptr, out, n_polys, L, n_polys, stream);
+}
+
+int shm_multiply_plain(const shm_context *ctx, const uint64_t *ct, const uint64_t *pt, uint64_t *out,
+                       uint32_t n_polys, uint32_t L, void *stream) {
+    return ew(ctx, shm::EwOp::MulPlain, ct, pt, out, n_polys, L, 1, stream);
+}
+
+int shm_multiply(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_cts,
+                 uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::tensor(c, a, b, out, n_cts, L, S(stream));
+    });
+}
+
+size_t shm_rescale_workspace_bytes(const shm_context *ctx, uint32_t n_polys, uint32_t L) {
+    return ctx && ctx->c ? shm::rescale_ws_words(*ctx->c, n_polys, L) * 8 : 0;
+}
+
+int shm_rescale(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        if (L < 2) throw std::invalid_argument("rescale needs at least two limbs");
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::rescale_ws_words(c, n_polys, L));
+        shm::rescale(c, in, out, n_polys, L, ws, S(stream));
+    });
+}
+
+size_t shm_keyswitch_workspace_bytes(const shm_context *ctx, uint32_t n_cts, uint32_t L) {
+    return ctx && ctx->c ? shm::keyswitch_ws_words(*ctx->c, n_cts, L) * 8 : 0;
+}
+
+int shm_keyswitch(const shm_context *ctx, const uint64_t *d, const uint64_t *key, uint64_t *out, uint32_t n_cts,
+                  uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::keyswitch_ws_words(c, n_cts, L));
+        const size_t ln = (size_t)L * c.n;
+        shm::KsOutput o{out, out + ln, nullptr, nullptr, 2 * ln};
+        shm::keyswitch(c, d, ln, n_cts, L, key, o, ws, S(stream));
+    });
+}
+
+int shm_relinearize(const shm_context *ctx, const uint64_t *ct3, const uint64_t *relin_key, uint64_t *out,
+                    uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::keyswitch_ws_words(c, n_cts, L));
+        const size_t ln = (size_t)L * c.n;
+        if (out == ct3 && n_cts > 1) throw std::invalid_argument("in-place relinearize needs n_cts == 1");
+        // key switch c2 first (it only reads ct3), then out_h = c_h + cx_h in the combine step;
+        // (c0, c1) are read with the size-3 stride through the add pointers
+        shm::KsOutput o{out, out + ln, ct3, ct3 + ln, 2 * ln};
+        if (out != ct3) {
+            // the combine reads add and writes out with one stride: stage (c0, c1) into out
+            SHM_CUDA(cudaMemcpy2DAsync(out, 2 * ln * 8, ct3, 3 * ln * 8, 2 * ln * 8, n_cts,
+                                       cudaMemcpyDeviceToDevice, S(stream)));
+            o.add0 = out;
+            o.add1 = out + ln;
+        }
+        shm::keyswitch(c, ct3 + 2 * ln, 3 * ln, n_cts, L, relin_key, o, ws, S(stream));
+    });
+}
+
+uint32_t shm_galois_elt_from_step(const shm_context *ctx, int step) {
+    if (!ctx || !ctx->c) return 0;
+    const uint32_t n = ctx->c->n;
+    const uint64_t m = 2ull * n;
+    if (step == 0) return (uint32_t)(m - 1);
+    // left rotation by |step| slots uses 5^step; right rotation by s uses 5^(N/2 - s)
+    uint32_t pos = (uint32_t)(step < 0 ? -step : step);
+    if (pos >= n / 2) return 0;
+    uint32_t e = step < 0 ? n / 2 - pos : pos;
+    uint64_t g = 1;
+    while (e--) g = (g * 5) & (m - 1);
+    return (uint32_t)g;
+}
+
+int shm_apply_galois(const shm_context *ctx, const uint64_t *ct, uint32_t galois_elt, const uint64_t *galois_key,
+                     uint64_t *out, uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes,
+                     void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        set_device(c);
+        const size_t ln = (size_t)L * c.n;
+        const size_t ks_words = shm::keyswitch_ws_words(c, n_cts, L);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, ks_words + (size_t)n_cts * 2 * ln);
+        uint64_t *perm = ws + ks_words;  // permuted (c0, c1) of every ciphertext
+        shm::apply_galois(c, ct, perm, n_cts * 2 * L, galois_elt, S(stream));
+        shm::KsOutput o{out, out + ln, perm, nullptr, 2 * ln};
+        shm::keyswitch(c, perm + ln, 2 * ln, n_cts, L, galois_key, o, ws, S(stream));
+    });
+}
+
+int shm_rotate(const shm_context *ctx, const uint64_t *ct, int step, const uint64_t *galois_key, uint64_t *out,
+               uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    uint32_t elt = shm_galois_elt_from_step(ctx, step);
+    if (!elt) {
+        g_err = "rotation step out of range";
+        return SHM_EINVAL;
+    }
+    return shm_apply_galois(ctx, ct, elt, galois_key, out, n_cts, L, workspace, workspace_bytes, stream);
+}
+
+size_t shm_ctpt_matmul_workspace_bytes(const shm_context *ctx, uint32_t n_in, uint32_t n_out, uint32_t L) {
+    return ctx && ctx->c ? shm::ctpt_ws_words(*ctx->c, n_in, n_out, L) * 8 : 0;
+}
+
+int shm_ctpt_matmul(const shm_context *ctx, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in,
+                    uint32_t n_out, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::ctpt_ws_words(c, n_in, n_out, L));
+        shm::ctpt_matmul(c, X, W, Y, n_in, n_out, L, ws, S(stream));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// Internal interface of the CKKS core: the device-resident context and the
+// kernel launchers.  The public surface is the C ABI in include/shmoai_ckks.h.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "modarith.cuh"
+#include "ntt.cuh"
+
+namespace shm {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+// Number of kernels this library has launched (reported by shm_kernel_launches).
+extern std::atomic<unsigned long long> g_launches;
+#define SHM_LAUNCHED(k) ::shm::g_launches.fetch_add((k), std::memory_order_relaxed)
+
+#define SHM_CUDA(call)                                                                                       \
+    do {                                                                                                     \
+        cudaError_t e_ = (call);                                                                             \
+        if (e_ != cudaSuccess)                                                                               \
+            throw ::shm::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " __FILE__ ":" + \
+                                   std::to_string(__LINE__));                                                \
+    } while (0)
+
+// Per-level constants of hybrid key switching with L data limbs.
+struct LevelKS {
+    uint32_t L = 0, beta = 0;
+    uint64_t *modup_scale = nullptr;  // [L][4]: N^-1 * qhat_i^-1 (digit-relative), for the INTT's last stage
+    uint64_t *modup_conv = nullptr;   // [beta][L+np][alpha]: qhat_i mod t_j (0 on the digit's own rows)
+};
+
+struct Context {
+    int device = 0;
+    uint32_t log_n = 0, n = 0, nq = 0, np = 0, dnum = 0;
+    std::vector<uint64_t> primes;       // nq + np
+    std::vector<PrimeConst> h_pc;       // host copy
+    PrimeConst *pc = nullptr;           // [QP]
+    uint64_t *tw = nullptr;             // [QP][4][N]
+    uint64_t *inv_scale_plain = nullptr;  // [QP][4]: N^-1 for a plain INTT, indexed by prime
+    uint64_t *moddown_scale = nullptr;  // [np][4]: N^-1 * phat_k^-1
+    uint64_t *moddown_conv = nullptr;   // [nq][np]: phat_k mod q_j
+    uint64_t *p_inv = nullptr;          // [nq][2]: P^-1 mod q_j and Shoup companion
+    uint64_t *rescale_inv = nullptr;    // [nq][nq][2]: q_{L-1}^-1 mod q_j (row L-1), Shoup
+    std::vector<LevelKS> ks;            // index L (1..nq)
+    std::map<uint32_t, uint32_t *> galois_perm;  // elt -> [N] permutation
+    std::mutex mu;
+
+    // internal arena for calls that pass no workspace
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
+
+    ~Context();
+    const uint32_t *perm(uint32_t elt);
+    void *workspace(size_t bytes);
+};
+
+Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uint32_t nq, uint32_t np, int device);
+
+// ---------------- launchers (all asynchronous on `st`) ----------------
+// NTT of `rows` limbs of N words; limb r uses prime map.prime[r % slots] (255 = skip).
+void ntt_forward(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                 cudaStream_t st);
+// Inverse NTT; `scale` is [slots - scale_base][4] (c, c', c*psi^-(N/2), shoup), or nullptr
+// for the plain N^-1 of each limb's prime.
+void ntt_inverse(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                 const uint64_t *scale, cudaStream_t st, uint32_t scale_base = 0);
+
+LimbMap q_map(uint32_t L);
+
+enum class EwOp { Add, Sub, Negate, MulPlain };
+void elementwise(const Context &c, EwOp op, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+                 uint32_t L, uint32_t b_polys, cudaStream_t st);
+void tensor(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_cts, uint32_t L,
+            cudaStream_t st);
+void apply_galois(const Context &c, const uint64_t *in, uint64_t *out, uint32_t rows, uint32_t elt, cudaStream_t st);
+void rescale(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *ws,
+             cudaStream_t st);
+size_t rescale_ws_words(const Context &c, uint32_t n_polys, uint32_t L);
+
+// Hybrid key switch of n_cts polynomials d (NTT form, [n_cts][L][N], stride d_stride words)
+// with key [dnum][2][QP][N].  out0/out1 ([n_cts][L][N], stride out_stride):
+//   out0 = add0 + cx0, out1 = add1 + cx1 (add0/add1 may be null meaning zero).
+struct KsOutput {
+    uint64_t *out0, *out1;
+    const uint64_t *add0, *add1;
+    size_t stride;  // words between consecutive ciphertexts for out/add
+};
+void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_cts, uint32_t L, const uint64_t *key,
+               const KsOutput &o, uint64_t *ws, cudaStream_t st);
+size_t keyswitch_ws_words(const Context &c, uint32_t n_cts, uint32_t L);
+
+void ctpt_matmul(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
+                 uint32_t L, uint64_t *ws, cudaStream_t st);
+size_t ctpt_ws_words(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);
+
+}  // namespace shm

@@ -1,0 +1,151 @@
+// Element-wise RNS kernels: add / sub / negate / multiply_plain, the 2x2 tensor
+// product, NTT-domain automorphisms and the floor rescale.
+//
+// Reference semantics: thirdparty/phantom-fhe/src/polymath.cu:17-230 (pointwise mod q),
+// :468-504 (tensor), src/galois.cu:8-21 (NTT-domain permutation),
+// src/rns.cu:1125-1181 (rescale = (c_j - NTT(c_last mod q_j)) * q_last^-1, floor).
+#include "core.hpp"
+
+namespace shm {
+
+namespace {
+
+constexpr int kEwThreads = 256;
+
+// Grid: (N/2/256 chunks) x rows; each thread handles 2 consecutive words of one limb.
+template <EwOp OP>
+__global__ void ew_kernel(const uint64_t *__restrict__ a, const uint64_t *__restrict__ b, uint64_t *__restrict__ out,
+                          uint32_t L, uint32_t log_n, uint32_t b_polys, const PrimeConst *__restrict__ pc) {
+    const uint32_t row = blockIdx.y;
+    const uint32_t limb = row % L;
+    const PrimeConst p = pc[limb];
+    const size_t off = ((size_t)row << log_n) + 2 * (blockIdx.x * kEwThreads + threadIdx.x);
+    const size_t boff = ((size_t)((row / L) % b_polys * L + limb) << log_n) + 2 * (blockIdx.x * kEwThreads + threadIdx.x);
+    ulonglong2 x = *reinterpret_cast<const ulonglong2 *>(a + off), r;
+    if constexpr (OP == EwOp::Negate) {
+        r.x = x.x ? p.q - x.x : 0;
+        r.y = x.y ? p.q - x.y : 0;
+    } else {
+        ulonglong2 y = *reinterpret_cast<const ulonglong2 *>(b + boff);
+        if constexpr (OP == EwOp::Add) {
+            r.x = add_mod(x.x, y.x, p.q);
+            r.y = add_mod(x.y, y.y, p.q);
+        } else if constexpr (OP == EwOp::Sub) {
+            r.x = sub_mod(x.x, y.x, p.q);
+            r.y = sub_mod(x.y, y.y, p.q);
+        } else {
+            r.x = mul_mod(x.x, y.x, p);
+            r.y = mul_mod(x.y, y.y, p);
+        }
+    }
+    *reinterpret_cast<ulonglong2 *>(out + off) = r;
+}
+
+// (a0, a1) x (b0, b1) -> (a0 b0, a0 b1 + a1 b0, a1 b1) per ciphertext
+__global__ void tensor_kernel(const uint64_t *__restrict__ a, const uint64_t *__restrict__ b, uint64_t *__restrict__ out,
+                              uint32_t L, uint32_t log_n, const PrimeConst *__restrict__ pc) {
+    const uint32_t limb = blockIdx.y, ct = blockIdx.z;
+    const PrimeConst p = pc[limb];
+    const size_t ln = (size_t)L << log_n;
+    const size_t k = ((size_t)limb << log_n) + blockIdx.x * kEwThreads + threadIdx.x;
+    const uint64_t *A = a + ct * 2 * ln, *B = b + ct * 2 * ln;
+    uint64_t *O = out + ct * 3 * ln;
+    uint64_t a0 = A[k], a1 = A[ln + k], b0 = B[k], b1 = B[ln + k];
+    O[k] = mul_mod(a0, b0, p);
+    u128 m = mul_wide(a0, b1);
+    mac(m, a1, b0);
+    O[ln + k] = barrett(m, p);
+    O[2 * ln + k] = mul_mod(a1, b1, p);
+}
+
+__global__ void galois_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ out,
+                              const uint32_t *__restrict__ perm, uint32_t log_n) {
+    const size_t row = blockIdx.y;
+    const uint32_t k = blockIdx.x * kEwThreads + threadIdx.x;
+    out[(row << log_n) + k] = in[(row << log_n) + __ldg(perm + k)];
+}
+
+// t_j = c_last mod q_j for j < L-1 (c_last already in coefficient form)
+__global__ void rescale_spread(const uint64_t *__restrict__ last, uint64_t *__restrict__ t, uint32_t L, uint32_t log_n,
+                               const PrimeConst *__restrict__ pc) {
+    const uint32_t j = blockIdx.y, poly = blockIdx.z;
+    const uint32_t k = blockIdx.x * kEwThreads + threadIdx.x;
+    const uint64_t v = last[((size_t)poly << log_n) + k];
+    t[(((size_t)poly * (L - 1) + j) << log_n) + k] = barrett({v, 0}, pc[j]);
+}
+
+// out_j = (c_j - t_j) * q_last^-1 mod q_j
+__global__ void rescale_combine(const uint64_t *__restrict__ in, const uint64_t *__restrict__ t,
+                                uint64_t *__restrict__ out, uint32_t L, uint32_t log_n,
+                                const PrimeConst *__restrict__ pc, const uint64_t *__restrict__ inv) {
+    const uint32_t j = blockIdx.y, poly = blockIdx.z;
+    const uint32_t k = blockIdx.x * kEwThreads + threadIdx.x;
+    const uint64_t q = pc[j].q, w = inv[2 * j], ws = inv[2 * j + 1];
+    const size_t o = (((size_t)poly * (L - 1) + j) << log_n) + k;
+    const uint64_t c = in[(((size_t)poly * L + j) << log_n) + k];
+    out[o] = shoup(sub_mod(c, t[o], q), w, ws, q);
+}
+
+// copy the last limb of every polynomial into a contiguous buffer
+__global__ void gather_last(const uint64_t *__restrict__ in, uint64_t *__restrict__ last, uint32_t L, uint32_t log_n) {
+    const uint32_t poly = blockIdx.y;
+    const uint32_t k = blockIdx.x * kEwThreads + threadIdx.x;
+    last[((size_t)poly << log_n) + k] = in[(((size_t)poly * L + L - 1) << log_n) + k];
+}
+
+}  // namespace
+
+void elementwise(const Context &c, EwOp op, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+                 uint32_t L, uint32_t b_polys, cudaStream_t st) {
+    if (n_polys == 0 || L == 0) return;
+    dim3 grid(c.n / 2 / kEwThreads, n_polys * L);
+    if (b_polys == 0) b_polys = n_polys;
+    switch (op) {
+        case EwOp::Add: SHM_LAUNCHED(1); ew_kernel<EwOp::Add><<<grid, kEwThreads, 0, st>>>(a, b, out, L, c.log_n, b_polys, c.pc); break;
+        case EwOp::Sub: SHM_LAUNCHED(1); ew_kernel<EwOp::Sub><<<grid, kEwThreads, 0, st>>>(a, b, out, L, c.log_n, b_polys, c.pc); break;
+        case EwOp::Negate:
+            SHM_LAUNCHED(1); ew_kernel<EwOp::Negate><<<grid, kEwThreads, 0, st>>>(a, b, out, L, c.log_n, b_polys, c.pc);
+            break;
+        case EwOp::MulPlain:
+            SHM_LAUNCHED(1); ew_kernel<EwOp::MulPlain><<<grid, kEwThreads, 0, st>>>(a, b, out, L, c.log_n, b_polys, c.pc);
+            break;
+    }
+    SHM_CUDA(cudaGetLastError());
+}
+
+void tensor(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_cts, uint32_t L,
+            cudaStream_t st) {
+    if (n_cts == 0) return;
+    SHM_LAUNCHED(1); tensor_kernel<<<dim3(c.n / kEwThreads, L, n_cts), kEwThreads, 0, st>>>(a, b, out, L, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+}
+
+void apply_galois(const Context &c, const uint64_t *in, uint64_t *out, uint32_t rows, uint32_t elt, cudaStream_t st) {
+    if (rows == 0) return;
+    const uint32_t *perm = const_cast<Context &>(c).perm(elt);
+    SHM_LAUNCHED(1); galois_kernel<<<dim3(c.n / kEwThreads, rows), kEwThreads, 0, st>>>(in, out, perm, c.log_n);
+    SHM_CUDA(cudaGetLastError());
+}
+
+size_t rescale_ws_words(const Context &c, uint32_t n_polys, uint32_t L) {
+    return (size_t)n_polys * L * c.n;  // last limbs (n_polys) + spread (n_polys * (L-1))
+}
+
+void rescale(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *ws,
+             cudaStream_t st) {
+    if (L < 2) throw std::invalid_argument("rescale needs at least two limbs");
+    uint64_t *last = ws, *t = ws + ((size_t)n_polys << c.log_n);
+    const uint32_t chunks = c.n / kEwThreads;
+    SHM_LAUNCHED(1); gather_last<<<dim3(chunks, n_polys), kEwThreads, 0, st>>>(in, last, L, c.log_n);
+    LimbMap m;
+    for (int i = 0; i < 512; i++) m.prime[i] = 255;
+    m.prime[0] = (uint8_t)(L - 1);
+    ntt_inverse(c, last, n_polys, 1, m, nullptr, st);
+    SHM_LAUNCHED(1); rescale_spread<<<dim3(chunks, L - 1, n_polys), kEwThreads, 0, st>>>(last, t, L, c.log_n, c.pc);
+    ntt_forward(c, t, n_polys * (L - 1), L - 1, q_map(L - 1), st);
+    SHM_LAUNCHED(1); rescale_combine<<<dim3(chunks, L - 1, n_polys), kEwThreads, 0, st>>>(in, t, out, L, c.log_n, c.pc,
+                                                                         c.rescale_inv + 2 * (size_t)(L - 1) * c.nq);
+    SHM_CUDA(cudaGetLastError());
+}
+
+}  // namespace shm

@@ -82,7 +82,11 @@ inline std::vector<uint64_t> create_primes(int log_n, const std::vector<int> &bi
     return out;
 }
 
-inline uint32_t bitrev(uint32_t x, int bits) { return bits ? __builtin_bitreverse32(x) >> (32 - bits) : 0; }
+inline uint32_t bitrev(uint32_t x, int bits) {
+    uint32_t r = 0;
+    for (int i = 0; i < bits; i++, x >>= 1) r = (r << 1) | (x & 1);
+    return r;
+}
 
 inline uint64_t minimal_root(uint64_t q, int log_n) {
     const uint64_t two_n = 2ull << log_n, n = 1ull << log_n;

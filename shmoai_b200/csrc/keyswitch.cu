@@ -1,0 +1,193 @@
+// Hybrid (dnum-digit) key switching for a batch of polynomials sharing one key.
+//
+// Reference semantics (bit-identical): thirdparty/phantom-fhe/src/eval_key_switch.cu:91-178
+//   ModUp     src/rns_bconv.cu:530-628: per digit b (limbs [b*alpha, min((b+1)*alpha, L))),
+//             y_i = INTT(d_i) * qhat_i^-1 mod q_i; every other limb t_j of QlP gets
+//             sum_i y_i * (qhat_i mod t_j) mod t_j (no correction term), then NTT;
+//             the digit's own limbs keep d_i unchanged.
+//   product   src/eval_key_switch.cu:12-66: cx_h[j] = sum_b up_b[j] * key_b[h][prime(j)].
+//   ModDown   src/rns_bconv.cu:776-828: z_k = INTT(cx_h[L+k]) * phat_k^-1,
+//             delta_j = NTT(sum_k z_k * (phat_k mod q_j)), out = (cx_h[j] - delta_j) * P^-1.
+//
+// Batch layout: the key is read once per coefficient for all n_cts polynomials
+// (the inner-product kernel loops over the batch with the key digits in registers).
+#include "core.hpp"
+
+namespace shm {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxAlpha = 16;
+constexpr int kMaxBeta = 16;
+
+// up[ct][b][j][k] for j outside digit b; digit rows copy d (NTT form).
+__global__ void modup_conv_kernel(const uint64_t *__restrict__ x, const uint64_t *__restrict__ d, size_t d_stride,
+                                  uint64_t *__restrict__ up, const uint64_t *__restrict__ conv, uint32_t L,
+                                  uint32_t np, uint32_t nq, uint32_t log_n, const PrimeConst *__restrict__ pc) {
+    __shared__ uint64_t s_conv[64 * kMaxAlpha];
+    const uint32_t b = blockIdx.y, ct = blockIdx.z;
+    const uint32_t alpha = np, LP = L + np, beta = gridDim.y;
+    const uint32_t s = b * alpha, e = min(s + alpha, L), na = e - s;
+    for (uint32_t i = threadIdx.x; i < LP * alpha; i += blockDim.x) s_conv[i] = conv[(size_t)b * LP * alpha + i];
+    __syncthreads();
+    const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
+    const size_t n = (size_t)1 << log_n;
+    uint64_t y[kMaxAlpha];
+    const uint64_t *xc = x + (size_t)ct * L * n;
+#pragma unroll
+    for (int i = 0; i < kMaxAlpha; i++)
+        if (i < (int)na) y[i] = xc[(size_t)(s + i) * n + k];
+    uint64_t *o = up + ((size_t)ct * beta + b) * LP * n;
+    const uint64_t *dc = d + (size_t)ct * d_stride;
+    for (uint32_t j = 0; j < LP; j++) {
+        if (j >= s && j < e) {
+            o[(size_t)j * n + k] = dc[(size_t)j * n + k];
+            continue;
+        }
+        const PrimeConst &p = pc[j < L ? j : nq + (j - L)];
+        const uint64_t *cj = s_conv + j * alpha;
+        u128 acc = {0, 0};
+#pragma unroll
+        for (int i = 0; i < kMaxAlpha; i++)
+            if (i < (int)na) mac(acc, y[i], cj[i]);
+        o[(size_t)j * n + k] = barrett(acc, p);
+    }
+}
+
+// acc[ct][h][j][k] = sum_b up[ct][b][j][k] * key[b][h][prime(j)][k]
+__global__ void inner_product_kernel(const uint64_t *__restrict__ up, const uint64_t *__restrict__ key,
+                                     uint64_t *__restrict__ acc, uint32_t n_cts, uint32_t L, uint32_t np, uint32_t nq,
+                                     uint32_t beta, uint32_t log_n, const PrimeConst *__restrict__ pc) {
+    const uint32_t j = blockIdx.y;
+    const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
+    const size_t n = (size_t)1 << log_n;
+    const uint32_t LP = L + np, QP = nq + np;
+    const uint32_t pj = j < L ? j : nq + (j - L);
+    const PrimeConst p = pc[pj];
+    uint64_t k0[kMaxBeta], k1[kMaxBeta];
+#pragma unroll
+    for (int b = 0; b < kMaxBeta; b++) {
+        if (b < (int)beta) {
+            const uint64_t *kb = key + (size_t)b * 2 * QP * n;
+            k0[b] = kb[(size_t)pj * n + k];
+            k1[b] = kb[((size_t)QP + pj) * n + k];
+        }
+    }
+    for (uint32_t ct = 0; ct < n_cts; ct++) {
+        const uint64_t *u = up + (size_t)ct * beta * LP * n + (size_t)j * n + k;
+        u128 a0 = {0, 0}, a1 = {0, 0};
+#pragma unroll
+        for (int b = 0; b < kMaxBeta; b++) {
+            if (b < (int)beta) {
+                uint64_t v = u[(size_t)b * LP * n];
+                mac(a0, v, k0[b]);
+                mac(a1, v, k1[b]);
+            }
+        }
+        uint64_t *o = acc + (size_t)ct * 2 * LP * n + (size_t)j * n + k;
+        o[0] = barrett(a0, p);
+        o[(size_t)LP * n] = barrett(a1, p);
+    }
+}
+
+// delta[ct][h][j][k] = sum_k' z[ct][h][L+k'][k] * (phat_k' mod q_j), j < L
+__global__ void moddown_conv_kernel(const uint64_t *__restrict__ acc, uint64_t *__restrict__ delta,
+                                    const uint64_t *__restrict__ conv, uint32_t L, uint32_t np, uint32_t log_n,
+                                    const PrimeConst *__restrict__ pc) {
+    const uint32_t hc = blockIdx.y;  // ct * 2 + h
+    const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
+    const size_t n = (size_t)1 << log_n;
+    const uint32_t LP = L + np;
+    const uint64_t *z = acc + (size_t)hc * LP * n + (size_t)L * n + k;
+    uint64_t zv[kMaxAlpha];
+#pragma unroll
+    for (int i = 0; i < kMaxAlpha; i++)
+        if (i < (int)np) zv[i] = z[(size_t)i * n];
+    uint64_t *o = delta + (size_t)hc * L * n + k;
+    for (uint32_t j = 0; j < L; j++) {
+        const uint64_t *cj = conv + (size_t)j * np;
+        u128 a = {0, 0};
+#pragma unroll
+        for (int i = 0; i < kMaxAlpha; i++)
+            if (i < (int)np) mac(a, zv[i], __ldg(cj + i));
+        o[(size_t)j * n] = barrett(a, pc[j]);
+    }
+}
+
+// out_h[j] = add_h[j] + (acc_h[j] - delta_h[j]) * P^-1
+__global__ void ks_combine_kernel(const uint64_t *__restrict__ acc, const uint64_t *__restrict__ delta, KsOutput o,
+                                  uint32_t L, uint32_t np, uint32_t log_n, const PrimeConst *__restrict__ pc,
+                                  const uint64_t *__restrict__ pinv) {
+    const uint32_t j = blockIdx.y, hc = blockIdx.z, ct = hc >> 1, h = hc & 1;
+    const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
+    const size_t n = (size_t)1 << log_n;
+    const uint64_t q = pc[j].q;
+    const uint64_t a = acc[((size_t)hc * (L + np) + j) * n + k];
+    const uint64_t dl = delta[((size_t)hc * L + j) * n + k];
+    uint64_t r = shoup(sub_mod(a, dl, q), pinv[2 * j], pinv[2 * j + 1], q);
+    const size_t off = (size_t)ct * o.stride + (size_t)j * n + k;
+    const uint64_t *add = h ? o.add1 : o.add0;
+    if (add) r = add_mod(r, add[off], q);
+    (h ? o.out1 : o.out0)[off] = r;
+}
+
+}  // namespace
+
+size_t keyswitch_ws_words(const Context &c, uint32_t n_cts, uint32_t L) {
+    const uint32_t beta = (L + c.np - 1) / c.np, LP = L + c.np;
+    return (size_t)n_cts * c.n * (L + (size_t)beta * LP + 2 * (size_t)LP);
+}
+
+void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_cts, uint32_t L, const uint64_t *key,
+               const KsOutput &o, uint64_t *ws, cudaStream_t st) {
+    if (n_cts == 0) return;
+    if (c.np == 0) throw std::invalid_argument("context has no special primes: key switching unavailable");
+    if (L < 1 || L > c.nq) throw std::invalid_argument("level out of range");
+    const uint32_t np = c.np, beta = (L + np - 1) / np, LP = L + np;
+    if (beta > c.dnum) throw std::invalid_argument("level needs more key digits than the key holds");
+    if (np > kMaxAlpha || beta > kMaxBeta || LP > 64) throw std::invalid_argument("key-switching shape too large");
+    const size_t n = c.n;
+    uint64_t *x = ws;                                   // [n_cts][L][N]
+    uint64_t *up = x + (size_t)n_cts * L * n;           // [n_cts][beta][LP][N]
+    uint64_t *acc = up + (size_t)n_cts * beta * LP * n; // [n_cts][2][LP][N]
+    uint64_t *delta = up;                               // reuses up: [n_cts][2][L][N]
+    const LevelKS &ks = c.ks[L];
+
+    // 1. coefficient form of every limb, scaled by the digit factor qhat_i^-1
+    SHM_CUDA(cudaMemcpy2DAsync(x, L * n * 8, d, d_stride * 8, L * n * 8, n_cts, cudaMemcpyDeviceToDevice, st));
+    ntt_inverse(c, x, n_cts * L, L, q_map(L), ks.modup_scale, st);
+    // 2. base conversion of each digit to the rest of QlP
+    SHM_LAUNCHED(1); modup_conv_kernel<<<dim3(n / kThreads, beta, n_cts), kThreads, 0, st>>>(x, d, d_stride, up, ks.modup_conv, L, np,
+                                                                            c.nq, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+    // 3. NTT of the converted limbs (digit rows are already NTT form)
+    LimbMap m;
+    for (uint32_t s = 0; s < 512; s++) {
+        if (s >= beta * LP) {
+            m.prime[s] = 255;
+            continue;
+        }
+        uint32_t b = s / LP, j = s % LP;
+        bool own = j >= b * np && j < std::min((b + 1) * np, L);
+        m.prime[s] = own ? 255 : (uint8_t)(j < L ? j : c.nq + (j - L));
+    }
+    ntt_forward(c, up, n_cts * beta * LP, beta * LP, m, st);
+    // 4. inner product with the key digits
+    SHM_LAUNCHED(1); inner_product_kernel<<<dim3(n / kThreads, LP), kThreads, 0, st>>>(up, key, acc, n_cts, L, np, c.nq, beta, c.log_n,
+                                                                      c.pc);
+    SHM_CUDA(cudaGetLastError());
+    // 5. ModDown: INTT of the P limbs (scaled by phat_k^-1), convert to Ql, NTT, combine
+    LimbMap mp;
+    for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
+    ntt_inverse(c, acc, n_cts * 2 * LP, LP, mp, c.moddown_scale, st, L);
+    SHM_LAUNCHED(1); moddown_conv_kernel<<<dim3(n / kThreads, n_cts * 2), kThreads, 0, st>>>(acc, delta, c.moddown_conv, L, np,
+                                                                            c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+    ntt_forward(c, delta, n_cts * 2 * L, L, q_map(L), st);
+    SHM_LAUNCHED(1); ks_combine_kernel<<<dim3(n / kThreads, L, n_cts * 2), kThreads, 0, st>>>(acc, delta, o, L, np, c.log_n, c.pc,
+                                                                             c.p_inv);
+    SHM_CUDA(cudaGetLastError());
+}
+
+}  // namespace shm

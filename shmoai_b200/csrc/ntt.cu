@@ -1,0 +1,213 @@
+// Batched NTT / INTT kernels (see ntt.cuh for the decomposition).
+#include "core.hpp"
+
+namespace shm {
+
+namespace {
+
+template <int R>
+struct Geo {
+    static constexpr int LOGM = 2 * R;
+    static constexpr uint32_t M = 1u << LOGM;  // sub-transform length
+    static constexpr int LOGN = 2 * LOGM;
+    static constexpr uint32_t N = 1u << LOGN;
+    static constexpr int E = 1 << R;  // elements per thread
+    static constexpr uint32_t THREADS = kNttSubs * E;
+    static constexpr uint32_t CHUNKS = M / kNttSubs;  // CTAs per limb
+    static constexpr uint32_t PAD_M = M + M / 16;     // padded block row in shared memory
+};
+
+__device__ __forceinline__ uint32_t padded(uint32_t p) { return p + (p >> 4); }
+
+// ---------------- forward, phase 1: columns (global stages 0 .. LOGM-1)
+template <int R>
+__global__ void __launch_bounds__(Geo<R>::THREADS) fwd_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+                                                            const uint64_t *__restrict__ tw,
+                                                            const PrimeConst *__restrict__ pc) {
+    using G = Geo<R>;
+    __shared__ uint64_t sm[G::M * kNttSubs];
+    const uint32_t row = blockIdx.x / G::CHUNKS, chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t pidx = map.prime[row % slots];
+    if (pidx == 255) return;
+    const uint64_t q = pc[pidx].q;
+    const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN), *ws = w + G::N;
+    uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * kNttSubs;
+    const uint32_t sig = threadIdx.x % kNttSubs, lane = threadIdx.x / kNttSubs;
+
+    uint64_t a[G::E];
+#pragma unroll
+    for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane + m * G::E)];
+    fwd_pass<R>(a, w, ws, 1, 0, 0, q);
+#pragma unroll
+    for (int m = 0; m < G::E; m++) sm[(lane + m * G::E) * kNttSubs + sig] = a[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < G::E; m++) a[m] = sm[(lane * G::E + m) * kNttSubs + sig];
+    fwd_pass<R>(a, w, ws, 1, R, lane, q);
+#pragma unroll
+    for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane * G::E + m)] = a[m];
+}
+
+// ---------------- forward, phase 2: blocks (global stages LOGM .. 2*LOGM-1), fully reduced output
+template <int R>
+__global__ void __launch_bounds__(Geo<R>::THREADS) fwd_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+                                                            const uint64_t *__restrict__ tw,
+                                                            const PrimeConst *__restrict__ pc) {
+    using G = Geo<R>;
+    __shared__ uint64_t sm[kNttSubs * G::PAD_M];
+    const uint32_t row = blockIdx.x / G::CHUNKS, chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t pidx = map.prime[row % slots];
+    if (pidx == 255) return;
+    const uint64_t q = pc[pidx].q;
+    const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN), *ws = w + G::N;
+    uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * kNttSubs * G::M;
+    const uint32_t sig = threadIdx.x / G::E, lane = threadIdx.x % G::E;
+    const uint32_t b = chunk * kNttSubs + sig;
+    uint64_t *x = xc + (size_t)sig * G::M;
+    uint64_t *s = sm + sig * G::PAD_M;
+
+    uint64_t a[G::E];
+#pragma unroll
+    for (int m = 0; m < G::E; m++) a[m] = x[lane + m * G::E];
+    fwd_pass<R>(a, w, ws, G::M + b, 0, 0, q);
+#pragma unroll
+    for (int m = 0; m < G::E; m++) s[padded(lane + m * G::E)] = a[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
+    fwd_pass<R>(a, w, ws, G::M + b, R, lane, q);
+    const uint64_t q2 = 2 * q;
+#pragma unroll
+    for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = csub(csub(a[m], q2), q);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < G::E; i++) {
+        uint32_t e = threadIdx.x + i * G::THREADS;
+        xc[e] = sm[(e / G::M) * G::PAD_M + padded(e % G::M)];
+    }
+}
+
+// ---------------- inverse, phase 1: blocks (global stages 2*LOGM-1 .. LOGM)
+template <int R>
+__global__ void __launch_bounds__(Geo<R>::THREADS) inv_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+                                                            const uint64_t *__restrict__ tw,
+                                                            const PrimeConst *__restrict__ pc) {
+    using G = Geo<R>;
+    __shared__ uint64_t sm[kNttSubs * G::PAD_M];
+    const uint32_t row = blockIdx.x / G::CHUNKS, chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t pidx = map.prime[row % slots];
+    if (pidx == 255) return;
+    const uint64_t q = pc[pidx].q;
+    const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN) + 2 * G::N, *ws = w + G::N;
+    uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * kNttSubs * G::M;
+    const uint32_t sig = threadIdx.x / G::E, lane = threadIdx.x % G::E;
+    const uint32_t b = chunk * kNttSubs + sig;
+    uint64_t *s = sm + sig * G::PAD_M;
+
+#pragma unroll
+    for (int i = 0; i < G::E; i++) {
+        uint32_t e = threadIdx.x + i * G::THREADS;
+        sm[(e / G::M) * G::PAD_M + padded(e % G::M)] = xc[e];
+    }
+    __syncthreads();
+    uint64_t a[G::E];
+#pragma unroll
+    for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
+    inv_pass<R>(a, w, ws, G::M + b, R, lane, q, 0);
+#pragma unroll
+    for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = a[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < G::E; m++) a[m] = s[padded(lane + m * G::E)];
+    inv_pass<R>(a, w, ws, G::M + b, 0, 0, q, 0);
+    uint64_t *x = xc + (size_t)sig * G::M;
+#pragma unroll
+    for (int m = 0; m < G::E; m++) x[lane + m * G::E] = a[m];
+}
+
+// ---------------- inverse, phase 2: columns (global stages LOGM-1 .. 0) with the folded scale
+template <int R>
+__global__ void __launch_bounds__(Geo<R>::THREADS) inv_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+                                                            const uint64_t *__restrict__ tw,
+                                                            const PrimeConst *__restrict__ pc,
+                                                            const uint64_t *__restrict__ scale, int scale_by_prime,
+                                                            uint32_t scale_base) {
+    using G = Geo<R>;
+    __shared__ uint64_t sm[G::M * kNttSubs];
+    const uint32_t row = blockIdx.x / G::CHUNKS, chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t slot = row % slots;
+    const uint32_t pidx = map.prime[slot];
+    if (pidx == 255) return;
+    const uint64_t q = pc[pidx].q;
+    const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN) + 2 * G::N, *ws = w + G::N;
+    const uint64_t *sc = scale + 4 * (scale_by_prime ? pidx : slot - scale_base);
+    uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * kNttSubs;
+    const uint32_t sig = threadIdx.x % kNttSubs, lane = threadIdx.x / kNttSubs;
+
+    uint64_t a[G::E];
+#pragma unroll
+    for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane * G::E + m)];
+    inv_pass<R>(a, w, ws, 1, R, lane, q, 0);
+#pragma unroll
+    for (int m = 0; m < G::E; m++) sm[(lane * G::E + m) * kNttSubs + sig] = a[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < G::E; m++) a[m] = sm[(lane + m * G::E) * kNttSubs + sig];
+    inv_pass<R>(a, w, ws, 1, 0, 0, q, 1);
+    const uint64_t c0 = sc[0], c0s = sc[1], c1 = sc[2], c1s = sc[3], q2 = 2 * q;
+#pragma unroll
+    for (int m = 0; m < G::E / 2; m++) {
+        uint64_t u = a[m], v = a[m + G::E / 2];
+        a[m] = shoup(u + v, c0, c0s, q);
+        a[m + G::E / 2] = shoup(u - v + q2, c1, c1s, q);
+    }
+#pragma unroll
+    for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane + m * G::E)] = a[m];
+}
+
+template <int R>
+void launch_fwd(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                cudaStream_t st) {
+    using G = Geo<R>;
+    dim3 grid(rows * G::CHUNKS);
+    SHM_LAUNCHED(1); fwd_col<R><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+    SHM_LAUNCHED(1); fwd_blk<R><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+}
+
+template <int R>
+void launch_inv(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                const uint64_t *scale, uint32_t scale_base, cudaStream_t st) {
+    using G = Geo<R>;
+    dim3 grid(rows * G::CHUNKS);
+    SHM_LAUNCHED(1); inv_blk<R><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+    SHM_LAUNCHED(1); inv_col<R><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, scale ? scale : c.inv_scale_plain,
+                                           scale ? 0 : 1, scale_base);
+}
+
+}  // namespace
+
+LimbMap q_map(uint32_t L) {
+    LimbMap m;
+    for (int i = 0; i < 512; i++) m.prime[i] = (uint32_t)i < L ? (uint8_t)i : 255;
+    return m;
+}
+
+void ntt_forward(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                 cudaStream_t st) {
+    if (rows == 0) return;
+    if (c.log_n == 16) launch_fwd<4>(c, data, rows, slots, map, st);
+    else if (c.log_n == 12) launch_fwd<3>(c, data, rows, slots, map, st);
+    else throw std::invalid_argument("NTT supports N = 2^12 and 2^16");
+    SHM_CUDA(cudaGetLastError());
+}
+
+void ntt_inverse(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                 const uint64_t *scale, cudaStream_t st, uint32_t scale_base) {
+    if (rows == 0) return;
+    if (c.log_n == 16) launch_inv<4>(c, data, rows, slots, map, scale, scale_base, st);
+    else if (c.log_n == 12) launch_inv<3>(c, data, rows, slots, map, scale, scale_base, st);
+    else throw std::invalid_argument("NTT supports N = 2^12 and 2^16");
+    SHM_CUDA(cudaGetLastError());
+}
+
+}  // namespace shm

@@ -26,7 +26,7 @@ namespace shm {
 constexpr int kNttSubs = 16;  // columns / blocks per CTA
 
 struct LimbMap {
-    uint8_t prime[256];  // limb slot within a polynomial -> prime index; 255 = leave untouched
+    uint8_t prime[512];  // limb slot within a polynomial -> prime index; 255 = leave untouched
 };
 
 // scale constants of the inverse's last stage, per limb slot: c, c', c*psi^-(N/2), (c*psi^-(N/2))'
