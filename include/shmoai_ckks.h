@@ -115,6 +115,32 @@ uint32_t shm_galois_elt_from_step(const shm_context *ctx, int step);
 int shm_rotate(const shm_context *ctx, const uint64_t *ct, int step, const uint64_t *galois_key, uint64_t *out,
                uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
 
+/* out = a * s (per-limb scalar residues s[0..L), host array) over n_polys polynomials.
+ * Replaces multiply_const_inplace's constant multiply (ckks_evaluator_parallel.cuh:245-262;
+ * a constant plaintext in NTT form is one residue per limb). */
+int shm_multiply_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *scalars, uint64_t *out,
+                        uint32_t n_polys, uint32_t L, void *stream);
+/* c0 of each of n_cts ciphertexts gets + s[limb]; c1 is copied.
+ * Replaces add_const_inplace (ckks_evaluator_parallel.cuh:263-280). */
+int shm_add_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *scalars, uint64_t *out,
+                   uint32_t n_cts, uint32_t L, void *stream);
+/* out (+)= sum_t X[t] * P[t] over k terms: X[t] are [n_polys][L][N] device
+ * buffers, P[t] are [L][N] plaintexts (host arrays of device pointers).
+ * Replaces the per-diagonal multiply_plain + add_inplace inner loop of
+ * Bootstrapper::bsgs_linear_transform (src/include/source/bootstrapping/Bootstrapper.cu:2168-2340). */
+int shm_multiply_plain_accumulate(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
+                                  uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
+                                  void *stream);
+/* Mod-raise n_polys one-limb polynomials (mod q0, NTT form) to L limbs by the
+ * centred lift.  Replaces Bootstrapper::modraise_inplace (Bootstrapper.cu:3271-3356). */
+size_t shm_modraise_workspace_bytes(const shm_context *ctx, uint32_t n_polys);
+int shm_modraise(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                 void *workspace, size_t workspace_bytes, void *stream);
+/* Keep the first L_out of L_in limbs of n_polys polynomials (modulus drop without
+ * rescale).  Replaces mod_switch_drop_to_next / mod_switch_to_inplace (evaluate.cu:1445-1520). */
+int shm_drop_limbs(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L_in,
+                   uint32_t L_out, void *stream);
+
 /* Rotation-free ct-pt matmul: Y[o] = sum_i X[i] * W[i][o] over n_in input
  * ciphertexts X [n_in][2][L][N] and signed integer weights W [n_in][n_out]
  * (the encoded constants round(w * scale)); Y is [n_out][2][L][N] before the

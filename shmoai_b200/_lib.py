@@ -53,6 +53,13 @@ def _declare(L):
         "shm_apply_galois": (ctypes.c_int, [_P, _P, _U32, _P, _P, _U32, _U32, _P, _SZ, _P]),
         "shm_galois_elt_from_step": (_U32, [_P, ctypes.c_int]),
         "shm_rotate": (ctypes.c_int, [_P, _P, ctypes.c_int, _P, _P, _U32, _U32, _P, _SZ, _P]),
+        "shm_multiply_scalar": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint64), _P, _U32, _U32, _P]),
+        "shm_add_scalar": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint64), _P, _U32, _U32, _P]),
+        "shm_multiply_plain_accumulate": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _U32, _P, _U32,
+                                                         _U32, ctypes.c_int, _P]),
+        "shm_modraise_workspace_bytes": (_SZ, [_P, _U32]),
+        "shm_modraise": (ctypes.c_int, [_P, _P, _P, _U32, _U32, _P, _SZ, _P]),
+        "shm_drop_limbs": (ctypes.c_int, [_P, _P, _P, _U32, _U32, _U32, _P]),
         "shm_ctpt_matmul_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),
         "shm_ctpt_matmul": (ctypes.c_int, [_P, _P, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
     }

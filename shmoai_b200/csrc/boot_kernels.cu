@@ -1,0 +1,114 @@
+// Kernels used by the bootstrapping pipeline and the scale-exact evaluator:
+// per-limb scalar multiply / add, multiply-plain-accumulate (the inner sums of
+// the baby-step giant-step linear transforms), the mod-raise lift and the
+// limb drop.
+//
+// Reference counterparts: multiply_const / add_const in the moai adapter
+// (src/include/source/ckks_evaluator_parallel.cuh:245-280), the per-diagonal
+// multiply_plain + add_inplace of Bootstrapper::bsgs_linear_transform
+// (src/include/source/bootstrapping/Bootstrapper.cu:2168-2340) and
+// Bootstrapper::modraise_inplace (Bootstrapper.cu:3271-3356: centred lift of
+// the q0 limb into every prime).
+#include "core.hpp"
+
+namespace shm {
+
+namespace {
+
+constexpr int kT = 256;
+
+// out[row] = a[row] * s[limb] (Shoup), rows = n_polys * L
+__global__ void mul_scalar_kernel(const uint64_t *__restrict__ a, uint64_t *__restrict__ out, ScalarTab s, uint32_t L,
+                                  uint32_t log_n, const PrimeConst *__restrict__ pc) {
+    const uint32_t row = blockIdx.y, limb = row % L;
+    const uint64_t q = pc[limb].q, w = s.v[limb], ws = s.shoup[limb];
+    const size_t off = ((size_t)row << log_n) + 2 * (blockIdx.x * kT + threadIdx.x);
+    ulonglong2 x = *reinterpret_cast<const ulonglong2 *>(a + off);
+    x.x = shoup(x.x, w, ws, q);
+    x.y = shoup(x.y, w, ws, q);
+    *reinterpret_cast<ulonglong2 *>(out + off) = x;
+}
+
+// c0 rows of every ciphertext get + s[limb]; c1 rows are copied
+__global__ void add_scalar_kernel(const uint64_t *__restrict__ a, uint64_t *__restrict__ out, ScalarTab s, uint32_t L,
+                                  uint32_t log_n, const PrimeConst *__restrict__ pc) {
+    const uint32_t row = blockIdx.y, limb = row % L, poly = (row / L) & 1;
+    const size_t off = ((size_t)row << log_n) + 2 * (blockIdx.x * kT + threadIdx.x);
+    ulonglong2 x = *reinterpret_cast<const ulonglong2 *>(a + off);
+    if (poly == 0) {
+        const uint64_t q = pc[limb].q, c = s.v[limb];
+        x.x = add_mod(x.x, c, q);
+        x.y = add_mod(x.y, c, q);
+    }
+    *reinterpret_cast<ulonglong2 *>(out + off) = x;
+}
+
+// out[c] = sum_t X_t[c] * P_t   over k terms (X_t: [n_polys][L][N], P_t: [L][N])
+__global__ void mul_plain_acc_kernel(PtrTab X, PtrTab P, uint32_t k, uint64_t *__restrict__ out, uint32_t L,
+                                     uint32_t log_n, const PrimeConst *__restrict__ pc, int accumulate) {
+    const uint32_t row = blockIdx.y, limb = row % L;
+    const PrimeConst p = pc[limb];
+    const size_t off = ((size_t)row << log_n) + blockIdx.x * kT + threadIdx.x;
+    const size_t poff = ((size_t)limb << log_n) + blockIdx.x * kT + threadIdx.x;
+    u128 acc = {0, 0};
+    for (uint32_t t = 0; t < k; t++) mac(acc, X.p[t][off], P.p[t][poff]);
+    uint64_t r = barrett(acc, p);
+    if (accumulate) r = add_mod(r, out[off], p.q);
+    out[off] = r;
+}
+
+// t_j = centred lift of c (mod q0) into prime j, for j < L
+__global__ void modraise_spread(const uint64_t *__restrict__ c0, uint64_t *__restrict__ out, uint32_t L,
+                                uint32_t log_n, const PrimeConst *__restrict__ pc) {
+    const uint32_t j = blockIdx.y, poly = blockIdx.z;
+    const uint32_t k = blockIdx.x * kT + threadIdx.x;
+    const uint64_t q0 = pc[0].q;
+    const uint64_t v = c0[((size_t)poly << log_n) + k];
+    const PrimeConst p = pc[j];
+    uint64_t r = barrett({v, 0}, p);
+    if (v > (q0 >> 1)) r = sub_mod(r, barrett({q0, 0}, p), p.q);
+    out[(((size_t)poly * L + j) << log_n) + k] = r;
+}
+
+}  // namespace
+
+void mul_scalar(const Context &c, const uint64_t *a, uint64_t *out, const ScalarTab &s, uint32_t n_polys, uint32_t L,
+                cudaStream_t st) {
+    if (!n_polys) return;
+    SHM_LAUNCHED(1);
+    mul_scalar_kernel<<<dim3(c.n / 2 / kT, n_polys * L), kT, 0, st>>>(a, out, s, L, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+}
+
+void add_scalar(const Context &c, const uint64_t *a, uint64_t *out, const ScalarTab &s, uint32_t n_cts, uint32_t L,
+                cudaStream_t st) {
+    if (!n_cts) return;
+    SHM_LAUNCHED(1);
+    add_scalar_kernel<<<dim3(c.n / 2 / kT, n_cts * 2 * L), kT, 0, st>>>(a, out, s, L, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+}
+
+void mul_plain_acc(const Context &c, const PtrTab &X, const PtrTab &P, uint32_t k, uint64_t *out, uint32_t n_polys,
+                   uint32_t L, bool accumulate, cudaStream_t st) {
+    if (!n_polys || !k) return;
+    SHM_LAUNCHED(1);
+    mul_plain_acc_kernel<<<dim3(c.n / kT, n_polys * L), kT, 0, st>>>(X, P, k, out, L, c.log_n, c.pc,
+                                                                      accumulate ? 1 : 0);
+    SHM_CUDA(cudaGetLastError());
+}
+
+void modraise(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *ws,
+              cudaStream_t st) {
+    // limb 0 of each polynomial (already contiguous when the input has one limb)
+    SHM_CUDA(cudaMemcpyAsync(ws, in, (size_t)n_polys * c.n * 8, cudaMemcpyDeviceToDevice, st));
+    LimbMap m;
+    for (int i = 0; i < 512; i++) m.prime[i] = 255;
+    m.prime[0] = 0;
+    ntt_inverse(c, ws, n_polys, 1, m, nullptr, st);
+    SHM_LAUNCHED(1);
+    modraise_spread<<<dim3(c.n / kT, L, n_polys), kT, 0, st>>>(ws, out, L, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+    ntt_forward(c, out, n_polys * L, L, q_map(L), st);
+}
+
+}  // namespace shm

@@ -210,8 +210,10 @@ shm::Context &ctx_of(const shm_context *h) {
 
 cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Element-wise operations and NTTs accept key-level polynomials (all nq + np primes);
+// level-changing operations check L <= nq themselves.
 void check_level(const shm::Context &c, uint32_t L) {
-    if (L < 1 || L > c.nq) throw std::invalid_argument("level (limb count) out of range");
+    if (L < 1 || L > c.nq + c.np) throw std::invalid_argument("level (limb count) out of range");
 }
 
 uint64_t *ws_of(shm::Context &c, void *ws, size_t have, size_t need_words) {
@@ -340,7 +342,7 @@ int shm_rescale(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint3
     return guard([&] {
         auto &c = const_cast<shm::Context &>(ctx_of(ctx));
         check_level(c, L);
-        if (L < 2) throw std::invalid_argument("rescale needs at least two limbs");
+        if (L < 2 || L > c.nq) throw std::invalid_argument("rescale needs 2 <= L <= n_q limbs");
         set_device(c);
         uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::rescale_ws_words(c, n_polys, L));
         shm::rescale(c, in, out, n_polys, L, ws, S(stream));
@@ -426,6 +428,94 @@ int shm_rotate(const shm_context *ctx, const uint64_t *ct, int step, const uint6
         return SHM_EINVAL;
     }
     return shm_apply_galois(ctx, ct, elt, galois_key, out, n_cts, L, workspace, workspace_bytes, stream);
+}
+
+static shm::ScalarTab scalar_tab(const shm::Context &c, const uint64_t *scalars, uint32_t L) {
+    if (!scalars) throw std::invalid_argument("null scalars");
+    if (L > 64) throw std::invalid_argument("at most 64 limbs for scalar operations");
+    shm::ScalarTab s{};
+    for (uint32_t i = 0; i < L; i++) {
+        uint64_t q = c.primes[i];
+        if (scalars[i] >= q) throw std::invalid_argument("scalar residue must be below its prime");
+        s.v[i] = scalars[i];
+        s.shoup[i] = shm::host::shoup_of(scalars[i], q);
+    }
+    return s;
+}
+
+int shm_multiply_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *scalars, uint64_t *out,
+                        uint32_t n_polys, uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::mul_scalar(c, a, out, scalar_tab(c, scalars, L), n_polys, L, S(stream));
+    });
+}
+
+int shm_add_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *scalars, uint64_t *out,
+                   uint32_t n_cts, uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::add_scalar(c, a, out, scalar_tab(c, scalars, L), n_cts, L, S(stream));
+    });
+}
+
+int shm_multiply_plain_accumulate(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
+                                  uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
+                                  void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        if (!X || !P) throw std::invalid_argument("null term arrays");
+        set_device(c);
+        // sum of `chunk` products must stay below the Barrett bound 2^(63 + bits(q))
+        uint32_t chunk = shm::kMaxAccTerms;
+        for (uint32_t i = 0; i < L; i++) {
+            int b = shm::host::bit_length(c.primes[i]);
+            uint32_t lim = 2 * b >= 63 + b ? 1u : (63 + b - 2 * b >= 5 ? 32u : (1u << (63 + b - 2 * b)));
+            chunk = std::min(chunk, lim);
+        }
+        for (uint32_t t0 = 0; t0 < k; t0 += chunk) {
+            uint32_t kk = std::min(chunk, k - t0);
+            shm::PtrTab x{}, p{};
+            for (uint32_t t = 0; t < kk; t++) {
+                x.p[t] = X[t0 + t];
+                p.p[t] = P[t0 + t];
+            }
+            shm::mul_plain_acc(c, x, p, kk, out, n_polys, L, accumulate || t0 > 0, S(stream));
+        }
+    });
+}
+
+size_t shm_modraise_workspace_bytes(const shm_context *ctx, uint32_t n_polys) {
+    return ctx && ctx->c ? (size_t)n_polys * ctx->c->n * 8 : 0;
+}
+
+int shm_modraise(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                 void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, (size_t)n_polys * c.n);
+        shm::modraise(c, in, out, n_polys, L, ws, S(stream));
+    });
+}
+
+int shm_drop_limbs(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L_in,
+                   uint32_t L_out, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L_in);
+        if (L_out < 1 || L_out > L_in) throw std::invalid_argument("L_out must be in [1, L_in]");
+        set_device(c);
+        const size_t n = c.n;
+        SHM_CUDA(cudaMemcpy2DAsync(out, L_out * n * 8, in, L_in * n * 8, L_out * n * 8, n_polys,
+                                   cudaMemcpyDeviceToDevice, S(stream)));
+    });
 }
 
 size_t shm_ctpt_matmul_workspace_bytes(const shm_context *ctx, uint32_t n_in, uint32_t n_out, uint32_t L) {

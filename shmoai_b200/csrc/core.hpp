@@ -99,6 +99,24 @@ void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_
                const KsOutput &o, uint64_t *ws, cudaStream_t st);
 size_t keyswitch_ws_words(const Context &c, uint32_t n_cts, uint32_t L);
 
+// per-limb scalars passed by value (residue and Shoup companion per limb)
+struct ScalarTab {
+    uint64_t v[64], shoup[64];
+};
+constexpr int kMaxAccTerms = 32;
+struct PtrTab {
+    const uint64_t *p[kMaxAccTerms];
+};
+void mul_scalar(const Context &c, const uint64_t *a, uint64_t *out, const ScalarTab &s, uint32_t n_polys, uint32_t L,
+                cudaStream_t st);
+void add_scalar(const Context &c, const uint64_t *a, uint64_t *out, const ScalarTab &s, uint32_t n_cts, uint32_t L,
+                cudaStream_t st);
+void mul_plain_acc(const Context &c, const PtrTab &X, const PtrTab &P, uint32_t k, uint64_t *out, uint32_t n_polys,
+                   uint32_t L, bool accumulate, cudaStream_t st);
+// one-limb polynomials (mod q0, NTT form) -> L-limb centred lift (NTT form); ws: n_polys * N words
+void modraise(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *ws,
+              cudaStream_t st);
+
 void ctpt_matmul(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
                  uint32_t L, uint64_t *ws, cudaStream_t st);
 size_t ctpt_ws_words(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);

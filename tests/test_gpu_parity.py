@@ -152,9 +152,11 @@ def test_errors_are_reported_not_thrown():
 
     g = GoldenSet("tiny")
     ctx = CKKSContext(g.log_n, primes=g.primes, n_special=g.np)
-    t = torch.zeros(2, g.L + 1, g.n, dtype=torch.int64, device="cuda")
+    t = torch.zeros(2, g.nq + g.np + 1, g.n, dtype=torch.int64, device="cuda")
     with pytest.raises(ShmError):
         ctx.ntt_forward_(t)  # more limbs than the chain holds
+    with pytest.raises(ShmError):
+        ctx.rescale(torch.zeros(2, g.nq + 1, g.n, dtype=torch.int64, device="cuda"))  # key level
     with pytest.raises(ValueError):
         ctx.galois_elt(g.n)  # step too large
     ctx.close()
