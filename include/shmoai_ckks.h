@@ -90,6 +90,22 @@ size_t shm_rescale_workspace_bytes(const shm_context *ctx, uint32_t n_polys, uin
 int shm_rescale(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
                 void *workspace, size_t workspace_bytes, void *stream);
 
+/* Rescale that allocates nothing: the same computation and result as
+ * shm_rescale, for callers that cannot call cudaMalloc (hosts whose own pool
+ * owns all device memory, latency-critical paths that cannot take cudaMalloc's
+ * implicit synchronisation, FFI callers without a device allocator).  Scratch
+ * comes from a fixed 32 MiB device array inside the library, which every GPU
+ * that loads the library holds until exit; requests needing more than
+ * shm_rescale_noalloc_max_words() words (n_polys * L * N) fail with SHM_EINVAL.
+ * The first call on a device looks up the array's device address (make that
+ * first call before any stream capture).  All calls share the one array, so
+ * calls that overlap on the GPU (other streams, other threads) race; the array
+ * needs no clearing (every call overwrites what it reads).
+ * No counterpart in the reference: its rescale allocates per call. */
+size_t shm_rescale_noalloc_max_words(void);
+int shm_rescale_noalloc(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                        void *stream);
+
 /* Key switch of n_cts polynomials d [n_cts][L][N]: out (a [n_cts][2][L][N] buffer)
  * receives (cx0, cx1).  Replaces keyswitch_inplace's modup / inner product /
  * moddown (src/eval_key_switch.cu:91-178). */

@@ -534,3 +534,55 @@ int shm_ctpt_matmul(const shm_context *ctx, const uint64_t *X, const int64_t *W,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Rescale for callers that cannot allocate device memory.
+//
+// Some hosts own every byte of device memory through their own pool and forbid
+// direct cudaMalloc (a serving runtime with a fixed memory budget), some cannot
+// afford cudaMalloc's implicit device-wide synchronisation on a latency-critical
+// path, and some FFI callers have no device allocator binding at all.  For them
+// shm_rescale_noalloc runs the same rescale as shm_rescale but takes its scratch
+// from the fixed array below instead of a caller workspace or the context arena.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB, held by every GPU that loads the library
+static __device__ __align__(256) uint64_t g_noalloc_scratch[kNoAllocScratchBytes / 8];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint64_t *g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of the scratch array on `device` (which must be current).  The
+// host-side symbol g_noalloc_scratch is only a stand-in and must never be passed
+// to a kernel; the address comes from cudaGetSymbolAddress, once per device.
+uint64_t *noalloc_scratch(int device) {
+    if (device < 0 || device >= kMaxDevices) throw std::invalid_argument("device index out of range");
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void *p = nullptr;
+        SHM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[device] = static_cast<uint64_t *>(p);
+    }
+    return g_noalloc_addr[device];
+}
+
+}  // namespace
+
+extern "C" size_t shm_rescale_noalloc_max_words(void) { return kNoAllocScratchBytes / 8; }
+
+extern "C" int shm_rescale_noalloc(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys,
+                                   uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        if (L < 2 || L > c.nq) throw std::invalid_argument("rescale needs 2 <= L <= n_q limbs");
+        const size_t need = shm::rescale_ws_words(c, n_polys, L);
+        if (need > kNoAllocScratchBytes / 8)
+            throw std::invalid_argument("shm_rescale_noalloc: n_polys * L * N exceeds the fixed scratch of " +
+                                        std::to_string(kNoAllocScratchBytes / 8) + " words (32 MiB)");
+        set_device(c);
+        shm::rescale(c, in, out, n_polys, L, noalloc_scratch(c.device), S(stream));
+    });
+}
