@@ -1,22 +1,28 @@
 """Benchmark of the CKKS evaluator hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload prim|ctpt]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload boot|prim] [--batch B]
 
-One JSON line on rank 0.  Workloads (all synthetic, seeded; RLWE ciphertexts are
-uniform residues, so random limbs have the cost profile of real ones):
+Prints one JSON line on rank 0.  Workloads (synthetic, seeded):
 
-  prim  config-1 primitive chain on one ciphertext, N = 2^16, Q = [60] + 23x[50],
-        P = 8x[60] (dnum 3): inverse+forward NTT of all limbs, HRotate by one slot,
+  boot  (default; the headline metric) S2C-first bootstrapping, reference
+        parameters N = 2^16, Q = [51] + 20x[46] + 14x[51], P = 5x[51] (dnum 7),
+        Delta = 2^46, h = 192, inputs at 4 primes with 2^15 slots uniform in
+        [-1, 1]^2.  One step = one batch of B ciphertexts (default 32; the
+        768-ciphertext job of the reference is 24 such steps).  Unit: bootstraps/s.
+        The decryption error of the last batch is reported beside the speed.
+  prim  config-1 chain on one ciphertext (N = 2^16, Q = [60] + 23x[50], P = 8x[60],
+        dnum 3): inverse+forward NTT of all limbs, HRotate by one slot,
         multiply + relinearize + rescale.  Unit: chains/s.
 
-Multi-GPU: ciphertexts are independent, so every rank runs its own replica of
-the step (weak scaling, no data-path collective); the step time is the max
-over ranks.
+Multi-GPU: ciphertexts are independent, so each rank bootstraps its own batch
+(weak scaling, no data-path collective); the step time is the max over ranks.
 
---impl reference times the reference's CPU path for the same workload: the
-reference has no CPU implementation of these operations, so this is the CPU
-oracle (oracle/ckks_oracle.c, a scalar OpenMP restatement of the reference's
-arithmetic), run on all host cores, one chain per step.
+--impl reference: the reference has no CPU implementation of these operations,
+so the CPU arm is the oracle (oracle/ckks_oracle.c, a scalar OpenMP restatement
+of the reference's arithmetic) on all host cores: for boot, one HRotate at the
+C2S level and one relinearisation at the EvalMod level per step, scaled by the
+bootstrap's own count of rotations and relinearisations.
 """
 from __future__ import annotations
 
@@ -35,6 +41,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PRIM = dict(log_n=16, bits=[60] + [50] * 23 + [60] * 8, n_special=8)
+BOOT = dict(log_n=16, bits=[51] + [46] * 20 + [51] * 14 + [51] * 5, n_special=5, scale=2.0 ** 46, h=192,
+            input_level=4)
+# key switches of one bootstrap (counted from the pipeline: rotations in the six linear
+# transforms + the conjugation, relinearisations of EvalMod on the re and im halves)
+BOOT_METRIC = "bootstraps/s (S2C-first, N=2^16, 35+5 primes, dnum 7, h=192, 2^15 slots, mean err <= 2e-5)"
+PRIM_METRIC = "config-1 primitive chains/s (NTT inv+fwd, HRotate, mult+relin+rescale; N=2^16, L=24, dnum=3)"
 
 
 def measured_peaks():
@@ -46,7 +58,7 @@ def measured_peaks():
 
 
 def traffic_from_profiles(kernel: str):
-    """dram bytes per launch of `kernel` recorded from an ncu capture (profiles/traffic.txt)."""
+    """dram bytes per unit (limb) of `kernel` recorded from an ncu capture (profiles/traffic.txt)."""
     p = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(p):
         return None
@@ -58,12 +70,14 @@ def traffic_from_profiles(kernel: str):
 
 
 class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 50 ms while running."""
+
     def __init__(self, index: int):
         self.index = index
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
 
-    def __enter__(self):
+    def start(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -73,11 +87,12 @@ class ClockSampler:
                                       stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+        time.sleep(0.5)
         return self
 
-    def __exit__(self, *a):
+    def stop(self):
         if self.p:
-            self.p.send_signal(2)  # SIGINT lets nvidia-smi flush its output
+            self.p.send_signal(2)
             try:
                 self.p.wait(timeout=5)
             except subprocess.TimeoutExpired:
@@ -85,9 +100,8 @@ class ClockSampler:
             self.p = None
 
     def summary(self):
-        """Median SM clock and the throttle reasons over samples taken while the GPU was loaded
-        (power above idle)."""
-        self.__exit__()
+        """Median SM clock and throttle reasons over the samples taken while the GPU was loaded."""
+        self.stop()
         self.f.flush()
         rows = []
         for line in open(self.f.name):
@@ -109,11 +123,182 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(busy), "power_w_max": max(r[2] for r in rows)}
 
 
+def timed_steps(torch, step, steps, dist, flush):
+    """Device time of exactly `steps` calls (CUDA events on the launching stream), max over ranks."""
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(steps):
+        if flush is not None:
+            flush.zero_()
+        starts[i].record()
+        step()
+        ends[i].record()
+    torch.cuda.synchronize()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+    return ms / steps
+
+
+def ntt_roofline(torch, ctx, L, limbs_target=4096):
+    """Achieved HBM bandwidth of the batched forward NTT (fwd_col + fwd_blk), the kernel pair
+    that dominates every key switch, on a batch larger than L2."""
+    n = ctx.n
+    rows = max(1, limbs_target // L)
+    g = torch.Generator(device="cuda").manual_seed(123)
+    pr = torch.tensor(ctx.primes[:L].astype(np.int64), device="cuda").view(1, L, 1)
+    nt = torch.remainder(torch.randint(0, 2 ** 62, (rows, L, n), device="cuda", generator=g), pr)
+    for _ in range(3):
+        ctx.ntt_forward_(nt)
+    torch.cuda.synchronize()
+    reps = 20
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        ctx.ntt_forward_(nt)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / reps
+    limbs = rows * L
+    algo = limbs * n * 8 * 2 * 2  # two phase kernels, each reads and writes every word once
+    peak, kind = measured_peaks()
+    achieved = algo / (ms * 1e-3) / 1e9
+    tr = traffic_from_profiles("ntt_forward_pair_bytes_per_limb")
+    return {"kernel": "ntt forward (fwd_col + fwd_blk launch pair), batched limbs", "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_source": kind, "traffic": None if tr is None else round(tr * limbs),
+            "algorithmic_bytes_per_launch_pair": algo, "limbs_per_launch": limbs,
+            "launch_pair_ms": round(ms, 4)}
+
+
 # ---------------------------------------------------------------------------
-# our arm
+# bootstrapping workload
 
 
-def run_ours(args, rank, world, dist):
+def setup_boot(torch, dev, rank):
+    from shmoai_b200.backend import GpuBackend
+    from shmoai_b200.bootstrap import Bootstrapper
+    from shmoai_b200.ckks import CKKSContext
+    from shmoai_b200.evaluator import Evaluator
+    from shmoai_b200.keygen import KeyGenerator
+
+    ctx = CKKSContext(BOOT["log_n"], bits=BOOT["bits"], n_special=BOOT["n_special"], device=dev)
+    be = GpuBackend(ctx)
+    kg = KeyGenerator(be, hamming_weight=BOOT["h"], seed=0x5EED + rank)
+    ev = Evaluator(be, relin_key=kg.relin_key())
+    bs = Bootstrapper(ev, scale=BOOT["scale"], input_level=BOOT["input_level"])
+    for elt in bs.galois_elts():
+        ev.galois_keys[elt] = kg.galois_key(elt)
+    return ctx, be, kg, ev, bs
+
+
+def run_boot(args, rank, world, dist):
+    import torch
+
+    import shmoai_b200
+    from shmoai_b200.evaluator import Ct
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = shmoai_b200.lib()
+    ctx, be, kg, ev, bs = setup_boot(torch, dev, rank)
+    B = args.batch
+    rng = np.random.default_rng(1000 + rank)
+    n = be.n // 2
+    z = rng.uniform(-1, 1, (B, n)) + 1j * rng.uniform(-1, 1, (B, n))
+    ct = kg.encrypt(z, BOOT["scale"], BOOT["input_level"])
+    holder = {}
+
+    def step():
+        holder["out"] = bs.bootstrap(ct)
+
+    clk = ClockSampler(dev).start()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    l0 = lib.shm_kernel_launches()
+    ms = timed_steps(torch, step, args.steps, dist, None)  # a batch is ~1 GB of live data per step > L2
+    launches = lib.shm_kernel_launches() - l0
+    err = np.abs(kg.decrypt(holder["out"]) - z)
+    out_level = holder["out"].level
+
+    # end to end: pinned host input -> device -> bootstrap -> host output, every step
+    h_in = ct.data.cpu().pin_memory()
+    h_out = torch.empty(tuple(holder["out"].data.shape), dtype=torch.int64).pin_memory()
+    d_in = torch.empty_like(ct.data)
+
+    def e2e_step():
+        d_in.copy_(h_in, non_blocking=True)
+        o = bs.bootstrap(Ct(d_in, ct.scale))
+        h_out.copy_(o.data, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = timed_steps(torch, e2e_step, max(1, args.steps // 2), dist, None)
+    roof = ntt_roofline(torch, ctx, BOOT["bits"].__len__() - BOOT["n_special"])
+    clocks = clk.summary()
+    return {
+        "metric": BOOT_METRIC, "value": round(world * B * 1000.0 / ms, 3), "unit": "bootstraps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded uniform slot values in [-1,1]^2, symmetric encryption, random keys)",
+        "config": {"workload": "boot: S2C-first bootstrap of a batch of ciphertexts per GPU per step",
+                   "batch_per_gpu": B, "N": be.n, "slots": n, "input_primes": BOOT["input_level"],
+                   "output_primes": out_level, "Q": "[51]+20x[46]+14x[51]", "P": "5x[51]", "dnum": be.dnum,
+                   "h": BOOT["h"], "evalmod": "Chebyshev deg 47, K=25, 3 double angles",
+                   "err_mean": float(err.mean()), "err_max": float(err.max()),
+                   "l2": "not flushed: the step's live data (~1 GB per batch of 32) exceeds the 126 MB L2",
+                   "reference_published": "2.30 (ordinary) / 3.67 (n=4) / 3.97 (n=8) bootstraps/s on RTX PRO 6000"},
+        "e2e": {"value": round(world * B * 1000.0 / e2e_ms, 3), "unit": "bootstraps/s",
+                "h2d_bytes_per_step": int(h_in.numel() * 8), "d2h_bytes_per_step": int(h_out.numel() * 8)},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "clocks": clocks,
+    }
+
+
+# key switches per bootstrapped ciphertext in this pipeline at N = 2^16: C2S 7+7, 7+7, 7+4
+# rotations at 35/34/33 primes plus the conjugation; S2C the same 39 at 4/3/2 primes;
+# EvalMod 17 relinearisations on each of the two halves (7 baby + 2 giant basis products,
+# 5 split products, 3 double angles) at 32..23 primes.
+BOOT_OPS = {"rot_high": 40, "rot_low": 39, "relin": 34}
+
+
+def cpu_boot_estimate():
+    """CPU oracle on all host cores (N = 2^16): one HRotate at 34 primes, one at 3 primes and
+    one relinearisation at 27 primes, scaled by BOOT_OPS -> bootstraps/s."""
+    from oracle import oracle as O
+
+    o = O.Oracle.from_bits(BOOT["log_n"], BOOT["bits"], BOOT["n_special"])
+    n, QP = o.n, o.nq + o.np
+    key = np.stack([O.fill(900 + d, (2, QP, n), list(o.primes) * 2) for d in range(o.dnum)])
+    t = {}
+    for name, L, poly in (("rot_high", 34, 2), ("rot_low", 3, 2), ("relin", 27, 3)):
+        x = O.fill(901, (poly, L, n), list(o.primes[:L]) * poly)
+        t0 = time.perf_counter()
+        if name == "relin":
+            o.relinearize(x, key)
+        else:
+            o.apply_galois_ct(x, 5, key)
+        t[name] = time.perf_counter() - t0
+    per_boot = sum(BOOT_OPS[k] * t[k] for k in BOOT_OPS)
+    sample = (f"one HRotate at 34 primes ({t['rot_high']:.2f} s), one at 3 primes ({t['rot_low']:.2f} s) and "
+              f"one relinearisation at 27 primes ({t['relin']:.2f} s) on the CPU oracle (OpenMP over limbs), "
+              f"scaled by {BOOT_OPS['rot_high']} + {BOOT_OPS['rot_low']} rotations and {BOOT_OPS['relin']} "
+              "relinearisations per bootstrapped ciphertext")
+    return 1.0 / per_boot, os.cpu_count(), sample
+
+
+# ---------------------------------------------------------------------------
+# primitive-chain workload
+
+
+def run_prim(args, rank, world, dist):
     import torch
 
     import shmoai_b200
@@ -126,30 +311,23 @@ def run_ours(args, rank, world, dist):
     n, L, QP, dnum = ctx.n, ctx.nq, ctx.nq + ctx.np, ctx.dnum
     B = args.batch
     g = torch.Generator(device="cuda").manual_seed(0x5EED + rank)
-    primes_t = torch.tensor(ctx.primes.astype(np.int64), device="cuda")
+    pt = torch.tensor(ctx.primes.astype(np.int64), device="cuda")
 
-    def residues(*shape, rows_primes):
-        # uniform residues: 62 random bits reduced mod the row's prime
+    def residues(shape, primes):
         x = torch.randint(0, 2 ** 62, shape, device="cuda", generator=g, dtype=torch.int64)
-        return torch.remainder(x, rows_primes.view(*([1] * (len(shape) - 2)), -1, 1))
+        return torch.remainder(x, primes.view(*([1] * (len(shape) - 2)), -1, 1))
 
-    qL = primes_t[:L]
-    ct = residues(B, 2, L, n, rows_primes=qL)
-    ct2 = residues(B, 2, L, n, rows_primes=qL)
-    gk = torch.remainder(torch.randint(0, 2 ** 62, (dnum, 2, QP, n), device="cuda", generator=g),
-                         primes_t.view(1, 1, -1, 1))
-    rk = torch.remainder(torch.randint(0, 2 ** 62, (dnum, 2, QP, n), device="cuda", generator=g),
-                         primes_t.view(1, 1, -1, 1))
+    ct = residues((B, 2, L, n), pt[:L])
+    ct2 = residues((B, 2, L, n), pt[:L])
+    gk = residues((dnum, 2, QP, n), pt)
+    rk = residues((dnum, 2, QP, n), pt)
     ws = torch.empty(max(ctx.workspace_bytes("keyswitch", B, L) // 8 + B * 2 * L * n,
                          ctx.workspace_bytes("rescale", 2 * B, L) // 8), dtype=torch.int64, device="cuda")
-    work = ct.clone()
-    rot = torch.empty_like(ct)
-    rel = torch.empty_like(ct)
+    work, rot, rel = ct.clone(), torch.empty_like(ct), torch.empty_like(ct)
     out = torch.empty(B, 2, L - 1, n, dtype=torch.int64, device="cuda")
-    # L2 flush buffer (inputs of one chain are ~50 MB; the 126 MB L2 is flushed between steps)
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.int64, device="cuda")
 
-    def step(src):
+    def chain(src):
         work.copy_(src)
         ctx.ntt_inverse_(work)
         ctx.ntt_forward_(work)
@@ -158,117 +336,41 @@ def run_ours(args, rank, world, dist):
         ctx.relinearize(m, rk, out=rel, workspace=ws)
         ctx.rescale(rel, out=out, workspace=ws)
 
-    # clocks are sampled from before the warm-up (nvidia-smi needs ~0.3 s to start) through
-    # the timed region; only samples taken while the GPU is busy count
-    clk = ClockSampler(dev).__enter__()
-    time.sleep(0.5)
+    clk = ClockSampler(dev).start()
     for _ in range(args.warmup):
-        step(ct)
+        chain(ct)
     torch.cuda.synchronize()
-
-    # ---- device-resident timing
-    launches0 = lib.shm_kernel_launches()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    if True:  # timed region
-        for i in range(args.steps):
-            flush.zero_()
-            starts[i].record()
-            step(ct)
-            ends[i].record()
-        torch.cuda.synchronize()
-    launches = lib.shm_kernel_launches() - launches0
-    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    if dist:
-        t = torch.tensor([dev_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = t.item()
-    ms_per_step = dev_ms / args.steps
-    value = world * B * 1000.0 / ms_per_step
-
-    # ---- end to end through the API with host buffers (pinned), copies inside the timed region
+    l0 = lib.shm_kernel_launches()
+    ms = timed_steps(torch, lambda: chain(ct), args.steps, dist, flush)
+    launches = lib.shm_kernel_launches() - l0
     h_in = ct.cpu().pin_memory()
     h_out = torch.empty(out.shape, dtype=torch.int64).pin_memory()
     d_in = torch.empty_like(ct)
-    e2e_s, e2e_e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for _ in range(2):
-        d_in.copy_(h_in, non_blocking=True)
-        step(d_in)
-        h_out.copy_(out, non_blocking=True)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e2e_s.record()
-    for _ in range(args.steps):
-        d_in.copy_(h_in, non_blocking=True)
-        step(d_in)
-        h_out.copy_(out, non_blocking=True)
-    e2e_e.record()
-    torch.cuda.synchronize()
-    e2e_ms = e2e_s.elapsed_time(e2e_e) / args.steps
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = t.item()
 
-    # ---- dominant kernel: the batched NTT (both phases), timed alone with events
-    nt = torch.empty(B * 2 * (L + ctx.np) * 3, L, n, dtype=torch.int64, device="cuda")
-    nt.copy_(torch.remainder(torch.randint(0, 2 ** 62, nt.shape, device="cuda", generator=g), qL.view(1, -1, 1)))
-    reps = 20
-    for _ in range(3):
-        ctx.ntt_forward_(nt)
-    torch.cuda.synchronize()
-    ks, ke = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ks.record()
-    for _ in range(reps):
-        ctx.ntt_forward_(nt)
-    ke.record()
-    torch.cuda.synchronize()
-    ntt_ms = ks.elapsed_time(ke) / reps
-    limbs = nt.numel() // n
-    ntt_bytes = limbs * n * 8 * 2 * 2  # two phase kernels, each reads and writes every word once
-    peak, peak_kind = measured_peaks()
-    achieved = ntt_bytes / (ntt_ms * 1e-3) / 1e9
-    tr = traffic_from_profiles("ntt_forward_pair_per_limb")
+    def e2e():
+        d_in.copy_(h_in, non_blocking=True)
+        chain(d_in)
+        h_out.copy_(out, non_blocking=True)
 
+    e2e()
+    e2e_ms = timed_steps(torch, e2e, args.steps, dist, None)
+    roof = ntt_roofline(torch, ctx, L)
     clocks = clk.summary()
-    res = {
-        "metric": "config-1 primitive chains/s (NTT inv+fwd, HRotate, mult+relin+rescale; N=2^16, L=24, dnum=3)",
-        "value": round(value, 3),
-        "unit": "chains/s",
-        "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": round(ms_per_step, 4),
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "u64",
+    return {
+        "metric": PRIM_METRIC, "value": round(world * B * 1000.0 / ms, 3), "unit": "chains/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic (seeded uniform RNS residues; random key material)",
         "config": {"workload": "prim: config-1 chain, one ciphertext per GPU per step", "N": n, "L": L,
                    "special_primes": ctx.np, "dnum": dnum, "batch_per_gpu": B,
                    "l2": "flushed between timed steps (256 MiB write)"},
         "e2e": {"value": round(world * B * 1000.0 / e2e_ms, 3), "unit": "chains/s",
                 "h2d_bytes_per_step": int(h_in.numel() * 8), "d2h_bytes_per_step": int(h_out.numel() * 8)},
-        "gpu_launches": int(launches),
-        "roofline": {"kernel": "ntt fwd (fwd_col + fwd_blk), batch of limbs", "bound": "hbm",
-                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                     "traffic": None if tr is None else tr * limbs,
-                     "algorithmic_bytes_per_launch_pair": ntt_bytes, "launch_pair_ms": round(ntt_ms, 4)},
-        "clocks": clocks,
+        "gpu_launches": int(launches), "roofline": roof, "clocks": clocks,
     }
-    return res
 
 
-# ---------------------------------------------------------------------------
-# CPU baseline: the oracle on host cores
-
-
-def run_cpu_chain(sample_chains=1):
+def cpu_prim_chain():
     from oracle import oracle as O
 
     o = O.Oracle.from_bits(PRIM["log_n"], PRIM["bits"], PRIM["n_special"])
@@ -277,25 +379,27 @@ def run_cpu_chain(sample_chains=1):
     ct, ct2 = O.fill(11, (2, L, n), rows), O.fill(12, (2, L, n), rows)
     key = np.stack([O.fill(13 + d, (2, QP, n), list(o.primes) * 2) for d in range(o.dnum)])
     t0 = time.perf_counter()
-    for _ in range(sample_chains):
-        w = o.ntt(o.intt(ct))
-        r = o.apply_galois_ct(w, 5, key)
-        m = o.tensor(r, ct2)
-        o.rescale(o.relinearize(m, key))
-    dt = time.perf_counter() - t0
-    return sample_chains / dt, os.cpu_count()
+    w = o.ntt(o.intt(ct))
+    r = o.apply_galois_ct(w, 5, key)
+    o.rescale(o.relinearize(o.tensor(r, ct2), key))
+    return 1.0 / (time.perf_counter() - t0), os.cpu_count()
+
+
+# ---------------------------------------------------------------------------
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="prim", choices=["prim"])
-    ap.add_argument("--batch", type=int, default=1)
+    ap.add_argument("--workload", default="boot", choices=["boot", "prim"])
+    ap.add_argument("--batch", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.batch is None:
+        args.batch = 32 if args.workload == "boot" else 1
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -303,24 +407,26 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        per_step = []
-        for _ in range(args.warmup):
-            run_cpu_chain(1)
-        for _ in range(args.steps):
-            v, cores = run_cpu_chain(1)
-            per_step.append(1.0 / v)
-        ms = 1000.0 * statistics.mean(per_step)
-        value = 1000.0 / ms
+        vals = []
+        for i in range(args.warmup + args.steps):
+            if args.workload == "boot":
+                v, cores, sample = cpu_boot_estimate()
+            else:
+                v, cores = cpu_prim_chain()
+                sample = "one full config-1 chain per step"
+            if i >= args.warmup:
+                vals.append(v)
+        value = statistics.mean(vals)
+        unit = "bootstraps/s" if args.workload == "boot" else "chains/s"
         print(json.dumps({
-            "impl": "reference",
-            "metric": "config-1 primitive chains/s (NTT inv+fwd, HRotate, mult+relin+rescale; N=2^16, L=24, dnum=3)",
-            "value": round(value, 4), "unit": "chains/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform RNS residues)",
-            "config": {"workload": "prim: config-1 chain, one ciphertext per step"},
-            "cpu_baseline": {"value": round(value, 4), "unit": "chains/s", "cores": os.cpu_count(), "kind": "port",
-                             "sample": "one full chain per step (the reference has no CPU path; oracle/ckks_oracle.c)"},
-            "e2e": {"value": round(value, 4), "unit": "chains/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "impl": "reference", "metric": BOOT_METRIC if args.workload == "boot" else PRIM_METRIC,
+            "value": round(value, 6), "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000.0 / value, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": args.workload + " (reference CPU arm: the oracle restatement)"},
+            "cpu_baseline": {"value": round(value, 6), "unit": unit, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 6), "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }))
         return
 
@@ -330,14 +436,19 @@ def main():
 
         import torch.distributed as tdist
 
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
-    res = run_ours(args, rank, world, dist)
+    res = run_boot(args, rank, world, dist) if args.workload == "boot" else run_prim(args, rank, world, dist)
     if rank == 0:
         if not args.no_cpu_baseline:
-            v, cores = run_cpu_chain(1)
-            res["cpu_baseline"] = {"value": round(v, 4), "unit": "chains/s", "cores": cores, "kind": "port",
-                                   "sample": "one config-1 chain on the CPU oracle (OpenMP over limbs)"}
+            if args.workload == "boot":
+                v, cores, sample = cpu_boot_estimate()
+                res["cpu_baseline"] = {"value": round(v, 6), "unit": "bootstraps/s", "cores": cores,
+                                       "kind": "port", "sample": sample}
+            else:
+                v, cores = cpu_prim_chain()
+                res["cpu_baseline"] = {"value": round(v, 4), "unit": "chains/s", "cores": cores, "kind": "port",
+                                       "sample": "one config-1 chain on the CPU oracle (OpenMP over limbs)"}
         print(json.dumps(res))
     if dist:
         dist.barrier()
