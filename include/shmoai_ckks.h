@@ -123,6 +123,18 @@ int shm_relinearize(const shm_context *ctx, const uint64_t *ct3, const uint64_t 
 int shm_apply_galois(const shm_context *ctx, const uint64_t *ct, uint32_t galois_elt, const uint64_t *galois_key,
                      uint64_t *out, uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes,
                      void *stream);
+/* Hoisted automorphisms of the same n_cts ciphertexts: ModUp of c1 once, then for
+ * each of n_elts Galois elements the permuted inner product with keys[e] and
+ * ModDown: outs[e] = (sigma(c0) + cx0, cx1).  keys / outs are host arrays of
+ * device pointers; outputs must not alias the input.  Counterpart of the
+ * reference's hoisted rotations (thirdparty/phantom-fhe/src/evaluate.cu:1727-1920),
+ * used here for the baby steps of the bootstrapping linear transforms.  Decrypts
+ * like shm_apply_galois; the limbs differ in the ModUp error term, so bit-exact
+ * parity for this entry point is against the oracle's hoisted restatement. */
+size_t shm_apply_galois_hoisted_workspace_bytes(const shm_context *ctx, uint32_t n_cts, uint32_t L);
+int shm_apply_galois_hoisted(const shm_context *ctx, const uint64_t *ct, uint32_t n_elts, const uint32_t *elts,
+                             const uint64_t *const *keys, uint64_t *const *outs, uint32_t n_cts, uint32_t L,
+                             void *workspace, size_t workspace_bytes, void *stream);
 /* Galois element of a rotation by `step` slots (0 = conjugation).
  * Replaces PhantomGaloisTool::get_elt_from_step (src/galois.cu:47-91). */
 uint32_t shm_galois_elt_from_step(const shm_context *ctx, int step);

@@ -453,6 +453,55 @@ void orc_keyswitch(const orc_ctx *c, const uint64_t *d, uint32_t L, const uint64
     free(up);
 }
 
+/* Hoisted Galois key switching (Halevi-Shoup): ModUp of c1 once, then for each
+ * element g the automorphism is applied to the extended digits (an NTT-domain
+ * permutation of every limb), followed by the inner product with g's key and
+ * ModDown: out_g = (sigma_g(c0) + cx0, cx1).  keys[e] -> [dnum][2][QP][N],
+ * outs[e] -> [2][L][N]. */
+void orc_apply_galois_hoisted(const orc_ctx *c, const uint64_t *ct, uint32_t L, uint32_t n_elts,
+                              const uint32_t *elts, const uint64_t *const *keys, uint32_t dnum, uint64_t *const *outs) {
+    size_t n = c->n, ln = (size_t)L * n;
+    uint32_t alpha = c->np, beta = (L + alpha - 1) / alpha, LP = L + c->np, QP = c->nq + c->np;
+    (void)dnum;
+    uint64_t *up = (uint64_t *)malloc(sizeof(uint64_t) * beta * LP * n);
+    orc_modup(c, ct + ln, L, up);
+    uint32_t *perm = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * 2 * LP * n);
+    for (uint32_t e = 0; e < n_elts; e++) {
+        orc_galois_perm(c->log_n, elts[e], perm);
+        const uint64_t *key = keys[e];
+#pragma omp parallel for
+        for (int j = 0; j < (int)LP; j++) {
+            uint32_t pj = ext_prime(c, L, j);
+            uint64_t t = c->primes[pj];
+            for (size_t k = 0; k < n; k++) {
+                u128 a0 = 0, a1 = 0;
+                for (uint32_t b = 0; b < beta; b++) {
+                    uint64_t v = up[((size_t)b * LP + j) * n + perm[k]];
+                    const uint64_t *kb = key + (size_t)b * 2 * QP * n;
+                    a0 = (a0 + (u128)v * kb[(size_t)pj * n + k]) % t;
+                    a1 = (a1 + (u128)v * kb[((size_t)QP + pj) * n + k]) % t;
+                }
+                cx[(size_t)j * n + k] = (uint64_t)a0;
+                cx[((size_t)LP + j) * n + k] = (uint64_t)a1;
+            }
+        }
+        uint64_t *out = outs[e];
+        moddown_one(c, cx, L, out);
+        moddown_one(c, cx + (size_t)LP * n, L, out + ln);
+        /* out0 += sigma(c0) */
+#pragma omp parallel for
+        for (int i = 0; i < (int)L; i++) {
+            uint64_t q = c->primes[i];
+            for (size_t k = 0; k < n; k++)
+                out[(size_t)i * n + k] = addmod(out[(size_t)i * n + k], ct[(size_t)i * n + perm[k]], q);
+        }
+    }
+    free(cx);
+    free(perm);
+    free(up);
+}
+
 /* Relinearize a size-3 ciphertext: (c0 + cx0, c1 + cx1) with cx = KS(c2). */
 void orc_relinearize(const orc_ctx *c, const uint64_t *ct3, uint32_t L, const uint64_t *key, uint32_t dnum,
                      uint64_t *out) {

@@ -67,6 +67,8 @@ def lib():
         L.orc_relinearize.argtypes = [vp, _u64p, u32, _u64p, u32, _u64p]
         L.orc_apply_galois_ct.argtypes = [vp, _u64p, u32, u32, _u64p, u32, _u64p]
         L.orc_ctpt_matmul.argtypes = [vp, _u64p, ctypes.POINTER(ctypes.c_int64), u32, u32, u32, _u64p]
+        L.orc_apply_galois_hoisted.argtypes = [vp, _u64p, u32, u32, ctypes.POINTER(ctypes.c_uint32),
+                                               ctypes.POINTER(_u64p), u32, ctypes.POINTER(_u64p)]
         L.orc_signed_residue.argtypes = [ctypes.c_int64, u64]
         L.orc_signed_residue.restype = u64
         _lib = L
@@ -192,6 +194,18 @@ class Oracle:
         out = np.empty((2, L, self.n), dtype=np.uint64)
         lib().orc_apply_galois_ct(self._h, _p(ct), L, elt, _p(key), self.dnum, _p(out))
         return out
+
+    def apply_galois_hoisted(self, ct, elts, keys):
+        """[2][L][N] ciphertext, one ModUp, one output per Galois element."""
+        L = ct.shape[-2]
+        ct = np.ascontiguousarray(ct, dtype=np.uint64)
+        keys = [np.ascontiguousarray(k, dtype=np.uint64) for k in keys]
+        outs = [np.empty((2, L, self.n), dtype=np.uint64) for _ in elts]
+        e = (ctypes.c_uint32 * len(elts))(*elts)
+        kp = (_u64p * len(keys))(*[_p(k) for k in keys])
+        op = (_u64p * len(outs))(*[_p(o) for o in outs])
+        lib().orc_apply_galois_hoisted(self._h, _p(ct), L, len(elts), e, kp, self.dnum, op)
+        return outs
 
     def ctpt_matmul(self, X, W):
         n_in, _, L, _ = X.shape

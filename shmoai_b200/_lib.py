@@ -52,6 +52,9 @@ def _declare(L):
         "shm_relinearize": (ctypes.c_int, [_P, _P, _P, _P, _U32, _U32, _P, _SZ, _P]),
         "shm_apply_galois": (ctypes.c_int, [_P, _P, _U32, _P, _P, _U32, _U32, _P, _SZ, _P]),
         "shm_galois_elt_from_step": (_U32, [_P, ctypes.c_int]),
+        "shm_apply_galois_hoisted_workspace_bytes": (_SZ, [_P, _U32, _U32]),
+        "shm_apply_galois_hoisted": (ctypes.c_int, [_P, _P, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_P),
+                                                    ctypes.POINTER(_P), _U32, _U32, _P, _SZ, _P]),
         "shm_rotate": (ctypes.c_int, [_P, _P, ctypes.c_int, _P, _P, _U32, _U32, _P, _SZ, _P]),
         "shm_multiply_scalar": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint64), _P, _U32, _U32, _P]),
         "shm_add_scalar": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint64), _P, _U32, _U32, _P]),

@@ -103,6 +103,20 @@ class GpuBackend:
         ws = self.workspace(words)
         return self.ctx.apply_galois(ct, elt, key, workspace=ws, stream=self.stream)
 
+    def apply_galois_many(self, ct, elts, keys):
+        """Hoisted: one ModUp, one output batch per Galois element."""
+        L = ct.shape[-2]
+        n_cts = ct.numel() // (2 * L * self.n)
+        outs = [torch.empty_like(ct) for _ in elts]
+        ws = self.workspace(lib().shm_apply_galois_hoisted_workspace_bytes(self.ctx._h, n_cts, L) // 8)
+        k = len(elts)
+        E = (ctypes.c_uint32 * k)(*elts)
+        K = (ctypes.c_void_p * k)(*[_ptr(x).value for x in keys])
+        O = (ctypes.c_void_p * k)(*[_ptr(x).value for x in outs])
+        check(lib().shm_apply_galois_hoisted(self.ctx._h, _ptr(ct), k, E, K, O, n_cts, L, _ptr(ws), ws.numel() * 8,
+                                             self._s()))
+        return outs
+
     def permute_plain(self, pt, elt):
         """NTT-domain automorphism of plaintext rows without key switching (key generation only)."""
         return pt[..., self._perm(elt)].contiguous()

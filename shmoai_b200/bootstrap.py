@@ -210,7 +210,8 @@ class LinearTransform:
         ev, be = self.ev, self.ev.be
         if x.level != self.level:
             x = ev.drop(x, self.level)
-        rot = {v: (x if v == 0 else ev.rotate(x, v * self.b)) for v in self.baby}
+        hoisted = ev.rotate_many(x, [v * self.b for v in self.baby if v])
+        rot = {v: (x if v == 0 else hoisted[v * self.b]) for v in self.baby}
         acc = None
         for u, lst in sorted(self.groups.items()):
             inner = be.mul_plain_acc([rot[v].data for v, _ in lst], [p for _, p in lst])

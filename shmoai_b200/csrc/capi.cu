@@ -420,6 +420,25 @@ int shm_apply_galois(const shm_context *ctx, const uint64_t *ct, uint32_t galois
     });
 }
 
+size_t shm_apply_galois_hoisted_workspace_bytes(const shm_context *ctx, uint32_t n_cts, uint32_t L) {
+    return ctx && ctx->c ? shm::hoisted_ws_words(*ctx->c, n_cts, L) * 8 : 0;
+}
+
+int shm_apply_galois_hoisted(const shm_context *ctx, const uint64_t *ct, uint32_t n_elts, const uint32_t *elts,
+                             const uint64_t *const *keys, uint64_t *const *outs, uint32_t n_cts, uint32_t L,
+                             void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        if (!elts || !keys || !outs) throw std::invalid_argument("null element, key or output array");
+        for (uint32_t e = 0; e < n_elts; e++)
+            if (outs[e] == ct) throw std::invalid_argument("hoisted outputs must not alias the input");
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::hoisted_ws_words(c, n_cts, L));
+        shm::apply_galois_hoisted(c, ct, n_cts, L, n_elts, elts, keys, outs, ws, S(stream));
+    });
+}
+
 int shm_rotate(const shm_context *ctx, const uint64_t *ct, int step, const uint64_t *galois_key, uint64_t *out,
                uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
     uint32_t elt = shm_galois_elt_from_step(ctx, step);

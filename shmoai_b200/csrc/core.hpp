@@ -93,11 +93,18 @@ size_t rescale_ws_words(const Context &c, uint32_t n_polys, uint32_t L);
 struct KsOutput {
     uint64_t *out0, *out1;
     const uint64_t *add0, *add1;
-    size_t stride;  // words between consecutive ciphertexts for out/add
+    size_t stride;                // words between consecutive ciphertexts for out/add
+    const uint32_t *add0_perm;    // if set, add0 is read at add0_perm[k] (an automorphism)
 };
 void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_cts, uint32_t L, const uint64_t *key,
                const KsOutput &o, uint64_t *ws, cudaStream_t st);
 size_t keyswitch_ws_words(const Context &c, uint32_t n_cts, uint32_t L);
+// Hoisted automorphisms: one ModUp of the c1 of n_cts ciphertexts `ct` ([n_cts][2][L][N]),
+// then per element e: outs[e] = (sigma_e(c0) + cx0, cx1) with keys[e].
+void apply_galois_hoisted(const Context &c, const uint64_t *ct, uint32_t n_cts, uint32_t L, uint32_t n_elts,
+                          const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs, uint64_t *ws,
+                          cudaStream_t st);
+size_t hoisted_ws_words(const Context &c, uint32_t n_cts, uint32_t L);
 
 // per-limb scalars passed by value (residue and Shoup companion per limb)
 struct ScalarTab {

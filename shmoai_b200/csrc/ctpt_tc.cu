@@ -1,0 +1,410 @@
+// Rotation-free ct-pt matmul on the INT8 tensor cores (tcgen05.mma kind::i8), exact.
+//
+// Y[o][r] = sum_i X[i][r] * W[i][o] mod q_limb(r): X rows r of the n_in input
+// ciphertexts (2 L N residues each), W the signed integer weights.  This is the
+// reference's multiply_plain + add_inplace loop over constant plaintexts
+// (src/include/source/matrix_mul/Ct_pt_matrix_mul.cuh:112-158) computed as one
+// dense contraction.
+//
+// Exactness by a small-modulus residue system: the integer S = sum_i x_i w_i
+// (|S| < n_in * max q * max|W|) is computed modulo T pairwise-coprime moduli
+// m_t <= 251 whose product exceeds 8|S|, each as an int8 GEMM with balanced
+// residues in [-125, 125] (|acc| < n_in * 125^2 < 2^31), then rebuilt by the CRT:
+//   S = sum_t r_t c_t - v M,  c_t = (M/m_t) [(M/m_t)^-1]_{m_t},  v = round(sum_t r_t inv_t / m_t),
+// and reduced mod q_l with per-limb constants.  T GEMMs replace the 35 byte-slice
+// products of a positional split.
+//
+// Pipeline per modulus: X residue planes [R][K] and W residue planes [N][K]
+// (both K-major) -> tcgen05 GEMM tile M = 128 columns of X x N = 256 outputs,
+// K in 64-byte stages (4-stage cp.async ring, one mbarrier per stage), s32
+// accumulator in TMEM (256 columns) -> epilogue tcgen05.ld, acc mod m_t -> uint8
+// residue planes -> CRT kernel.
+#include <cstring>
+
+#include "core.hpp"
+#include "host_math.hpp"
+
+namespace shm {
+
+namespace {
+
+constexpr int kMaxMods = 20;
+constexpr uint32_t kBM = 128;   // X columns per tile (MMA M)
+constexpr uint32_t kBN = 256;   // outputs per tile (MMA N)
+constexpr uint32_t kKB = 64;    // K bytes per stage (two k32 MMAs)
+constexpr int kStages = 4;
+constexpr uint32_t kStageA = kBM * kKB;  // 8 KB
+constexpr uint32_t kStageB = kBN * kKB;  // 16 KB
+constexpr uint32_t kSmem = kStages * (kStageA + kStageB) + 1024;
+constexpr uint32_t kThreads = 128;
+constexpr long long kSpinLimit = 1ll << 28;
+
+struct ModTab {
+    uint32_t t;
+    uint32_t m[kMaxMods];
+    float frac[kMaxMods];  // [(M/m_t)^-1]_{m_t} / m_t
+};
+
+__constant__ ModTab c_mods;
+
+// ---------------------------------------------------------------- residues
+__device__ __forceinline__ int8_t balanced(uint32_t r, uint32_t m) { return (int8_t)(r > m / 2 ? (int)r - (int)m : (int)r); }
+
+__device__ __forceinline__ uint32_t mod_small(uint64_t x, uint32_t m) {
+    // x = a 2^48 + b 2^24 + d; every partial term stays below 2^32
+    uint32_t a = (uint32_t)(x >> 48), b = (uint32_t)((x >> 24) & 0xFFFFFF), d = (uint32_t)(x & 0xFFFFFF);
+    uint32_t c24 = (1u << 24) % m, c48 = (uint32_t)(((uint64_t)c24 * c24) % m);
+    uint64_t s = (uint64_t)a * c48 + (uint64_t)b * c24 + d;
+    return (uint32_t)(s % m);
+}
+
+// X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via a 64 x 64 shared-memory transpose
+__global__ void xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__ XP, uint32_t n_in, uint32_t Kp,
+                            uint64_t R, uint64_t r0) {
+    __shared__ uint64_t tile[64][65];
+    const uint32_t i0 = blockIdx.y * 64;
+    const uint64_t rb = (uint64_t)blockIdx.x * 64;
+    const uint32_t tx = threadIdx.x & 63, ty = threadIdx.x >> 6;  // 256 threads: 64 x 4
+    for (uint32_t i = ty; i < 64; i += 4) {
+        uint32_t ii = i0 + i;
+        tile[i][tx] = ii < n_in ? X[(uint64_t)ii * R + r0 + rb + tx] : 0;
+    }
+    __syncthreads();
+    const uint64_t chunk = (uint64_t)gridDim.x * 64;
+    for (uint32_t rr = ty; rr < 64; rr += 4) {
+        uint64_t x = tile[tx][rr];
+        for (uint32_t t = 0; t < c_mods.t; t++) {
+            uint32_t m = c_mods.m[t];
+            XP[((uint64_t)t * chunk + rb + rr) * Kp + i0 + tx] = balanced(mod_small(x, m), m);
+        }
+    }
+}
+
+// W [n_in][n_out] (int64) -> WP [t][Np][Kp] (int8)
+__global__ void wres_kernel(const int64_t *__restrict__ W, int8_t *__restrict__ WP, uint32_t n_in, uint32_t n_out,
+                            uint32_t Kp, uint32_t Np) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // input index (K)
+    const uint32_t o = blockIdx.y;
+    if (i >= Kp) return;
+    int64_t w = (i < n_in && o < n_out) ? W[(uint64_t)i * n_out + o] : 0;
+    for (uint32_t t = 0; t < c_mods.t; t++) {
+        int64_t m = c_mods.m[t];
+        int64_t r = w % m;
+        if (r < 0) r += m;
+        WP[((uint64_t)t * Np + o) * Kp + i] = balanced((uint32_t)r, (uint32_t)m);
+    }
+}
+
+// ---------------------------------------------------------------- tcgen05 GEMM
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// K-major, no-swizzle ("interleaved") operand: core matrices of 8 rows x 16 bytes,
+// K-adjacent core matrices 128 B apart (LBO), 8-row groups (KB / 16) * 128 B apart (SBO).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)(128 >> 4) << 16;             // leading byte offset (K direction)
+    d |= (uint64_t)((kKB / 16 * 128) >> 4) << 32;  // stride byte offset (M/N direction)
+    d |= (uint64_t)1 << 46;                      // descriptor version for sm_100
+    return d;                                    // base offset 0, lbo mode 0, layout SWIZZLE_NONE
+}
+
+// byte offset of (row, k-chunk) inside one stage operand of `rows` x kKB bytes
+__device__ __forceinline__ uint32_t core_off(uint32_t row, uint32_t kc) {
+    return ((row >> 3) * (kKB / 16) + kc) * 128 + (row & 7) * 16;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long it = 0; it < kSpinLimit; it++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity));
+        if (ok) return true;
+    }
+    return false;
+}
+
+// grid: (R_chunk / 128, Np / 256, T); one modulus per blockIdx.z
+__global__ void __launch_bounds__(kThreads, 1) mma_kernel(const int8_t *__restrict__ XP, const int8_t *__restrict__ WP,
+                                                          uint8_t *__restrict__ RES, uint32_t Kp, uint32_t Np,
+                                                          uint32_t n_out, uint64_t chunk, int *__restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bars[kStages];
+    __shared__ uint32_t tmem_base;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t t = blockIdx.z;
+    const uint64_t rbase = (uint64_t)blockIdx.x * kBM;
+    const uint32_t obase = blockIdx.y * kBN;
+    const int8_t *A = XP + ((uint64_t)t * chunk + rbase) * Kp;  // [128][Kp]
+    const int8_t *B = WP + ((uint64_t)t * Np + obase) * Kp;     // [256][Kp]
+    uint8_t *sA = smem, *sB = smem + kStages * kStageA;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base)),
+                     "r"(kBN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kStages; s++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[s])));
+        asm volatile("fence.mbarrier_init.release.cluster;\n");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n");
+    const uint32_t tmem = tmem_base;
+    const uint32_t nkb = Kp / kKB;
+    // instruction descriptor: s32 accumulate, A and B signed int8, both K-major, N = 256, M = 128
+    const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((kBN >> 3) << 17) | ((kBM >> 4) << 24);
+
+    auto load_stage = [&](uint32_t kb) {
+        const uint32_t s = kb % kStages;
+        const uint32_t a_dst = smem_u32(sA + s * kStageA), b_dst = smem_u32(sB + s * kStageB);
+        const uint64_t koff = (uint64_t)kb * kKB;
+        // A: 128 rows x 4 chunks of 16 B = 512 copies; B: 256 x 4 = 1024
+        for (uint32_t c = tid; c < kBM * (kKB / 16); c += kThreads) {
+            uint32_t row = c / (kKB / 16), kc = c % (kKB / 16);
+            cp_async16(a_dst + core_off(row, kc), A + (uint64_t)row * Kp + koff + kc * 16);
+        }
+        for (uint32_t c = tid; c < kBN * (kKB / 16); c += kThreads) {
+            uint32_t row = c / (kKB / 16), kc = c % (kKB / 16);
+            cp_async16(b_dst + core_off(row, kc), B + (uint64_t)row * Kp + koff + kc * 16);
+        }
+        asm volatile("cp.async.commit_group;\n");
+    };
+
+    bool ok = true;
+    for (uint32_t kb = 0; kb < kStages - 1 && kb < nkb; kb++) load_stage(kb);
+    for (uint32_t kb = 0; kb < nkb; kb++) {
+        // stage kb has landed once at most kStages - 2 newer groups are pending
+        if (kb + kStages - 1 <= nkb) asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2));
+        else asm volatile("cp.async.wait_group 0;\n");
+        asm volatile("fence.proxy.async.shared::cta;\n");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n");
+            const uint32_t s = kb % kStages;
+            const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sB + s * kStageB);
+#pragma unroll
+            for (uint32_t k = 0; k < kKB / 32; k++) {
+                uint64_t ad = smem_desc(a0 + k * 256), bd = smem_desc(b0 + k * 256);
+                uint32_t acc = (kb | k) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                smem_u32(&bars[s])));
+        }
+        // refill the stage used by the previous block once its MMAs have read it
+        const uint32_t nxt = kb + kStages - 1;
+        if (nxt < nkb) {
+            if (kb >= 1) {
+                const uint32_t ps = (kb - 1) % kStages;
+                if (!mbar_wait(smem_u32(&bars[ps]), ((kb - 1) / kStages) & 1)) ok = false;
+            }
+            load_stage(nxt);
+        }
+    }
+    // the last commit completes after every earlier MMA
+    {
+        const uint32_t ls = (nkb - 1) % kStages;
+        if (!mbar_wait(smem_u32(&bars[ls]), ((nkb - 1) / kStages) & 1)) ok = false;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n");
+    if (!ok) {
+        if (lane == 0) atomicExch(err, 1);
+    } else {
+        // epilogue: warp w reads TMEM lanes 32w..32w+31 (X columns), 32 output columns at a time
+        const uint32_t m = c_mods.m[t];
+        const uint64_t r = rbase + warp * 32 + lane;
+        for (uint32_t c0 = 0; c0 < kBN; c0 += 32) {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((warp * 32) << 16) + c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n");
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const uint32_t o = obase + c0 + j;
+                if (o < n_out) {
+                    int a = (int)v[j] % (int)m;
+                    if (a < 0) a += m;
+                    RES[((uint64_t)t * n_out + o) * chunk + r] = (uint8_t)a;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kBN));
+}
+
+// ---------------------------------------------------------------- CRT fold
+struct CrtLimb {
+    uint64_t c[kMaxMods];  // c_t mod q_l
+    uint64_t M;            // M mod q_l
+};
+
+__global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict__ Y, const CrtLimb *__restrict__ tab,
+                           uint32_t n_out, uint64_t chunk, uint64_t r0, uint64_t R, uint32_t L, uint32_t log_n,
+                           const PrimeConst *__restrict__ pc) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t o = blockIdx.y;
+    if (r >= chunk) return;
+    const uint64_t rg = r0 + r;
+    const uint32_t limb = (uint32_t)((rg >> log_n) % L);
+    const CrtLimb &cl = tab[limb];
+    u128 pos = {0, 0};
+    float v = 0.f;
+    for (uint32_t t = 0; t < c_mods.t; t++) {
+        uint32_t rt = RES[((uint64_t)t * n_out + o) * chunk + r];
+        mac(pos, rt, cl.c[t]);
+        v += (float)rt * c_mods.frac[t];
+    }
+    const uint64_t vi = (uint64_t)(int64_t)rintf(v);
+    const PrimeConst p = pc[limb];
+    const uint64_t y = sub_mod(barrett(pos, p), barrett(mul_wide(vi, cl.M), p), p.q);
+    Y[(uint64_t)o * R + rg] = y;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+
+namespace {
+
+struct Plan {
+    ModTab mods;
+    std::vector<CrtLimb> limbs;
+};
+
+Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) {
+    // |S| < n_in * max q * max|W|; the moduli product must exceed 8 |S| (CRT margin)
+    static const uint32_t cand[] = {251, 241, 239, 233, 229, 227, 223, 211, 199, 197, 193, 191, 181, 179, 173,
+                                    167, 163, 157, 151, 149};
+    uint64_t maxq = 0;
+    for (uint32_t l = 0; l < L; l++) maxq = std::max(maxq, c.primes[l]);
+    const double need = std::log2((double)n_in) + std::log2((double)maxq) + std::log2((double)std::max<uint64_t>(max_abs_w, 1)) + 4.0;
+    Plan p{};
+    double have = 0;
+    uint32_t T = 0;
+    while (have < need) {
+        if (T >= (uint32_t)kMaxMods) throw std::invalid_argument("ct-pt matmul: weights or inputs too large");
+        p.mods.m[T] = cand[T];
+        have += std::log2((double)cand[T]);
+        T++;
+    }
+    p.mods.t = T;
+    // CRT constants: c_t = (M/m_t) * [(M/m_t)^-1 mod m_t]; per limb mod q_l
+    for (uint32_t t = 0; t < T; t++) {
+        uint32_t m = p.mods.m[t], Mt_mod_m = 1;
+        for (uint32_t u = 0; u < T; u++)
+            if (u != t) Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (p.mods.m[u] % m) % m);
+        uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);  // m prime
+        p.mods.frac[t] = (float)inv / (float)m;
+    }
+    p.limbs.resize(L);
+    for (uint32_t l = 0; l < L; l++) {
+        uint64_t q = c.primes[l], M = 1;
+        for (uint32_t u = 0; u < T; u++) M = host::mulmod(M, p.mods.m[u], q);
+        p.limbs[l].M = M;
+        for (uint32_t t = 0; t < T; t++) {
+            uint32_t m = p.mods.m[t], Mt_mod_m = 1;
+            uint64_t Mt = 1;
+            for (uint32_t u = 0; u < T; u++)
+                if (u != t) {
+                    Mt = host::mulmod(Mt, p.mods.m[u], q);
+                    Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (p.mods.m[u] % m) % m);
+                }
+            uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);
+            p.limbs[l].c[t] = host::mulmod(Mt, inv, q);
+        }
+    }
+    return p;
+}
+
+}  // namespace
+
+// columns of X processed per pass (bounds the residue workspaces)
+constexpr uint64_t kChunkCols = 131072;
+
+size_t ctpt_tc_ws_bytes(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L) {
+    const uint64_t R = 2ull * L * c.n;
+    const uint64_t chunk = std::min<uint64_t>(R, kChunkCols);
+    const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBN - 1) / kBN * kBN;
+    return (size_t)kMaxMods * (chunk * Kp + (uint64_t)Np * Kp + (uint64_t)n_out * chunk) + 4096 +
+           sizeof(CrtLimb) * 64;
+}
+
+void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
+                    uint32_t L, void *ws, uint64_t max_abs_w, cudaStream_t st) {
+    if (n_in == 0 || n_out == 0) return;
+    const uint64_t R = 2ull * L * c.n;
+    if (R % kBM) throw std::invalid_argument("ct-pt matmul: 2 L N must be a multiple of 128");
+    const uint64_t chunk = std::min<uint64_t>(R, kChunkCols);
+    if (R % chunk) throw std::invalid_argument("ct-pt matmul: column count not a multiple of the chunk");
+    const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBN - 1) / kBN * kBN;
+    Plan plan = make_plan(c, n_in, L, max_abs_w);
+    const uint32_t T = plan.mods.t;
+    SHM_CUDA(cudaMemcpyToSymbolAsync(c_mods, &plan.mods, sizeof(ModTab), 0, cudaMemcpyHostToDevice, st));
+    // workspace carve-up
+    uint8_t *base = static_cast<uint8_t *>(ws);
+    int *err = reinterpret_cast<int *>(base);
+    CrtLimb *tab = reinterpret_cast<CrtLimb *>(base + 256);
+    int8_t *XP = reinterpret_cast<int8_t *>(base + 4096 + sizeof(CrtLimb) * 64);
+    int8_t *WP = XP + (size_t)T * chunk * Kp;
+    uint8_t *RES = reinterpret_cast<uint8_t *>(WP + (size_t)T * Np * Kp);
+    SHM_CUDA(cudaMemcpyAsync(tab, plan.limbs.data(), sizeof(CrtLimb) * L, cudaMemcpyHostToDevice, st));
+    SHM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    // zero-padded K tail of the X planes stays zero: clear once per call
+    if (Kp != n_in) SHM_CUDA(cudaMemsetAsync(XP, 0, (size_t)T * chunk * Kp, st));
+    SHM_LAUNCHED(1);
+    wres_kernel<<<dim3((Kp + 255) / 256, Np), 256, 0, st>>>(W, WP, n_in, n_out, Kp, Np);
+    SHM_CUDA(cudaGetLastError());
+    static bool attr_set = false;
+    if (!attr_set) {
+        SHM_CUDA(cudaFuncSetAttribute(mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+        attr_set = true;
+    }
+    for (uint64_t r0 = 0; r0 < R; r0 += chunk) {
+        SHM_LAUNCHED(1);
+        xres_kernel<<<dim3((uint32_t)(chunk / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0);
+        SHM_CUDA(cudaGetLastError());
+        SHM_LAUNCHED(1);
+        mma_kernel<<<dim3((uint32_t)(chunk / kBM), Np / kBN, T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
+                                                                                       chunk, err);
+        SHM_CUDA(cudaGetLastError());
+        SHM_LAUNCHED(1);
+        crt_kernel<<<dim3((uint32_t)((chunk + 255) / 256), n_out), 256, 0, st>>>(RES, Y, tab, n_out, chunk, r0, R, L,
+                                                                                c.log_n, c.pc);
+        SHM_CUDA(cudaGetLastError());
+    }
+}
+
+int ctpt_tc_error(void *ws, cudaStream_t st) {
+    int h = 0;
+    SHM_CUDA(cudaMemcpyAsync(&h, ws, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SHM_CUDA(cudaStreamSynchronize(st));
+    return h;
+}
+
+}  // namespace shm

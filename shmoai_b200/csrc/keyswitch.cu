@@ -55,12 +55,16 @@ __global__ void modup_conv_kernel(const uint64_t *__restrict__ x, const uint64_t
     }
 }
 
-// acc[ct][h][j][k] = sum_b up[ct][b][j][k] * key[b][h][prime(j)][k]
+// acc[ct][h][j][k] = sum_b up[ct][b][j][perm[k]] * key[b][h][prime(j)][k]   (perm = identity if null)
+// An NTT-domain automorphism maps every aligned block of 32 slots onto an aligned block
+// of 32 slots, so the permuted read of a warp stays within one 256-byte segment.
 __global__ void inner_product_kernel(const uint64_t *__restrict__ up, const uint64_t *__restrict__ key,
                                      uint64_t *__restrict__ acc, uint32_t n_cts, uint32_t L, uint32_t np, uint32_t nq,
-                                     uint32_t beta, uint32_t log_n, const PrimeConst *__restrict__ pc) {
+                                     uint32_t beta, uint32_t log_n, const PrimeConst *__restrict__ pc,
+                                     const uint32_t *__restrict__ perm) {
     const uint32_t j = blockIdx.y;
     const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
+    const uint32_t ks = perm ? __ldg(perm + k) : k;
     const size_t n = (size_t)1 << log_n;
     const uint32_t LP = L + np, QP = nq + np;
     const uint32_t pj = j < L ? j : nq + (j - L);
@@ -75,7 +79,7 @@ __global__ void inner_product_kernel(const uint64_t *__restrict__ up, const uint
         }
     }
     for (uint32_t ct = 0; ct < n_cts; ct++) {
-        const uint64_t *u = up + (size_t)ct * beta * LP * n + (size_t)j * n + k;
+        const uint64_t *u = up + (size_t)ct * beta * LP * n + (size_t)j * n + ks;
         u128 a0 = {0, 0}, a1 = {0, 0};
 #pragma unroll
         for (int b = 0; b < kMaxBeta; b++) {
@@ -85,7 +89,7 @@ __global__ void inner_product_kernel(const uint64_t *__restrict__ up, const uint
                 mac(a1, v, k1[b]);
             }
         }
-        uint64_t *o = acc + (size_t)ct * 2 * LP * n + (size_t)j * n + k;
+        uint64_t *o = acc + (size_t)ct * 2 * LP * n + (size_t)j * n + k;  // output in natural slot order
         o[0] = barrett(a0, p);
         o[(size_t)LP * n] = barrett(a1, p);
     }
@@ -128,7 +132,11 @@ __global__ void ks_combine_kernel(const uint64_t *__restrict__ acc, const uint64
     uint64_t r = shoup(sub_mod(a, dl, q), pinv[2 * j], pinv[2 * j + 1], q);
     const size_t off = (size_t)ct * o.stride + (size_t)j * n + k;
     const uint64_t *add = h ? o.add1 : o.add0;
-    if (add) r = add_mod(r, add[off], q);
+    if (add) {
+        const size_t aoff = (h == 0 && o.add0_perm) ? (size_t)ct * o.stride + (size_t)j * n + __ldg(o.add0_perm + k)
+                                                    : off;
+        r = add_mod(r, add[aoff], q);
+    }
     (h ? o.out1 : o.out0)[off] = r;
 }
 
@@ -175,7 +183,7 @@ void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_
     ntt_forward(c, up, n_cts * beta * LP, beta * LP, m, st);
     // 4. inner product with the key digits
     SHM_LAUNCHED(1); inner_product_kernel<<<dim3(n / kThreads, LP), kThreads, 0, st>>>(up, key, acc, n_cts, L, np, c.nq, beta, c.log_n,
-                                                                      c.pc);
+                                                                      c.pc, nullptr);
     SHM_CUDA(cudaGetLastError());
     // 5. ModDown: INTT of the P limbs (scaled by phat_k^-1), convert to Ql, NTT, combine
     LimbMap mp;
@@ -188,6 +196,70 @@ void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_
     SHM_LAUNCHED(1); ks_combine_kernel<<<dim3(n / kThreads, L, n_cts * 2), kThreads, 0, st>>>(acc, delta, o, L, np, c.log_n, c.pc,
                                                                              c.p_inv);
     SHM_CUDA(cudaGetLastError());
+}
+
+size_t hoisted_ws_words(const Context &c, uint32_t n_cts, uint32_t L) {
+    // x, up (kept for every element), acc and a separate delta
+    return keyswitch_ws_words(c, n_cts, L) + (size_t)n_cts * 2 * L * c.n;
+}
+
+void apply_galois_hoisted(const Context &c, const uint64_t *ct, uint32_t n_cts, uint32_t L, uint32_t n_elts,
+                          const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs, uint64_t *ws,
+                          cudaStream_t st) {
+    if (n_cts == 0 || n_elts == 0) return;
+    if (c.np == 0) throw std::invalid_argument("context has no special primes: key switching unavailable");
+    if (L < 1 || L > c.nq) throw std::invalid_argument("level out of range");
+    const uint32_t np = c.np, beta = (L + np - 1) / np, LP = L + np;
+    if (beta > c.dnum) throw std::invalid_argument("level needs more key digits than the key holds");
+    if (np > kMaxAlpha || beta > kMaxBeta || LP > 64) throw std::invalid_argument("key-switching shape too large");
+    const size_t n = c.n, ln = (size_t)L * n;
+    uint64_t *x = ws;
+    uint64_t *up = x + (size_t)n_cts * L * n;
+    uint64_t *acc = up + (size_t)n_cts * beta * LP * n;
+    uint64_t *delta = acc + (size_t)n_cts * 2 * LP * n;  // up must survive every element
+    const LevelKS &ks = c.ks[L];
+    const uint64_t *d = ct + ln;  // c1 of every ciphertext, stride 2 ln
+
+    // ModUp once (identical to keyswitch steps 1-3)
+    SHM_CUDA(cudaMemcpy2DAsync(x, ln * 8, d, 2 * ln * 8, ln * 8, n_cts, cudaMemcpyDeviceToDevice, st));
+    ntt_inverse(c, x, n_cts * L, L, q_map(L), ks.modup_scale, st);
+    SHM_LAUNCHED(1);
+    modup_conv_kernel<<<dim3(n / kThreads, beta, n_cts), kThreads, 0, st>>>(x, d, 2 * ln, up, ks.modup_conv, L, np,
+                                                                            c.nq, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+    LimbMap m;
+    for (uint32_t s = 0; s < 512; s++) {
+        if (s >= beta * LP) {
+            m.prime[s] = 255;
+            continue;
+        }
+        uint32_t b = s / LP, j = s % LP;
+        bool own = j >= b * np && j < std::min((b + 1) * np, L);
+        m.prime[s] = own ? 255 : (uint8_t)(j < L ? j : c.nq + (j - L));
+    }
+    ntt_forward(c, up, n_cts * beta * LP, beta * LP, m, st);
+    LimbMap mp;
+    for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
+
+    // per element: permuted inner product, ModDown, combine with sigma(c0)
+    for (uint32_t e = 0; e < n_elts; e++) {
+        const uint32_t *perm = const_cast<Context &>(c).perm(elts[e]);
+        SHM_LAUNCHED(1);
+        inner_product_kernel<<<dim3(n / kThreads, LP), kThreads, 0, st>>>(up, keys[e], acc, n_cts, L, np, c.nq, beta,
+                                                                          c.log_n, c.pc, perm);
+        SHM_CUDA(cudaGetLastError());
+        ntt_inverse(c, acc, n_cts * 2 * LP, LP, mp, c.moddown_scale, st, L);
+        SHM_LAUNCHED(1);
+        moddown_conv_kernel<<<dim3(n / kThreads, n_cts * 2), kThreads, 0, st>>>(acc, delta, c.moddown_conv, L, np,
+                                                                                c.log_n, c.pc);
+        SHM_CUDA(cudaGetLastError());
+        ntt_forward(c, delta, n_cts * 2 * L, L, q_map(L), st);
+        KsOutput o{outs[e], outs[e] + ln, ct, nullptr, 2 * ln, perm};
+        SHM_LAUNCHED(1);
+        ks_combine_kernel<<<dim3(n / kThreads, L, n_cts * 2), kThreads, 0, st>>>(acc, delta, o, L, np, c.log_n, c.pc,
+                                                                                 c.p_inv);
+        SHM_CUDA(cudaGetLastError());
+    }
 }
 
 }  // namespace shm

@@ -19,14 +19,23 @@ struct Geo {
 
 __device__ __forceinline__ uint32_t padded(uint32_t p) { return p + (p >> 4); }
 
+// CTAs are issued limb-major: consecutive CTAs work on the same limb slot (one prime) of
+// successive polynomials, so the CTAs in flight share one prime's twiddle table in L2.
+// rows = polys * slots; CTA index t -> (poly = t % polys, slot = t / polys).
+__device__ __forceinline__ uint32_t limb_major_row(uint32_t t, uint32_t slots, uint32_t rows) {
+    const uint32_t polys = rows / slots;
+    return (t % polys) * slots + t / polys;
+}
+
 // ---------------- forward, phase 1: columns (global stages 0 .. LOGM-1)
 template <int R>
-__global__ void __launch_bounds__(Geo<R>::THREADS) fwd_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+__global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const PrimeConst *__restrict__ pc) {
     using G = Geo<R>;
     __shared__ uint64_t sm[G::M * kNttSubs];
-    const uint32_t row = blockIdx.x / G::CHUNKS, chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t pidx = map.prime[row % slots];
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
@@ -50,12 +59,13 @@ __global__ void __launch_bounds__(Geo<R>::THREADS) fwd_col(uint64_t *__restrict_
 
 // ---------------- forward, phase 2: blocks (global stages LOGM .. 2*LOGM-1), fully reduced output
 template <int R>
-__global__ void __launch_bounds__(Geo<R>::THREADS) fwd_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+__global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const PrimeConst *__restrict__ pc) {
     using G = Geo<R>;
     __shared__ uint64_t sm[kNttSubs * G::PAD_M];
-    const uint32_t row = blockIdx.x / G::CHUNKS, chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t pidx = map.prime[row % slots];
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
@@ -89,12 +99,13 @@ __global__ void __launch_bounds__(Geo<R>::THREADS) fwd_blk(uint64_t *__restrict_
 
 // ---------------- inverse, phase 1: blocks (global stages 2*LOGM-1 .. LOGM)
 template <int R>
-__global__ void __launch_bounds__(Geo<R>::THREADS) inv_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+__global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const PrimeConst *__restrict__ pc) {
     using G = Geo<R>;
     __shared__ uint64_t sm[kNttSubs * G::PAD_M];
-    const uint32_t row = blockIdx.x / G::CHUNKS, chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t pidx = map.prime[row % slots];
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
@@ -127,14 +138,15 @@ __global__ void __launch_bounds__(Geo<R>::THREADS) inv_blk(uint64_t *__restrict_
 
 // ---------------- inverse, phase 2: columns (global stages LOGM-1 .. 0) with the folded scale
 template <int R>
-__global__ void __launch_bounds__(Geo<R>::THREADS) inv_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+__global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const PrimeConst *__restrict__ pc,
                                                             const uint64_t *__restrict__ scale, int scale_by_prime,
                                                             uint32_t scale_base) {
     using G = Geo<R>;
     __shared__ uint64_t sm[G::M * kNttSubs];
-    const uint32_t row = blockIdx.x / G::CHUNKS, chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t chunk = blockIdx.x % G::CHUNKS;
+    const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t slot = row % slots;
     const uint32_t pidx = map.prime[slot];
     if (pidx == 255) return;

@@ -148,6 +148,21 @@ class Evaluator:
             raise ValueError(f"Galois key for step {step} (elt {elt}) not present")
         return Ct(self.be.apply_galois(a.data, elt, self.galois_keys[elt]), a.scale)
 
+    def rotate_many(self, a: Ct, steps) -> dict:
+        """Rotations of the same ciphertext by several steps with one hoisted ModUp."""
+        steps = [s for s in steps if s % (self.be.n // 2)]
+        out = {}
+        if not steps:
+            return out
+        elts = [self.galois_elt(s) for s in steps]
+        for e, s in zip(elts, steps):
+            if e not in self.galois_keys:
+                raise ValueError(f"Galois key for step {s} (elt {e}) not present")
+        res = self.be.apply_galois_many(a.data, elts, [self.galois_keys[e] for e in elts])
+        for s, r in zip(steps, res):
+            out[s] = Ct(r, a.scale)
+        return out
+
     def conjugate(self, a: Ct) -> Ct:
         elt = 2 * self.be.n - 1
         if elt not in self.galois_keys:

@@ -85,6 +85,10 @@ class OracleBackend:
     def apply_galois(self, ct, elt, key):
         return np.stack([self.o.apply_galois_ct(np.ascontiguousarray(c), elt, key) for c in ct])
 
+    def apply_galois_many(self, ct, elts, keys):
+        per_ct = [self.o.apply_galois_hoisted(np.ascontiguousarray(c), elts, keys) for c in ct]
+        return [np.stack([per_ct[i][e] for i in range(len(ct))]) for e in range(len(elts))]
+
     def permute_plain(self, pt, elt):
         return np.ascontiguousarray(pt[..., O.galois_perm(self.log_n, elt)])
 
