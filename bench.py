@@ -386,6 +386,105 @@ def cpu_prim_chain():
 
 
 # ---------------------------------------------------------------------------
+# kernel workloads (config 2 and the profiling cases)
+
+CTPT = dict(n_in=768, n_out=768, L=13)  # config 2: one BERT-base projection at level 12
+
+
+def run_ctpt(args, rank, world, dist):
+    """Config 2: 768 ciphertexts at 13 limbs (N = 2^16) times a 768 x 768 integer weight
+    matrix (N(0, 0.02^2) at scale 2^40) on the INT8 tensor cores; step = the whole projection."""
+    import torch
+
+    import shmoai_b200
+    from shmoai_b200.ckks import CKKSContext
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = shmoai_b200.lib()
+    ctx = CKKSContext(BOOT["log_n"], bits=BOOT["bits"], n_special=BOOT["n_special"], device=dev)
+    n, L, n_in, n_out = ctx.n, CTPT["L"], CTPT["n_in"], CTPT["n_out"]
+    g = torch.Generator(device="cuda").manual_seed(2 + rank)
+    pr = torch.tensor(ctx.primes[:L].astype(np.int64), device="cuda").view(1, 1, L, 1)
+    X = torch.remainder(torch.randint(0, 2 ** 62, (n_in, 2, L, n), device="cuda", generator=g), pr)
+    W = torch.round(torch.randn(n_in, n_out, device="cuda", generator=g, dtype=torch.float64) * 0.02 * 2 ** 40
+                    ).to(torch.int64)
+    ws = torch.empty(ctx.workspace_bytes("ctpt", n_in, L, n_out) // 8 + 1, dtype=torch.int64, device="cuda")
+    Y = torch.empty(n_out, 2, L, n, dtype=torch.int64, device="cuda")
+
+    def step():
+        ctx.ctpt_matmul(X, W, out=Y, workspace=ws)
+
+    clk = ClockSampler(dev).start()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    l0 = lib.shm_kernel_launches()
+    ms = timed_steps(torch, step, args.steps, dist, None)  # X and Y (20 GB) exceed L2
+    launches = lib.shm_kernel_launches() - l0
+    macs = n_in * n_out * 2 * L * n
+    peak_i8 = 4500.0  # dense INT8 TOPS, datasheet (not measured on this pool)
+    res = {
+        "metric": "ct-pt matmul output ciphertexts/s (768 -> 768, 13 limbs, N=2^16, exact)",
+        "value": round(world * n_out * 1000.0 / ms, 2), "unit": "output ciphertexts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (int8 tensor-core residues)",
+        "data": "synthetic (uniform residues; W ~ N(0, 0.02^2) * 2^40)",
+        "config": {"workload": "ctpt: config 2, one 768x768 projection per GPU per step", "n_in": n_in,
+                   "n_out": n_out, "L": L, "N": n, "modular_macs": macs},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "whole projection", "bound": "tensor",
+                     "achieved": round(macs * 13 * 2 / (ms * 1e-3) / 1e12, 1), "peak": peak_i8,
+                     "unit": "TOPS (int8, 13 residue GEMMs)",
+                     "frac": round(macs * 13 * 2 / (ms * 1e-3) / 1e12 / peak_i8, 4),
+                     "peak_source": "datasheet dense INT8 (no measured INT8 peak)", "traffic": None},
+        "clocks": clk.summary(),
+    }
+    return res
+
+
+def run_kernel_case(args, rank, world, dist):
+    """Profiling cases: 'ntt' = forward NTT of 4095 limbs (2 GB, > L2) at the bootstrap primes;
+    'ks' = one hoisted-free rotation of 4 ciphertexts at 35 limbs (the C2S key switch)."""
+    import torch
+
+    from shmoai_b200.ckks import CKKSContext
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    ctx = CKKSContext(BOOT["log_n"], bits=BOOT["bits"], n_special=BOOT["n_special"], device=dev)
+    n, L, QP = ctx.n, 35, 40
+    g = torch.Generator(device="cuda").manual_seed(3)
+    pr = torch.tensor(ctx.primes.astype(np.int64), device="cuda")
+    if args.workload == "ntt":
+        x = torch.remainder(torch.randint(0, 2 ** 62, (117, L, n), device="cuda", generator=g), pr[:L].view(1, L, 1))
+
+        def step():
+            ctx.ntt_forward_(x)
+        unit, per = "limbs/s", 117 * L
+    else:
+        ct = torch.remainder(torch.randint(0, 2 ** 62, (4, 2, L, n), device="cuda", generator=g),
+                             pr[:L].view(1, 1, L, 1))
+        key = torch.remainder(torch.randint(0, 2 ** 62, (7, 2, QP, n), device="cuda", generator=g),
+                              pr.view(1, 1, QP, 1))
+        ws = torch.empty(ctx.workspace_bytes("keyswitch", 4, L) // 8 + 4 * 2 * L * n, dtype=torch.int64,
+                         device="cuda")
+        out = torch.empty_like(ct)
+
+        def step():
+            ctx.rotate(ct, 1, key, out=out, workspace=ws)
+        unit, per = "ciphertext rotations/s", 4
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ms = timed_steps(torch, step, args.steps, dist, None)
+    return {"metric": f"{args.workload} kernel case", "value": round(per * 1000.0 / ms, 2), "unit": unit,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic", "config": {"workload": args.workload}}
+
+
+# ---------------------------------------------------------------------------
 
 
 def main():
@@ -394,7 +493,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="boot", choices=["boot", "prim"])
+    ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks"])
     ap.add_argument("--batch", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -438,9 +537,11 @@ def main():
 
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
-    res = run_boot(args, rank, world, dist) if args.workload == "boot" else run_prim(args, rank, world, dist)
+    runner = {"boot": run_boot, "prim": run_prim, "ctpt": run_ctpt, "ntt": run_kernel_case,
+              "ks": run_kernel_case}[args.workload]
+    res = runner(args, rank, world, dist)
     if rank == 0:
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and args.workload in ("boot", "prim"):
             if args.workload == "boot":
                 v, cores, sample = cpu_boot_estimate()
                 res["cpu_baseline"] = {"value": round(v, 6), "unit": "bootstraps/s", "cores": cores,

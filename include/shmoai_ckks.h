@@ -175,8 +175,16 @@ int shm_drop_limbs(const shm_context *ctx, const uint64_t *in, uint64_t *out, ui
  * rescale.  Replaces the multiply_plain + add_inplace loop of
  * ct_pt_matrix_mul_wo_pre (src/include/source/matrix_mul/Ct_pt_matrix_mul.cuh:112-158). */
 size_t shm_ctpt_matmul_workspace_bytes(const shm_context *ctx, uint32_t n_in, uint32_t n_out, uint32_t L);
+/* Computed on the INT8 tensor cores (tcgen05.mma kind::i8) through a small-modulus
+ * residue system: exact for |W| < 2^40 (larger weights: SHM_EINVAL).  The call
+ * reads W back to the host once to size the residue system, so it synchronises
+ * `stream`. */
 int shm_ctpt_matmul(const shm_context *ctx, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in,
                     uint32_t n_out, uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
+/* The same contraction on the CUDA cores (64-bit multiply-accumulate, |W| < 2^40):
+ * the plain path the tensor-core kernel is measured against. */
+int shm_ctpt_matmul_cuda_core(const shm_context *ctx, const uint64_t *X, const int64_t *W, uint64_t *Y,
+                              uint32_t n_in, uint32_t n_out, uint32_t L, void *stream);
 
 #ifdef __cplusplus
 }

@@ -64,6 +64,7 @@ def _declare(L):
         "shm_modraise": (ctypes.c_int, [_P, _P, _P, _U32, _U32, _P, _SZ, _P]),
         "shm_drop_limbs": (ctypes.c_int, [_P, _P, _P, _U32, _U32, _U32, _P]),
         "shm_ctpt_matmul_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),
+        "shm_ctpt_matmul_cuda_core": (ctypes.c_int, [_P, _P, _P, _P, _U32, _U32, _U32, _P]),
         "shm_ctpt_matmul": (ctypes.c_int, [_P, _P, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
     }
     for name, (res, args) in sig.items():

@@ -552,6 +552,16 @@ int shm_ctpt_matmul(const shm_context *ctx, const uint64_t *X, const int64_t *W,
     });
 }
 
+int shm_ctpt_matmul_cuda_core(const shm_context *ctx, const uint64_t *X, const int64_t *W, uint64_t *Y,
+                              uint32_t n_in, uint32_t n_out, uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::ctpt_matmul_cuda_core(c, X, W, Y, n_in, n_out, L, S(stream));
+    });
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

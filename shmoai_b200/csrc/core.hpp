@@ -126,6 +126,12 @@ void modraise(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_po
 
 void ctpt_matmul(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
                  uint32_t L, uint64_t *ws, cudaStream_t st);
+void ctpt_matmul_cuda_core(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in,
+                           uint32_t n_out, uint32_t L, cudaStream_t st);
+size_t ctpt_tc_ws_bytes(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);
+void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
+                    uint32_t L, void *ws, uint64_t max_abs_w, cudaStream_t st);
+int ctpt_tc_error(void *ws, cudaStream_t st);
 size_t ctpt_ws_words(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);
 
 }  // namespace shm

@@ -63,15 +63,32 @@ __global__ void __launch_bounds__(kCtThreads) ctpt_cuda_core(const uint64_t *__r
 
 }  // namespace
 
-size_t ctpt_ws_words(const Context &, uint32_t, uint32_t, uint32_t) { return 0; }
-
-void ctpt_matmul(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
-                 uint32_t L, uint64_t *, cudaStream_t st) {
+void ctpt_matmul_cuda_core(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in,
+                           uint32_t n_out, uint32_t L, cudaStream_t st) {
     if (n_in == 0 || n_out == 0) return;
     if (L < 1 || L > c.nq) throw std::invalid_argument("level out of range");
     dim3 grid(c.n / kCtThreads, 2 * L, (n_out + kOutTile - 1) / kOutTile);
     SHM_LAUNCHED(1); ctpt_cuda_core<<<grid, kCtThreads, 0, st>>>(X, W, Y, n_in, n_out, L, c.log_n, c.pc);
     SHM_CUDA(cudaGetLastError());
+}
+
+size_t ctpt_ws_words(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L) {
+    return (ctpt_tc_ws_bytes(c, n_in, n_out, L) + 7) / 8;
+}
+
+void ctpt_matmul(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
+                 uint32_t L, uint64_t *ws, cudaStream_t st) {
+    if (n_in == 0 || n_out == 0) return;
+    if (L < 1 || L > c.nq) throw std::invalid_argument("level out of range");
+    // the residue system is sized from max|W| (one small device-to-host copy of the weights)
+    std::vector<int64_t> hw((size_t)n_in * n_out);
+    SHM_CUDA(cudaMemcpyAsync(hw.data(), W, hw.size() * 8, cudaMemcpyDeviceToHost, st));
+    SHM_CUDA(cudaStreamSynchronize(st));
+    uint64_t mx = 0;
+    for (int64_t w : hw) mx = std::max<uint64_t>(mx, w < 0 ? (uint64_t)(-(w + 1)) + 1 : (uint64_t)w);
+    if (mx >= (1ull << 40)) throw std::invalid_argument("ct-pt matmul: |W| must be below 2^40");
+    ctpt_matmul_tc(c, X, W, Y, n_in, n_out, L, ws, mx, st);
+    if (ctpt_tc_error(ws, st)) throw CudaError("ct-pt matmul: tensor-core pipeline wait timed out");
 }
 
 }  // namespace shm

@@ -37,12 +37,17 @@ constexpr uint32_t kStageA = kBM * kKB;  // 8 KB
 constexpr uint32_t kStageB = kBN * kKB;  // 16 KB
 constexpr uint32_t kSmem = kStages * (kStageA + kStageB) + 1024;
 constexpr uint32_t kThreads = 128;
-constexpr long long kSpinLimit = 1ll << 28;
+constexpr long long kSpinLimit = 1ll << 24;
 
 struct ModTab {
     uint32_t t;
     uint32_t m[kMaxMods];
-    float frac[kMaxMods];  // [(M/m_t)^-1]_{m_t} / m_t
+    float frac[kMaxMods];   // [(M/m_t)^-1]_{m_t} / m_t
+    uint32_t c24[kMaxMods];  // 2^20 mod m_t
+    uint32_t c48[kMaxMods];  // 2^40 mod m_t
+    uint32_t magic[kMaxMods];  // ceil(2^32 / m_t)
+    double inv[kMaxMods];    // 1 / m_t
+    float invf[kMaxMods];
 };
 
 __constant__ ModTab c_mods;
@@ -50,12 +55,24 @@ __constant__ ModTab c_mods;
 // ---------------------------------------------------------------- residues
 __device__ __forceinline__ int8_t balanced(uint32_t r, uint32_t m) { return (int8_t)(r > m / 2 ? (int)r - (int)m : (int)r); }
 
-__device__ __forceinline__ uint32_t mod_small(uint64_t x, uint32_t m) {
-    // x = a 2^48 + b 2^24 + d; every partial term stays below 2^32
-    uint32_t a = (uint32_t)(x >> 48), b = (uint32_t)((x >> 24) & 0xFFFFFF), d = (uint32_t)(x & 0xFFFFFF);
-    uint32_t c24 = (1u << 24) % m, c48 = (uint32_t)(((uint64_t)c24 * c24) % m);
-    uint64_t s = (uint64_t)a * c48 + (uint64_t)b * c24 + d;
-    return (uint32_t)(s % m);
+// x mod m_t for x < 2^61 in 32-bit arithmetic: x = a 2^40 + b 2^20 + d (a < 2^21, b, d < 2^20)
+// folds to s = a (2^40 mod m) + b (2^20 mod m) + d < 2^30; the quotient
+// umulhi(s, ceil(2^32 / m)) is floor(s / m) or one more.
+__device__ __forceinline__ uint32_t mod_small(uint64_t x, uint32_t t) {
+    const uint32_t m = c_mods.m[t];
+    const uint32_t a = (uint32_t)(x >> 40), b = (uint32_t)(x >> 20) & 0xFFFFF, d = (uint32_t)x & 0xFFFFF;
+    const uint32_t s = a * c_mods.c48[t] + b * c_mods.c24[t] + d;
+    int r = (int)(s - __umulhi(s, c_mods.magic[t]) * m);
+    return (uint32_t)(r < 0 ? r + (int)m : r);
+}
+
+// a mod m_t in [0, m_t) for any int32 accumulator (exact in a double; |a| < n_in * 125^2)
+__device__ __forceinline__ uint32_t mod_acc(int a, uint32_t t) {
+    const int m = (int)c_mods.m[t];
+    int r = a - (int)floor((double)a * c_mods.inv[t]) * m;
+    if (r < 0) r += m;
+    else if (r >= m) r -= m;
+    return (uint32_t)r;
 }
 
 // X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via a 64 x 64 shared-memory transpose
@@ -73,10 +90,10 @@ __global__ void xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__
     const uint64_t chunk = (uint64_t)gridDim.x * 64;
     for (uint32_t rr = ty; rr < 64; rr += 4) {
         uint64_t x = tile[tx][rr];
-        for (uint32_t t = 0; t < c_mods.t; t++) {
-            uint32_t m = c_mods.m[t];
-            XP[((uint64_t)t * chunk + rb + rr) * Kp + i0 + tx] = balanced(mod_small(x, m), m);
-        }
+#pragma unroll
+        for (uint32_t t = 0; t < kMaxMods; t++)
+            if (t < c_mods.t)
+                XP[((uint64_t)t * chunk + rb + rr) * Kp + i0 + tx] = balanced(mod_small(x, t), c_mods.m[t]);
     }
 }
 
@@ -226,7 +243,6 @@ __global__ void __launch_bounds__(kThreads, 1) mma_kernel(const int8_t *__restri
         if (lane == 0) atomicExch(err, 1);
     } else {
         // epilogue: warp w reads TMEM lanes 32w..32w+31 (X columns), 32 output columns at a time
-        const uint32_t m = c_mods.m[t];
         const uint64_t r = rbase + warp * 32 + lane;
         for (uint32_t c0 = 0; c0 < kBN; c0 += 32) {
             uint32_t v[32];
@@ -245,11 +261,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_kernel(const int8_t *__restri
 #pragma unroll
             for (int j = 0; j < 32; j++) {
                 const uint32_t o = obase + c0 + j;
-                if (o < n_out) {
-                    int a = (int)v[j] % (int)m;
-                    if (a < 0) a += m;
-                    RES[((uint64_t)t * n_out + o) * chunk + r] = (uint8_t)a;
-                }
+                if (o < n_out) RES[((uint64_t)t * n_out + o) * chunk + r] = (uint8_t)mod_acc((int)v[j], t);
             }
         }
     }
@@ -273,13 +285,25 @@ __global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict
     const uint64_t rg = r0 + r;
     const uint32_t limb = (uint32_t)((rg >> log_n) % L);
     const CrtLimb &cl = tab[limb];
-    u128 pos = {0, 0};
+    // sum_t r_t c_t as two 64-bit partial sums over the 32-bit halves of c_t (r_t < 2^8)
+    uint64_t lo = 0, hi = 0;
     float v = 0.f;
-    for (uint32_t t = 0; t < c_mods.t; t++) {
-        uint32_t rt = RES[((uint64_t)t * n_out + o) * chunk + r];
-        mac(pos, rt, cl.c[t]);
-        v += (float)rt * c_mods.frac[t];
+    const uint32_t T = c_mods.t;
+    uint32_t res[kMaxMods];
+#pragma unroll
+    for (uint32_t t = 0; t < kMaxMods; t++)  // all loads in flight before any use
+        res[t] = t < T ? RES[((uint64_t)t * n_out + o) * chunk + r] : 0u;
+#pragma unroll
+    for (uint32_t t = 0; t < kMaxMods; t++) {
+        if (t < T) {
+            const uint32_t rt = res[t];
+            const uint64_t c = cl.c[t];
+            lo += (uint64_t)rt * (uint32_t)c;
+            hi += (uint64_t)rt * (uint32_t)(c >> 32);
+            v += (float)rt * c_mods.frac[t];
+        }
     }
+    u128 pos = {lo + (hi << 32), (hi >> 32) + ((lo + (hi << 32)) < lo ? 1ull : 0ull)};
     const uint64_t vi = (uint64_t)(int64_t)rintf(v);
     const PrimeConst p = pc[limb];
     const uint64_t y = sub_mod(barrett(pos, p), barrett(mul_wide(vi, cl.M), p), p.q);
@@ -321,6 +345,11 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
             if (u != t) Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (p.mods.m[u] % m) % m);
         uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);  // m prime
         p.mods.frac[t] = (float)inv / (float)m;
+        p.mods.c24[t] = (1u << 20) % m;
+        p.mods.c48[t] = (uint32_t)((uint64_t)p.mods.c24[t] * p.mods.c24[t] % m);
+        p.mods.magic[t] = (uint32_t)(((1ull << 32) + m - 1) / m);
+        p.mods.inv[t] = 1.0 / m;
+        p.mods.invf[t] = 1.0f / (float)m;
     }
     p.limbs.resize(L);
     for (uint32_t l = 0; l < L; l++) {
@@ -380,11 +409,7 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     SHM_LAUNCHED(1);
     wres_kernel<<<dim3((Kp + 255) / 256, Np), 256, 0, st>>>(W, WP, n_in, n_out, Kp, Np);
     SHM_CUDA(cudaGetLastError());
-    static bool attr_set = false;
-    if (!attr_set) {
-        SHM_CUDA(cudaFuncSetAttribute(mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
-        attr_set = true;
-    }
+    SHM_CUDA(cudaFuncSetAttribute(mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
     for (uint64_t r0 = 0; r0 < R; r0 += chunk) {
         SHM_LAUNCHED(1);
         xres_kernel<<<dim3((uint32_t)(chunk / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0);
