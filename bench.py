@@ -237,10 +237,13 @@ def run_boot(args, rank, world, dist):
         o = bs.bootstrap(Ct(d_in, ct.scale))
         h_out.copy_(o.data, non_blocking=True)
 
-    e2e_step()
-    torch.cuda.synchronize()
-    e2e_ms = timed_steps(torch, e2e_step, max(1, args.steps // 2), dist, None)
-    roof = ntt_roofline(torch, ctx, BOOT["bits"].__len__() - BOOT["n_special"])
+    if args.no_extras:
+        e2e_ms, roof = ms, None
+    else:
+        e2e_step()
+        torch.cuda.synchronize()
+        e2e_ms = timed_steps(torch, e2e_step, max(1, args.steps // 2), dist, None)
+        roof = ntt_roofline(torch, ctx, BOOT["bits"].__len__() - BOOT["n_special"])
     clocks = clk.summary()
     return {
         "metric": BOOT_METRIC, "value": round(world * B * 1000.0 / ms, 3), "unit": "bootstraps/s",
@@ -496,7 +499,13 @@ def main():
     ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks"])
     ap.add_argument("--batch", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="time the step only (no e2e, roofline or CPU legs): used for ncu launch lists")
+    ap.add_argument("--small", action="store_true",
+                    help="ctpt: 256 -> 256 ciphertexts at 4 limbs (about 1 GB on the device) for ncu captures")
     args = ap.parse_args()
+    if args.small:
+        CTPT.update(n_in=256, n_out=256, L=4)
     if args.batch is None:
         args.batch = 32 if args.workload == "boot" else 1
 

@@ -135,6 +135,36 @@ size_t shm_apply_galois_hoisted_workspace_bytes(const shm_context *ctx, uint32_t
 int shm_apply_galois_hoisted(const shm_context *ctx, const uint64_t *ct, uint32_t n_elts, const uint32_t *elts,
                              const uint64_t *const *keys, uint64_t *const *outs, uint32_t n_cts, uint32_t L,
                              void *workspace, size_t workspace_bytes, void *stream);
+/* Shared-a batches (multi-secret RLWE): n_groups groups of n_members ciphertexts,
+ * each group stored as [n_members + 1][L][N] = (b_0 .. b_{n-1}, a) with
+ * b_i + a s'_i ~ m_i (src/include/source/bootstrapping/SharedACiphertext.cuh:9-21).
+ *
+ * Sh-Rot of every group by each of n_elts Galois elements with one ModUp of the
+ * shared a (hoisted): keys[e] is [dnum][n_members + 1][QP][N] (halves B_0..B_{n-1}, A),
+ * outs[e] receives the rotated batch.  Replaces shared_a_rotate
+ * (src/include/source/bootstrapping/ShRotate.cu:201-257). */
+size_t shm_shared_rotate_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members, uint32_t L);
+int shm_shared_rotate_hoisted(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members,
+                              uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs,
+                              uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
+/* FmtSwitch forward: n_groups * n_members ordinary ciphertexts [.][2][L][N] under s
+ * -> shared-a batch [n_groups][n_members + 1][L][N] under s'_i, with the format key
+ * [n_members][n_members + 1][QP][N] (halves B_fmt[j][0..n-1], a_fmt[j]); the a_j are
+ * extended exactly from Ql to QlP.  Replaces fmt_switch_forward
+ * (src/include/source/bootstrapping/FmtSwitch.cu:276-394). */
+size_t shm_fmt_switch_forward_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                              uint32_t L);
+int shm_fmt_switch_forward(const shm_context *ctx, const uint64_t *cts, uint32_t n_groups, uint32_t n_members,
+                           const uint64_t *key, uint64_t *out, uint32_t L, void *workspace, size_t workspace_bytes,
+                           void *stream);
+/* FmtSwitch backward: shared-a batch -> n_groups * n_members ordinary ciphertexts
+ * under s, keys[i] the switching key s'_i -> s ([dnum][2][QP][N]); one ModUp of each
+ * shared a serves all members.  Replaces fmt_switch_backward (FmtSwitch.cu:396-429). */
+size_t shm_fmt_switch_backward_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                               uint32_t L);
+int shm_fmt_switch_backward(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members,
+                            const uint64_t *const *keys, uint64_t *out, uint32_t L, void *workspace,
+                            size_t workspace_bytes, void *stream);
 /* Galois element of a rotation by `step` slots (0 = conjugation).
  * Replaces PhantomGaloisTool::get_elt_from_step (src/galois.cu:47-91). */
 uint32_t shm_galois_elt_from_step(const shm_context *ctx, int step);

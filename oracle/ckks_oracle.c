@@ -502,6 +502,149 @@ void orc_apply_galois_hoisted(const orc_ctx *c, const uint64_t *ct, uint32_t L, 
     free(up);
 }
 
+/* ---------------- shared-a batches (multi-secret RLWE) -----------------------
+ * One group = [n+1][L][N] = (b_0 .. b_{n-1}, a), b_i + a s'_i ~ m_i
+ * (src/include/source/bootstrapping/SharedACiphertext.cuh:9-21).                */
+
+/* inner products of the extended digits ext [beta][LP][N] (read at perm[k]) with
+ * key halves key [beta][H][QP][N] -> cx [H][LP][N] */
+static void ip_multi(const orc_ctx *c, const uint64_t *ext, uint32_t beta, uint32_t L, const uint64_t *key, uint32_t H,
+                     const uint32_t *perm, uint64_t *cx) {
+    size_t n = c->n;
+    uint32_t LP = L + c->np, QP = c->nq + c->np;
+#pragma omp parallel for
+    for (int j = 0; j < (int)LP; j++) {
+        uint32_t pj = ext_prime(c, L, j);
+        uint64_t t = c->primes[pj];
+        for (size_t k = 0; k < n; k++) {
+            size_t ks = perm ? perm[k] : k;
+            for (uint32_t h = 0; h < H; h++) {
+                u128 a = 0;
+                for (uint32_t b = 0; b < beta; b++)
+                    a = (a + (u128)ext[((size_t)b * LP + j) * n + ks] *
+                                 key[(((size_t)b * H + h) * QP + pj) * n + k]) % t;
+                cx[((size_t)h * LP + j) * n + k] = (uint64_t)a;
+            }
+        }
+    }
+}
+
+/* Sh-Rot (ShRotate.cu:201-257), hoisted over several elements: one ModUp of a, then per
+ * element g: b'_i = sigma_g(b_i) + ModDown(<up, B_i>), a' = ModDown(<up, A>).
+ * keys[e]: [dnum][n+1][QP][N]; outs[e]: [n+1][L][N]. */
+void orc_shared_rotate_hoisted(const orc_ctx *c, const uint64_t *sh, uint32_t n_mem, uint32_t L, uint32_t n_elts,
+                               const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs) {
+    size_t n = c->n, ln = (size_t)L * n;
+    uint32_t alpha = c->np, beta = (L + alpha - 1) / alpha, LP = L + c->np, H = n_mem + 1;
+    uint64_t *up = (uint64_t *)malloc(sizeof(uint64_t) * beta * LP * n);
+    orc_modup(c, sh + (size_t)n_mem * ln, L, up);
+    uint32_t *perm = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * H * LP * n);
+    for (uint32_t e = 0; e < n_elts; e++) {
+        orc_galois_perm(c->log_n, elts[e], perm);
+        ip_multi(c, up, beta, L, keys[e], H, perm, cx);
+        for (uint32_t h = 0; h < H; h++) {
+            uint64_t *o = outs[e] + (size_t)h * ln;
+            moddown_one(c, cx + (size_t)h * LP * n, L, o);
+            if (h < n_mem) {
+                const uint64_t *b = sh + (size_t)h * ln;
+                for (uint32_t i = 0; i < L; i++)
+                    for (size_t k = 0; k < n; k++)
+                        o[(size_t)i * n + k] = addmod(o[(size_t)i * n + k], b[(size_t)i * n + perm[k]], c->primes[i]);
+            }
+        }
+    }
+    free(cx);
+    free(perm);
+    free(up);
+}
+
+/* Exact extension of a (NTT form, L limbs) to QlP: the Ql rows keep a, the P rows get
+ * (sum_i y_i qhat_i - v Q) mod p_k with y_i = [x_i qhat_i^-1]_{q_i} (x = INTT(a)) and
+ * v = floor(sum_i y_i / q_i) in double arithmetic (FmtSwitch.cu:82-108). */
+static void exact_extend(const orc_ctx *c, const uint64_t *a, uint32_t L, uint64_t *ext) {
+    size_t n = c->n;
+    uint32_t LP = L + c->np;
+    uint64_t *y = (uint64_t *)malloc(sizeof(uint64_t) * L * n);
+    memcpy(y, a, sizeof(uint64_t) * L * n);
+    memcpy(ext, a, sizeof(uint64_t) * L * n);
+    for (uint32_t i = 0; i < L; i++) {
+        uint64_t qi = c->primes[i], h = 1;
+        orc_ntt_inv(y + (size_t)i * n, c->log_n, qi, c->irp + (size_t)i * n);
+        for (uint32_t k = 0; k < L; k++)
+            if (k != i) h = mulmod(h, c->primes[k] % qi, qi);
+        uint64_t hinv = orc_invmod(h, qi);
+        for (size_t t = 0; t < n; t++) y[(size_t)i * n + t] = mulmod(y[(size_t)i * n + t], hinv, qi);
+    }
+#pragma omp parallel for
+    for (int kk = 0; kk < (int)c->np; kk++) {
+        uint32_t pk = c->nq + kk;
+        uint64_t p = c->primes[pk], Qm = 1, hm[64];
+        for (uint32_t i = 0; i < L; i++) {
+            uint64_t h = 1;
+            for (uint32_t k = 0; k < L; k++)
+                if (k != i) h = mulmod(h, c->primes[k] % p, p);
+            hm[i] = h;
+            Qm = mulmod(Qm, c->primes[i] % p, p);
+        }
+        uint64_t *o = ext + (size_t)(L + kk) * n;
+        for (size_t t = 0; t < n; t++) {
+            double frac = 0.0;
+            u128 acc = 0;
+            for (uint32_t i = 0; i < L; i++) {
+                uint64_t yi = y[(size_t)i * n + t];
+                double prod = (double)yi * (1.0 / (double)c->primes[i]);
+                frac = frac + prod;
+                acc += (u128)yi * hm[i];
+            }
+            uint64_t v = (uint64_t)frac;
+            o[t] = submod((uint64_t)(acc % p), mulmod(v, Qm, p), p);
+        }
+        orc_ntt_fwd(o, c->log_n, p, c->rp + (size_t)pk * n);
+    }
+    (void)LP;
+    free(y);
+}
+
+/* FmtSwitch forward (FmtSwitch.cu:276-394) of one group: cts [n][2][L][N] under s ->
+ * out [n+1][L][N] under s'_i with key [n][n+1][QP][N] (B_fmt[j][i], a_fmt[j]). */
+void orc_fmt_forward(const orc_ctx *c, const uint64_t *cts, uint32_t n_mem, uint32_t L, const uint64_t *key,
+                     uint64_t *out) {
+    size_t n = c->n, ln = (size_t)L * n;
+    uint32_t LP = L + c->np, H = n_mem + 1;
+    uint64_t *ext = (uint64_t *)malloc(sizeof(uint64_t) * n_mem * LP * n);
+    for (uint32_t j = 0; j < n_mem; j++) exact_extend(c, cts + ((size_t)j * 2 + 1) * ln, L, ext + (size_t)j * LP * n);
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * H * LP * n);
+    ip_multi(c, ext, n_mem, L, key, H, NULL, cx);
+    for (uint32_t h = 0; h < H; h++) {
+        uint64_t *o = out + (size_t)h * ln;
+        moddown_one(c, cx + (size_t)h * LP * n, L, o);
+        if (h < n_mem) orc_add(c, o, cts + (size_t)h * 2 * ln, o, 1, L);
+    }
+    free(cx);
+    free(ext);
+}
+
+/* FmtSwitch backward (FmtSwitch.cu:396-429) of one group, hoisted: one ModUp of a, then
+ * member i -> (b_i + cx0, cx1) with keys[i] [dnum][2][QP][N]; out [n][2][L][N]. */
+void orc_fmt_backward(const orc_ctx *c, const uint64_t *sh, uint32_t n_mem, uint32_t L, const uint64_t *const *keys,
+                      uint64_t *out) {
+    size_t n = c->n, ln = (size_t)L * n;
+    uint32_t alpha = c->np, beta = (L + alpha - 1) / alpha, LP = L + c->np;
+    uint64_t *up = (uint64_t *)malloc(sizeof(uint64_t) * beta * LP * n);
+    orc_modup(c, sh + (size_t)n_mem * ln, L, up);
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * 2 * LP * n);
+    for (uint32_t i = 0; i < n_mem; i++) {
+        ip_multi(c, up, beta, L, keys[i], 2, NULL, cx);
+        uint64_t *o = out + (size_t)i * 2 * ln;
+        moddown_one(c, cx, L, o);
+        moddown_one(c, cx + (size_t)LP * n, L, o + ln);
+        orc_add(c, o, sh + (size_t)i * ln, o, 1, L);
+    }
+    free(cx);
+    free(up);
+}
+
 /* Relinearize a size-3 ciphertext: (c0 + cx0, c1 + cx1) with cx = KS(c2). */
 void orc_relinearize(const orc_ctx *c, const uint64_t *ct3, uint32_t L, const uint64_t *key, uint32_t dnum,
                      uint64_t *out) {

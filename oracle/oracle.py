@@ -69,6 +69,10 @@ def lib():
         L.orc_ctpt_matmul.argtypes = [vp, _u64p, ctypes.POINTER(ctypes.c_int64), u32, u32, u32, _u64p]
         L.orc_apply_galois_hoisted.argtypes = [vp, _u64p, u32, u32, ctypes.POINTER(ctypes.c_uint32),
                                                ctypes.POINTER(_u64p), u32, ctypes.POINTER(_u64p)]
+        L.orc_shared_rotate_hoisted.argtypes = [vp, _u64p, u32, u32, u32, ctypes.POINTER(ctypes.c_uint32),
+                                                ctypes.POINTER(_u64p), ctypes.POINTER(_u64p)]
+        L.orc_fmt_forward.argtypes = [vp, _u64p, u32, u32, _u64p, _u64p]
+        L.orc_fmt_backward.argtypes = [vp, _u64p, u32, u32, ctypes.POINTER(_u64p), _u64p]
         L.orc_signed_residue.argtypes = [ctypes.c_int64, u64]
         L.orc_signed_residue.restype = u64
         _lib = L
@@ -206,6 +210,38 @@ class Oracle:
         op = (_u64p * len(outs))(*[_p(o) for o in outs])
         lib().orc_apply_galois_hoisted(self._h, _p(ct), L, len(elts), e, kp, self.dnum, op)
         return outs
+
+    # ---- shared-a groups [n + 1][L][N] = (b_0 .. b_{n-1}, a)
+    def shared_rotate_hoisted(self, sh, elts, keys):
+        """One ModUp of a; per element a rotated group with keys[e] [dnum][n+1][QP][N]."""
+        H, L = sh.shape[0], sh.shape[1]
+        sh = np.ascontiguousarray(sh, dtype=np.uint64)
+        keys = [np.ascontiguousarray(k, dtype=np.uint64) for k in keys]
+        outs = [np.empty((H, L, self.n), dtype=np.uint64) for _ in elts]
+        e = (ctypes.c_uint32 * len(elts))(*elts)
+        kp = (_u64p * len(keys))(*[_p(k) for k in keys])
+        op = (_u64p * len(outs))(*[_p(o) for o in outs])
+        lib().orc_shared_rotate_hoisted(self._h, _p(sh), H - 1, L, len(elts), e, kp, op)
+        return outs
+
+    def fmt_forward(self, cts, key):
+        """[n][2][L][N] ciphertexts under s -> one shared-a group [n+1][L][N]."""
+        m, _, L, _ = cts.shape
+        cts = np.ascontiguousarray(cts, dtype=np.uint64)
+        key = np.ascontiguousarray(key, dtype=np.uint64)
+        out = np.empty((m + 1, L, self.n), dtype=np.uint64)
+        lib().orc_fmt_forward(self._h, _p(cts), m, L, _p(key), _p(out))
+        return out
+
+    def fmt_backward(self, sh, keys):
+        """shared-a group [n+1][L][N] -> [n][2][L][N] under s; keys[i] [dnum][2][QP][N]."""
+        H, L = sh.shape[0], sh.shape[1]
+        sh = np.ascontiguousarray(sh, dtype=np.uint64)
+        keys = [np.ascontiguousarray(k, dtype=np.uint64) for k in keys]
+        out = np.empty((H - 1, 2, L, self.n), dtype=np.uint64)
+        kp = (_u64p * len(keys))(*[_p(k) for k in keys])
+        lib().orc_fmt_backward(self._h, _p(sh), H - 1, L, kp, _p(out))
+        return out
 
     def ctpt_matmul(self, X, W):
         n_in, _, L, _ = X.shape

@@ -66,6 +66,14 @@ def _declare(L):
         "shm_ctpt_matmul_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),
         "shm_ctpt_matmul_cuda_core": (ctypes.c_int, [_P, _P, _P, _P, _U32, _U32, _U32, _P]),
         "shm_ctpt_matmul": (ctypes.c_int, [_P, _P, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
+        "shm_shared_rotate_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),
+        "shm_shared_rotate_hoisted": (ctypes.c_int, [_P, _P, _U32, _U32, _U32, ctypes.POINTER(_U32),
+                                                     ctypes.POINTER(_P), ctypes.POINTER(_P), _U32, _P, _SZ, _P]),
+        "shm_fmt_switch_forward_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),
+        "shm_fmt_switch_forward": (ctypes.c_int, [_P, _P, _U32, _U32, _P, _P, _U32, _P, _SZ, _P]),
+        "shm_fmt_switch_backward_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),
+        "shm_fmt_switch_backward": (ctypes.c_int, [_P, _P, _U32, _U32, ctypes.POINTER(_P), _P, _U32, _P, _SZ,
+                                                   _P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

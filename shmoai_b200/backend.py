@@ -117,6 +117,41 @@ class GpuBackend:
                                              self._s()))
         return outs
 
+    # ---- shared-a groups [G][n + 1][L][N] = (b_0 .. b_{n-1}, a)
+    def sh_rotate_many(self, sh, elts, keys):
+        """Sh-Rot of every group, one ModUp of each a serving all elements."""
+        G, H, L = sh.shape[0], sh.shape[1], sh.shape[2]
+        outs = [torch.empty_like(sh) for _ in elts]
+        ws = self.workspace(lib().shm_shared_rotate_workspace_bytes(self.ctx._h, G, H - 1, L) // 8)
+        k = len(elts)
+        E = (ctypes.c_uint32 * k)(*elts)
+        K = (ctypes.c_void_p * k)(*[_ptr(x).value for x in keys])
+        O = (ctypes.c_void_p * k)(*[_ptr(x).value for x in outs])
+        check(lib().shm_shared_rotate_hoisted(self.ctx._h, _ptr(sh), G, H - 1, k, E, K, O, L, _ptr(ws),
+                                              ws.numel() * 8, self._s()))
+        return outs
+
+    def fmt_forward(self, cts, n, key):
+        """[G * n][2][L][N] ciphertexts under s -> [G][n + 1][L][N] shared-a groups."""
+        m, L = cts.shape[0], cts.shape[2]
+        G = m // n
+        out = torch.empty((G, n + 1, L, self.n), dtype=cts.dtype, device=cts.device)
+        ws = self.workspace(lib().shm_fmt_switch_forward_workspace_bytes(self.ctx._h, G, n, L) // 8)
+        check(lib().shm_fmt_switch_forward(self.ctx._h, _ptr(cts), G, n, _ptr(key), _ptr(out), L, _ptr(ws),
+                                           ws.numel() * 8, self._s()))
+        return out
+
+    def fmt_backward(self, sh, keys):
+        """[G][n + 1][L][N] shared-a groups -> [G * n][2][L][N] ciphertexts under s."""
+        G, H, L = sh.shape[0], sh.shape[1], sh.shape[2]
+        n = H - 1
+        out = torch.empty((G * n, 2, L, self.n), dtype=sh.dtype, device=sh.device)
+        ws = self.workspace(lib().shm_fmt_switch_backward_workspace_bytes(self.ctx._h, G, n, L) // 8)
+        K = (ctypes.c_void_p * n)(*[_ptr(x).value for x in keys])
+        check(lib().shm_fmt_switch_backward(self.ctx._h, _ptr(sh), G, n, K, _ptr(out), L, _ptr(ws), ws.numel() * 8,
+                                            self._s()))
+        return out
+
     def permute_plain(self, pt, elt):
         """NTT-domain automorphism of plaintext rows without key switching (key generation only)."""
         return pt[..., self._perm(elt)].contiguous()

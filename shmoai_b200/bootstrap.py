@@ -215,7 +215,7 @@ class LinearTransform:
         acc = None
         for u, lst in sorted(self.groups.items()):
             inner = be.mul_plain_acc([rot[v].data for v, _ in lst], [p for _, p in lst])
-            inner = Ct(inner, x.scale * self.pt_scale)
+            inner = x.like(inner, x.scale * self.pt_scale)
             if u:
                 inner = ev.rotate(inner, self.g1 * u * self.b)
             acc = inner if acc is None else ev.add(acc, inner)
@@ -335,20 +335,35 @@ class Bootstrapper:
         return Ct(y.data, y.scale / self.c_fin)
 
     # ---------------- pipeline ----------------
-    def bootstrap(self, ct: Ct) -> Ct:
+    def _slots_to_re_im(self, x: Ct):
+        """SlotToCoeff, modraise, CoeffToSlot and the conjugation split: returns the
+        real and imaginary parts (t / K) of the raised slots, same kind as x."""
         ev, be = self.ev, self.ev.be
-        if ct.level != self.input_level:
+        if x.level != self.input_level:
             raise ValueError(f"bootstrap input must have {self.input_level} primes")
-        x = ct
         for lt in self.s2c:
             x = lt.apply(x)
-        raised = Ct(be.modraise(x.data, self.top), self.q0)
-        w = raised
+        w = x.like(be.modraise(x.data, self.top), self.q0)
         for lt in self.c2s:
             w = lt.apply(w)
         wc = ev.conjugate(w)
-        re = ev.add(w, wc)
-        im = ev.mul_i(ev.sub(w, wc), sign=-1)
+        return ev.add(w, wc), ev.mul_i(ev.sub(w, wc), sign=-1)
+
+    def _finish(self, re: Ct, im: Ct) -> Ct:
+        ev, be = self.ev, self.ev.be
         y = self.evalmod(Ct(be.cat([re.data, im.data]), re.scale))
-        nb = ct.batch
+        nb = re.batch
         return ev.add(Ct(y.data[:nb], y.scale), ev.mul_i(Ct(y.data[nb:], y.scale)))
+
+    def bootstrap(self, ct: Ct) -> Ct:
+        return self._finish(*self._slots_to_re_im(ct))
+
+    def bootstrap_shared(self, ct: Ct, n: int) -> Ct:
+        """Shared-a S2C-first bootstrapping of groups of n consecutive ciphertexts
+        (bootstrap_shared_a_s2c_first, BatchBootstrap.cuh:719-819): FmtSwitch forward at
+        the input level, SlotToCoeff / modraise / CoeffToSlot / conjugation on the
+        shared-a groups with Sh-Rots, FmtSwitch backward of the real and imaginary
+        parts, then EvalMod on ordinary ciphertexts."""
+        ev = self.ev
+        re, im = self._slots_to_re_im(ev.to_shared(ct, n))
+        return self._finish(ev.from_shared(re), ev.from_shared(im))

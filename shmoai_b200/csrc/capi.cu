@@ -41,6 +41,8 @@ Context::~Context() {
         if (l.modup_conv) cudaFree(l.modup_conv);
     }
     for (auto &kv : galois_perm) cudaFree(kv.second);
+    for (auto &kv : ext_consts)
+        for (void *p : kv.second) cudaFree(p);
 }
 
 const uint32_t *Context::perm(uint32_t elt) {
@@ -436,6 +438,61 @@ int shm_apply_galois_hoisted(const shm_context *ctx, const uint64_t *ct, uint32_
         set_device(c);
         uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::hoisted_ws_words(c, n_cts, L));
         shm::apply_galois_hoisted(c, ct, n_cts, L, n_elts, elts, keys, outs, ws, S(stream));
+    });
+}
+
+size_t shm_shared_rotate_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members, uint32_t L) {
+    return ctx && ctx->c ? shm::shared_rotate_ws_words(*ctx->c, n_groups, n_members, L) * 8 : 0;
+}
+
+int shm_shared_rotate_hoisted(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members,
+                              uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs,
+                              uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        if (!elts || !keys || !outs || n_members == 0) throw std::invalid_argument("bad shared-a rotation arguments");
+        for (uint32_t e = 0; e < n_elts; e++)
+            if (outs[e] == sh) throw std::invalid_argument("outputs must not alias the input");
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::shared_rotate_ws_words(c, n_groups, n_members, L));
+        shm::shared_rotate_hoisted(c, sh, n_groups, n_members, L, n_elts, elts, keys, outs, ws, S(stream));
+    });
+}
+
+size_t shm_fmt_switch_forward_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                              uint32_t L) {
+    return ctx && ctx->c ? shm::fmt_forward_ws_words(*ctx->c, n_groups, n_members, L) * 8 : 0;
+}
+
+int shm_fmt_switch_forward(const shm_context *ctx, const uint64_t *cts, uint32_t n_groups, uint32_t n_members,
+                           const uint64_t *key, uint64_t *out, uint32_t L, void *workspace, size_t workspace_bytes,
+                           void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        if (!key || n_members == 0) throw std::invalid_argument("bad format-switch arguments");
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::fmt_forward_ws_words(c, n_groups, n_members, L));
+        shm::fmt_forward(c, cts, n_groups, n_members, L, key, out, ws, S(stream));
+    });
+}
+
+size_t shm_fmt_switch_backward_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                               uint32_t L) {
+    return ctx && ctx->c ? shm::fmt_backward_ws_words(*ctx->c, n_groups, n_members, L) * 8 : 0;
+}
+
+int shm_fmt_switch_backward(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members,
+                            const uint64_t *const *keys, uint64_t *out, uint32_t L, void *workspace,
+                            size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        if (!keys || n_members == 0) throw std::invalid_argument("bad format-switch arguments");
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::fmt_backward_ws_words(c, n_groups, n_members, L));
+        shm::fmt_backward(c, sh, n_groups, n_members, L, keys, out, ws, S(stream));
     });
 }
 

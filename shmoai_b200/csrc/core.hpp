@@ -53,6 +53,7 @@ struct Context {
     uint64_t *rescale_inv = nullptr;    // [nq][nq][2]: q_{L-1}^-1 mod q_j (row L-1), Shoup
     std::vector<LevelKS> ks;            // index L (1..nq)
     std::map<uint32_t, uint32_t *> galois_perm;  // elt -> [N] permutation
+    std::map<uint32_t, std::vector<void *>> ext_consts;  // L -> exact Ql->P extension tables (shared.cu)
     std::mutex mu;
 
     // internal arena for calls that pass no workspace
@@ -129,6 +130,22 @@ void ctpt_matmul(const Context &c, const uint64_t *X, const int64_t *W, uint64_t
 void ctpt_matmul_cuda_core(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in,
                            uint32_t n_out, uint32_t L, cudaStream_t st);
 size_t ctpt_tc_ws_bytes(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);
+
+// ModUp of n_cts polynomials d (stride d_stride words) into up [n_cts][beta][LP][N]; x: [n_cts][L][N] scratch
+void modup_into(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_cts, uint32_t L, uint64_t *x,
+                uint64_t *up, cudaStream_t st);
+
+// shared-a batches [n_groups][n + 1][L][N] = (b_0 .. b_{n-1}, a) (shared.cu)
+size_t shared_rotate_ws_words(const Context &c, uint32_t n_groups, uint32_t n, uint32_t L);
+void shared_rotate_hoisted(const Context &c, const uint64_t *sh, uint32_t n_groups, uint32_t n, uint32_t L,
+                           uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs,
+                           uint64_t *ws, cudaStream_t st);
+size_t fmt_forward_ws_words(const Context &c, uint32_t n_groups, uint32_t n, uint32_t L);
+void fmt_forward(const Context &c, const uint64_t *cts, uint32_t n_groups, uint32_t n, uint32_t L,
+                 const uint64_t *key, uint64_t *out, uint64_t *ws, cudaStream_t st);
+size_t fmt_backward_ws_words(const Context &c, uint32_t n_groups, uint32_t n, uint32_t L);
+void fmt_backward(const Context &c, const uint64_t *sh, uint32_t n_groups, uint32_t n, uint32_t L,
+                  const uint64_t *const *keys, uint64_t *out, uint64_t *ws, cudaStream_t st);
 void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
                     uint32_t L, void *ws, uint64_t max_abs_w, cudaStream_t st);
 int ctpt_tc_error(void *ws, cudaStream_t st);

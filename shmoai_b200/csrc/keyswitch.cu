@@ -198,6 +198,33 @@ void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_
     SHM_CUDA(cudaGetLastError());
 }
 
+// ModUp of n_cts polynomials d (stride d_stride words) into up [n_cts][beta][LP][N]; x is
+// an [n_cts][L][N] scratch.  Shared by the shared-a operations (shared.cu).
+void modup_into(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_cts, uint32_t L, uint64_t *x,
+                uint64_t *up, cudaStream_t st) {
+    const uint32_t np = c.np, beta = (L + np - 1) / np, LP = L + np;
+    if (np > kMaxAlpha || beta > kMaxBeta || LP > 64) throw std::invalid_argument("key-switching shape too large");
+    const size_t n = c.n, ln = (size_t)L * n;
+    const LevelKS &ks = c.ks[L];
+    SHM_CUDA(cudaMemcpy2DAsync(x, ln * 8, d, d_stride * 8, ln * 8, n_cts, cudaMemcpyDeviceToDevice, st));
+    ntt_inverse(c, x, n_cts * L, L, q_map(L), ks.modup_scale, st);
+    SHM_LAUNCHED(1);
+    modup_conv_kernel<<<dim3(n / kThreads, beta, n_cts), kThreads, 0, st>>>(x, d, d_stride, up, ks.modup_conv, L, np,
+                                                                            c.nq, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+    LimbMap m;
+    for (uint32_t s = 0; s < 512; s++) {
+        if (s >= beta * LP) {
+            m.prime[s] = 255;
+            continue;
+        }
+        uint32_t b = s / LP, j = s % LP;
+        bool own = j >= b * np && j < std::min((b + 1) * np, L);
+        m.prime[s] = own ? 255 : (uint8_t)(j < L ? j : c.nq + (j - L));
+    }
+    ntt_forward(c, up, n_cts * beta * LP, beta * LP, m, st);
+}
+
 size_t hoisted_ws_words(const Context &c, uint32_t n_cts, uint32_t L) {
     // x, up (kept for every element), acc and a separate delta
     return keyswitch_ws_words(c, n_cts, L) + (size_t)n_cts * 2 * L * c.n;

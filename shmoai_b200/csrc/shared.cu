@@ -1,0 +1,288 @@
+// Shared-a (multi-secret RLWE) batches: Sh-Rot, FmtSwitch forward and backward.
+//
+// A group of n ciphertexts is held as n + 1 polynomials [b_0 .. b_{n-1}, a] with
+// b_i + a s'_i ~ m_i under auxiliary secrets s'_i (reference:
+// src/include/source/bootstrapping/SharedACiphertext.cuh:9-21).  All three
+// operations are "one ModUp-like extension of a shared polynomial, then H inner
+// products against key halves, H ModDowns and a combine":
+//
+//   Sh-Rot (ShRotate.cu:201-257): extension = ModUp(a); key [dnum][n+1][QP][N] with
+//     halves B_{g,0..n-1}, A_g; out b_i = sigma(b_i) + ModDown(<up, B_i>),
+//     out a = ModDown(<up, A>).  Several rotation steps of the same batch share
+//     one ModUp (hoisting; the automorphism is applied to the extended digits).
+//   FmtSwitch forward (FmtSwitch.cu:276-394): the "digits" are the n members' a_j,
+//     each extended exactly from Ql to QlP (floor-corrected CRT, FmtSwitch.cu:82-108);
+//     key [n][n+1][QP][N] with halves B_fmt[j][0..n-1], a_fmt[j];
+//     out b'_i = b_i + ModDown(<a_ext, B_fmt[:, i]>), a' = ModDown(<a_ext, a_fmt>).
+//   FmtSwitch backward (FmtSwitch.cu:396-429): n ordinary key switches of the
+//     shared a from s'_i to s, hoisted: one ModUp(a), per member one inner product
+//     with its key [dnum][2][QP][N], ModDown, combine with b_i.
+#include "core.hpp"
+#include "host_math.hpp"
+
+namespace shm {
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kMaxB = 16;
+
+// acc[ct][h][j][k] = sum_b up[ct][b][j][perm(k)] * key[b][h][prime(j)][k], h < H
+__global__ void ip_multi_kernel(const uint64_t *__restrict__ up, const uint64_t *__restrict__ key,
+                                uint64_t *__restrict__ acc, uint32_t n_cts, uint32_t L, uint32_t np, uint32_t nq,
+                                uint32_t beta, uint32_t H, uint32_t log_n, const PrimeConst *__restrict__ pc,
+                                const uint32_t *__restrict__ perm) {
+    const uint32_t j = blockIdx.y;
+    const uint32_t k = blockIdx.x * kT + threadIdx.x;
+    const uint32_t ks = perm ? __ldg(perm + k) : k;
+    const size_t n = (size_t)1 << log_n;
+    const uint32_t LP = L + np, QP = nq + np;
+    const uint32_t pj = j < L ? j : nq + (j - L);
+    const PrimeConst p = pc[pj];
+    for (uint32_t ct = 0; ct < n_cts; ct++) {
+        uint64_t u[kMaxB];
+        const uint64_t *up_c = up + (size_t)ct * beta * LP * n + (size_t)j * n + ks;
+#pragma unroll
+        for (int b = 0; b < kMaxB; b++)
+            if (b < (int)beta) u[b] = up_c[(size_t)b * LP * n];
+        for (uint32_t h = 0; h < H; h++) {
+            u128 a = {0, 0};
+            const uint64_t *kp = key + ((size_t)h * QP + pj) * n + k;
+#pragma unroll
+            for (int b = 0; b < kMaxB; b++)
+                if (b < (int)beta) mac(a, u[b], __ldg(kp + (size_t)b * H * QP * n));
+            acc[(((size_t)ct * H + h) * LP + j) * n + k] = barrett(a, p);
+        }
+    }
+}
+
+__global__ void moddown_multi_conv(const uint64_t *__restrict__ acc, uint64_t *__restrict__ delta,
+                                   const uint64_t *__restrict__ conv, uint32_t L, uint32_t np, uint32_t log_n,
+                                   const PrimeConst *__restrict__ pc) {
+    const uint32_t poly = blockIdx.y;
+    const uint32_t k = blockIdx.x * kT + threadIdx.x;
+    const size_t n = (size_t)1 << log_n;
+    const uint32_t LP = L + np;
+    const uint64_t *z = acc + (size_t)poly * LP * n + (size_t)L * n + k;
+    uint64_t zv[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+        if (i < (int)np) zv[i] = z[(size_t)i * n];
+    uint64_t *o = delta + (size_t)poly * L * n + k;
+    for (uint32_t j = 0; j < L; j++) {
+        const uint64_t *cj = conv + (size_t)j * np;
+        u128 a = {0, 0};
+#pragma unroll
+        for (int i = 0; i < 16; i++)
+            if (i < (int)np) mac(a, zv[i], __ldg(cj + i));
+        o[(size_t)j * n] = barrett(a, pc[j]);
+    }
+}
+
+struct Target {
+    const uint64_t *key;  // [beta][H][QP][N]
+    const uint32_t *perm;
+    uint64_t *out;
+    size_t out_ct, out_h;
+    const uint64_t *add;
+    size_t add_ct, add_h;
+    uint32_t n_add;
+};
+
+// out[ct][h][j] = add[ct][h][j @ perm] (h < n_add) + (acc - delta) * P^-1
+__global__ void combine_multi(const uint64_t *__restrict__ acc, const uint64_t *__restrict__ delta, Target t,
+                              uint32_t H, uint32_t L, uint32_t np, uint32_t log_n, const PrimeConst *__restrict__ pc,
+                              const uint64_t *__restrict__ pinv) {
+    const uint32_t j = blockIdx.y, hc = blockIdx.z, ct = hc / H, h = hc % H;
+    const uint32_t k = blockIdx.x * kT + threadIdx.x;
+    const size_t n = (size_t)1 << log_n;
+    const uint64_t q = pc[j].q;
+    const uint64_t a = acc[((size_t)hc * (L + np) + j) * n + k];
+    const uint64_t dl = delta[((size_t)hc * L + j) * n + k];
+    uint64_t r = shoup(sub_mod(a, dl, q), pinv[2 * j], pinv[2 * j + 1], q);
+    if (h < t.n_add) {
+        const uint32_t ka = t.perm ? __ldg(t.perm + k) : k;
+        r = add_mod(r, t.add[ct * t.add_ct + h * t.add_h + (size_t)j * n + ka], q);
+    }
+    t.out[ct * t.out_ct + h * t.out_h + (size_t)j * n + k] = r;
+}
+
+// exact Ql -> P extension (floor-corrected CRT): x = sum_i y_i qhat_i - v Q, v = floor(sum_i y_i / q_i),
+// y_i = [x_i qhat_i^-1]_{q_i} already in the coefficient buffer; writes the P rows of ext
+__global__ void exact_ext_kernel(const uint64_t *__restrict__ y, uint64_t *__restrict__ ext, const uint64_t *__restrict__ tab,
+                                 const double *__restrict__ qinv, uint32_t L, uint32_t np, uint32_t nq, uint32_t log_n,
+                                 const PrimeConst *__restrict__ pc) {
+    const uint32_t poly = blockIdx.y;
+    const uint32_t k = blockIdx.x * kT + threadIdx.x;
+    const size_t n = (size_t)1 << log_n;
+    const uint64_t *yp = y + (size_t)poly * L * n + k;
+    uint64_t yv[64];
+    double frac = 0.0;
+    for (uint32_t i = 0; i < L; i++) {
+        yv[i] = yp[(size_t)i * n];
+        frac = __dadd_rn(frac, __dmul_rn((double)yv[i], qinv[i]));  // no contraction: reproducible
+    }
+    const uint64_t v = (uint64_t)frac;
+    uint64_t *o = ext + (size_t)poly * (L + np) * n + (size_t)L * n + k;
+    for (uint32_t kk = 0; kk < np; kk++) {
+        const uint64_t *row = tab + (size_t)kk * (L + 1);  // qhat_i mod p_k (L values), Q mod p_k
+        const PrimeConst p = pc[nq + kk];
+        u128 a = {0, 0};
+        for (uint32_t i = 0; i < L; i++) mac(a, yv[i], __ldg(row + i));
+        o[(size_t)kk * n] = sub_mod(barrett(a, p), barrett(mul_wide(v, __ldg(row + L)), p), p.q);
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+
+namespace {
+
+struct ExtConsts {
+    uint64_t *scale = nullptr;  // [L][4] inverse-NTT last-stage constants with qhat_i^-1 folded
+    uint64_t *tab = nullptr;    // [np][L+1]
+    double *qinv = nullptr;     // [L]
+};
+
+ExtConsts ext_consts(Context &c, uint32_t L) {
+    std::lock_guard<std::mutex> g(c.mu);
+    auto it = c.ext_consts.find(L);
+    if (it != c.ext_consts.end())
+        return ExtConsts{(uint64_t *)it->second[0], (uint64_t *)it->second[1], (double *)it->second[2]};
+    ExtConsts e;
+    std::vector<uint64_t> Q(c.primes.begin(), c.primes.begin() + L), sc, tab;
+    std::vector<double> qi(L);
+    for (uint32_t i = 0; i < L; i++) {
+        uint64_t q = Q[i], h = host::partial_product(Q, i, q);
+        uint64_t cc = host::mulmod(host::invmod(h, q), c.h_pc[i].n_inv, q);
+        uint64_t psi_half_inv = 0;
+        // psi^-(N/2) sits at index 1 of the inverse twiddle table
+        SHM_CUDA(cudaMemcpy(&psi_half_inv, c.tw + (size_t)i * 4 * c.n + 2 * c.n + 1, 8, cudaMemcpyDeviceToHost));
+        uint64_t c1 = host::mulmod(cc, psi_half_inv, q);
+        sc.insert(sc.end(), {cc, host::shoup_of(cc, q), c1, host::shoup_of(c1, q)});
+        qi[i] = 1.0 / (double)q;
+    }
+    for (uint32_t k = 0; k < c.np; k++) {
+        uint64_t p = c.primes[c.nq + k], Qm = 1;
+        for (uint32_t i = 0; i < L; i++) {
+            tab.push_back(host::partial_product(Q, i, p));
+            Qm = host::mulmod(Qm, Q[i] % p, p);
+        }
+        tab.push_back(Qm);
+    }
+    SHM_CUDA(cudaMalloc(&e.scale, sc.size() * 8));
+    SHM_CUDA(cudaMemcpy(e.scale, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice));
+    SHM_CUDA(cudaMalloc(&e.tab, tab.size() * 8));
+    SHM_CUDA(cudaMemcpy(e.tab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice));
+    SHM_CUDA(cudaMalloc(&e.qinv, qi.size() * 8));
+    SHM_CUDA(cudaMemcpy(e.qinv, qi.data(), qi.size() * 8, cudaMemcpyHostToDevice));
+    c.ext_consts[L] = {e.scale, e.tab, e.qinv};
+    return e;
+}
+
+void check_shape(const Context &c, uint32_t L, uint32_t beta, uint32_t H) {
+    if (c.np == 0) throw std::invalid_argument("context has no special primes");
+    if (L < 1 || L > c.nq) throw std::invalid_argument("level out of range");
+    if (beta > (uint32_t)kMaxB || L + c.np > 64 || c.np > 16 || H < 2 || H > 64)
+        throw std::invalid_argument("shared-a shape too large");
+}
+
+// inner products, ModDown and combine for one target; acc/delta are workspace
+void apply_target(const Context &c, const uint64_t *up, uint32_t n_cts, uint32_t L, uint32_t beta, uint32_t H,
+                  const Target &t, uint64_t *acc, uint64_t *delta, cudaStream_t st) {
+    const size_t n = c.n;
+    const uint32_t np = c.np, LP = L + np;
+    SHM_LAUNCHED(1);
+    ip_multi_kernel<<<dim3(n / kT, LP), kT, 0, st>>>(up, t.key, acc, n_cts, L, np, c.nq, beta, H, c.log_n, c.pc,
+                                                     t.perm);
+    SHM_CUDA(cudaGetLastError());
+    LimbMap mp;
+    for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
+    ntt_inverse(c, acc, n_cts * H * LP, LP, mp, c.moddown_scale, st, L);
+    SHM_LAUNCHED(1);
+    moddown_multi_conv<<<dim3(n / kT, n_cts * H), kT, 0, st>>>(acc, delta, c.moddown_conv, L, np, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+    ntt_forward(c, delta, n_cts * H * L, L, q_map(L), st);
+    SHM_LAUNCHED(1);
+    combine_multi<<<dim3(n / kT, L, n_cts * H), kT, 0, st>>>(acc, delta, t, H, L, np, c.log_n, c.pc, c.p_inv);
+    SHM_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+size_t shared_rotate_ws_words(const Context &c, uint32_t n_groups, uint32_t n, uint32_t L) {
+    const uint32_t beta = (L + c.np - 1) / c.np, LP = L + c.np, H = n + 1;
+    return (size_t)n_groups * c.n * (L + (size_t)beta * LP + (size_t)H * LP + (size_t)H * L);
+}
+
+void shared_rotate_hoisted(const Context &c, const uint64_t *sh, uint32_t n_groups, uint32_t n, uint32_t L,
+                           uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs,
+                           uint64_t *ws, cudaStream_t st) {
+    const uint32_t beta = (L + c.np - 1) / c.np, LP = L + c.np, H = n + 1;
+    check_shape(c, L, beta, H);
+    if (beta > c.dnum) throw std::invalid_argument("level needs more key digits than the key holds");
+    const size_t ln = (size_t)L * c.n;
+    uint64_t *x = ws, *up = x + (size_t)n_groups * ln, *acc = up + (size_t)n_groups * beta * LP * c.n;
+    uint64_t *delta = acc + (size_t)n_groups * H * LP * c.n;
+    modup_into(c, sh + (size_t)n * ln, (size_t)H * ln, n_groups, L, x, up, st);
+    for (uint32_t e = 0; e < n_elts; e++) {
+        Target t{keys[e], const_cast<Context &>(c).perm(elts[e]), outs[e], (size_t)H * ln, ln, sh, (size_t)H * ln,
+                 ln, n};
+        apply_target(c, up, n_groups, L, beta, H, t, acc, delta, st);
+    }
+}
+
+size_t fmt_forward_ws_words(const Context &c, uint32_t n_groups, uint32_t n, uint32_t L) {
+    const uint32_t LP = L + c.np, H = n + 1;
+    return (size_t)n_groups * c.n * ((size_t)n * L + (size_t)n * LP + (size_t)H * LP + (size_t)H * L);
+}
+
+void fmt_forward(const Context &c, const uint64_t *cts, uint32_t n_groups, uint32_t n, uint32_t L,
+                 const uint64_t *key, uint64_t *out, uint64_t *ws, cudaStream_t st) {
+    const uint32_t LP = L + c.np, H = n + 1;
+    check_shape(c, L, n, H);
+    const size_t ln = (size_t)L * c.n, N = c.n;
+    const uint32_t m = n_groups * n;  // member ciphertexts
+    uint64_t *y = ws, *ext = y + (size_t)m * ln, *acc = ext + (size_t)m * LP * N;
+    uint64_t *delta = acc + (size_t)n_groups * H * LP * N;
+    ExtConsts e = ext_consts(const_cast<Context &>(c), L);
+    // y = INTT(a_j) * qhat^-1 ; the Ql rows of ext keep a_j in NTT form
+    SHM_CUDA(cudaMemcpy2DAsync(y, ln * 8, cts + ln, 2 * ln * 8, ln * 8, m, cudaMemcpyDeviceToDevice, st));
+    ntt_inverse(c, y, m * L, L, q_map(L), e.scale, st);
+    SHM_CUDA(cudaMemcpy2DAsync(ext, LP * N * 8, cts + ln, 2 * ln * 8, ln * 8, m, cudaMemcpyDeviceToDevice, st));
+    SHM_LAUNCHED(1);
+    exact_ext_kernel<<<dim3(N / kT, m), kT, 0, st>>>(y, ext, e.tab, e.qinv, L, c.np, c.nq, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+    LimbMap mp;
+    for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
+    ntt_forward(c, ext, m * LP, LP, mp, st);
+    // digits = the n members of a group: ext is [G][n][LP][N]
+    Target t{key, nullptr, out, (size_t)H * ln, ln, cts, (size_t)n * 2 * ln, 2 * ln, n};
+    apply_target(c, ext, n_groups, L, n, H, t, acc, delta, st);
+}
+
+size_t fmt_backward_ws_words(const Context &c, uint32_t n_groups, uint32_t n, uint32_t L) {
+    const uint32_t beta = (L + c.np - 1) / c.np, LP = L + c.np;
+    (void)n;
+    return (size_t)n_groups * c.n * (L + (size_t)beta * LP + 2 * (size_t)LP + 2 * (size_t)L);
+}
+
+void fmt_backward(const Context &c, const uint64_t *sh, uint32_t n_groups, uint32_t n, uint32_t L,
+                  const uint64_t *const *keys, uint64_t *out, uint64_t *ws, cudaStream_t st) {
+    const uint32_t beta = (L + c.np - 1) / c.np, LP = L + c.np, H = n + 1;
+    check_shape(c, L, beta, 2);
+    if (beta > c.dnum) throw std::invalid_argument("level needs more key digits than the key holds");
+    const size_t ln = (size_t)L * c.n;
+    uint64_t *x = ws, *up = x + (size_t)n_groups * ln, *acc = up + (size_t)n_groups * beta * LP * c.n;
+    uint64_t *delta = acc + (size_t)n_groups * 2 * LP * c.n;
+    modup_into(c, sh + (size_t)n * ln, (size_t)H * ln, n_groups, L, x, up, st);
+    for (uint32_t i = 0; i < n; i++) {
+        // member i of group g -> ordinary ciphertext g * n + i = (b_i + cx0, cx1)
+        Target t{keys[i], nullptr, out + (size_t)i * 2 * ln, (size_t)n * 2 * ln, ln, sh + (size_t)i * ln,
+                 (size_t)H * ln, 0, 1};
+        apply_target(c, up, n_groups, L, beta, 2, t, acc, delta, st);
+    }
+}
+
+}  // namespace shm

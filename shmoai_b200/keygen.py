@@ -96,6 +96,84 @@ class KeyGenerator:
     def galois_key(self, elt: int):
         return self.switching_key(self.be.permute_plain(self.s, elt))
 
+    # ---------------- shared-a keys ----------------
+    def aux_secrets(self, n: int, hamming_weight: int = 192):
+        """n auxiliary secrets s'_i of a shared-a group (SharedAKeyGen, FmtSwitch.cuh:235-305),
+        ternary with exactly `hamming_weight` non-zero coefficients, NTT form over QP."""
+        out = []
+        for _ in range(n):
+            s = np.zeros(self.n, dtype=np.int64)
+            pos = self.rng.choice(self.n, size=hamming_weight, replace=False)
+            s[pos] = self.rng.choice(np.array([-1, 1], dtype=np.int64), size=hamming_weight)
+            out.append(self._ntt_qp(s))
+        self.aux = out
+        return out
+
+    def _p_units(self, digit: int | None):
+        """Residues of P * E_digit over QP (E the CRT unit of the digit's primes), or of P
+        on every Q prime when digit is None."""
+        be, nq = self.be, self.be.nq
+        P = 1
+        for p in be.primes[nq:]:
+            P *= p
+        unit = np.zeros(self.QP, dtype=np.uint64)
+        rows = range(nq) if digit is None else range(digit * be.np, min((digit + 1) * be.np, nq))
+        for i in rows:
+            unit[i] = P % be.primes[i]
+        return unit
+
+    def _multi_key(self, olds, adds):
+        """[D][n + 1][QP][N]: digit d = (B_{d,0} .. B_{d,n-1}, A_d) with
+        B_{d,i} = e_{d,i} - A_d * olds[i] (+ unit * s_new for each (i, unit, s_new) in adds[d])."""
+        be = self.be
+        digits = []
+        for add in adds:
+            A = self._uniform((1, self.QP, self.n))
+            rows = []
+            for so in olds:
+                e = self._error_ntt((1,), self.QP)
+                rows.append(be.sub(e, be.mul_plain(A, so)))
+            for i, unit, sn in add:
+                rows[i] = be.add(rows[i], be.mul_scalar(self._as_poly(sn), unit))
+            rows.append(A)
+            digits.append(be.cat(rows))
+        return be.stack(digits)
+
+    def shared_galois_key(self, elt: int):
+        """Sh-Galois key of element g (gen_shared_galois_key, ShRotate.cu:54-162):
+        [dnum][n + 1][QP][N], B_{d,i} = -A_d s'_i + e + P E_d sigma_g(s'_i), one A_d per digit."""
+        news = [self.be.permute_plain(s, elt) for s in self.aux]
+        adds = [[(i, self._p_units(d), news[i]) for i in range(len(self.aux))] for d in range(self.be.dnum)]
+        return self._multi_key(self.aux, adds)
+
+    def format_key(self):
+        """FmtSwitch forward key (gen_format_key, FmtSwitch.cu:165-270): [n][n + 1][QP][N],
+        digit j = member j's a; B_fmt[j][i] = -a_fmt[j] s'_i + e + [i == j] P s."""
+        n = len(self.aux)
+        unit = self._p_units(None)
+        return self._multi_key(self.aux, [[(j, unit, self.s)] for j in range(n)])
+
+    def backward_keys(self):
+        """FmtSwitch backward keys: the switching key s'_i -> s of every member."""
+        return [self.switching_key(s) for s in self.aux]
+
+    def decrypt_shared_coeffs(self, sh) -> np.ndarray:
+        """Centred coefficients [G * n][N] of shared-a groups [G][n + 1][L][N] (b_i + a s'_i)."""
+        be = self.be
+        d = be.drop(sh, 1) if sh.shape[-2] > 1 else sh
+        n = d.shape[1] - 1
+        out = []
+        for g in range(d.shape[0]):
+            grp = d[g]
+            for i in range(n):
+                m = be.add(grp[i:i + 1], be.mul_plain(grp[n:n + 1], self.aux[i][:1]))
+                m = be.ntt_inv(be.clone(m))
+                out.append(self.enc.centered(be.to_host(m)[:, 0, :], be.primes[0])[0])
+        return np.stack(out)
+
+    def decrypt_shared(self, sh, scale: float) -> np.ndarray:
+        return np.stack([self.enc.decode(c, scale) for c in self.decrypt_shared_coeffs(sh)])
+
     # ---------------- encryption ----------------
     def encrypt(self, z_batch, scale: float, L: int) -> Ct:
         """Encrypt each row of z_batch (complex slot vectors) at level L and `scale`."""

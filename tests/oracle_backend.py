@@ -89,6 +89,16 @@ class OracleBackend:
         per_ct = [self.o.apply_galois_hoisted(np.ascontiguousarray(c), elts, keys) for c in ct]
         return [np.stack([per_ct[i][e] for i in range(len(ct))]) for e in range(len(elts))]
 
+    def sh_rotate_many(self, sh, elts, keys):
+        per_g = [self.o.shared_rotate_hoisted(np.ascontiguousarray(g), elts, keys) for g in sh]
+        return [np.stack([per_g[g][e] for g in range(len(sh))]) for e in range(len(elts))]
+
+    def fmt_forward(self, cts, n, key):
+        return np.stack([self.o.fmt_forward(cts[g * n:(g + 1) * n], key) for g in range(cts.shape[0] // n)])
+
+    def fmt_backward(self, sh, keys):
+        return np.concatenate([self.o.fmt_backward(np.ascontiguousarray(g), keys) for g in sh])
+
     def permute_plain(self, pt, elt):
         return np.ascontiguousarray(pt[..., O.galois_perm(self.log_n, elt)])
 
