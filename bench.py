@@ -180,7 +180,9 @@ def ntt_roofline(torch, ctx, L, limbs_target=4096):
 # bootstrapping workload
 
 
-def setup_boot(torch, dev, rank):
+def setup_boot(torch, dev, rank, shared=0):
+    """Context, keys and bootstrapper at the reference parameters; with shared = n the
+    Sh-Galois, format and backward keys of shared-a groups of n replace the Galois keys."""
     from shmoai_b200.backend import GpuBackend
     from shmoai_b200.bootstrap import Bootstrapper
     from shmoai_b200.ckks import CKKSContext
@@ -192,8 +194,15 @@ def setup_boot(torch, dev, rank):
     kg = KeyGenerator(be, hamming_weight=BOOT["h"], seed=0x5EED + rank)
     ev = Evaluator(be, relin_key=kg.relin_key())
     bs = Bootstrapper(ev, scale=BOOT["scale"], input_level=BOOT["input_level"])
-    for elt in bs.galois_elts():
-        ev.galois_keys[elt] = kg.galois_key(elt)
+    if shared:
+        kg.aux_secrets(shared, hamming_weight=BOOT["h"])
+        ev.shared.fmt = kg.format_key()
+        ev.shared.backward = kg.backward_keys()
+        for elt in bs.galois_elts():
+            ev.shared.galois[elt] = kg.shared_galois_key(elt)
+    else:
+        for elt in bs.galois_elts():
+            ev.galois_keys[elt] = kg.galois_key(elt)
     return ctx, be, kg, ev, bs
 
 
@@ -206,16 +215,22 @@ def run_boot(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     lib = shmoai_b200.lib()
-    ctx, be, kg, ev, bs = setup_boot(torch, dev, rank)
+    S = args.shared
     B = args.batch
+    if S and B % S:
+        raise SystemExit("--batch must be a multiple of --shared")
+    ctx, be, kg, ev, bs = setup_boot(torch, dev, rank, S)
     rng = np.random.default_rng(1000 + rank)
     n = be.n // 2
     z = rng.uniform(-1, 1, (B, n)) + 1j * rng.uniform(-1, 1, (B, n))
     ct = kg.encrypt(z, BOOT["scale"], BOOT["input_level"])
     holder = {}
 
+    def boot(x):
+        return bs.bootstrap_shared(x, S) if S else bs.bootstrap(x)
+
     def step():
-        holder["out"] = bs.bootstrap(ct)
+        holder["out"] = boot(ct)
 
     clk = ClockSampler(dev).start()
     for _ in range(args.warmup):
@@ -234,7 +249,7 @@ def run_boot(args, rank, world, dist):
 
     def e2e_step():
         d_in.copy_(h_in, non_blocking=True)
-        o = bs.bootstrap(Ct(d_in, ct.scale))
+        o = boot(Ct(d_in, ct.scale))
         h_out.copy_(o.data, non_blocking=True)
 
     if args.no_extras:
@@ -250,8 +265,9 @@ def run_boot(args, rank, world, dist):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic (seeded uniform slot values in [-1,1]^2, symmetric encryption, random keys)",
-        "config": {"workload": "boot: S2C-first bootstrap of a batch of ciphertexts per GPU per step",
-                   "batch_per_gpu": B, "N": be.n, "slots": n, "input_primes": BOOT["input_level"],
+        "config": {"workload": ("boot: shared-a S2C-first bootstrap of a batch of ciphertexts per GPU per step"
+                                if S else "boot: S2C-first bootstrap of a batch of ciphertexts per GPU per step"),
+                   "batch_per_gpu": B, "shared_a_group": S or None, "N": be.n, "slots": n, "input_primes": BOOT["input_level"],
                    "output_primes": out_level, "Q": "[51]+20x[46]+14x[51]", "P": "5x[51]", "dnum": be.dnum,
                    "h": BOOT["h"], "evalmod": "Chebyshev deg 47, K=25, 3 double angles",
                    "err_mean": float(err.mean()), "err_max": float(err.max()),
@@ -498,6 +514,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks"])
     ap.add_argument("--batch", type=int, default=None)
+    ap.add_argument("--shared", type=int, default=0,
+                    help="boot: shared-a group size n (0 = ordinary ciphertexts)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the step only (no e2e, roofline or CPU legs): used for ncu launch lists")

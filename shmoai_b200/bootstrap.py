@@ -206,7 +206,10 @@ class LinearTransform:
         s |= {self.g1 * u * self.b for u in self.groups if u}
         return s
 
-    def apply(self, x: Ct) -> Ct:
+    def apply(self, x: Ct, rescale: bool = True) -> Ct:
+        """With rescale=False the accumulator is returned at scale x.scale * q, one prime
+        above the rescaled result, so that key switches applied to it next add noise
+        divided by q (as the giant steps here do)."""
         ev, be = self.ev, self.ev.be
         if x.level != self.level:
             x = ev.drop(x, self.level)
@@ -219,7 +222,7 @@ class LinearTransform:
             if u:
                 inner = ev.rotate(inner, self.g1 * u * self.b)
             acc = inner if acc is None else ev.add(acc, inner)
-        return ev.rescale(acc)
+        return ev.rescale(acc) if rescale else acc
 
 
 class Bootstrapper:
@@ -337,21 +340,29 @@ class Bootstrapper:
     # ---------------- pipeline ----------------
     def _slots_to_re_im(self, x: Ct):
         """SlotToCoeff, modraise, CoeffToSlot and the conjugation split: returns the
-        real and imaginary parts (t / K) of the raised slots, same kind as x."""
+        real and imaginary parts (t / K) of the raised slots, same kind as x, NOT yet
+        rescaled.  The last CoeffToSlot layer stops before its rescale, so the
+        conjugation (and, for shared-a groups, the backward format switch) runs at
+        scale q0 * q: the low-frequency part of a key switch's noise (its uncorrected
+        ModUp digits are not centred) lands at the slots next to slot 0, and EvalMod
+        multiplies input errors by about 2 pi K c_fin, so at scale q0 alone one
+        key switch there costs ~1e-4 of output precision in those slots."""
         ev, be = self.ev, self.ev.be
         if x.level != self.input_level:
             raise ValueError(f"bootstrap input must have {self.input_level} primes")
         for lt in self.s2c:
             x = lt.apply(x)
         w = x.like(be.modraise(x.data, self.top), self.q0)
-        for lt in self.c2s:
+        for lt in self.c2s[:-1]:
             w = lt.apply(w)
+        w = self.c2s[-1].apply(w, rescale=False)
         wc = ev.conjugate(w)
         return ev.add(w, wc), ev.mul_i(ev.sub(w, wc), sign=-1)
 
     def _finish(self, re: Ct, im: Ct) -> Ct:
+        """Rescale the parts, EvalMod on both at once, recombine re + i im."""
         ev, be = self.ev, self.ev.be
-        y = self.evalmod(Ct(be.cat([re.data, im.data]), re.scale))
+        y = self.evalmod(ev.rescale(Ct(be.cat([re.data, im.data]), re.scale)))
         nb = re.batch
         return ev.add(Ct(y.data[:nb], y.scale), ev.mul_i(Ct(y.data[nb:], y.scale)))
 
