@@ -130,12 +130,14 @@ def timed_steps(torch, step, steps, dist, flush):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")  # lets `ncu --nvtx --nvtx-include timed/` list the timed launches only
     for i in range(steps):
         if flush is not None:
             flush.zero_()
         starts[i].record()
         step()
         ends[i].record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     if dist:
@@ -180,37 +182,28 @@ def ntt_roofline(torch, ctx, L, limbs_target=4096):
 # bootstrapping workload
 
 
-def setup_boot(torch, dev, rank, shared=0):
-    """Context, keys and bootstrapper at the reference parameters; with shared = n the
-    Sh-Galois, format and backward keys of shared-a groups of n replace the Galois keys."""
-    from shmoai_b200.backend import GpuBackend
-    from shmoai_b200.bootstrap import Bootstrapper
-    from shmoai_b200.ckks import CKKSContext
-    from shmoai_b200.evaluator import Evaluator
-    from shmoai_b200.keygen import KeyGenerator
+def setup_boot(dev, rank, shared=0):
+    """C++ host (context, secret key, relinearisation key) and bootstrapper at the
+    reference parameters; with shared = n the Sh-Galois, format and backward keys of
+    shared-a groups of n replace the Galois keys."""
+    from shmoai_b200.host import Bootstrapper, Host
 
-    ctx = CKKSContext(BOOT["log_n"], bits=BOOT["bits"], n_special=BOOT["n_special"], device=dev)
-    be = GpuBackend(ctx)
-    kg = KeyGenerator(be, hamming_weight=BOOT["h"], seed=0x5EED + rank)
-    ev = Evaluator(be, relin_key=kg.relin_key())
-    bs = Bootstrapper(ev, scale=BOOT["scale"], input_level=BOOT["input_level"])
+    h = Host(BOOT["log_n"], bits=BOOT["bits"], n_special=BOOT["n_special"], hamming_weight=BOOT["h"],
+             seed=0x5EED + rank, device=dev)
+    h.gen_relin_key()
+    bs = Bootstrapper(h, BOOT["scale"], BOOT["input_level"])
     if shared:
-        kg.aux_secrets(shared, hamming_weight=BOOT["h"])
-        ev.shared.fmt = kg.format_key()
-        ev.shared.backward = kg.backward_keys()
-        for elt in bs.galois_elts():
-            ev.shared.galois[elt] = kg.shared_galois_key(elt)
+        h.gen_shared_keys(shared, bs.galois_elts(), hamming_weight=BOOT["h"])
     else:
-        for elt in bs.galois_elts():
-            ev.galois_keys[elt] = kg.galois_key(elt)
-    return ctx, be, kg, ev, bs
+        h.gen_galois_keys(bs.galois_elts())
+    return h, bs
 
 
 def run_boot(args, rank, world, dist):
     import torch
 
     import shmoai_b200
-    from shmoai_b200.evaluator import Ct
+    from shmoai_b200.ckks import CKKSContext
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
@@ -219,18 +212,15 @@ def run_boot(args, rank, world, dist):
     B = args.batch
     if S and B % S:
         raise SystemExit("--batch must be a multiple of --shared")
-    ctx, be, kg, ev, bs = setup_boot(torch, dev, rank, S)
+    h, bs = setup_boot(dev, rank, S)
     rng = np.random.default_rng(1000 + rank)
-    n = be.n // 2
+    n = h.n // 2
     z = rng.uniform(-1, 1, (B, n)) + 1j * rng.uniform(-1, 1, (B, n))
-    ct = kg.encrypt(z, BOOT["scale"], BOOT["input_level"])
+    ct = h.encrypt(z, BOOT["scale"], BOOT["input_level"])
     holder = {}
 
-    def boot(x):
-        return bs.bootstrap_shared(x, S) if S else bs.bootstrap(x)
-
     def step():
-        holder["out"] = boot(ct)
+        holder["out"] = bs.run(ct, S)
 
     clk = ClockSampler(dev).start()
     for _ in range(args.warmup):
@@ -239,18 +229,18 @@ def run_boot(args, rank, world, dist):
     l0 = lib.shm_kernel_launches()
     ms = timed_steps(torch, step, args.steps, dist, None)  # a batch is ~1 GB of live data per step > L2
     launches = lib.shm_kernel_launches() - l0
-    err = np.abs(kg.decrypt(holder["out"]) - z)
-    out_level = holder["out"].level
+    out = holder["out"]
+    err = np.abs(h.decrypt(out) - z)
+    out_level = out.level
 
-    # end to end: pinned host input -> device -> bootstrap -> host output, every step
-    h_in = ct.data.cpu().pin_memory()
-    h_out = torch.empty(tuple(holder["out"].data.shape), dtype=torch.int64).pin_memory()
-    d_in = torch.empty_like(ct.data)
+    # end to end through the host C ABI: pinned host input -> device (shm_ct_from_host),
+    # bootstrap (shm_boot_run), device -> pinned host output (shm_ct_to_host), every step
+    h_in = torch.from_numpy(ct.to_host().view(np.int64)).pin_memory()
+    h_out = torch.empty((out.count, out.size, out.level, h.n), dtype=torch.int64).pin_memory()
 
     def e2e_step():
-        d_in.copy_(h_in, non_blocking=True)
-        o = boot(Ct(d_in, ct.scale))
-        h_out.copy_(o.data, non_blocking=True)
+        d_in = h.ct_from_ptr(h_in.data_ptr(), ct.count, ct.size, ct.level, ct.scale)
+        bs.run(d_in, S).to_ptr(h_out.data_ptr())
 
     if args.no_extras:
         e2e_ms, roof = ms, None
@@ -258,7 +248,9 @@ def run_boot(args, rank, world, dist):
         e2e_step()
         torch.cuda.synchronize()
         e2e_ms = timed_steps(torch, e2e_step, max(1, args.steps // 2), dist, None)
-        roof = ntt_roofline(torch, ctx, BOOT["bits"].__len__() - BOOT["n_special"])
+        ctx = CKKSContext(BOOT["log_n"], primes=h.primes, n_special=BOOT["n_special"], device=dev)
+        roof = ntt_roofline(torch, ctx, len(BOOT["bits"]) - BOOT["n_special"])
+        ctx.close()
     clocks = clk.summary()
     return {
         "metric": BOOT_METRIC, "value": round(world * B * 1000.0 / ms, 3), "unit": "bootstraps/s",
@@ -267,8 +259,9 @@ def run_boot(args, rank, world, dist):
         "data": "synthetic (seeded uniform slot values in [-1,1]^2, symmetric encryption, random keys)",
         "config": {"workload": ("boot: shared-a S2C-first bootstrap of a batch of ciphertexts per GPU per step"
                                 if S else "boot: S2C-first bootstrap of a batch of ciphertexts per GPU per step"),
-                   "batch_per_gpu": B, "shared_a_group": S or None, "N": be.n, "slots": n, "input_primes": BOOT["input_level"],
-                   "output_primes": out_level, "Q": "[51]+20x[46]+14x[51]", "P": "5x[51]", "dnum": be.dnum,
+                   "batch_per_gpu": B, "shared_a_group": S or None, "N": h.n, "slots": n,
+                   "input_primes": BOOT["input_level"], "output_primes": out_level, "Q": "[51]+20x[46]+14x[51]",
+                   "P": "5x[51]", "dnum": h.nq // h.np, "path": "C++ host library (shm_boot_run) over the C ABI",
                    "h": BOOT["h"], "evalmod": "Chebyshev deg 47, K=25, 3 double angles",
                    "err_mean": float(err.mean()), "err_max": float(err.max()),
                    "l2": "not flushed: the step's live data (~1 GB per batch of 32) exceeds the 126 MB L2",
@@ -288,28 +281,50 @@ def run_boot(args, rank, world, dist):
 BOOT_OPS = {"rot_high": 40, "rot_low": 39, "relin": 34}
 
 
-def cpu_boot_estimate():
-    """CPU oracle on all host cores (N = 2^16): one HRotate at 34 primes, one at 3 primes and
-    one relinearisation at 27 primes, scaled by BOOT_OPS -> bootstraps/s."""
+def cpu_boot_estimate(shared: int = 0):
+    """CPU oracle on all host cores (N = 2^16) -> bootstraps/s.  Ordinary: one HRotate at 34
+    primes, one at 3 primes and one relinearisation at 27 primes, scaled by BOOT_OPS.
+    Shared-a groups of n: one Sh-Rot of a group at 34 and at 3 primes and one FmtSwitch
+    backward of a group at 33 primes, per ciphertext (/ n), plus the EvalMod
+    relinearisations (ordinary ciphertexts)."""
     from oracle import oracle as O
 
     o = O.Oracle.from_bits(BOOT["log_n"], BOOT["bits"], BOOT["n_special"])
     n, QP = o.n, o.nq + o.np
     key = np.stack([O.fill(900 + d, (2, QP, n), list(o.primes) * 2) for d in range(o.dnum)])
     t = {}
-    for name, L, poly in (("rot_high", 34, 2), ("rot_low", 3, 2), ("relin", 27, 3)):
-        x = O.fill(901, (poly, L, n), list(o.primes[:L]) * poly)
-        t0 = time.perf_counter()
-        if name == "relin":
-            o.relinearize(x, key)
-        else:
+    if shared:
+        H = shared + 1
+        shkey = np.stack([O.fill(910 + d, (H, QP, n), list(o.primes) * H) for d in range(o.dnum)])
+        cases = (("rot_high", 34), ("rot_low", 3), ("bwd", 33))
+        for name, L in cases:
+            g = O.fill(911, (H, L, n), list(o.primes[:L]) * H)
+            t0 = time.perf_counter()
+            if name == "bwd":
+                o.fmt_backward(g, [key] * shared)
+            else:
+                o.shared_rotate_hoisted(g, [5], [shkey])
+            t[name] = (time.perf_counter() - t0) / shared
+    else:
+        for name, L in (("rot_high", 34), ("rot_low", 3)):
+            x = O.fill(901, (2, L, n), list(o.primes[:L]) * 2)
+            t0 = time.perf_counter()
             o.apply_galois_ct(x, 5, key)
-        t[name] = time.perf_counter() - t0
-    per_boot = sum(BOOT_OPS[k] * t[k] for k in BOOT_OPS)
-    sample = (f"one HRotate at 34 primes ({t['rot_high']:.2f} s), one at 3 primes ({t['rot_low']:.2f} s) and "
-              f"one relinearisation at 27 primes ({t['relin']:.2f} s) on the CPU oracle (OpenMP over limbs), "
-              f"scaled by {BOOT_OPS['rot_high']} + {BOOT_OPS['rot_low']} rotations and {BOOT_OPS['relin']} "
-              "relinearisations per bootstrapped ciphertext")
+            t[name] = time.perf_counter() - t0
+        t["bwd"] = 0.0
+    x = O.fill(902, (3, 27, n), list(o.primes[:27]) * 3)
+    t0 = time.perf_counter()
+    o.relinearize(x, key)
+    t["relin"] = time.perf_counter() - t0
+    per_boot = sum(BOOT_OPS[k] * t[k] for k in BOOT_OPS) + 2 * t["bwd"]
+    what = (f"one Sh-Rot of a group of {shared} at 34 primes ({t['rot_high'] * shared:.2f} s), one at 3 primes "
+            f"({t['rot_low'] * shared:.2f} s), one FmtSwitch backward of the group at 33 primes "
+            f"({t['bwd'] * shared:.2f} s), each / {shared} per ciphertext" if shared else
+            f"one HRotate at 34 primes ({t['rot_high']:.2f} s), one at 3 primes ({t['rot_low']:.2f} s)")
+    sample = (f"{what}, and one relinearisation at 27 primes ({t['relin']:.2f} s) on the CPU oracle (OpenMP "
+              f"over limbs), scaled by {BOOT_OPS['rot_high']} + {BOOT_OPS['rot_low']} rotations"
+              f"{' + 2 backward switches' if shared else ''} and {BOOT_OPS['relin']} relinearisations per "
+              "bootstrapped ciphertext")
     return 1.0 / per_boot, os.cpu_count(), sample
 
 
@@ -514,7 +529,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks"])
     ap.add_argument("--batch", type=int, default=None)
-    ap.add_argument("--shared", type=int, default=0,
+    ap.add_argument("--shared", type=int, default=8,
                     help="boot: shared-a group size n (0 = ordinary ciphertexts)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
@@ -536,7 +551,7 @@ def main():
         vals = []
         for i in range(args.warmup + args.steps):
             if args.workload == "boot":
-                v, cores, sample = cpu_boot_estimate()
+                v, cores, sample = cpu_boot_estimate(args.shared)
             else:
                 v, cores = cpu_prim_chain()
                 sample = "one full config-1 chain per step"
@@ -549,7 +564,8 @@ def main():
             "value": round(value, 6), "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1000.0 / value, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": args.workload + " (reference CPU arm: the oracle restatement)"},
+            "config": {"workload": args.workload + " (reference CPU arm: the oracle restatement)",
+                       "shared_a_group": (args.shared or None) if args.workload == "boot" else None},
             "cpu_baseline": {"value": round(value, 6), "unit": unit, "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(value, 6), "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -570,7 +586,7 @@ def main():
     if rank == 0:
         if not args.no_cpu_baseline and args.workload in ("boot", "prim"):
             if args.workload == "boot":
-                v, cores, sample = cpu_boot_estimate()
+                v, cores, sample = cpu_boot_estimate(args.shared)
                 res["cpu_baseline"] = {"value": round(v, 6), "unit": "bootstraps/s", "cores": cores,
                                        "kind": "port", "sample": sample}
             else:

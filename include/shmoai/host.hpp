@@ -1,0 +1,315 @@
+// C++ host API of the B200 CKKS core: the evaluator, key material and S2C-first
+// (shared-a) batched bootstrapping that the MOAI driver calls, over the C ABI of
+// include/shmoai_ckks.h.
+//
+// Mirrors the reference's host classes (src/include/source/ckks_evaluator_parallel.cuh:13-680:
+// moai::Encoder / Encryptor / Evaluator / Decryptor / CKKSEvaluator) and
+// BatchBootstrapper::{prepare, prepare_shared_keys, bootstrap_ordinary_s2c_first,
+// bootstrap_shared_a_s2c_first} (src/include/source/bootstrapping/BatchBootstrap.cuh:470-820),
+// with two differences that the B200 design asks for:
+//   * a Ciphertext is a BATCH [count][size][L][N] (one launch per operation for the
+//     whole batch); a shared-a batch is the same type with `shared` set, holding
+//     [groups][members + 1][L][N] = (b_0 .. b_{n-1}, a) per group
+//     (SharedACiphertextBatch, SharedACiphertext.cuh:22-99);
+//   * scales are tracked exactly (products and quotients of primes and encoded
+//     constants), and adding ciphertexts whose scales differ throws, instead of the
+//     reference's assumed-nominal scales and *_reduced_error level alignment.
+// Errors throw shmoai::Error with the C ABI's message.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../shmoai_ckks.h"
+
+namespace shmoai {
+
+using cplx = std::complex<double>;
+
+struct Error : std::runtime_error {
+    explicit Error(const std::string &msg, int code_ = SHM_EINVAL) : std::runtime_error(msg), code(code_) {}
+    int code;  // the SHM_E* status behind it
+};
+
+class Context;
+
+// Move-only owner of shm_malloc'd device words.
+class DeviceBuffer {
+   public:
+    DeviceBuffer() = default;
+    DeviceBuffer(const Context &c, size_t words);
+    ~DeviceBuffer();
+    DeviceBuffer(DeviceBuffer &&o) noexcept;
+    DeviceBuffer &operator=(DeviceBuffer &&o) noexcept;
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    uint64_t *data() const { return p_; }
+    size_t words() const { return words_; }
+    DeviceBuffer clone() const;
+
+   private:
+    const Context *ctx_ = nullptr;
+    uint64_t *p_ = nullptr;
+    size_t words_ = 0;
+};
+
+// Ring parameters, prime chain Q (nq primes) + special primes P (np), device, stream.
+class Context {
+   public:
+    Context(uint32_t log_n, const std::vector<int> &bits, uint32_t n_special, int device = 0, void *stream = nullptr);
+    Context(uint32_t log_n, const std::vector<uint64_t> &primes, uint32_t n_special, int device = 0,
+            void *stream = nullptr);
+    ~Context();
+    Context(const Context &) = delete;
+    Context &operator=(const Context &) = delete;
+
+    shm_context *handle() const { return h_; }
+    void *stream() const { return stream_; }
+    void check(int rc) const;  // throws Error unless rc == SHM_OK
+    void synchronize() const;
+    size_t slot_count() const { return n / 2; }
+    // reference chain index of a ciphertext with L primes (context.cu:148-174)
+    size_t chain_index(uint32_t L) const { return nq - L + 1; }
+
+    uint32_t log_n = 0, n = 0, nq = 0, np = 0, dnum = 0;
+    std::vector<uint64_t> primes;
+
+   private:
+    void init();
+    shm_context *h_ = nullptr;
+    void *stream_ = nullptr;
+};
+
+struct Plaintext {
+    DeviceBuffer data;  // [L][N], NTT form
+    uint32_t L = 0;
+    double scale = 1.0;
+    size_t coeff_modulus_size() const { return L; }
+};
+
+// A batch of ciphertexts [count][size][L][N] (NTT form), or, with `shared`, a batch
+// of shared-a groups [count][size][L][N] with size = members + 1.
+struct Ciphertext {
+    DeviceBuffer data;
+    uint32_t count = 0, size = 2, L = 0;
+    double scale_ = 1.0;
+    bool shared = false;
+
+    double scale() const { return scale_; }
+    void set_scale(double s) { scale_ = s; }
+    size_t coeff_modulus_size() const { return L; }
+    uint32_t members() const { return shared ? size - 1 : 1; }
+    size_t polys() const { return (size_t)count * size; }
+};
+
+class Encoder {
+   public:
+    explicit Encoder(const Context &c);
+    size_t slot_count() const { return c_.n / 2; }
+    // unrounded coefficients of the polynomial whose slots are z * scale (z padded with 0)
+    std::vector<double> encode_float(const cplx *z, size_t len, double scale) const;
+    // rounded (half to even) integer coefficients; |c| < 2^62 or Error
+    std::vector<int64_t> encode_coeffs(const cplx *z, size_t len, double scale) const;
+    Plaintext encode(const std::vector<cplx> &z, uint32_t L, double scale) const;
+    // a constant: the single coefficient round(value * scale)
+    // (moai::Encoder::encode(double), ckks_evaluator_parallel.cuh:73-92)
+    Plaintext encode(double value, uint32_t L, double scale) const;
+    std::vector<cplx> decode(const std::vector<double> &coeffs, double scale) const;
+    // signed integer coefficients [n_polys][N] (host) -> NTT-form residues [n_polys][L][N] at `out`
+    void upload(const int64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const;
+
+   private:
+    void fft(std::vector<cplx> &a, bool inverse) const;
+    const Context &c_;
+    std::vector<uint32_t> exps_;  // 5^j mod 2N
+    std::vector<cplx> roots_;     // exp(2 pi i k / 2N)
+};
+
+// The keys of one group size of shared-a batches.
+struct SharedAKeys {
+    uint32_t members = 0;
+    std::map<uint32_t, DeviceBuffer> galois;  // element -> [dnum][members + 1][QP][N]
+    DeviceBuffer format;                      // [members][members + 1][QP][N]
+    std::vector<DeviceBuffer> backward;       // members x [dnum][2][QP][N] (s'_i -> s)
+};
+
+// Secret key, auxiliary secrets and every evaluation key (the reference's
+// PhantomSecretKey key generation, secretkey.cu:328-646, and SharedAKeyGen,
+// FmtSwitch.cuh:235-305 / ShRotate.cu:54-162 / FmtSwitch.cu:165-270), plus symmetric
+// encryption and decryption.  Deterministic in `seed`.
+class KeyGenerator {
+   public:
+    KeyGenerator(const Context &c, uint32_t hamming_weight = 192, uint64_t seed = 0x5EED);
+    const DeviceBuffer &secret() const { return s_; }  // [QP][N] NTT form
+    DeviceBuffer switching_key(const DeviceBuffer &s_new);  // [dnum][2][QP][N]: s_new -> s
+    DeviceBuffer relin_key();
+    DeviceBuffer galois_key(uint32_t elt);
+    std::map<uint32_t, DeviceBuffer> galois_keys(const std::vector<uint32_t> &elts);
+
+    void gen_aux_secrets(uint32_t members, uint32_t hamming_weight = 192);
+    DeviceBuffer shared_galois_key(uint32_t elt);
+    DeviceBuffer format_key();
+    std::vector<DeviceBuffer> backward_keys();
+    SharedAKeys shared_keys(uint32_t members, const std::vector<uint32_t> &elts, uint32_t hamming_weight = 192);
+
+    // z: count rows of up to N/2 slot values
+    Ciphertext encrypt(const std::vector<std::vector<cplx>> &z, double scale, uint32_t L);
+    // centred limb-0 coefficients of every member (exact while |m| < q0 / 2)
+    std::vector<std::vector<double>> decrypt_coeffs(const Ciphertext &ct);
+    std::vector<std::vector<cplx>> decrypt(const Ciphertext &ct);
+
+   private:
+    uint64_t next_seed();
+    std::vector<int64_t> ternary(uint32_t hamming_weight);
+    DeviceBuffer ntt_qp(const std::vector<int64_t> &coeffs) const;  // [QP][N]
+    DeviceBuffer automorph(const std::vector<int64_t> &coeffs, uint32_t elt) const;
+    // B_{d,row} += unit * s (unit: residues over QP)
+    struct KeyTerm {
+        uint32_t row;
+        std::vector<uint64_t> unit;
+        const DeviceBuffer *s;
+    };
+    // [D][olds + 1][QP][N]: digit d = (B_{d,0} .. B_{d,n-1}, A_d), B_{d,i} = e - A_d olds[i] + terms
+    DeviceBuffer multi_key(const std::vector<const DeviceBuffer *> &olds, const std::vector<std::vector<KeyTerm>> &adds);
+    std::vector<uint64_t> p_units(int digit) const;
+
+    const Context &c_;
+    Encoder enc_;
+    uint64_t seed_, ctr_ = 0;
+    std::vector<int64_t> s_coeffs_;
+    DeviceBuffer s_;
+    std::vector<std::vector<int64_t>> aux_coeffs_;
+    std::vector<DeviceBuffer> aux_;
+};
+
+// moai::Encryptor / moai::Decryptor names over the key generator's secret.
+class Encryptor {
+   public:
+    explicit Encryptor(KeyGenerator &kg) : kg_(kg) {}
+    Ciphertext encrypt(const std::vector<std::vector<cplx>> &z, double scale, uint32_t L) {
+        return kg_.encrypt(z, scale, L);
+    }
+
+   private:
+    KeyGenerator &kg_;
+};
+
+class Decryptor {
+   public:
+    explicit Decryptor(KeyGenerator &kg) : kg_(kg) {}
+    std::vector<std::vector<cplx>> decrypt(const Ciphertext &ct) { return kg_.decrypt(ct); }
+
+   private:
+    KeyGenerator &kg_;
+};
+
+// moai::Evaluator over batches, with exact scale tracking.
+class Evaluator {
+   public:
+    Evaluator(const Context &c, const Encoder &enc);
+    const Context &context() const { return c_; }
+    const Encoder &encoder() const { return enc_; }
+
+    // keys (not owned)
+    const DeviceBuffer *relin_key = nullptr;
+    const std::map<uint32_t, DeviceBuffer> *galois_keys = nullptr;
+    const SharedAKeys *shared_keys = nullptr;
+
+    static bool same_scale(double a, double b, double rel = 1e-11);
+
+    Ciphertext mod_switch_to(const Ciphertext &a, uint32_t L) const;  // drop limbs
+    Ciphertext add(const Ciphertext &a, const Ciphertext &b) const;
+    Ciphertext sub(const Ciphertext &a, const Ciphertext &b) const;
+    Ciphertext negate(const Ciphertext &a) const;
+    Ciphertext multiply_plain(const Ciphertext &a, const Plaintext &p) const;
+    Ciphertext multiply_int(const Ciphertext &a, int64_t k) const;
+    Ciphertext add_const(const Ciphertext &a, double c) const;
+    Ciphertext rescale_to_next(const Ciphertext &a) const;
+    // a * round(c * T) with T = target * q / a.scale, then rescale: result at exactly `target`
+    Ciphertext multiply_const(const Ciphertext &a, double c, double target) const;
+    Ciphertext multiply_const(const Ciphertext &a, double c) const { return multiply_const(a, c, a.scale_); }
+    // a * round(c * T) without rescale; the result's scale is a.scale * T
+    Ciphertext multiply_const_unscaled(const Ciphertext &a, double c, double T) const;
+    Ciphertext adjust(const Ciphertext &a, uint32_t L, double scale) const;
+    Ciphertext multiply(const Ciphertext &a, const Ciphertext &b, bool rescale = true) const;
+    Ciphertext square(const Ciphertext &a) const { return multiply(a, a); }
+    // sum_k X_k * P_k (same level and scale), one launch; result scale X.scale * P.scale
+    Ciphertext multiply_plain_accumulate(const std::vector<const Ciphertext *> &X,
+                                         const std::vector<const Plaintext *> &P) const;
+
+    uint32_t galois_elt(int step) const;
+    Ciphertext rotate_vector(const Ciphertext &a, int step) const;
+    std::map<int, Ciphertext> rotate_many(const Ciphertext &a, const std::vector<int> &steps) const;
+    Ciphertext complex_conjugate(const Ciphertext &a) const;
+    // times i (sign +1) or -i, through the monomial X^(N/2): exact, no level
+    Ciphertext multiply_i(const Ciphertext &a, int sign = 1) const;
+    Ciphertext mod_raise(const Ciphertext &a1, uint32_t L) const;  // 1 prime -> L primes, centred lift
+    Ciphertext concat(const Ciphertext &a, const Ciphertext &b) const;
+    Ciphertext slice(const Ciphertext &a, uint32_t first, uint32_t count) const;
+
+    Ciphertext to_shared(const Ciphertext &a, uint32_t members) const;  // FmtSwitch forward
+    Ciphertext from_shared(const Ciphertext &a) const;                  // FmtSwitch backward
+
+   private:
+    std::vector<uint64_t> residues(double integral, uint32_t L) const;
+    std::vector<Ciphertext> automorphisms(const Ciphertext &a, const std::vector<uint32_t> &elts) const;
+    uint64_t *ws(size_t bytes) const;
+    Ciphertext like(const Ciphertext &a, uint32_t L) const;
+    const Plaintext &monomial_half() const;
+
+    const Context &c_;
+    const Encoder &enc_;
+    mutable DeviceBuffer ws_;
+    mutable Plaintext mono_;
+};
+
+struct BootstrapParams {
+    double scale = 70368744177664.0;  // 2^46
+    uint32_t input_level = 4;         // primes of the input (S2C-first)
+    int K = 25;                       // EvalMod range
+    int degree = 47;                  // Chebyshev degree
+    int double_angles = 3;
+    double F = 1.0 / 16;  // amplitude factor of SlotToCoeff (Bootstrapper.cuh:31)
+};
+
+class LinearTransform;
+
+// S2C-first batched bootstrapping, ordinary and shared-a (BatchBootstrap.cuh:674-819).
+class BatchBootstrapper {
+   public:
+    BatchBootstrapper(Evaluator &ev, BootstrapParams p = BootstrapParams());
+    ~BatchBootstrapper();
+    // encode the slot-transform diagonals (resident) and the EvalMod polynomial
+    void prepare();
+    std::vector<int> rotation_steps() const;
+    std::vector<uint32_t> galois_elts() const;
+    // the shared-a keys of groups of `members` for this bootstrapper's rotations
+    SharedAKeys prepare_shared_keys(KeyGenerator &kg, uint32_t members, uint32_t hamming_weight = 192) const;
+    Ciphertext bootstrap_ordinary_s2c_first(const Ciphertext &ct) const;
+    // groups of `members` consecutive ciphertexts; needs ev.shared_keys for that size
+    Ciphertext bootstrap_shared_a_s2c_first(const Ciphertext &ct, uint32_t members) const;
+    // EvalMod of ciphertexts holding t / K: c_fin * sin(2 pi t) read at scale Delta
+    Ciphertext evalmod(const Ciphertext &x) const;
+    const BootstrapParams &params() const { return p_; }
+
+   private:
+    void slots_to_re_im(Ciphertext x, Ciphertext &re, Ciphertext &im) const;
+    Ciphertext finish(const Ciphertext &re, const Ciphertext &im) const;
+
+    Evaluator &ev_;
+    BootstrapParams p_;
+    std::vector<LinearTransform *> s2c_, c2s_;
+    std::vector<double> cheb_;
+    double q0_ = 0, c_fin_ = 0;
+    uint32_t top_ = 0;
+};
+
+// max |V w - layers(w)| / max |V w| of the slot-transform factorisation at n slots
+// (a self-check of the planning code on random input)
+double slot_transform_selfcheck(uint32_t log_slots);
+
+}  // namespace shmoai

@@ -216,6 +216,37 @@ int shm_ctpt_matmul(const shm_context *ctx, const uint64_t *X, const int64_t *W,
 int shm_ctpt_matmul_cuda_core(const shm_context *ctx, const uint64_t *X, const int64_t *W, uint64_t *Y,
                               uint32_t n_in, uint32_t n_out, uint32_t L, void *stream);
 
+/* ---- device memory (the allocator of the host library, include/shmoai/host.hpp) ----
+ * Stream-ordered blocks from a per-context pool that keeps freed blocks for reuse, so
+ * the pipeline's many short-lived buffers cost no driver calls or synchronisation.
+ * Replaces the reference's cuda_auto_ptr over its cudaMallocAsync pool
+ * (thirdparty/phantom-fhe/include/cuda_wrapper.cuh:78-211). */
+#define SHM_COPY_H2D 0
+#define SHM_COPY_D2H 1
+#define SHM_COPY_D2D 2
+int shm_malloc(const shm_context *ctx, size_t bytes, void **out, void *stream);
+int shm_free(const shm_context *ctx, void *ptr, void *stream);
+/* Copies involving host memory return when the copy is done; device-to-device copies are
+ * asynchronous on `stream`. */
+int shm_memcpy(const shm_context *ctx, void *dst, const void *src, size_t bytes, int kind, void *stream);
+int shm_synchronize(const shm_context *ctx, void *stream);
+
+/* ---- sampling (key generation, encryption) ----
+ * Counter-based: value i of a call is a function of (seed, i) only, so the GPU and the
+ * CPU restatement draw identical keys and ciphertexts.  Distributions as in the
+ * reference's samplers (thirdparty/phantom-fhe/src/prng.cu:142-240); the streams differ.
+ * Uniform residues: out [n_polys][L][N], limb i uniform mod prime i (L <= nq + np). */
+int shm_sample_uniform(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed,
+                       void *stream);
+/* Centred binomial over 21 + 21 bits (sigma ~ 3.24), one integer polynomial per poly,
+ * written as residues mod each of the first L primes (coefficient form). */
+int shm_sample_cbd(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed,
+                   void *stream);
+/* Signed coefficients [n_polys][N] (device) -> residues [n_polys][L][N] (coefficient form).
+ * Replaces the signed decomposition of the encoder (rns_base.cu:51-200). */
+int shm_lift_signed(const shm_context *ctx, const int64_t *coeffs, uint64_t *out, uint32_t n_polys, uint32_t L,
+                    void *stream);
+
 #ifdef __cplusplus
 }
 #endif

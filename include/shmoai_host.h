@@ -1,0 +1,98 @@
+/* C ABI of the C++ host library (include/shmoai/host.hpp): key material, encryption,
+ * the batched evaluator and S2C-first (shared-a) bootstrapping behind opaque handles,
+ * for C callers and FFI bindings (ctypes in this repository's Python layer).
+ *
+ * Replaces the entry points the MOAI driver reaches through the reference's C++ classes:
+ *   shm_host_*      moai::Encoder / Encryptor / Evaluator / Decryptor and key generation
+ *                   (src/include/source/ckks_evaluator_parallel.cuh:13-598,
+ *                   thirdparty/phantom-fhe/src/secretkey.cu:328-646);
+ *   shm_host_*shared*  SharedAKeyGen, fmt_switch_forward / fmt_switch_backward, shared_a_rotate
+ *                   (src/include/source/bootstrapping/FmtSwitch.cu:154-429, ShRotate.cu:54-257);
+ *   shm_boot_*      BatchBootstrapper::{prepare, prepare_shared_keys,
+ *                   bootstrap_ordinary_s2c_first, bootstrap_shared_a_s2c_first}
+ *                   (src/include/source/bootstrapping/BatchBootstrap.cuh:470-819).
+ * Status codes are those of include/shmoai_ckks.h; shm_host_last_error() explains the
+ * last failure of the calling thread.  A shm_ct is a batch: ordinary ciphertexts
+ * [count][size][L][N], or shared-a groups [count][members + 1][L][N] (shared = 1). */
+#ifndef SHMOAI_HOST_H
+#define SHMOAI_HOST_H
+#include <stddef.h>
+#include <stdint.h>
+
+#include "shmoai_ckks.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct shm_host shm_host;
+typedef struct shm_ct shm_ct;
+typedef struct shm_boot shm_boot;
+
+const char *shm_host_last_error(void);
+
+/* Context (n_primes = n_q + n_special, special primes last), secret key of Hamming weight
+ * `hamming_weight`, deterministic in `seed`. */
+int shm_host_create(shm_host **out, uint32_t log_n, const uint64_t *primes, uint32_t n_primes, uint32_t n_special,
+                    int device, uint32_t hamming_weight, uint64_t seed);
+int shm_host_create_from_bits(shm_host **out, uint32_t log_n, const int *bits, uint32_t n_primes,
+                              uint32_t n_special, int device, uint32_t hamming_weight, uint64_t seed);
+void shm_host_destroy(shm_host *h);
+const shm_context *shm_host_context(const shm_host *h);
+/* the n_q + n_special primes of the host's context */
+int shm_host_primes(const shm_host *h, uint64_t *out);
+int shm_host_synchronize(shm_host *h);
+
+int shm_host_gen_relin_key(shm_host *h);
+int shm_host_gen_galois_keys(shm_host *h, const uint32_t *elts, uint32_t n_elts);
+/* auxiliary secrets, format key, backward keys and the Sh-Galois keys of `elts` for
+ * shared-a groups of `members` */
+int shm_host_gen_shared_keys(shm_host *h, uint32_t members, uint32_t hamming_weight, const uint32_t *elts,
+                             uint32_t n_elts);
+uint32_t shm_host_galois_elt(const shm_host *h, int step);
+
+/* Encrypt `count` rows of n_values complex slot values (re, im: [count][n_values]) at L
+ * primes and `scale`. */
+int shm_host_encrypt(shm_host *h, const double *re, const double *im, uint32_t count, uint32_t n_values, uint32_t L,
+                     double scale, shm_ct **out);
+/* Decrypt to [members in the batch][N/2] slot values (shared-a groups: member i of group
+ * g is row g * members + i). */
+int shm_host_decrypt(shm_host *h, const shm_ct *ct, double *re, double *im);
+
+int shm_ct_from_host(shm_host *h, const uint64_t *data, uint32_t count, uint32_t size, uint32_t L, double scale,
+                     int shared, shm_ct **out);
+int shm_ct_to_host(shm_host *h, const shm_ct *ct, uint64_t *data);
+int shm_ct_info(const shm_ct *ct, uint32_t *count, uint32_t *size, uint32_t *L, double *scale, int *shared);
+const uint64_t *shm_ct_device_data(const shm_ct *ct);
+void shm_ct_destroy(shm_ct *ct);
+
+int shm_host_add(shm_host *h, const shm_ct *a, const shm_ct *b, shm_ct **out);
+int shm_host_sub(shm_host *h, const shm_ct *a, const shm_ct *b, shm_ct **out);
+/* multiply + relinearise + rescale */
+int shm_host_multiply(shm_host *h, const shm_ct *a, const shm_ct *b, shm_ct **out);
+int shm_host_rescale(shm_host *h, const shm_ct *a, shm_ct **out);
+int shm_host_multiply_const(shm_host *h, const shm_ct *a, double value, shm_ct **out);
+int shm_host_rotate(shm_host *h, const shm_ct *a, int step, shm_ct **out);
+int shm_host_conjugate(shm_host *h, const shm_ct *a, shm_ct **out);
+int shm_host_multiply_i(shm_host *h, const shm_ct *a, int sign, shm_ct **out);
+int shm_host_to_shared(shm_host *h, const shm_ct *a, uint32_t members, shm_ct **out);
+int shm_host_from_shared(shm_host *h, const shm_ct *a, shm_ct **out);
+
+/* Bootstrapper at the host's parameters (scale Delta, input at `input_level` primes);
+ * prepares the slot-transform diagonals and the EvalMod polynomial. */
+int shm_boot_create(shm_host *h, double scale, uint32_t input_level, shm_boot **out);
+void shm_boot_destroy(shm_boot *b);
+/* the Galois elements its rotations need (n_out set; at most `cap` written) */
+int shm_boot_galois_elts(const shm_boot *b, uint32_t *out, uint32_t cap, uint32_t *n_out);
+/* bootstrap a batch at input_level primes; members = 0: ordinary ciphertexts,
+ * members = n: shared-a groups of n consecutive ciphertexts (keys from
+ * shm_host_gen_shared_keys) */
+int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out);
+
+/* self-check of the slot-transform factorisation at 2^log_slots slots (max error) */
+double shm_slot_transform_selfcheck(uint32_t log_slots);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SHMOAI_HOST_H */

@@ -1,0 +1,485 @@
+/* TEST INFRASTRUCTURE ONLY.  The CPU oracle behind the C ABI of include/shmoai_ckks.h:
+ * every entry point the C++ host library (include/shmoai/host.hpp) calls, implemented on
+ * host memory with the oracle's restatement of the reference arithmetic (ckks_oracle.c).
+ * oracle/Makefile links the host library's unchanged sources against this file to get
+ * the whole pipeline (key generation, evaluator, bootstrapping) on the CPU, which the
+ * tests compare bit for bit with the same pipeline on the CUDA library.  Nothing in the
+ * product links or loads it.
+ *
+ * "Device" memory is host memory here; streams and workspaces are ignored.  The samplers
+ * use the same counter-based function as the CUDA library (splitmix64's output mix of
+ * seed + (index + 1) * golden gamma), so keys and ciphertexts are identical. */
+#include <stdio.h>
+
+#include "ckks_oracle.c"
+
+#include "../include/shmoai_ckks.h"
+
+struct shm_context {
+    orc_ctx *c;
+    uint32_t dnum;
+};
+
+static __thread char g_err[256];
+
+static int fail(const char *msg) {
+    snprintf(g_err, sizeof g_err, "%s", msg);
+    return SHM_EINVAL;
+}
+
+const char *shm_last_error(void) { return g_err; }
+uint64_t shm_kernel_launches(void) { return 0; }
+
+static int make_ctx(shm_context **out, uint32_t log_n, const uint64_t *primes, uint32_t nq, uint32_t np) {
+    if (!out) return fail("null output");
+    if (log_n != 12 && log_n != 16) return fail("log_n must be 12 or 16");
+    shm_context *h = (shm_context *)calloc(1, sizeof(shm_context));
+    h->c = orc_ctx_create(log_n, primes, nq, np);
+    h->dnum = np ? nq / np : 0;
+    *out = h;
+    return SHM_OK;
+}
+
+int shm_context_create(shm_context **out, uint32_t log_n, const int *bits, uint32_t n_q, uint32_t n_p, int device) {
+    (void)device;
+    uint64_t *p = (uint64_t *)malloc(sizeof(uint64_t) * (n_q + n_p));
+    if (orc_gen_primes(log_n, bits, n_q + n_p, p) != 0) {
+        free(p);
+        return fail("not enough primes");
+    }
+    int rc = make_ctx(out, log_n, p, n_q, n_p);
+    free(p);
+    return rc;
+}
+
+int shm_context_create_from_primes(shm_context **out, uint32_t log_n, const uint64_t *primes, uint32_t n_q,
+                                   uint32_t n_p, int device) {
+    (void)device;
+    return make_ctx(out, log_n, primes, n_q, n_p);
+}
+
+void shm_context_destroy(shm_context *ctx) {
+    if (!ctx) return;
+    orc_ctx_destroy(ctx->c);
+    free(ctx);
+}
+
+int shm_context_info(const shm_context *ctx, uint32_t *log_n, uint32_t *n_q, uint32_t *n_p, uint32_t *dnum) {
+    if (!ctx) return fail("null context");
+    if (log_n) *log_n = ctx->c->log_n;
+    if (n_q) *n_q = ctx->c->nq;
+    if (n_p) *n_p = ctx->c->np;
+    if (dnum) *dnum = ctx->dnum;
+    return SHM_OK;
+}
+
+int shm_context_primes(const shm_context *ctx, uint64_t *out) {
+    if (!ctx) return fail("null context");
+    memcpy(out, ctx->c->primes, sizeof(uint64_t) * (ctx->c->nq + ctx->c->np));
+    return SHM_OK;
+}
+
+uint32_t shm_galois_elt_from_step(const shm_context *ctx, int step) {
+    return ctx ? orc_galois_elt_from_step(ctx->c->log_n, step) : 0;
+}
+
+/* ---- memory */
+
+int shm_malloc(const shm_context *ctx, size_t bytes, void **out, void *stream) {
+    (void)ctx;
+    (void)stream;
+    if (!out) return fail("null output pointer");
+    *out = NULL;
+    if (!bytes) return SHM_OK;
+    if (posix_memalign(out, 64, (bytes + 63) & ~(size_t)63)) {
+        *out = NULL;
+        snprintf(g_err, sizeof g_err, "host allocation of %zu bytes failed", bytes);
+        return SHM_ENOMEM;
+    }
+    return SHM_OK;
+}
+
+int shm_free(const shm_context *ctx, void *ptr, void *stream) {
+    (void)ctx;
+    (void)stream;
+    free(ptr);
+    return SHM_OK;
+}
+
+int shm_memcpy(const shm_context *ctx, void *dst, const void *src, size_t bytes, int kind, void *stream) {
+    (void)ctx;
+    (void)stream;
+    if (kind < SHM_COPY_H2D || kind > SHM_COPY_D2D) return fail("bad copy kind");
+    if (bytes) memmove(dst, src, bytes);
+    return SHM_OK;
+}
+
+int shm_synchronize(const shm_context *ctx, void *stream) {
+    (void)ctx;
+    (void)stream;
+    return SHM_OK;
+}
+
+/* ---- sampling (same function as shmoai_b200/csrc/sampling.cu) */
+
+static inline uint64_t mix64(uint64_t seed, uint64_t idx) {
+    uint64_t z = seed + (idx + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+int shm_sample_uniform(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed,
+                       void *stream) {
+    (void)stream;
+    const orc_ctx *c = ctx->c;
+    if (L < 1 || L > c->nq + c->np) return fail("level out of range");
+    size_t n = c->n;
+#pragma omp parallel for
+    for (int row = 0; row < (int)(n_polys * L); row++) {
+        uint64_t q = c->primes[row % L];
+        for (size_t k = 0; k < n; k++) {
+            uint64_t idx = ((uint64_t)row << c->log_n) + k;
+            uint64_t h1 = mix64(seed, 2 * idx), h2 = mix64(seed, 2 * idx + 1);
+            u128 t = (u128)h1 * q + (uint64_t)(((u128)h2 * q) >> 64);
+            out[(size_t)row * n + k] = (uint64_t)(t >> 64);
+        }
+    }
+    return SHM_OK;
+}
+
+int shm_sample_cbd(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed,
+                   void *stream) {
+    (void)stream;
+    const orc_ctx *c = ctx->c;
+    if (L < 1 || L > c->nq + c->np) return fail("level out of range");
+    size_t n = c->n;
+#pragma omp parallel for
+    for (int p = 0; p < (int)n_polys; p++)
+        for (size_t k = 0; k < n; k++) {
+            uint64_t h = mix64(seed, ((uint64_t)p << c->log_n) + k);
+            int e = __builtin_popcountll(h & 0x1FFFFFull) - __builtin_popcountll((h >> 21) & 0x1FFFFFull);
+            for (uint32_t i = 0; i < L; i++) {
+                uint64_t q = c->primes[i];
+                out[((size_t)p * L + i) * n + k] = e >= 0 ? (uint64_t)e : q - (uint64_t)(-e);
+            }
+        }
+    return SHM_OK;
+}
+
+int shm_lift_signed(const shm_context *ctx, const int64_t *coeffs, uint64_t *out, uint32_t n_polys, uint32_t L,
+                    void *stream) {
+    (void)stream;
+    const orc_ctx *c = ctx->c;
+    if (L < 1 || L > c->nq + c->np) return fail("level out of range");
+    size_t n = c->n;
+    for (uint32_t p = 0; p < n_polys; p++)
+        for (uint32_t i = 0; i < L; i++)
+            for (size_t k = 0; k < n; k++)
+                out[((size_t)p * L + i) * n + k] = signed_residue(coeffs[(size_t)p * n + k], c->primes[i]);
+    return SHM_OK;
+}
+
+/* ---- element-wise */
+
+static int lvl_ok(const shm_context *ctx, uint32_t L) { return ctx && L >= 1 && L <= ctx->c->nq + ctx->c->np; }
+
+int shm_ntt_forward(const shm_context *ctx, uint64_t *data, uint32_t n_polys, uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    orc_ntt(ctx->c, data, n_polys, L, 0);
+    return SHM_OK;
+}
+
+int shm_ntt_inverse(const shm_context *ctx, uint64_t *data, uint32_t n_polys, uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    orc_ntt(ctx->c, data, n_polys, L, 1);
+    return SHM_OK;
+}
+
+int shm_add(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+            uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    orc_add(ctx->c, a, b, out, n_polys, L);
+    return SHM_OK;
+}
+
+int shm_sub(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+            uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    size_t n = ctx->c->n;
+    for (size_t r = 0; r < (size_t)n_polys * L; r++) {
+        uint64_t q = ctx->c->primes[r % L];
+        for (size_t k = 0; k < n; k++) out[r * n + k] = submod(a[r * n + k], b[r * n + k], q);
+    }
+    return SHM_OK;
+}
+
+int shm_negate(const shm_context *ctx, const uint64_t *a, uint64_t *out, uint32_t n_polys, uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    size_t n = ctx->c->n;
+    for (size_t r = 0; r < (size_t)n_polys * L; r++) {
+        uint64_t q = ctx->c->primes[r % L];
+        for (size_t k = 0; k < n; k++) out[r * n + k] = a[r * n + k] ? q - a[r * n + k] : 0;
+    }
+    return SHM_OK;
+}
+
+int shm_multiply_plain(const shm_context *ctx, const uint64_t *ct, const uint64_t *pt, uint64_t *out,
+                       uint32_t n_polys, uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    orc_multiply_plain(ctx->c, ct, pt, out, n_polys, L);
+    return SHM_OK;
+}
+
+int shm_multiply(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_cts,
+                 uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    size_t ln = (size_t)L * ctx->c->n;
+    for (uint32_t i = 0; i < n_cts; i++) orc_tensor(ctx->c, a + i * 2 * ln, b + i * 2 * ln, out + i * 3 * ln, L);
+    return SHM_OK;
+}
+
+int shm_multiply_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *scalars, uint64_t *out,
+                        uint32_t n_polys, uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    size_t n = ctx->c->n;
+    for (size_t r = 0; r < (size_t)n_polys * L; r++) {
+        uint64_t q = ctx->c->primes[r % L], w = scalars[r % L];
+        for (size_t k = 0; k < n; k++) out[r * n + k] = mulmod(a[r * n + k], w, q);
+    }
+    return SHM_OK;
+}
+
+int shm_add_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *scalars, uint64_t *out,
+                   uint32_t n_cts, uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    size_t n = ctx->c->n, ln = (size_t)L * n;
+    for (uint32_t i = 0; i < n_cts; i++) {
+        const uint64_t *ai = a + i * 2 * ln;
+        uint64_t *oi = out + i * 2 * ln;
+        for (uint32_t j = 0; j < L; j++) {
+            uint64_t q = ctx->c->primes[j];
+            for (size_t k = 0; k < n; k++) oi[j * n + k] = addmod(ai[j * n + k], scalars[j], q);
+        }
+        memmove(oi + ln, ai + ln, ln * 8);
+    }
+    return SHM_OK;
+}
+
+int shm_multiply_plain_accumulate(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
+                                  uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
+                                  void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    size_t n = ctx->c->n;
+#pragma omp parallel for
+    for (int r = 0; r < (int)(n_polys * L); r++) {
+        uint32_t limb = (uint32_t)r % L;
+        uint64_t q = ctx->c->primes[limb];
+        for (size_t c = 0; c < n; c++) {
+            uint64_t acc = accumulate ? out[(size_t)r * n + c] : 0;
+            for (uint32_t t = 0; t < k; t++)
+                acc = addmod(acc, mulmod(X[t][(size_t)r * n + c], P[t][(size_t)limb * n + c], q), q);
+            out[(size_t)r * n + c] = acc;
+        }
+    }
+    return SHM_OK;
+}
+
+int shm_drop_limbs(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L_in,
+                   uint32_t L_out, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L_in) || L_out < 1 || L_out > L_in) return fail("bad limb counts");
+    size_t n = ctx->c->n;
+    for (uint32_t p = 0; p < n_polys; p++) memmove(out + (size_t)p * L_out * n, in + (size_t)p * L_in * n, L_out * n * 8);
+    return SHM_OK;
+}
+
+/* centred lift of one-limb polynomials (mod q0, NTT form) to L limbs (NTT form) */
+size_t shm_modraise_workspace_bytes(const shm_context *ctx, uint32_t n_polys) {
+    (void)ctx;
+    (void)n_polys;
+    return 0;
+}
+
+int shm_modraise(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                 void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    const orc_ctx *c = ctx->c;
+    if (L < 1 || L > c->nq) return fail("level out of range");
+    size_t n = c->n;
+    uint64_t q0 = c->primes[0], *x = (uint64_t *)malloc(n * 8);
+    for (uint32_t p = 0; p < n_polys; p++) {
+        memcpy(x, in + (size_t)p * n, n * 8);
+        orc_ntt_inv(x, c->log_n, q0, c->irp);
+        for (uint32_t j = 0; j < L; j++) {
+            uint64_t qj = c->primes[j], *o = out + ((size_t)p * L + j) * n;
+            for (size_t k = 0; k < n; k++) o[k] = x[k] > q0 / 2 ? submod(x[k] % qj, q0 % qj, qj) : x[k] % qj;
+        }
+    }
+    free(x);
+    orc_ntt(c, out, n_polys, L, 0);
+    return SHM_OK;
+}
+
+/* ---- level and key switching */
+
+size_t shm_rescale_workspace_bytes(const shm_context *ctx, uint32_t n_polys, uint32_t L) {
+    (void)ctx;
+    (void)n_polys;
+    (void)L;
+    return 0;
+}
+
+int shm_rescale(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ctx || L < 2 || L > ctx->c->nq) return fail("rescale needs 2 <= L <= n_q limbs");
+    orc_rescale(ctx->c, in, out, n_polys, L);
+    return SHM_OK;
+}
+
+static int ks_level(const shm_context *ctx, uint32_t L) {
+    const orc_ctx *c = ctx->c;
+    return L >= 1 && L <= c->nq && c->np && (L + c->np - 1) / c->np <= ctx->dnum;
+}
+
+size_t shm_keyswitch_workspace_bytes(const shm_context *ctx, uint32_t n_cts, uint32_t L) {
+    (void)ctx;
+    (void)n_cts;
+    (void)L;
+    return 0;
+}
+
+int shm_relinearize(const shm_context *ctx, const uint64_t *ct3, const uint64_t *relin_key, uint64_t *out,
+                    uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ks_level(ctx, L)) return fail("level out of range for key switching");
+    size_t ln = (size_t)L * ctx->c->n;
+    for (uint32_t i = 0; i < n_cts; i++) orc_relinearize(ctx->c, ct3 + i * 3 * ln, L, relin_key, ctx->dnum, out + i * 2 * ln);
+    return SHM_OK;
+}
+
+int shm_apply_galois(const shm_context *ctx, const uint64_t *ct, uint32_t galois_elt, const uint64_t *galois_key,
+                     uint64_t *out, uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes,
+                     void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ks_level(ctx, L)) return fail("level out of range for key switching");
+    if (!(galois_elt & 1) || galois_elt >= 2 * ctx->c->n) return fail("Galois element must be odd and < 2N");
+    size_t ln = (size_t)L * ctx->c->n;
+    for (uint32_t i = 0; i < n_cts; i++)
+        orc_apply_galois_ct(ctx->c, ct + i * 2 * ln, L, galois_elt, galois_key, ctx->dnum, out + i * 2 * ln);
+    return SHM_OK;
+}
+
+size_t shm_apply_galois_hoisted_workspace_bytes(const shm_context *ctx, uint32_t n_cts, uint32_t L) {
+    (void)ctx;
+    (void)n_cts;
+    (void)L;
+    return 0;
+}
+
+int shm_apply_galois_hoisted(const shm_context *ctx, const uint64_t *ct, uint32_t n_elts, const uint32_t *elts,
+                             const uint64_t *const *keys, uint64_t *const *outs, uint32_t n_cts, uint32_t L,
+                             void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ks_level(ctx, L)) return fail("level out of range for key switching");
+    size_t ln = (size_t)L * ctx->c->n;
+    uint64_t **o = (uint64_t **)malloc(sizeof(uint64_t *) * (n_elts ? n_elts : 1));
+    for (uint32_t i = 0; i < n_cts; i++) {
+        for (uint32_t e = 0; e < n_elts; e++) o[e] = outs[e] + i * 2 * ln;
+        orc_apply_galois_hoisted(ctx->c, ct + i * 2 * ln, L, n_elts, elts, keys, ctx->dnum, (uint64_t *const *)o);
+    }
+    free(o);
+    return SHM_OK;
+}
+
+size_t shm_shared_rotate_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members, uint32_t L) {
+    (void)ctx;
+    (void)n_groups;
+    (void)n_members;
+    (void)L;
+    return 0;
+}
+
+int shm_shared_rotate_hoisted(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members,
+                              uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs,
+                              uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ks_level(ctx, L)) return fail("level out of range for key switching");
+    size_t gl = (size_t)(n_members + 1) * L * ctx->c->n;
+    uint64_t **o = (uint64_t **)malloc(sizeof(uint64_t *) * (n_elts ? n_elts : 1));
+    for (uint32_t g = 0; g < n_groups; g++) {
+        for (uint32_t e = 0; e < n_elts; e++) o[e] = outs[e] + g * gl;
+        orc_shared_rotate_hoisted(ctx->c, sh + g * gl, n_members, L, n_elts, elts, keys, (uint64_t *const *)o);
+    }
+    free(o);
+    return SHM_OK;
+}
+
+size_t shm_fmt_switch_forward_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                              uint32_t L) {
+    (void)ctx;
+    (void)n_groups;
+    (void)n_members;
+    (void)L;
+    return 0;
+}
+
+int shm_fmt_switch_forward(const shm_context *ctx, const uint64_t *cts, uint32_t n_groups, uint32_t n_members,
+                           const uint64_t *key, uint64_t *out, uint32_t L, void *workspace, size_t workspace_bytes,
+                           void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ctx || L < 1 || L > ctx->c->nq) return fail("level out of range");
+    size_t ln = (size_t)L * ctx->c->n;
+    for (uint32_t g = 0; g < n_groups; g++)
+        orc_fmt_forward(ctx->c, cts + (size_t)g * n_members * 2 * ln, n_members, L, key,
+                        out + (size_t)g * (n_members + 1) * ln);
+    return SHM_OK;
+}
+
+size_t shm_fmt_switch_backward_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                               uint32_t L) {
+    (void)ctx;
+    (void)n_groups;
+    (void)n_members;
+    (void)L;
+    return 0;
+}
+
+int shm_fmt_switch_backward(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members,
+                            const uint64_t *const *keys, uint64_t *out, uint32_t L, void *workspace,
+                            size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ks_level(ctx, L)) return fail("level out of range for key switching");
+    size_t ln = (size_t)L * ctx->c->n;
+    for (uint32_t g = 0; g < n_groups; g++)
+        orc_fmt_backward(ctx->c, sh + (size_t)g * (n_members + 1) * ln, n_members, L, keys,
+                         out + (size_t)g * n_members * 2 * ln);
+    return SHM_OK;
+}

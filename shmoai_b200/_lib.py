@@ -22,8 +22,10 @@ _SZ = ctypes.c_size_t
 
 
 def build(jobs: int = 8) -> str:
-    """Compile the CUDA library for sm_100a in place (nvcc; no GPU needed)."""
+    """Compile the CUDA library for sm_100a and the C++ host library over it, in place
+    (nvcc / g++; no GPU needed)."""
     subprocess.run(["make", "-s", f"-j{jobs}", "-C", CSRC], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(HERE, "host")], check=True)
     return LIB_PATH
 
 

@@ -1,19 +1,19 @@
-"""Host-side mirror of ShMOAI's evaluator interface over the C ABI.
+"""Python binding of the C ABI (include/shmoai_ckks.h) on torch device tensors.
 
-``CKKSContext`` owns a device context (prime chain, twiddles, RNS constants)
-and exposes the batched entry points of include/shmoai_ckks.h on torch
-device tensors.  ``Ciphertext`` / ``Plaintext`` / ``Evaluator`` mirror the
-names, argument meaning and error behaviour of ``moai::Evaluator``
-(src/include/source/ckks_evaluator_parallel.cuh:150-562): level or scale
-mismatches raise ``ValueError`` (the reference throws std::invalid_argument).
+``CKKSContext`` owns a device context (prime chain, twiddles, RNS constants) and
+exposes the batched primitives -- NTT, element-wise ops, rescale, key switching,
+hoisted and shared-a (Sh-Rot, FmtSwitch) automorphisms, the ct-pt matmul -- for
+the parity tests and the kernel benchmarks.  The evaluator, key material and
+bootstrapping API (moai::Evaluator and BatchBootstrapper names) is the C++ host
+library, bound in shmoai_b200.host.
 
 Tensors are torch.int64 on the context's device holding uint64 residues
-(bit pattern preserved), shaped [..., L, N].
+(bit pattern preserved), shaped [..., L, N].  Errors raise ShmError with the
+library's message (the reference throws std::invalid_argument).
 """
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass, field
 
 import numpy as np
 import torch
@@ -193,104 +193,50 @@ class CKKSContext:
             return None, 0
         return _ptr(workspace), workspace.numel() * 8
 
+    # ---------------- hoisted and shared-a automorphisms ----------------
+    def apply_galois_hoisted(self, ct, elts, keys, stream=None):
+        """[n][2][L][N]: one ModUp of the c1 polynomials, one output batch per Galois element."""
+        p, L = self._levels(ct)
+        outs = [torch.empty_like(ct) for _ in elts]
+        ws = self.empty(max(1, lib().shm_apply_galois_hoisted_workspace_bytes(self._h, p // 2, L) // 8))
+        k = len(elts)
+        E = (ctypes.c_uint32 * k)(*elts)
+        K = (ctypes.c_void_p * k)(*[_ptr(x).value for x in keys])
+        O = (ctypes.c_void_p * k)(*[_ptr(x).value for x in outs])
+        check(lib().shm_apply_galois_hoisted(self._h, _ptr(ct), k, E, K, O, p // 2, L, _ptr(ws), ws.numel() * 8,
+                                             _stream(stream)))
+        return outs
 
-# ---------------------------------------------------------------------------
-# moai-style objects
+    def shared_rotate_hoisted(self, sh, elts, keys, stream=None):
+        """Shared-a groups [G][n + 1][L][N]: Sh-Rot by every element, one ModUp of each a."""
+        G, H, L = sh.shape[0], sh.shape[1], sh.shape[2]
+        outs = [torch.empty_like(sh) for _ in elts]
+        ws = self.empty(max(1, lib().shm_shared_rotate_workspace_bytes(self._h, G, H - 1, L) // 8))
+        k = len(elts)
+        E = (ctypes.c_uint32 * k)(*elts)
+        K = (ctypes.c_void_p * k)(*[_ptr(x).value for x in keys])
+        O = (ctypes.c_void_p * k)(*[_ptr(x).value for x in outs])
+        check(lib().shm_shared_rotate_hoisted(self._h, _ptr(sh), G, H - 1, k, E, K, O, L, _ptr(ws), ws.numel() * 8,
+                                              _stream(stream)))
+        return outs
 
-
-@dataclass
-class Ciphertext:
-    data: torch.Tensor  # [size][L][N]
-    scale: float
-    is_ntt_form: bool = True
-
-    @property
-    def coeff_modulus_size(self) -> int:
-        return self.data.shape[-2]
-
-    @property
-    def size(self) -> int:
-        return self.data.shape[0]
-
-
-@dataclass
-class Plaintext:
-    data: torch.Tensor  # [L][N]
-    scale: float
-
-
-@dataclass
-class Evaluator:
-    """moai::Evaluator method names over one CKKSContext."""
-
-    ctx: CKKSContext
-    relin_key: torch.Tensor | None = None
-    galois_keys: dict = field(default_factory=dict)  # elt -> key tensor
-
-    def _same(self, a: Ciphertext, b: Ciphertext, rel=1e-12):
-        if a.coeff_modulus_size != b.coeff_modulus_size:
-            raise ValueError("encrypted1 and encrypted2 parameter mismatch")
-        if abs(a.scale - b.scale) > rel * max(a.scale, b.scale):
-            raise ValueError("scale mismatch")
-
-    def add(self, a: Ciphertext, b: Ciphertext) -> Ciphertext:
-        self._same(a, b)
-        return Ciphertext(self.ctx.add(a.data, b.data), a.scale)
-
-    def add_inplace(self, a: Ciphertext, b: Ciphertext):
-        self._same(a, b)
-        self.ctx.add(a.data, b.data, out=a.data)
-
-    def sub(self, a: Ciphertext, b: Ciphertext) -> Ciphertext:
-        self._same(a, b)
-        return Ciphertext(self.ctx.sub(a.data, b.data), a.scale)
-
-    def negate(self, a: Ciphertext) -> Ciphertext:
-        return Ciphertext(self.ctx.negate(a.data), a.scale)
-
-    def multiply_plain(self, a: Ciphertext, p: Plaintext) -> Ciphertext:
-        if p.data.shape[-2] != a.coeff_modulus_size:
-            raise ValueError("encrypted and plain parameter mismatch")
-        return Ciphertext(self.ctx.multiply_plain(a.data, p.data), a.scale * p.scale)
-
-    def multiply(self, a: Ciphertext, b: Ciphertext) -> Ciphertext:
-        self._same(a, b, rel=float("inf"))
-        return Ciphertext(self.ctx.multiply(a.data, b.data), a.scale * b.scale)
-
-    def relinearize_inplace(self, a: Ciphertext):
-        if self.relin_key is None:
-            raise ValueError("relinearization key not set")
-        if a.size != 3:
-            raise ValueError("relinearize needs a size-3 ciphertext")
-        a.data = self.ctx.relinearize(a.data, self.relin_key)
-
-    def rescale_to_next_inplace(self, a: Ciphertext):
-        if a.coeff_modulus_size < 2:
-            raise ValueError("end of modulus switching chain reached")
-        q_last = float(self.ctx.primes[a.coeff_modulus_size - 1])
-        a.data = self.ctx.rescale(a.data)
-        a.scale = a.scale / q_last
-
-    def apply_galois_inplace(self, a: Ciphertext, elt: int):
-        if elt not in self.galois_keys:
-            raise ValueError("Galois elt not present")
-        a.data = self.ctx.apply_galois(a.data, elt, self.galois_keys[elt])
-
-    def rotate_vector_inplace(self, a: Ciphertext, step: int):
-        self.apply_galois_inplace(a, self.ctx.galois_elt(step))
-
-    def rotate_vector(self, a: Ciphertext, step: int) -> Ciphertext:
-        out = Ciphertext(a.data.clone(), a.scale)
-        self.rotate_vector_inplace(out, step)
+    def fmt_forward(self, cts, n, key, stream=None):
+        """[G * n][2][L][N] ciphertexts under s -> [G][n + 1][L][N] shared-a groups."""
+        m, L = cts.shape[0], cts.shape[2]
+        G = m // n
+        out = self.empty(G, n + 1, L, self.n)
+        ws = self.empty(max(1, lib().shm_fmt_switch_forward_workspace_bytes(self._h, G, n, L) // 8))
+        check(lib().shm_fmt_switch_forward(self._h, _ptr(cts), G, n, _ptr(key), _ptr(out), L, _ptr(ws),
+                                           ws.numel() * 8, _stream(stream)))
         return out
 
-    def complex_conjugate_inplace(self, a: Ciphertext):
-        self.apply_galois_inplace(a, self.ctx.galois_elt(0))
-
-    def transform_from_ntt_inplace(self, a: Ciphertext):
-        self.ctx.ntt_inverse_(a.data)
-        a.is_ntt_form = False
-
-    def transform_to_ntt_inplace(self, a: Ciphertext):
-        self.ctx.ntt_forward_(a.data)
-        a.is_ntt_form = True
+    def fmt_backward(self, sh, keys, stream=None):
+        """[G][n + 1][L][N] shared-a groups -> [G * n][2][L][N] ciphertexts under s."""
+        G, H, L = sh.shape[0], sh.shape[1], sh.shape[2]
+        n = H - 1
+        out = self.empty(G * n, 2, L, self.n)
+        ws = self.empty(max(1, lib().shm_fmt_switch_backward_workspace_bytes(self._h, G, n, L) // 8))
+        K = (ctypes.c_void_p * n)(*[_ptr(x).value for x in keys])
+        check(lib().shm_fmt_switch_backward(self._h, _ptr(sh), G, n, K, _ptr(out), L, _ptr(ws), ws.numel() * 8,
+                                            _stream(stream)))
+        return out

@@ -43,6 +43,24 @@ Context::~Context() {
     for (auto &kv : galois_perm) cudaFree(kv.second);
     for (auto &kv : ext_consts)
         for (void *p : kv.second) cudaFree(p);
+    if (pool) {
+        cudaDeviceSynchronize();
+        cudaMemPoolDestroy(pool);
+    }
+}
+
+cudaMemPool_t Context::mempool() {
+    std::lock_guard<std::mutex> g(mu);
+    if (!pool) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        SHM_CUDA(cudaMemPoolCreate(&pool, &props));
+        uint64_t keep = ~0ull;  // never return freed blocks to the driver on synchronisation
+        SHM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    return pool;
 }
 
 const uint32_t *Context::perm(uint32_t elt) {
@@ -591,6 +609,82 @@ int shm_drop_limbs(const shm_context *ctx, const uint64_t *in, uint64_t *out, ui
         const size_t n = c.n;
         SHM_CUDA(cudaMemcpy2DAsync(out, L_out * n * 8, in, L_in * n * 8, L_out * n * 8, n_polys,
                                    cudaMemcpyDeviceToDevice, S(stream)));
+    });
+}
+
+// ---- device memory of the host library
+
+int shm_malloc(const shm_context *ctx, size_t bytes, void **out, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        if (!out) throw std::invalid_argument("null output pointer");
+        *out = nullptr;
+        set_device(c);
+        cudaMemPool_t pool = c.mempool();
+        if (bytes == 0) return;
+        SHM_CUDA(cudaMallocFromPoolAsync(out, bytes, pool, S(stream)));
+    });
+}
+
+int shm_free(const shm_context *ctx, void *ptr, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        if (!ptr) return;
+        set_device(c);
+        SHM_CUDA(cudaFreeAsync(ptr, S(stream)));
+    });
+}
+
+int shm_memcpy(const shm_context *ctx, void *dst, const void *src, size_t bytes, int kind, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        cudaMemcpyKind k = kind == SHM_COPY_H2D   ? cudaMemcpyHostToDevice
+                           : kind == SHM_COPY_D2H ? cudaMemcpyDeviceToHost
+                           : kind == SHM_COPY_D2D ? cudaMemcpyDeviceToDevice
+                                                  : throw std::invalid_argument("bad copy kind");
+        if (!bytes) return;
+        set_device(c);
+        SHM_CUDA(cudaMemcpyAsync(dst, src, bytes, k, S(stream)));
+        if (kind != SHM_COPY_D2D) SHM_CUDA(cudaStreamSynchronize(S(stream)));  // host buffers may be pageable
+    });
+}
+
+int shm_synchronize(const shm_context *ctx, void *stream) {
+    return guard([&] {
+        set_device(ctx_of(ctx));
+        SHM_CUDA(cudaStreamSynchronize(S(stream)));
+    });
+}
+
+// ---- sampling and lifting
+
+int shm_sample_uniform(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed,
+                       void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::sample_uniform(c, out, n_polys, L, seed, S(stream));
+    });
+}
+
+int shm_sample_cbd(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed,
+                   void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::sample_cbd(c, out, n_polys, L, seed, S(stream));
+    });
+}
+
+int shm_lift_signed(const shm_context *ctx, const int64_t *coeffs, uint64_t *out, uint32_t n_polys, uint32_t L,
+                    void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::lift_signed(c, coeffs, out, n_polys, L, S(stream));
     });
 }
 

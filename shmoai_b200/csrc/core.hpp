@@ -60,9 +60,14 @@ struct Context {
     void *arena = nullptr;
     size_t arena_bytes = 0;
 
+    // stream-ordered allocation pool of shm_malloc / shm_free (created on first use);
+    // freed blocks stay in the pool for reuse
+    cudaMemPool_t pool = nullptr;
+
     ~Context();
     const uint32_t *perm(uint32_t elt);
     void *workspace(size_t bytes);
+    cudaMemPool_t mempool();
 };
 
 Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uint32_t nq, uint32_t np, int device);
@@ -130,6 +135,11 @@ void ctpt_matmul(const Context &c, const uint64_t *X, const int64_t *W, uint64_t
 void ctpt_matmul_cuda_core(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in,
                            uint32_t n_out, uint32_t L, cudaStream_t st);
 size_t ctpt_tc_ws_bytes(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);
+
+// counter-based samplers and the signed lift (sampling.cu)
+void sample_uniform(const Context &c, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed, cudaStream_t st);
+void sample_cbd(const Context &c, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed, cudaStream_t st);
+void lift_signed(const Context &c, const int64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, cudaStream_t st);
 
 // ModUp of n_cts polynomials d (stride d_stride words) into up [n_cts][beta][LP][N]; x: [n_cts][L][N] scratch
 void modup_into(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_cts, uint32_t L, uint64_t *x,

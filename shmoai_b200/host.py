@@ -1,0 +1,281 @@
+"""Python binding of the C++ host library (include/shmoai_host.h) through ctypes.
+
+`Host` owns a context, the secret key and the evaluation keys; `Ct` owns one
+ciphertext batch (ordinary [count][2][L][N], or shared-a groups
+[count][members + 1][L][N]); `Bootstrapper` runs S2C-first (shared-a) batched
+bootstrapping.  By default the CUDA build (shmoai_b200/_build/libshmoai_host.so) is
+loaded; `Host(..., lib=path)` loads another build of the same library.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_DIR = os.path.dirname(os.path.abspath(__file__))
+PRODUCT_LIB = os.path.join(_DIR, "_build", "libshmoai_host.so")
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_libs: dict[str, ctypes.CDLL] = {}
+
+
+def build(jobs: int = 8) -> str:
+    """Build the CUDA library and the host library in place; returns the host library path."""
+    from ._lib import build as build_all
+
+    build_all(jobs)
+    return PRODUCT_LIB
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    path = os.path.abspath(path or PRODUCT_LIB)
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
+        raise RuntimeError(f"host library not built: {path} (run shmoai_b200.host.build())")
+    L = ctypes.CDLL(path)
+    u64p, dp, i32 = ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double), ctypes.c_int
+    pp = ctypes.POINTER(_P)
+    sig = {
+        "shm_host_last_error": (ctypes.c_char_p, []),
+        "shm_host_create": (i32, [pp, _U32, u64p, _U32, _U32, i32, _U32, ctypes.c_uint64]),
+        "shm_host_create_from_bits": (i32, [pp, _U32, ctypes.POINTER(ctypes.c_int), _U32, _U32, i32, _U32,
+                                            ctypes.c_uint64]),
+        "shm_host_primes": (i32, [_P, u64p]),
+        "shm_host_destroy": (None, [_P]),
+        "shm_host_context": (_P, [_P]),
+        "shm_host_synchronize": (i32, [_P]),
+        "shm_host_gen_relin_key": (i32, [_P]),
+        "shm_host_gen_galois_keys": (i32, [_P, ctypes.POINTER(_U32), _U32]),
+        "shm_host_gen_shared_keys": (i32, [_P, _U32, _U32, ctypes.POINTER(_U32), _U32]),
+        "shm_host_galois_elt": (_U32, [_P, i32]),
+        "shm_host_encrypt": (i32, [_P, dp, dp, _U32, _U32, _U32, ctypes.c_double, pp]),
+        "shm_host_decrypt": (i32, [_P, _P, dp, dp]),
+        "shm_ct_from_host": (i32, [_P, u64p, _U32, _U32, _U32, ctypes.c_double, i32, pp]),
+        "shm_ct_to_host": (i32, [_P, _P, u64p]),
+        "shm_ct_info": (i32, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(_U32), dp,
+                              ctypes.POINTER(i32)]),
+        "shm_ct_device_data": (_P, [_P]),
+        "shm_ct_destroy": (None, [_P]),
+        "shm_host_add": (i32, [_P, _P, _P, pp]),
+        "shm_host_sub": (i32, [_P, _P, _P, pp]),
+        "shm_host_multiply": (i32, [_P, _P, _P, pp]),
+        "shm_host_rescale": (i32, [_P, _P, pp]),
+        "shm_host_multiply_const": (i32, [_P, _P, ctypes.c_double, pp]),
+        "shm_host_rotate": (i32, [_P, _P, i32, pp]),
+        "shm_host_conjugate": (i32, [_P, _P, pp]),
+        "shm_host_multiply_i": (i32, [_P, _P, i32, pp]),
+        "shm_host_to_shared": (i32, [_P, _P, _U32, pp]),
+        "shm_host_from_shared": (i32, [_P, _P, pp]),
+        "shm_boot_create": (i32, [_P, ctypes.c_double, _U32, pp]),
+        "shm_boot_destroy": (None, [_P]),
+        "shm_boot_galois_elts": (i32, [_P, ctypes.POINTER(_U32), _U32, ctypes.POINTER(_U32)]),
+        "shm_boot_run": (i32, [_P, _P, _U32, pp]),
+        "shm_slot_transform_selfcheck": (ctypes.c_double, [_U32]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _libs[path] = L
+    return L
+
+
+class HostError(RuntimeError):
+    pass
+
+
+class Host:
+    def __init__(self, log_n: int, primes=None, n_special: int = 0, hamming_weight: int = 192, seed: int = 0x5EED,
+                 device: int = 0, lib: str | None = None, bits=None):
+        self.lib = load(lib)
+        h = _P()
+        if primes is None:
+            if bits is None:
+                raise ValueError("give primes or bits")
+            b = (ctypes.c_int * len(bits))(*bits)
+            self._check(self.lib.shm_host_create_from_bits(ctypes.byref(h), log_n, b, len(bits), n_special, device,
+                                                           hamming_weight, seed))
+            pr = np.zeros(len(bits), dtype=np.uint64)
+            self._check(self.lib.shm_host_primes(h, pr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        else:
+            pr = np.ascontiguousarray(primes, dtype=np.uint64)
+            self._check(self.lib.shm_host_create(ctypes.byref(h), log_n,
+                                                 pr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(pr),
+                                                 n_special, device, hamming_weight, seed))
+        self._h = h
+        self.primes = [int(p) for p in pr]
+        self.log_n, self.n = log_n, 1 << log_n
+        self.nq, self.np = len(pr) - n_special, n_special
+
+    def _check(self, rc):
+        if rc != 0:
+            raise HostError(f"{rc}: {self.lib.shm_host_last_error().decode()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.shm_host_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- keys
+    def gen_relin_key(self):
+        self._check(self.lib.shm_host_gen_relin_key(self._h))
+
+    def gen_galois_keys(self, elts):
+        e = (_U32 * len(elts))(*elts)
+        self._check(self.lib.shm_host_gen_galois_keys(self._h, e, len(elts)))
+
+    def gen_shared_keys(self, members: int, elts, hamming_weight: int = 192):
+        e = (_U32 * len(elts))(*elts)
+        self._check(self.lib.shm_host_gen_shared_keys(self._h, members, hamming_weight, e, len(elts)))
+
+    def galois_elt(self, step: int) -> int:
+        return int(self.lib.shm_host_galois_elt(self._h, step))
+
+    def synchronize(self):
+        self._check(self.lib.shm_host_synchronize(self._h))
+
+    # ---- ciphertexts
+    def _out(self, fn, *args) -> "Ct":
+        o = _P()
+        self._check(fn(self._h, *args, ctypes.byref(o)))
+        return Ct(self, o)
+
+    def encrypt(self, z, scale: float, L: int) -> "Ct":
+        z = np.atleast_2d(np.asarray(z, dtype=np.complex128))
+        re = np.ascontiguousarray(z.real)
+        im = np.ascontiguousarray(z.imag)
+        dp = ctypes.POINTER(ctypes.c_double)
+        return self._out(self.lib.shm_host_encrypt, re.ctypes.data_as(dp), im.ctypes.data_as(dp), z.shape[0],
+                         z.shape[1], L, scale)
+
+    def decrypt(self, ct: "Ct") -> np.ndarray:
+        rows = ct.count * ct.members
+        re = np.zeros((rows, self.n // 2))
+        im = np.zeros((rows, self.n // 2))
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._check(self.lib.shm_host_decrypt(self._h, ct._c, re.ctypes.data_as(dp), im.ctypes.data_as(dp)))
+        return re + 1j * im
+
+    def ct_from_host(self, data: np.ndarray, scale: float, shared: bool = False) -> "Ct":
+        d = np.ascontiguousarray(data, dtype=np.uint64)
+        count, size, L, _ = d.shape
+        return self._out(self.lib.shm_ct_from_host, d.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), count, size,
+                         L, scale, 1 if shared else 0)
+
+    def ct_from_ptr(self, ptr: int, count: int, size: int, L: int, scale: float, shared: bool = False) -> "Ct":
+        """Copy a batch from host memory at address `ptr` (e.g. a pinned buffer) to the device."""
+        return self._out(self.lib.shm_ct_from_host, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_uint64)), count, size,
+                         L, scale, 1 if shared else 0)
+
+    def add(self, a, b):
+        return self._out(self.lib.shm_host_add, a._c, b._c)
+
+    def sub(self, a, b):
+        return self._out(self.lib.shm_host_sub, a._c, b._c)
+
+    def multiply(self, a, b):
+        return self._out(self.lib.shm_host_multiply, a._c, b._c)
+
+    def rescale(self, a):
+        return self._out(self.lib.shm_host_rescale, a._c)
+
+    def multiply_const(self, a, v: float):
+        return self._out(self.lib.shm_host_multiply_const, a._c, v)
+
+    def rotate(self, a, step: int):
+        return self._out(self.lib.shm_host_rotate, a._c, step)
+
+    def conjugate(self, a):
+        return self._out(self.lib.shm_host_conjugate, a._c)
+
+    def multiply_i(self, a, sign: int = 1):
+        return self._out(self.lib.shm_host_multiply_i, a._c, sign)
+
+    def to_shared(self, a, members: int):
+        return self._out(self.lib.shm_host_to_shared, a._c, members)
+
+    def from_shared(self, a):
+        return self._out(self.lib.shm_host_from_shared, a._c)
+
+
+class Ct:
+    def __init__(self, host: Host, handle):
+        self.host, self._c = host, handle
+        c, s, L, sh = _U32(), _U32(), _U32(), ctypes.c_int()
+        sc = ctypes.c_double()
+        host._check(host.lib.shm_ct_info(handle, ctypes.byref(c), ctypes.byref(s), ctypes.byref(L), ctypes.byref(sc),
+                                         ctypes.byref(sh)))
+        self.count, self.size, self.level, self.scale, self.shared = c.value, s.value, L.value, sc.value, bool(sh.value)
+
+    @property
+    def members(self) -> int:
+        return self.size - 1 if self.shared else 1
+
+    def to_host(self) -> np.ndarray:
+        out = np.empty((self.count, self.size, self.level, self.host.n), dtype=np.uint64)
+        self.host._check(self.host.lib.shm_ct_to_host(self.host._h, self._c,
+                                                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out
+
+    def to_ptr(self, ptr: int):
+        """Copy the batch to host memory at address `ptr` (count * size * L * N words)."""
+        self.host._check(self.host.lib.shm_ct_to_host(self.host._h, self._c,
+                                                      ctypes.cast(ptr, ctypes.POINTER(ctypes.c_uint64))))
+
+    def device_ptr(self) -> int:
+        return int(self.host.lib.shm_ct_device_data(self._c) or 0)
+
+    def close(self):
+        if getattr(self, "_c", None):
+            self.host.lib.shm_ct_destroy(self._c)
+            self._c = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Bootstrapper:
+    def __init__(self, host: Host, scale: float = 2.0 ** 46, input_level: int = 4):
+        self.host = host
+        b = _P()
+        host._check(host.lib.shm_boot_create(host._h, scale, input_level, ctypes.byref(b)))
+        self._b = b
+        self.scale, self.input_level = scale, input_level
+
+    def galois_elts(self) -> list[int]:
+        n = _U32()
+        buf = (_U32 * 4096)()
+        self.host._check(self.host.lib.shm_boot_galois_elts(self._b, buf, 4096, ctypes.byref(n)))
+        return [int(buf[i]) for i in range(n.value)]
+
+    def run(self, ct: Ct, members: int = 0) -> Ct:
+        o = _P()
+        self.host._check(self.host.lib.shm_boot_run(self._b, ct._c, members, ctypes.byref(o)))
+        return Ct(self.host, o)
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self.host.lib.shm_boot_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def slot_transform_selfcheck(log_slots: int, lib: str | None = None) -> float:
+    return float(load(lib).shm_slot_transform_selfcheck(log_slots))

@@ -1,0 +1,534 @@
+// S2C-first CKKS bootstrapping over ciphertext batches, ordinary and shared-a
+// (the reference's BatchBootstrapper::bootstrap_ordinary_s2c_first and
+// bootstrap_shared_a_s2c_first, src/include/source/bootstrapping/BatchBootstrap.cuh:674-819).
+//
+// Pipeline (input at `input_level` primes):
+//   [shared-a: FmtSwitch forward of groups of n]
+//   SlotToCoeff: 3 BSGS layers (input_level -> input_level - 3 primes), factor F on the last
+//   ModRaise: 1 -> nq primes, scale := q0
+//   CoeffToSlot: 3 BSGS layers (nq -> nq - 2 primes, the last NOT rescaled), 1/(2K) folded
+//     into the first
+//   conjugation split re = w + conj w, im = -i (w - conj w), run before the last rescale
+//     so the key switch's low-frequency noise is divided by that prime
+//   [shared-a: FmtSwitch backward of re and im]
+//   rescale, EvalMod on re and im as one batch: Chebyshev interpolant of
+//     cos(2 pi (K x - 1/4) / 2^r), degree 47, K = 25, r = 3 double angles -> sin(2 pi t);
+//     the constant c_fin = q0 / (2 pi Delta F) and the scale Delta are reached through
+//     exact scale targets, not an extra level
+//   recombination re + i im (i = the monomial X^(N/2), free).
+//
+// Slot transforms: the slot-to-coefficient map V (V_jk = omega_j^k, slot order 5^j)
+// factors, after a bit reversal that both directions absorb, into log2(n) radix-2
+// butterfly stages (the special FFT of thirdparty/phantom-fhe/src/fft.cu:358-439);
+// stages are grouped 5/5/5 for n = 2^15 (the reference's logn/3 split,
+// BatchBootstrap.cuh:84-88) into three sparse matrices of <= 63 diagonals, applied by
+// baby-step giant-step with pre-rotated diagonals: one hoisted ModUp for all baby steps,
+// one multiply-plain-accumulate launch per giant step, one rescale per layer.  The
+// diagonal plaintexts are encoded once and stay resident on the device (the reference
+// re-encodes them on every call, SharedACoeffToSlot.cu:50-57).
+//
+// EvalMod uses a Chebyshev interpolant (degree 47) with three double angles where the
+// reference uses an NTL Remez fit of degree 59 with two (ModularReducer.cu:40-54); with
+// two double angles the interpolant leaves ~2e-7 error, too much for the 2e-5 target
+// after the x512 amplitude correction, with three ~1e-13.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <set>
+
+#include "internal.hpp"
+
+namespace shmoai {
+
+namespace {
+
+using Vec = std::vector<cplx>;
+using Diags = std::map<uint32_t, Vec>;  // offset mod n -> diagonal: (D x)_a = sum_d D_d[a] x_{a+d}
+
+void accumulate(Diags &D, uint32_t k, const Vec &v) {
+    auto it = D.find(k);
+    if (it == D.end()) {
+        D.emplace(k, v);
+        return;
+    }
+    for (size_t i = 0; i < v.size(); i++) it->second[i] += v[i];
+}
+
+// out[i] = v[(i - shift) mod n]
+Vec roll(const Vec &v, int64_t shift) {
+    const int64_t n = (int64_t)v.size();
+    const int64_t s = ((shift % n) + n) % n;
+    Vec out(v.size());
+    for (int64_t i = 0; i < n; i++) out[(i + s) % n] = v[i];
+    return out;
+}
+
+Vec apply_diags(const Diags &D, const Vec &x) {
+    Vec out(x.size(), cplx(0, 0));
+    const size_t n = x.size();
+    for (auto &kv : D)
+        for (size_t a = 0; a < n; a++) out[a] += kv.second[a] * x[(a + kv.first) % n];
+    return out;
+}
+
+struct Twiddles {
+    uint32_t n, M;
+    std::vector<uint64_t> rot;  // 5^j mod 4n
+    std::vector<cplx> ksi;      // exp(2 pi i k / 4n)
+    explicit Twiddles(uint32_t n_) : n(n_), M(4 * n_), rot(n_), ksi(4 * n_) {
+        uint64_t e = 1;
+        for (uint32_t j = 0; j < n; j++) {
+            rot[j] = e;
+            e = (e * 5) % M;
+        }
+        for (uint32_t k = 0; k < M; k++) {
+            const double ang = 2.0 * M_PI * (double)k / (double)M;
+            ksi[k] = cplx(std::cos(ang), std::sin(ang));
+        }
+    }
+    // twiddle of the butterfly with half-width h at position a (lower partner's value)
+    cplx t(uint32_t h, uint32_t a) const {
+        const uint32_t ln = 2 * h, j = a % ln, jj = j < h ? j : j - h;
+        return ksi[(rot[jj] % (4 * (uint64_t)ln)) * (M / (4 * ln))];
+    }
+};
+
+// butterfly stages S_1 .. S_log2(n) with V R^-1 = S_log2(n) ... S_1
+std::vector<Diags> special_fft_stages(const Twiddles &tw) {
+    const uint32_t n = tw.n;
+    std::vector<Diags> stages;
+    for (uint32_t ln = 2; ln <= n; ln *= 2) {
+        const uint32_t h = ln / 2;
+        Vec d0(n), dp(n), dm(n);
+        for (uint32_t a = 0; a < n; a++) {
+            const bool lower = (a % ln) < h;
+            const cplx t = tw.t(h, a);
+            d0[a] = lower ? cplx(1, 0) : -t;
+            dp[a] = lower ? t : cplx(0, 0);
+            dm[a] = lower ? cplx(0, 0) : cplx(1, 0);
+        }
+        Diags D;
+        accumulate(D, 0, d0);
+        accumulate(D, h % n, dp);
+        accumulate(D, (n - h) % n, dm);
+        stages.push_back(std::move(D));
+    }
+    return stages;
+}
+
+// inverse of the stage with half-width h: x_a = (y_a + y_{a+h}) / 2, x_{a+h} = (y_a - y_{a+h}) / (2 t_a)
+Diags inverse_stage(const Twiddles &tw, uint32_t h) {
+    const uint32_t n = tw.n;
+    Vec d0(n), dp(n), dm(n);
+    for (uint32_t a = 0; a < n; a++) {
+        const bool lower = (a % (2 * h)) < h;
+        const cplx inv2t = 1.0 / (2.0 * tw.t(h, a));
+        d0[a] = lower ? cplx(0.5, 0) : -inv2t;
+        dp[a] = lower ? cplx(0.5, 0) : cplx(0, 0);
+        dm[a] = lower ? cplx(0, 0) : inv2t;
+    }
+    Diags D;
+    accumulate(D, 0, d0);
+    accumulate(D, h % n, dp);
+    accumulate(D, (n - h) % n, dm);
+    return D;
+}
+
+// diagonals of P Q (Q applied first): (PQ)_{d+e} += P_d * Rot_d(Q_e)
+Diags compose(const Diags &P, const Diags &Q, uint32_t n) {
+    Diags out;
+    for (auto &pd : P)
+        for (auto &qe : Q) {
+            const uint32_t k = (pd.first + qe.first) % n;
+            Vec v(n);
+            for (uint32_t a = 0; a < n; a++) v[a] = pd.second[a] * qe.second[(a + pd.first) % n];
+            accumulate(out, k, v);
+        }
+    for (auto it = out.begin(); it != out.end();) {
+        double mx = 0;
+        for (auto &z : it->second) mx = std::max(mx, std::abs(z));
+        it = mx > 0 ? std::next(it) : out.erase(it);
+    }
+    return out;
+}
+
+std::vector<uint32_t> layer_split(uint32_t logn) {
+    const uint32_t d1 = logn / 3, d2 = (logn - d1) / 2;
+    return {d1, d2, logn - d1 - d2};
+}
+
+// three grouped layers A, B, C with V R^-1 = C B A (A applied first)
+std::vector<Diags> s2c_layers(const Twiddles &tw) {
+    std::vector<Diags> st = special_fft_stages(tw);
+    const uint32_t logn = (uint32_t)st.size();
+    std::vector<Diags> out;
+    uint32_t i = 0;
+    for (uint32_t size : layer_split(logn)) {
+        Diags M = st[i];
+        for (uint32_t k = i + 1; k < i + size; k++) M = compose(st[k], M, tw.n);
+        out.push_back(std::move(M));
+        i += size;
+    }
+    return out;
+}
+
+// three grouped layers with (V R^-1)^-1 = A^-1 B^-1 C^-1 (C^-1 applied first)
+std::vector<Diags> c2s_layers(const Twiddles &tw) {
+    const uint32_t logn = (uint32_t)std::lround(std::log2((double)tw.n));
+    std::vector<Diags> inv;
+    for (uint32_t k = 0; k < logn; k++) inv.push_back(inverse_stage(tw, 1u << k));
+    std::vector<std::vector<uint32_t>> groups;
+    uint32_t i = 0;
+    for (uint32_t size : layer_split(logn)) {
+        std::vector<uint32_t> g;
+        for (uint32_t k = i; k < i + size; k++) g.push_back(k);
+        groups.push_back(g);
+        i += size;
+    }
+    std::vector<Diags> out;
+    for (auto g = groups.rbegin(); g != groups.rend(); ++g) {
+        Diags M = inv[g->back()];
+        for (auto k = g->rbegin() + 1; k != g->rend(); ++k) M = compose(inv[*k], M, tw.n);
+        out.push_back(std::move(M));
+    }
+    return out;
+}
+
+// Chebyshev interpolant of f(K x) on [-1, 1] at the deg + 1 Chebyshev nodes
+std::vector<double> cheb_interp(double (*f)(double, int), int r, double K, int deg) {
+    const int m = deg + 1;
+    std::vector<double> fx(m), c(m, 0.0);
+    for (int k = 0; k < m; k++) fx[k] = f(K * std::cos(M_PI * (k + 0.5) / m), r);
+    for (int j = 0; j < m; j++) {
+        double s = 0;
+        for (int k = 0; k < m; k++) s += fx[k] * std::cos(M_PI * j * (k + 0.5) / m);
+        c[j] = (j ? 2.0 : 1.0) * s / m;
+    }
+    return c;
+}
+
+double evalmod_target(double t, int r) { return std::cos(2.0 * M_PI * (t - 0.25) / std::ldexp(1.0, r)); }
+
+// p = q T_m + r for Chebyshev coefficients c (degree < 2m)
+void cheb_divide(const std::vector<double> &c, int m, std::vector<double> &q, std::vector<double> &r) {
+    const int d = (int)c.size() - 1;
+    q.assign(1, c[m]);
+    for (int j = 1; j <= d - m; j++) q.push_back(2.0 * c[m + j]);
+    r.assign(c.begin(), c.begin() + m);
+    for (int j = 1; j <= d - m; j++) r[m - j] -= c[m + j];
+}
+
+int bitlen(uint32_t d) { return d ? 32 - __builtin_clz(d) : 0; }
+
+int64_t floordiv(int64_t a, int64_t b) {
+    int64_t q = a / b;
+    if ((a % b != 0) && ((a < 0) != (b < 0))) q--;
+    return q;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ LinearTransform
+
+// sum_d D_d * Rot_d(x) at one level by baby-step giant-step: offsets t (in units of
+// the gcd b) split as t = g1 u + v; baby steps Rot_{v b}(x) share one hoisted ModUp,
+// diagonals are pre-rotated by -g1 u b, so each giant step is one rotation of
+// sum_v Rot_{-g1 u b}(D_t) * Rot_{v b}(x).
+class LinearTransform {
+   public:
+    LinearTransform(const Evaluator &ev, const Diags &diags, uint32_t level) : ev_(ev), level_(level) {
+        const Context &c = ev.context();
+        const int64_t n = c.n / 2;
+        int64_t b = 0;
+        for (auto &kv : diags) b = std::gcd(b, (int64_t)kv.first);
+        b_ = b ? b : 1;
+        const int64_t span = n / b_;
+        std::map<int64_t, const Vec *> ts;
+        for (auto &kv : diags) {
+            int64_t t = (int64_t)kv.first / b_;
+            if (t > span / 2) t -= span;
+            ts[t] = &kv.second;
+        }
+        g1_ = (int64_t)1 << (int)std::ceil(std::log2(std::sqrt((double)ts.size())));
+        pt_scale_ = (double)c.primes[level - 1];
+        for (auto &kv : ts) {
+            const int64_t u = floordiv(kv.first, g1_), v = kv.first - u * g1_;
+            Vec P = roll(*kv.second, g1_ * u * b_);
+            groups_[u].emplace_back(v, ev.encoder().encode(P, level, pt_scale_));
+        }
+        std::set<int64_t> bs;
+        for (auto &g : groups_)
+            for (auto &vp : g.second) bs.insert(vp.first);
+        baby_.assign(bs.begin(), bs.end());
+    }
+
+    std::set<int> steps() const {
+        std::set<int> s;
+        for (int64_t v : baby_)
+            if (v) s.insert((int)(v * b_));
+        for (auto &g : groups_)
+            if (g.first) s.insert((int)(g1_ * g.first * b_));
+        return s;
+    }
+
+    Ciphertext apply(const Ciphertext &x, bool rescale = true) const {
+        const Ciphertext *xp = &x;
+        Ciphertext dropped;
+        if (x.L != level_) {
+            dropped = ev_.mod_switch_to(x, level_);
+            xp = &dropped;
+        }
+        std::vector<int> bsteps;
+        for (int64_t v : baby_)
+            if (v) bsteps.push_back((int)(v * b_));
+        std::map<int, Ciphertext> rot = ev_.rotate_many(*xp, bsteps);
+        Ciphertext acc;
+        bool have = false;
+        for (auto &g : groups_) {
+            std::vector<const Ciphertext *> X;
+            std::vector<const Plaintext *> P;
+            for (auto &vp : g.second) {
+                X.push_back(vp.first ? &rot.at((int)(vp.first * b_)) : xp);
+                P.push_back(&vp.second);
+            }
+            Ciphertext inner = ev_.multiply_plain_accumulate(X, P);
+            inner.scale_ = xp->scale_ * pt_scale_;
+            if (g.first) inner = ev_.rotate_vector(inner, (int)(g1_ * g.first * b_));
+            if (!have) {
+                acc = std::move(inner);
+                have = true;
+            } else {
+                acc = ev_.add(acc, inner);
+            }
+        }
+        return rescale ? ev_.rescale_to_next(acc) : std::move(acc);
+    }
+
+   private:
+    const Evaluator &ev_;
+    uint32_t level_;
+    int64_t b_ = 1, g1_ = 1;
+    double pt_scale_ = 1;
+    std::map<int64_t, std::vector<std::pair<int64_t, Plaintext>>> groups_;  // u -> (v, pre-rotated diagonal)
+    std::vector<int64_t> baby_;
+};
+
+// ------------------------------------------------------------------ BatchBootstrapper
+
+BatchBootstrapper::BatchBootstrapper(Evaluator &ev, BootstrapParams p) : ev_(ev), p_(p) {}
+
+BatchBootstrapper::~BatchBootstrapper() {
+    for (auto *lt : s2c_) delete lt;
+    for (auto *lt : c2s_) delete lt;
+}
+
+void BatchBootstrapper::prepare() {
+    const Context &c = ev_.context();
+    if (p_.input_level < 4 || p_.input_level > c.nq) throw Error("input level must be in [4, nq]");
+    for (auto *lt : s2c_) delete lt;
+    for (auto *lt : c2s_) delete lt;
+    s2c_.clear();
+    c2s_.clear();
+    const Twiddles tw(c.n / 2);
+    std::vector<Diags> s = s2c_layers(tw);
+    for (auto &kv : s[2])
+        for (auto &z : kv.second) z *= p_.F;
+    for (uint32_t i = 0; i < 3; i++) s2c_.push_back(new LinearTransform(ev_, s[i], p_.input_level - i));
+    std::vector<Diags> ci = c2s_layers(tw);
+    for (auto &kv : ci[0])
+        for (auto &z : kv.second) z /= 2.0 * p_.K;
+    for (uint32_t i = 0; i < 3; i++) c2s_.push_back(new LinearTransform(ev_, ci[i], c.nq - i));
+    top_ = c.nq;
+    q0_ = (double)c.primes[0];
+    cheb_ = cheb_interp(evalmod_target, p_.double_angles, p_.K, p_.degree);
+    c_fin_ = q0_ / (2.0 * M_PI * p_.scale * p_.F);
+}
+
+std::vector<int> BatchBootstrapper::rotation_steps() const {
+    std::set<int> s;
+    for (auto *lt : s2c_) {
+        std::set<int> t = lt->steps();
+        s.insert(t.begin(), t.end());
+    }
+    for (auto *lt : c2s_) {
+        std::set<int> t = lt->steps();
+        s.insert(t.begin(), t.end());
+    }
+    return std::vector<int>(s.begin(), s.end());
+}
+
+std::vector<uint32_t> BatchBootstrapper::galois_elts() const {
+    std::set<uint32_t> e;
+    for (int st : rotation_steps()) e.insert(ev_.galois_elt(st));
+    e.insert(2 * ev_.context().n - 1);
+    return std::vector<uint32_t>(e.begin(), e.end());
+}
+
+SharedAKeys BatchBootstrapper::prepare_shared_keys(KeyGenerator &kg, uint32_t members, uint32_t hw) const {
+    return kg.shared_keys(members, galois_elts(), hw);
+}
+
+namespace {
+
+using Basis = std::map<int, Ciphertext>;
+
+// T_1 .. T_8 and T_16, T_32, ... by products 2 T_a T_b - T_{a-b}
+Basis cheb_basis(const Evaluator &ev, const Ciphertext &x, int deg) {
+    Basis T;
+    T.emplace(1, ev.adjust(x, x.L, x.scale_));
+    auto prod = [&](int a, int b) {
+        Ciphertext p = ev.multiply_int(ev.multiply(T.at(a), T.at(b)), 2);
+        if (a == b) return ev.add_const(p, -1.0);
+        return ev.sub(p, ev.adjust(T.at(a - b), p.L, p.scale_));
+    };
+    const int g = 8;
+    for (int k = 2; k <= g && k <= deg; k++) {
+        if (k % 2 == 0) {
+            T.emplace(k, prod(k / 2, k / 2));
+        } else {
+            const int a = 1 << (bitlen((uint32_t)k) - 1);
+            T.emplace(k, prod(a, k - a));
+        }
+    }
+    for (int m = 2 * g; m <= deg; m *= 2) T.emplace(m, prod(m / 2, m / 2));
+    return T;
+}
+
+bool feasible(const Basis &T, int ncoef, uint32_t lvl) {
+    const int d = ncoef - 1;
+    if (d < 8) {
+        for (int i = 1; i <= d; i++)
+            if (T.at(i).L < lvl + 1) return false;
+        return true;
+    }
+    const int m = 1 << (bitlen((uint32_t)d) - 1);
+    return T.at(m).L >= lvl + 1 && feasible(T, d - m + 1, lvl + 1) && feasible(T, m, lvl);
+}
+
+// sum_i c_i T_i, output at exactly scale S and lvl primes (baby-step giant-step)
+Ciphertext cheb_eval(const Evaluator &ev, const Basis &T, const std::vector<double> &c, double S, uint32_t lvl) {
+    const Context &ctx = ev.context();
+    const int d = (int)c.size() - 1;
+    if (d < 1) throw Error("Chebyshev piece of degree 0");
+    if (d < 8) {
+        const double q = (double)ctx.primes[lvl];
+        Ciphertext acc;
+        for (int i = 1; i <= d; i++) {
+            Ciphertext Ti = ev.mod_switch_to(T.at(i), lvl + 1);
+            Ciphertext term = ev.multiply_const_unscaled(Ti, c[i], S * q / Ti.scale_);
+            term.scale_ = S * q;
+            acc = i == 1 ? std::move(term) : ev.add(acc, term);
+        }
+        acc = ev.add_const(acc, c[0]);
+        Ciphertext out = ev.rescale_to_next(acc);
+        out.scale_ = S;
+        return out;
+    }
+    const int m = 1 << (bitlen((uint32_t)d) - 1);
+    std::vector<double> qc, rc;
+    cheb_divide(c, m, qc, rc);
+    Ciphertext Tm = ev.mod_switch_to(T.at(m), lvl + 1);
+    const double Sq = S * (double)ctx.primes[lvl] / Tm.scale_;
+    Ciphertext qct = cheb_eval(ev, T, qc, Sq, lvl + 1);
+    Ciphertext prod = ev.multiply(qct, Tm);
+    prod.scale_ = S;
+    return ev.add(prod, cheb_eval(ev, T, rc, S, lvl));
+}
+
+}  // namespace
+
+// x holds t / K; returns c_fin * sin(2 pi t) read at scale Delta.  Backward scale
+// targets: the i-th double angle squares at level lvl - i and drops prime lvl - 1 - i,
+// so s_in = sqrt(s_out * q); the last output scale is Delta * c_fin, which reads as the
+// value c_fin * y at scale Delta.
+Ciphertext BatchBootstrapper::evalmod(const Ciphertext &x) const {
+    const Context &c = ev_.context();
+    const int deg = (int)cheb_.size() - 1;
+    Basis T = cheb_basis(ev_, x, deg);
+    uint32_t lvl = x.L - 1;
+    while (!feasible(T, deg + 1, lvl)) {
+        if (lvl == 0) throw Error("not enough levels for EvalMod");
+        lvl--;
+    }
+    double s = p_.scale * c_fin_;
+    for (int i = p_.double_angles - 1; i >= 0; i--) s = std::sqrt(s * (double)c.primes[lvl - 1 - i]);
+    Ciphertext y = cheb_eval(ev_, T, cheb_, s, lvl);
+    for (int i = 0; i < p_.double_angles; i++) y = ev_.add_const(ev_.multiply_int(ev_.square(y), 2), -1.0);
+    y.scale_ /= c_fin_;
+    return y;
+}
+
+void BatchBootstrapper::slots_to_re_im(Ciphertext x, Ciphertext &re, Ciphertext &im) const {
+    if (s2c_.empty()) throw Error("call prepare() first");
+    if (x.L != p_.input_level) throw Error("bootstrap input must have input_level primes");
+    for (auto *lt : s2c_) x = lt->apply(x);
+    Ciphertext w = ev_.mod_raise(x, top_);
+    w.scale_ = q0_;
+    w = c2s_[0]->apply(w);
+    w = c2s_[1]->apply(w);
+    w = c2s_[2]->apply(w, false);
+    Ciphertext wc = ev_.complex_conjugate(w);
+    re = ev_.add(w, wc);
+    im = ev_.multiply_i(ev_.sub(w, wc), -1);
+}
+
+Ciphertext BatchBootstrapper::finish(const Ciphertext &re, const Ciphertext &im) const {
+    Ciphertext y = evalmod(ev_.rescale_to_next(ev_.concat(re, im)));
+    const uint32_t nb = re.count;
+    return ev_.add(ev_.slice(y, 0, nb), ev_.multiply_i(ev_.slice(y, nb, nb)));
+}
+
+Ciphertext BatchBootstrapper::bootstrap_ordinary_s2c_first(const Ciphertext &ct) const {
+    if (ct.shared || ct.size != 2) throw Error("bootstrap takes ordinary size-2 ciphertexts");
+    Ciphertext re, im;
+    slots_to_re_im(ev_.adjust(ct, ct.L, ct.scale_), re, im);
+    return finish(re, im);
+}
+
+Ciphertext BatchBootstrapper::bootstrap_shared_a_s2c_first(const Ciphertext &ct, uint32_t members) const {
+    Ciphertext re, im;
+    slots_to_re_im(ev_.to_shared(ct, members), re, im);
+    return finish(ev_.from_shared(re), ev_.from_shared(im));
+}
+
+double slot_transform_selfcheck(uint32_t log_slots) {
+    const uint32_t n = 1u << log_slots, N = 2 * n, M = 2 * N;
+    const Twiddles tw(n);
+    Vec w(n);
+    for (uint32_t i = 0; i < n; i++) {
+        const double a = (double)(detail::mix64(7, 2 * i) >> 11) * 0x1.0p-53 - 0.5;
+        const double b = (double)(detail::mix64(7, 2 * i + 1) >> 11) * 0x1.0p-53 - 0.5;
+        w[i] = cplx(a, b);
+    }
+    std::vector<uint64_t> ex(n);
+    uint64_t e = 1;
+    for (uint32_t j = 0; j < n; j++) {
+        ex[j] = e;
+        e = (e * 5) % M;
+    }
+    Vec Vw(n, cplx(0, 0));
+    double vmax = 0;
+    for (uint32_t j = 0; j < n; j++) {
+        for (uint32_t k = 0; k < n; k++) {
+            const double ang = 2.0 * M_PI * (double)((ex[j] * k) % M) / (double)M;
+            Vw[j] += w[k] * cplx(std::cos(ang), std::sin(ang));
+        }
+        vmax = std::max(vmax, std::abs(Vw[j]));
+    }
+    Vec y(n);
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t r = 0;
+        for (uint32_t b = 0; b < log_slots; b++) r |= ((i >> b) & 1u) << (log_slots - 1 - b);
+        y[i] = w[r];
+    }
+    const Vec wr = y;
+    for (auto &L : s2c_layers(tw)) y = apply_diags(L, y);
+    double err = 0;
+    for (uint32_t j = 0; j < n; j++) err = std::max(err, std::abs(y[j] - Vw[j]) / vmax);
+    Vec z = Vw;
+    for (auto &L : c2s_layers(tw)) z = apply_diags(L, z);
+    for (uint32_t j = 0; j < n; j++) err = std::max(err, std::abs(z[j] - wr[j]));
+    return err;
+}
+
+}  // namespace shmoai

@@ -1,0 +1,332 @@
+// extern "C" entry points of include/shmoai_host.h over the C++ host classes.
+#include <cstring>
+#include <memory>
+
+#include "../../include/shmoai_host.h"
+#include "internal.hpp"
+
+using namespace shmoai;
+
+struct shm_host {
+    std::unique_ptr<Context> ctx;
+    std::unique_ptr<Encoder> enc;
+    std::unique_ptr<KeyGenerator> kg;
+    std::unique_ptr<Evaluator> ev;
+    DeviceBuffer relin;
+    std::map<uint32_t, DeviceBuffer> galois;
+    std::map<uint32_t, SharedAKeys> shared;  // group size -> keys
+
+    void use_shared(uint32_t members) {
+        auto it = shared.find(members);
+        if (it == shared.end()) throw Error("no shared-a keys for groups of " + std::to_string(members));
+        ev->shared_keys = &it->second;
+    }
+};
+
+struct shm_ct {
+    Ciphertext ct;
+};
+
+struct shm_boot {
+    shm_host *h;
+    std::unique_ptr<BatchBootstrapper> b;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <typename F>
+int guard(F &&f) {
+    try {
+        f();
+        return SHM_OK;
+    } catch (const Error &e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        g_err = "host out of memory";
+        return SHM_ENOMEM;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return SHM_EINTERNAL;
+    } catch (...) {
+        g_err = "unknown error";
+        return SHM_EINTERNAL;
+    }
+}
+
+shm_host &H(shm_host *h) {
+    if (!h || !h->ctx) throw Error("null host handle");
+    return *h;
+}
+
+const Ciphertext &C(const shm_ct *c) {
+    if (!c) throw Error("null ciphertext handle");
+    return c->ct;
+}
+
+void put(shm_ct **out, Ciphertext &&ct) {
+    if (!out) throw Error("null output handle");
+    *out = new shm_ct{std::move(ct)};
+}
+
+void prepare_for(shm_host &h, const Ciphertext &a) {
+    if (a.shared) h.use_shared(a.members());
+}
+
+void finish_create(shm_host *h, uint32_t hw, uint64_t seed) {
+    h->enc.reset(new Encoder(*h->ctx));
+    h->kg.reset(new KeyGenerator(*h->ctx, hw, seed));
+    h->ev.reset(new Evaluator(*h->ctx, *h->enc));
+    h->ev->relin_key = &h->relin;
+    h->ev->galois_keys = &h->galois;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *shm_host_last_error(void) { return g_err.c_str(); }
+
+int shm_host_create(shm_host **out, uint32_t log_n, const uint64_t *primes, uint32_t n_primes, uint32_t n_special,
+                    int device, uint32_t hamming_weight, uint64_t seed) {
+    return guard([&] {
+        if (!out || !primes) throw Error("null argument");
+        std::unique_ptr<shm_host> h(new shm_host);
+        h->ctx.reset(new Context(log_n, std::vector<uint64_t>(primes, primes + n_primes), n_special, device));
+        finish_create(h.get(), hamming_weight, seed);
+        *out = h.release();
+    });
+}
+
+int shm_host_create_from_bits(shm_host **out, uint32_t log_n, const int *bits, uint32_t n_primes,
+                              uint32_t n_special, int device, uint32_t hamming_weight, uint64_t seed) {
+    return guard([&] {
+        if (!out || !bits) throw Error("null argument");
+        std::unique_ptr<shm_host> h(new shm_host);
+        h->ctx.reset(new Context(log_n, std::vector<int>(bits, bits + n_primes), n_special, device));
+        finish_create(h.get(), hamming_weight, seed);
+        *out = h.release();
+    });
+}
+
+void shm_host_destroy(shm_host *h) {
+    if (!h) return;
+    // keys and buffers are returned to the context's pool before the context goes
+    h->ev.reset();
+    h->kg.reset();
+    h->shared.clear();
+    h->galois.clear();
+    h->relin = DeviceBuffer();
+    h->enc.reset();
+    h->ctx.reset();
+    delete h;
+}
+
+const shm_context *shm_host_context(const shm_host *h) { return h && h->ctx ? h->ctx->handle() : nullptr; }
+
+int shm_host_primes(const shm_host *h, uint64_t *out) {
+    return guard([&] {
+        if (!h || !h->ctx || !out) throw Error("null argument");
+        std::copy(h->ctx->primes.begin(), h->ctx->primes.end(), out);
+    });
+}
+
+int shm_host_synchronize(shm_host *h) {
+    return guard([&] { H(h).ctx->synchronize(); });
+}
+
+int shm_host_gen_relin_key(shm_host *h) {
+    return guard([&] { H(h).relin = H(h).kg->relin_key(); });
+}
+
+int shm_host_gen_galois_keys(shm_host *h, const uint32_t *elts, uint32_t n_elts) {
+    return guard([&] {
+        auto &hh = H(h);
+        for (uint32_t i = 0; i < n_elts; i++)
+            if (!hh.galois.count(elts[i])) hh.galois.emplace(elts[i], hh.kg->galois_key(elts[i]));
+    });
+}
+
+int shm_host_gen_shared_keys(shm_host *h, uint32_t members, uint32_t hamming_weight, const uint32_t *elts,
+                             uint32_t n_elts) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!members) throw Error("group size must be positive");
+        hh.ev->shared_keys = nullptr;
+        hh.shared.erase(members);
+        hh.shared.emplace(members, hh.kg->shared_keys(members, std::vector<uint32_t>(elts, elts + n_elts),
+                                                      hamming_weight));
+    });
+}
+
+uint32_t shm_host_galois_elt(const shm_host *h, int step) {
+    return h && h->ev ? h->ev->galois_elt(step) : 0;
+}
+
+int shm_host_encrypt(shm_host *h, const double *re, const double *im, uint32_t count, uint32_t n_values, uint32_t L,
+                     double scale, shm_ct **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        std::vector<std::vector<cplx>> z(count, std::vector<cplx>(n_values));
+        for (uint32_t i = 0; i < count; i++)
+            for (uint32_t j = 0; j < n_values; j++)
+                z[i][j] = cplx(re[(size_t)i * n_values + j], im ? im[(size_t)i * n_values + j] : 0.0);
+        put(out, hh.kg->encrypt(z, scale, L));
+    });
+}
+
+int shm_host_decrypt(shm_host *h, const shm_ct *ct, double *re, double *im) {
+    return guard([&] {
+        auto &hh = H(h);
+        // shared-a groups decrypt with the auxiliary secrets of the last shm_host_gen_shared_keys
+        std::vector<std::vector<cplx>> z = hh.kg->decrypt(C(ct));
+        const size_t slots = hh.ctx->n / 2;
+        for (size_t r = 0; r < z.size(); r++)
+            for (size_t j = 0; j < slots; j++) {
+                re[r * slots + j] = z[r][j].real();
+                if (im) im[r * slots + j] = z[r][j].imag();
+            }
+    });
+}
+
+int shm_ct_from_host(shm_host *h, const uint64_t *data, uint32_t count, uint32_t size, uint32_t L, double scale,
+                     int shared, shm_ct **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!count || !size || !L) throw Error("empty ciphertext batch");
+        Ciphertext c;
+        const size_t words = (size_t)count * size * L * hh.ctx->n;
+        c.data = DeviceBuffer(*hh.ctx, words);
+        c.count = count;
+        c.size = size;
+        c.L = L;
+        c.scale_ = scale;
+        c.shared = shared != 0;
+        hh.ctx->check(shm_memcpy(hh.ctx->handle(), c.data.data(), data, words * 8, SHM_COPY_H2D, hh.ctx->stream()));
+        put(out, std::move(c));
+    });
+}
+
+int shm_ct_to_host(shm_host *h, const shm_ct *ct, uint64_t *data) {
+    return guard([&] {
+        auto &hh = H(h);
+        const Ciphertext &c = C(ct);
+        hh.ctx->check(shm_memcpy(hh.ctx->handle(), data, c.data.data(), c.polys() * c.L * hh.ctx->n * 8,
+                                 SHM_COPY_D2H, hh.ctx->stream()));
+    });
+}
+
+int shm_ct_info(const shm_ct *ct, uint32_t *count, uint32_t *size, uint32_t *L, double *scale, int *shared) {
+    return guard([&] {
+        const Ciphertext &c = C(ct);
+        if (count) *count = c.count;
+        if (size) *size = c.size;
+        if (L) *L = c.L;
+        if (scale) *scale = c.scale_;
+        if (shared) *shared = c.shared ? 1 : 0;
+    });
+}
+
+const uint64_t *shm_ct_device_data(const shm_ct *ct) { return ct ? ct->ct.data.data() : nullptr; }
+
+void shm_ct_destroy(shm_ct *ct) { delete ct; }
+
+int shm_host_add(shm_host *h, const shm_ct *a, const shm_ct *b, shm_ct **out) {
+    return guard([&] { put(out, H(h).ev->add(C(a), C(b))); });
+}
+
+int shm_host_sub(shm_host *h, const shm_ct *a, const shm_ct *b, shm_ct **out) {
+    return guard([&] { put(out, H(h).ev->sub(C(a), C(b))); });
+}
+
+int shm_host_multiply(shm_host *h, const shm_ct *a, const shm_ct *b, shm_ct **out) {
+    return guard([&] { put(out, H(h).ev->multiply(C(a), C(b), true)); });
+}
+
+int shm_host_rescale(shm_host *h, const shm_ct *a, shm_ct **out) {
+    return guard([&] { put(out, H(h).ev->rescale_to_next(C(a))); });
+}
+
+int shm_host_multiply_const(shm_host *h, const shm_ct *a, double value, shm_ct **out) {
+    return guard([&] { put(out, H(h).ev->multiply_const(C(a), value)); });
+}
+
+int shm_host_rotate(shm_host *h, const shm_ct *a, int step, shm_ct **out) {
+    return guard([&] {
+        prepare_for(H(h), C(a));
+        put(out, H(h).ev->rotate_vector(C(a), step));
+    });
+}
+
+int shm_host_conjugate(shm_host *h, const shm_ct *a, shm_ct **out) {
+    return guard([&] {
+        prepare_for(H(h), C(a));
+        put(out, H(h).ev->complex_conjugate(C(a)));
+    });
+}
+
+int shm_host_multiply_i(shm_host *h, const shm_ct *a, int sign, shm_ct **out) {
+    return guard([&] { put(out, H(h).ev->multiply_i(C(a), sign)); });
+}
+
+int shm_host_to_shared(shm_host *h, const shm_ct *a, uint32_t members, shm_ct **out) {
+    return guard([&] {
+        H(h).use_shared(members);
+        put(out, H(h).ev->to_shared(C(a), members));
+    });
+}
+
+int shm_host_from_shared(shm_host *h, const shm_ct *a, shm_ct **out) {
+    return guard([&] {
+        prepare_for(H(h), C(a));
+        put(out, H(h).ev->from_shared(C(a)));
+    });
+}
+
+int shm_boot_create(shm_host *h, double scale, uint32_t input_level, shm_boot **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!out) throw Error("null output handle");
+        BootstrapParams p;
+        p.scale = scale;
+        p.input_level = input_level;
+        std::unique_ptr<shm_boot> b(new shm_boot{h, std::unique_ptr<BatchBootstrapper>(new BatchBootstrapper(*hh.ev, p))});
+        b->b->prepare();
+        *out = b.release();
+    });
+}
+
+void shm_boot_destroy(shm_boot *b) { delete b; }
+
+int shm_boot_galois_elts(const shm_boot *b, uint32_t *out, uint32_t cap, uint32_t *n_out) {
+    return guard([&] {
+        if (!b) throw Error("null bootstrapper");
+        std::vector<uint32_t> e = b->b->galois_elts();
+        if (n_out) *n_out = (uint32_t)e.size();
+        for (size_t i = 0; i < e.size() && i < cap; i++) out[i] = e[i];
+    });
+}
+
+int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out) {
+    return guard([&] {
+        if (!b) throw Error("null bootstrapper");
+        if (members) {
+            b->h->use_shared(members);
+            put(out, b->b->bootstrap_shared_a_s2c_first(C(in), members));
+        } else {
+            put(out, b->b->bootstrap_ordinary_s2c_first(C(in)));
+        }
+    });
+}
+
+double shm_slot_transform_selfcheck(uint32_t log_slots) {
+    try {
+        return slot_transform_selfcheck(log_slots);
+    } catch (...) {
+        return -1.0;
+    }
+}
+
+}  // extern "C"

@@ -165,18 +165,16 @@ def test_errors_are_reported_not_thrown():
 def test_hoisted_rotations_match_oracle():
     """One ModUp, several Galois elements: equal to the oracle's hoisted restatement
     bit for bit, and decrypting like the plain rotation (same message, tiny noise)."""
-    from shmoai_b200.backend import GpuBackend
     from shmoai_b200.ckks import CKKSContext, to_device, to_host
 
     g = GoldenSet("tiny")
     ctx = CKKSContext(g.log_n, primes=g.primes, n_special=g.np)
-    be = GpuBackend(ctx)
     o = O.Oracle(g.log_n, g.primes, g.nq, g.np)
     elts = [5, 25, 2 * g.n - 1, pow(5, 7, 2 * g.n)]
     keys = [g.key(1000 + 10 * i) for i in range(len(elts))]
     for L in (2, 5, 6):
         X = np.stack([g.ct(900 + L * 10 + i, L) for i in range(3)])
-        outs = be.apply_galois_many(to_device(X), elts, [to_device(k) for k in keys])
+        outs = ctx.apply_galois_hoisted(to_device(X), elts, [to_device(k) for k in keys])
         for i in range(3):
             want = o.apply_galois_hoisted(np.ascontiguousarray(X[i]), elts, keys)
             for e in range(len(elts)):

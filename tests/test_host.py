@@ -1,0 +1,189 @@
+"""The C++ host library (include/shmoai/host.hpp through include/shmoai_host.h):
+key generation, encryption, the batched evaluator, FmtSwitch / Sh-Rot on shared-a
+groups and S2C-first (shared-a) batched bootstrapping.
+
+CPU: the library's sources built against the oracle's implementation of the C ABI
+(oracle/_build/libshmoai_host_oracle.so) run the whole pipeline at N = 2^12; results
+are judged by decryption, the way the reference's own tests judge them (mean |err|
+over slots, README 1.33e-5 after bootstrapping; the shared-a stage probes decrypt with
+the auxiliary secrets, test_shared_a.cuh:33-248, 1499-1510).
+GPU: the same sources on the CUDA library give bit-identical keys, ciphertexts and
+bootstrapping outputs (the samplers are counter-based), and the reference parameter
+set (N = 2^16) meets the 2e-5 target through the host library.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from shmoai_b200.host import Bootstrapper, Host, HostError, slot_transform_selfcheck
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_HOST = os.path.join(ROOT, "oracle", "_build", "libshmoai_host_oracle.so")
+SMALL_BITS = [51] + [46] * 6 + [51] * 13 + [51] * 5  # N = 2^12, nq = 20, np = 5 (dnum 4)
+REF_BITS = [51] + [46] * 20 + [51] * 14 + [51] * 5  # test_shared_a.cuh:1208-1250
+DELTA = 2.0 ** 46
+
+
+def _small_primes():
+    return O.gen_primes(12, SMALL_BITS)
+
+
+def _z(rng, count, n):
+    return rng.uniform(-1, 1, (count, n)) + 1j * rng.uniform(-1, 1, (count, n))
+
+
+@pytest.fixture(scope="module")
+def small():
+    h = Host(12, _small_primes(), 5, hamming_weight=64, seed=11, lib=ORACLE_HOST)
+    h.gen_relin_key()
+    bs = Bootstrapper(h, DELTA, 4)
+    elts = bs.galois_elts()
+    h.gen_galois_keys(elts)
+    h.gen_shared_keys(2, elts, hamming_weight=64)
+    return h, bs
+
+
+@pytest.mark.parametrize("log_slots", [6, 9, 12])
+def test_slot_transform_factorisation(log_slots):
+    assert 0 <= slot_transform_selfcheck(log_slots, ORACLE_HOST) < 1e-9
+
+
+def test_encrypt_decrypt_and_basic_ops(small):
+    h, _ = small
+    rng = np.random.default_rng(1)
+    n = h.n // 2
+    z, w = _z(rng, 2, n), _z(rng, 2, n)
+    a, b = h.encrypt(z, 2.0 ** 40, 6), h.encrypt(w, 2.0 ** 40, 6)
+    assert (a.count, a.size, a.level, a.scale, a.shared) == (2, 2, 6, 2.0 ** 40, False)
+    assert np.abs(h.decrypt(a) - z).max() < 1e-8
+    assert np.abs(h.decrypt(h.add(a, b)) - (z + w)).max() < 1e-8
+    assert np.abs(h.decrypt(h.sub(a, b)) - (z - w)).max() < 1e-8
+    m = h.multiply(a, b)
+    assert m.level == 5 and np.abs(h.decrypt(m) - z * w).max() < 1e-6
+    assert np.abs(h.decrypt(h.rotate(a, 1)) - np.roll(z, -1, axis=1)).max() < 1e-6
+    assert np.abs(h.decrypt(h.conjugate(a)) - np.conj(z)).max() < 1e-6
+    assert np.abs(h.decrypt(h.multiply_i(a, -1)) + 1j * z).max() < 1e-8
+    c = h.multiply_const(a, 0.75)
+    assert c.level == 5 and c.scale == a.scale and np.abs(h.decrypt(c) - 0.75 * z).max() < 1e-6
+
+
+def test_errors_are_reported(small):
+    h, bs = small
+    rng = np.random.default_rng(2)
+    a = h.encrypt(_z(rng, 1, 8), 2.0 ** 40, 5)
+    b = h.encrypt(_z(rng, 1, 8), 2.0 ** 30, 5)
+    with pytest.raises(HostError, match="scale mismatch"):
+        h.add(a, b)
+    missing = next(s for s in range(1, h.n // 2) if h.galois_elt(s) not in bs.galois_elts())
+    with pytest.raises(HostError, match="Galois key"):
+        h.rotate(a, missing)
+    with pytest.raises(HostError, match="no shared-a keys for groups of 3"):
+        h.to_shared(a, 3)
+    with pytest.raises(HostError):
+        h.encrypt(_z(rng, 1, 8), 2.0 ** 40, 99)
+
+
+def test_format_switch_round_trip_and_sh_rot(small):
+    h, bs = small
+    rng = np.random.default_rng(3)
+    n = h.n // 2
+    z = _z(rng, 4, n)
+    ct = h.encrypt(z, 2.0 ** 40, 4)
+    sh = h.to_shared(ct, 2)
+    assert (sh.count, sh.size, sh.level, sh.shared) == (2, 3, 4, True)
+    assert np.abs(h.decrypt(sh) - z).max() < 1e-6  # members decrypt with s'_i
+    assert np.abs(h.decrypt(h.from_shared(sh)) - z).max() < 1e-6
+    step = next(s for s in range(1, n) if h.galois_elt(s) in bs.galois_elts())
+    r = h.rotate(sh, step)
+    assert r.shared and np.abs(h.decrypt(r) - np.roll(z, -step, axis=1)).max() < 1e-6
+    assert np.abs(h.decrypt(h.conjugate(sh)) - np.conj(z)).max() < 1e-6
+    assert np.abs(h.decrypt(h.multiply_i(h.add(sh, sh))) - 2j * z).max() < 1e-6
+
+
+def test_bootstrap_ordinary_on_oracle(small):
+    h, bs = small
+    rng = np.random.default_rng(4)
+    z = _z(rng, 2, h.n // 2)
+    out = bs.run(h.encrypt(z, DELTA, 4))
+    err = np.abs(h.decrypt(out) - z)
+    assert out.level == 20 - 3 - 9 and abs(out.scale - DELTA) < 1e-6 * DELTA
+    assert err.mean() < 2e-5, err.mean()
+    assert err.max() < 1e-4, err.max()
+
+
+def test_bootstrap_shared_on_oracle(small):
+    h, bs = small
+    rng = np.random.default_rng(5)
+    z = _z(rng, 4, h.n // 2)
+    out = bs.run(h.encrypt(z, DELTA, 4), members=2)
+    err = np.abs(h.decrypt(out) - z)
+    assert out.count == 4 and not out.shared and out.level == 20 - 3 - 9
+    assert err.mean() < 2e-5, err.mean()
+    assert err.max() < 1e-4, err.max()
+    with pytest.raises(HostError, match="multiple of the group size"):
+        bs.run(h.encrypt(z[:3], DELTA, 4), members=2)
+    with pytest.raises(HostError, match="input_level"):
+        bs.run(h.encrypt(z[:2], DELTA, 5))
+
+
+# ------------------------------------------------------------------ GPU
+
+
+def _pair(seed):
+    primes = _small_primes()
+    return (Host(12, primes, 5, hamming_weight=64, seed=seed),
+            Host(12, primes, 5, hamming_weight=64, seed=seed, lib=ORACLE_HOST))
+
+
+@pytest.mark.gpu
+def test_host_cuda_matches_oracle_build_bit_for_bit():
+    """Same sources, same seed: identical keys and ciphertexts, identical results of the
+    evaluator and of both bootstrapping pipelines (one C++ pipeline, two C ABIs)."""
+    g, c = _pair(21)
+    rng = np.random.default_rng(6)
+    z = _z(rng, 4, g.n // 2)
+    cg, cc = g.encrypt(z, DELTA, 4), c.encrypt(z, DELTA, 4)
+    assert np.array_equal(cg.to_host(), cc.to_host()), "encryption (samplers, encoder, NTT)"
+    for h in (g, c):
+        h.gen_relin_key()
+    bg, bc = Bootstrapper(g, DELTA, 4), Bootstrapper(c, DELTA, 4)
+    elts = bg.galois_elts()
+    assert elts == bc.galois_elts()
+    for h in (g, c):
+        h.gen_galois_keys(elts)
+        h.gen_shared_keys(2, elts, hamming_weight=64)
+    a6g, a6c = g.encrypt(z[:2], 2.0 ** 40, 6), c.encrypt(z[:2], 2.0 ** 40, 6)
+    assert np.array_equal(g.multiply(a6g, a6g).to_host(), c.multiply(a6c, a6c).to_host())
+    og, oc = bg.run(cg), bc.run(cc)
+    assert (og.level, og.scale) == (oc.level, oc.scale)
+    assert np.array_equal(og.to_host(), oc.to_host()), "ordinary bootstrap"
+    sg, sc = bg.run(cg, members=2), bc.run(cc, members=2)
+    assert np.array_equal(sg.to_host(), sc.to_host()), "shared-a bootstrap"
+    err = np.abs(g.decrypt(sg) - z)
+    assert err.mean() < 2e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("members", [0, 4])
+def test_bootstrap_reference_parameters_on_b200(members):
+    """N = 2^16, Q = [51] + 20x[46] + 14x[51], P = 5x[51], Delta = 2^46, h = 192, input at
+    4 primes, full 2^15 slots uniform in [-1, 1]^2; ordinary and shared-a groups of 4."""
+    primes = O.gen_primes(16, REF_BITS)
+    h = Host(16, primes, 5, hamming_weight=192, seed=7)
+    h.gen_relin_key()
+    bs = Bootstrapper(h, DELTA, 4)
+    if members:
+        h.gen_shared_keys(members, bs.galois_elts())
+    else:
+        h.gen_galois_keys(bs.galois_elts())
+    rng = np.random.default_rng(11)
+    z = _z(rng, 8, h.n // 2)
+    out = bs.run(h.encrypt(z, DELTA, 4), members=members)
+    err = np.abs(h.decrypt(out) - z)
+    print(f"bootstrap N=2^16 members={members}: level {out.level}, mean |err| {err.mean():.3e}, "
+          f"max {err.max():.3e}")
+    assert out.level == 35 - 3 - 9
+    assert err.mean() < 2e-5, err.mean()
+    assert err.max() < 2e-4, err.max()
