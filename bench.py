@@ -329,6 +329,161 @@ def cpu_boot_estimate(shared: int = 0):
 
 
 # ---------------------------------------------------------------------------
+# serving workload: a Poisson stream of mixed jobs through the serving loop, against
+# the same jobs executed one after the other on the plain per-ciphertext path
+
+SERVE = dict(n_jobs=24, rate=3.0, seed=5, p_rot=0.65, p_mm=0.15, members=8, boot_batch=32, mm_n=192, mm_L=13,
+             rot_steps=(1, 2, 4, 8), rot_max=64, rot_levels=(4, 24), slots=3, budget_gb=32)
+
+
+def serve_jobs(rng):
+    """(kind, count, level, step or members, arrival time) of each job, Poisson arrivals."""
+    S, t, jobs = SERVE, 0.0, []
+    for _ in range(S["n_jobs"]):
+        t += rng.exponential(1.0 / S["rate"])
+        u = rng.random()
+        if u < S["p_rot"]:
+            lo, hi = S["rot_levels"]
+            jobs.append(("rot", int(rng.integers(1, S["rot_max"] + 1)), int(rng.integers(lo, hi + 1)),
+                         int(rng.choice(S["rot_steps"])), t))
+        elif u < S["p_rot"] + S["p_mm"]:
+            jobs.append(("mm", S["mm_n"], S["mm_L"], 0, t))
+        else:
+            jobs.append(("boot", S["boot_batch"], BOOT["input_level"], S["members"], t))
+    return jobs
+
+
+def run_serve(args, rank, world, dist):
+    import threading
+
+    import torch
+
+    import shmoai_b200
+    from shmoai_b200.host import Bootstrapper, Host, Server
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = shmoai_b200.lib()
+    S = SERVE
+    h = Host(BOOT["log_n"], bits=BOOT["bits"], n_special=BOOT["n_special"], hamming_weight=BOOT["h"],
+             seed=0x5EED + rank, device=dev)
+    h.gen_relin_key()
+    bs = Bootstrapper(h, BOOT["scale"], BOOT["input_level"])
+    h.gen_galois_keys(sorted(set(bs.galois_elts()) | {h.galois_elt(s) for s in S["rot_steps"]}))
+    h.gen_shared_keys(S["members"], bs.galois_elts(), hamming_weight=BOOT["h"])
+    jobs = serve_jobs(np.random.default_rng(S["seed"] + rank))
+    rng = np.random.default_rng(77 + rank)
+    w_scale = 2.0 ** 20
+    W = np.rint(rng.normal(0, 0.02, (S["mm_n"], S["mm_n"])) * w_scale).astype(np.int64)
+    inputs = []
+    for kind, count, L, _, _ in jobs:
+        z = rng.uniform(-1, 1, (count, h.n // 2)) + 1j * rng.uniform(-1, 1, (count, h.n // 2))
+        inputs.append((z, h.encrypt(z, BOOT["scale"] if kind != "rot" else 2.0 ** 40, L)))
+    h.synchronize()
+
+    def submit(srv, i):
+        kind, count, L, arg, _ = jobs[i]
+        ct = h.slice(inputs[i][1])
+        if kind == "rot":
+            return srv.submit_rotate(ct, arg)
+        if kind == "mm":
+            return srv.submit_matmul(ct, W, w_scale)
+        return srv.submit_bootstrap(ct, arg)
+
+    # warm-up: one job of each kind through a server, then the timed stream
+    srv = Server(h, bs, hbm_budget=S["budget_gb"] << 30, slots=S["slots"])
+    for kind in ("rot", "mm", "boot"):
+        i = next((k for k, j in enumerate(jobs) if j[0] == kind), None)
+        if i is not None:
+            srv.wait(submit(srv, i))
+    srv.close()
+    srv = Server(h, bs, hbm_budget=S["budget_gb"] << 30, slots=S["slots"])
+    clk = ClockSampler(dev).start()
+    ids = [None] * len(jobs)
+    l0 = lib.shm_kernel_launches()
+    t0 = time.perf_counter()
+
+    def feeder():
+        for i, j in enumerate(jobs):
+            delay = t0 + j[4] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids[i] = submit(srv, i)
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    th.join()
+    served = [srv.wait(j) for j in ids]
+    launches = lib.shm_kernel_launches() - l0
+    stats = srv.stats()
+    clocks = clk.summary()
+    srv.close()
+    lat = np.array([t[2] - t[0] for _, t, _ in served])
+    span = max(t[2] for _, t, _ in served) - min(t[0] for _, t, _ in served)
+    # results to the host (device memory back for the plain run); bootstraps judged by decryption
+    boot_err, results = [], []
+    for i, (out, _, _) in enumerate(served):
+        if jobs[i][0] == "boot":
+            boot_err.append(float(np.abs(h.decrypt(out) - inputs[i][0]).mean()))
+            results.append(None)
+        else:
+            results.append(out.to_host())
+        out.close()
+    del served
+
+    # serial plain execution on the same GPU: jobs in arrival order, one ciphertext per call,
+    # ordinary bootstrapping, the CUDA-core matmul; latency from the measured service times
+    service, plain = [], []
+    for i, (kind, count, L, arg, _) in enumerate(jobs):
+        x = inputs[i][1]
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        if kind == "mm":
+            outs = [h.ctpt_matmul(x, W, w_scale, tensor_cores=False)]
+        else:
+            outs = []
+            for c in range(count):
+                one = h.slice(x, c, 1)
+                outs.append(h.rotate(one, arg) if kind == "rot" else bs.run(one, 0))
+        h.synchronize()
+        service.append(time.perf_counter() - t)
+        plain.append(None if kind == "boot" else np.concatenate([o.to_host() for o in outs]))
+        del outs
+    finish, plat = 0.0, []
+    for (kind, _, _, _, arr), s in zip(jobs, service):
+        finish = max(finish, arr) + s
+        plat.append(finish - arr)
+    plat = np.array(plat)
+
+    same = {"rot": True, "mm": True}
+    for i, (kind, *_rest) in enumerate(jobs):
+        if kind != "boot":
+            same[kind] = same[kind] and bool(np.array_equal(results[i], plain[i]))
+    n_cts = sum(j[1] for j in jobs)
+    kinds = {k: sum(1 for j in jobs if j[0] == k) for k in ("rot", "mm", "boot")}
+    ms = lambda a, q: round(float(np.percentile(a, q)) * 1000.0, 2)  # noqa: E731
+    return {
+        "metric": "serving: jobs/s of a Poisson mix (rotation batches, ct-pt matmuls, shared-a bootstraps)",
+        "value": round(len(jobs) / span, 3), "unit": "jobs/s", "n_gpus": world, "steps": len(jobs), "warmup": 3,
+        "ms_per_step": round(span * 1000.0 / len(jobs), 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform slot values, random keys)",
+        "config": {"workload": "serve: Poisson arrivals at N=2^16 with resident keys, HBM-budget admission",
+                   "rate_jobs_per_s": S["rate"], "jobs": kinds, "ciphertexts": n_cts, "slots": S["slots"],
+                   "budget_gb": S["budget_gb"], "rotation_batches": f"1-{S['rot_max']} cts at {S['rot_levels']} limbs",
+                   "matmul": f"{S['mm_n']}x{S['mm_n']} at {S['mm_L']} limbs",
+                   "bootstrap": f"{S['boot_batch']} cts, shared-a n={S['members']}"},
+        "serving": {"p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99), "jobs_per_s": round(len(jobs) / span, 3),
+                    "cts_per_s": round(n_cts / span, 2), "peak_admitted_gb": round(stats["peak_admitted"] / 2**30, 2),
+                    "max_inflight": stats["max_inflight"], "batches": stats["batches"], "jobs_done": stats["jobs"]},
+        "plain_serial": {"p50_ms": ms(plat, 50), "p99_ms": ms(plat, 99),
+                         "jobs_per_s": round(len(jobs) / sum(service), 3),
+                         "path": "one ciphertext per call, ordinary bootstrapping, CUDA-core matmul"},
+        "bit_exact_vs_plain": same, "bootstrap_err_mean_max": max(boot_err) if boot_err else None,
+        "gpu_launches": int(launches), "clocks": clocks,
+    }
+
+
+# ---------------------------------------------------------------------------
 # primitive-chain workload
 
 
@@ -527,7 +682,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks"])
+    ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks", "serve"])
     ap.add_argument("--batch", type=int, default=None)
     ap.add_argument("--shared", type=int, default=8,
                     help="boot: shared-a group size n (0 = ordinary ciphertexts)")
@@ -580,7 +735,7 @@ def main():
 
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
-    runner = {"boot": run_boot, "prim": run_prim, "ctpt": run_ctpt, "ntt": run_kernel_case,
+    runner = {"boot": run_boot, "prim": run_prim, "ctpt": run_ctpt, "serve": run_serve, "ntt": run_kernel_case,
               "ks": run_kernel_case}[args.workload]
     res = runner(args, rank, world, dist)
     if rank == 0:

@@ -20,6 +20,7 @@
 #include <complex>
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -50,6 +51,9 @@ class DeviceBuffer {
     uint64_t *data() const { return p_; }
     size_t words() const { return words_; }
     DeviceBuffer clone() const;
+    // free through `c` (a view of the same context) from now on; the caller has made
+    // sure no work on the allocating stream still uses the buffer
+    void rebind(const Context &c) { ctx_ = &c; }
 
    private:
     const Context *ctx_ = nullptr;
@@ -63,6 +67,9 @@ class Context {
     Context(uint32_t log_n, const std::vector<int> &bits, uint32_t n_special, int device = 0, void *stream = nullptr);
     Context(uint32_t log_n, const std::vector<uint64_t> &primes, uint32_t n_special, int device = 0,
             void *stream = nullptr);
+    // a non-owning view of `base` (same device tables) whose operations run on `stream`;
+    // `base` must outlive it, and it must outlive every buffer allocated through it
+    Context(const Context &base, void *stream);
     ~Context();
     Context(const Context &) = delete;
     Context &operator=(const Context &) = delete;
@@ -82,6 +89,7 @@ class Context {
     void init();
     shm_context *h_ = nullptr;
     void *stream_ = nullptr;
+    bool owner_ = true;
 };
 
 struct Plaintext {
@@ -254,6 +262,13 @@ class Evaluator {
     Ciphertext to_shared(const Ciphertext &a, uint32_t members) const;  // FmtSwitch forward
     Ciphertext from_shared(const Ciphertext &a) const;                  // FmtSwitch backward
 
+    // Rotation-free ct-pt matmul Y[o] = sum_i X[i] * W[i][o] (W: [n_in][n_out] integers, the
+    // encoded weights round(w * w_scale)) followed by a rescale: the reference's
+    // multiply_plain + add_inplace + rescale loop (Ct_pt_matrix_mul.cuh:112-158).  Tensor
+    // cores (exact residue GEMMs) or the CUDA-core kernel; both exact.
+    Ciphertext ctpt_matmul(const Ciphertext &X, const std::vector<int64_t> &W, uint32_t n_out, double w_scale,
+                           bool tensor_cores = true) const;
+
    private:
     std::vector<uint64_t> residues(double integral, uint32_t L) const;
     std::vector<Ciphertext> automorphisms(const Ciphertext &a, const std::vector<uint32_t> &elts) const;
@@ -289,16 +304,20 @@ class BatchBootstrapper {
     std::vector<uint32_t> galois_elts() const;
     // the shared-a keys of groups of `members` for this bootstrapper's rotations
     SharedAKeys prepare_shared_keys(KeyGenerator &kg, uint32_t members, uint32_t hamming_weight = 192) const;
-    Ciphertext bootstrap_ordinary_s2c_first(const Ciphertext &ct) const;
+    // The prepared diagonals are read-only, so any evaluator over the same context (for
+    // instance one per serving slot, each on its own stream) may run the pipeline;
+    // `ev` defaults to the one the bootstrapper was built with.
+    Ciphertext bootstrap_ordinary_s2c_first(const Ciphertext &ct, const Evaluator *ev = nullptr) const;
     // groups of `members` consecutive ciphertexts; needs ev.shared_keys for that size
-    Ciphertext bootstrap_shared_a_s2c_first(const Ciphertext &ct, uint32_t members) const;
+    Ciphertext bootstrap_shared_a_s2c_first(const Ciphertext &ct, uint32_t members,
+                                            const Evaluator *ev = nullptr) const;
     // EvalMod of ciphertexts holding t / K: c_fin * sin(2 pi t) read at scale Delta
-    Ciphertext evalmod(const Ciphertext &x) const;
+    Ciphertext evalmod(const Ciphertext &x, const Evaluator *ev = nullptr) const;
     const BootstrapParams &params() const { return p_; }
 
    private:
-    void slots_to_re_im(Ciphertext x, Ciphertext &re, Ciphertext &im) const;
-    Ciphertext finish(const Ciphertext &re, const Ciphertext &im) const;
+    void slots_to_re_im(const Evaluator &ev, Ciphertext x, Ciphertext &re, Ciphertext &im) const;
+    Ciphertext finish(const Evaluator &ev, const Ciphertext &re, const Ciphertext &im) const;
 
     Evaluator &ev_;
     BootstrapParams p_;
@@ -311,5 +330,60 @@ class BatchBootstrapper {
 // max |V w - layers(w)| / max |V w| of the slot-transform factorisation at n slots
 // (a self-check of the planning code on random input)
 double slot_transform_selfcheck(uint32_t log_slots);
+
+// ------------------------------------------------------------------ serving loop
+
+enum class JobKind : int { Rotate = 0, Matmul = 1, Bootstrap = 2 };
+
+struct ServeResult {
+    Ciphertext output;
+    double t_submit = 0, t_start = 0, t_end = 0;  // seconds on the server's steady clock
+    uint32_t batched_with = 1;                    // jobs that shared its launches (continuous batching)
+    std::string error;                            // empty on success
+};
+
+struct ServeStats {
+    size_t budget = 0, peak_admitted = 0;  // admission estimates, bytes
+    uint32_t max_inflight = 0;             // most batches on the device at once
+    uint64_t batches = 0, jobs = 0;        // launches groups run, jobs completed
+};
+
+// A request loop over one device: jobs (key-switch / rotation batches, ct-pt matmuls,
+// shared-a or ordinary bootstraps) are admitted while their estimated device memory fits
+// the HBM budget and a slot is free; each slot is a worker thread with its own stream and
+// evaluator, so admitted batches overlap on the GPU; queued jobs of the same kind and
+// shape join the batch a slot starts (continuous batching).  Keys and the bootstrapper's
+// diagonals stay resident and are shared read-only.  Every result equals the job run
+// alone: ciphertexts are independent units and shared-a groups never span two jobs.
+class Server {
+   public:
+    Server(const Evaluator &base, const BatchBootstrapper *boot, const std::map<uint32_t, SharedAKeys> *shared,
+           size_t hbm_budget, uint32_t slots, uint32_t max_merge = 64);
+    ~Server();  // finishes the queued jobs, then stops the slots
+    uint64_t submit_rotate(Ciphertext &&ct, int step);
+    uint64_t submit_matmul(Ciphertext &&X, std::vector<int64_t> W, uint32_t n_out, double w_scale);
+    uint64_t submit_bootstrap(Ciphertext &&ct, uint32_t members);
+    ServeResult wait(uint64_t id);  // blocks until the job is done and hands its result over
+    // while paused, slots start no new batch (queued jobs wait; running ones finish)
+    void set_paused(bool paused);
+    ServeStats stats() const;
+    static double now();
+
+   private:
+    struct Job;
+    struct Slot;
+    uint64_t enqueue(std::unique_ptr<Job> j);
+    size_t estimate(const Job &j) const;
+    void worker(uint32_t slot);
+    void run(Slot &s, std::vector<Job *> &batch);
+
+    const Evaluator &base_;
+    const BatchBootstrapper *boot_;
+    const std::map<uint32_t, SharedAKeys> *shared_;
+    size_t budget_;
+    uint32_t max_merge_;
+    struct State;
+    std::unique_ptr<State> st_;
+};
 
 }  // namespace shmoai

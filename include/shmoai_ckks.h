@@ -230,6 +230,9 @@ int shm_free(const shm_context *ctx, void *ptr, void *stream);
  * asynchronous on `stream`. */
 int shm_memcpy(const shm_context *ctx, void *dst, const void *src, size_t bytes, int kind, void *stream);
 int shm_synchronize(const shm_context *ctx, void *stream);
+/* A non-blocking stream on the context's device (the serving loop runs one per slot). */
+int shm_stream_create(const shm_context *ctx, void **stream);
+int shm_stream_destroy(const shm_context *ctx, void *stream);
 
 /* ---- sampling (key generation, encryption) ----
  * Counter-based: value i of a call is a function of (seed, i) only, so the GPU and the

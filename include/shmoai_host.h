@@ -63,6 +63,8 @@ int shm_ct_from_host(shm_host *h, const uint64_t *data, uint32_t count, uint32_t
                      int shared, shm_ct **out);
 int shm_ct_to_host(shm_host *h, const shm_ct *ct, uint64_t *data);
 int shm_ct_info(const shm_ct *ct, uint32_t *count, uint32_t *size, uint32_t *L, double *scale, int *shared);
+/* a device copy of ciphertexts [first, first + count) of a batch */
+int shm_host_slice(shm_host *h, const shm_ct *ct, uint32_t first, uint32_t count, shm_ct **out);
 const uint64_t *shm_ct_device_data(const shm_ct *ct);
 void shm_ct_destroy(shm_ct *ct);
 
@@ -75,6 +77,10 @@ int shm_host_multiply_const(shm_host *h, const shm_ct *a, double value, shm_ct *
 int shm_host_rotate(shm_host *h, const shm_ct *a, int step, shm_ct **out);
 int shm_host_conjugate(shm_host *h, const shm_ct *a, shm_ct **out);
 int shm_host_multiply_i(shm_host *h, const shm_ct *a, int sign, shm_ct **out);
+/* rotation-free ct-pt matmul + rescale: W host [n_in][n_out] encoded integer weights
+ * (|W| < 2^40) at w_scale; tensor_cores = 0 runs the CUDA-core kernel (the plain path) */
+int shm_host_ctpt_matmul(shm_host *h, const shm_ct *X, const int64_t *W, uint32_t n_out, double w_scale,
+                         int tensor_cores, shm_ct **out);
 int shm_host_to_shared(shm_host *h, const shm_ct *a, uint32_t members, shm_ct **out);
 int shm_host_from_shared(shm_host *h, const shm_ct *a, shm_ct **out);
 
@@ -91,6 +97,28 @@ int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out);
 
 /* self-check of the slot-transform factorisation at 2^log_slots slots (max error) */
 double shm_slot_transform_selfcheck(uint32_t log_slots);
+
+/* ---- serving loop (shmoai::Server): jobs admitted by an HBM budget onto `slots`
+ * concurrent streams, queued jobs of the same kind and shape batched together.  Submit
+ * calls take ownership of the ciphertext handle (it is destroyed, the caller must not use
+ * it again); results come back through shm_server_wait.  `boot` may be NULL (no
+ * bootstrap jobs).  The host, the bootstrapper and the keys must outlive the server. */
+typedef struct shm_server shm_server;
+int shm_server_create(shm_host *h, shm_boot *boot, size_t hbm_budget_bytes, uint32_t slots, uint32_t max_merge,
+                      shm_server **out);
+void shm_server_destroy(shm_server *s); /* finishes queued jobs first */
+int shm_server_submit_rotate(shm_server *s, shm_ct *ct, int step, uint64_t *job);
+/* W: host [n_in][n_out] encoded integer weights (|W| < 2^40), output rescaled once */
+int shm_server_submit_matmul(shm_server *s, shm_ct *X, const int64_t *W, uint32_t n_out, double w_scale,
+                             uint64_t *job);
+int shm_server_submit_bootstrap(shm_server *s, shm_ct *ct, uint32_t members, uint64_t *job);
+/* blocks until `job` is done; times = {submit, start, end} in seconds (steady clock);
+ * batched_with = jobs that shared its launches; the job's error is returned as a status */
+int shm_server_wait(shm_server *s, uint64_t job, shm_ct **out, double *times, uint32_t *batched_with);
+/* paused = 1: slots start no new batch until resumed (queued jobs wait, running ones finish) */
+int shm_server_set_paused(shm_server *s, int paused);
+int shm_server_stats(const shm_server *s, size_t *budget, size_t *peak_admitted, uint32_t *max_inflight,
+                     uint64_t *batches, uint64_t *jobs);
 
 #ifdef __cplusplus
 }

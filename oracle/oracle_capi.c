@@ -120,6 +120,21 @@ int shm_synchronize(const shm_context *ctx, void *stream) {
     return SHM_OK;
 }
 
+static char g_stream_token;
+
+int shm_stream_create(const shm_context *ctx, void **stream) {
+    (void)ctx;
+    if (!stream) return fail("null output pointer");
+    *stream = &g_stream_token; /* host work is synchronous: any non-null token will do */
+    return SHM_OK;
+}
+
+int shm_stream_destroy(const shm_context *ctx, void *stream) {
+    (void)ctx;
+    (void)stream;
+    return SHM_OK;
+}
+
 /* ---- sampling (same function as shmoai_b200/csrc/sampling.cu) */
 
 static inline uint64_t mix64(uint64_t seed, uint64_t idx) {
@@ -331,6 +346,31 @@ int shm_modraise(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint
     free(x);
     orc_ntt(c, out, n_polys, L, 0);
     return SHM_OK;
+}
+
+/* ---- ct-pt matmul (both entry points are the same exact contraction here) */
+
+size_t shm_ctpt_matmul_workspace_bytes(const shm_context *ctx, uint32_t n_in, uint32_t n_out, uint32_t L) {
+    (void)ctx;
+    (void)n_in;
+    (void)n_out;
+    (void)L;
+    return 0;
+}
+
+int shm_ctpt_matmul_cuda_core(const shm_context *ctx, const uint64_t *X, const int64_t *W, uint64_t *Y,
+                              uint32_t n_in, uint32_t n_out, uint32_t L, void *stream) {
+    (void)stream;
+    if (!ctx || L < 1 || L > ctx->c->nq) return fail("level out of range");
+    orc_ctpt_matmul(ctx->c, X, W, n_in, n_out, L, Y);
+    return SHM_OK;
+}
+
+int shm_ctpt_matmul(const shm_context *ctx, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in,
+                    uint32_t n_out, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    return shm_ctpt_matmul_cuda_core(ctx, X, W, Y, n_in, n_out, L, stream);
 }
 
 /* ---- level and key switching */

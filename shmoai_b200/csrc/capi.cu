@@ -656,6 +656,23 @@ int shm_synchronize(const shm_context *ctx, void *stream) {
     });
 }
 
+int shm_stream_create(const shm_context *ctx, void **stream) {
+    return guard([&] {
+        if (!stream) throw std::invalid_argument("null output pointer");
+        set_device(ctx_of(ctx));
+        cudaStream_t s = nullptr;
+        SHM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        *stream = s;
+    });
+}
+
+int shm_stream_destroy(const shm_context *ctx, void *stream) {
+    return guard([&] {
+        set_device(ctx_of(ctx));
+        if (stream) SHM_CUDA(cudaStreamDestroy(S(stream)));
+    });
+}
+
 // ---- sampling and lifting
 
 int shm_sample_uniform(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed,

@@ -68,12 +68,25 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_conjugate": (i32, [_P, _P, pp]),
         "shm_host_multiply_i": (i32, [_P, _P, i32, pp]),
         "shm_host_to_shared": (i32, [_P, _P, _U32, pp]),
+        "shm_host_slice": (i32, [_P, _P, _U32, _U32, pp]),
+        "shm_host_ctpt_matmul": (i32, [_P, _P, ctypes.POINTER(ctypes.c_int64), _U32, ctypes.c_double, i32, pp]),
         "shm_host_from_shared": (i32, [_P, _P, pp]),
         "shm_boot_create": (i32, [_P, ctypes.c_double, _U32, pp]),
         "shm_boot_destroy": (None, [_P]),
         "shm_boot_galois_elts": (i32, [_P, ctypes.POINTER(_U32), _U32, ctypes.POINTER(_U32)]),
         "shm_boot_run": (i32, [_P, _P, _U32, pp]),
         "shm_slot_transform_selfcheck": (ctypes.c_double, [_U32]),
+        "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
+        "shm_server_destroy": (None, [_P]),
+        "shm_server_submit_rotate": (i32, [_P, _P, i32, ctypes.POINTER(ctypes.c_uint64)]),
+        "shm_server_submit_matmul": (i32, [_P, _P, ctypes.POINTER(ctypes.c_int64), _U32, ctypes.c_double,
+                                           ctypes.POINTER(ctypes.c_uint64)]),
+        "shm_server_submit_bootstrap": (i32, [_P, _P, _U32, ctypes.POINTER(ctypes.c_uint64)]),
+        "shm_server_wait": (i32, [_P, ctypes.c_uint64, pp, dp, ctypes.POINTER(_U32)]),
+        "shm_server_set_paused": (i32, [_P, i32]),
+        "shm_server_stats": (i32, [_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
+                                   ctypes.POINTER(_U32), ctypes.POINTER(ctypes.c_uint64),
+                                   ctypes.POINTER(ctypes.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -200,6 +213,15 @@ class Host:
     def multiply_i(self, a, sign: int = 1):
         return self._out(self.lib.shm_host_multiply_i, a._c, sign)
 
+    def slice(self, a, first: int = 0, count: int | None = None):
+        """A device copy of ciphertexts [first, first + count) (the whole batch by default)."""
+        return self._out(self.lib.shm_host_slice, a._c, first, a.count - first if count is None else count)
+
+    def ctpt_matmul(self, X, W: np.ndarray, w_scale: float, tensor_cores: bool = True):
+        W = np.ascontiguousarray(W, dtype=np.int64)
+        return self._out(self.lib.shm_host_ctpt_matmul, X._c, W.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                         W.shape[1], w_scale, 1 if tensor_cores else 0)
+
     def to_shared(self, a, members: int):
         return self._out(self.lib.shm_host_to_shared, a._c, members)
 
@@ -269,6 +291,69 @@ class Bootstrapper:
         if getattr(self, "_b", None):
             self.host.lib.shm_boot_destroy(self._b)
             self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The serving loop (shm_server_*): HBM-budget admission onto `slots` concurrent
+    streams, continuous batching of queued jobs of the same kind and shape.  Submitting
+    a ciphertext hands it over (the Ct object is emptied)."""
+
+    def __init__(self, host: Host, boot: Bootstrapper | None = None, hbm_budget: int = 64 << 30, slots: int = 2,
+                 max_merge: int = 64):
+        self.host = host
+        s = _P()
+        host._check(host.lib.shm_server_create(host._h, boot._b if boot else None, hbm_budget, slots, max_merge,
+                                               ctypes.byref(s)))
+        self._s = s
+
+    def _submit(self, fn, ct: Ct, *args) -> int:
+        job = ctypes.c_uint64()
+        handle, ct._c = ct._c, None  # ownership moves to the server (freed even on error)
+        self.host._check(fn(self._s, handle, *args, ctypes.byref(job)))
+        return int(job.value)
+
+    def submit_rotate(self, ct: Ct, step: int) -> int:
+        return self._submit(self.host.lib.shm_server_submit_rotate, ct, step)
+
+    def submit_matmul(self, ct: Ct, W: np.ndarray, w_scale: float) -> int:
+        W = np.ascontiguousarray(W, dtype=np.int64)
+        if W.shape[0] != ct.count:
+            raise ValueError("W must be [n_in][n_out]")
+        return self._submit(self.host.lib.shm_server_submit_matmul, ct,
+                            W.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), W.shape[1], w_scale)
+
+    def submit_bootstrap(self, ct: Ct, members: int = 0) -> int:
+        return self._submit(self.host.lib.shm_server_submit_bootstrap, ct, members)
+
+    def wait(self, job: int):
+        """(result Ct, (t_submit, t_start, t_end), jobs that shared its launches)"""
+        o = _P()
+        t = (ctypes.c_double * 3)()
+        b = _U32()
+        self.host._check(self.host.lib.shm_server_wait(self._s, job, ctypes.byref(o), t, ctypes.byref(b)))
+        return Ct(self.host, o), (t[0], t[1], t[2]), int(b.value)
+
+    def pause(self, paused: bool = True):
+        self.host._check(self.host.lib.shm_server_set_paused(self._s, 1 if paused else 0))
+
+    def resume(self):
+        self.pause(False)
+
+    def stats(self) -> dict:
+        v = [ctypes.c_size_t(), ctypes.c_size_t(), _U32(), ctypes.c_uint64(), ctypes.c_uint64()]
+        self.host._check(self.host.lib.shm_server_stats(self._s, *[ctypes.byref(x) for x in v]))
+        return dict(zip(("budget", "peak_admitted", "max_inflight", "batches", "jobs"), (x.value for x in v)))
+
+    def close(self):
+        if getattr(self, "_s", None):
+            self.host.lib.shm_server_destroy(self._s)
+            self._s = None
 
     def __del__(self):
         try:

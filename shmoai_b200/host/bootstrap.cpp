@@ -236,7 +236,7 @@ int64_t floordiv(int64_t a, int64_t b) {
 // sum_v Rot_{-g1 u b}(D_t) * Rot_{v b}(x).
 class LinearTransform {
    public:
-    LinearTransform(const Evaluator &ev, const Diags &diags, uint32_t level) : ev_(ev), level_(level) {
+    LinearTransform(const Evaluator &ev, const Diags &diags, uint32_t level) : level_(level) {
         const Context &c = ev.context();
         const int64_t n = c.n / 2;
         int64_t b = 0;
@@ -271,17 +271,17 @@ class LinearTransform {
         return s;
     }
 
-    Ciphertext apply(const Ciphertext &x, bool rescale = true) const {
+    Ciphertext apply(const Evaluator &ev, const Ciphertext &x, bool rescale = true) const {
         const Ciphertext *xp = &x;
         Ciphertext dropped;
         if (x.L != level_) {
-            dropped = ev_.mod_switch_to(x, level_);
+            dropped = ev.mod_switch_to(x, level_);
             xp = &dropped;
         }
         std::vector<int> bsteps;
         for (int64_t v : baby_)
             if (v) bsteps.push_back((int)(v * b_));
-        std::map<int, Ciphertext> rot = ev_.rotate_many(*xp, bsteps);
+        std::map<int, Ciphertext> rot = ev.rotate_many(*xp, bsteps);
         Ciphertext acc;
         bool have = false;
         for (auto &g : groups_) {
@@ -291,21 +291,20 @@ class LinearTransform {
                 X.push_back(vp.first ? &rot.at((int)(vp.first * b_)) : xp);
                 P.push_back(&vp.second);
             }
-            Ciphertext inner = ev_.multiply_plain_accumulate(X, P);
+            Ciphertext inner = ev.multiply_plain_accumulate(X, P);
             inner.scale_ = xp->scale_ * pt_scale_;
-            if (g.first) inner = ev_.rotate_vector(inner, (int)(g1_ * g.first * b_));
+            if (g.first) inner = ev.rotate_vector(inner, (int)(g1_ * g.first * b_));
             if (!have) {
                 acc = std::move(inner);
                 have = true;
             } else {
-                acc = ev_.add(acc, inner);
+                acc = ev.add(acc, inner);
             }
         }
-        return rescale ? ev_.rescale_to_next(acc) : std::move(acc);
+        return rescale ? ev.rescale_to_next(acc) : std::move(acc);
     }
 
    private:
-    const Evaluator &ev_;
     uint32_t level_;
     int64_t b_ = 1, g1_ = 1;
     double pt_scale_ = 1;
@@ -342,6 +341,7 @@ void BatchBootstrapper::prepare() {
     q0_ = (double)c.primes[0];
     cheb_ = cheb_interp(evalmod_target, p_.double_angles, p_.K, p_.degree);
     c_fin_ = q0_ / (2.0 * M_PI * p_.scale * p_.F);
+    c.synchronize();  // the diagonals are read from other streams later
 }
 
 std::vector<int> BatchBootstrapper::rotation_steps() const {
@@ -441,10 +441,11 @@ Ciphertext cheb_eval(const Evaluator &ev, const Basis &T, const std::vector<doub
 // targets: the i-th double angle squares at level lvl - i and drops prime lvl - 1 - i,
 // so s_in = sqrt(s_out * q); the last output scale is Delta * c_fin, which reads as the
 // value c_fin * y at scale Delta.
-Ciphertext BatchBootstrapper::evalmod(const Ciphertext &x) const {
-    const Context &c = ev_.context();
+Ciphertext BatchBootstrapper::evalmod(const Ciphertext &x, const Evaluator *evp) const {
+    const Evaluator &ev = evp ? *evp : ev_;
+    const Context &c = ev.context();
     const int deg = (int)cheb_.size() - 1;
-    Basis T = cheb_basis(ev_, x, deg);
+    Basis T = cheb_basis(ev, x, deg);
     uint32_t lvl = x.L - 1;
     while (!feasible(T, deg + 1, lvl)) {
         if (lvl == 0) throw Error("not enough levels for EvalMod");
@@ -452,43 +453,46 @@ Ciphertext BatchBootstrapper::evalmod(const Ciphertext &x) const {
     }
     double s = p_.scale * c_fin_;
     for (int i = p_.double_angles - 1; i >= 0; i--) s = std::sqrt(s * (double)c.primes[lvl - 1 - i]);
-    Ciphertext y = cheb_eval(ev_, T, cheb_, s, lvl);
-    for (int i = 0; i < p_.double_angles; i++) y = ev_.add_const(ev_.multiply_int(ev_.square(y), 2), -1.0);
+    Ciphertext y = cheb_eval(ev, T, cheb_, s, lvl);
+    for (int i = 0; i < p_.double_angles; i++) y = ev.add_const(ev.multiply_int(ev.square(y), 2), -1.0);
     y.scale_ /= c_fin_;
     return y;
 }
 
-void BatchBootstrapper::slots_to_re_im(Ciphertext x, Ciphertext &re, Ciphertext &im) const {
+void BatchBootstrapper::slots_to_re_im(const Evaluator &ev, Ciphertext x, Ciphertext &re, Ciphertext &im) const {
     if (s2c_.empty()) throw Error("call prepare() first");
     if (x.L != p_.input_level) throw Error("bootstrap input must have input_level primes");
-    for (auto *lt : s2c_) x = lt->apply(x);
-    Ciphertext w = ev_.mod_raise(x, top_);
+    for (auto *lt : s2c_) x = lt->apply(ev, x);
+    Ciphertext w = ev.mod_raise(x, top_);
     w.scale_ = q0_;
-    w = c2s_[0]->apply(w);
-    w = c2s_[1]->apply(w);
-    w = c2s_[2]->apply(w, false);
-    Ciphertext wc = ev_.complex_conjugate(w);
-    re = ev_.add(w, wc);
-    im = ev_.multiply_i(ev_.sub(w, wc), -1);
+    w = c2s_[0]->apply(ev, w);
+    w = c2s_[1]->apply(ev, w);
+    w = c2s_[2]->apply(ev, w, false);
+    Ciphertext wc = ev.complex_conjugate(w);
+    re = ev.add(w, wc);
+    im = ev.multiply_i(ev.sub(w, wc), -1);
 }
 
-Ciphertext BatchBootstrapper::finish(const Ciphertext &re, const Ciphertext &im) const {
-    Ciphertext y = evalmod(ev_.rescale_to_next(ev_.concat(re, im)));
+Ciphertext BatchBootstrapper::finish(const Evaluator &ev, const Ciphertext &re, const Ciphertext &im) const {
+    Ciphertext y = evalmod(ev.rescale_to_next(ev.concat(re, im)), &ev);
     const uint32_t nb = re.count;
-    return ev_.add(ev_.slice(y, 0, nb), ev_.multiply_i(ev_.slice(y, nb, nb)));
+    return ev.add(ev.slice(y, 0, nb), ev.multiply_i(ev.slice(y, nb, nb)));
 }
 
-Ciphertext BatchBootstrapper::bootstrap_ordinary_s2c_first(const Ciphertext &ct) const {
+Ciphertext BatchBootstrapper::bootstrap_ordinary_s2c_first(const Ciphertext &ct, const Evaluator *evp) const {
+    const Evaluator &ev = evp ? *evp : ev_;
     if (ct.shared || ct.size != 2) throw Error("bootstrap takes ordinary size-2 ciphertexts");
     Ciphertext re, im;
-    slots_to_re_im(ev_.adjust(ct, ct.L, ct.scale_), re, im);
-    return finish(re, im);
+    slots_to_re_im(ev, ev.adjust(ct, ct.L, ct.scale_), re, im);
+    return finish(ev, re, im);
 }
 
-Ciphertext BatchBootstrapper::bootstrap_shared_a_s2c_first(const Ciphertext &ct, uint32_t members) const {
+Ciphertext BatchBootstrapper::bootstrap_shared_a_s2c_first(const Ciphertext &ct, uint32_t members,
+                                                           const Evaluator *evp) const {
+    const Evaluator &ev = evp ? *evp : ev_;
     Ciphertext re, im;
-    slots_to_re_im(ev_.to_shared(ct, members), re, im);
-    return finish(ev_.from_shared(re), ev_.from_shared(im));
+    slots_to_re_im(ev, ev.to_shared(ct, members), re, im);
+    return finish(ev, ev.from_shared(re), ev.from_shared(im));
 }
 
 double slot_transform_selfcheck(uint32_t log_slots) {

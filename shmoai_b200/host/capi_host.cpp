@@ -32,6 +32,10 @@ struct shm_boot {
     std::unique_ptr<BatchBootstrapper> b;
 };
 
+struct shm_server {
+    std::unique_ptr<Server> s;
+};
+
 namespace {
 
 thread_local std::string g_err;
@@ -271,6 +275,20 @@ int shm_host_multiply_i(shm_host *h, const shm_ct *a, int sign, shm_ct **out) {
     return guard([&] { put(out, H(h).ev->multiply_i(C(a), sign)); });
 }
 
+int shm_host_slice(shm_host *h, const shm_ct *ct, uint32_t first, uint32_t count, shm_ct **out) {
+    return guard([&] { put(out, H(h).ev->slice(C(ct), first, count)); });
+}
+
+int shm_host_ctpt_matmul(shm_host *h, const shm_ct *X, const int64_t *W, uint32_t n_out, double w_scale,
+                         int tensor_cores, shm_ct **out) {
+    return guard([&] {
+        const Ciphertext &x = C(X);
+        if (!W) throw Error("null weights");
+        put(out, H(h).ev->ctpt_matmul(x, std::vector<int64_t>(W, W + (size_t)x.count * n_out), n_out, w_scale,
+                                      tensor_cores != 0));
+    });
+}
+
 int shm_host_to_shared(shm_host *h, const shm_ct *a, uint32_t members, shm_ct **out) {
     return guard([&] {
         H(h).use_shared(members);
@@ -318,6 +336,85 @@ int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out) 
         } else {
             put(out, b->b->bootstrap_ordinary_s2c_first(C(in)));
         }
+    });
+}
+
+int shm_server_create(shm_host *h, shm_boot *boot, size_t hbm_budget_bytes, uint32_t slots, uint32_t max_merge,
+                      shm_server **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!out) throw Error("null output handle");
+        *out = new shm_server{std::unique_ptr<Server>(
+            new Server(*hh.ev, boot ? boot->b.get() : nullptr, &hh.shared, hbm_budget_bytes, slots, max_merge))};
+    });
+}
+
+void shm_server_destroy(shm_server *s) { delete s; }
+
+namespace {
+Server &SV(shm_server *s) {
+    if (!s || !s->s) throw Error("null server handle");
+    return *s->s;
+}
+Ciphertext take(shm_ct *ct) {
+    if (!ct) throw Error("null ciphertext handle");
+    Ciphertext c = std::move(ct->ct);
+    delete ct;
+    return c;
+}
+}  // namespace
+
+int shm_server_submit_rotate(shm_server *s, shm_ct *ct, int step, uint64_t *job) {
+    return guard([&] {
+        Server &sv = SV(s);
+        *job = sv.submit_rotate(take(ct), step);
+    });
+}
+
+int shm_server_submit_matmul(shm_server *s, shm_ct *X, const int64_t *W, uint32_t n_out, double w_scale,
+                             uint64_t *job) {
+    return guard([&] {
+        Server &sv = SV(s);
+        if (!X || !W) throw Error("null argument");
+        const size_t n_in = X->ct.count;
+        *job = sv.submit_matmul(take(X), std::vector<int64_t>(W, W + n_in * n_out), n_out, w_scale);
+    });
+}
+
+int shm_server_submit_bootstrap(shm_server *s, shm_ct *ct, uint32_t members, uint64_t *job) {
+    return guard([&] {
+        Server &sv = SV(s);
+        *job = sv.submit_bootstrap(take(ct), members);
+    });
+}
+
+int shm_server_wait(shm_server *s, uint64_t job, shm_ct **out, double *times, uint32_t *batched_with) {
+    return guard([&] {
+        ServeResult r = SV(s).wait(job);
+        if (times) {
+            times[0] = r.t_submit;
+            times[1] = r.t_start;
+            times[2] = r.t_end;
+        }
+        if (batched_with) *batched_with = r.batched_with;
+        if (!r.error.empty()) throw Error(r.error);
+        put(out, std::move(r.output));
+    });
+}
+
+int shm_server_set_paused(shm_server *s, int paused) {
+    return guard([&] { SV(s).set_paused(paused != 0); });
+}
+
+int shm_server_stats(const shm_server *s, size_t *budget, size_t *peak_admitted, uint32_t *max_inflight,
+                     uint64_t *batches, uint64_t *jobs) {
+    return guard([&] {
+        ServeStats st = SV(const_cast<shm_server *>(s)).stats();
+        if (budget) *budget = st.budget;
+        if (peak_admitted) *peak_admitted = st.peak_admitted;
+        if (max_inflight) *max_inflight = st.max_inflight;
+        if (batches) *batches = st.batches;
+        if (jobs) *jobs = st.jobs;
     });
 }
 

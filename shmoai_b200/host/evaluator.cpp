@@ -355,6 +355,31 @@ Ciphertext Evaluator::slice(const Ciphertext &a, uint32_t first, uint32_t count)
     return o;
 }
 
+Ciphertext Evaluator::ctpt_matmul(const Ciphertext &X, const std::vector<int64_t> &W, uint32_t n_out,
+                                  double w_scale, bool tensor_cores) const {
+    if (X.shared || X.size != 2) throw Error("ct-pt matmul takes ordinary ciphertexts");
+    const uint32_t n_in = X.count;
+    if (W.size() != (size_t)n_in * n_out) throw Error("weight matrix must be [n_in][n_out]");
+    shm_context *h = c_.handle();
+    DeviceBuffer Wd(c_, W.size());
+    c_.check(shm_memcpy(h, Wd.data(), W.data(), W.size() * 8, SHM_COPY_H2D, c_.stream()));
+    Ciphertext Y;
+    Y.data = DeviceBuffer(c_, (size_t)n_out * 2 * X.L * c_.n);
+    Y.count = n_out;
+    Y.size = 2;
+    Y.L = X.L;
+    Y.scale_ = X.scale_ * w_scale;
+    const int64_t *w = reinterpret_cast<const int64_t *>(Wd.data());
+    if (tensor_cores) {
+        uint64_t *wsp = ws(shm_ctpt_matmul_workspace_bytes(h, n_in, n_out, X.L));
+        c_.check(shm_ctpt_matmul(h, X.data.data(), w, Y.data.data(), n_in, n_out, X.L, wsp, ws_.words() * 8,
+                                 c_.stream()));
+    } else {
+        c_.check(shm_ctpt_matmul_cuda_core(h, X.data.data(), w, Y.data.data(), n_in, n_out, X.L, c_.stream()));
+    }
+    return rescale_to_next(Y);
+}
+
 Ciphertext Evaluator::to_shared(const Ciphertext &a, uint32_t members) const {
     if (a.shared || a.size != 2) throw Error("to_shared takes ordinary ciphertexts");
     if (!members || a.count % members) throw Error("batch is not a multiple of the group size");

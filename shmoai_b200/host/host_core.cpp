@@ -27,6 +27,10 @@ Context::Context(uint32_t log_n_, const std::vector<uint64_t> &p, uint32_t n_spe
     init();
 }
 
+Context::Context(const Context &base, void *stream)
+    : log_n(base.log_n), n(base.n), nq(base.nq), np(base.np), dnum(base.dnum), primes(base.primes), h_(base.h_),
+      stream_(stream), owner_(false) {}
+
 void Context::init() {
     check(shm_context_info(h_, &log_n, &nq, &np, &dnum));
     n = 1u << log_n;
@@ -35,10 +39,8 @@ void Context::init() {
 }
 
 Context::~Context() {
-    if (h_) {
-        shm_synchronize(h_, stream_);
-        shm_context_destroy(h_);
-    }
+    if (h_) shm_synchronize(h_, stream_);
+    if (h_ && owner_) shm_context_destroy(h_);
 }
 
 void Context::check(int rc) const {
