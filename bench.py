@@ -222,6 +222,7 @@ def run_boot(args, rank, world, dist):
     def step():
         holder["out"] = bs.run(ct, S)
 
+    resident, _ = h.device_memory(reset_peak=True)  # keys, diagonals, the input batch
     clk = ClockSampler(dev).start()
     for _ in range(args.warmup):
         step()
@@ -229,6 +230,7 @@ def run_boot(args, rank, world, dist):
     l0 = lib.shm_kernel_launches()
     ms = timed_steps(torch, step, args.steps, dist, None)  # a batch is ~1 GB of live data per step > L2
     launches = lib.shm_kernel_launches() - l0
+    _, peak = h.device_memory()
     out = holder["out"]
     err = np.abs(h.decrypt(out) - z)
     out_level = out.level
@@ -262,6 +264,8 @@ def run_boot(args, rank, world, dist):
                    "batch_per_gpu": B, "shared_a_group": S or None, "N": h.n, "slots": n,
                    "input_primes": BOOT["input_level"], "output_primes": out_level, "Q": "[51]+20x[46]+14x[51]",
                    "P": "5x[51]", "dnum": h.nq // h.np, "path": "C++ host library (shm_boot_run) over the C ABI",
+                   "device_gb": {"resident_keys_plan_input": round(resident / 2 ** 30, 2),
+                                 "peak": round(peak / 2 ** 30, 2)},
                    "h": BOOT["h"], "evalmod": "Chebyshev deg 47, K=25, 3 double angles",
                    "err_mean": float(err.mean()), "err_max": float(err.max()),
                    "l2": "not flushed: the step's live data (~1 GB per batch of 32) exceeds the 126 MB L2",
@@ -333,7 +337,7 @@ def cpu_boot_estimate(shared: int = 0):
 # the same jobs executed one after the other on the plain per-ciphertext path
 
 SERVE = dict(n_jobs=24, rate=3.0, seed=5, p_rot=0.65, p_mm=0.15, members=8, boot_batch=32, mm_n=192, mm_L=13,
-             rot_steps=(1, 2, 4, 8), rot_max=64, rot_levels=(4, 24), slots=3, budget_gb=32)
+             rot_steps=(1, 2, 4, 8), rot_max=32, rot_levels=(4, 24), slots=3, budget_gb=48)
 
 
 def serve_jobs(rng):
@@ -398,6 +402,7 @@ def run_serve(args, rank, world, dist):
             srv.wait(submit(srv, i))
     srv.close()
     srv = Server(h, bs, hbm_budget=S["budget_gb"] << 30, slots=S["slots"])
+    resident, _ = h.device_memory(reset_peak=True)
     clk = ClockSampler(dev).start()
     ids = [None] * len(jobs)
     l0 = lib.shm_kernel_launches()
@@ -415,6 +420,7 @@ def run_serve(args, rank, world, dist):
     th.join()
     served = [srv.wait(j) for j in ids]
     launches = lib.shm_kernel_launches() - l0
+    _, peak = h.device_memory()
     stats = srv.stats()
     clocks = clk.summary()
     srv.close()
@@ -474,7 +480,8 @@ def run_serve(args, rank, world, dist):
                    "bootstrap": f"{S['boot_batch']} cts, shared-a n={S['members']}"},
         "serving": {"p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99), "jobs_per_s": round(len(jobs) / span, 3),
                     "cts_per_s": round(n_cts / span, 2), "peak_admitted_gb": round(stats["peak_admitted"] / 2**30, 2),
-                    "max_inflight": stats["max_inflight"], "batches": stats["batches"], "jobs_done": stats["jobs"]},
+                    "max_inflight": stats["max_inflight"], "batches": stats["batches"], "jobs_done": stats["jobs"],
+                    "device_gb_resident": round(resident / 2 ** 30, 2), "device_gb_peak": round(peak / 2 ** 30, 2)},
         "plain_serial": {"p50_ms": ms(plat, 50), "p99_ms": ms(plat, 99),
                          "jobs_per_s": round(len(jobs) / sum(service), 3),
                          "path": "one ciphertext per call, ordinary bootstrapping, CUDA-core matmul"},

@@ -230,6 +230,9 @@ int shm_free(const shm_context *ctx, void *ptr, void *stream);
  * asynchronous on `stream`. */
 int shm_memcpy(const shm_context *ctx, void *dst, const void *src, size_t bytes, int kind, void *stream);
 int shm_synchronize(const shm_context *ctx, void *stream);
+/* Bytes the context's pool holds from the driver, bytes in use, and the high-water mark of
+ * bytes in use (reset to the current use when reset_high != 0); any pointer may be NULL. */
+int shm_pool_usage(const shm_context *ctx, size_t *reserved, size_t *used, size_t *used_high, int reset_high);
 /* A non-blocking stream on the context's device (the serving loop runs one per slot). */
 int shm_stream_create(const shm_context *ctx, void **stream);
 int shm_stream_destroy(const shm_context *ctx, void *stream);

@@ -42,6 +42,9 @@ const shm_context *shm_host_context(const shm_host *h);
 /* the n_q + n_special primes of the host's context */
 int shm_host_primes(const shm_host *h, uint64_t *out);
 int shm_host_synchronize(shm_host *h);
+/* device bytes the host library holds now and at its peak (keys, ciphertexts, workspaces);
+ * reset_peak != 0 restarts the peak from the current use */
+int shm_host_device_memory(shm_host *h, size_t *in_use, size_t *peak, int reset_peak);
 
 int shm_host_gen_relin_key(shm_host *h);
 int shm_host_gen_galois_keys(shm_host *h, const uint32_t *elts, uint32_t n_elts);

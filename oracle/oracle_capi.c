@@ -120,6 +120,15 @@ int shm_synchronize(const shm_context *ctx, void *stream) {
     return SHM_OK;
 }
 
+int shm_pool_usage(const shm_context *ctx, size_t *reserved, size_t *used, size_t *used_high, int reset_high) {
+    (void)ctx;
+    (void)reset_high;
+    if (reserved) *reserved = 0; /* host memory: not tracked */
+    if (used) *used = 0;
+    if (used_high) *used_high = 0;
+    return SHM_OK;
+}
+
 static char g_stream_token;
 
 int shm_stream_create(const shm_context *ctx, void **stream) {

@@ -622,7 +622,40 @@ int shm_malloc(const shm_context *ctx, size_t bytes, void **out, void *stream) {
         set_device(c);
         cudaMemPool_t pool = c.mempool();
         if (bytes == 0) return;
-        SHM_CUDA(cudaMallocFromPoolAsync(out, bytes, pool, S(stream)));
+        cudaError_t e = cudaMallocFromPoolAsync(out, bytes, pool, S(stream));
+        if (e == cudaErrorMemoryAllocation) {
+            // blocks freed on other streams become reusable once their work is done: wait for
+            // the device once and retry before reporting out of memory
+            cudaGetLastError();
+            SHM_CUDA(cudaDeviceSynchronize());
+            e = cudaMallocFromPoolAsync(out, bytes, pool, S(stream));
+        }
+        SHM_CUDA(e);
+    });
+}
+
+int shm_pool_usage(const shm_context *ctx, size_t *reserved, size_t *used, size_t *used_high, int reset_high) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        set_device(c);
+        cudaMemPool_t pool = c.mempool();
+        uint64_t v = 0;
+        if (reserved) {
+            SHM_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v));
+            *reserved = v;
+        }
+        if (used) {
+            SHM_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &v));
+            *used = v;
+        }
+        if (used_high) {
+            SHM_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &v));
+            *used_high = v;
+        }
+        if (reset_high) {
+            uint64_t zero = 0;
+            SHM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
+        }
     });
 }
 

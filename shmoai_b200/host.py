@@ -47,6 +47,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_destroy": (None, [_P]),
         "shm_host_context": (_P, [_P]),
         "shm_host_synchronize": (i32, [_P]),
+        "shm_host_device_memory": (i32, [_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
+                                         i32]),
         "shm_host_gen_relin_key": (i32, [_P]),
         "shm_host_gen_galois_keys": (i32, [_P, ctypes.POINTER(_U32), _U32]),
         "shm_host_gen_shared_keys": (i32, [_P, _U32, _U32, ctypes.POINTER(_U32), _U32]),
@@ -155,6 +157,13 @@ class Host:
 
     def synchronize(self):
         self._check(self.lib.shm_host_synchronize(self._h))
+
+    def device_memory(self, reset_peak: bool = False) -> tuple[int, int]:
+        """(bytes in use, peak bytes in use) of the host library's device pool."""
+        used, peak = ctypes.c_size_t(), ctypes.c_size_t()
+        self._check(self.lib.shm_host_device_memory(self._h, ctypes.byref(used), ctypes.byref(peak),
+                                                    1 if reset_peak else 0))
+        return used.value, peak.value
 
     # ---- ciphertexts
     def _out(self, fn, *args) -> "Ct":

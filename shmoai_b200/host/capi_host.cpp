@@ -141,6 +141,13 @@ int shm_host_synchronize(shm_host *h) {
     return guard([&] { H(h).ctx->synchronize(); });
 }
 
+int shm_host_device_memory(shm_host *h, size_t *in_use, size_t *peak, int reset_peak) {
+    return guard([&] {
+        auto &hh = H(h);
+        hh.ctx->check(shm_pool_usage(hh.ctx->handle(), nullptr, in_use, peak, reset_peak));
+    });
+}
+
 int shm_host_gen_relin_key(shm_host *h) {
     return guard([&] { H(h).relin = H(h).kg->relin_key(); });
 }

@@ -3,6 +3,7 @@
 // queued jobs of the same kind and shape.  The reference has no serving loop (its driver
 // runs operators one after the other, src/include/test/bootstrapping/test_shared_a.cuh);
 // this is the request loop the north-star workload asks for.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -101,12 +102,17 @@ size_t Server::estimate(const Job &j) const {
             return (cnt + 2 * (size_t)j.n_out) * ct + j.W.size() * 8 +
                    shm_ctpt_matmul_workspace_bytes(c.handle(), (uint32_t)cnt, j.n_out, (uint32_t)L);
         case JobKind::Bootstrap: {
-            // peak inside CoeffToSlot at nq primes: ~8 ciphertexts of baby steps and sums plus the
-            // hoisted ModUp digits (dnum x (nq + np) limbs) per ciphertext or shared-a group
-            const size_t top = 2 * (size_t)c.nq * word, digits = (size_t)c.dnum * (c.nq + c.np) * word;
+            // CoeffToSlot at nq primes: ~8 polynomials per input polynomial (baby steps, sums)
+            // plus the hoisted ModUp digits (dnum x (nq + np) limbs) per ciphertext or group.
+            // EvalMod on 2 x cnt ciphertexts (real and imaginary parts) near nq - 4 primes: ~12
+            // batches of the Chebyshev basis and products plus the relinearisation digits.
+            // The two phases do not overlap; the larger one sets the peak.
+            const size_t top_poly = (size_t)c.nq * word, digits = (size_t)c.dnum * (c.nq + c.np) * word;
             const size_t units = j.members ? cnt / j.members : cnt;
             const size_t polys_per_unit = j.members ? j.members + 1 : 2;
-            return units * (polys_per_unit * (4 * top + digits) / 2) + 2 * units * top;
+            const size_t c2s = units * (polys_per_unit * 8 * top_poly + digits);
+            const size_t evalmod = 2 * cnt * (12 * 2 * (size_t)(c.nq - 4) * word + digits);
+            return std::max(c2s, evalmod) + 2 * cnt * 2 * top_poly;
         }
     }
     return 0;
