@@ -337,7 +337,7 @@ def cpu_boot_estimate(shared: int = 0):
 # the same jobs executed one after the other on the plain per-ciphertext path
 
 SERVE = dict(n_jobs=24, rate=3.0, seed=5, p_rot=0.65, p_mm=0.15, members=8, boot_batch=32, mm_n=192, mm_L=13,
-             rot_steps=(1, 2, 4, 8), rot_max=32, rot_levels=(4, 24), slots=3, budget_gb=48)
+             rot_steps=(1, 2, 4, 8), rot_max=32, rot_levels=(4, 24), slots=3, budget_gb=80)
 
 
 def serve_jobs(rng):
@@ -437,6 +437,21 @@ def run_serve(args, rank, world, dist):
         out.close()
     del served
 
+    # capacity: the same jobs all queued at once (throughput with the slots saturated)
+    srv = Server(h, bs, hbm_budget=S["budget_gb"] << 30, slots=S["slots"])
+    srv.pause()
+    cap_ids = [submit(srv, i) for i in range(len(jobs))]
+    srv.resume()
+    cap = [srv.wait(j) for j in cap_ids]
+    cap_span = max(t[2] for _, t, _ in cap) - min(t[0] for _, t, _ in cap)
+    cap_stats = srv.stats()
+    for i, (out, _, _) in enumerate(cap):
+        if results[i] is not None and not np.array_equal(out.to_host(), results[i]):
+            raise AssertionError(f"serving job {i} differs between the two runs")
+        out.close()
+    del cap
+    srv.close()
+
     # serial plain execution on the same GPU: jobs in arrival order, one ciphertext per call,
     # ordinary bootstrapping, the CUDA-core matmul; latency from the measured service times
     service, plain = [], []
@@ -469,17 +484,20 @@ def run_serve(args, rank, world, dist):
     kinds = {k: sum(1 for j in jobs if j[0] == k) for k in ("rot", "mm", "boot")}
     ms = lambda a, q: round(float(np.percentile(a, q)) * 1000.0, 2)  # noqa: E731
     return {
-        "metric": "serving: jobs/s of a Poisson mix (rotation batches, ct-pt matmuls, shared-a bootstraps)",
-        "value": round(len(jobs) / span, 3), "unit": "jobs/s", "n_gpus": world, "steps": len(jobs), "warmup": 3,
-        "ms_per_step": round(span * 1000.0 / len(jobs), 3), "higher_is_better": True, "scaling": "weak",
+        "metric": "serving throughput, jobs/s with every job queued (rotation batches, ct-pt matmuls, shared-a "
+                  "bootstraps); p50/p99 latency at Poisson arrivals",
+        "value": round(len(jobs) / cap_span, 3), "unit": "jobs/s", "n_gpus": world, "steps": len(jobs), "warmup": 3,
+        "ms_per_step": round(cap_span * 1000.0 / len(jobs), 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform slot values, random keys)",
         "config": {"workload": "serve: Poisson arrivals at N=2^16 with resident keys, HBM-budget admission",
                    "rate_jobs_per_s": S["rate"], "jobs": kinds, "ciphertexts": n_cts, "slots": S["slots"],
                    "budget_gb": S["budget_gb"], "rotation_batches": f"1-{S['rot_max']} cts at {S['rot_levels']} limbs",
                    "matmul": f"{S['mm_n']}x{S['mm_n']} at {S['mm_L']} limbs",
                    "bootstrap": f"{S['boot_batch']} cts, shared-a n={S['members']}"},
-        "serving": {"p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99), "jobs_per_s": round(len(jobs) / span, 3),
-                    "cts_per_s": round(n_cts / span, 2), "peak_admitted_gb": round(stats["peak_admitted"] / 2**30, 2),
+        "serving": {"p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99), "poisson_jobs_per_s": round(len(jobs) / span, 3),
+                    "capacity_jobs_per_s": round(len(jobs) / cap_span, 3),
+                    "capacity_cts_per_s": round(n_cts / cap_span, 2), "capacity_batches": cap_stats["batches"],
+                    "peak_admitted_gb": round(stats["peak_admitted"] / 2**30, 2),
                     "max_inflight": stats["max_inflight"], "batches": stats["batches"], "jobs_done": stats["jobs"],
                     "device_gb_resident": round(resident / 2 ** 30, 2), "device_gb_peak": round(peak / 2 ** 30, 2)},
         "plain_serial": {"p50_ms": ms(plat, 50), "p99_ms": ms(plat, 99),

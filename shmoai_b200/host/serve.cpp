@@ -104,14 +104,16 @@ size_t Server::estimate(const Job &j) const {
         case JobKind::Bootstrap: {
             // CoeffToSlot at nq primes: ~8 polynomials per input polynomial (baby steps, sums)
             // plus the hoisted ModUp digits (dnum x (nq + np) limbs) per ciphertext or group.
-            // EvalMod on 2 x cnt ciphertexts (real and imaginary parts) near nq - 4 primes: ~12
-            // batches of the Chebyshev basis and products plus the relinearisation digits.
-            // The two phases do not overlap; the larger one sets the peak.
+            // EvalMod on 2 x cnt ciphertexts (real and imaginary parts) near nq - 4 primes:
+            // ~24 ciphertexts each (Chebyshev basis, products, partial sums, dropped copies)
+            // plus two sets of relinearisation digits -- calibrated on the pool's high-water
+            // mark (~60 GB for 32 ciphertexts at the reference parameters).  The two phases
+            // do not overlap; the larger one sets the peak.
             const size_t top_poly = (size_t)c.nq * word, digits = (size_t)c.dnum * (c.nq + c.np) * word;
             const size_t units = j.members ? cnt / j.members : cnt;
             const size_t polys_per_unit = j.members ? j.members + 1 : 2;
             const size_t c2s = units * (polys_per_unit * 8 * top_poly + digits);
-            const size_t evalmod = 2 * cnt * (12 * 2 * (size_t)(c.nq - 4) * word + digits);
+            const size_t evalmod = 2 * cnt * (24 * 2 * (size_t)(c.nq - 4) * word + 2 * digits);
             return std::max(c2s, evalmod) + 2 * cnt * 2 * top_poly;
         }
     }
