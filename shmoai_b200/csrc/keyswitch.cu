@@ -58,9 +58,12 @@ __global__ void modup_conv_kernel(const uint64_t *__restrict__ x, const uint64_t
 // acc[ct][h][j][k] = sum_b up[ct][b][j][perm[k]] * key[b][h][prime(j)][k]   (perm = identity if null)
 // An NTT-domain automorphism maps every aligned block of 32 slots onto an aligned block
 // of 32 slots, so the permuted read of a warp stays within one 256-byte segment.
+// B = beta at compile time: the key rows held in registers for the whole batch are
+// exactly 2B words, so small digit counts keep more warps resident.
+template <int B>
 __global__ void inner_product_kernel(const uint64_t *__restrict__ up, const uint64_t *__restrict__ key,
                                      uint64_t *__restrict__ acc, uint32_t n_cts, uint32_t L, uint32_t np, uint32_t nq,
-                                     uint32_t beta, uint32_t log_n, const PrimeConst *__restrict__ pc,
+                                     uint32_t log_n, const PrimeConst *__restrict__ pc,
                                      const uint32_t *__restrict__ perm) {
     const uint32_t j = blockIdx.y;
     const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
@@ -69,30 +72,45 @@ __global__ void inner_product_kernel(const uint64_t *__restrict__ up, const uint
     const uint32_t LP = L + np, QP = nq + np;
     const uint32_t pj = j < L ? j : nq + (j - L);
     const PrimeConst p = pc[pj];
-    uint64_t k0[kMaxBeta], k1[kMaxBeta];
+    uint64_t k0[B], k1[B];
 #pragma unroll
-    for (int b = 0; b < kMaxBeta; b++) {
-        if (b < (int)beta) {
-            const uint64_t *kb = key + (size_t)b * 2 * QP * n;
-            k0[b] = kb[(size_t)pj * n + k];
-            k1[b] = kb[((size_t)QP + pj) * n + k];
-        }
+    for (int b = 0; b < B; b++) {
+        const uint64_t *kb = key + (size_t)b * 2 * QP * n;
+        k0[b] = kb[(size_t)pj * n + k];
+        k1[b] = kb[((size_t)QP + pj) * n + k];
     }
     for (uint32_t ct = 0; ct < n_cts; ct++) {
-        const uint64_t *u = up + (size_t)ct * beta * LP * n + (size_t)j * n + ks;
+        const uint64_t *u = up + (size_t)ct * B * LP * n + (size_t)j * n + ks;
+        uint64_t v[B];
+#pragma unroll
+        for (int b = 0; b < B; b++) v[b] = u[(size_t)b * LP * n];
         u128 a0 = {0, 0}, a1 = {0, 0};
 #pragma unroll
-        for (int b = 0; b < kMaxBeta; b++) {
-            if (b < (int)beta) {
-                uint64_t v = u[(size_t)b * LP * n];
-                mac(a0, v, k0[b]);
-                mac(a1, v, k1[b]);
-            }
+        for (int b = 0; b < B; b++) {
+            mac(a0, v[b], k0[b]);
+            mac(a1, v[b], k1[b]);
         }
         uint64_t *o = acc + (size_t)ct * 2 * LP * n + (size_t)j * n + k;  // output in natural slot order
         o[0] = barrett(a0, p);
         o[(size_t)LP * n] = barrett(a1, p);
     }
+}
+
+void launch_inner_product(dim3 grid, cudaStream_t st, const uint64_t *up, const uint64_t *key, uint64_t *acc,
+                          uint32_t n_cts, uint32_t L, uint32_t np, uint32_t nq, uint32_t beta, uint32_t log_n,
+                          const PrimeConst *pc, const uint32_t *perm) {
+#define SHM_IP_CASE(B)                                                                                          \
+    case B:                                                                                                     \
+        inner_product_kernel<B><<<grid, kThreads, 0, st>>>(up, key, acc, n_cts, L, np, nq, log_n, pc, perm); \
+        break;
+    switch (beta) {
+        SHM_IP_CASE(1) SHM_IP_CASE(2) SHM_IP_CASE(3) SHM_IP_CASE(4) SHM_IP_CASE(5) SHM_IP_CASE(6) SHM_IP_CASE(7)
+        SHM_IP_CASE(8) SHM_IP_CASE(9) SHM_IP_CASE(10) SHM_IP_CASE(11) SHM_IP_CASE(12) SHM_IP_CASE(13)
+        SHM_IP_CASE(14) SHM_IP_CASE(15) SHM_IP_CASE(16)
+        default:
+            throw std::invalid_argument("key-switching digit count out of range");
+    }
+#undef SHM_IP_CASE
 }
 
 // delta[ct][h][j][k] = sum_k' z[ct][h][L+k'][k] * (phat_k' mod q_j), j < L
@@ -182,7 +200,7 @@ void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_
     }
     ntt_forward(c, up, n_cts * beta * LP, beta * LP, m, st);
     // 4. inner product with the key digits
-    SHM_LAUNCHED(1); inner_product_kernel<<<dim3(n / kThreads, LP), kThreads, 0, st>>>(up, key, acc, n_cts, L, np, c.nq, beta, c.log_n,
+    SHM_LAUNCHED(1); launch_inner_product(dim3(n / kThreads, LP), st, up, key, acc, n_cts, L, np, c.nq, beta, c.log_n,
                                                                       c.pc, nullptr);
     SHM_CUDA(cudaGetLastError());
     // 5. ModDown: INTT of the P limbs (scaled by phat_k^-1), convert to Ql, NTT, combine
@@ -272,8 +290,8 @@ void apply_galois_hoisted(const Context &c, const uint64_t *ct, uint32_t n_cts, 
     for (uint32_t e = 0; e < n_elts; e++) {
         const uint32_t *perm = const_cast<Context &>(c).perm(elts[e]);
         SHM_LAUNCHED(1);
-        inner_product_kernel<<<dim3(n / kThreads, LP), kThreads, 0, st>>>(up, keys[e], acc, n_cts, L, np, c.nq, beta,
-                                                                          c.log_n, c.pc, perm);
+        launch_inner_product(dim3(n / kThreads, LP), st, up, keys[e], acc, n_cts, L, np, c.nq, beta, c.log_n, c.pc,
+                             perm);
         SHM_CUDA(cudaGetLastError());
         ntt_inverse(c, acc, n_cts * 2 * LP, LP, mp, c.moddown_scale, st, L);
         SHM_LAUNCHED(1);

@@ -43,16 +43,23 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_col(uint64_t *__restri
     uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * kNttSubs;
     const uint32_t sig = threadIdx.x % kNttSubs, lane = threadIdx.x / kNttSubs;
 
+    const bool grow = q < kGrowPrimeLimit;  // uniform per CTA (one limb)
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane + m * G::E)];
-    fwd_pass<R>(a, w, ws, 1, 0, 0, q);
+    if (grow)
+        fwd_pass<R, true>(a, w, ws, 1, 0, 0, q);
+    else
+        fwd_pass<R>(a, w, ws, 1, 0, 0, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) sm[(lane + m * G::E) * kNttSubs + sig] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = sm[(lane * G::E + m) * kNttSubs + sig];
-    fwd_pass<R>(a, w, ws, 1, R, lane, q);
+    if (grow)
+        fwd_pass<R, true>(a, w, ws, 1, R, lane, q);
+    else
+        fwd_pass<R>(a, w, ws, 1, R, lane, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane * G::E + m)] = a[m];
 }
@@ -76,19 +83,30 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_blk(uint64_t *__restri
     uint64_t *x = xc + (size_t)sig * G::M;
     uint64_t *s = sm + sig * G::PAD_M;
 
+    const bool grow = q < kGrowPrimeLimit;  // the same choice fwd_col made for this limb
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = x[lane + m * G::E];
-    fwd_pass<R>(a, w, ws, G::M + b, 0, 0, q);
+    if (grow)
+        fwd_pass<R, true>(a, w, ws, G::M + b, 0, 0, q);
+    else
+        fwd_pass<R>(a, w, ws, G::M + b, 0, 0, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) s[padded(lane + m * G::E)] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
-    fwd_pass<R>(a, w, ws, G::M + b, R, lane, q);
-    const uint64_t q2 = 2 * q;
+    if (grow) {
+        fwd_pass<R, true>(a, w, ws, G::M + b, R, lane, q);
+        const PrimeConst p = pc[pidx];
 #pragma unroll
-    for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = csub(csub(a[m], q2), q);
+        for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = barrett({a[m], 0}, p);  // < 36q -> [0, q)
+    } else {
+        fwd_pass<R>(a, w, ws, G::M + b, R, lane, q);
+        const uint64_t q2 = 2 * q;
+#pragma unroll
+        for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = csub(csub(a[m], q2), q);
+    }
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < G::E; i++) {

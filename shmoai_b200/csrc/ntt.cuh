@@ -42,6 +42,18 @@ __device__ __forceinline__ void ct_bf(uint64_t &x, uint64_t &y, uint64_t w, uint
     y = a - t + q2;
 }
 
+// Cooley-Tukey butterfly without the reduction of x: outputs exceed the inputs by less
+// than 2q (Shoup's lazy product is below 2q for any 64-bit multiplicand).  From inputs
+// below 4q, 16 stages stay below 36q, so this is exact for primes q < 2^58.
+constexpr uint64_t kGrowPrimeLimit = 1ull << 58;
+
+__device__ __forceinline__ void ct_bf_grow(uint64_t &x, uint64_t &y, uint64_t w, uint64_t ws, uint64_t q) {
+    uint64_t t = shoup_lazy(y, w, ws, q);
+    uint64_t a = x;
+    x = a + t;
+    y = a - t + 2 * q;
+}
+
 __device__ __forceinline__ void gs_bf(uint64_t &x, uint64_t &y, uint64_t w, uint64_t ws, uint64_t q) {
     uint64_t q2 = 2 * q;
     uint64_t a = x + y;
@@ -52,7 +64,9 @@ __device__ __forceinline__ void gs_bf(uint64_t &x, uint64_t &y, uint64_t w, uint
 
 // R forward stages on E = 2^R registers.  Stage r of the pass is global stage
 // s0 + r; the twiddle of the pair starting at m is tw[(tb << (s0 + r)) + (g << r) + (m >> (R - r))].
-template <int R>
+// GROW: use ct_bf_grow (primes below kGrowPrimeLimit), else the Harvey butterfly that
+// keeps values in [0, 4q).
+template <int R, bool GROW = false>
 __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
                                          const uint64_t *__restrict__ ws, uint32_t tb, uint32_t s0, uint32_t g,
                                          uint64_t q) {
@@ -64,7 +78,10 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
         for (int m = 0; m < (1 << R); m++) {
             if (m & half) continue;
             uint32_t idx = base + (m >> (R - r));
-            ct_bf(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
+            if (GROW)
+                ct_bf_grow(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
+            else
+                ct_bf(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
         }
     }
 }

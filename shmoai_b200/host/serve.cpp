@@ -126,6 +126,9 @@ uint64_t Server::enqueue(std::unique_ptr<Job> j) {
         throw Error("job needs ~" + std::to_string(j->bytes >> 20) + " MiB, above the HBM budget of " +
                     std::to_string(budget_ >> 20) + " MiB");
     j->result.t_submit = now();
+    // The input was produced on the base context's stream; the slots' streams do not wait for
+    // it (they are non-blocking), so the input must be complete before a slot can pick it up.
+    base_.context().synchronize();
     std::lock_guard<std::mutex> g(st_->mu);
     if (st_->stop) throw Error("server is stopping");
     j->id = st_->next_id++;
