@@ -1,28 +1,34 @@
 """Benchmark of the CKKS evaluator hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload boot|prim] [--batch B]
+                    [--workload boot|prim|ctpt|serve|ntt|ks] [--batch B] [--shared n]
 
 Prints one JSON line on rank 0.  Workloads (synthetic, seeded):
 
-  boot  (default; the headline metric) S2C-first bootstrapping, reference
-        parameters N = 2^16, Q = [51] + 20x[46] + 14x[51], P = 5x[51] (dnum 7),
-        Delta = 2^46, h = 192, inputs at 4 primes with 2^15 slots uniform in
-        [-1, 1]^2.  One step = one batch of B ciphertexts (default 32; the
+  boot  (default; the headline metric) S2C-first bootstrapping through the C++ host
+        library, reference parameters N = 2^16, Q = [51] + 20x[46] + 14x[51],
+        P = 5x[51] (dnum 7), Delta = 2^46, h = 192, inputs at 4 primes with 2^15 slots
+        uniform in [-1, 1]^2; shared-a groups of --shared n (default 8; 0 = ordinary
+        ciphertexts).  One step = one batch of B ciphertexts (default 32; the
         768-ciphertext job of the reference is 24 such steps).  Unit: bootstraps/s.
         The decryption error of the last batch is reported beside the speed.
   prim  config-1 chain on one ciphertext (N = 2^16, Q = [60] + 23x[50], P = 8x[60],
         dnum 3): inverse+forward NTT of all limbs, HRotate by one slot,
         multiply + relinearize + rescale.  Unit: chains/s.
+  ctpt  config-2 rotation-free ct-pt matmul (768 -> 768 ciphertexts at 13 limbs) on
+        the INT8 tensor cores.  Unit: output ciphertexts/s.
+  serve config-5 serving loop: a Poisson stream of mixed jobs (rotation batches,
+        matmuls, shared-a bootstraps) against serial plain execution.  Unit: jobs/s.
+  ntt / ks  kernel cases for profiling (batched forward NTT; one rotation batch).
 
 Multi-GPU: ciphertexts are independent, so each rank bootstraps its own batch
 (weak scaling, no data-path collective); the step time is the max over ranks.
 
 --impl reference: the reference has no CPU implementation of these operations,
 so the CPU arm is the oracle (oracle/ckks_oracle.c, a scalar OpenMP restatement
-of the reference's arithmetic) on all host cores: for boot, one HRotate at the
-C2S level and one relinearisation at the EvalMod level per step, scaled by the
-bootstrap's own count of rotations and relinearisations.
+of the reference's arithmetic) on all host cores: for boot, one (Sh-)rotation at the
+C2S level and at the S2C level and one relinearisation at the EvalMod level per
+step, scaled by the bootstrap's own count of rotations and relinearisations.
 """
 from __future__ import annotations
 

@@ -66,13 +66,11 @@ __device__ __forceinline__ uint32_t mod_small(uint64_t x, uint32_t t) {
     return (uint32_t)(r < 0 ? r + (int)m : r);
 }
 
-// a mod m_t in [0, m_t) for any int32 accumulator (exact in a double; |a| < n_in * 125^2)
+// a mod m_t in [0, m_t) for any int32 accumulator: a + m * 2^24 (a multiple of m above
+// 2^31, the moduli being > 128) is non-negative and below 2^33, then the 32-bit fold above
 __device__ __forceinline__ uint32_t mod_acc(int a, uint32_t t) {
-    const int m = (int)c_mods.m[t];
-    int r = a - (int)floor((double)a * c_mods.inv[t]) * m;
-    if (r < 0) r += m;
-    else if (r >= m) r -= m;
-    return (uint32_t)r;
+    const uint64_t x = (uint64_t)((int64_t)a + ((int64_t)c_mods.m[t] << 24));
+    return mod_small(x, t);
 }
 
 // X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via a 64 x 64 shared-memory transpose
@@ -150,7 +148,9 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 }
 
 // grid: (R_chunk / 128, Np / 256, T); one modulus per blockIdx.z
-__global__ void __launch_bounds__(kThreads, 1) mma_kernel(const int8_t *__restrict__ XP, const int8_t *__restrict__ WP,
+// Two CTAs per SM (2 x 97 KB shared memory, 2 x 256 TMEM columns): one CTA's loads and
+// epilogue overlap the other's MMAs.
+__global__ void __launch_bounds__(kThreads, 2) mma_kernel(const int8_t *__restrict__ XP, const int8_t *__restrict__ WP,
                                                           uint8_t *__restrict__ RES, uint32_t Kp, uint32_t Np,
                                                           uint32_t n_out, uint64_t chunk, int *__restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -276,38 +276,46 @@ struct CrtLimb {
     uint64_t M;            // M mod q_l
 };
 
+// one thread folds 4 consecutive columns r (one limb, 4 | N): 4-byte residue loads and
+// two 16-byte stores instead of byte loads and 8-byte stores
 __global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict__ Y, const CrtLimb *__restrict__ tab,
                            uint32_t n_out, uint64_t chunk, uint64_t r0, uint64_t R, uint32_t L, uint32_t log_n,
                            const PrimeConst *__restrict__ pc) {
-    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const uint32_t o = blockIdx.y;
     if (r >= chunk) return;
     const uint64_t rg = r0 + r;
     const uint32_t limb = (uint32_t)((rg >> log_n) % L);
     const CrtLimb &cl = tab[limb];
-    // sum_t r_t c_t as two 64-bit partial sums over the 32-bit halves of c_t (r_t < 2^8)
-    uint64_t lo = 0, hi = 0;
-    float v = 0.f;
     const uint32_t T = c_mods.t;
     uint32_t res[kMaxMods];
 #pragma unroll
     for (uint32_t t = 0; t < kMaxMods; t++)  // all loads in flight before any use
-        res[t] = t < T ? RES[((uint64_t)t * n_out + o) * chunk + r] : 0u;
-#pragma unroll
-    for (uint32_t t = 0; t < kMaxMods; t++) {
-        if (t < T) {
-            const uint32_t rt = res[t];
-            const uint64_t c = cl.c[t];
-            lo += (uint64_t)rt * (uint32_t)c;
-            hi += (uint64_t)rt * (uint32_t)(c >> 32);
-            v += (float)rt * c_mods.frac[t];
-        }
-    }
-    u128 pos = {lo + (hi << 32), (hi >> 32) + ((lo + (hi << 32)) < lo ? 1ull : 0ull)};
-    const uint64_t vi = (uint64_t)(int64_t)rintf(v);
+        res[t] = t < T ? *reinterpret_cast<const uint32_t *>(RES + ((uint64_t)t * n_out + o) * chunk + r) : 0u;
     const PrimeConst p = pc[limb];
-    const uint64_t y = sub_mod(barrett(pos, p), barrett(mul_wide(vi, cl.M), p), p.q);
-    Y[(uint64_t)o * R + rg] = y;
+    uint64_t y[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        // sum_t r_t c_t as two 64-bit partial sums over the 32-bit halves of c_t (r_t < 2^8)
+        uint64_t lo = 0, hi = 0;
+        float v = 0.f;
+#pragma unroll
+        for (uint32_t t = 0; t < kMaxMods; t++) {
+            if (t < T) {
+                const uint32_t rt = (res[t] >> (8 * e)) & 0xFF;
+                const uint64_t c = cl.c[t];
+                lo += (uint64_t)rt * (uint32_t)c;
+                hi += (uint64_t)rt * (uint32_t)(c >> 32);
+                v += (float)rt * c_mods.frac[t];
+            }
+        }
+        u128 pos = {lo + (hi << 32), (hi >> 32) + ((lo + (hi << 32)) < lo ? 1ull : 0ull)};
+        const uint64_t vi = (uint64_t)(int64_t)rintf(v);
+        y[e] = sub_mod(barrett(pos, p), barrett(mul_wide(vi, cl.M), p), p.q);
+    }
+    ulonglong2 *out = reinterpret_cast<ulonglong2 *>(Y + (uint64_t)o * R + rg);
+    out[0] = make_ulonglong2(y[0], y[1]);
+    out[1] = make_ulonglong2(y[2], y[3]);
 }
 
 }  // namespace
@@ -419,8 +427,8 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
                                                                                        chunk, err);
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
-        crt_kernel<<<dim3((uint32_t)((chunk + 255) / 256), n_out), 256, 0, st>>>(RES, Y, tab, n_out, chunk, r0, R, L,
-                                                                                c.log_n, c.pc);
+        crt_kernel<<<dim3((uint32_t)((chunk / 4 + 255) / 256), n_out), 256, 0, st>>>(RES, Y, tab, n_out, chunk, r0, R,
+                                                                                    L, c.log_n, c.pc);
         SHM_CUDA(cudaGetLastError());
     }
 }

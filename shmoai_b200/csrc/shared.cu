@@ -27,31 +27,47 @@ namespace {
 constexpr int kT = 256;
 constexpr int kMaxB = 16;
 
-// acc[ct][h][j][k] = sum_b up[ct][b][j][perm(k)] * key[b][h][prime(j)][k], h < H
-__global__ void ip_multi_kernel(const uint64_t *__restrict__ up, const uint64_t *__restrict__ key,
-                                uint64_t *__restrict__ acc, uint32_t n_cts, uint32_t L, uint32_t np, uint32_t nq,
-                                uint32_t beta, uint32_t H, uint32_t log_n, const PrimeConst *__restrict__ pc,
-                                const uint32_t *__restrict__ perm) {
+// acc[ct][h][j][k] = sum_b up[ct][b][j][perm(k)] * key[b][h][prime(j)][k], h < H.
+// A block handles `chunk` groups: each thread stages its own extended-digit words of those
+// groups in shared memory (a column per thread, so no synchronisation), then, half by
+// half, holds the key digits in registers and serves every group of the chunk: the key
+// (n + 1 halves of dnum x QP limbs, far larger than L2 at the top level) is read once per
+// chunk instead of once per group.
+constexpr int kIpT = 128;
+constexpr size_t kIpSmem = 32 * 1024;
+
+__global__ void __launch_bounds__(kIpT) ip_multi_kernel(const uint64_t *__restrict__ up,
+                                                        const uint64_t *__restrict__ key, uint64_t *__restrict__ acc,
+                                                        uint32_t n_cts, uint32_t chunk, uint32_t L, uint32_t np,
+                                                        uint32_t nq, uint32_t beta, uint32_t H, uint32_t log_n,
+                                                        const PrimeConst *__restrict__ pc,
+                                                        const uint32_t *__restrict__ perm) {
+    extern __shared__ uint64_t su[];  // [chunk * beta][kIpT]
     const uint32_t j = blockIdx.y;
-    const uint32_t k = blockIdx.x * kT + threadIdx.x;
+    const uint32_t k = blockIdx.x * kIpT + threadIdx.x;
     const uint32_t ks = perm ? __ldg(perm + k) : k;
     const size_t n = (size_t)1 << log_n;
     const uint32_t LP = L + np, QP = nq + np;
     const uint32_t pj = j < L ? j : nq + (j - L);
     const PrimeConst p = pc[pj];
-    for (uint32_t ct = 0; ct < n_cts; ct++) {
-        uint64_t u[kMaxB];
-        const uint64_t *up_c = up + (size_t)ct * beta * LP * n + (size_t)j * n + ks;
+    const uint32_t c0 = blockIdx.z * chunk, nc = min(chunk, n_cts - c0);
+    for (uint32_t ct = 0; ct < nc; ct++) {
+        const uint64_t *up_c = up + (size_t)(c0 + ct) * beta * LP * n + (size_t)j * n + ks;
+        for (uint32_t b = 0; b < beta; b++) su[(ct * beta + b) * kIpT + threadIdx.x] = up_c[(size_t)b * LP * n];
+    }
+    for (uint32_t h = 0; h < H; h++) {
+        uint64_t kk[kMaxB];
+        const uint64_t *kp = key + ((size_t)h * QP + pj) * n + k;
 #pragma unroll
         for (int b = 0; b < kMaxB; b++)
-            if (b < (int)beta) u[b] = up_c[(size_t)b * LP * n];
-        for (uint32_t h = 0; h < H; h++) {
+            if (b < (int)beta) kk[b] = __ldg(kp + (size_t)b * H * QP * n);
+        for (uint32_t ct = 0; ct < nc; ct++) {
             u128 a = {0, 0};
-            const uint64_t *kp = key + ((size_t)h * QP + pj) * n + k;
+            const uint64_t *s = su + ct * beta * kIpT + threadIdx.x;
 #pragma unroll
             for (int b = 0; b < kMaxB; b++)
-                if (b < (int)beta) mac(a, u[b], __ldg(kp + (size_t)b * H * QP * n));
-            acc[(((size_t)ct * H + h) * LP + j) * n + k] = barrett(a, p);
+                if (b < (int)beta) mac(a, s[b * kIpT], kk[b]);
+            acc[(((size_t)(c0 + ct) * H + h) * LP + j) * n + k] = barrett(a, p);
         }
     }
 }
@@ -193,9 +209,10 @@ void apply_target(const Context &c, const uint64_t *up, uint32_t n_cts, uint32_t
                   const Target &t, uint64_t *acc, uint64_t *delta, cudaStream_t st) {
     const size_t n = c.n;
     const uint32_t np = c.np, LP = L + np;
+    const uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_cts, kIpSmem / (beta * kIpT * 8)));
     SHM_LAUNCHED(1);
-    ip_multi_kernel<<<dim3(n / kT, LP), kT, 0, st>>>(up, t.key, acc, n_cts, L, np, c.nq, beta, H, c.log_n, c.pc,
-                                                     t.perm);
+    ip_multi_kernel<<<dim3(n / kIpT, LP, (n_cts + chunk - 1) / chunk), kIpT, (size_t)chunk * beta * kIpT * 8, st>>>(
+        up, t.key, acc, n_cts, chunk, L, np, c.nq, beta, H, c.log_n, c.pc, t.perm);
     SHM_CUDA(cudaGetLastError());
     LimbMap mp;
     for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
