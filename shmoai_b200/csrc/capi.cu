@@ -120,6 +120,10 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
         p.q = q;
         p.mu = host::barrett_mu(q);
         p.shift = host::bit_length(q) - 1;
+        {
+            const uint32_t k = p.shift + 1, s = k > 25 ? k - 25 : 0;
+            p.red_m = (uint32_t)(((unsigned __int128)1 << (32 + s)) / q);
+        }
         p.n_inv = host::invmod(n, q);
         p.n_inv_shoup = host::shoup_of(p.n_inv, q);
         c->h_pc.push_back(p);

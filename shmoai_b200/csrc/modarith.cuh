@@ -17,7 +17,7 @@ struct PrimeConst {
     uint64_t q;      // the prime
     uint64_t mu;     // floor(2^(63+k) / q)
     uint32_t shift;  // k - 1, k = bit length of q
-    uint32_t pad;
+    uint32_t red_m;  // floor(2^(32+s) / q), s = max(0, k - 25): the multiplier of reduce_small
     uint64_t n_inv;        // N^-1 mod q
     uint64_t n_inv_shoup;  // Shoup companion of n_inv
 };
@@ -37,6 +37,30 @@ __device__ __forceinline__ uint64_t shoup_lazy(uint64_t a, uint64_t w, uint64_t 
 
 __device__ __forceinline__ uint64_t shoup(uint64_t a, uint64_t w, uint64_t ws, uint64_t q) {
     return csub(shoup_lazy(a, w, ws, q), q);
+}
+
+// a * w mod q in [0, 4q), any a < 2^64, with three 32-bit multiplies for the quotient
+// instead of a full 64 x 64 high product.  With a = a1 2^32 + a0 and w' = s1 2^32 + s0,
+// floor(a w' / 2^64) = a1 s1 + hi(a1 s0) + hi(a0 s1) + floor(F), where F collects the low
+// words of the two cross products and a0 s0 / 2^64, so F < 3: dropping it leaves the
+// quotient low by at most 2 and adds at most 2q to Shoup's remainder (below 2q).
+__device__ __forceinline__ uint64_t shoup_lazy4(uint64_t a, uint64_t w, uint64_t ws, uint64_t q) {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+    const uint32_t s0 = (uint32_t)ws, s1 = (uint32_t)(ws >> 32);
+    const uint64_t qh = (uint64_t)a1 * s1 + ((uint64_t)__umulhi(a1, s0) + __umulhi(a0, s1));
+    return a * w - qh * q;
+}
+
+// x mod q for x < 2^(k+7), k = bit length of q.  With X = x >> s < 2^32 (s = max(0, k - 25))
+// and red_m = floor(2^(32+s) / q) <= 2^8 (or < 2^32 when s = 0), qq = floor(X red_m / 2^32)
+// never exceeds floor(x / q) and falls short of it by at most 2 (the truncations of X and
+// of red_m each cost less than one, x_lo / q < 2^-24), so x - qq q lies in [0, 3q).
+__device__ __forceinline__ uint64_t reduce_small(uint64_t x, const PrimeConst &p) {
+    const uint32_t s = p.shift > 24 ? p.shift - 24 : 0;
+    const uint32_t qq = __umulhi((uint32_t)(x >> s), p.red_m);
+    uint64_t r = x - (uint64_t)qq * p.q;
+    r = csub(r, 2 * p.q);
+    return csub(r, p.q);
 }
 
 // 128-bit accumulator

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_blk(uint64_t *__restri
         fwd_pass<R, true>(a, w, ws, G::M + b, R, lane, q);
         const PrimeConst p = pc[pidx];
 #pragma unroll
-        for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = barrett({a[m], 0}, p);  // < 36q -> [0, q)
+        for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = reduce_small(a[m], p);  // < 68q -> [0, q)
     } else {
         fwd_pass<R>(a, w, ws, G::M + b, R, lane, q);
         const uint64_t q2 = 2 * q;
@@ -142,13 +142,20 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_blk(uint64_t *__restri
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
-    inv_pass<R>(a, w, ws, G::M + b, R, lane, q, 0);
+    const bool grow = q < kGrowPrimeLimit;  // uniform per CTA (one limb)
+    if (grow)
+        inv_pass<R, true>(a, w, ws, G::M + b, R, lane, q, 0);
+    else
+        inv_pass<R>(a, w, ws, G::M + b, R, lane, q, 0);
 #pragma unroll
     for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane + m * G::E)];
-    inv_pass<R>(a, w, ws, G::M + b, 0, 0, q, 0);
+    if (grow)
+        inv_pass<R, true>(a, w, ws, G::M + b, 0, 0, q, 0);
+    else
+        inv_pass<R>(a, w, ws, G::M + b, 0, 0, q, 0);
     uint64_t *x = xc + (size_t)sig * G::M;
 #pragma unroll
     for (int m = 0; m < G::E; m++) x[lane + m * G::E] = a[m];
@@ -177,14 +184,22 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_col(uint64_t *__restri
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane * G::E + m)];
-    inv_pass<R>(a, w, ws, 1, R, lane, q, 0);
+    const bool grow = q < kGrowPrimeLimit;  // the same choice inv_blk made for this limb
+    if (grow)
+        inv_pass<R, true>(a, w, ws, 1, R, lane, q, 0);
+    else
+        inv_pass<R>(a, w, ws, 1, R, lane, q, 0);
 #pragma unroll
     for (int m = 0; m < G::E; m++) sm[(lane * G::E + m) * kNttSubs + sig] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = sm[(lane + m * G::E) * kNttSubs + sig];
-    inv_pass<R>(a, w, ws, 1, 0, 0, q, 1);
-    const uint64_t c0 = sc[0], c0s = sc[1], c1 = sc[2], c1s = sc[3], q2 = 2 * q;
+    if (grow)
+        inv_pass<R, true>(a, w, ws, 1, 0, 0, q, 1);
+    else
+        inv_pass<R>(a, w, ws, 1, 0, 0, q, 1);
+    // values in [0, 4q) (grow) or [0, 2q)
+    const uint64_t c0 = sc[0], c0s = sc[1], c1 = sc[2], c1s = sc[3], q2 = (grow ? 4 : 2) * q;
 #pragma unroll
     for (int m = 0; m < G::E / 2; m++) {
         uint64_t u = a[m], v = a[m + G::E / 2];

@@ -43,15 +43,16 @@ __device__ __forceinline__ void ct_bf(uint64_t &x, uint64_t &y, uint64_t w, uint
 }
 
 // Cooley-Tukey butterfly without the reduction of x: outputs exceed the inputs by less
-// than 2q (Shoup's lazy product is below 2q for any 64-bit multiplicand).  From inputs
-// below 4q, 16 stages stay below 36q, so this is exact for primes q < 2^58.
-constexpr uint64_t kGrowPrimeLimit = 1ull << 58;
+// than 4q (shoup_lazy4 is below 4q for any 64-bit multiplicand).  From inputs below 4q,
+// 16 stages stay below 68q < 2^(k+7), so this is exact for primes q < 2^57 and the last
+// stage's output is reduced by reduce_small.
+constexpr uint64_t kGrowPrimeLimit = 1ull << 57;
 
 __device__ __forceinline__ void ct_bf_grow(uint64_t &x, uint64_t &y, uint64_t w, uint64_t ws, uint64_t q) {
-    uint64_t t = shoup_lazy(y, w, ws, q);
+    uint64_t t = shoup_lazy4(y, w, ws, q);
     uint64_t a = x;
     x = a + t;
-    y = a - t + 2 * q;
+    y = a - t + 4 * q;
 }
 
 __device__ __forceinline__ void gs_bf(uint64_t &x, uint64_t &y, uint64_t w, uint64_t ws, uint64_t q) {
@@ -60,6 +61,15 @@ __device__ __forceinline__ void gs_bf(uint64_t &x, uint64_t &y, uint64_t w, uint
     uint64_t d = x - y + q2;
     x = csub(a, q2);
     y = shoup_lazy(d, w, ws, q);
+}
+
+// Gentleman-Sande butterfly on [0, 4q) with the cheaper quotient of shoup_lazy4 (needs 8q < 2^64)
+__device__ __forceinline__ void gs_bf4(uint64_t &x, uint64_t &y, uint64_t w, uint64_t ws, uint64_t q) {
+    uint64_t q4 = 4 * q;
+    uint64_t a = x + y;
+    uint64_t d = x - y + q4;
+    x = csub(a, q4);
+    y = shoup_lazy4(d, w, ws, q);
 }
 
 // R forward stages on E = 2^R registers.  Stage r of the pass is global stage
@@ -86,7 +96,8 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
     }
 }
 
-template <int R>
+// GROW: gs_bf4 on [0, 4q) (primes below kGrowPrimeLimit), else gs_bf on [0, 2q)
+template <int R, bool GROW = false>
 __device__ __forceinline__ void inv_pass(uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
                                          const uint64_t *__restrict__ ws, uint32_t tb, uint32_t s0, uint32_t g,
                                          uint64_t q, int skip_stage0) {
@@ -99,7 +110,10 @@ __device__ __forceinline__ void inv_pass(uint64_t (&a)[1 << R], const uint64_t *
         for (int m = 0; m < (1 << R); m++) {
             if (m & half) continue;
             uint32_t idx = base + (m >> (R - r));
-            gs_bf(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
+            if (GROW)
+                gs_bf4(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
+            else
+                gs_bf(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
         }
     }
 }
