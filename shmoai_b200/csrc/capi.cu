@@ -1,4 +1,5 @@
 // Context construction and the extern "C" entry points of include/shmoai_ckks.h.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -110,6 +111,7 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
         if (np && (uint64_t)np * q >= (1ull << 63))
             throw std::invalid_argument("alpha * q must stay below 2^63 for the lazy base conversion");
     }
+    c->s52 = *std::max_element(primes.begin(), primes.end()) < kS52PrimeLimit;
     // per-prime constants and twiddles
     std::vector<uint64_t> tw((size_t)QP * 4 * n), psi_half_inv(QP), sc_plain;
     for (uint32_t i = 0; i < QP; i++) {

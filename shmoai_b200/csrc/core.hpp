@@ -43,6 +43,7 @@ struct Context {
     int device = 0;
     uint32_t log_n = 0, n = 0, nq = 0, np = 0, dnum = 0;
     std::vector<uint64_t> primes;       // nq + np
+    bool s52 = false;                   // every prime below kS52PrimeLimit (Acc<true> kernels)
     std::vector<PrimeConst> h_pc;       // host copy
     PrimeConst *pc = nullptr;           // [QP]
     uint64_t *tw = nullptr;             // [QP][4][N]

@@ -22,6 +22,7 @@ constexpr int kMaxAlpha = 16;
 constexpr int kMaxBeta = 16;
 
 // up[ct][b][j][k] for j outside digit b; digit rows copy d (NTT form).
+template <bool S52>
 __global__ void modup_conv_kernel(const uint64_t *__restrict__ x, const uint64_t *__restrict__ d, size_t d_stride,
                                   uint64_t *__restrict__ up, const uint64_t *__restrict__ conv, uint32_t L,
                                   uint32_t np, uint32_t nq, uint32_t log_n, const PrimeConst *__restrict__ pc) {
@@ -47,11 +48,11 @@ __global__ void modup_conv_kernel(const uint64_t *__restrict__ x, const uint64_t
         }
         const PrimeConst &p = pc[j < L ? j : nq + (j - L)];
         const uint64_t *cj = s_conv + j * alpha;
-        u128 acc = {0, 0};
+        Acc<S52> acc;
 #pragma unroll
         for (int i = 0; i < kMaxAlpha; i++)
-            if (i < (int)na) mac(acc, y[i], cj[i]);
-        o[(size_t)j * n + k] = barrett(acc, p);
+            if (i < (int)na) acc.add(y[i], cj[i]);
+        o[(size_t)j * n + k] = barrett(acc.get(), p);
     }
 }
 
@@ -60,7 +61,7 @@ __global__ void modup_conv_kernel(const uint64_t *__restrict__ x, const uint64_t
 // of 32 slots, so the permuted read of a warp stays within one 256-byte segment.
 // B = beta at compile time: the key rows held in registers for the whole batch are
 // exactly 2B words, so small digit counts keep more warps resident.
-template <int B>
+template <int B, bool S52>
 __global__ void inner_product_kernel(const uint64_t *__restrict__ up, const uint64_t *__restrict__ key,
                                      uint64_t *__restrict__ acc, uint32_t n_cts, uint32_t L, uint32_t np, uint32_t nq,
                                      uint32_t log_n, const PrimeConst *__restrict__ pc,
@@ -84,24 +85,25 @@ __global__ void inner_product_kernel(const uint64_t *__restrict__ up, const uint
         uint64_t v[B];
 #pragma unroll
         for (int b = 0; b < B; b++) v[b] = u[(size_t)b * LP * n];
-        u128 a0 = {0, 0}, a1 = {0, 0};
+        Acc<S52> a0, a1;
 #pragma unroll
         for (int b = 0; b < B; b++) {
-            mac(a0, v[b], k0[b]);
-            mac(a1, v[b], k1[b]);
+            a0.add(v[b], k0[b]);
+            a1.add(v[b], k1[b]);
         }
         uint64_t *o = acc + (size_t)ct * 2 * LP * n + (size_t)j * n + k;  // output in natural slot order
-        o[0] = barrett(a0, p);
-        o[(size_t)LP * n] = barrett(a1, p);
+        o[0] = barrett(a0.get(), p);
+        o[(size_t)LP * n] = barrett(a1.get(), p);
     }
 }
 
+template <bool S52>
 void launch_inner_product(dim3 grid, cudaStream_t st, const uint64_t *up, const uint64_t *key, uint64_t *acc,
                           uint32_t n_cts, uint32_t L, uint32_t np, uint32_t nq, uint32_t beta, uint32_t log_n,
                           const PrimeConst *pc, const uint32_t *perm) {
-#define SHM_IP_CASE(B)                                                                                          \
-    case B:                                                                                                     \
-        inner_product_kernel<B><<<grid, kThreads, 0, st>>>(up, key, acc, n_cts, L, np, nq, log_n, pc, perm); \
+#define SHM_IP_CASE(B)                                                                                               \
+    case B:                                                                                                          \
+        inner_product_kernel<B, S52><<<grid, kThreads, 0, st>>>(up, key, acc, n_cts, L, np, nq, log_n, pc, perm); \
         break;
     switch (beta) {
         SHM_IP_CASE(1) SHM_IP_CASE(2) SHM_IP_CASE(3) SHM_IP_CASE(4) SHM_IP_CASE(5) SHM_IP_CASE(6) SHM_IP_CASE(7)
@@ -114,6 +116,7 @@ void launch_inner_product(dim3 grid, cudaStream_t st, const uint64_t *up, const 
 }
 
 // delta[ct][h][j][k] = sum_k' z[ct][h][L+k'][k] * (phat_k' mod q_j), j < L
+template <bool S52>
 __global__ void moddown_conv_kernel(const uint64_t *__restrict__ acc, uint64_t *__restrict__ delta,
                                     const uint64_t *__restrict__ conv, uint32_t L, uint32_t np, uint32_t log_n,
                                     const PrimeConst *__restrict__ pc) {
@@ -129,11 +132,11 @@ __global__ void moddown_conv_kernel(const uint64_t *__restrict__ acc, uint64_t *
     uint64_t *o = delta + (size_t)hc * L * n + k;
     for (uint32_t j = 0; j < L; j++) {
         const uint64_t *cj = conv + (size_t)j * np;
-        u128 a = {0, 0};
+        Acc<S52> a;
 #pragma unroll
         for (int i = 0; i < kMaxAlpha; i++)
-            if (i < (int)np) mac(a, zv[i], __ldg(cj + i));
-        o[(size_t)j * n] = barrett(a, pc[j]);
+            if (i < (int)np) a.add(zv[i], __ldg(cj + i));
+        o[(size_t)j * n] = barrett(a.get(), pc[j]);
     }
 }
 
@@ -158,6 +161,43 @@ __global__ void ks_combine_kernel(const uint64_t *__restrict__ acc, const uint64
     (h ? o.out1 : o.out0)[off] = r;
 }
 
+// the kernels above for one context: Acc<true> when every prime is below 2^52
+void launch_modup_conv(const Context &c, uint32_t n_cts, uint32_t L, const uint64_t *x, const uint64_t *d,
+                       size_t d_stride, uint64_t *up, cudaStream_t st) {
+    const uint32_t np = c.np, beta = (L + np - 1) / np;
+    const dim3 grid(c.n / kThreads, beta, n_cts);
+    const uint64_t *conv = c.ks[L].modup_conv;
+    SHM_LAUNCHED(1);
+    if (c.s52)
+        modup_conv_kernel<true><<<grid, kThreads, 0, st>>>(x, d, d_stride, up, conv, L, np, c.nq, c.log_n, c.pc);
+    else
+        modup_conv_kernel<false><<<grid, kThreads, 0, st>>>(x, d, d_stride, up, conv, L, np, c.nq, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+}
+
+void launch_ip(const Context &c, uint32_t n_cts, uint32_t L, const uint64_t *up, const uint64_t *key, uint64_t *acc,
+               const uint32_t *perm, cudaStream_t st) {
+    const uint32_t np = c.np, beta = (L + np - 1) / np, LP = L + np;
+    const dim3 grid(c.n / kThreads, LP);
+    SHM_LAUNCHED(1);
+    if (c.s52)
+        launch_inner_product<true>(grid, st, up, key, acc, n_cts, L, np, c.nq, beta, c.log_n, c.pc, perm);
+    else
+        launch_inner_product<false>(grid, st, up, key, acc, n_cts, L, np, c.nq, beta, c.log_n, c.pc, perm);
+    SHM_CUDA(cudaGetLastError());
+}
+
+void launch_moddown_conv(const Context &c, uint32_t n_polys, uint32_t L, const uint64_t *acc, uint64_t *delta,
+                         cudaStream_t st) {
+    const dim3 grid(c.n / kThreads, n_polys);
+    SHM_LAUNCHED(1);
+    if (c.s52)
+        moddown_conv_kernel<true><<<grid, kThreads, 0, st>>>(acc, delta, c.moddown_conv, L, c.np, c.log_n, c.pc);
+    else
+        moddown_conv_kernel<false><<<grid, kThreads, 0, st>>>(acc, delta, c.moddown_conv, L, c.np, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+}
+
 }  // namespace
 
 size_t keyswitch_ws_words(const Context &c, uint32_t n_cts, uint32_t L) {
@@ -178,38 +218,17 @@ void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_
     uint64_t *up = x + (size_t)n_cts * L * n;           // [n_cts][beta][LP][N]
     uint64_t *acc = up + (size_t)n_cts * beta * LP * n; // [n_cts][2][LP][N]
     uint64_t *delta = up;                               // reuses up: [n_cts][2][L][N]
-    const LevelKS &ks = c.ks[L];
 
-    // 1. coefficient form of every limb, scaled by the digit factor qhat_i^-1
-    SHM_CUDA(cudaMemcpy2DAsync(x, L * n * 8, d, d_stride * 8, L * n * 8, n_cts, cudaMemcpyDeviceToDevice, st));
-    ntt_inverse(c, x, n_cts * L, L, q_map(L), ks.modup_scale, st);
-    // 2. base conversion of each digit to the rest of QlP
-    SHM_LAUNCHED(1); modup_conv_kernel<<<dim3(n / kThreads, beta, n_cts), kThreads, 0, st>>>(x, d, d_stride, up, ks.modup_conv, L, np,
-                                                                            c.nq, c.log_n, c.pc);
-    SHM_CUDA(cudaGetLastError());
-    // 3. NTT of the converted limbs (digit rows are already NTT form)
-    LimbMap m;
-    for (uint32_t s = 0; s < 512; s++) {
-        if (s >= beta * LP) {
-            m.prime[s] = 255;
-            continue;
-        }
-        uint32_t b = s / LP, j = s % LP;
-        bool own = j >= b * np && j < std::min((b + 1) * np, L);
-        m.prime[s] = own ? 255 : (uint8_t)(j < L ? j : c.nq + (j - L));
-    }
-    ntt_forward(c, up, n_cts * beta * LP, beta * LP, m, st);
+    // 1-3. ModUp: coefficient form scaled by qhat_i^-1, base conversion of each digit to
+    // the rest of QlP, NTT of the converted limbs (digit rows are already NTT form)
+    modup_into(c, d, d_stride, n_cts, L, x, up, st);
     // 4. inner product with the key digits
-    SHM_LAUNCHED(1); launch_inner_product(dim3(n / kThreads, LP), st, up, key, acc, n_cts, L, np, c.nq, beta, c.log_n,
-                                                                      c.pc, nullptr);
-    SHM_CUDA(cudaGetLastError());
+    launch_ip(c, n_cts, L, up, key, acc, nullptr, st);
     // 5. ModDown: INTT of the P limbs (scaled by phat_k^-1), convert to Ql, NTT, combine
     LimbMap mp;
     for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
     ntt_inverse(c, acc, n_cts * 2 * LP, LP, mp, c.moddown_scale, st, L);
-    SHM_LAUNCHED(1); moddown_conv_kernel<<<dim3(n / kThreads, n_cts * 2), kThreads, 0, st>>>(acc, delta, c.moddown_conv, L, np,
-                                                                            c.log_n, c.pc);
-    SHM_CUDA(cudaGetLastError());
+    launch_moddown_conv(c, n_cts * 2, L, acc, delta, st);
     ntt_forward(c, delta, n_cts * 2 * L, L, q_map(L), st);
     SHM_LAUNCHED(1); ks_combine_kernel<<<dim3(n / kThreads, L, n_cts * 2), kThreads, 0, st>>>(acc, delta, o, L, np, c.log_n, c.pc,
                                                                              c.p_inv);
@@ -226,10 +245,7 @@ void modup_into(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n
     const LevelKS &ks = c.ks[L];
     SHM_CUDA(cudaMemcpy2DAsync(x, ln * 8, d, d_stride * 8, ln * 8, n_cts, cudaMemcpyDeviceToDevice, st));
     ntt_inverse(c, x, n_cts * L, L, q_map(L), ks.modup_scale, st);
-    SHM_LAUNCHED(1);
-    modup_conv_kernel<<<dim3(n / kThreads, beta, n_cts), kThreads, 0, st>>>(x, d, d_stride, up, ks.modup_conv, L, np,
-                                                                            c.nq, c.log_n, c.pc);
-    SHM_CUDA(cudaGetLastError());
+    launch_modup_conv(c, n_cts, L, x, d, d_stride, up, st);
     LimbMap m;
     for (uint32_t s = 0; s < 512; s++) {
         if (s >= beta * LP) {
@@ -262,42 +278,19 @@ void apply_galois_hoisted(const Context &c, const uint64_t *ct, uint32_t n_cts, 
     uint64_t *up = x + (size_t)n_cts * L * n;
     uint64_t *acc = up + (size_t)n_cts * beta * LP * n;
     uint64_t *delta = acc + (size_t)n_cts * 2 * LP * n;  // up must survive every element
-    const LevelKS &ks = c.ks[L];
     const uint64_t *d = ct + ln;  // c1 of every ciphertext, stride 2 ln
 
     // ModUp once (identical to keyswitch steps 1-3)
-    SHM_CUDA(cudaMemcpy2DAsync(x, ln * 8, d, 2 * ln * 8, ln * 8, n_cts, cudaMemcpyDeviceToDevice, st));
-    ntt_inverse(c, x, n_cts * L, L, q_map(L), ks.modup_scale, st);
-    SHM_LAUNCHED(1);
-    modup_conv_kernel<<<dim3(n / kThreads, beta, n_cts), kThreads, 0, st>>>(x, d, 2 * ln, up, ks.modup_conv, L, np,
-                                                                            c.nq, c.log_n, c.pc);
-    SHM_CUDA(cudaGetLastError());
-    LimbMap m;
-    for (uint32_t s = 0; s < 512; s++) {
-        if (s >= beta * LP) {
-            m.prime[s] = 255;
-            continue;
-        }
-        uint32_t b = s / LP, j = s % LP;
-        bool own = j >= b * np && j < std::min((b + 1) * np, L);
-        m.prime[s] = own ? 255 : (uint8_t)(j < L ? j : c.nq + (j - L));
-    }
-    ntt_forward(c, up, n_cts * beta * LP, beta * LP, m, st);
+    modup_into(c, d, 2 * ln, n_cts, L, x, up, st);
     LimbMap mp;
     for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
 
     // per element: permuted inner product, ModDown, combine with sigma(c0)
     for (uint32_t e = 0; e < n_elts; e++) {
         const uint32_t *perm = const_cast<Context &>(c).perm(elts[e]);
-        SHM_LAUNCHED(1);
-        launch_inner_product(dim3(n / kThreads, LP), st, up, keys[e], acc, n_cts, L, np, c.nq, beta, c.log_n, c.pc,
-                             perm);
-        SHM_CUDA(cudaGetLastError());
+        launch_ip(c, n_cts, L, up, keys[e], acc, perm, st);
         ntt_inverse(c, acc, n_cts * 2 * LP, LP, mp, c.moddown_scale, st, L);
-        SHM_LAUNCHED(1);
-        moddown_conv_kernel<<<dim3(n / kThreads, n_cts * 2), kThreads, 0, st>>>(acc, delta, c.moddown_conv, L, np,
-                                                                                c.log_n, c.pc);
-        SHM_CUDA(cudaGetLastError());
+        launch_moddown_conv(c, n_cts * 2, L, acc, delta, st);
         ntt_forward(c, delta, n_cts * 2 * L, L, q_map(L), st);
         KsOutput o{outs[e], outs[e] + ln, ct, nullptr, 2 * ln, perm};
         SHM_LAUNCHED(1);

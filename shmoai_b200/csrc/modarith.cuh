@@ -75,6 +75,40 @@ __device__ __forceinline__ void mac(u128 &acc, uint64_t a, uint64_t b) {
     asm("add.cc.u64 %0, %0, %2;\n\taddc.u64 %1, %1, %3;" : "+l"(acc.lo), "+l"(acc.hi) : "l"(lo), "l"(hi));
 }
 
+// Sum of products, generic (Acc<false>: 128-bit accumulator, any 64-bit operands) or for
+// operands below 2^52 (Acc<true>, the limbs of primes below 2^52).  With a = a1 2^32 + a0
+// and b = b1 2^32 + b0 (a1, b1 < 2^20), Acc<true> adds the 32 x 32-bit partial products into
+// three 64-bit sums, hi = sum a1 b1, mid = sum (a0 b1 + a1 b0 + hi32(a0 b0)) and
+// lo = sum lo32(a0 b0), which cannot overflow below 2^11 terms: four wide multiplies and no
+// carry chain per term, one fold at the end.
+template <bool S52>
+struct Acc {
+    u128 v{0, 0};
+    __device__ __forceinline__ void add(uint64_t a, uint64_t b) { mac(v, a, b); }
+    __device__ __forceinline__ u128 get() const { return v; }
+};
+
+template <>
+struct Acc<true> {
+    uint64_t lo = 0, mid = 0, hi = 0;
+    __device__ __forceinline__ void add(uint64_t a, uint64_t b) {
+        const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+        const uint64_t t = (uint64_t)a0 * b0;
+        lo += (uint32_t)t;
+        mid += (t >> 32) + (uint64_t)a0 * b1 + (uint64_t)a1 * b0;
+        hi += (uint64_t)a1 * b1;
+    }
+    __device__ __forceinline__ u128 get() const {
+        u128 x;
+        x.lo = lo + (mid << 32);
+        x.hi = hi + (mid >> 32) + (x.lo < lo ? 1 : 0);
+        return x;
+    }
+};
+
+// every prime of the chain below 2^52: the kernels may use Acc<true>
+constexpr uint64_t kS52PrimeLimit = 1ull << 52;
+
 __device__ __forceinline__ uint64_t barrett(u128 x, const PrimeConst &p) {
     uint64_t t = (x.hi << (64 - p.shift)) | (x.lo >> p.shift);
     uint64_t qh = mulhi64(t, p.mu);

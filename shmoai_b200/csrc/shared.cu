@@ -36,6 +36,7 @@ constexpr int kMaxB = 16;
 constexpr int kIpT = 128;
 constexpr size_t kIpSmem = 32 * 1024;
 
+template <bool S52>
 __global__ void __launch_bounds__(kIpT) ip_multi_kernel(const uint64_t *__restrict__ up,
                                                         const uint64_t *__restrict__ key, uint64_t *__restrict__ acc,
                                                         uint32_t n_cts, uint32_t chunk, uint32_t L, uint32_t np,
@@ -62,16 +63,17 @@ __global__ void __launch_bounds__(kIpT) ip_multi_kernel(const uint64_t *__restri
         for (int b = 0; b < kMaxB; b++)
             if (b < (int)beta) kk[b] = __ldg(kp + (size_t)b * H * QP * n);
         for (uint32_t ct = 0; ct < nc; ct++) {
-            u128 a = {0, 0};
+            Acc<S52> a;
             const uint64_t *s = su + ct * beta * kIpT + threadIdx.x;
 #pragma unroll
             for (int b = 0; b < kMaxB; b++)
-                if (b < (int)beta) mac(a, s[b * kIpT], kk[b]);
-            acc[(((size_t)(c0 + ct) * H + h) * LP + j) * n + k] = barrett(a, p);
+                if (b < (int)beta) a.add(s[b * kIpT], kk[b]);
+            acc[(((size_t)(c0 + ct) * H + h) * LP + j) * n + k] = barrett(a.get(), p);
         }
     }
 }
 
+template <bool S52>
 __global__ void moddown_multi_conv(const uint64_t *__restrict__ acc, uint64_t *__restrict__ delta,
                                    const uint64_t *__restrict__ conv, uint32_t L, uint32_t np, uint32_t log_n,
                                    const PrimeConst *__restrict__ pc) {
@@ -87,11 +89,11 @@ __global__ void moddown_multi_conv(const uint64_t *__restrict__ acc, uint64_t *_
     uint64_t *o = delta + (size_t)poly * L * n + k;
     for (uint32_t j = 0; j < L; j++) {
         const uint64_t *cj = conv + (size_t)j * np;
-        u128 a = {0, 0};
+        Acc<S52> a;
 #pragma unroll
         for (int i = 0; i < 16; i++)
-            if (i < (int)np) mac(a, zv[i], __ldg(cj + i));
-        o[(size_t)j * n] = barrett(a, pc[j]);
+            if (i < (int)np) a.add(zv[i], __ldg(cj + i));
+        o[(size_t)j * n] = barrett(a.get(), pc[j]);
     }
 }
 
@@ -210,15 +212,26 @@ void apply_target(const Context &c, const uint64_t *up, uint32_t n_cts, uint32_t
     const size_t n = c.n;
     const uint32_t np = c.np, LP = L + np;
     const uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_cts, kIpSmem / (beta * kIpT * 8)));
+    const dim3 grid(n / kIpT, LP, (n_cts + chunk - 1) / chunk);
+    const size_t smem = (size_t)chunk * beta * kIpT * 8;
     SHM_LAUNCHED(1);
-    ip_multi_kernel<<<dim3(n / kIpT, LP, (n_cts + chunk - 1) / chunk), kIpT, (size_t)chunk * beta * kIpT * 8, st>>>(
-        up, t.key, acc, n_cts, chunk, L, np, c.nq, beta, H, c.log_n, c.pc, t.perm);
+    if (c.s52)
+        ip_multi_kernel<true><<<grid, kIpT, smem, st>>>(up, t.key, acc, n_cts, chunk, L, np, c.nq, beta, H, c.log_n,
+                                                        c.pc, t.perm);
+    else
+        ip_multi_kernel<false><<<grid, kIpT, smem, st>>>(up, t.key, acc, n_cts, chunk, L, np, c.nq, beta, H, c.log_n,
+                                                         c.pc, t.perm);
     SHM_CUDA(cudaGetLastError());
     LimbMap mp;
     for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
     ntt_inverse(c, acc, n_cts * H * LP, LP, mp, c.moddown_scale, st, L);
     SHM_LAUNCHED(1);
-    moddown_multi_conv<<<dim3(n / kT, n_cts * H), kT, 0, st>>>(acc, delta, c.moddown_conv, L, np, c.log_n, c.pc);
+    if (c.s52)
+        moddown_multi_conv<true><<<dim3(n / kT, n_cts * H), kT, 0, st>>>(acc, delta, c.moddown_conv, L, np, c.log_n,
+                                                                         c.pc);
+    else
+        moddown_multi_conv<false><<<dim3(n / kT, n_cts * H), kT, 0, st>>>(acc, delta, c.moddown_conv, L, np, c.log_n,
+                                                                          c.pc);
     SHM_CUDA(cudaGetLastError());
     ntt_forward(c, delta, n_cts * H * L, L, q_map(L), st);
     SHM_LAUNCHED(1);
