@@ -233,22 +233,34 @@ def run_boot(args, rank, world, dist):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    l0 = lib.shm_kernel_launches()
-    ms = timed_steps(torch, step, args.steps, dist, None)  # a batch is ~1 GB of live data per step > L2
-    launches = lib.shm_kernel_launches() - l0
     _, peak = h.device_memory()
-    out = holder["out"]
+    # eager: one shm_boot_run per step (every kernel launched from the host)
+    eager_ms = timed_steps(torch, step, max(1, args.steps // 2), dist, None)
+    eager_out = holder.pop("out").to_host()
+
+    # the timed path: the same bootstrap recorded once as a CUDA graph (BatchBootstrapper::capture)
+    # and replayed; its output must equal the eager one bit for bit
+    graph, out = bs.capture(ct, S)
+    for _ in range(args.warmup):
+        graph.launch()
+    torch.cuda.synchronize()
+    if not np.array_equal(out.to_host(), eager_out):
+        raise SystemExit("graph replay differs from the eager bootstrap")
+    l0 = lib.shm_kernel_launches()
+    ms = timed_steps(torch, graph.launch, args.steps, dist, None)  # a batch is ~1 GB of live data > L2
+    launches = lib.shm_kernel_launches() - l0
     err = np.abs(h.decrypt(out) - z)
     out_level = out.level
 
-    # end to end through the host C ABI: pinned host input -> device (shm_ct_from_host),
-    # bootstrap (shm_boot_run), device -> pinned host output (shm_ct_to_host), every step
+    # end to end through the host C ABI: pinned host input -> the graph's input batch
+    # (shm_ct_write), graph replay, output -> pinned host memory (shm_ct_to_host), every step
     h_in = torch.from_numpy(ct.to_host().view(np.int64)).pin_memory()
     h_out = torch.empty((out.count, out.size, out.level, h.n), dtype=torch.int64).pin_memory()
 
     def e2e_step():
-        d_in = h.ct_from_ptr(h_in.data_ptr(), ct.count, ct.size, ct.level, ct.scale)
-        bs.run(d_in, S).to_ptr(h_out.data_ptr())
+        ct.write_from_ptr(h_in.data_ptr())
+        graph.launch()
+        out.to_ptr(h_out.data_ptr())
 
     if args.no_extras:
         e2e_ms, roof = ms, None
@@ -259,6 +271,8 @@ def run_boot(args, rank, world, dist):
         ctx = CKKSContext(BOOT["log_n"], primes=h.primes, n_special=BOOT["n_special"], device=dev)
         roof = ntt_roofline(torch, ctx, len(BOOT["bits"]) - BOOT["n_special"])
         ctx.close()
+    graph_kernels = graph.kernels
+    graph.close()
     clocks = clk.summary()
     return {
         "metric": BOOT_METRIC, "value": round(world * B * 1000.0 / ms, 3), "unit": "bootstraps/s",
@@ -269,7 +283,10 @@ def run_boot(args, rank, world, dist):
                                 if S else "boot: S2C-first bootstrap of a batch of ciphertexts per GPU per step"),
                    "batch_per_gpu": B, "shared_a_group": S or None, "N": h.n, "slots": n,
                    "input_primes": BOOT["input_level"], "output_primes": out_level, "Q": "[51]+20x[46]+14x[51]",
-                   "P": "5x[51]", "dnum": h.nq // h.np, "path": "C++ host library (shm_boot_run) over the C ABI",
+                   "P": "5x[51]", "dnum": h.nq // h.np,
+                   "path": "C++ host library over the C ABI: shm_boot_capture once, shm_host_graph_launch per step",
+                   "graph_kernels_per_step": int(graph_kernels),
+                   "eager_ms_per_step": round(eager_ms, 3),
                    "device_gb": {"resident_keys_plan_input": round(resident / 2 ** 30, 2),
                                  "peak": round(peak / 2 ** 30, 2)},
                    "h": BOOT["h"], "evalmod": "Chebyshev deg 47, K=25, 3 double angles",
@@ -544,36 +561,48 @@ def run_prim(args, rank, world, dist):
     ws = torch.empty(max(ctx.workspace_bytes("keyswitch", B, L) // 8 + B * 2 * L * n,
                          ctx.workspace_bytes("rescale", 2 * B, L) // 8), dtype=torch.int64, device="cuda")
     work, rot, rel = ct.clone(), torch.empty_like(ct), torch.empty_like(ct)
+    m = torch.empty(B, 3, L, n, dtype=torch.int64, device="cuda")
     out = torch.empty(B, 2, L - 1, n, dtype=torch.int64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.int64, device="cuda")
+    d_in = ct.clone()
 
-    def chain(src):
-        work.copy_(src)
+    def chain():
+        work.copy_(d_in)
         ctx.ntt_inverse_(work)
         ctx.ntt_forward_(work)
         ctx.rotate(work, 1, gk, out=rot, workspace=ws)
-        m = ctx.multiply(rot, ct2)
+        ctx.multiply(rot, ct2, out=m)
         ctx.relinearize(m, rk, out=rel, workspace=ws)
         ctx.rescale(rel, out=out, workspace=ws)
 
     clk = ClockSampler(dev).start()
     for _ in range(args.warmup):
-        chain(ct)
+        chain()
     torch.cuda.synchronize()
+    eager_ms = timed_steps(torch, chain, args.steps, dist, flush)  # every kernel launched from the host
+    eager_out = out.clone()
+    # the timed path: the chain recorded once as a CUDA graph (shm_graph_begin / _end) and replayed
+    graph = ctx.capture(chain)
+    for _ in range(args.warmup):
+        graph.launch()
+    torch.cuda.synchronize()
+    if not torch.equal(out, eager_out):
+        raise SystemExit("graph replay differs from the eager chain")
     l0 = lib.shm_kernel_launches()
-    ms = timed_steps(torch, lambda: chain(ct), args.steps, dist, flush)
+    ms = timed_steps(torch, graph.launch, args.steps, dist, flush)
     launches = lib.shm_kernel_launches() - l0
     h_in = ct.cpu().pin_memory()
     h_out = torch.empty(out.shape, dtype=torch.int64).pin_memory()
-    d_in = torch.empty_like(ct)
 
     def e2e():
         d_in.copy_(h_in, non_blocking=True)
-        chain(d_in)
+        graph.launch()
         h_out.copy_(out, non_blocking=True)
 
     e2e()
     e2e_ms = timed_steps(torch, e2e, args.steps, dist, None)
+    graph_kernels = graph.kernels
+    graph.close()
     roof = ntt_roofline(torch, ctx, L)
     clocks = clk.summary()
     return {
@@ -583,7 +612,9 @@ def run_prim(args, rank, world, dist):
         "data": "synthetic (seeded uniform RNS residues; random key material)",
         "config": {"workload": "prim: config-1 chain, one ciphertext per GPU per step", "N": n, "L": L,
                    "special_primes": ctx.np, "dnum": dnum, "batch_per_gpu": B,
-                   "l2": "flushed between timed steps (256 MiB write)"},
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "path": "CUDA graph of the chain (shm_graph_begin / shm_graph_end), one replay per step",
+                   "graph_kernels_per_step": int(graph_kernels), "eager_ms_per_step": round(eager_ms, 4)},
         "e2e": {"value": round(world * B * 1000.0 / e2e_ms, 3), "unit": "chains/s",
                 "h2d_bytes_per_step": int(h_in.numel() * 8), "d2h_bytes_per_step": int(h_out.numel() * 8)},
         "gpu_launches": int(launches), "roofline": roof, "clocks": clocks,

@@ -19,6 +19,7 @@
 
 #include <complex>
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -294,6 +295,33 @@ struct BootstrapParams {
 class LinearTransform;
 
 // S2C-first batched bootstrapping, ordinary and shared-a (BatchBootstrap.cuh:674-819).
+// ------------------------------------------------------------------ CUDA graphs
+
+// One recorded batch of device work, replayed with a single launch.  Graph(base, fn) makes a
+// private stream, a view of base's context on it and an evaluator over the view with base's
+// keys, runs fn(ev) once as is (workspaces grow, lazily built tables fill), then once under
+// stream capture.  launch() replays the capture on base's stream.  fn must read and write
+// only buffers that outlive the graph, free everything it allocates, and allocate the same
+// sizes on every run.  No reference counterpart: the reference launches every kernel from
+// the host per call.
+class Graph {
+   public:
+    Graph(const Evaluator &base, const std::function<void(const Evaluator &ev)> &fn);
+    ~Graph();
+    Graph(const Graph &) = delete;
+    Graph &operator=(const Graph &) = delete;
+    void launch() const;
+    uint64_t kernels() const;
+
+   private:
+    const Context &base_;
+    void *stream_ = nullptr;
+    std::unique_ptr<Context> view_;
+    std::unique_ptr<Encoder> enc_;
+    std::unique_ptr<Evaluator> ev_;
+    shm_graph *g_ = nullptr;
+};
+
 class BatchBootstrapper {
    public:
     BatchBootstrapper(Evaluator &ev, BootstrapParams p = BootstrapParams());
@@ -313,6 +341,10 @@ class BatchBootstrapper {
                                             const Evaluator *ev = nullptr) const;
     // EvalMod of ciphertexts holding t / K: c_fin * sin(2 pi t) read at scale Delta
     Ciphertext evalmod(const Ciphertext &x, const Evaluator *ev = nullptr) const;
+    // A CUDA graph of one bootstrap of `in` (members = 0: ordinary ciphertexts).  `out`
+    // receives a buffer of the output's shape, rewritten by every Graph::launch; write the
+    // next batch into `in` (same count and level) between launches.
+    std::unique_ptr<Graph> capture(const Ciphertext &in, uint32_t members, Ciphertext &out) const;
     const BootstrapParams &params() const { return p_; }
 
    private:

@@ -237,6 +237,24 @@ int shm_pool_usage(const shm_context *ctx, size_t *reserved, size_t *used, size_
 int shm_stream_create(const shm_context *ctx, void **stream);
 int shm_stream_destroy(const shm_context *ctx, void *stream);
 
+/* ---- CUDA graphs of whole operation sequences ----
+ * No reference counterpart: the reference issues every kernel from the host per call
+ * (thirdparty/phantom-fhe/src/evaluate.cu).  Between shm_graph_begin and shm_graph_end the
+ * calls that work on `stream` are recorded instead of run; shm_graph_launch then replays all
+ * of them with one launch, on any stream.  The recorded calls must make no host round trip
+ * (no host copies, no synchronisation) and must free on the stream, before shm_graph_end,
+ * every buffer they allocate with shm_malloc; run the sequence once outside the capture first
+ * so that lazily built tables exist.  `stream` must come from shm_stream_create (the legacy
+ * default stream cannot be captured).  shm_graph_begin releases the context pool's unused
+ * blocks: the graph's own allocations come from the device's graph memory. */
+typedef struct shm_graph shm_graph;
+int shm_graph_begin(const shm_context *ctx, void *stream);
+int shm_graph_end(const shm_context *ctx, void *stream, shm_graph **out);
+int shm_graph_launch(const shm_graph *g, void *stream);
+/* kernels recorded in the graph (added to shm_kernel_launches by every replay) */
+uint64_t shm_graph_kernels(const shm_graph *g);
+void shm_graph_destroy(shm_graph *g);
+
 /* ---- sampling (key generation, encryption) ----
  * Counter-based: value i of a call is a function of (seed, i) only, so the GPU and the
  * CPU restatement draw identical keys and ciphertexts.  Distributions as in the

@@ -65,6 +65,9 @@ int shm_host_decrypt(shm_host *h, const shm_ct *ct, double *re, double *im);
 int shm_ct_from_host(shm_host *h, const uint64_t *data, uint32_t count, uint32_t size, uint32_t L, double scale,
                      int shared, shm_ct **out);
 int shm_ct_to_host(shm_host *h, const shm_ct *ct, uint64_t *data);
+/* overwrite the residues of an existing batch from host words laid out as shm_ct_to_host
+ * writes them (same count, size and level) */
+int shm_ct_write(shm_host *h, shm_ct *ct, const uint64_t *data);
 int shm_ct_info(const shm_ct *ct, uint32_t *count, uint32_t *size, uint32_t *L, double *scale, int *shared);
 /* a device copy of ciphertexts [first, first + count) of a batch */
 int shm_host_slice(shm_host *h, const shm_ct *ct, uint32_t first, uint32_t count, shm_ct **out);
@@ -97,6 +100,18 @@ int shm_boot_galois_elts(const shm_boot *b, uint32_t *out, uint32_t cap, uint32_
  * members = n: shared-a groups of n consecutive ciphertexts (keys from
  * shm_host_gen_shared_keys) */
 int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out);
+
+/* CUDA graph of one shm_boot_run of `in` (shmoai::BatchBootstrapper::capture): the
+ * bootstrap runs once on the host's stream and once on a private stream before it is
+ * recorded; *out receives the output ciphertext, which every shm_host_graph_launch
+ * rewrites.  Put the next batch into `in` with shm_ct_write between launches; `in` must
+ * outlive the graph. */
+typedef struct shm_host_graph shm_host_graph;
+int shm_boot_capture(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out, shm_host_graph **graph);
+/* replay on the host's stream */
+int shm_host_graph_launch(shm_host_graph *g);
+uint64_t shm_host_graph_kernels(const shm_host_graph *g);
+void shm_host_graph_destroy(shm_host_graph *g);
 
 /* self-check of the slot-transform factorisation at 2^log_slots slots (max error) */
 double shm_slot_transform_selfcheck(uint32_t log_slots);

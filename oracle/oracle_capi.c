@@ -144,6 +144,38 @@ int shm_stream_destroy(const shm_context *ctx, void *stream) {
     return SHM_OK;
 }
 
+/* CUDA graphs record device work; host arithmetic has nothing to record, so the oracle
+ * refuses them (the graph tests run on the CUDA library only) */
+struct shm_graph {
+    int unused;
+};
+
+int shm_graph_begin(const shm_context *ctx, void *stream) {
+    (void)ctx;
+    (void)stream;
+    return fail("CUDA graphs need the CUDA library");
+}
+
+int shm_graph_end(const shm_context *ctx, void *stream, shm_graph **out) {
+    (void)ctx;
+    (void)stream;
+    if (out) *out = NULL;
+    return fail("CUDA graphs need the CUDA library");
+}
+
+int shm_graph_launch(const shm_graph *g, void *stream) {
+    (void)g;
+    (void)stream;
+    return fail("CUDA graphs need the CUDA library");
+}
+
+uint64_t shm_graph_kernels(const shm_graph *g) {
+    (void)g;
+    return 0;
+}
+
+void shm_graph_destroy(shm_graph *g) { (void)g; }
+
 /* ---- sampling (same function as shmoai_b200/csrc/sampling.cu) */
 
 static inline uint64_t mix64(uint64_t seed, uint64_t idx) {

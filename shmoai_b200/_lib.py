@@ -76,6 +76,13 @@ def _declare(L):
         "shm_fmt_switch_backward_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),
         "shm_fmt_switch_backward": (ctypes.c_int, [_P, _P, _U32, _U32, ctypes.POINTER(_P), _P, _U32, _P, _SZ,
                                                    _P]),
+        "shm_stream_create": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+        "shm_stream_destroy": (ctypes.c_int, [_P, _P]),
+        "shm_graph_begin": (ctypes.c_int, [_P, _P]),
+        "shm_graph_end": (ctypes.c_int, [_P, _P, ctypes.POINTER(_P)]),
+        "shm_graph_launch": (ctypes.c_int, [_P, _P]),
+        "shm_graph_kernels": (ctypes.c_uint64, [_P]),
+        "shm_graph_destroy": (None, [_P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -42,6 +42,32 @@ def to_host(t: torch.Tensor) -> np.ndarray:
     return t.detach().cpu().numpy().view(np.uint64)
 
 
+class Graph:
+    """A recorded sequence of library calls (shm_graph); launch() replays it with one launch."""
+
+    def __init__(self, ctx: "CKKSContext", handle, stream):
+        self._ctx, self._g, self._s = ctx, handle, stream
+
+    @property
+    def kernels(self) -> int:
+        return int(lib().shm_graph_kernels(self._g))
+
+    def launch(self, stream=None):
+        check(lib().shm_graph_launch(self._g, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_g", None):
+            lib().shm_graph_destroy(self._g)
+            lib().shm_stream_destroy(self._ctx._h, self._s)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class CKKSContext:
     """Device context over Q (n_q primes) followed by special primes P (n_p)."""
 
@@ -76,6 +102,32 @@ class CKKSContext:
             self.close()
         except Exception:
             pass
+
+    def capture(self, fn) -> "Graph":
+        """A CUDA graph (shm_graph_begin / shm_graph_end) of the library calls fn() makes.
+        fn runs twice on a private stream, once as is and once under capture; it must
+        allocate nothing (pass `out` and `workspace` tensors) and only touch tensors that
+        outlive the graph.  Graph.launch() replays it on the current stream."""
+        s = ctypes.c_void_p()
+        check(lib().shm_stream_create(self._h, ctypes.byref(s)))
+        ext = torch.cuda.ExternalStream(s.value, device=self.device)
+        torch.cuda.synchronize(self.device)  # inputs made on other streams are complete
+        g = ctypes.c_void_p()
+        try:
+            with torch.cuda.stream(ext):
+                fn()
+                check(lib().shm_graph_begin(self._h, s))
+                try:
+                    fn()
+                finally:
+                    rc = lib().shm_graph_end(self._h, s, ctypes.byref(g))
+                check(rc)
+        except BaseException:
+            if g.value:
+                lib().shm_graph_destroy(g)
+            lib().shm_stream_destroy(self._h, s)
+            raise
+        return Graph(self, g, s)
 
     # ---------------- helpers ----------------
     def empty(self, *shape) -> torch.Tensor:
@@ -123,11 +175,11 @@ class CKKSContext:
         check(lib().shm_multiply_plain(self._h, _ptr(ct), _ptr(pt), _ptr(out), p, L, _stream(stream)))
         return out
 
-    def multiply(self, a, b, stream=None):
+    def multiply(self, a, b, out=None, stream=None):
         """[n][2][L][N] x [n][2][L][N] -> [n][3][L][N] (a single ct may omit the batch axis)."""
         p, L = self._levels(a)
         n_cts = p // 2
-        out = self.empty(*(a.shape[:-3] + (3, L, self.n)))
+        out = self.empty(*(a.shape[:-3] + (3, L, self.n))) if out is None else out
         check(lib().shm_multiply(self._h, _ptr(a), _ptr(b), _ptr(out), n_cts, L, _stream(stream)))
         return out
 

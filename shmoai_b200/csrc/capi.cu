@@ -712,6 +712,74 @@ int shm_stream_destroy(const shm_context *ctx, void *stream) {
     });
 }
 
+// ---- CUDA graphs
+
+struct shm_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;
+    int device = 0;
+};
+
+int shm_graph_begin(const shm_context *ctx, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        if (!stream) throw std::invalid_argument("the legacy default stream cannot be captured");
+        set_device(c);
+        // blocks the pool keeps for reuse would sit beside the graph's own allocations
+        SHM_CUDA(cudaStreamSynchronize(S(stream)));
+        SHM_CUDA(cudaMemPoolTrimTo(c.mempool(), 0));
+        SHM_CUDA(cudaStreamBeginCapture(S(stream), cudaStreamCaptureModeThreadLocal));
+    });
+}
+
+int shm_graph_end(const shm_context *ctx, void *stream, shm_graph **out) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        if (!out) throw std::invalid_argument("null output pointer");
+        *out = nullptr;
+        set_device(c);
+        std::unique_ptr<shm_graph> g(new shm_graph);
+        g->device = c.device;
+        SHM_CUDA(cudaStreamEndCapture(S(stream), &g->graph));
+        size_t n = 0;
+        SHM_CUDA(cudaGraphGetNodes(g->graph, nullptr, &n));
+        std::vector<cudaGraphNode_t> nodes(n);
+        if (n) SHM_CUDA(cudaGraphGetNodes(g->graph, nodes.data(), &n));
+        for (cudaGraphNode_t nd : nodes) {
+            cudaGraphNodeType t;
+            SHM_CUDA(cudaGraphNodeGetType(nd, &t));
+            if (t == cudaGraphNodeTypeKernel) g->kernels++;
+        }
+        // no auto-free: a replay fails loudly if the recorded calls left an allocation alive
+        SHM_CUDA(cudaGraphInstantiateWithFlags(&g->exec, g->graph, 0));
+        *out = g.release();
+    });
+}
+
+int shm_graph_launch(const shm_graph *g, void *stream) {
+    return guard([&] {
+        if (!g || !g->exec) throw std::invalid_argument("null graph");
+        SHM_CUDA(cudaSetDevice(g->device));
+        SHM_CUDA(cudaGraphLaunch(g->exec, S(stream)));
+        SHM_LAUNCHED(g->kernels);
+    });
+}
+
+uint64_t shm_graph_kernels(const shm_graph *g) { return g ? g->kernels : 0; }
+
+void shm_graph_destroy(shm_graph *g) {
+    if (!g) return;
+    cudaSetDevice(g->device);
+    if (g->exec) {
+        cudaDeviceSynchronize();  // a replay may still run
+        cudaGraphExecDestroy(g->exec);
+    }
+    if (g->graph) cudaGraphDestroy(g->graph);
+    cudaDeviceGraphMemTrim(g->device);
+    delete g;
+}
+
 // ---- sampling and lifting
 
 int shm_sample_uniform(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed,

@@ -77,6 +77,11 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_boot_destroy": (None, [_P]),
         "shm_boot_galois_elts": (i32, [_P, ctypes.POINTER(_U32), _U32, ctypes.POINTER(_U32)]),
         "shm_boot_run": (i32, [_P, _P, _U32, pp]),
+        "shm_boot_capture": (i32, [_P, _P, _U32, pp, pp]),
+        "shm_host_graph_launch": (i32, [_P]),
+        "shm_host_graph_kernels": (ctypes.c_uint64, [_P]),
+        "shm_host_graph_destroy": (None, [_P]),
+        "shm_ct_write": (i32, [_P, _P, u64p]),
         "shm_slot_transform_selfcheck": (ctypes.c_double, [_U32]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
@@ -262,6 +267,11 @@ class Ct:
         self.host._check(self.host.lib.shm_ct_to_host(self.host._h, self._c,
                                                       ctypes.cast(ptr, ctypes.POINTER(ctypes.c_uint64))))
 
+    def write_from_ptr(self, ptr: int):
+        """Overwrite the batch's residues from host memory at `ptr` (the to_ptr layout)."""
+        self.host._check(self.host.lib.shm_ct_write(self.host._h, self._c,
+                                                    ctypes.cast(ptr, ctypes.POINTER(ctypes.c_uint64))))
+
     def device_ptr(self) -> int:
         return int(self.host.lib.shm_ct_device_data(self._c) or 0)
 
@@ -296,10 +306,42 @@ class Bootstrapper:
         self.host._check(self.host.lib.shm_boot_run(self._b, ct._c, members, ctypes.byref(o)))
         return Ct(self.host, o)
 
+    def capture(self, ct: Ct, members: int = 0) -> tuple["Graph", Ct]:
+        """A CUDA graph of run(ct, members) and the output batch every launch rewrites;
+        write the next input into `ct` (Ct.write_from_ptr) between launches."""
+        o, g = _P(), _P()
+        self.host._check(self.host.lib.shm_boot_capture(self._b, ct._c, members, ctypes.byref(o), ctypes.byref(g)))
+        return Graph(self.host, g, keep=ct), Ct(self.host, o)
+
     def close(self):
         if getattr(self, "_b", None):
             self.host.lib.shm_boot_destroy(self._b)
             self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    """A recorded batch of device work (shm_host_graph); launch() replays it on the host's stream."""
+
+    def __init__(self, host: Host, handle, keep=None):
+        self.host, self._g, self._keep = host, handle, keep  # the captured input must outlive the graph
+
+    @property
+    def kernels(self) -> int:
+        return int(self.host.lib.shm_host_graph_kernels(self._g))
+
+    def launch(self):
+        self.host._check(self.host.lib.shm_host_graph_launch(self._g))
+
+    def close(self):
+        if getattr(self, "_g", None):
+            self.host.lib.shm_host_graph_destroy(self._g)
+            self._g = None
 
     def __del__(self):
         try:

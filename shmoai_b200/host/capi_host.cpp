@@ -32,6 +32,10 @@ struct shm_boot {
     std::unique_ptr<BatchBootstrapper> b;
 };
 
+struct shm_host_graph {
+    std::unique_ptr<Graph> g;
+};
+
 struct shm_server {
     std::unique_ptr<Server> s;
 };
@@ -240,6 +244,16 @@ int shm_ct_info(const shm_ct *ct, uint32_t *count, uint32_t *size, uint32_t *L, 
     });
 }
 
+int shm_ct_write(shm_host *h, shm_ct *ct, const uint64_t *data) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!ct) throw Error("null ciphertext handle");
+        Ciphertext &c = ct->ct;
+        hh.ctx->check(shm_memcpy(hh.ctx->handle(), c.data.data(), data, c.polys() * c.L * hh.ctx->n * 8,
+                                 SHM_COPY_H2D, hh.ctx->stream()));
+    });
+}
+
 const uint64_t *shm_ct_device_data(const shm_ct *ct) { return ct ? ct->ct.data.data() : nullptr; }
 
 void shm_ct_destroy(shm_ct *ct) { delete ct; }
@@ -345,6 +359,29 @@ int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out) 
         }
     });
 }
+
+int shm_boot_capture(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out, shm_host_graph **graph) {
+    return guard([&] {
+        if (!b) throw Error("null bootstrapper");
+        if (!graph || !out) throw Error("null output handle");
+        if (members) b->h->use_shared(members);
+        Ciphertext o;
+        std::unique_ptr<Graph> g = b->b->capture(C(in), members, o);
+        *graph = new shm_host_graph{std::move(g)};
+        put(out, std::move(o));
+    });
+}
+
+int shm_host_graph_launch(shm_host_graph *g) {
+    return guard([&] {
+        if (!g) throw Error("null graph");
+        g->g->launch();
+    });
+}
+
+uint64_t shm_host_graph_kernels(const shm_host_graph *g) { return g ? g->g->kernels() : 0; }
+
+void shm_host_graph_destroy(shm_host_graph *g) { delete g; }
 
 int shm_server_create(shm_host *h, shm_boot *boot, size_t hbm_budget_bytes, uint32_t slots, uint32_t max_merge,
                       shm_server **out) {
