@@ -188,16 +188,18 @@ def ntt_roofline(torch, ctx, L, limbs_target=4096):
 # bootstrapping workload
 
 
-def setup_boot(dev, rank, shared=0):
+def setup_boot(dev, rank, shared=0, tune_batch=0):
     """C++ host (context, secret key, relinearisation key) and bootstrapper at the
     reference parameters; with shared = n the Sh-Galois, format and backward keys of
-    shared-a groups of n replace the Galois keys."""
+    shared-a groups of n replace the Galois keys.  tune_batch > 0 autotunes the kernel tiles
+    and the BSGS split for batches of that size first (the split decides the keys)."""
     from shmoai_b200.host import Bootstrapper, Host
 
     h = Host(BOOT["log_n"], bits=BOOT["bits"], n_special=BOOT["n_special"], hamming_weight=BOOT["h"],
              seed=0x5EED + rank, device=dev)
     h.gen_relin_key()
     bs = Bootstrapper(h, BOOT["scale"], BOOT["input_level"])
+    bs.tuning = bs.tune(tune_batch, shared) if tune_batch else []
     if shared:
         h.gen_shared_keys(shared, bs.galois_elts(), hamming_weight=BOOT["h"])
     else:
@@ -218,7 +220,7 @@ def run_boot(args, rank, world, dist):
     B = args.batch
     if S and B % S:
         raise SystemExit("--batch must be a multiple of --shared")
-    h, bs = setup_boot(dev, rank, S)
+    h, bs = setup_boot(dev, rank, S, tune_batch=0 if args.no_tune else B)
     rng = np.random.default_rng(1000 + rank)
     n = h.n // 2
     z = rng.uniform(-1, 1, (B, n)) + 1j * rng.uniform(-1, 1, (B, n))
@@ -235,7 +237,7 @@ def run_boot(args, rank, world, dist):
     torch.cuda.synchronize()
     _, peak = h.device_memory()
     # eager: one shm_boot_run per step (every kernel launched from the host)
-    eager_ms = timed_steps(torch, step, max(1, args.steps // 2), dist, None)
+    eager_ms = timed_steps(torch, step, args.steps, dist, None)
     eager_out = holder.pop("out").to_host()
 
     # the timed path: the same bootstrap recorded once as a CUDA graph (BatchBootstrapper::capture)
@@ -287,6 +289,9 @@ def run_boot(args, rank, world, dist):
                    "path": "C++ host library over the C ABI: shm_boot_capture once, shm_host_graph_launch per step",
                    "graph_kernels_per_step": int(graph_kernels),
                    "eager_ms_per_step": round(eager_ms, 3),
+                   "autotune": {r["knob"]: r["candidates"][r["chosen"]] for r in bs.tuning} or None,
+                   "autotune_ms": {r["knob"]: dict(zip(r["candidates"], [round(t, 3) for t in r["ms"]]))
+                                   for r in bs.tuning} or None,
                    "device_gb": {"resident_keys_plan_input": round(resident / 2 ** 30, 2),
                                  "peak": round(peak / 2 ** 30, 2)},
                    "h": BOOT["h"], "evalmod": "Chebyshev deg 47, K=25, 3 double angles",
@@ -749,6 +754,7 @@ def main():
     ap.add_argument("--shared", type=int, default=8,
                     help="boot: shared-a group size n (0 = ordinary ciphertexts)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="boot: skip the autotuner (default tiles and BSGS split)")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the step only (no e2e, roofline or CPU legs): used for ncu launch lists")
     ap.add_argument("--small", action="store_true",

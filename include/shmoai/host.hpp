@@ -290,11 +290,13 @@ struct BootstrapParams {
     int degree = 47;                  // Chebyshev degree
     int double_angles = 3;
     double F = 1.0 / 16;  // amplitude factor of SlotToCoeff (Bootstrapper.cuh:31)
+    // baby-step count g1 of each slot-transform layer (S2C 0-2, C2S 3-5); 0 = the power of two
+    // nearest above sqrt(diagonals); BatchBootstrapper::tune sets them
+    int bsgs_g1[6] = {0, 0, 0, 0, 0, 0};
 };
 
 class LinearTransform;
 
-// S2C-first batched bootstrapping, ordinary and shared-a (BatchBootstrap.cuh:674-819).
 // ------------------------------------------------------------------ CUDA graphs
 
 // One recorded batch of device work, replayed with a single launch.  Graph(base, fn) makes a
@@ -322,6 +324,16 @@ class Graph {
     shm_graph *g_ = nullptr;
 };
 
+// One autotuning decision: the candidates, their milliseconds (measured for the kernel
+// tiles, modelled from measured rotation costs for the BSGS splits) and the pick.
+struct TuneRecord {
+    std::string knob;
+    std::vector<std::string> candidates;
+    std::vector<double> ms;
+    size_t chosen = 0;
+};
+
+// S2C-first batched bootstrapping, ordinary and shared-a (BatchBootstrap.cuh:674-819).
 class BatchBootstrapper {
    public:
     BatchBootstrapper(Evaluator &ev, BootstrapParams p = BootstrapParams());
@@ -341,6 +353,14 @@ class BatchBootstrapper {
                                             const Evaluator *ev = nullptr) const;
     // EvalMod of ciphertexts holding t / K: c_fin * sin(2 pi t) read at scale Delta
     Ciphertext evalmod(const Ciphertext &x, const Evaluator *ev = nullptr) const;
+    // Autotuning for batches of `count` ciphertexts (members per shared-a group, 0 =
+    // ordinary): the NTT tile and, for shared-a, the Sh-Rot inner-product chunk (timed on
+    // scratch data), then each slot-transform layer's BSGS split, modelled from a hoisted
+    // ModUp and a per-step key switch timed at the layer's level; re-prepares the layers.
+    // The split decides the rotation steps, so call it before generating Galois keys.
+    std::vector<TuneRecord> tune(uint32_t count, uint32_t members);
+    // a stored split (BootstrapParams::bsgs_g1 layout); re-prepares the layers
+    void set_split(const int g1[6]);
     // A CUDA graph of one bootstrap of `in` (members = 0: ordinary ciphertexts).  `out`
     // receives a buffer of the output's shape, rewritten by every Graph::launch; write the
     // next batch into `in` (same count and level) between launches.

@@ -255,6 +255,26 @@ int shm_graph_launch(const shm_graph *g, void *stream);
 uint64_t shm_graph_kernels(const shm_graph *g);
 void shm_graph_destroy(shm_graph *g);
 
+/* ---- autotuning of kernel tiles ----
+ * No reference counterpart (its launch shapes are fixed).  Times every candidate of one
+ * knob with CUDA events on scratch data shaped like the caller's workload and keeps the
+ * fastest for this context; later calls on any stream use it.  Synchronises the device.
+ *   SHM_TUNE_NTT_TILE  tile variant of the NTT kernels, candidates 0..3 = (columns per CTA,
+ *                      minimum resident CTAs per SM) (16, 4), (16, 3), (8, 8), (8, 6);
+ *                      workload: forward + inverse NTT of `size` limbs.
+ *   SHM_TUNE_IP_CHUNK  shared memory of one Sh-Rot inner-product block, candidates 0..3 =
+ *                      16, 32, 64, 96 KB (more groups of a chunk share each key read);
+ *                      workload: `size` groups of `members` at `level` primes.
+ * times (NULL or room for `cap` values) receives the candidates' milliseconds in order;
+ * *chosen the winner's index. */
+#define SHM_TUNE_NTT_TILE 0
+#define SHM_TUNE_IP_CHUNK 1
+int shm_autotune(shm_context *ctx, int knob, uint32_t size, uint32_t level, uint32_t members, float *times,
+                 uint32_t cap, uint32_t *chosen);
+/* the candidate index a knob uses now / force one (e.g. a stored tuning result) */
+int shm_tune_get(const shm_context *ctx, int knob, uint32_t *index);
+int shm_tune_set(shm_context *ctx, int knob, uint32_t index);
+
 /* ---- sampling (key generation, encryption) ----
  * Counter-based: value i of a call is a function of (seed, i) only, so the GPU and the
  * CPU restatement draw identical keys and ciphertexts.  Distributions as in the

@@ -100,6 +100,16 @@ int shm_boot_galois_elts(const shm_boot *b, uint32_t *out, uint32_t cap, uint32_
  * members = n: shared-a groups of n consecutive ciphertexts (keys from
  * shm_host_gen_shared_keys) */
 int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out);
+/* autotuning for batches of `count` (shmoai::BatchBootstrapper::tune): NTT tile, Sh-Rot
+ * inner-product chunk, BSGS split per slot-transform layer; call before generating the
+ * Galois / Sh-Galois keys (shm_boot_galois_elts changes with the split).  Writes a JSON
+ * array of {"knob", "candidates", "ms", "chosen"} into `json` (NUL-terminated, truncated at
+ * cap); *needed (may be NULL) = the full length + 1. */
+int shm_boot_tune(shm_boot *b, uint32_t count, uint32_t members, char *json, size_t cap, size_t *needed);
+/* the BSGS baby-step counts of the six slot-transform layers (S2C 0-2, C2S 3-5; 0 = default):
+ * read the tuned split, or set a stored one (re-prepares the layers) */
+int shm_boot_get_split(const shm_boot *b, int *g1);
+int shm_boot_set_split(shm_boot *b, const int *g1);
 
 /* CUDA graph of one shm_boot_run of `in` (shmoai::BatchBootstrapper::capture): the
  * bootstrap runs once on the host's stream and once on a private stream before it is

@@ -176,6 +176,38 @@ uint64_t shm_graph_kernels(const shm_graph *g) {
 
 void shm_graph_destroy(shm_graph *g) { (void)g; }
 
+/* kernel tiles do not exist on the host: the knobs are remembered (so the host library's
+ * tuning code runs unchanged) and every candidate reports zero time */
+static uint32_t g_tune[2];
+
+int shm_autotune(shm_context *ctx, int knob, uint32_t size, uint32_t level, uint32_t members, float *times,
+                 uint32_t cap, uint32_t *chosen) {
+    (void)ctx;
+    (void)size;
+    (void)level;
+    (void)members;
+    if (knob != SHM_TUNE_NTT_TILE && knob != SHM_TUNE_IP_CHUNK) return fail("unknown tuning knob");
+    for (uint32_t i = 0; times && i < cap && i < 4; i++) times[i] = 0.0f;
+    if (chosen) *chosen = g_tune[knob];
+    return SHM_OK;
+}
+
+int shm_tune_get(const shm_context *ctx, int knob, uint32_t *index) {
+    (void)ctx;
+    if (knob != SHM_TUNE_NTT_TILE && knob != SHM_TUNE_IP_CHUNK) return fail("unknown tuning knob");
+    if (!index) return fail("null output pointer");
+    *index = g_tune[knob];
+    return SHM_OK;
+}
+
+int shm_tune_set(shm_context *ctx, int knob, uint32_t index) {
+    (void)ctx;
+    if (knob != SHM_TUNE_NTT_TILE && knob != SHM_TUNE_IP_CHUNK) return fail("unknown tuning knob");
+    if (index >= 4) return fail("candidate out of range");
+    g_tune[knob] = index;
+    return SHM_OK;
+}
+
 /* ---- sampling (same function as shmoai_b200/csrc/sampling.cu) */
 
 static inline uint64_t mix64(uint64_t seed, uint64_t idx) {

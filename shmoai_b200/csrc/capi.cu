@@ -768,6 +768,59 @@ int shm_graph_launch(const shm_graph *g, void *stream) {
 
 uint64_t shm_graph_kernels(const shm_graph *g) { return g ? g->kernels : 0; }
 
+// ---- autotuning
+
+int shm_autotune(shm_context *ctx, int knob, uint32_t size, uint32_t level, uint32_t members, float *times,
+                 uint32_t cap, uint32_t *chosen) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        set_device(c);
+        std::vector<float> ms;
+        uint32_t best;
+        if (knob == SHM_TUNE_NTT_TILE)
+            best = shm::tune_ntt_tile(c, size, ms);
+        else if (knob == SHM_TUNE_IP_CHUNK)
+            best = shm::tune_ip_chunk(c, size, level, members, ms);
+        else
+            throw std::invalid_argument("unknown tuning knob");
+        for (uint32_t i = 0; times && i < cap && i < ms.size(); i++) times[i] = ms[i];
+        if (chosen) *chosen = best;
+    });
+}
+
+int shm_tune_get(const shm_context *ctx, int knob, uint32_t *index) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        if (!index) throw std::invalid_argument("null output pointer");
+        if (knob == SHM_TUNE_NTT_TILE) {
+            *index = (uint32_t)c.ntt_variant;
+        } else if (knob == SHM_TUNE_IP_CHUNK) {
+            const uint32_t *b = std::begin(shm::kIpChunkCandidates), *e = std::end(shm::kIpChunkCandidates);
+            *index = (uint32_t)(std::find(b, e, c.ip_chunk_bytes) - b);
+        } else {
+            throw std::invalid_argument("unknown tuning knob");
+        }
+    });
+}
+
+int shm_tune_set(shm_context *ctx, int knob, uint32_t index) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        set_device(c);
+        if (knob == SHM_TUNE_NTT_TILE) {
+            if (index >= (uint32_t)shm::kNttVariantCount) throw std::invalid_argument("tile variant out of range");
+            SHM_CUDA(cudaDeviceSynchronize());  // launches in flight keep their shape
+            c.ntt_variant = (int)index;
+        } else if (knob == SHM_TUNE_IP_CHUNK) {
+            if (index >= std::size(shm::kIpChunkCandidates)) throw std::invalid_argument("chunk candidate out of range");
+            SHM_CUDA(cudaDeviceSynchronize());
+            c.ip_chunk_bytes = shm::kIpChunkCandidates[index];
+        } else {
+            throw std::invalid_argument("unknown tuning knob");
+        }
+    });
+}
+
 void shm_graph_destroy(shm_graph *g) {
     if (!g) return;
     cudaSetDevice(g->device);

@@ -44,6 +44,8 @@ struct Context {
     uint32_t log_n = 0, n = 0, nq = 0, np = 0, dnum = 0;
     std::vector<uint64_t> primes;       // nq + np
     bool s52 = false;                   // every prime below kS52PrimeLimit (Acc<true> kernels)
+    int ntt_variant = 0;                // index into kNttVariants (set by the autotuner)
+    uint32_t ip_chunk_bytes = 32768;    // shared memory per Sh-Rot inner-product block (autotuned)
     std::vector<PrimeConst> h_pc;       // host copy
     PrimeConst *pc = nullptr;           // [QP]
     uint64_t *tw = nullptr;             // [QP][4][N]
@@ -161,5 +163,13 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
                     uint32_t L, void *ws, uint64_t max_abs_w, cudaStream_t st);
 int ctpt_tc_error(void *ws, cudaStream_t st);
 size_t ctpt_ws_words(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);
+// acc [n_cts][H][LP][N] = inner products of up [n_cts][beta][LP][N] with key [beta][H][QP][N]
+void ip_multi(const Context &c, const uint64_t *up, const uint64_t *key, uint64_t *acc, uint32_t n_cts, uint32_t L,
+              uint32_t beta, uint32_t H, const uint32_t *perm, cudaStream_t st);
+
+// autotuning (tune.cu): time the candidates of one knob, keep the fastest in the context
+constexpr uint32_t kIpChunkCandidates[] = {16384, 32768, 65536, 98304};
+uint32_t tune_ntt_tile(Context &c, uint32_t rows, std::vector<float> &ms);
+uint32_t tune_ip_chunk(Context &c, uint32_t groups, uint32_t L, uint32_t members, std::vector<float> &ms);
 
 }  // namespace shm

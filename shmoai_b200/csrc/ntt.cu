@@ -5,15 +5,15 @@ namespace shm {
 
 namespace {
 
-template <int R>
+template <int R, int S>
 struct Geo {
     static constexpr int LOGM = 2 * R;
     static constexpr uint32_t M = 1u << LOGM;  // sub-transform length
     static constexpr int LOGN = 2 * LOGM;
     static constexpr uint32_t N = 1u << LOGN;
     static constexpr int E = 1 << R;  // elements per thread
-    static constexpr uint32_t THREADS = kNttSubs * E;
-    static constexpr uint32_t CHUNKS = M / kNttSubs;  // CTAs per limb
+    static constexpr uint32_t THREADS = S * E;
+    static constexpr uint32_t CHUNKS = M / S;  // CTAs per limb
     static constexpr uint32_t PAD_M = M + M / 16;     // padded block row in shared memory
 };
 
@@ -28,20 +28,20 @@ __device__ __forceinline__ uint32_t limb_major_row(uint32_t t, uint32_t slots, u
 }
 
 // ---------------- forward, phase 1: columns (global stages 0 .. LOGM-1)
-template <int R>
-__global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+template <int R, int S, int MINB>
+__global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const PrimeConst *__restrict__ pc) {
-    using G = Geo<R>;
-    __shared__ uint64_t sm[G::M * kNttSubs];
+    using G = Geo<R, S>;
+    __shared__ uint64_t sm[G::M * S];
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
     const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t pidx = map.prime[row % slots];
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN), *ws = w + G::N;
-    uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * kNttSubs;
-    const uint32_t sig = threadIdx.x % kNttSubs, lane = threadIdx.x / kNttSubs;
+    uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * S;
+    const uint32_t sig = threadIdx.x % S, lane = threadIdx.x / S;
 
     const bool grow = q < kGrowPrimeLimit;  // uniform per CTA (one limb)
     uint64_t a[G::E];
@@ -52,10 +52,10 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_col(uint64_t *__restri
     else
         fwd_pass<R>(a, w, ws, 1, 0, 0, q);
 #pragma unroll
-    for (int m = 0; m < G::E; m++) sm[(lane + m * G::E) * kNttSubs + sig] = a[m];
+    for (int m = 0; m < G::E; m++) sm[(lane + m * G::E) * S + sig] = a[m];
     __syncthreads();
 #pragma unroll
-    for (int m = 0; m < G::E; m++) a[m] = sm[(lane * G::E + m) * kNttSubs + sig];
+    for (int m = 0; m < G::E; m++) a[m] = sm[(lane * G::E + m) * S + sig];
     if (grow)
         fwd_pass<R, true>(a, w, ws, 1, R, lane, q);
     else
@@ -65,21 +65,21 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_col(uint64_t *__restri
 }
 
 // ---------------- forward, phase 2: blocks (global stages LOGM .. 2*LOGM-1), fully reduced output
-template <int R>
-__global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+template <int R, int S, int MINB>
+__global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const PrimeConst *__restrict__ pc) {
-    using G = Geo<R>;
-    __shared__ uint64_t sm[kNttSubs * G::PAD_M];
+    using G = Geo<R, S>;
+    __shared__ uint64_t sm[S * G::PAD_M];
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
     const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t pidx = map.prime[row % slots];
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN), *ws = w + G::N;
-    uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * kNttSubs * G::M;
+    uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * S * G::M;
     const uint32_t sig = threadIdx.x / G::E, lane = threadIdx.x % G::E;
-    const uint32_t b = chunk * kNttSubs + sig;
+    const uint32_t b = chunk * S + sig;
     uint64_t *x = xc + (size_t)sig * G::M;
     uint64_t *s = sm + sig * G::PAD_M;
 
@@ -116,21 +116,21 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) fwd_blk(uint64_t *__restri
 }
 
 // ---------------- inverse, phase 1: blocks (global stages 2*LOGM-1 .. LOGM)
-template <int R>
-__global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+template <int R, int S, int MINB>
+__global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const PrimeConst *__restrict__ pc) {
-    using G = Geo<R>;
-    __shared__ uint64_t sm[kNttSubs * G::PAD_M];
+    using G = Geo<R, S>;
+    __shared__ uint64_t sm[S * G::PAD_M];
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
     const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t pidx = map.prime[row % slots];
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN) + 2 * G::N, *ws = w + G::N;
-    uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * kNttSubs * G::M;
+    uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * S * G::M;
     const uint32_t sig = threadIdx.x / G::E, lane = threadIdx.x % G::E;
-    const uint32_t b = chunk * kNttSubs + sig;
+    const uint32_t b = chunk * S + sig;
     uint64_t *s = sm + sig * G::PAD_M;
 
 #pragma unroll
@@ -162,14 +162,14 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_blk(uint64_t *__restri
 }
 
 // ---------------- inverse, phase 2: columns (global stages LOGM-1 .. 0) with the folded scale
-template <int R>
-__global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
+template <int R, int S, int MINB>
+__global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const PrimeConst *__restrict__ pc,
                                                             const uint64_t *__restrict__ scale, int scale_by_prime,
                                                             uint32_t scale_base) {
-    using G = Geo<R>;
-    __shared__ uint64_t sm[G::M * kNttSubs];
+    using G = Geo<R, S>;
+    __shared__ uint64_t sm[G::M * S];
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
     const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t slot = row % slots;
@@ -178,8 +178,8 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_col(uint64_t *__restri
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN) + 2 * G::N, *ws = w + G::N;
     const uint64_t *sc = scale + 4 * (scale_by_prime ? pidx : slot - scale_base);
-    uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * kNttSubs;
-    const uint32_t sig = threadIdx.x % kNttSubs, lane = threadIdx.x / kNttSubs;
+    uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * S;
+    const uint32_t sig = threadIdx.x % S, lane = threadIdx.x / S;
 
     uint64_t a[G::E];
 #pragma unroll
@@ -190,10 +190,10 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_col(uint64_t *__restri
     else
         inv_pass<R>(a, w, ws, 1, R, lane, q, 0);
 #pragma unroll
-    for (int m = 0; m < G::E; m++) sm[(lane * G::E + m) * kNttSubs + sig] = a[m];
+    for (int m = 0; m < G::E; m++) sm[(lane * G::E + m) * S + sig] = a[m];
     __syncthreads();
 #pragma unroll
-    for (int m = 0; m < G::E; m++) a[m] = sm[(lane + m * G::E) * kNttSubs + sig];
+    for (int m = 0; m < G::E; m++) a[m] = sm[(lane + m * G::E) * S + sig];
     if (grow)
         inv_pass<R, true>(a, w, ws, 1, 0, 0, q, 1);
     else
@@ -210,23 +210,50 @@ __global__ void __launch_bounds__(Geo<R>::THREADS, 4) inv_col(uint64_t *__restri
     for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane + m * G::E)] = a[m];
 }
 
+template <int R, int S, int MINB>
+void launch_fwd_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                  cudaStream_t st) {
+    using G = Geo<R, S>;
+    dim3 grid(rows * G::CHUNKS);
+    SHM_LAUNCHED(1);
+    fwd_col<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+    SHM_LAUNCHED(1);
+    fwd_blk<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+}
+
+template <int R, int S, int MINB>
+void launch_inv_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                  const uint64_t *scale, uint32_t scale_base, cudaStream_t st) {
+    using G = Geo<R, S>;
+    dim3 grid(rows * G::CHUNKS);
+    SHM_LAUNCHED(1);
+    inv_blk<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+    SHM_LAUNCHED(1);
+    inv_col<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc,
+                                                     scale ? scale : c.inv_scale_plain, scale ? 0 : 1, scale_base);
+}
+
+// the tile variants of kNttVariants (ntt.cuh), selected per context by c.ntt_variant
 template <int R>
 void launch_fwd(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
                 cudaStream_t st) {
-    using G = Geo<R>;
-    dim3 grid(rows * G::CHUNKS);
-    SHM_LAUNCHED(1); fwd_col<R><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
-    SHM_LAUNCHED(1); fwd_blk<R><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+    switch (c.ntt_variant) {
+        case 1: launch_fwd_v<R, 16, 3>(c, data, rows, slots, map, st); break;
+        case 2: launch_fwd_v<R, 8, 8>(c, data, rows, slots, map, st); break;
+        case 3: launch_fwd_v<R, 8, 6>(c, data, rows, slots, map, st); break;
+        default: launch_fwd_v<R, 16, 4>(c, data, rows, slots, map, st); break;
+    }
 }
 
 template <int R>
 void launch_inv(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
                 const uint64_t *scale, uint32_t scale_base, cudaStream_t st) {
-    using G = Geo<R>;
-    dim3 grid(rows * G::CHUNKS);
-    SHM_LAUNCHED(1); inv_blk<R><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
-    SHM_LAUNCHED(1); inv_col<R><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, scale ? scale : c.inv_scale_plain,
-                                           scale ? 0 : 1, scale_base);
+    switch (c.ntt_variant) {
+        case 1: launch_inv_v<R, 16, 3>(c, data, rows, slots, map, scale, scale_base, st); break;
+        case 2: launch_inv_v<R, 8, 8>(c, data, rows, slots, map, scale, scale_base, st); break;
+        case 3: launch_inv_v<R, 8, 6>(c, data, rows, slots, map, scale, scale_base, st); break;
+        default: launch_inv_v<R, 16, 4>(c, data, rows, slots, map, scale, scale_base, st); break;
+    }
 }
 
 }  // namespace

@@ -8,11 +8,11 @@
 // Decomposition: N = M * M (M = 2^(2R)).  The first log M forward stages only
 // combine elements of one "column" {c + M*p : p < M}; the last log M stages only
 // combine elements of one contiguous "block" {b*M + p : p < M}.  Each phase is one
-// kernel in which a CTA owns 16 columns (or 16 blocks) of one limb; a thread owns
-// 2^R elements and runs R radix-2 stages in registers, twice, with one shared-memory
-// exchange in between.  Global loads and stores are 128-byte coalesced (16
-// consecutive words per column row / per block segment).  Values between the two
-// phases are lazy in [0, 4q) (Harvey butterflies; q < 2^62).
+// kernel in which a CTA owns S columns (or S blocks) of one limb (S = 16 or 8, the tile
+// variant); a thread owns 2^R elements and runs R radix-2 stages in registers, twice, with
+// one shared-memory exchange in between.  Global loads and stores move S consecutive words
+// per column row / per block segment (128 bytes at S = 16).  Values between the two
+// phases are lazy: below 36q (grow butterflies, q < 2^57) or in [0, 4q) (Harvey).
 //
 // The inverse's last stage folds a per-limb scale c (N^-1, or N^-1 times the
 // ModUp digit factor) into both outputs: (X+Y)*c and (X-Y)*psi^-(N/2)*c.
@@ -23,7 +23,13 @@
 
 namespace shm {
 
-constexpr int kNttSubs = 16;  // columns / blocks per CTA
+// Tile variants of the NTT kernels (columns or blocks per CTA, minimum resident CTAs per SM,
+// which caps the registers a thread may use); the autotuner picks one per context.
+struct NttVariant {
+    int subs, min_blocks;
+};
+constexpr NttVariant kNttVariants[] = {{16, 4}, {16, 3}, {8, 8}, {8, 6}};
+constexpr int kNttVariantCount = 4;
 
 struct LimbMap {
     uint8_t prime[512];  // limb slot within a polynomial -> prime index; 255 = leave untouched

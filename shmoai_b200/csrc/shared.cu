@@ -17,6 +17,8 @@
 //   FmtSwitch backward (FmtSwitch.cu:396-429): n ordinary key switches of the
 //     shared a from s'_i to s, hoisted: one ModUp(a), per member one inner product
 //     with its key [dnum][2][QP][N], ModDown, combine with b_i.
+#include <mutex>
+
 #include "core.hpp"
 #include "host_math.hpp"
 
@@ -34,7 +36,7 @@ constexpr int kMaxB = 16;
 // (n + 1 halves of dnum x QP limbs, far larger than L2 at the top level) is read once per
 // chunk instead of once per group.
 constexpr int kIpT = 128;
-constexpr size_t kIpSmem = 32 * 1024;
+constexpr size_t kIpSmemMax = 96 * 1024;  // largest chunk the autotuner may pick
 
 template <bool S52>
 __global__ void __launch_bounds__(kIpT) ip_multi_kernel(const uint64_t *__restrict__ up,
@@ -199,6 +201,34 @@ ExtConsts ext_consts(Context &c, uint32_t L) {
     return e;
 }
 
+}  // namespace
+
+// The Sh-Rot / FmtSwitch inner products: groups are served in chunks that fit
+// c.ip_chunk_bytes of shared memory, each chunk reading the key once.
+void ip_multi(const Context &c, const uint64_t *up, const uint64_t *key, uint64_t *acc, uint32_t n_cts, uint32_t L,
+              uint32_t beta, uint32_t H, const uint32_t *perm, cudaStream_t st) {
+    static std::once_flag attr;
+    std::call_once(attr, [] {
+        for (const void *f : {(const void *)ip_multi_kernel<true>, (const void *)ip_multi_kernel<false>})
+            SHM_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kIpSmemMax));
+    });
+    const uint32_t np = c.np, LP = L + np;
+    const size_t cap = std::min<size_t>(c.ip_chunk_bytes, kIpSmemMax);
+    const uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_cts, (uint32_t)(cap / (beta * kIpT * 8))));
+    const dim3 grid(c.n / kIpT, LP, (n_cts + chunk - 1) / chunk);
+    const size_t smem = (size_t)chunk * beta * kIpT * 8;
+    SHM_LAUNCHED(1);
+    if (c.s52)
+        ip_multi_kernel<true><<<grid, kIpT, smem, st>>>(up, key, acc, n_cts, chunk, L, np, c.nq, beta, H, c.log_n,
+                                                        c.pc, perm);
+    else
+        ip_multi_kernel<false><<<grid, kIpT, smem, st>>>(up, key, acc, n_cts, chunk, L, np, c.nq, beta, H, c.log_n,
+                                                         c.pc, perm);
+    SHM_CUDA(cudaGetLastError());
+}
+
+namespace {
+
 void check_shape(const Context &c, uint32_t L, uint32_t beta, uint32_t H) {
     if (c.np == 0) throw std::invalid_argument("context has no special primes");
     if (L < 1 || L > c.nq) throw std::invalid_argument("level out of range");
@@ -211,17 +241,7 @@ void apply_target(const Context &c, const uint64_t *up, uint32_t n_cts, uint32_t
                   const Target &t, uint64_t *acc, uint64_t *delta, cudaStream_t st) {
     const size_t n = c.n;
     const uint32_t np = c.np, LP = L + np;
-    const uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_cts, kIpSmem / (beta * kIpT * 8)));
-    const dim3 grid(n / kIpT, LP, (n_cts + chunk - 1) / chunk);
-    const size_t smem = (size_t)chunk * beta * kIpT * 8;
-    SHM_LAUNCHED(1);
-    if (c.s52)
-        ip_multi_kernel<true><<<grid, kIpT, smem, st>>>(up, t.key, acc, n_cts, chunk, L, np, c.nq, beta, H, c.log_n,
-                                                        c.pc, t.perm);
-    else
-        ip_multi_kernel<false><<<grid, kIpT, smem, st>>>(up, t.key, acc, n_cts, chunk, L, np, c.nq, beta, H, c.log_n,
-                                                         c.pc, t.perm);
-    SHM_CUDA(cudaGetLastError());
+    ip_multi(c, up, t.key, acc, n_cts, L, beta, H, t.perm, st);
     LimbMap mp;
     for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
     ntt_inverse(c, acc, n_cts * H * LP, LP, mp, c.moddown_scale, st, L);

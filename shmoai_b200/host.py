@@ -9,6 +9,7 @@ loaded; `Host(..., lib=path)` loads another build of the same library.
 from __future__ import annotations
 
 import ctypes
+import json
 import os
 
 import numpy as np
@@ -78,6 +79,9 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_boot_galois_elts": (i32, [_P, ctypes.POINTER(_U32), _U32, ctypes.POINTER(_U32)]),
         "shm_boot_run": (i32, [_P, _P, _U32, pp]),
         "shm_boot_capture": (i32, [_P, _P, _U32, pp, pp]),
+        "shm_boot_tune": (i32, [_P, _U32, _U32, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+        "shm_boot_get_split": (i32, [_P, ctypes.POINTER(ctypes.c_int)]),
+        "shm_boot_set_split": (i32, [_P, ctypes.POINTER(ctypes.c_int)]),
         "shm_host_graph_launch": (i32, [_P]),
         "shm_host_graph_kernels": (ctypes.c_uint64, [_P]),
         "shm_host_graph_destroy": (None, [_P]),
@@ -305,6 +309,25 @@ class Bootstrapper:
         o = _P()
         self.host._check(self.host.lib.shm_boot_run(self._b, ct._c, members, ctypes.byref(o)))
         return Ct(self.host, o)
+
+    def tune(self, count: int, members: int = 0) -> list[dict]:
+        """Autotune for batches of `count` (shm_boot_tune); generate Galois keys afterwards."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        need = ctypes.c_size_t()
+        self.host._check(self.host.lib.shm_boot_tune(self._b, count, members, buf, len(buf), ctypes.byref(need)))
+        return json.loads(buf.value.decode())
+
+    @property
+    def split(self) -> list[int]:
+        """BSGS baby-step counts of the six slot-transform layers (0 = default)."""
+        g = (ctypes.c_int * 6)()
+        self.host._check(self.host.lib.shm_boot_get_split(self._b, g))
+        return list(g)
+
+    @split.setter
+    def split(self, g1):
+        g = (ctypes.c_int * 6)(*g1)
+        self.host._check(self.host.lib.shm_boot_set_split(self._b, g))
 
     def capture(self, ct: Ct, members: int = 0) -> tuple["Graph", Ct]:
         """A CUDA graph of run(ct, members) and the output batch every launch rewrites;

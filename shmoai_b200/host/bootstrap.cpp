@@ -32,6 +32,7 @@
 // two double angles the interpolant leaves ~2e-7 error, too much for the 2e-5 target
 // after the x512 amplitude correction, with three ~1e-13.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <numeric>
 #include <set>
@@ -226,6 +227,37 @@ int64_t floordiv(int64_t a, int64_t b) {
     return q;
 }
 
+// the diagonal offsets of a layer in units of their gcd b, centred to (-span/2, span/2]
+std::map<int64_t, const Vec *> centred_offsets(const Diags &diags, int64_t slots, int64_t &b) {
+    b = 0;
+    for (auto &kv : diags) b = std::gcd(b, (int64_t)kv.first);
+    if (!b) b = 1;
+    const int64_t span = slots / b;
+    std::map<int64_t, const Vec *> ts;
+    for (auto &kv : diags) {
+        int64_t t = (int64_t)kv.first / b;
+        if (t > span / 2) t -= span;
+        ts[t] = &kv.second;
+    }
+    return ts;
+}
+
+int64_t default_g1(size_t diagonals) {
+    return (int64_t)1 << (int)std::ceil(std::log2(std::sqrt((double)diagonals)));
+}
+
+// nonzero baby steps v and giant steps u of the split t = g1 u + v
+void split_counts(const std::map<int64_t, const Vec *> &ts, int64_t g1, size_t &baby, size_t &giant) {
+    std::set<int64_t> us, vs;
+    for (auto &kv : ts) {
+        const int64_t u = floordiv(kv.first, g1);
+        us.insert(u);
+        vs.insert(kv.first - u * g1);
+    }
+    baby = vs.size() - vs.count(0);
+    giant = us.size() - us.count(0);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ LinearTransform
@@ -236,20 +268,11 @@ int64_t floordiv(int64_t a, int64_t b) {
 // sum_v Rot_{-g1 u b}(D_t) * Rot_{v b}(x).
 class LinearTransform {
    public:
-    LinearTransform(const Evaluator &ev, const Diags &diags, uint32_t level) : level_(level) {
+    // g1 = baby-step count (0: default_g1)
+    LinearTransform(const Evaluator &ev, const Diags &diags, uint32_t level, int64_t g1 = 0) : level_(level) {
         const Context &c = ev.context();
-        const int64_t n = c.n / 2;
-        int64_t b = 0;
-        for (auto &kv : diags) b = std::gcd(b, (int64_t)kv.first);
-        b_ = b ? b : 1;
-        const int64_t span = n / b_;
-        std::map<int64_t, const Vec *> ts;
-        for (auto &kv : diags) {
-            int64_t t = (int64_t)kv.first / b_;
-            if (t > span / 2) t -= span;
-            ts[t] = &kv.second;
-        }
-        g1_ = (int64_t)1 << (int)std::ceil(std::log2(std::sqrt((double)ts.size())));
+        const std::map<int64_t, const Vec *> ts = centred_offsets(diags, c.n / 2, b_);
+        g1_ = g1 > 0 ? g1 : default_g1(ts.size());
         pt_scale_ = (double)c.primes[level - 1];
         for (auto &kv : ts) {
             const int64_t u = floordiv(kv.first, g1_), v = kv.first - u * g1_;
@@ -332,11 +355,11 @@ void BatchBootstrapper::prepare() {
     std::vector<Diags> s = s2c_layers(tw);
     for (auto &kv : s[2])
         for (auto &z : kv.second) z *= p_.F;
-    for (uint32_t i = 0; i < 3; i++) s2c_.push_back(new LinearTransform(ev_, s[i], p_.input_level - i));
+    for (uint32_t i = 0; i < 3; i++) s2c_.push_back(new LinearTransform(ev_, s[i], p_.input_level - i, p_.bsgs_g1[i]));
     std::vector<Diags> ci = c2s_layers(tw);
     for (auto &kv : ci[0])
         for (auto &z : kv.second) z /= 2.0 * p_.K;
-    for (uint32_t i = 0; i < 3; i++) c2s_.push_back(new LinearTransform(ev_, ci[i], c.nq - i));
+    for (uint32_t i = 0; i < 3; i++) c2s_.push_back(new LinearTransform(ev_, ci[i], c.nq - i, p_.bsgs_g1[3 + i]));
     top_ = c.nq;
     q0_ = (double)c.primes[0];
     cheb_ = cheb_interp(evalmod_target, p_.double_angles, p_.K, p_.degree);
@@ -493,6 +516,112 @@ Ciphertext BatchBootstrapper::bootstrap_shared_a_s2c_first(const Ciphertext &ct,
     Ciphertext re, im;
     slots_to_re_im(ev, ev.to_shared(ct, members), re, im);
     return finish(ev, ev.from_shared(re), ev.from_shared(im));
+}
+
+// ------------------------------------------------------------------ autotuning
+
+namespace {
+
+// milliseconds of one hoisted rotation batch with k targets (one ModUp, k inner products,
+// ModDowns and combines) of `count` ciphertexts (groups of `members` when members > 0) at L
+// primes, on uniform scratch residues and a scratch key (timing only)
+double time_rotations(const Evaluator &ev, uint32_t count, uint32_t members, uint32_t L, uint32_t k) {
+    const Context &c = ev.context();
+    shm_context *h = c.handle();
+    const uint32_t QP = c.nq + c.np, H = members ? members + 1 : 2, units = members ? count / members : count;
+    const size_t ln = (size_t)L * c.n;
+    DeviceBuffer x(c, units * H * ln), key(c, (size_t)c.dnum * H * QP * c.n);
+    c.check(shm_sample_uniform(h, x.data(), units * H, L, 0x7E5A, c.stream()));
+    c.check(shm_sample_uniform(h, key.data(), c.dnum * H, QP, 0x7E5B, c.stream()));
+    std::vector<DeviceBuffer> outs;
+    std::vector<uint64_t *> optr;
+    std::vector<const uint64_t *> keys(k, key.data());
+    std::vector<uint32_t> elts;
+    for (uint32_t i = 0; i < k; i++) {
+        outs.emplace_back(c, units * H * ln);
+        optr.push_back(outs.back().data());
+        elts.push_back(ev.galois_elt((int)i + 1));
+    }
+    const size_t wsb = members ? shm_shared_rotate_workspace_bytes(h, units, members, L)
+                               : shm_apply_galois_hoisted_workspace_bytes(h, units, L);
+    DeviceBuffer ws(c, wsb / 8 + 1);
+    auto run = [&] {
+        if (members)
+            c.check(shm_shared_rotate_hoisted(h, x.data(), units, members, k, elts.data(), keys.data(), optr.data(), L,
+                                              ws.data(), ws.words() * 8, c.stream()));
+        else
+            c.check(shm_apply_galois_hoisted(h, x.data(), k, elts.data(), keys.data(), optr.data(), units, L,
+                                             ws.data(), ws.words() * 8, c.stream()));
+    };
+    run();
+    c.synchronize();
+    const int reps = 3;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int r = 0; r < reps; r++) run();
+    c.synchronize();
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / reps;
+}
+
+}  // namespace
+
+void BatchBootstrapper::set_split(const int g1[6]) {
+    for (int i = 0; i < 6; i++) {
+        if (g1[i] < 0) throw Error("BSGS split: baby-step counts must be >= 0");
+        p_.bsgs_g1[i] = g1[i];
+    }
+    prepare();
+}
+
+std::vector<TuneRecord> BatchBootstrapper::tune(uint32_t count, uint32_t members) {
+    const Context &c = ev_.context();
+    shm_context *h = c.handle();
+    if (!count || (members && count % members)) throw Error("tune: count must be a positive multiple of members");
+    std::vector<TuneRecord> out;
+    auto kernel_knob = [&](const char *name, int knob, uint32_t size, uint32_t level, uint32_t mem,
+                           std::vector<std::string> names) {
+        float t[8] = {0};
+        uint32_t best = 0;
+        c.check(shm_autotune(h, knob, size, level, mem, t, 8, &best));
+        TuneRecord r{name, names, {}, best};
+        for (size_t i = 0; i < names.size(); i++) r.ms.push_back(t[i]);
+        out.push_back(r);
+    };
+    // EvalMod's key switches dominate: ~4096 limbs is one relinearisation's ModUp batch scale
+    kernel_knob("ntt_tile", SHM_TUNE_NTT_TILE, std::min<uint32_t>(4096, 2 * count * c.nq), 0, 0,
+                {"16 cols, 4 CTAs/SM", "16 cols, 3 CTAs/SM", "8 cols, 8 CTAs/SM", "8 cols, 6 CTAs/SM"});
+    if (members)
+        kernel_knob("ip_chunk", SHM_TUNE_IP_CHUNK, count / members, c.nq, members, {"16 KB", "32 KB", "64 KB", "96 KB"});
+
+    // BSGS split per layer: cost(g1) = (1 + giant) ModUps + (baby + giant) per-step switches,
+    // both timed at the layer's level (one and three targets of a hoisted batch)
+    const Twiddles tw(c.n / 2);
+    const std::vector<Diags> layers[2] = {s2c_layers(tw), c2s_layers(tw)};
+    for (int layer = 0; layer < 6; layer++) {
+        const uint32_t L = layer < 3 ? p_.input_level - layer : c.nq - (layer - 3);
+        const double t1 = time_rotations(ev_, count, members, L, 1), t3 = time_rotations(ev_, count, members, L, 3);
+        const double step = std::max(0.0, (t3 - t1) / 2), modup = std::max(0.0, t1 - step);
+        int64_t b = 1;
+        const auto ts = centred_offsets(layers[layer / 3][layer % 3], c.n / 2, b);
+        TuneRecord r{"bsgs_g1[" + std::string(layer < 3 ? "S2C " : "C2S ") + std::to_string(layer % 3) + "] at " +
+                         std::to_string(L) + " primes",
+                     {}, {}, 0};
+        double best = 1e300;
+        for (int64_t g1 = 1; g1 <= (int64_t)ts.size() * 2; g1 *= 2) {
+            size_t baby = 0, giant = 0;
+            split_counts(ts, g1, baby, giant);
+            const double cost = (1 + giant) * modup + (baby + giant) * step;
+            r.candidates.push_back(std::to_string(g1));
+            r.ms.push_back(cost);
+            if (cost < best) {
+                best = cost;
+                r.chosen = r.candidates.size() - 1;
+                p_.bsgs_g1[layer] = (int)g1;
+            }
+        }
+        out.push_back(r);
+    }
+    prepare();
+    return out;
 }
 
 double slot_transform_selfcheck(uint32_t log_slots) {

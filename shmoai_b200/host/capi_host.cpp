@@ -1,4 +1,6 @@
 // extern "C" entry points of include/shmoai_host.h over the C++ host classes.
+#include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 
@@ -357,6 +359,63 @@ int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out) 
         } else {
             put(out, b->b->bootstrap_ordinary_s2c_first(C(in)));
         }
+    });
+}
+
+namespace {
+
+std::string json_str(const std::string &v) {
+    std::string o = "\"";
+    for (char ch : v) {
+        if (ch == '"' || ch == '\\') o += '\\';
+        o += ch;
+    }
+    return o + "\"";
+}
+
+std::string tune_json(const std::vector<TuneRecord> &rs) {
+    std::string o = "[";
+    for (size_t i = 0; i < rs.size(); i++) {
+        const TuneRecord &r = rs[i];
+        o += (i ? ", " : "") + std::string("{\"knob\": ") + json_str(r.knob) + ", \"candidates\": [";
+        for (size_t j = 0; j < r.candidates.size(); j++) o += (j ? ", " : "") + json_str(r.candidates[j]);
+        o += "], \"ms\": [";
+        for (size_t j = 0; j < r.ms.size(); j++) {
+            char buf[64];
+            snprintf(buf, sizeof buf, "%s%.6g", j ? ", " : "", r.ms[j]);
+            o += buf;
+        }
+        o += "], \"chosen\": " + std::to_string(r.chosen) + "}";
+    }
+    return o + "]";
+}
+
+}  // namespace
+
+int shm_boot_tune(shm_boot *b, uint32_t count, uint32_t members, char *json, size_t cap, size_t *needed) {
+    return guard([&] {
+        if (!b) throw Error("null bootstrapper");
+        const std::string j = tune_json(b->b->tune(count, members));
+        if (needed) *needed = j.size() + 1;
+        if (json && cap) {
+            const size_t n = std::min(cap - 1, j.size());
+            std::memcpy(json, j.data(), n);
+            json[n] = 0;
+        }
+    });
+}
+
+int shm_boot_get_split(const shm_boot *b, int *g1) {
+    return guard([&] {
+        if (!b || !g1) throw Error("null argument");
+        for (int i = 0; i < 6; i++) g1[i] = b->b->params().bsgs_g1[i];
+    });
+}
+
+int shm_boot_set_split(shm_boot *b, const int *g1) {
+    return guard([&] {
+        if (!b || !g1) throw Error("null argument");
+        b->b->set_split(g1);
     });
 }
 

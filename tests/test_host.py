@@ -187,3 +187,51 @@ def test_bootstrap_reference_parameters_on_b200(members):
     assert out.level == 35 - 3 - 9
     assert err.mean() < 2e-5, err.mean()
     assert err.max() < 2e-4, err.max()
+
+
+def test_tune_then_keys_then_bootstrap_on_oracle():
+    """The autotuner's flow: tune (kernel knobs, BSGS split per layer), then Galois keys for
+    the tuned rotation steps, then a bootstrap that still meets the error bound.  On the
+    oracle build the kernel knobs report zero time and the split follows CPU timings."""
+    h = Host(12, _small_primes(), 5, hamming_weight=64, seed=13, lib=ORACLE_HOST)
+    h.gen_relin_key()
+    bs = Bootstrapper(h, DELTA, 4)
+    rep = bs.tune(2, 0)
+    knobs = [r["knob"] for r in rep]
+    assert knobs[0] == "ntt_tile" and sum(k.startswith("bsgs_g1") for k in knobs) == 6
+    for r in rep:
+        assert len(r["candidates"]) == len(r["ms"]) and 0 <= r["chosen"] < len(r["candidates"])
+    split = bs.split
+    assert split == [int(r["candidates"][r["chosen"]]) for r in rep if r["knob"].startswith("bsgs_g1")]
+    h.gen_galois_keys(bs.galois_elts())
+    rng = np.random.default_rng(12)
+    z = _z(rng, 2, h.n // 2)
+    err = np.abs(h.decrypt(bs.run(h.encrypt(z, DELTA, 4))) - z)
+    assert err.mean() < 2e-5, err.mean()
+    with pytest.raises(HostError, match="count must be a positive multiple"):
+        bs.tune(3, 2)
+    with pytest.raises(HostError, match=">= 0"):
+        bs.split = [-1, 0, 0, 0, 0, 0]
+
+
+@pytest.mark.gpu
+def test_tuned_split_is_bit_exact_between_builds():
+    """The CUDA build tunes (kernel tiles measured on the B200, BSGS split modelled from
+    timed rotations); the oracle build takes the same split; both bootstrap identically."""
+    g, c = _pair(23)
+    for h in (g, c):
+        h.gen_relin_key()
+    bg, bc = Bootstrapper(g, DELTA, 4), Bootstrapper(c, DELTA, 4)
+    rep = bg.tune(4, 2)
+    assert [r["knob"] for r in rep][:2] == ["ntt_tile", "ip_chunk"]
+    assert all(t > 0 for r in rep[:2] for t in r["ms"])
+    bc.split = bg.split
+    elts = bg.galois_elts()
+    assert elts == bc.galois_elts()
+    for h in (g, c):
+        h.gen_shared_keys(2, elts, hamming_weight=64)
+    rng = np.random.default_rng(14)
+    z = _z(rng, 4, g.n // 2)
+    og, oc = bg.run(g.encrypt(z, DELTA, 4), members=2), bc.run(c.encrypt(z, DELTA, 4), members=2)
+    assert np.array_equal(og.to_host(), oc.to_host())
+    assert np.abs(g.decrypt(og) - z).mean() < 2e-5
