@@ -245,6 +245,11 @@ class Evaluator {
     Ciphertext multiply_const_unscaled(const Ciphertext &a, double c, double T) const;
     Ciphertext adjust(const Ciphertext &a, uint32_t L, double scale) const;
     Ciphertext multiply(const Ciphertext &a, const Ciphertext &b, bool rescale = true) const;
+    // the tensor product only: a size-3 batch at scale a.scale * b.scale (the reference's
+    // multiply before relinearize_inplace, evaluate.cu:350-402); it may be rescaled, added
+    // to (also to size-2 batches) and relinearised later
+    Ciphertext multiply_lazy(const Ciphertext &a, const Ciphertext &b) const;
+    Ciphertext relinearize(const Ciphertext &a) const;  // size 3 -> 2 (evaluate.cu:1358-1390)
     Ciphertext square(const Ciphertext &a) const { return multiply(a, a); }
     // sum_k X_k * P_k (same level and scale), one launch; result scale X.scale * P.scale
     Ciphertext multiply_plain_accumulate(const std::vector<const Ciphertext *> &X,

@@ -71,6 +71,12 @@ int shm_add(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64
             uint32_t L, void *stream);
 int shm_sub(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
             uint32_t L, void *stream);
+/* Sum of two batches of n_cts ciphertexts of different sizes (a_size >= b_size, e.g. an
+ * unrelinearised product and an ordinary ciphertext): out[ct][p] = a[ct][p] + b[ct][p] for
+ * p < b_size, a[ct][p] above.  Replaces add_inplace on ciphertexts of different sizes
+ * (thirdparty/phantom-fhe/src/evaluate.cu:114-160). */
+int shm_add_sizes(const shm_context *ctx, const uint64_t *a, uint32_t a_size, const uint64_t *b, uint32_t b_size,
+                  uint64_t *out, uint32_t n_cts, uint32_t L, void *stream);
 int shm_negate(const shm_context *ctx, const uint64_t *a, uint64_t *out, uint32_t n_polys, uint32_t L, void *stream);
 
 /* out[c] = ct[c] * pt for n_polys polynomials and one plaintext [L][N].

@@ -306,6 +306,28 @@ int shm_sub(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64
     return SHM_OK;
 }
 
+int shm_add_sizes(const shm_context *ctx, const uint64_t *a, uint32_t a_size, const uint64_t *b, uint32_t b_size,
+                  uint64_t *out, uint32_t n_cts, uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    if (b_size > a_size || b_size == 0) return fail("add_sizes: need a_size >= b_size >= 1");
+    size_t n = ctx->c->n;
+    for (size_t ct = 0; ct < n_cts; ct++)
+        for (size_t p = 0; p < a_size; p++)
+            for (size_t l = 0; l < L; l++) {
+                const uint64_t q = ctx->c->primes[l];
+                const uint64_t *x = a + ((ct * a_size + p) * L + l) * n;
+                uint64_t *o = out + ((ct * a_size + p) * L + l) * n;
+                if (p < b_size) {
+                    const uint64_t *y = b + ((ct * b_size + p) * L + l) * n;
+                    for (size_t k = 0; k < n; k++) o[k] = addmod(x[k], y[k], q);
+                } else {
+                    memmove(o, x, n * sizeof(uint64_t));
+                }
+            }
+    return SHM_OK;
+}
+
 int shm_negate(const shm_context *ctx, const uint64_t *a, uint64_t *out, uint32_t n_polys, uint32_t L, void *stream) {
     (void)stream;
     if (!lvl_ok(ctx, L)) return fail("level out of range");

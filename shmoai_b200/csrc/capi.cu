@@ -340,6 +340,16 @@ int shm_sub(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64
     return ew(ctx, shm::EwOp::Sub, a, b, out, n_polys, L, n_polys, stream);
 }
 
+int shm_add_sizes(const shm_context *ctx, const uint64_t *a, uint32_t a_size, const uint64_t *b, uint32_t b_size,
+                  uint64_t *out, uint32_t n_cts, uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        set_device(c);
+        shm::add_sizes(c, a, a_size, b, b_size, out, n_cts, L, S(stream));
+    });
+}
+
 int shm_negate(const shm_context *ctx, const uint64_t *a, uint64_t *out, uint32_t n_polys, uint32_t L, void *stream) {
     return ew(ctx, shm::EwOp::Negate, a, nullptr, out, n_polys, L, n_polys, stream);
 }

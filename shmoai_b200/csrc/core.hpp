@@ -91,6 +91,8 @@ void elementwise(const Context &c, EwOp op, const uint64_t *a, const uint64_t *b
                  uint32_t L, uint32_t b_polys, cudaStream_t st);
 void tensor(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_cts, uint32_t L,
             cudaStream_t st);
+void add_sizes(const Context &c, const uint64_t *a, uint32_t sa, const uint64_t *b, uint32_t sb, uint64_t *out,
+               uint32_t n_cts, uint32_t L, cudaStream_t st);
 void apply_galois(const Context &c, const uint64_t *in, uint64_t *out, uint32_t rows, uint32_t elt, cudaStream_t st);
 void rescale(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *ws,
              cudaStream_t st);

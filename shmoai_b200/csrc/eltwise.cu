@@ -41,6 +41,24 @@ __global__ void ew_kernel(const uint64_t *__restrict__ a, const uint64_t *__rest
     *reinterpret_cast<ulonglong2 *>(out + off) = r;
 }
 
+// out[ct][p] = a[ct][p] + (p < sb ? b[ct][p] : 0); rows ct * sa * L + p * L + limb
+__global__ void add_sizes_kernel(const uint64_t *__restrict__ a, const uint64_t *__restrict__ b,
+                                 uint64_t *__restrict__ out, uint32_t sa, uint32_t sb, uint32_t L, uint32_t log_n,
+                                 const PrimeConst *__restrict__ pc) {
+    const uint32_t row = blockIdx.y, limb = row % L, p = (row / L) % sa, ct = row / (L * sa);
+    const size_t col = 2 * (blockIdx.x * kEwThreads + threadIdx.x);
+    const size_t off = ((size_t)row << log_n) + col;
+    ulonglong2 x = *reinterpret_cast<const ulonglong2 *>(a + off);
+    if (p < sb) {
+        const size_t boff = (((size_t)(ct * sb + p) * L + limb) << log_n) + col;
+        const ulonglong2 y = *reinterpret_cast<const ulonglong2 *>(b + boff);
+        const uint64_t q = pc[limb].q;
+        x.x = add_mod(x.x, y.x, q);
+        x.y = add_mod(x.y, y.y, q);
+    }
+    *reinterpret_cast<ulonglong2 *>(out + off) = x;
+}
+
 // (a0, a1) x (b0, b1) -> (a0 b0, a0 b1 + a1 b0, a1 b1) per ciphertext
 __global__ void tensor_kernel(const uint64_t *__restrict__ a, const uint64_t *__restrict__ b, uint64_t *__restrict__ out,
                               uint32_t L, uint32_t log_n, const PrimeConst *__restrict__ pc) {
@@ -110,6 +128,17 @@ void elementwise(const Context &c, EwOp op, const uint64_t *a, const uint64_t *b
             SHM_LAUNCHED(1); ew_kernel<EwOp::MulPlain><<<grid, kEwThreads, 0, st>>>(a, b, out, L, c.log_n, b_polys, c.pc);
             break;
     }
+    SHM_CUDA(cudaGetLastError());
+}
+
+void add_sizes(const Context &c, const uint64_t *a, uint32_t sa, const uint64_t *b, uint32_t sb, uint64_t *out,
+               uint32_t n_cts, uint32_t L, cudaStream_t st) {
+    if (n_cts == 0 || L == 0) return;
+    if (sb > sa || sb == 0) throw std::invalid_argument("add_sizes: need a_size >= b_size >= 1");
+    if ((size_t)n_cts * sa * L > 65535) throw std::invalid_argument("add_sizes: batch too large for one launch");
+    SHM_LAUNCHED(1);
+    add_sizes_kernel<<<dim3(c.n / 2 / kEwThreads, n_cts * sa * L), kEwThreads, 0, st>>>(a, b, out, sa, sb, L, c.log_n,
+                                                                                         c.pc);
     SHM_CUDA(cudaGetLastError());
 }
 

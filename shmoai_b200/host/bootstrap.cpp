@@ -428,8 +428,13 @@ bool feasible(const Basis &T, int ncoef, uint32_t lvl) {
     return T.at(m).L >= lvl + 1 && feasible(T, d - m + 1, lvl + 1) && feasible(T, m, lvl);
 }
 
-// sum_i c_i T_i, output at exactly scale S and lvl primes (baby-step giant-step)
-Ciphertext cheb_eval(const Evaluator &ev, const Basis &T, const std::vector<double> &c, double S, uint32_t lvl) {
+// sum_i c_i T_i, output at exactly scale S and lvl primes (baby-step giant-step).  A
+// giant-step product is only added to, so it stays unrelinearised (size 3) through its
+// rescale and the sum; the sum is relinearised once, where it is needed as a multiplicand
+// or at the top (lazy = false), instead of every product on its own: two relinearisations
+// fewer at degree 47.
+Ciphertext cheb_eval(const Evaluator &ev, const Basis &T, const std::vector<double> &c, double S, uint32_t lvl,
+                     bool lazy = false) {
     const Context &ctx = ev.context();
     const int d = (int)c.size() - 1;
     if (d < 1) throw Error("Chebyshev piece of degree 0");
@@ -452,10 +457,11 @@ Ciphertext cheb_eval(const Evaluator &ev, const Basis &T, const std::vector<doub
     cheb_divide(c, m, qc, rc);
     Ciphertext Tm = ev.mod_switch_to(T.at(m), lvl + 1);
     const double Sq = S * (double)ctx.primes[lvl] / Tm.scale_;
-    Ciphertext qct = cheb_eval(ev, T, qc, Sq, lvl + 1);
-    Ciphertext prod = ev.multiply(qct, Tm);
+    Ciphertext qct = cheb_eval(ev, T, qc, Sq, lvl + 1);  // a multiplicand: relinearised
+    Ciphertext prod = ev.rescale_to_next(ev.multiply_lazy(qct, Tm));
     prod.scale_ = S;
-    return ev.add(prod, cheb_eval(ev, T, rc, S, lvl));
+    Ciphertext sum = ev.add(prod, cheb_eval(ev, T, rc, S, lvl, true));
+    return lazy ? std::move(sum) : ev.relinearize(sum);
 }
 
 }  // namespace

@@ -66,6 +66,20 @@ static void same_shape(const Ciphertext &a, const Ciphertext &b) {
 }
 
 Ciphertext Evaluator::add(const Ciphertext &a, const Ciphertext &b) const {
+    if (a.size != b.size && !a.shared && !b.shared && a.count == b.count) {
+        // an unrelinearised product plus an ordinary ciphertext (evaluate.cu:114-160 extends
+        // the shorter operand with zero polynomials)
+        if (!same_scale(a.scale_, b.scale_)) throw Error("scale mismatch in add");
+        if (a.L != b.L) {
+            const uint32_t L = std::min(a.L, b.L);
+            return a.L > L ? add(mod_switch_to(a, L), b) : add(a, mod_switch_to(b, L));
+        }
+        const Ciphertext &big = a.size > b.size ? a : b, &small = a.size > b.size ? b : a;
+        Ciphertext o = like(big, big.L);
+        c_.check(shm_add_sizes(c_.handle(), big.data.data(), big.size, small.data.data(), small.size, o.data.data(),
+                               a.count, a.L, c_.stream()));
+        return o;
+    }
     same_shape(a, b);
     if (!same_scale(a.scale_, b.scale_)) throw Error("scale mismatch in add");
     if (a.L != b.L) {
@@ -176,6 +190,37 @@ Ciphertext Evaluator::adjust(const Ciphertext &a, uint32_t L, double scale) cons
     }
     if (a.L > L + 1) return multiply_const(mod_switch_to(a, L + 1), 1.0, scale);
     return multiply_const(a, 1.0, scale);
+}
+
+Ciphertext Evaluator::multiply_lazy(const Ciphertext &a, const Ciphertext &b) const {
+    if (a.shared || b.shared || a.size != 2 || b.size != 2) throw Error("multiply needs ordinary ciphertexts");
+    if (a.count != b.count) throw Error("batches of different sizes");
+    if (a.L != b.L) {
+        const uint32_t L = std::min(a.L, b.L);
+        return a.L > L ? multiply_lazy(mod_switch_to(a, L), b) : multiply_lazy(a, mod_switch_to(b, L));
+    }
+    Ciphertext r;
+    r.data = DeviceBuffer(c_, (size_t)a.count * 3 * a.L * c_.n);
+    r.count = a.count;
+    r.size = 3;
+    r.L = a.L;
+    r.scale_ = a.scale_ * b.scale_;
+    c_.check(shm_multiply(c_.handle(), a.data.data(), b.data.data(), r.data.data(), a.count, a.L, c_.stream()));
+    return r;
+}
+
+Ciphertext Evaluator::relinearize(const Ciphertext &a) const {
+    if (a.shared || a.size != 3) throw Error("relinearize takes size-3 ciphertexts");
+    if (!relin_key) throw Error("no relinearisation key");
+    Ciphertext r;
+    r.data = DeviceBuffer(c_, (size_t)a.count * 2 * a.L * c_.n);
+    r.count = a.count;
+    r.L = a.L;
+    r.scale_ = a.scale_;
+    uint64_t *w = ws(shm_keyswitch_workspace_bytes(c_.handle(), a.count, a.L));
+    c_.check(shm_relinearize(c_.handle(), a.data.data(), relin_key->data(), r.data.data(), a.count, a.L, w,
+                             ws_.words() * 8, c_.stream()));
+    return r;
 }
 
 Ciphertext Evaluator::multiply(const Ciphertext &a, const Ciphertext &b, bool rescale) const {
