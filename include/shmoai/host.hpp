@@ -250,6 +250,11 @@ class Evaluator {
     // to (also to size-2 batches) and relinearised later
     Ciphertext multiply_lazy(const Ciphertext &a, const Ciphertext &b) const;
     Ciphertext relinearize(const Ciphertext &a) const;  // size 3 -> 2 (evaluate.cu:1358-1390)
+    // sum_i w_i X_i + w0 (added to c0) at L primes in one pass, the X_i read at their first L
+    // limbs; w_i and w0 are integers held exactly by doubles; the result is given `scale`
+    // (the terms' common scale times the weights' factor)
+    Ciphertext linear_combination(const std::vector<const Ciphertext *> &X, const std::vector<double> &w, double w0,
+                                  uint32_t L, double scale) const;
     Ciphertext square(const Ciphertext &a) const { return multiply(a, a); }
     // sum_k X_k * P_k (same level and scale), one launch; result scale X.scale * P.scale
     Ciphertext multiply_plain_accumulate(const std::vector<const Ciphertext *> &X,

@@ -195,6 +195,16 @@ int shm_add_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *sc
 int shm_multiply_plain_accumulate(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
                                   uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
                                   void *stream);
+/* out = sum_t w[t] * X[t] + w0 for n_cts size-2 ciphertexts at L limbs, one pass: X[t] is
+ * [n_cts][2][X_levels[t]][N] with X_levels[t] >= L (only its first L limbs are read, so no
+ * limb drop is needed), w is [k][L] residues (the weight of term t mod each prime), w0 is [L]
+ * residues added to c0 (NULL: none); k <= 8, L <= 64.  Replaces the mod_switch_to +
+ * multiply_const + add_inplace per term and the final add_const of a polynomial leaf
+ * (src/include/source/ckks_evaluator_parallel.cuh:245-280, thirdparty/phantom-fhe/src/
+ * evaluate.cu:114-160); the sums mod q are the same, so the result is identical. */
+int shm_linear_combination(const shm_context *ctx, const uint64_t *const *X, const uint32_t *X_levels,
+                           const uint64_t *w, uint32_t k, const uint64_t *w0, uint64_t *out, uint32_t n_cts,
+                           uint32_t L, void *stream);
 /* Mod-raise n_polys one-limb polynomials (mod q0, NTT form) to L limbs by the
  * centred lift.  Replaces Bootstrapper::modraise_inplace (Bootstrapper.cu:3271-3356). */
 size_t shm_modraise_workspace_bytes(const shm_context *ctx, uint32_t n_polys);

@@ -385,6 +385,31 @@ int shm_add_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *sc
     return SHM_OK;
 }
 
+int shm_linear_combination(const shm_context *ctx, const uint64_t *const *X, const uint32_t *X_levels,
+                           const uint64_t *w, uint32_t k, const uint64_t *w0, uint64_t *out, uint32_t n_cts,
+                           uint32_t L, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L) || L > 64) return fail("level out of range");
+    if (!X || !X_levels || !w) return fail("null term arrays");
+    if (k < 1 || k > 8) return fail("linear combination of 1..8 terms");
+    for (uint32_t t = 0; t < k; t++)
+        if (X_levels[t] < L) return fail("a term has fewer limbs than the result");
+    const size_t n = ctx->c->n;
+    for (size_t ct = 0; ct < n_cts; ct++)
+        for (size_t p = 0; p < 2; p++)
+            for (size_t l = 0; l < L; l++) {
+                const uint64_t q = ctx->c->primes[l];
+                uint64_t *o = out + ((ct * 2 + p) * L + l) * n;
+                for (size_t j = 0; j < n; j++) {
+                    uint64_t s = (p == 0 && w0) ? w0[l] % q : 0;
+                    for (uint32_t t = 0; t < k; t++)
+                        s = addmod(s, mulmod(X[t][((ct * 2 + p) * X_levels[t] + l) * n + j], w[t * L + l], q), q);
+                    o[j] = s;
+                }
+            }
+    return SHM_OK;
+}
+
 int shm_multiply_plain_accumulate(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
                                   uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
                                   void *stream) {

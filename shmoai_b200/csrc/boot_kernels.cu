@@ -57,6 +57,32 @@ __global__ void mul_plain_acc_kernel(PtrTab X, PtrTab P, uint32_t k, uint64_t *_
     out[off] = r;
 }
 
+// out[ct][p][limb] = sum_t w_t[limb] X_t[ct][p][limb] (+ w0[limb] for p = 0); each lazy Shoup
+// product is below 2q and the running sum is kept below 4q (one conditional subtraction
+// per term), so the sum stays below 5q < 2^(k+7) for every prime below 2^61 and one
+// reduce_small finishes it.  Grid (N/2/256, L, 2 n_cts).
+__global__ void lin_comb_kernel(LinTerms t, uint64_t *__restrict__ out, uint32_t L, uint32_t log_n,
+                                const PrimeConst *__restrict__ pc) {
+    const uint32_t limb = blockIdx.y, poly = blockIdx.z, ct = poly >> 1, p = poly & 1;
+    const PrimeConst pr = pc[limb];
+    const size_t col = 2 * (blockIdx.x * kT + threadIdx.x);
+    uint64_t a0 = 0, a1 = 0;
+    for (uint32_t i = 0; i < t.k; i++) {
+        const size_t off = ((((size_t)ct * 2 + p) * t.levels[i] + limb) << log_n) + col;
+        const ulonglong2 x = *reinterpret_cast<const ulonglong2 *>(t.x[i] + off);
+        a0 = csub(a0 + shoup_lazy(x.x, t.w[i][limb], t.ws[i][limb], pr.q), 2 * pr.q);
+        a1 = csub(a1 + shoup_lazy(x.y, t.w[i][limb], t.ws[i][limb], pr.q), 2 * pr.q);
+    }
+    if (p == 0 && t.has_w0) {
+        a0 += t.w0[limb];
+        a1 += t.w0[limb];
+    }
+    ulonglong2 r;
+    r.x = reduce_small(a0, pr);
+    r.y = reduce_small(a1, pr);
+    *reinterpret_cast<ulonglong2 *>(out + ((((size_t)ct * 2 + p) * L + limb) << log_n) + col) = r;
+}
+
 // t_j = centred lift of c (mod q0) into prime j, for j < L
 __global__ void modraise_spread(const uint64_t *__restrict__ c0, uint64_t *__restrict__ out, uint32_t L,
                                 uint32_t log_n, const PrimeConst *__restrict__ pc) {
@@ -94,6 +120,18 @@ void mul_plain_acc(const Context &c, const PtrTab &X, const PtrTab &P, uint32_t 
     SHM_LAUNCHED(1);
     mul_plain_acc_kernel<<<dim3(c.n / kT, n_polys * L), kT, 0, st>>>(X, P, k, out, L, c.log_n, c.pc,
                                                                       accumulate ? 1 : 0);
+    SHM_CUDA(cudaGetLastError());
+}
+
+void linear_combination(const Context &c, const LinTerms &t, uint64_t *out, uint32_t n_cts, uint32_t L,
+                        cudaStream_t st) {
+    if (!n_cts) return;
+    if (t.k < 1 || t.k > (uint32_t)kMaxLinTerms) throw std::invalid_argument("linear combination of 1..8 terms");
+    if (L < 1 || L > 64) throw std::invalid_argument("level out of range");
+    for (uint32_t i = 0; i < t.k; i++)
+        if (t.levels[i] < L) throw std::invalid_argument("a term has fewer limbs than the result");
+    SHM_LAUNCHED(1);
+    lin_comb_kernel<<<dim3(c.n / 2 / kT, L, 2 * n_cts), kT, 0, st>>>(t, out, L, c.log_n, c.pc);
     SHM_CUDA(cudaGetLastError());
 }
 

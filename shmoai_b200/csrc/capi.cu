@@ -573,6 +573,37 @@ int shm_add_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *sc
     });
 }
 
+int shm_linear_combination(const shm_context *ctx, const uint64_t *const *X, const uint32_t *X_levels,
+                           const uint64_t *w, uint32_t k, const uint64_t *w0, uint64_t *out, uint32_t n_cts,
+                           uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        if (!X || !X_levels || !w) throw std::invalid_argument("null term arrays");
+        if (k < 1 || k > (uint32_t)shm::kMaxLinTerms) throw std::invalid_argument("linear combination of 1..8 terms");
+        if (L > 64) throw std::invalid_argument("level out of range");
+        set_device(c);
+        std::unique_ptr<shm::LinTerms> t(new shm::LinTerms{});
+        t->k = k;
+        for (uint32_t i = 0; i < k; i++) {
+            t->x[i] = X[i];
+            t->levels[i] = X_levels[i];
+            for (uint32_t l = 0; l < L; l++) {
+                const uint64_t q = c.primes[l], v = w[(size_t)i * L + l];
+                if (v >= q) throw std::invalid_argument("weights must be residues below their prime");
+                t->w[i][l] = v;
+                t->ws[i][l] = shm::host::shoup_of(v, q);
+            }
+        }
+        t->has_w0 = w0 ? 1 : 0;
+        for (uint32_t l = 0; w0 && l < L; l++) {
+            if (w0[l] >= c.primes[l]) throw std::invalid_argument("constant residues must be below their prime");
+            t->w0[l] = w0[l];
+        }
+        shm::linear_combination(c, *t, out, n_cts, L, S(stream));
+    });
+}
+
 int shm_multiply_plain_accumulate(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
                                   uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
                                   void *stream) {

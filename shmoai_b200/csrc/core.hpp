@@ -131,6 +131,18 @@ void add_scalar(const Context &c, const uint64_t *a, uint64_t *out, const Scalar
                 cudaStream_t st);
 void mul_plain_acc(const Context &c, const PtrTab &X, const PtrTab &P, uint32_t k, uint64_t *out, uint32_t n_polys,
                    uint32_t L, bool accumulate, cudaStream_t st);
+// sum_t w_t X_t + w0 (c0 only) over size-2 ciphertexts; weights passed by value
+constexpr int kMaxLinTerms = 8;
+struct LinTerms {
+    const uint64_t *x[kMaxLinTerms];
+    uint32_t levels[kMaxLinTerms];
+    uint64_t w[kMaxLinTerms][64], ws[kMaxLinTerms][64];  // residue and Shoup companion per limb
+    uint64_t w0[64];
+    uint32_t k;
+    int has_w0;
+};
+void linear_combination(const Context &c, const LinTerms &t, uint64_t *out, uint32_t n_cts, uint32_t L,
+                        cudaStream_t st);
 // one-limb polynomials (mod q0, NTT form) -> L-limb centred lift (NTT form); ws: n_polys * N words
 void modraise(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *ws,
               cudaStream_t st);

@@ -439,15 +439,16 @@ Ciphertext cheb_eval(const Evaluator &ev, const Basis &T, const std::vector<doub
     const int d = (int)c.size() - 1;
     if (d < 1) throw Error("Chebyshev piece of degree 0");
     if (d < 8) {
+        // c_0 + sum_i c_i T_i with each term at scale S q: weight round(c_i S q / scale(T_i)),
+        // one linear-combination pass (T_i read at their first lvl + 1 limbs), then the rescale
         const double q = (double)ctx.primes[lvl];
-        Ciphertext acc;
+        std::vector<const Ciphertext *> X;
+        std::vector<double> w;
         for (int i = 1; i <= d; i++) {
-            Ciphertext Ti = ev.mod_switch_to(T.at(i), lvl + 1);
-            Ciphertext term = ev.multiply_const_unscaled(Ti, c[i], S * q / Ti.scale_);
-            term.scale_ = S * q;
-            acc = i == 1 ? std::move(term) : ev.add(acc, term);
+            X.push_back(&T.at(i));
+            w.push_back(std::nearbyint(c[i] * (S * q / T.at(i).scale_)));
         }
-        acc = ev.add_const(acc, c[0]);
+        Ciphertext acc = ev.linear_combination(X, w, std::nearbyint(c[0] * (S * q)), lvl + 1, S * q);
         Ciphertext out = ev.rescale_to_next(acc);
         out.scale_ = S;
         return out;
@@ -483,7 +484,10 @@ Ciphertext BatchBootstrapper::evalmod(const Ciphertext &x, const Evaluator *evp)
     double s = p_.scale * c_fin_;
     for (int i = p_.double_angles - 1; i >= 0; i--) s = std::sqrt(s * (double)c.primes[lvl - 1 - i]);
     Ciphertext y = cheb_eval(ev, T, cheb_, s, lvl);
-    for (int i = 0; i < p_.double_angles; i++) y = ev.add_const(ev.multiply_int(ev.square(y), 2), -1.0);
+    for (int i = 0; i < p_.double_angles; i++) {  // y = 2 y^2 - 1, the affine part in one pass
+        const Ciphertext sq = ev.square(y);
+        y = ev.linear_combination({&sq}, {2.0}, std::nearbyint(-1.0 * sq.scale_), sq.L, sq.scale_);
+    }
     y.scale_ /= c_fin_;
     return y;
 }

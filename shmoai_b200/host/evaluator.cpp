@@ -163,6 +163,32 @@ Ciphertext Evaluator::multiply_const(const Ciphertext &a, double c, double targe
     return o;
 }
 
+Ciphertext Evaluator::linear_combination(const std::vector<const Ciphertext *> &X, const std::vector<double> &w,
+                                         double w0, uint32_t L, double scale) const {
+    if (X.empty() || X.size() != w.size() || X.size() > 8) throw Error("linear_combination: 1..8 terms and weights");
+    std::vector<const uint64_t *> xp;
+    std::vector<uint32_t> lv;
+    std::vector<uint64_t> wr;
+    for (size_t i = 0; i < X.size(); i++) {
+        const Ciphertext &x = *X[i];
+        if (x.shared || x.size != 2 || x.count != X[0]->count) throw Error("linear_combination: size-2 batches of one count");
+        if (x.L < L) throw Error("linear_combination: a term has fewer primes than the result");
+        xp.push_back(x.data.data());
+        lv.push_back(x.L);
+        const std::vector<uint64_t> r = residues(w[i], L);
+        wr.insert(wr.end(), r.begin(), r.end());
+    }
+    const std::vector<uint64_t> r0 = residues(w0, L);
+    Ciphertext o;
+    o.data = DeviceBuffer(c_, (size_t)X[0]->count * 2 * L * c_.n);
+    o.count = X[0]->count;
+    o.L = L;
+    o.scale_ = scale;
+    c_.check(shm_linear_combination(c_.handle(), xp.data(), lv.data(), wr.data(), (uint32_t)xp.size(),
+                                    w0 != 0.0 ? r0.data() : nullptr, o.data.data(), o.count, L, c_.stream()));
+    return o;
+}
+
 Ciphertext Evaluator::multiply_const_unscaled(const Ciphertext &a, double c, double T) const {
     std::vector<uint64_t> r = residues(std::nearbyint(c * T), a.L);
     Ciphertext o = like(a, a.L);
