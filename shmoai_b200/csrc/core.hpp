@@ -85,6 +85,10 @@ void ntt_inverse(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots
                  const uint64_t *scale, cudaStream_t st, uint32_t scale_base = 0);
 
 LimbMap q_map(uint32_t L);
+// forward NTT of the rescale's spread limbs fused with the spread and the combine (RescaleIO);
+// t: [n_polys][L-1][N] scratch between the two phases
+void ntt_forward_rescale(const Context &c, const RescaleIO &io, uint64_t *t, uint32_t n_polys, uint32_t L,
+                         cudaStream_t st);
 
 enum class EwOp { Add, Sub, Negate, MulPlain };
 void elementwise(const Context &c, EwOp op, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,

@@ -83,27 +83,6 @@ __global__ void galois_kernel(const uint64_t *__restrict__ in, uint64_t *__restr
     out[(row << log_n) + k] = in[(row << log_n) + __ldg(perm + k)];
 }
 
-// t_j = c_last mod q_j for j < L-1 (c_last already in coefficient form)
-__global__ void rescale_spread(const uint64_t *__restrict__ last, uint64_t *__restrict__ t, uint32_t L, uint32_t log_n,
-                               const PrimeConst *__restrict__ pc) {
-    const uint32_t j = blockIdx.y, poly = blockIdx.z;
-    const uint32_t k = blockIdx.x * kEwThreads + threadIdx.x;
-    const uint64_t v = last[((size_t)poly << log_n) + k];
-    t[(((size_t)poly * (L - 1) + j) << log_n) + k] = barrett({v, 0}, pc[j]);
-}
-
-// out_j = (c_j - t_j) * q_last^-1 mod q_j
-__global__ void rescale_combine(const uint64_t *__restrict__ in, const uint64_t *__restrict__ t,
-                                uint64_t *__restrict__ out, uint32_t L, uint32_t log_n,
-                                const PrimeConst *__restrict__ pc, const uint64_t *__restrict__ inv) {
-    const uint32_t j = blockIdx.y, poly = blockIdx.z;
-    const uint32_t k = blockIdx.x * kEwThreads + threadIdx.x;
-    const uint64_t q = pc[j].q, w = inv[2 * j], ws = inv[2 * j + 1];
-    const size_t o = (((size_t)poly * (L - 1) + j) << log_n) + k;
-    const uint64_t c = in[(((size_t)poly * L + j) << log_n) + k];
-    out[o] = shoup(sub_mod(c, t[o], q), w, ws, q);
-}
-
 // copy the last limb of every polynomial into a contiguous buffer
 __global__ void gather_last(const uint64_t *__restrict__ in, uint64_t *__restrict__ last, uint32_t L, uint32_t log_n) {
     const uint32_t poly = blockIdx.y;
@@ -170,11 +149,13 @@ void rescale(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_pol
     for (int i = 0; i < 512; i++) m.prime[i] = 255;
     m.prime[0] = (uint8_t)(L - 1);
     ntt_inverse(c, last, n_polys, 1, m, nullptr, st);
-    SHM_LAUNCHED(1); rescale_spread<<<dim3(chunks, L - 1, n_polys), kEwThreads, 0, st>>>(last, t, L, c.log_n, c.pc);
-    ntt_forward(c, t, n_polys * (L - 1), L - 1, q_map(L - 1), st);
-    SHM_LAUNCHED(1); rescale_combine<<<dim3(chunks, L - 1, n_polys), kEwThreads, 0, st>>>(in, t, out, L, c.log_n, c.pc,
-                                                                         c.rescale_inv + 2 * (size_t)(L - 1) * c.nq);
-    SHM_CUDA(cudaGetLastError());
+    // t_j = c_last mod q_j, its NTT and out_j = (c_j - t_j) q_last^-1 in one NTT launch pair
+    RescaleIO io;
+    io.last = last;
+    io.in = in;
+    io.out = out;
+    io.inv = c.rescale_inv + 2 * (size_t)(L - 1) * c.nq;
+    ntt_forward_rescale(c, io, t, n_polys, L, st);
 }
 
 }  // namespace shm

@@ -28,10 +28,12 @@ __device__ __forceinline__ uint32_t limb_major_row(uint32_t t, uint32_t slots, u
 }
 
 // ---------------- forward, phase 1: columns (global stages 0 .. LOGM-1)
-template <int R, int S, int MINB>
+// RS (the rescale's transform, RescaleIO): row (poly, j) is read as c_last[poly] mod q_j from
+// the coefficient-form last limbs instead of from `data`
+template <int R, int S, int MINB, bool RS = false>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
-                                                            const PrimeConst *__restrict__ pc) {
+                                                            const PrimeConst *__restrict__ pc, RescaleIO io) {
     using G = Geo<R, S>;
     __shared__ uint64_t sm[G::M * S];
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
@@ -45,8 +47,15 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 
     const bool grow = q < kGrowPrimeLimit;  // uniform per CTA (one limb)
     uint64_t a[G::E];
+    if constexpr (RS) {
+        const PrimeConst p = pc[pidx];
+        const uint64_t *src = io.last + ((size_t)(row / slots) << G::LOGN) + chunk * S;
 #pragma unroll
-    for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane + m * G::E)];
+        for (int m = 0; m < G::E; m++) a[m] = barrett({src[sig + (size_t)G::M * (lane + m * G::E)], 0}, p);
+    } else {
+#pragma unroll
+        for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane + m * G::E)];
+    }
     if (grow)
         fwd_pass<R, true>(a, w, ws, 1, 0, 0, q);
     else
@@ -65,10 +74,11 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 }
 
 // ---------------- forward, phase 2: blocks (global stages LOGM .. 2*LOGM-1), fully reduced output
-template <int R, int S, int MINB>
+// RS: instead of storing t = NTT(...) of row (poly, j), write (c_j - t) q_last^-1 to io.out
+template <int R, int S, int MINB, bool RS = false>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
-                                                            const PrimeConst *__restrict__ pc) {
+                                                            const PrimeConst *__restrict__ pc, RescaleIO io) {
     using G = Geo<R, S>;
     __shared__ uint64_t sm[S * G::PAD_M];
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
@@ -108,10 +118,24 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
         for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = csub(csub(a[m], q2), q);
     }
     __syncthreads();
+    if constexpr (RS) {
+        const uint32_t poly = row / slots, j = row % slots;
+        const size_t off = (size_t)chunk * S * G::M;
+        const uint64_t *cin = io.in + (((size_t)poly * (slots + 1) + j) << G::LOGN) + off;
+        uint64_t *o = io.out + ((size_t)row << G::LOGN) + off;
+        const uint64_t iw = io.inv[2 * j], iws = io.inv[2 * j + 1];
 #pragma unroll
-    for (int i = 0; i < G::E; i++) {
-        uint32_t e = threadIdx.x + i * G::THREADS;
-        xc[e] = sm[(e / G::M) * G::PAD_M + padded(e % G::M)];
+        for (int i = 0; i < G::E; i++) {
+            uint32_t e = threadIdx.x + i * G::THREADS;
+            const uint64_t t = sm[(e / G::M) * G::PAD_M + padded(e % G::M)];
+            o[e] = shoup(sub_mod(cin[e], t, q), iw, iws, q);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < G::E; i++) {
+            uint32_t e = threadIdx.x + i * G::THREADS;
+            xc[e] = sm[(e / G::M) * G::PAD_M + padded(e % G::M)];
+        }
     }
 }
 
@@ -210,15 +234,15 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__
     for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane + m * G::E)] = a[m];
 }
 
-template <int R, int S, int MINB>
+template <int R, int S, int MINB, bool RS = false>
 void launch_fwd_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
-                  cudaStream_t st) {
+                  cudaStream_t st, const RescaleIO &io = RescaleIO{}) {
     using G = Geo<R, S>;
     dim3 grid(rows * G::CHUNKS);
     SHM_LAUNCHED(1);
-    fwd_col<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+    fwd_col<R, S, MINB, RS><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
     SHM_LAUNCHED(1);
-    fwd_blk<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+    fwd_blk<R, S, MINB, RS><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
 }
 
 template <int R, int S, int MINB>
@@ -234,14 +258,14 @@ void launch_inv_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slot
 }
 
 // the tile variants of kNttVariants (ntt.cuh), selected per context by c.ntt_variant
-template <int R>
+template <int R, bool RS = false>
 void launch_fwd(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
-                cudaStream_t st) {
+                cudaStream_t st, const RescaleIO &io = RescaleIO{}) {
     switch (c.ntt_variant) {
-        case 1: launch_fwd_v<R, 16, 3>(c, data, rows, slots, map, st); break;
-        case 2: launch_fwd_v<R, 8, 8>(c, data, rows, slots, map, st); break;
-        case 3: launch_fwd_v<R, 8, 6>(c, data, rows, slots, map, st); break;
-        default: launch_fwd_v<R, 16, 4>(c, data, rows, slots, map, st); break;
+        case 1: launch_fwd_v<R, 16, 3, RS>(c, data, rows, slots, map, st, io); break;
+        case 2: launch_fwd_v<R, 8, 8, RS>(c, data, rows, slots, map, st, io); break;
+        case 3: launch_fwd_v<R, 8, 6, RS>(c, data, rows, slots, map, st, io); break;
+        default: launch_fwd_v<R, 16, 4, RS>(c, data, rows, slots, map, st, io); break;
     }
 }
 
@@ -269,6 +293,15 @@ void ntt_forward(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots
     if (rows == 0) return;
     if (c.log_n == 16) launch_fwd<4>(c, data, rows, slots, map, st);
     else if (c.log_n == 12) launch_fwd<3>(c, data, rows, slots, map, st);
+    else throw std::invalid_argument("NTT supports N = 2^12 and 2^16");
+    SHM_CUDA(cudaGetLastError());
+}
+
+void ntt_forward_rescale(const Context &c, const RescaleIO &io, uint64_t *t, uint32_t n_polys, uint32_t L,
+                         cudaStream_t st) {
+    if (n_polys == 0) return;
+    if (c.log_n == 16) launch_fwd<4, true>(c, t, n_polys * (L - 1), L - 1, q_map(L - 1), st, io);
+    else if (c.log_n == 12) launch_fwd<3, true>(c, t, n_polys * (L - 1), L - 1, q_map(L - 1), st, io);
     else throw std::invalid_argument("NTT supports N = 2^12 and 2^16");
     SHM_CUDA(cudaGetLastError());
 }

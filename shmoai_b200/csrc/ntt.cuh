@@ -35,6 +35,15 @@ struct LimbMap {
     uint8_t prime[512];  // limb slot within a polynomial -> prime index; 255 = leave untouched
 };
 
+// The rescale's forward NTT (ntt_forward_rescale): rows (poly, j < L-1) are read as
+// last[poly] mod q_j and written as (in[poly][j] - NTT(...)) * q_{L-1}^-1 into out[poly][j]
+struct RescaleIO {
+    const uint64_t *last = nullptr;  // [polys][N], c_{L-1} in coefficient form
+    const uint64_t *in = nullptr;    // [polys][L][N]
+    uint64_t *out = nullptr;         // [polys][L-1][N]
+    const uint64_t *inv = nullptr;   // [L-1][2]: q_{L-1}^-1 mod q_j and its Shoup companion
+};
+
 // scale constants of the inverse's last stage, per limb slot: c, c', c*psi^-(N/2), (c*psi^-(N/2))'
 struct InvScale {
     const uint64_t *c;  // [slots][4]
