@@ -89,6 +89,10 @@ LimbMap q_map(uint32_t L);
 // t: [n_polys][L-1][N] scratch between the two phases
 void ntt_forward_rescale(const Context &c, const RescaleIO &io, uint64_t *t, uint32_t n_polys, uint32_t L,
                          cudaStream_t st);
+// ModDown's conversion, forward NTT and combine in one launch pair (ModDownIO); delta:
+// [n_polys][L][N] scratch between the two phases
+void ntt_forward_moddown(const Context &c, const ModDownIO &md, uint64_t *delta, uint32_t n_polys, uint32_t L,
+                         cudaStream_t st);
 
 enum class EwOp { Add, Sub, Negate, MulPlain };
 void elementwise(const Context &c, EwOp op, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,

@@ -115,52 +115,6 @@ void launch_inner_product(dim3 grid, cudaStream_t st, const uint64_t *up, const 
 #undef SHM_IP_CASE
 }
 
-// delta[ct][h][j][k] = sum_k' z[ct][h][L+k'][k] * (phat_k' mod q_j), j < L
-template <bool S52>
-__global__ void moddown_conv_kernel(const uint64_t *__restrict__ acc, uint64_t *__restrict__ delta,
-                                    const uint64_t *__restrict__ conv, uint32_t L, uint32_t np, uint32_t log_n,
-                                    const PrimeConst *__restrict__ pc) {
-    const uint32_t hc = blockIdx.y;  // ct * 2 + h
-    const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
-    const size_t n = (size_t)1 << log_n;
-    const uint32_t LP = L + np;
-    const uint64_t *z = acc + (size_t)hc * LP * n + (size_t)L * n + k;
-    uint64_t zv[kMaxAlpha];
-#pragma unroll
-    for (int i = 0; i < kMaxAlpha; i++)
-        if (i < (int)np) zv[i] = z[(size_t)i * n];
-    uint64_t *o = delta + (size_t)hc * L * n + k;
-    for (uint32_t j = 0; j < L; j++) {
-        const uint64_t *cj = conv + (size_t)j * np;
-        Acc<S52> a;
-#pragma unroll
-        for (int i = 0; i < kMaxAlpha; i++)
-            if (i < (int)np) a.add(zv[i], __ldg(cj + i));
-        o[(size_t)j * n] = barrett(a.get(), pc[j]);
-    }
-}
-
-// out_h[j] = add_h[j] + (acc_h[j] - delta_h[j]) * P^-1
-__global__ void ks_combine_kernel(const uint64_t *__restrict__ acc, const uint64_t *__restrict__ delta, KsOutput o,
-                                  uint32_t L, uint32_t np, uint32_t log_n, const PrimeConst *__restrict__ pc,
-                                  const uint64_t *__restrict__ pinv) {
-    const uint32_t j = blockIdx.y, hc = blockIdx.z, ct = hc >> 1, h = hc & 1;
-    const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
-    const size_t n = (size_t)1 << log_n;
-    const uint64_t q = pc[j].q;
-    const uint64_t a = acc[((size_t)hc * (L + np) + j) * n + k];
-    const uint64_t dl = delta[((size_t)hc * L + j) * n + k];
-    uint64_t r = shoup(sub_mod(a, dl, q), pinv[2 * j], pinv[2 * j + 1], q);
-    const size_t off = (size_t)ct * o.stride + (size_t)j * n + k;
-    const uint64_t *add = h ? o.add1 : o.add0;
-    if (add) {
-        const size_t aoff = (h == 0 && o.add0_perm) ? (size_t)ct * o.stride + (size_t)j * n + __ldg(o.add0_perm + k)
-                                                    : off;
-        r = add_mod(r, add[aoff], q);
-    }
-    (h ? o.out1 : o.out0)[off] = r;
-}
-
 // the kernels above for one context: Acc<true> when every prime is below 2^52
 void launch_modup_conv(const Context &c, uint32_t n_cts, uint32_t L, const uint64_t *x, const uint64_t *d,
                        size_t d_stride, uint64_t *up, cudaStream_t st) {
@@ -187,16 +141,28 @@ void launch_ip(const Context &c, uint32_t n_cts, uint32_t L, const uint64_t *up,
     SHM_CUDA(cudaGetLastError());
 }
 
-void launch_moddown_conv(const Context &c, uint32_t n_polys, uint32_t L, const uint64_t *acc, uint64_t *delta,
-                         cudaStream_t st) {
-    const dim3 grid(c.n / kThreads, n_polys);
-    SHM_LAUNCHED(1);
-    if (c.s52)
-        moddown_conv_kernel<true><<<grid, kThreads, 0, st>>>(acc, delta, c.moddown_conv, L, c.np, c.log_n, c.pc);
-    else
-        moddown_conv_kernel<false><<<grid, kThreads, 0, st>>>(acc, delta, c.moddown_conv, L, c.np, c.log_n, c.pc);
-    SHM_CUDA(cudaGetLastError());
+// the fused ModDown's addressing for a KsOutput (out1 = out0 + L N, add1 = add0 + L N or null,
+// one stride for out and add; add0 read through add0_perm when set)
+ModDownIO moddown_io(const Context &c, const uint64_t *acc, const KsOutput &o) {
+    ModDownIO md;
+    md.acc = acc;
+    md.conv = c.moddown_conv;
+    md.pinv = c.p_inv;
+    md.out = o.out0;
+    md.out_ct = (long long)o.stride;
+    md.out_h = (long long)(o.out1 - o.out0);
+    md.add = o.add0;
+    md.add_ct = (long long)o.stride;
+    md.add_h = o.add1 ? (long long)(o.add1 - o.add0) : 0;
+    md.n_add = o.add0 ? (o.add1 ? 2 : 1) : 0;
+    md.perm = o.add0_perm;
+    md.n_perm = 1;
+    md.H = 2;
+    md.np = c.np;
+    md.s52 = c.s52 ? 1 : 0;
+    return md;
 }
+
 
 }  // namespace
 
@@ -228,11 +194,7 @@ void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_
     LimbMap mp;
     for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
     ntt_inverse(c, acc, n_cts * 2 * LP, LP, mp, c.moddown_scale, st, L);
-    launch_moddown_conv(c, n_cts * 2, L, acc, delta, st);
-    ntt_forward(c, delta, n_cts * 2 * L, L, q_map(L), st);
-    SHM_LAUNCHED(1); ks_combine_kernel<<<dim3(n / kThreads, L, n_cts * 2), kThreads, 0, st>>>(acc, delta, o, L, np, c.log_n, c.pc,
-                                                                             c.p_inv);
-    SHM_CUDA(cudaGetLastError());
+    ntt_forward_moddown(c, moddown_io(c, acc, o), delta, n_cts * 2, L, st);
 }
 
 // ModUp of n_cts polynomials d (stride d_stride words) into up [n_cts][beta][LP][N]; x is
@@ -290,13 +252,8 @@ void apply_galois_hoisted(const Context &c, const uint64_t *ct, uint32_t n_cts, 
         const uint32_t *perm = const_cast<Context &>(c).perm(elts[e]);
         launch_ip(c, n_cts, L, up, keys[e], acc, perm, st);
         ntt_inverse(c, acc, n_cts * 2 * LP, LP, mp, c.moddown_scale, st, L);
-        launch_moddown_conv(c, n_cts * 2, L, acc, delta, st);
-        ntt_forward(c, delta, n_cts * 2 * L, L, q_map(L), st);
         KsOutput o{outs[e], outs[e] + ln, ct, nullptr, 2 * ln, perm};
-        SHM_LAUNCHED(1);
-        ks_combine_kernel<<<dim3(n / kThreads, L, n_cts * 2), kThreads, 0, st>>>(acc, delta, o, L, np, c.log_n, c.pc,
-                                                                                 c.p_inv);
-        SHM_CUDA(cudaGetLastError());
+        ntt_forward_moddown(c, moddown_io(c, acc, o), delta, n_cts * 2, L, st);
     }
 }
 

@@ -28,12 +28,13 @@ __device__ __forceinline__ uint32_t limb_major_row(uint32_t t, uint32_t slots, u
 }
 
 // ---------------- forward, phase 1: columns (global stages 0 .. LOGM-1)
-// RS (the rescale's transform, RescaleIO): row (poly, j) is read as c_last[poly] mod q_j from
-// the coefficient-form last limbs instead of from `data`
-template <int R, int S, int MINB, bool RS = false>
+// IOK = kIoRescale: row (poly, j) is read as c_last[poly] mod q_j from the coefficient-form
+// last limbs; kIoModDown: as the base conversion of the special-prime limbs (ModDownIO);
+// kIoPlain: from `data`
+template <int R, int S, int MINB, int IOK = kIoPlain>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
-                                                            const PrimeConst *__restrict__ pc, RescaleIO io) {
+                                                            const PrimeConst *__restrict__ pc, NttIO io) {
     using G = Geo<R, S>;
     __shared__ uint64_t sm[G::M * S];
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
@@ -47,11 +48,31 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 
     const bool grow = q < kGrowPrimeLimit;  // uniform per CTA (one limb)
     uint64_t a[G::E];
-    if constexpr (RS) {
+    if constexpr (IOK == kIoRescale) {
         const PrimeConst p = pc[pidx];
-        const uint64_t *src = io.last + ((size_t)(row / slots) << G::LOGN) + chunk * S;
+        const uint64_t *src = io.rs.last + ((size_t)(row / slots) << G::LOGN) + chunk * S;
 #pragma unroll
         for (int m = 0; m < G::E; m++) a[m] = barrett({src[sig + (size_t)G::M * (lane + m * G::E)], 0}, p);
+    } else if constexpr (IOK == kIoModDown) {
+        __shared__ uint64_t sconv[16];
+        const uint32_t np = io.md.np, j = row % slots;
+        if (threadIdx.x < np) sconv[threadIdx.x] = io.md.conv[(size_t)j * np + threadIdx.x];
+        __syncthreads();
+        const PrimeConst p = pc[pidx];
+        const uint64_t *z = io.md.acc + ((size_t)((row / slots) * (slots + np) + slots) << G::LOGN) + chunk * S;
+#pragma unroll
+        for (int m = 0; m < G::E; m++) {
+            const size_t pos = sig + (size_t)G::M * (lane + m * G::E);
+            if (io.md.s52) {
+                Acc<true> acc;
+                for (uint32_t k = 0; k < np; k++) acc.add(z[((size_t)k << G::LOGN) + pos], sconv[k]);
+                a[m] = barrett(acc.get(), p);
+            } else {
+                Acc<false> acc;
+                for (uint32_t k = 0; k < np; k++) acc.add(z[((size_t)k << G::LOGN) + pos], sconv[k]);
+                a[m] = barrett(acc.get(), p);
+            }
+        }
     } else {
 #pragma unroll
         for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane + m * G::E)];
@@ -74,11 +95,12 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 }
 
 // ---------------- forward, phase 2: blocks (global stages LOGM .. 2*LOGM-1), fully reduced output
-// RS: instead of storing t = NTT(...) of row (poly, j), write (c_j - t) q_last^-1 to io.out
-template <int R, int S, int MINB, bool RS = false>
+// IOK = kIoRescale: instead of storing t = NTT(...) of row (poly, j), write (c_j - t) q_last^-1
+// to io.rs.out; kIoModDown: write (acc_j - t) P^-1 (+ add) to io.md.out
+template <int R, int S, int MINB, int IOK = kIoPlain>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
-                                                            const PrimeConst *__restrict__ pc, RescaleIO io) {
+                                                            const PrimeConst *__restrict__ pc, NttIO io) {
     using G = Geo<R, S>;
     __shared__ uint64_t sm[S * G::PAD_M];
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
@@ -118,17 +140,34 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
         for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = csub(csub(a[m], q2), q);
     }
     __syncthreads();
-    if constexpr (RS) {
+    if constexpr (IOK == kIoRescale) {
         const uint32_t poly = row / slots, j = row % slots;
         const size_t off = (size_t)chunk * S * G::M;
-        const uint64_t *cin = io.in + (((size_t)poly * (slots + 1) + j) << G::LOGN) + off;
-        uint64_t *o = io.out + ((size_t)row << G::LOGN) + off;
-        const uint64_t iw = io.inv[2 * j], iws = io.inv[2 * j + 1];
+        const uint64_t *cin = io.rs.in + (((size_t)poly * (slots + 1) + j) << G::LOGN) + off;
+        uint64_t *o = io.rs.out + ((size_t)row << G::LOGN) + off;
+        const uint64_t iw = io.rs.inv[2 * j], iws = io.rs.inv[2 * j + 1];
 #pragma unroll
         for (int i = 0; i < G::E; i++) {
             uint32_t e = threadIdx.x + i * G::THREADS;
             const uint64_t t = sm[(e / G::M) * G::PAD_M + padded(e % G::M)];
             o[e] = shoup(sub_mod(cin[e], t, q), iw, iws, q);
+        }
+    } else if constexpr (IOK == kIoModDown) {
+        const ModDownIO &md = io.md;
+        const uint32_t poly = row / slots, j = row % slots, ct = poly / md.H, h = poly % md.H;
+        const size_t off = (size_t)chunk * S * G::M;
+        const uint64_t *ain = md.acc + (((size_t)poly * (slots + md.np) + j) << G::LOGN) + off;
+        uint64_t *o = md.out + ct * md.out_ct + h * md.out_h + ((size_t)j << G::LOGN) + off;
+        const uint64_t iw = md.pinv[2 * j], iws = md.pinv[2 * j + 1];
+        const bool add = h < md.n_add, perm = add && h < md.n_perm && md.perm;
+        const uint64_t *ad = add ? md.add + ct * md.add_ct + h * md.add_h + ((size_t)j << G::LOGN) : nullptr;
+#pragma unroll
+        for (int i = 0; i < G::E; i++) {
+            uint32_t e = threadIdx.x + i * G::THREADS;
+            const uint64_t t = sm[(e / G::M) * G::PAD_M + padded(e % G::M)];
+            uint64_t r = shoup(sub_mod(ain[e], t, q), iw, iws, q);
+            if (add) r = add_mod(r, ad[perm ? __ldg(md.perm + off + e) : off + e], q);
+            o[e] = r;
         }
     } else {
 #pragma unroll
@@ -234,15 +273,15 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__
     for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane + m * G::E)] = a[m];
 }
 
-template <int R, int S, int MINB, bool RS = false>
+template <int R, int S, int MINB, int IOK = kIoPlain>
 void launch_fwd_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
-                  cudaStream_t st, const RescaleIO &io = RescaleIO{}) {
+                  cudaStream_t st, const NttIO &io = NttIO{}) {
     using G = Geo<R, S>;
     dim3 grid(rows * G::CHUNKS);
     SHM_LAUNCHED(1);
-    fwd_col<R, S, MINB, RS><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
+    fwd_col<R, S, MINB, IOK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
     SHM_LAUNCHED(1);
-    fwd_blk<R, S, MINB, RS><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
+    fwd_blk<R, S, MINB, IOK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
 }
 
 template <int R, int S, int MINB>
@@ -258,14 +297,14 @@ void launch_inv_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slot
 }
 
 // the tile variants of kNttVariants (ntt.cuh), selected per context by c.ntt_variant
-template <int R, bool RS = false>
+template <int R, int IOK = kIoPlain>
 void launch_fwd(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
-                cudaStream_t st, const RescaleIO &io = RescaleIO{}) {
+                cudaStream_t st, const NttIO &io = NttIO{}) {
     switch (c.ntt_variant) {
-        case 1: launch_fwd_v<R, 16, 3, RS>(c, data, rows, slots, map, st, io); break;
-        case 2: launch_fwd_v<R, 8, 8, RS>(c, data, rows, slots, map, st, io); break;
-        case 3: launch_fwd_v<R, 8, 6, RS>(c, data, rows, slots, map, st, io); break;
-        default: launch_fwd_v<R, 16, 4, RS>(c, data, rows, slots, map, st, io); break;
+        case 1: launch_fwd_v<R, 16, 3, IOK>(c, data, rows, slots, map, st, io); break;
+        case 2: launch_fwd_v<R, 8, 8, IOK>(c, data, rows, slots, map, st, io); break;
+        case 3: launch_fwd_v<R, 8, 6, IOK>(c, data, rows, slots, map, st, io); break;
+        default: launch_fwd_v<R, 16, 4, IOK>(c, data, rows, slots, map, st, io); break;
     }
 }
 
@@ -297,11 +336,25 @@ void ntt_forward(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots
     SHM_CUDA(cudaGetLastError());
 }
 
-void ntt_forward_rescale(const Context &c, const RescaleIO &io, uint64_t *t, uint32_t n_polys, uint32_t L,
+void ntt_forward_rescale(const Context &c, const RescaleIO &rs, uint64_t *t, uint32_t n_polys, uint32_t L,
                          cudaStream_t st) {
     if (n_polys == 0) return;
-    if (c.log_n == 16) launch_fwd<4, true>(c, t, n_polys * (L - 1), L - 1, q_map(L - 1), st, io);
-    else if (c.log_n == 12) launch_fwd<3, true>(c, t, n_polys * (L - 1), L - 1, q_map(L - 1), st, io);
+    NttIO io;
+    io.rs = rs;
+    if (c.log_n == 16) launch_fwd<4, kIoRescale>(c, t, n_polys * (L - 1), L - 1, q_map(L - 1), st, io);
+    else if (c.log_n == 12) launch_fwd<3, kIoRescale>(c, t, n_polys * (L - 1), L - 1, q_map(L - 1), st, io);
+    else throw std::invalid_argument("NTT supports N = 2^12 and 2^16");
+    SHM_CUDA(cudaGetLastError());
+}
+
+void ntt_forward_moddown(const Context &c, const ModDownIO &md, uint64_t *delta, uint32_t n_polys, uint32_t L,
+                         cudaStream_t st) {
+    if (n_polys == 0) return;
+    if (md.np > 16 || md.H == 0) throw std::invalid_argument("ModDown: shape out of range");
+    NttIO io;
+    io.md = md;
+    if (c.log_n == 16) launch_fwd<4, kIoModDown>(c, delta, n_polys * L, L, q_map(L), st, io);
+    else if (c.log_n == 12) launch_fwd<3, kIoModDown>(c, delta, n_polys * L, L, q_map(L), st, io);
     else throw std::invalid_argument("NTT supports N = 2^12 and 2^16");
     SHM_CUDA(cudaGetLastError());
 }

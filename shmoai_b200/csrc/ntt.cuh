@@ -44,6 +44,29 @@ struct RescaleIO {
     const uint64_t *inv = nullptr;   // [L-1][2]: q_{L-1}^-1 mod q_j and its Shoup companion
 };
 
+// The ModDown's forward NTT (ntt_forward_moddown): rows (poly, j < L) of the delta buffer are
+// read as the base conversion sum_k z_k (phat_k mod q_j) of the INTT'd special-prime limbs
+// z_k = acc[poly][L + k], and written as (acc[poly][j] - NTT(...)) P^-1 (+ add) into out;
+// poly = ct * H + h.  The add term of rows h < n_add is read at perm[pos] for rows h < n_perm.
+struct ModDownIO {
+    const uint64_t *acc = nullptr;   // [polys][L + np][N]
+    const uint64_t *conv = nullptr;  // [nq][np]: phat_k mod q_j
+    const uint64_t *pinv = nullptr;  // [nq][2]: P^-1 mod q_j and its Shoup companion
+    uint64_t *out = nullptr;
+    const uint64_t *add = nullptr;
+    const uint32_t *perm = nullptr;
+    long long out_ct = 0, out_h = 0, add_ct = 0, add_h = 0;  // word strides
+    uint32_t H = 2, np = 0, n_add = 0, n_perm = 0;
+    int s52 = 0;  // every prime below 2^52: Acc<true>
+};
+
+// the optional load / store transforms of the forward NTT kernels
+struct NttIO {
+    RescaleIO rs;
+    ModDownIO md;
+};
+constexpr int kIoPlain = 0, kIoRescale = 1, kIoModDown = 2;
+
 // scale constants of the inverse's last stage, per limb slot: c, c', c*psi^-(N/2), (c*psi^-(N/2))'
 struct InvScale {
     const uint64_t *c;  // [slots][4]

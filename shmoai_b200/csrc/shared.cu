@@ -75,30 +75,6 @@ __global__ void __launch_bounds__(kIpT) ip_multi_kernel(const uint64_t *__restri
     }
 }
 
-template <bool S52>
-__global__ void moddown_multi_conv(const uint64_t *__restrict__ acc, uint64_t *__restrict__ delta,
-                                   const uint64_t *__restrict__ conv, uint32_t L, uint32_t np, uint32_t log_n,
-                                   const PrimeConst *__restrict__ pc) {
-    const uint32_t poly = blockIdx.y;
-    const uint32_t k = blockIdx.x * kT + threadIdx.x;
-    const size_t n = (size_t)1 << log_n;
-    const uint32_t LP = L + np;
-    const uint64_t *z = acc + (size_t)poly * LP * n + (size_t)L * n + k;
-    uint64_t zv[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++)
-        if (i < (int)np) zv[i] = z[(size_t)i * n];
-    uint64_t *o = delta + (size_t)poly * L * n + k;
-    for (uint32_t j = 0; j < L; j++) {
-        const uint64_t *cj = conv + (size_t)j * np;
-        Acc<S52> a;
-#pragma unroll
-        for (int i = 0; i < 16; i++)
-            if (i < (int)np) a.add(zv[i], __ldg(cj + i));
-        o[(size_t)j * n] = barrett(a.get(), pc[j]);
-    }
-}
-
 struct Target {
     const uint64_t *key;  // [beta][H][QP][N]
     const uint32_t *perm;
@@ -108,24 +84,6 @@ struct Target {
     size_t add_ct, add_h;
     uint32_t n_add;
 };
-
-// out[ct][h][j] = add[ct][h][j @ perm] (h < n_add) + (acc - delta) * P^-1
-__global__ void combine_multi(const uint64_t *__restrict__ acc, const uint64_t *__restrict__ delta, Target t,
-                              uint32_t H, uint32_t L, uint32_t np, uint32_t log_n, const PrimeConst *__restrict__ pc,
-                              const uint64_t *__restrict__ pinv) {
-    const uint32_t j = blockIdx.y, hc = blockIdx.z, ct = hc / H, h = hc % H;
-    const uint32_t k = blockIdx.x * kT + threadIdx.x;
-    const size_t n = (size_t)1 << log_n;
-    const uint64_t q = pc[j].q;
-    const uint64_t a = acc[((size_t)hc * (L + np) + j) * n + k];
-    const uint64_t dl = delta[((size_t)hc * L + j) * n + k];
-    uint64_t r = shoup(sub_mod(a, dl, q), pinv[2 * j], pinv[2 * j + 1], q);
-    if (h < t.n_add) {
-        const uint32_t ka = t.perm ? __ldg(t.perm + k) : k;
-        r = add_mod(r, t.add[ct * t.add_ct + h * t.add_h + (size_t)j * n + ka], q);
-    }
-    t.out[ct * t.out_ct + h * t.out_h + (size_t)j * n + k] = r;
-}
 
 // exact Ql -> P extension (floor-corrected CRT): x = sum_i y_i qhat_i - v Q, v = floor(sum_i y_i / q_i),
 // y_i = [x_i qhat_i^-1]_{q_i} already in the coefficient buffer; writes the P rows of ext
@@ -239,24 +197,29 @@ void check_shape(const Context &c, uint32_t L, uint32_t beta, uint32_t H) {
 // inner products, ModDown and combine for one target; acc/delta are workspace
 void apply_target(const Context &c, const uint64_t *up, uint32_t n_cts, uint32_t L, uint32_t beta, uint32_t H,
                   const Target &t, uint64_t *acc, uint64_t *delta, cudaStream_t st) {
-    const size_t n = c.n;
     const uint32_t np = c.np, LP = L + np;
     ip_multi(c, up, t.key, acc, n_cts, L, beta, H, t.perm, st);
     LimbMap mp;
     for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
     ntt_inverse(c, acc, n_cts * H * LP, LP, mp, c.moddown_scale, st, L);
-    SHM_LAUNCHED(1);
-    if (c.s52)
-        moddown_multi_conv<true><<<dim3(n / kT, n_cts * H), kT, 0, st>>>(acc, delta, c.moddown_conv, L, np, c.log_n,
-                                                                         c.pc);
-    else
-        moddown_multi_conv<false><<<dim3(n / kT, n_cts * H), kT, 0, st>>>(acc, delta, c.moddown_conv, L, np, c.log_n,
-                                                                          c.pc);
-    SHM_CUDA(cudaGetLastError());
-    ntt_forward(c, delta, n_cts * H * L, L, q_map(L), st);
-    SHM_LAUNCHED(1);
-    combine_multi<<<dim3(n / kT, L, n_cts * H), kT, 0, st>>>(acc, delta, t, H, L, np, c.log_n, c.pc, c.p_inv);
-    SHM_CUDA(cudaGetLastError());
+    // conversion of the special-prime limbs, NTT and (acc - delta) P^-1 + sigma(add) fused
+    ModDownIO md;
+    md.acc = acc;
+    md.conv = c.moddown_conv;
+    md.pinv = c.p_inv;
+    md.out = t.out;
+    md.out_ct = (long long)t.out_ct;
+    md.out_h = (long long)t.out_h;
+    md.add = t.add;
+    md.add_ct = (long long)t.add_ct;
+    md.add_h = (long long)t.add_h;
+    md.n_add = t.add ? t.n_add : 0;
+    md.perm = t.perm;
+    md.n_perm = md.n_add;
+    md.H = H;
+    md.np = np;
+    md.s52 = c.s52 ? 1 : 0;
+    ntt_forward_moddown(c, md, delta, n_cts * H, L, st);
 }
 
 }  // namespace
