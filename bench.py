@@ -758,10 +758,11 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="time the step only (no e2e, roofline or CPU legs): used for ncu launch lists")
     ap.add_argument("--small", action="store_true",
-                    help="ctpt: 256 -> 256 ciphertexts at 4 limbs (about 1 GB on the device) for ncu captures")
+                    help="ctpt: 768 -> 768 ciphertexts at 1 limb, one column chunk of the full projection "
+                         "(about 4 GB on the device) for ncu captures")
     args = ap.parse_args()
     if args.small:
-        CTPT.update(n_in=256, n_out=256, L=4)
+        CTPT.update(L=1)
     if args.batch is None:
         args.batch = 32 if args.workload == "boot" else 1
 

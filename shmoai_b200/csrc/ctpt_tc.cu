@@ -19,6 +19,7 @@
 // K in 64-byte stages (4-stage cp.async ring, one mbarrier per stage), s32
 // accumulator in TMEM (256 columns) -> epilogue tcgen05.ld, acc mod m_t -> uint8
 // residue planes -> CRT kernel.
+#include <cmath>
 #include <cstring>
 
 #include "core.hpp"
@@ -29,20 +30,20 @@ namespace shm {
 namespace {
 
 constexpr int kMaxMods = 20;
-constexpr uint32_t kBM = 128;   // X columns per tile (MMA M)
-constexpr uint32_t kBN = 256;   // outputs per tile (MMA N)
+constexpr uint32_t kBM = 128;   // outputs per tile (MMA M: A = the weight residues)
+constexpr uint32_t kBN = 256;   // X columns per tile (MMA N: B = the X residues)
 constexpr uint32_t kKB = 64;    // K bytes per stage (two k32 MMAs)
 constexpr int kStages = 4;
 constexpr uint32_t kStageA = kBM * kKB;  // 8 KB
 constexpr uint32_t kStageB = kBN * kKB;  // 16 KB
 constexpr uint32_t kSmem = kStages * (kStageA + kStageB) + 1024;
-constexpr uint32_t kThreads = 128;
+constexpr uint32_t kThreads = 256;  // two warpgroups: loads shared, epilogue split by output columns
 constexpr long long kSpinLimit = 1ll << 24;
 
 struct ModTab {
     uint32_t t;
     uint32_t m[kMaxMods];
-    float frac[kMaxMods];   // [(M/m_t)^-1]_{m_t} / m_t
+    uint32_t fracx[kMaxMods];  // [(M/m_t)^-1]_{m_t} / m_t as a 32-bit fixed-point fraction
     uint32_t c24[kMaxMods];  // 2^20 mod m_t
     uint32_t c48[kMaxMods];  // 2^40 mod m_t
     uint32_t magic[kMaxMods];  // ceil(2^32 / m_t)
@@ -68,6 +69,18 @@ __device__ __forceinline__ uint32_t mod_small(uint64_t x, uint32_t t) {
 
 // a mod m_t in [0, m_t) for any int32 accumulator: a + m * 2^24 (a multiple of m above
 // 2^31, the moduli being > 128) is non-negative and below 2^33, then the 32-bit fold above
+// a mod m_t for |a| < 2^24 (every accumulator: n_in * 125^2 < 2^24 up to n_in = 1073): a is
+// exact in float, floor(a / m) from one float multiply is off by at most one (relative error
+// ~2^-24 of a quotient below 2^17), and two conditional corrections finish it
+__device__ __forceinline__ uint32_t mod_acc24(int a, uint32_t t) {
+    const int m = (int)c_mods.m[t];
+    const int q = __float2int_rd((float)a * c_mods.invf[t]);
+    int r = a - q * m;
+    r += r < 0 ? m : 0;
+    r -= r >= m ? m : 0;
+    return (uint32_t)r;
+}
+
 __device__ __forceinline__ uint32_t mod_acc(int a, uint32_t t) {
     const uint64_t x = (uint64_t)((int64_t)a + ((int64_t)c_mods.m[t] << 24));
     return mod_small(x, t);
@@ -147,22 +160,35 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
-// grid: (R_chunk / 128, Np / 256, T); one modulus per blockIdx.z
-// Two CTAs per SM (2 x 97 KB shared memory, 2 x 256 TMEM columns): one CTA's loads and
-// epilogue overlap the other's MMAs.
+// grid: (Np / 128, R_chunk / 256, T); one modulus per blockIdx.z.  D[o][r] = W[o] . X[r]: the
+// weights are A (128 outputs, TMEM lanes), the X residues B (256 columns, TMEM columns), so an
+// epilogue thread holds 32 consecutive columns of one output and writes them as two 16-byte
+// stores.  The output tiles are the fastest grid dimension: the CTAs that share an X tile
+// run together and read it from HBM once (then from L2).  Two CTAs per SM (2 x 97 KB shared
+// memory, 2 x 256 TMEM columns).
+//
+// Warp-specialised: warps 0-3 fill a kStages-deep ring with cp.async (each producer thread
+// waits for its own copies of the previous stage, fences them into the async proxy and
+// arrives on that stage's `full` barrier); one thread of warp 4 issues the MMAs of a stage
+// once it is full and frees it through tcgen05.commit on its `empty` barrier; after the
+// last commit (`done`) all eight warps read the accumulators back.  No block-wide barrier
+// inside the K loop; every wait is bounded (a timeout sets *err and skips the stores).
 __global__ void __launch_bounds__(kThreads, 2) mma_kernel(const int8_t *__restrict__ XP, const int8_t *__restrict__ WP,
                                                           uint8_t *__restrict__ RES, uint32_t Kp, uint32_t Np,
-                                                          uint32_t n_out, uint64_t chunk, int *__restrict__ err) {
+                                                          uint32_t n_out, uint64_t chunk, int *__restrict__ err,
+                                                          int acc24) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bars[kStages];
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages], done;
     __shared__ uint32_t tmem_base;
+    __shared__ int failed;
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t t = blockIdx.z;
-    const uint64_t rbase = (uint64_t)blockIdx.x * kBM;
-    const uint32_t obase = blockIdx.y * kBN;
-    const int8_t *A = XP + ((uint64_t)t * chunk + rbase) * Kp;  // [128][Kp]
-    const int8_t *B = WP + ((uint64_t)t * Np + obase) * Kp;     // [256][Kp]
+    const uint64_t rbase = (uint64_t)blockIdx.y * kBN;
+    const uint32_t obase = blockIdx.x * kBM;
+    const int8_t *A = WP + ((uint64_t)t * Np + obase) * Kp;     // [128][Kp]
+    const int8_t *B = XP + ((uint64_t)t * chunk + rbase) * Kp;  // [256][Kp]
     uint8_t *sA = smem, *sB = smem + kStages * kStageA;
+    constexpr uint32_t kProducers = 128;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base)),
@@ -170,9 +196,13 @@ __global__ void __launch_bounds__(kThreads, 2) mma_kernel(const int8_t *__restri
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
     }
     if (tid == 0) {
-        for (int s = 0; s < kStages; s++)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[s])));
+        for (int s = 0; s < kStages; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full[s])), "r"(kProducers));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&done)));
         asm volatile("fence.mbarrier_init.release.cluster;\n");
+        failed = 0;
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n");
     __syncthreads();
@@ -182,71 +212,75 @@ __global__ void __launch_bounds__(kThreads, 2) mma_kernel(const int8_t *__restri
     // instruction descriptor: s32 accumulate, A and B signed int8, both K-major, N = 256, M = 128
     const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((kBN >> 3) << 17) | ((kBM >> 4) << 24);
 
-    auto load_stage = [&](uint32_t kb) {
-        const uint32_t s = kb % kStages;
-        const uint32_t a_dst = smem_u32(sA + s * kStageA), b_dst = smem_u32(sB + s * kStageB);
-        const uint64_t koff = (uint64_t)kb * kKB;
-        // A: 128 rows x 4 chunks of 16 B = 512 copies; B: 256 x 4 = 1024
-        for (uint32_t c = tid; c < kBM * (kKB / 16); c += kThreads) {
-            uint32_t row = c / (kKB / 16), kc = c % (kKB / 16);
-            cp_async16(a_dst + core_off(row, kc), A + (uint64_t)row * Kp + koff + kc * 16);
-        }
-        for (uint32_t c = tid; c < kBN * (kKB / 16); c += kThreads) {
-            uint32_t row = c / (kKB / 16), kc = c % (kKB / 16);
-            cp_async16(b_dst + core_off(row, kc), B + (uint64_t)row * Kp + koff + kc * 16);
-        }
-        asm volatile("cp.async.commit_group;\n");
-    };
-
-    bool ok = true;
-    for (uint32_t kb = 0; kb < kStages - 1 && kb < nkb; kb++) load_stage(kb);
-    for (uint32_t kb = 0; kb < nkb; kb++) {
-        // stage kb has landed once at most kStages - 2 newer groups are pending
-        if (kb + kStages - 1 <= nkb) asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2));
-        else asm volatile("cp.async.wait_group 0;\n");
-        asm volatile("fence.proxy.async.shared::cta;\n");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;\n");
+    if (tid < kProducers) {
+        bool ok = true;
+        for (uint32_t kb = 0; kb < nkb; kb++) {
             const uint32_t s = kb % kStages;
-            const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sB + s * kStageB);
+            if (kb >= (uint32_t)kStages && !mbar_wait(smem_u32(&empty[s]), ((kb / kStages) - 1) & 1)) ok = false;
+            const uint32_t a_dst = smem_u32(sA + s * kStageA), b_dst = smem_u32(sB + s * kStageB);
+            const uint64_t koff = (uint64_t)kb * kKB;
+            if (ok) {
+                for (uint32_t c = tid; c < kBM * (kKB / 16); c += kProducers) {
+                    const uint32_t row = c / (kKB / 16), kc = c % (kKB / 16);
+                    cp_async16(a_dst + core_off(row, kc), A + (uint64_t)row * Kp + koff + kc * 16);
+                }
+                for (uint32_t c = tid; c < kBN * (kKB / 16); c += kProducers) {
+                    const uint32_t row = c / (kKB / 16), kc = c % (kKB / 16);
+                    cp_async16(b_dst + core_off(row, kc), B + (uint64_t)row * Kp + koff + kc * 16);
+                }
+            }
+            asm volatile("cp.async.commit_group;\n");
+            if (kb >= 1) {  // this thread's copies of stage kb - 1 have landed
+                asm volatile("cp.async.wait_group 1;\n");
+                asm volatile("fence.proxy.async.shared::cta;\n");
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&full[(kb - 1) % kStages])));
+            }
+        }
+        asm volatile("cp.async.wait_group 0;\n");
+        asm volatile("fence.proxy.async.shared::cta;\n");
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&full[(nkb - 1) % kStages])));
+        if (!ok) failed = 1;
+    } else if (tid == kProducers) {
+        bool ok = true;
+        for (uint32_t kb = 0; kb < nkb; kb++) {
+            const uint32_t s = kb % kStages;
+            if (!mbar_wait(smem_u32(&full[s]), (kb / kStages) & 1)) ok = false;
+            asm volatile("tcgen05.fence::after_thread_sync;\n");
+            if (ok) {
+                const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sB + s * kStageB);
 #pragma unroll
-            for (uint32_t k = 0; k < kKB / 32; k++) {
-                uint64_t ad = smem_desc(a0 + k * 256), bd = smem_desc(b0 + k * 256);
-                uint32_t acc = (kb | k) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+                for (uint32_t k = 0; k < kKB / 32; k++) {
+                    uint64_t ad = smem_desc(a0 + k * 256), bd = smem_desc(b0 + k * 256);
+                    uint32_t acc = (kb | k) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                        "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+                }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                smem_u32(&bars[s])));
+                smem_u32(&empty[s])));
         }
-        // refill the stage used by the previous block once its MMAs have read it
-        const uint32_t nxt = kb + kStages - 1;
-        if (nxt < nkb) {
-            if (kb >= 1) {
-                const uint32_t ps = (kb - 1) % kStages;
-                if (!mbar_wait(smem_u32(&bars[ps]), ((kb - 1) / kStages) & 1)) ok = false;
-            }
-            load_stage(nxt);
-        }
+        // completes once every MMA above has
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+            smem_u32(&done)));
+        if (!ok) failed = 1;
     }
-    // the last commit completes after every earlier MMA
-    {
-        const uint32_t ls = (nkb - 1) % kStages;
-        if (!mbar_wait(smem_u32(&bars[ls]), ((nkb - 1) / kStages) & 1)) ok = false;
-    }
+    // the idle warps wait here instead of spinning beside the producers and the MMA thread
+    __syncthreads();  // also publishes `failed` from the producer and MMA roles
+    const bool landed = mbar_wait(smem_u32(&done), 0);
     asm volatile("tcgen05.fence::after_thread_sync;\n");
-    if (!ok) {
-        if (lane == 0) atomicExch(err, 1);
+    if (!landed || failed) {
+        if (tid == 0) atomicExch(err, 1);
     } else {
-        // epilogue: warp w reads TMEM lanes 32w..32w+31 (X columns), 32 output columns at a time
-        const uint64_t r = rbase + warp * 32 + lane;
-        for (uint32_t c0 = 0; c0 < kBN; c0 += 32) {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (outputs); warpgroup w / 4 takes one
+        // half of the 256 X columns, 32 at a time
+        const uint32_t quarter = warp & 3, half = warp >> 2;
+        const uint32_t o = obase + quarter * 32 + lane;
+        for (uint32_t c0 = half * (kBN / 2); c0 < (half + 1) * (kBN / 2); c0 += 32) {
             uint32_t v[32];
-            const uint32_t taddr = tmem + ((warp * 32) << 16) + c0;
+            const uint32_t taddr = tmem + ((quarter * 32) << 16) + c0;
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -258,10 +292,19 @@ __global__ void __launch_bounds__(kThreads, 2) mma_kernel(const int8_t *__restri
                   "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n");
+            if (o < n_out) {
+                uint32_t pk[8];
 #pragma unroll
-            for (int j = 0; j < 32; j++) {
-                const uint32_t o = obase + c0 + j;
-                if (o < n_out) RES[((uint64_t)t * n_out + o) * chunk + r] = (uint8_t)mod_acc((int)v[j], t);
+                for (int j = 0; j < 8; j++) {
+                    uint32_t w = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; b++)
+                        w |= (acc24 ? mod_acc24((int)v[4 * j + b], t) : mod_acc((int)v[4 * j + b], t)) << (8 * b);
+                    pk[j] = w;
+                }
+                uint4 *dst = reinterpret_cast<uint4 *>(RES + ((uint64_t)t * n_out + o) * chunk + rbase + c0);
+                dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
             }
         }
     }
@@ -297,8 +340,9 @@ __global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict
 #pragma unroll
     for (int e = 0; e < 4; e++) {
         // sum_t r_t c_t as two 64-bit partial sums over the 32-bit halves of c_t (r_t < 2^8)
-        uint64_t lo = 0, hi = 0;
-        float v = 0.f;
+        // v = round(sum_t r_t frac_t) in 32-bit fixed point: each frac_t is within 2^-33 of the
+        // exact fraction, so v is off by < 20 * 255 * 2^-33 while the CRT margin is 1/8
+        uint64_t lo = 0, hi = 0, vx = 0;
 #pragma unroll
         for (uint32_t t = 0; t < kMaxMods; t++) {
             if (t < T) {
@@ -306,11 +350,11 @@ __global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict
                 const uint64_t c = cl.c[t];
                 lo += (uint64_t)rt * (uint32_t)c;
                 hi += (uint64_t)rt * (uint32_t)(c >> 32);
-                v += (float)rt * c_mods.frac[t];
+                vx += (uint64_t)rt * c_mods.fracx[t];
             }
         }
         u128 pos = {lo + (hi << 32), (hi >> 32) + ((lo + (hi << 32)) < lo ? 1ull : 0ull)};
-        const uint64_t vi = (uint64_t)(int64_t)rintf(v);
+        const uint64_t vi = (vx + (1ull << 31)) >> 32;
         y[e] = sub_mod(barrett(pos, p), barrett(mul_wide(vi, cl.M), p), p.q);
     }
     ulonglong2 *out = reinterpret_cast<ulonglong2 *>(Y + (uint64_t)o * R + rg);
@@ -352,7 +396,7 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
         for (uint32_t u = 0; u < T; u++)
             if (u != t) Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (p.mods.m[u] % m) % m);
         uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);  // m prime
-        p.mods.frac[t] = (float)inv / (float)m;
+        p.mods.fracx[t] = (uint32_t)std::llround((double)inv / (double)m * 4294967296.0);
         p.mods.c24[t] = (1u << 20) % m;
         p.mods.c48[t] = (uint32_t)((uint64_t)p.mods.c24[t] * p.mods.c24[t] % m);
         p.mods.magic[t] = (uint32_t)(((1ull << 32) + m - 1) / m);
@@ -387,7 +431,7 @@ constexpr uint64_t kChunkCols = 131072;
 size_t ctpt_tc_ws_bytes(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L) {
     const uint64_t R = 2ull * L * c.n;
     const uint64_t chunk = std::min<uint64_t>(R, kChunkCols);
-    const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBN - 1) / kBN * kBN;
+    const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBM - 1) / kBM * kBM;
     return (size_t)kMaxMods * (chunk * Kp + (uint64_t)Np * Kp + (uint64_t)n_out * chunk) + 4096 +
            sizeof(CrtLimb) * 64;
 }
@@ -396,10 +440,10 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
                     uint32_t L, void *ws, uint64_t max_abs_w, cudaStream_t st) {
     if (n_in == 0 || n_out == 0) return;
     const uint64_t R = 2ull * L * c.n;
-    if (R % kBM) throw std::invalid_argument("ct-pt matmul: 2 L N must be a multiple of 128");
+    if (R % kBN) throw std::invalid_argument("ct-pt matmul: 2 L N must be a multiple of 256");
     const uint64_t chunk = std::min<uint64_t>(R, kChunkCols);
     if (R % chunk) throw std::invalid_argument("ct-pt matmul: column count not a multiple of the chunk");
-    const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBN - 1) / kBN * kBN;
+    const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBM - 1) / kBM * kBM;
     Plan plan = make_plan(c, n_in, L, max_abs_w);
     const uint32_t T = plan.mods.t;
     SHM_CUDA(cudaMemcpyToSymbolAsync(c_mods, &plan.mods, sizeof(ModTab), 0, cudaMemcpyHostToDevice, st));
@@ -418,13 +462,14 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     wres_kernel<<<dim3((Kp + 255) / 256, Np), 256, 0, st>>>(W, WP, n_in, n_out, Kp, Np);
     SHM_CUDA(cudaGetLastError());
     SHM_CUDA(cudaFuncSetAttribute(mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    const int acc24 = (uint64_t)Kp * 125 * 125 < (1ull << 24) ? 1 : 0;  // accumulators exact in float
     for (uint64_t r0 = 0; r0 < R; r0 += chunk) {
         SHM_LAUNCHED(1);
         xres_kernel<<<dim3((uint32_t)(chunk / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0);
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
-        mma_kernel<<<dim3((uint32_t)(chunk / kBM), Np / kBN, T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
-                                                                                       chunk, err);
+        mma_kernel<<<dim3(Np / kBM, (uint32_t)(chunk / kBN), T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
+                                                                                       chunk, err, acc24);
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
         crt_kernel<<<dim3((uint32_t)((chunk / 4 + 255) / 256), n_out), 256, 0, st>>>(RES, Y, tab, n_out, chunk, r0, R,
