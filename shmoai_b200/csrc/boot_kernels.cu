@@ -44,9 +44,11 @@ __global__ void add_scalar_kernel(const uint64_t *__restrict__ a, uint64_t *__re
 }
 
 // out[c] = sum_t X_t[c] * P_t   over k terms (X_t: [n_polys][L][N], P_t: [L][N])
+// Limb-major block order: blockIdx.y = limb * n_polys + poly, so the polynomials that share a
+// plaintext limb run together and the k plaintext limbs stay in L2 for all of them.
 __global__ void mul_plain_acc_kernel(PtrTab X, PtrTab P, uint32_t k, uint64_t *__restrict__ out, uint32_t L,
                                      uint32_t log_n, const PrimeConst *__restrict__ pc, int accumulate) {
-    const uint32_t row = blockIdx.y, limb = row % L;
+    const uint32_t n_polys = gridDim.y / L, limb = blockIdx.y / n_polys, row = (blockIdx.y % n_polys) * L + limb;
     const PrimeConst p = pc[limb];
     const size_t off = ((size_t)row << log_n) + blockIdx.x * kT + threadIdx.x;
     const size_t poff = ((size_t)limb << log_n) + blockIdx.x * kT + threadIdx.x;
