@@ -124,12 +124,17 @@ class Encoder {
     // rounded (half to even) integer coefficients; |c| < 2^62 or Error
     std::vector<int64_t> encode_coeffs(const cplx *z, size_t len, double scale) const;
     Plaintext encode(const std::vector<cplx> &z, uint32_t L, double scale) const;
+    // the same plaintext over the extended basis QlP: L + n_p limbs (the Q limbs, then the
+    // special primes); its first L limbs are encode(z, L, scale).  L stays the Q limb count.
+    Plaintext encode_ext(const std::vector<cplx> &z, uint32_t L, double scale) const;
     // a constant: the single coefficient round(value * scale)
     // (moai::Encoder::encode(double), ckks_evaluator_parallel.cuh:73-92)
     Plaintext encode(double value, uint32_t L, double scale) const;
     std::vector<cplx> decode(const std::vector<double> &coeffs, double scale) const;
     // signed integer coefficients [n_polys][N] (host) -> NTT-form residues [n_polys][L][N] at `out`
     void upload(const int64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const;
+    // ... to [n_polys][L + n_p][N] over the extended basis QlP
+    void upload_ext(const int64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const;
 
    private:
     void fft(std::vector<cplx> &a, bool inverse) const;

@@ -171,6 +171,42 @@ size_t shm_fmt_switch_backward_workspace_bytes(const shm_context *ctx, uint32_t 
 int shm_fmt_switch_backward(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members,
                             const uint64_t *const *keys, uint64_t *out, uint32_t L, void *workspace,
                             size_t workspace_bytes, void *stream);
+
+/* ---- the extended basis QlP (double-hoisted linear transforms) ----
+ * An extended polynomial at level L has L + n_p limbs: the Q limbs 0..L-1 under q_0..q_{L-1},
+ * then the special primes p_0..p_{n_p-1}.  It stands for ModDown of itself, so the key
+ * switches of a baby-step giant-step transform can stay in QlP and be brought down once
+ * per transform (Bossuat et al.'s double hoisting); the reference ModDowns after every
+ * rotation (ShRotate.cu:201-257, Bootstrapper.cu:2168-2340).
+ * shm_extend: out = P * in (n_polys polynomials of L limbs -> L + n_p limbs, P limbs 0).
+ * shm_add_ext: out = a + b over extended polynomials.
+ * shm_moddown_ext: out [n_polys][L][N] = ModDown(ext); the P limbs of ext are overwritten.
+ * shm_multiply_plain_accumulate_ext: as shm_multiply_plain_accumulate over extended X[t]
+ *   and plaintexts P[t] of L + n_p limbs.
+ * shm_lift_signed_ext / shm_ntt_forward_ext: signed coefficients -> extended residues / NTT
+ *   of extended polynomials (plaintexts for the above).
+ * shm_shared_rotate_ext: Sh-Rot of shared-a groups with extended outputs outs[e]
+ *   [n_groups][n_members+1][L+n_p][N] (no ModDown); the input is ordinary groups
+ *   [n_groups][n_members+1][L][N] (in_ext = 0) or extended groups (in_ext = 1, whose a rows
+ *   are brought down once before the ModUp). */
+int shm_extend(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+               void *stream);
+int shm_add_ext(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+                uint32_t L, void *stream);
+size_t shm_moddown_ext_workspace_bytes(const shm_context *ctx, uint32_t n_polys, uint32_t L);
+int shm_moddown_ext(const shm_context *ctx, uint64_t *ext, uint64_t *out, uint32_t n_polys, uint32_t L,
+                    void *workspace, size_t workspace_bytes, void *stream);
+int shm_multiply_plain_accumulate_ext(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
+                                      uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
+                                      void *stream);
+int shm_lift_signed_ext(const shm_context *ctx, const int64_t *coeffs, uint64_t *out, uint32_t n_polys, uint32_t L,
+                        void *stream);
+int shm_ntt_forward_ext(const shm_context *ctx, uint64_t *data, uint32_t n_polys, uint32_t L, void *stream);
+size_t shm_shared_rotate_ext_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                             uint32_t L);
+int shm_shared_rotate_ext(const shm_context *ctx, const uint64_t *in, int in_ext, uint32_t n_groups,
+                          uint32_t n_members, uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys,
+                          uint64_t *const *outs, uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
 /* Galois element of a rotation by `step` slots (0 = conjugation).
  * Replaces PhantomGaloisTool::get_elt_from_step (src/galois.cu:47-91). */
 uint32_t shm_galois_elt_from_step(const shm_context *ctx, int step);

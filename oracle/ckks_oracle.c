@@ -559,6 +559,74 @@ void orc_shared_rotate_hoisted(const orc_ctx *c, const uint64_t *sh, uint32_t n_
     free(up);
 }
 
+/* ---------------- the extended basis QlP (double hoisting) ----------------
+ * An extended polynomial at level L has L + np limbs (Q limbs, then the special primes) and
+ * stands for its ModDown (Bossuat et al., double hoisting of BSGS key switches). */
+
+static uint64_t p_mod_q(const orc_ctx *c, uint64_t q) {
+    uint64_t P = 1;
+    for (uint32_t k = 0; k < c->np; k++) P = mulmod(P, c->primes[c->nq + k] % q, q);
+    return P;
+}
+
+/* out = P * in on the Q limbs, 0 on the special-prime limbs */
+void orc_extend(const orc_ctx *c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L) {
+    size_t n = c->n;
+    uint32_t LP = L + c->np;
+    for (uint32_t p = 0; p < n_polys; p++)
+        for (uint32_t j = 0; j < LP; j++) {
+            uint64_t *o = out + ((size_t)p * LP + j) * n;
+            if (j >= L) {
+                memset(o, 0, sizeof(uint64_t) * n);
+                continue;
+            }
+            uint64_t q = c->primes[j], P = p_mod_q(c, q);
+            const uint64_t *x = in + ((size_t)p * L + j) * n;
+            for (size_t k = 0; k < n; k++) o[k] = mulmod(x[k], P, q);
+        }
+}
+
+void orc_moddown_ext(const orc_ctx *c, const uint64_t *ext, uint64_t *out, uint32_t n_polys, uint32_t L) {
+    size_t n = c->n;
+    uint32_t LP = L + c->np;
+    for (uint32_t p = 0; p < n_polys; p++) moddown_one(c, ext + (size_t)p * LP * n, L, out + (size_t)p * L * n);
+}
+
+/* Sh-Rot with extended outputs: the input group is [n+1][L][N] (in_ext = 0) or extended
+ * [n+1][L+np][N] (in_ext = 1: its a row is brought down first); per element e,
+ * outs[e][h] = <up, key_h> over QlP, plus for the b rows sigma(b) scaled by P (ordinary input)
+ * or sigma(b_ext) (extended input). */
+void orc_shared_rotate_ext(const orc_ctx *c, const uint64_t *in, int in_ext, uint32_t n_mem, uint32_t L,
+                           uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs) {
+    size_t n = c->n;
+    uint32_t alpha = c->np, beta = (L + alpha - 1) / alpha, LP = L + c->np, H = n_mem + 1;
+    size_t rowl = (size_t)(in_ext ? LP : L) * n;
+    uint64_t *up = (uint64_t *)malloc(sizeof(uint64_t) * beta * LP * n);
+    if (in_ext) {
+        uint64_t *aq = (uint64_t *)malloc(sizeof(uint64_t) * L * n);
+        moddown_one(c, in + (size_t)n_mem * rowl, L, aq);
+        orc_modup(c, aq, L, up);
+        free(aq);
+    } else {
+        orc_modup(c, in + (size_t)n_mem * rowl, L, up);
+    }
+    uint32_t *perm = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    for (uint32_t e = 0; e < n_elts; e++) {
+        orc_galois_perm(c->log_n, elts[e], perm);
+        ip_multi(c, up, beta, L, keys[e], H, perm, outs[e]);
+        for (uint32_t h = 0; h < n_mem; h++)
+            for (uint32_t j = 0; j < LP; j++) {
+                if (!in_ext && j >= L) continue;
+                uint64_t q = c->primes[ext_prime(c, L, j)], P = in_ext ? 1 : p_mod_q(c, q);
+                const uint64_t *b = in + (size_t)h * rowl + (size_t)j * n;
+                uint64_t *o = outs[e] + ((size_t)h * LP + j) * n;
+                for (size_t k = 0; k < n; k++) o[k] = addmod(o[k], mulmod(b[perm[k]], P, q), q);
+            }
+    }
+    free(perm);
+    free(up);
+}
+
 /* Exact extension of a (NTT form, L limbs) to QlP: the Ql rows keep a, the P rows get
  * (sum_i y_i qhat_i - v Q) mod p_k with y_i = [x_i qhat_i^-1]_{q_i} (x = INTT(a)) and
  * v = floor(sum_i y_i / q_i) in double arithmetic (FmtSwitch.cu:82-108). */

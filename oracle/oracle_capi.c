@@ -410,6 +410,130 @@ int shm_linear_combination(const shm_context *ctx, const uint64_t *const *X, con
     return SHM_OK;
 }
 
+/* ---- the extended basis QlP (same semantics as the CUDA library) */
+
+static int ks_level(const shm_context *ctx, uint32_t L);
+
+static int ext_ok(const shm_context *ctx, uint32_t L) { return ctx && ctx->c->np && L >= 1 && L <= ctx->c->nq; }
+
+int shm_extend(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+               void *stream) {
+    (void)stream;
+    if (!ext_ok(ctx, L)) return fail("level out of range");
+    orc_extend(ctx->c, in, out, n_polys, L);
+    return SHM_OK;
+}
+
+int shm_add_ext(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+                uint32_t L, void *stream) {
+    (void)stream;
+    if (!ext_ok(ctx, L)) return fail("level out of range");
+    const orc_ctx *c = ctx->c;
+    size_t n = c->n;
+    uint32_t LP = L + c->np;
+    for (size_t r = 0; r < (size_t)n_polys * LP; r++) {
+        uint64_t q = c->primes[ext_prime(c, L, (uint32_t)(r % LP))];
+        for (size_t k = 0; k < n; k++) out[r * n + k] = addmod(a[r * n + k], b[r * n + k], q);
+    }
+    return SHM_OK;
+}
+
+size_t shm_moddown_ext_workspace_bytes(const shm_context *ctx, uint32_t n_polys, uint32_t L) {
+    (void)ctx;
+    (void)n_polys;
+    (void)L;
+    return 0;
+}
+
+int shm_moddown_ext(const shm_context *ctx, uint64_t *ext, uint64_t *out, uint32_t n_polys, uint32_t L,
+                    void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ext_ok(ctx, L)) return fail("level out of range");
+    orc_moddown_ext(ctx->c, ext, out, n_polys, L);
+    return SHM_OK;
+}
+
+int shm_multiply_plain_accumulate_ext(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
+                                      uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
+                                      void *stream) {
+    (void)stream;
+    if (!ext_ok(ctx, L)) return fail("level out of range");
+    const orc_ctx *c = ctx->c;
+    size_t n = c->n;
+    uint32_t LP = L + c->np;
+#pragma omp parallel for
+    for (int r = 0; r < (int)(n_polys * LP); r++) {
+        uint32_t limb = (uint32_t)r % LP;
+        uint64_t q = c->primes[ext_prime(c, L, limb)];
+        for (size_t i = 0; i < n; i++) {
+            uint64_t acc = accumulate ? out[(size_t)r * n + i] : 0;
+            for (uint32_t t = 0; t < k; t++)
+                acc = addmod(acc, mulmod(X[t][(size_t)r * n + i], P[t][(size_t)limb * n + i], q), q);
+            out[(size_t)r * n + i] = acc;
+        }
+    }
+    return SHM_OK;
+}
+
+int shm_lift_signed_ext(const shm_context *ctx, const int64_t *coeffs, uint64_t *out, uint32_t n_polys, uint32_t L,
+                        void *stream) {
+    (void)stream;
+    if (!ext_ok(ctx, L)) return fail("level out of range");
+    const orc_ctx *c = ctx->c;
+    size_t n = c->n;
+    uint32_t LP = L + c->np;
+    for (uint32_t p = 0; p < n_polys; p++)
+        for (uint32_t i = 0; i < LP; i++)
+            for (size_t k = 0; k < n; k++)
+                out[((size_t)p * LP + i) * n + k] = signed_residue(coeffs[(size_t)p * n + k], c->primes[ext_prime(c, L, i)]);
+    return SHM_OK;
+}
+
+int shm_ntt_forward_ext(const shm_context *ctx, uint64_t *data, uint32_t n_polys, uint32_t L, void *stream) {
+    (void)stream;
+    if (!ext_ok(ctx, L)) return fail("level out of range");
+    const orc_ctx *c = ctx->c;
+    size_t n = c->n;
+    uint32_t LP = L + c->np;
+#pragma omp parallel for collapse(2)
+    for (int p = 0; p < (int)n_polys; p++)
+        for (int j = 0; j < (int)LP; j++) {
+            uint32_t pj = ext_prime(c, L, (uint32_t)j);
+            orc_ntt_fwd(data + ((size_t)p * LP + j) * n, c->log_n, c->primes[pj], c->rp + (size_t)pj * n);
+        }
+    return SHM_OK;
+}
+
+size_t shm_shared_rotate_ext_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                             uint32_t L) {
+    (void)ctx;
+    (void)n_groups;
+    (void)n_members;
+    (void)L;
+    return 0;
+}
+
+int shm_shared_rotate_ext(const shm_context *ctx, const uint64_t *in, int in_ext, uint32_t n_groups,
+                          uint32_t n_members, uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys,
+                          uint64_t *const *outs, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ks_level(ctx, L)) return fail("level out of range for key switching");
+    if (!n_members) return fail("groups need at least one member");
+    const orc_ctx *c = ctx->c;
+    size_t n = c->n, H = n_members + 1, gin = H * (in_ext ? L + c->np : L) * n, gout = H * (L + c->np) * n;
+    uint64_t **o = (uint64_t **)malloc(sizeof(uint64_t *) * (n_elts ? n_elts : 1));
+    for (uint32_t g = 0; g < n_groups; g++) {
+        for (uint32_t e = 0; e < n_elts; e++) o[e] = outs[e] + g * gout;
+        orc_shared_rotate_ext(c, in + g * gin, in_ext, n_members, L, n_elts, elts, keys, (uint64_t *const *)o);
+    }
+    free(o);
+    return SHM_OK;
+}
+
 int shm_multiply_plain_accumulate(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
                                   uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
                                   void *stream) {

@@ -46,10 +46,12 @@ __global__ void add_scalar_kernel(const uint64_t *__restrict__ a, uint64_t *__re
 // out[c] = sum_t X_t[c] * P_t   over k terms (X_t: [n_polys][L][N], P_t: [L][N])
 // Limb-major block order: blockIdx.y = limb * n_polys + poly, so the polynomials that share a
 // plaintext limb run together and the k plaintext limbs stay in L2 for all of them.
+// L = limbs per row; limb l uses prime l when l < Lq, else the special prime nq + l - Lq
 __global__ void mul_plain_acc_kernel(PtrTab X, PtrTab P, uint32_t k, uint64_t *__restrict__ out, uint32_t L,
-                                     uint32_t log_n, const PrimeConst *__restrict__ pc, int accumulate) {
+                                     uint32_t log_n, const PrimeConst *__restrict__ pc, int accumulate, uint32_t Lq,
+                                     uint32_t nq) {
     const uint32_t n_polys = gridDim.y / L, limb = blockIdx.y / n_polys, row = (blockIdx.y % n_polys) * L + limb;
-    const PrimeConst p = pc[limb];
+    const PrimeConst p = pc[limb < Lq ? limb : nq + (limb - Lq)];
     const size_t off = ((size_t)row << log_n) + blockIdx.x * kT + threadIdx.x;
     const size_t poff = ((size_t)limb << log_n) + blockIdx.x * kT + threadIdx.x;
     u128 acc = {0, 0};
@@ -117,11 +119,12 @@ void add_scalar(const Context &c, const uint64_t *a, uint64_t *out, const Scalar
 }
 
 void mul_plain_acc(const Context &c, const PtrTab &X, const PtrTab &P, uint32_t k, uint64_t *out, uint32_t n_polys,
-                   uint32_t L, bool accumulate, cudaStream_t st) {
+                   uint32_t L, bool accumulate, cudaStream_t st, bool ext) {
     if (!n_polys || !k) return;
+    const uint32_t rows = ext ? L + c.np : L;
     SHM_LAUNCHED(1);
-    mul_plain_acc_kernel<<<dim3(c.n / kT, n_polys * L), kT, 0, st>>>(X, P, k, out, L, c.log_n, c.pc,
-                                                                      accumulate ? 1 : 0);
+    mul_plain_acc_kernel<<<dim3(c.n / kT, n_polys * rows), kT, 0, st>>>(X, P, k, out, rows, c.log_n, c.pc,
+                                                                         accumulate ? 1 : 0, L, c.nq);
     SHM_CUDA(cudaGetLastError());
 }
 

@@ -35,7 +35,7 @@ void push4(std::vector<uint64_t> &v, uint64_t c, uint64_t psi_half_inv, uint64_t
 Context::~Context() {
     cudaSetDevice(device);
     for (void *p : {(void *)pc, (void *)tw, (void *)inv_scale_plain, (void *)moddown_scale, (void *)moddown_conv,
-                    (void *)p_inv, (void *)rescale_inv, arena})
+                    (void *)p_inv, (void *)p_mod, (void *)rescale_inv, arena})
         if (p) cudaFree(p);
     for (auto &l : ks) {
         if (l.modup_scale) cudaFree(l.modup_scale);
@@ -164,9 +164,17 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
             pinv[2 * j] = v;
             pinv[2 * j + 1] = host::shoup_of(v, q);
         }
+        std::vector<uint64_t> pmod((size_t)nq * 2);
+        for (uint32_t j = 0; j < nq; j++) {
+            uint64_t q = primes[j], prod = 1;
+            for (uint32_t k = 0; k < np; k++) prod = host::mulmod(prod, P[k] % q, q);
+            pmod[2 * j] = prod;
+            pmod[2 * j + 1] = host::shoup_of(prod, q);
+        }
         c->moddown_scale = upload(mds);
         c->moddown_conv = upload(mdc);
         c->p_inv = upload(pinv);
+        c->p_mod = upload(pmod);
         // ModUp constants per level
         for (uint32_t L = 1; L <= nq; L++) {
             LevelKS &ks = c->ks[L];
@@ -527,6 +535,115 @@ int shm_fmt_switch_backward(const shm_context *ctx, const uint64_t *sh, uint32_t
         set_device(c);
         uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::fmt_backward_ws_words(c, n_groups, n_members, L));
         shm::fmt_backward(c, sh, n_groups, n_members, L, keys, out, ws, S(stream));
+    });
+}
+
+// ---- extended basis
+
+static void check_ext(const shm::Context &c, uint32_t L) {
+    if (c.np == 0) throw std::invalid_argument("context has no special primes");
+    if (L < 1 || L > c.nq) throw std::invalid_argument("level out of range");
+}
+
+int shm_extend(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+               void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_ext(c, L);
+        set_device(c);
+        shm::extend(c, in, out, n_polys, L, S(stream));
+    });
+}
+
+int shm_add_ext(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys,
+                uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_ext(c, L);
+        set_device(c);
+        shm::add_ext(c, a, b, out, n_polys, L, S(stream));
+    });
+}
+
+size_t shm_moddown_ext_workspace_bytes(const shm_context *ctx, uint32_t n_polys, uint32_t L) {
+    return ctx && ctx->c ? shm::moddown_ext_ws_words(*ctx->c, n_polys, L) * 8 : 0;
+}
+
+int shm_moddown_ext(const shm_context *ctx, uint64_t *ext, uint64_t *out, uint32_t n_polys, uint32_t L,
+                    void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_ext(c, L);
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::moddown_ext_ws_words(c, n_polys, L));
+        shm::moddown_ext(c, ext, out, n_polys, L, ws, S(stream));
+    });
+}
+
+int shm_multiply_plain_accumulate_ext(const shm_context *ctx, const uint64_t *const *X, const uint64_t *const *P,
+                                      uint32_t k, uint64_t *out, uint32_t n_polys, uint32_t L, int accumulate,
+                                      void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_ext(c, L);
+        if (!X || !P) throw std::invalid_argument("null term arrays");
+        set_device(c);
+        // sum of `chunk` products must stay below the Barrett bound 2^(63 + bits(q)) of every limb
+        uint32_t chunk = shm::kMaxAccTerms;
+        for (uint32_t i = 0; i < L + c.np; i++) {
+            const uint64_t q = c.primes[i < L ? i : c.nq + (i - L)];
+            int b = shm::host::bit_length(q);
+            uint32_t lim = 2 * b >= 63 + b ? 1u : (63 + b - 2 * b >= 5 ? 32u : (1u << (63 + b - 2 * b)));
+            chunk = std::min(chunk, lim);
+        }
+        for (uint32_t t0 = 0; t0 < k; t0 += chunk) {
+            uint32_t kk = std::min(chunk, k - t0);
+            shm::PtrTab x{}, p{};
+            for (uint32_t t = 0; t < kk; t++) {
+                x.p[t] = X[t0 + t];
+                p.p[t] = P[t0 + t];
+            }
+            shm::mul_plain_acc(c, x, p, kk, out, n_polys, L, accumulate || t0 > 0, S(stream), true);
+        }
+    });
+}
+
+int shm_lift_signed_ext(const shm_context *ctx, const int64_t *coeffs, uint64_t *out, uint32_t n_polys, uint32_t L,
+                        void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_ext(c, L);
+        set_device(c);
+        shm::lift_signed_ext(c, coeffs, out, n_polys, L, S(stream));
+    });
+}
+
+int shm_ntt_forward_ext(const shm_context *ctx, uint64_t *data, uint32_t n_polys, uint32_t L, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_ext(c, L);
+        set_device(c);
+        const uint32_t LP = L + c.np;
+        shm::ntt_forward(c, data, n_polys * LP, LP, shm::ext_map(L, c), S(stream));
+    });
+}
+
+size_t shm_shared_rotate_ext_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                             uint32_t L) {
+    return ctx && ctx->c ? shm::shared_rotate_ext_ws_words(*ctx->c, n_groups, n_members, L) * 8 : 0;
+}
+
+int shm_shared_rotate_ext(const shm_context *ctx, const uint64_t *in, int in_ext, uint32_t n_groups,
+                          uint32_t n_members, uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys,
+                          uint64_t *const *outs, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_ext(c, L);
+        if (n_elts && (!elts || !keys || !outs)) throw std::invalid_argument("null element arrays");
+        if (n_members == 0) throw std::invalid_argument("groups need at least one member");
+        set_device(c);
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::shared_rotate_ext_ws_words(c, n_groups, n_members, L));
+        shm::shared_rotate_ext(c, in, in_ext != 0, n_groups, n_members, L, n_elts, elts, keys, outs, ws, S(stream));
     });
 }
 

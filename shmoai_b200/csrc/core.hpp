@@ -53,6 +53,7 @@ struct Context {
     uint64_t *moddown_scale = nullptr;  // [np][4]: N^-1 * phat_k^-1
     uint64_t *moddown_conv = nullptr;   // [nq][np]: phat_k mod q_j
     uint64_t *p_inv = nullptr;          // [nq][2]: P^-1 mod q_j and Shoup companion
+    uint64_t *p_mod = nullptr;          // [nq][2]: P mod q_j and Shoup companion (extended basis)
     uint64_t *rescale_inv = nullptr;    // [nq][nq][2]: q_{L-1}^-1 mod q_j (row L-1), Shoup
     std::vector<LevelKS> ks;            // index L (1..nq)
     std::map<uint32_t, uint32_t *> galois_perm;  // elt -> [N] permutation
@@ -137,8 +138,9 @@ void mul_scalar(const Context &c, const uint64_t *a, uint64_t *out, const Scalar
                 cudaStream_t st);
 void add_scalar(const Context &c, const uint64_t *a, uint64_t *out, const ScalarTab &s, uint32_t n_cts, uint32_t L,
                 cudaStream_t st);
+// rows of L limbs (limb l -> prime l), or with ext the extended basis (rows of L + np limbs)
 void mul_plain_acc(const Context &c, const PtrTab &X, const PtrTab &P, uint32_t k, uint64_t *out, uint32_t n_polys,
-                   uint32_t L, bool accumulate, cudaStream_t st);
+                   uint32_t L, bool accumulate, cudaStream_t st, bool ext = false);
 // sum_t w_t X_t + w0 (c0 only) over size-2 ciphertexts; weights passed by value
 constexpr int kMaxLinTerms = 8;
 struct LinTerms {
@@ -185,6 +187,22 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
                     uint32_t L, void *ws, uint64_t max_abs_w, cudaStream_t st);
 int ctpt_tc_error(void *ws, cudaStream_t st);
 size_t ctpt_ws_words(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);
+// ---- the extended basis QlP: a polynomial at level L has L + np limbs, the Q limbs 0..L-1
+// (primes q_0 .. q_{L-1}) then the special primes p_0 .. p_{np-1} (shared.cu)
+LimbMap ext_map(uint32_t L, const Context &c);
+void extend(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, cudaStream_t st);
+void add_ext(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys, uint32_t L,
+             cudaStream_t st);
+size_t moddown_ext_ws_words(const Context &c, uint32_t n_polys, uint32_t L);
+void moddown_ext(const Context &c, uint64_t *ext, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *ws,
+                 cudaStream_t st);
+size_t shared_rotate_ext_ws_words(const Context &c, uint32_t n_groups, uint32_t n, uint32_t L);
+void shared_rotate_ext(const Context &c, const uint64_t *in, bool in_ext, uint32_t n_groups, uint32_t n, uint32_t L,
+                       uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs,
+                       uint64_t *ws, cudaStream_t st);
+void lift_signed_ext(const Context &c, const int64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                     cudaStream_t st);
+
 // acc [n_cts][H][LP][N] = inner products of up [n_cts][beta][LP][N] with key [beta][H][QP][N]
 void ip_multi(const Context &c, const uint64_t *up, const uint64_t *key, uint64_t *acc, uint32_t n_cts, uint32_t L,
               uint32_t beta, uint32_t H, const uint32_t *perm, cudaStream_t st);

@@ -50,15 +50,16 @@ __global__ void cbd_kernel(uint64_t *__restrict__ out, uint32_t L, uint32_t log_
     }
 }
 
+// rows of L limbs; limb i < Lq uses prime i, limb i >= Lq the special prime nq + i - Lq
 __global__ void lift_kernel(const int64_t *__restrict__ in, uint64_t *__restrict__ out, uint32_t L, uint32_t log_n,
-                            const PrimeConst *__restrict__ pc) {
+                            const PrimeConst *__restrict__ pc, uint32_t Lq, uint32_t nq) {
     const uint32_t p = blockIdx.y;
     const uint32_t k = blockIdx.x * kT + threadIdx.x;
     const int64_t v = in[((size_t)p << log_n) + k];
     const uint64_t mag = v < 0 ? (uint64_t)(-(v + 1)) + 1 : (uint64_t)v;  // |v| without overflow
     uint64_t *o = out + ((size_t)p * L << log_n) + k;
     for (uint32_t i = 0; i < L; i++) {
-        const uint64_t q = pc[i].q, r = mag % q;
+        const uint64_t q = pc[i < Lq ? i : nq + (i - Lq)].q, r = mag % q;
         o[(size_t)i << log_n] = (v < 0 && r) ? q - r : r;
     }
 }
@@ -82,7 +83,15 @@ void sample_cbd(const Context &c, uint64_t *out, uint32_t n_polys, uint32_t L, u
 void lift_signed(const Context &c, const int64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, cudaStream_t st) {
     if (!n_polys) return;
     SHM_LAUNCHED(1);
-    lift_kernel<<<dim3(c.n / kT, n_polys), kT, 0, st>>>(in, out, L, c.log_n, c.pc);
+    lift_kernel<<<dim3(c.n / kT, n_polys), kT, 0, st>>>(in, out, L, c.log_n, c.pc, L, c.nq);
+    SHM_CUDA(cudaGetLastError());
+}
+
+void lift_signed_ext(const Context &c, const int64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L,
+                     cudaStream_t st) {
+    if (!n_polys) return;
+    SHM_LAUNCHED(1);
+    lift_kernel<<<dim3(c.n / kT, n_polys), kT, 0, st>>>(in, out, L + c.np, c.log_n, c.pc, L, c.nq);
     SHM_CUDA(cudaGetLastError());
 }
 

@@ -298,4 +298,136 @@ void fmt_backward(const Context &c, const uint64_t *sh, uint32_t n_groups, uint3
     }
 }
 
+// ------------------------------------------------------------------ extended basis QlP
+
+namespace {
+
+// out[row][j] = P * in[row][j] mod q_j for j < L, 0 for the special-prime limbs.  Grid (N/kT, LP, rows)
+__global__ void extend_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ out, uint32_t L, uint32_t np,
+                              uint32_t log_n, const PrimeConst *__restrict__ pc, const uint64_t *__restrict__ pmod) {
+    const uint32_t j = blockIdx.y, row = blockIdx.z, LP = L + np;
+    const uint32_t k = blockIdx.x * kT + threadIdx.x;
+    uint64_t v = 0;
+    if (j < L) v = shoup(in[(((size_t)row * L + j) << log_n) + k], pmod[2 * j], pmod[2 * j + 1], pc[j].q);
+    out[(((size_t)row * LP + j) << log_n) + k] = v;
+}
+
+// rows of LP limbs, limb j under prime j (j < L) or the special prime nq + j - L.  Grid (N/kT, LP, rows)
+__global__ void add_ext_kernel(const uint64_t *__restrict__ a, const uint64_t *__restrict__ b, uint64_t *__restrict__ out,
+                               uint32_t L, uint32_t np, uint32_t nq, uint32_t log_n, const PrimeConst *__restrict__ pc) {
+    const uint32_t j = blockIdx.y, row = blockIdx.z, LP = L + np;
+    const size_t off = (((size_t)row * LP + j) << log_n) + blockIdx.x * kT + threadIdx.x;
+    out[off] = add_mod(a[off], b[off], pc[j < L ? j : nq + (j - L)].q);
+}
+
+// The extended Sh-Rot output of one target: out[g][h] = acc[g][h] (+ for the b rows h < n the
+// rotated b: over every limb sigma(b_ext) when the input is extended, else P sigma(b) on the
+// Q limbs).  Grid (N/kT, LP, groups * H)
+__global__ void combine_ext_kernel(const uint64_t *__restrict__ acc, uint64_t *__restrict__ out,
+                                   const uint64_t *__restrict__ bsrc, int b_ext, const uint32_t *__restrict__ perm,
+                                   uint32_t H, uint32_t L, uint32_t np, uint32_t nq, uint32_t log_n,
+                                   const PrimeConst *__restrict__ pc, const uint64_t *__restrict__ pmod) {
+    const uint32_t j = blockIdx.y, gh = blockIdx.z, h = gh % H, LP = L + np;
+    const uint32_t k = blockIdx.x * kT + threadIdx.x;
+    const size_t off = (((size_t)gh * LP + j) << log_n) + k;
+    uint64_t v = acc[off];
+    if (h + 1 < H) {
+        const uint32_t ks = perm ? __ldg(perm + k) : k;
+        const uint64_t q = pc[j < L ? j : nq + (j - L)].q;
+        if (b_ext)
+            v = add_mod(v, bsrc[(((size_t)gh * LP + j) << log_n) + ks], q);
+        else if (j < L)
+            v = add_mod(v, shoup(bsrc[(((size_t)gh * L + j) << log_n) + ks], pmod[2 * j], pmod[2 * j + 1], q), q);
+    }
+    out[off] = v;
+}
+
+// ModDown of n_polys extended polynomials (their special-prime limbs are overwritten by the
+// inverse NTT) into out [n_polys][L][N]; delta: [n_polys][L][N] scratch
+void moddown_rows(const Context &c, uint64_t *ext, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *delta,
+                  cudaStream_t st) {
+    const uint32_t LP = L + c.np;
+    LimbMap mp;
+    for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
+    ntt_inverse(c, ext, n_polys * LP, LP, mp, c.moddown_scale, st, L);
+    ModDownIO md;
+    md.acc = ext;
+    md.conv = c.moddown_conv;
+    md.pinv = c.p_inv;
+    md.out = out;
+    md.out_ct = (long long)L * c.n;
+    md.H = 1;
+    md.np = c.np;
+    md.s52 = c.s52 ? 1 : 0;
+    ntt_forward_moddown(c, md, delta, n_polys, L, st);
+}
+
+}  // namespace
+
+LimbMap ext_map(uint32_t L, const Context &c) {
+    LimbMap m;
+    for (uint32_t s = 0; s < 512; s++) m.prime[s] = s < L ? (uint8_t)s : (s < L + c.np ? (uint8_t)(c.nq + (s - L)) : 255);
+    return m;
+}
+
+void extend(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, cudaStream_t st) {
+    if (!n_polys) return;
+    SHM_LAUNCHED(1);
+    extend_kernel<<<dim3(c.n / kT, L + c.np, n_polys), kT, 0, st>>>(in, out, L, c.np, c.log_n, c.pc, c.p_mod);
+    SHM_CUDA(cudaGetLastError());
+}
+
+void add_ext(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_polys, uint32_t L,
+             cudaStream_t st) {
+    if (!n_polys) return;
+    SHM_LAUNCHED(1);
+    add_ext_kernel<<<dim3(c.n / kT, L + c.np, n_polys), kT, 0, st>>>(a, b, out, L, c.np, c.nq, c.log_n, c.pc);
+    SHM_CUDA(cudaGetLastError());
+}
+
+size_t moddown_ext_ws_words(const Context &c, uint32_t n_polys, uint32_t L) { return (size_t)n_polys * L * c.n; }
+
+void moddown_ext(const Context &c, uint64_t *ext, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *ws,
+                 cudaStream_t st) {
+    if (!n_polys) return;
+    if (c.np == 0) throw std::invalid_argument("context has no special primes");
+    moddown_rows(c, ext, out, n_polys, L, ws, st);
+}
+
+size_t shared_rotate_ext_ws_words(const Context &c, uint32_t n_groups, uint32_t n, uint32_t L) {
+    const uint32_t beta = (L + c.np - 1) / c.np, LP = L + c.np, H = n + 1;
+    // x, up, acc, the a rows (extended input), their ModDown and its delta
+    return (size_t)n_groups * c.n * (L + (size_t)beta * LP + (size_t)H * LP + LP + 2 * (size_t)L);
+}
+
+void shared_rotate_ext(const Context &c, const uint64_t *in, bool in_ext, uint32_t n_groups, uint32_t n, uint32_t L,
+                       uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs,
+                       uint64_t *ws, cudaStream_t st) {
+    const uint32_t beta = (L + c.np - 1) / c.np, LP = L + c.np, H = n + 1;
+    check_shape(c, L, beta, H);
+    if (beta > c.dnum) throw std::invalid_argument("level needs more key digits than the key holds");
+    const size_t N = c.n, ln = (size_t)L * N;
+    uint64_t *x = ws, *up = x + (size_t)n_groups * ln, *acc = up + (size_t)n_groups * beta * LP * N;
+    uint64_t *arow = acc + (size_t)n_groups * H * LP * N, *aq = arow + (size_t)n_groups * LP * N;
+    uint64_t *delta = aq + (size_t)n_groups * ln;
+    const size_t g_words = (size_t)H * (in_ext ? LP : L) * N;  // one input group
+    if (in_ext) {
+        // ModDown of the a row of every group, then ModUp of it
+        SHM_CUDA(cudaMemcpy2DAsync(arow, LP * N * 8, in + (size_t)n * LP * N, g_words * 8, LP * N * 8, n_groups,
+                                   cudaMemcpyDeviceToDevice, st));
+        moddown_rows(c, arow, aq, n_groups, L, delta, st);
+        modup_into(c, aq, ln, n_groups, L, x, up, st);
+    } else {
+        modup_into(c, in + (size_t)n * ln, g_words, n_groups, L, x, up, st);
+    }
+    for (uint32_t e = 0; e < n_elts; e++) {
+        const uint32_t *perm = const_cast<Context &>(c).perm(elts[e]);
+        ip_multi(c, up, keys[e], acc, n_groups, L, beta, H, perm, st);
+        SHM_LAUNCHED(1);
+        combine_ext_kernel<<<dim3(N / kT, LP, n_groups * H), kT, 0, st>>>(acc, outs[e], in, in_ext ? 1 : 0, perm, H, L,
+                                                                          c.np, c.nq, c.log_n, c.pc, c.p_mod);
+        SHM_CUDA(cudaGetLastError());
+    }
+}
+
 }  // namespace shm

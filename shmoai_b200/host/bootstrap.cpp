@@ -277,7 +277,10 @@ class LinearTransform {
         for (auto &kv : ts) {
             const int64_t u = floordiv(kv.first, g1_), v = kv.first - u * g1_;
             Vec P = roll(*kv.second, g1_ * u * b_);
-            groups_[u].emplace_back(v, ev.encoder().encode(P, level, pt_scale_));
+            // over QlP when the context has special primes: the first `level` limbs serve ordinary
+            // batches, all of them the double-hoisted shared-a path (apply_ext)
+            groups_[u].emplace_back(v, c.np ? ev.encoder().encode_ext(P, level, pt_scale_)
+                                            : ev.encoder().encode(P, level, pt_scale_));
         }
         std::set<int64_t> bs;
         for (auto &g : groups_)
@@ -301,6 +304,7 @@ class LinearTransform {
             dropped = ev.mod_switch_to(x, level_);
             xp = &dropped;
         }
+        if (xp->shared && ev.context().np) return apply_ext(ev, *xp, rescale);
         std::vector<int> bsteps;
         for (int64_t v : baby_)
             if (v) bsteps.push_back((int)(v * b_));
@@ -328,6 +332,87 @@ class LinearTransform {
     }
 
    private:
+    // Double hoisting (Bossuat et al.) for shared-a groups: the baby-step Sh-Rots stay in the
+    // extended basis QlP (no ModDown), the inner sums multiply QlP plaintexts, each giant step
+    // brings only its a row down before rotating, the giant-step results add up in QlP and
+    // one ModDown of all n + 1 rows ends the layer.  Every extended batch stands for its
+    // ModDown, so the result is the layer's product up to ModDown rounding (a few units).
+    Ciphertext apply_ext(const Evaluator &ev, const Ciphertext &x, bool rescale) const {
+        const Context &c = ev.context();
+        shm_context *h = c.handle();
+        if (!ev.shared_keys || ev.shared_keys->members != x.members())
+            throw Error("no shared-a keys for this group size");
+        const uint32_t G = x.count, n = x.members(), H = n + 1, L = level_;
+        const size_t E = (size_t)G * H * (L + c.np) * c.n;  // words of one extended batch
+        auto key_of = [&](int64_t step) {
+            const uint32_t elt = ev.galois_elt((int)step);
+            auto it = ev.shared_keys->galois.find(elt);
+            if (it == ev.shared_keys->galois.end()) throw Error("missing Galois key for element " + std::to_string(elt));
+            return std::make_pair(elt, (const uint64_t *)it->second.data());
+        };
+        const size_t wsb = std::max(shm_shared_rotate_ext_workspace_bytes(h, G, n, L),
+                                    shm_moddown_ext_workspace_bytes(h, G * H, L));
+        DeviceBuffer ws(c, wsb / 8 + 1);
+        // baby steps, one ModUp for all of them
+        std::vector<int64_t> babies;
+        for (int64_t v : baby_)
+            if (v) babies.push_back(v);
+        DeviceBuffer rots(c, E * babies.size());
+        std::map<int64_t, const uint64_t *> ext_of;
+        {
+            std::vector<uint32_t> elts;
+            std::vector<const uint64_t *> keys;
+            std::vector<uint64_t *> outs;
+            for (size_t i = 0; i < babies.size(); i++) {
+                auto k = key_of(babies[i] * b_);
+                elts.push_back(k.first);
+                keys.push_back(k.second);
+                outs.push_back(rots.data() + i * E);
+                ext_of[babies[i]] = outs.back();
+            }
+            if (!babies.empty())
+                c.check(shm_shared_rotate_ext(h, x.data.data(), 0, G, n, (uint32_t)babies.size(), elts.data(),
+                                              keys.data(), outs.data(), L, ws.data(), ws.words() * 8, c.stream()));
+        }
+        DeviceBuffer xext(c, E);
+        c.check(shm_extend(h, x.data.data(), xext.data(), G * H, L, c.stream()));
+        ext_of[0] = xext.data();
+        DeviceBuffer total, inner(c, E), rot(c, E);
+        for (auto &g : groups_) {
+            std::vector<const uint64_t *> X, P;
+            for (auto &vp : g.second) {
+                X.push_back(ext_of.at(vp.first));
+                P.push_back(vp.second.data.data());
+            }
+            c.check(shm_multiply_plain_accumulate_ext(h, X.data(), P.data(), (uint32_t)X.size(), inner.data(), G * H,
+                                                      L, 0, c.stream()));
+            DeviceBuffer *term = &inner;
+            if (g.first) {
+                auto k = key_of(g1_ * g.first * b_);
+                uint64_t *o = rot.data();
+                c.check(shm_shared_rotate_ext(h, inner.data(), 1, G, n, 1, &k.first, &k.second, &o, L, ws.data(),
+                                              ws.words() * 8, c.stream()));
+                term = &rot;
+            }
+            if (!total.data()) {
+                std::swap(total, *term);
+                if (!inner.data()) inner = DeviceBuffer(c, E);
+                if (!rot.data()) rot = DeviceBuffer(c, E);
+            } else {
+                c.check(shm_add_ext(h, total.data(), term->data(), total.data(), G * H, L, c.stream()));
+            }
+        }
+        Ciphertext out;
+        out.data = DeviceBuffer(c, (size_t)G * H * L * c.n);
+        out.count = G;
+        out.size = H;
+        out.L = L;
+        out.scale_ = x.scale_ * pt_scale_;
+        out.shared = true;
+        c.check(shm_moddown_ext(h, total.data(), out.data.data(), G * H, L, ws.data(), ws.words() * 8, c.stream()));
+        return rescale ? ev.rescale_to_next(out) : std::move(out);
+    }
+
     uint32_t level_;
     int64_t b_ = 1, g1_ = 1;
     double pt_scale_ = 1;
@@ -532,9 +617,10 @@ Ciphertext BatchBootstrapper::bootstrap_shared_a_s2c_first(const Ciphertext &ct,
 
 namespace {
 
-// milliseconds of one hoisted rotation batch with k targets (one ModUp, k inner products,
-// ModDowns and combines) of `count` ciphertexts (groups of `members` when members > 0) at L
-// primes, on uniform scratch residues and a scratch key (timing only)
+// milliseconds of one hoisted rotation batch with k targets of `count` ciphertexts at L primes:
+// one ModUp, k inner products, ModDowns and combines; for groups of `members` > 0 the
+// extended Sh-Rot of the double-hoisted layers (no ModDown per target).  Uniform scratch
+// residues and a scratch key (timing only)
 double time_rotations(const Evaluator &ev, uint32_t count, uint32_t members, uint32_t L, uint32_t k) {
     const Context &c = ev.context();
     shm_context *h = c.handle();
@@ -547,18 +633,20 @@ double time_rotations(const Evaluator &ev, uint32_t count, uint32_t members, uin
     std::vector<uint64_t *> optr;
     std::vector<const uint64_t *> keys(k, key.data());
     std::vector<uint32_t> elts;
+    // shared-a layers run extended (double hoisting): outputs over QlP, no ModDown per target
+    const size_t out_words = members ? (size_t)units * H * (L + c.np) * c.n : units * H * ln;
     for (uint32_t i = 0; i < k; i++) {
-        outs.emplace_back(c, units * H * ln);
+        outs.emplace_back(c, out_words);
         optr.push_back(outs.back().data());
         elts.push_back(ev.galois_elt((int)i + 1));
     }
-    const size_t wsb = members ? shm_shared_rotate_workspace_bytes(h, units, members, L)
+    const size_t wsb = members ? shm_shared_rotate_ext_workspace_bytes(h, units, members, L)
                                : shm_apply_galois_hoisted_workspace_bytes(h, units, L);
     DeviceBuffer ws(c, wsb / 8 + 1);
     auto run = [&] {
         if (members)
-            c.check(shm_shared_rotate_hoisted(h, x.data(), units, members, k, elts.data(), keys.data(), optr.data(), L,
-                                              ws.data(), ws.words() * 8, c.stream()));
+            c.check(shm_shared_rotate_ext(h, x.data(), 0, units, members, k, elts.data(), keys.data(), optr.data(), L,
+                                          ws.data(), ws.words() * 8, c.stream()));
         else
             c.check(shm_apply_galois_hoisted(h, x.data(), k, elts.data(), keys.data(), optr.data(), units, L,
                                              ws.data(), ws.words() * 8, c.stream()));

@@ -161,6 +161,24 @@ void Encoder::upload(const int64_t *coeffs, size_t n_polys, uint32_t L, uint64_t
     c_.check(shm_ntt_forward(c_.handle(), out, (uint32_t)n_polys, L, c_.stream()));
 }
 
+void Encoder::upload_ext(const int64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const {
+    DeviceBuffer tmp(c_, n_polys * c_.n);
+    c_.check(shm_memcpy(c_.handle(), tmp.data(), coeffs, n_polys * c_.n * 8, SHM_COPY_H2D, c_.stream()));
+    c_.check(shm_lift_signed_ext(c_.handle(), reinterpret_cast<const int64_t *>(tmp.data()), out, (uint32_t)n_polys,
+                                 L, c_.stream()));
+    c_.check(shm_ntt_forward_ext(c_.handle(), out, (uint32_t)n_polys, L, c_.stream()));
+}
+
+Plaintext Encoder::encode_ext(const std::vector<cplx> &z, uint32_t L, double scale) const {
+    std::vector<int64_t> coeffs = encode_coeffs(z.data(), z.size(), scale);
+    Plaintext p;
+    p.data = DeviceBuffer(c_, (size_t)(L + c_.np) * c_.n);
+    p.L = L;
+    p.scale = scale;
+    upload_ext(coeffs.data(), 1, L, p.data.data());
+    return p;
+}
+
 Plaintext Encoder::encode(const std::vector<cplx> &z, uint32_t L, double scale) const {
     std::vector<int64_t> coeffs = encode_coeffs(z.data(), z.size(), scale);
     Plaintext p;
