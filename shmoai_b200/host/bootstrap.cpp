@@ -304,7 +304,7 @@ class LinearTransform {
             dropped = ev.mod_switch_to(x, level_);
             xp = &dropped;
         }
-        if (xp->shared && ev.context().np) return apply_ext(ev, *xp, rescale);
+        if (ev.context().np && (xp->shared || xp->size == 2)) return apply_ext(ev, *xp, rescale);
         std::vector<int> bsteps;
         for (int64_t v : baby_)
             if (v) bsteps.push_back((int)(v * b_));
@@ -332,22 +332,31 @@ class LinearTransform {
     }
 
    private:
-    // Double hoisting (Bossuat et al.) for shared-a groups: the baby-step Sh-Rots stay in the
-    // extended basis QlP (no ModDown), the inner sums multiply QlP plaintexts, each giant step
-    // brings only its a row down before rotating, the giant-step results add up in QlP and
-    // one ModDown of all n + 1 rows ends the layer.  Every extended batch stands for its
-    // ModDown, so the result is the layer's product up to ModDown rounding (a few units).
+    // Double hoisting (Bossuat et al.): the baby-step rotations stay in the extended basis QlP
+    // (no ModDown), the inner sums multiply QlP plaintexts, each giant step brings only its a
+    // row down before rotating, the giant-step results add up in QlP and one ModDown of every
+    // row ends the layer.  Every extended batch stands for its ModDown, so the result is the
+    // layer's product up to ModDown rounding (a few units).  Shared-a groups of n use their
+    // Sh-Galois keys; an ordinary batch is the case n = 1 (an ordinary Galois key has the
+    // one-member Sh-Galois layout [dnum][2][QP][N]).
     Ciphertext apply_ext(const Evaluator &ev, const Ciphertext &x, bool rescale) const {
         const Context &c = ev.context();
         shm_context *h = c.handle();
-        if (!ev.shared_keys || ev.shared_keys->members != x.members())
-            throw Error("no shared-a keys for this group size");
-        const uint32_t G = x.count, n = x.members(), H = n + 1, L = level_;
+        const std::map<uint32_t, DeviceBuffer> *table = nullptr;
+        if (x.shared) {
+            if (!ev.shared_keys || ev.shared_keys->members != x.members())
+                throw Error("no shared-a keys for this group size");
+            table = &ev.shared_keys->galois;
+        } else {
+            if (!ev.galois_keys) throw Error("no Galois keys");
+            table = ev.galois_keys;
+        }
+        const uint32_t G = x.count, n = x.shared ? x.members() : 1, H = n + 1, L = level_;
         const size_t E = (size_t)G * H * (L + c.np) * c.n;  // words of one extended batch
         auto key_of = [&](int64_t step) {
             const uint32_t elt = ev.galois_elt((int)step);
-            auto it = ev.shared_keys->galois.find(elt);
-            if (it == ev.shared_keys->galois.end()) throw Error("missing Galois key for element " + std::to_string(elt));
+            auto it = table->find(elt);
+            if (it == table->end()) throw Error("missing Galois key for element " + std::to_string(elt));
             return std::make_pair(elt, (const uint64_t *)it->second.data());
         };
         const size_t wsb = std::max(shm_shared_rotate_ext_workspace_bytes(h, G, n, L),
@@ -408,7 +417,7 @@ class LinearTransform {
         out.size = H;
         out.L = L;
         out.scale_ = x.scale_ * pt_scale_;
-        out.shared = true;
+        out.shared = x.shared;
         c.check(shm_moddown_ext(h, total.data(), out.data.data(), G * H, L, ws.data(), ws.words() * 8, c.stream()));
         return rescale ? ev.rescale_to_next(out) : std::move(out);
     }
@@ -618,13 +627,13 @@ Ciphertext BatchBootstrapper::bootstrap_shared_a_s2c_first(const Ciphertext &ct,
 namespace {
 
 // milliseconds of one hoisted rotation batch with k targets of `count` ciphertexts at L primes:
-// one ModUp, k inner products, ModDowns and combines; for groups of `members` > 0 the
-// extended Sh-Rot of the double-hoisted layers (no ModDown per target).  Uniform scratch
-// residues and a scratch key (timing only)
+// one ModUp and k inner products with extended outputs, the rotation of the double-hoisted
+// layers; an ordinary batch is groups of one member.  Uniform scratch residues and a scratch
+// key (timing only)
 double time_rotations(const Evaluator &ev, uint32_t count, uint32_t members, uint32_t L, uint32_t k) {
     const Context &c = ev.context();
     shm_context *h = c.handle();
-    const uint32_t QP = c.nq + c.np, H = members ? members + 1 : 2, units = members ? count / members : count;
+    const uint32_t nm = members ? members : 1, H = nm + 1, units = count / nm, QP = c.nq + c.np;
     const size_t ln = (size_t)L * c.n;
     DeviceBuffer x(c, units * H * ln), key(c, (size_t)c.dnum * H * QP * c.n);
     c.check(shm_sample_uniform(h, x.data(), units * H, L, 0x7E5A, c.stream()));
@@ -633,23 +642,15 @@ double time_rotations(const Evaluator &ev, uint32_t count, uint32_t members, uin
     std::vector<uint64_t *> optr;
     std::vector<const uint64_t *> keys(k, key.data());
     std::vector<uint32_t> elts;
-    // shared-a layers run extended (double hoisting): outputs over QlP, no ModDown per target
-    const size_t out_words = members ? (size_t)units * H * (L + c.np) * c.n : units * H * ln;
     for (uint32_t i = 0; i < k; i++) {
-        outs.emplace_back(c, out_words);
+        outs.emplace_back(c, (size_t)units * H * (L + c.np) * c.n);
         optr.push_back(outs.back().data());
         elts.push_back(ev.galois_elt((int)i + 1));
     }
-    const size_t wsb = members ? shm_shared_rotate_ext_workspace_bytes(h, units, members, L)
-                               : shm_apply_galois_hoisted_workspace_bytes(h, units, L);
-    DeviceBuffer ws(c, wsb / 8 + 1);
+    DeviceBuffer ws(c, shm_shared_rotate_ext_workspace_bytes(h, units, nm, L) / 8 + 1);
     auto run = [&] {
-        if (members)
-            c.check(shm_shared_rotate_ext(h, x.data(), 0, units, members, k, elts.data(), keys.data(), optr.data(), L,
-                                          ws.data(), ws.words() * 8, c.stream()));
-        else
-            c.check(shm_apply_galois_hoisted(h, x.data(), k, elts.data(), keys.data(), optr.data(), units, L,
-                                             ws.data(), ws.words() * 8, c.stream()));
+        c.check(shm_shared_rotate_ext(h, x.data(), 0, units, nm, k, elts.data(), keys.data(), optr.data(), L,
+                                      ws.data(), ws.words() * 8, c.stream()));
     };
     run();
     c.synchronize();
