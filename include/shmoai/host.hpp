@@ -119,10 +119,17 @@ class Encoder {
    public:
     explicit Encoder(const Context &c);
     size_t slot_count() const { return c_.n / 2; }
-    // unrounded coefficients of the polynomial whose slots are z * scale (z padded with 0)
+    // unrounded coefficients of the polynomial whose slots are z * scale (z padded with 0), by
+    // the host's FFT: the restatement the device encoder (shm_encode) is checked against
     std::vector<double> encode_float(const cplx *z, size_t len, double scale) const;
-    // rounded (half to even) integer coefficients; |c| < 2^62 or Error
+    // rounded (half to even) integer coefficients; |c| < 2^62 or Error (shm_encode, FP64 on
+    // the device)
     std::vector<int64_t> encode_coeffs(const cplx *z, size_t len, double scale) const;
+    // the same for several slot vectors at once, into device memory [rows][N] (int64 words)
+    void encode_rows(const std::vector<std::vector<cplx>> &z, double scale, uint64_t *coeffs) const;
+    // device integer coefficients [n_polys][N] -> NTT-form residues [n_polys][L][N], or over QlP
+    void lift(const uint64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const;
+    void lift_ext(const uint64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const;
     Plaintext encode(const std::vector<cplx> &z, uint32_t L, double scale) const;
     // the same plaintext over the extended basis QlP: L + n_p limbs (the Q limbs, then the
     // special primes); its first L limbs are encode(z, L, scale).  L stays the Q limb count.
@@ -131,6 +138,8 @@ class Encoder {
     // (moai::Encoder::encode(double), ckks_evaluator_parallel.cuh:73-92)
     Plaintext encode(double value, uint32_t L, double scale) const;
     std::vector<cplx> decode(const std::vector<double> &coeffs, double scale) const;
+    // several coefficient vectors (real, centred) at once on the device (shm_decode)
+    std::vector<std::vector<cplx>> decode_rows(const std::vector<std::vector<double>> &coeffs, double scale) const;
     // signed integer coefficients [n_polys][N] (host) -> NTT-form residues [n_polys][L][N] at `out`
     void upload(const int64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const;
     // ... to [n_polys][L + n_p][N] over the extended basis QlP

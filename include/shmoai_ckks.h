@@ -338,6 +338,21 @@ int shm_sample_uniform(const shm_context *ctx, uint64_t *out, uint32_t n_polys, 
  * written as residues mod each of the first L primes (coefficient form). */
 int shm_sample_cbd(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed,
                    void *stream);
+/* ---- canonical-embedding encode / decode (FP64 on the GPU; the library's only
+ * floating-point work).  Replaces PhantomCKKSEncoder::encode_internal / decode_internal
+ * (thirdparty/phantom-fhe/src/ckks.cu:89-246, special FFT fft.cu:358-439) for a batch of
+ * vectors in one call.  Device arrays: re, im [n_vectors][n_values] slot values
+ * (n_values <= N/2, the rest zero) -> coeffs [n_vectors][N] = round-half-even of the
+ * coefficients of the polynomial whose slots are z * scale; SHM_EINVAL when one reaches 2^62
+ * (the call then synchronises the stream).  decode: coeffs [n_vectors][N] (real, centred)
+ * -> re, im [n_vectors][N/2] slot values / scale.  The FFT is the host encoder's
+ * (shmoai::Encoder::encode_float / decode) operation for operation, so both give the same
+ * bits. */
+size_t shm_encode_workspace_bytes(const shm_context *ctx, uint32_t n_vectors);
+int shm_encode(const shm_context *ctx, const double *re, const double *im, uint32_t n_vectors, uint32_t n_values,
+               double scale, int64_t *coeffs, void *workspace, size_t workspace_bytes, void *stream);
+int shm_decode(const shm_context *ctx, const double *coeffs, uint32_t n_vectors, double scale, double *re, double *im,
+               void *workspace, size_t workspace_bytes, void *stream);
 /* Signed coefficients [n_polys][N] (device) -> residues [n_polys][L][N] (coefficient form).
  * Replaces the signed decomposition of the encoder (rns_base.cu:51-200). */
 int shm_lift_signed(const shm_context *ctx, const int64_t *coeffs, uint64_t *out, uint32_t n_polys, uint32_t L,

@@ -65,6 +65,11 @@ int shm_host_decrypt(shm_host *h, const shm_ct *ct, double *re, double *im);
 int shm_ct_from_host(shm_host *h, const uint64_t *data, uint32_t count, uint32_t size, uint32_t L, double scale,
                      int shared, shm_ct **out);
 int shm_ct_to_host(shm_host *h, const shm_ct *ct, uint64_t *data);
+/* Integer coefficients [N] of one slot vector (re, im: n_values host doubles) at `scale`: by
+ * the device encoder (on_host = 0, shm_encode) or by the host's FFT restatement (on_host = 1,
+ * shmoai::Encoder::encode_float + round half to even); the two are equal bit for bit. */
+int shm_host_encode(shm_host *h, const double *re, const double *im, uint32_t n_values, double scale,
+                    int64_t *coeffs, int on_host);
 /* overwrite the residues of an existing batch from host words laid out as shm_ct_to_host
  * writes them (same count, size and level) */
 int shm_ct_write(shm_host *h, shm_ct *ct, const uint64_t *data);

@@ -9,6 +9,7 @@
  * "Device" memory is host memory here; streams and workspaces are ignored.  The samplers
  * use the same counter-based function as the CUDA library (splitmix64's output mix of
  * seed + (index + 1) * golden gamma), so keys and ciphertexts are identical. */
+#include <math.h>
 #include <stdio.h>
 
 #include "ckks_oracle.c"
@@ -252,6 +253,116 @@ int shm_sample_cbd(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint
                 out[((size_t)p * L + i) * n + k] = e >= 0 ? (uint64_t)e : q - (uint64_t)(-e);
             }
         }
+    return SHM_OK;
+}
+
+/* ---- canonical-embedding encode / decode: the host encoder's FFT (radix 2, bit reversal,
+ * then stages of len = 2 .. M; twiddles cos / sin (2 pi k / M), conjugated for the forward
+ * transform; every product and sum rounded on its own) */
+
+static void enc_fft(double *re, double *im, uint32_t M, int forward) {
+    for (uint32_t i = 1, j = 0; i < M; i++) {
+        uint32_t bit = M >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            double t = re[i];
+            re[i] = re[j];
+            re[j] = t;
+            t = im[i];
+            im[i] = im[j];
+            im[j] = t;
+        }
+    }
+    for (uint32_t len = 2; len <= M; len <<= 1) {
+        const uint32_t stride = M / len, half = len / 2;
+        for (uint32_t i = 0; i < M; i += len)
+            for (uint32_t k = 0; k < half; k++) {
+                const double ang = 2.0 * M_PI * (double)(k * stride) / (double)M;
+                const double wr = cos(ang), wi = forward ? -sin(ang) : sin(ang);
+                const double xr = re[i + k + half], xi = im[i + k + half];
+                const double vr = xr * wr - xi * wi, vi = xr * wi + xi * wr;
+                const double ur = re[i + k], ui = im[i + k];
+                re[i + k] = ur + vr;
+                im[i + k] = ui + vi;
+                re[i + k + half] = ur - vr;
+                im[i + k + half] = ui - vi;
+            }
+    }
+}
+
+static uint32_t *enc_exps(uint32_t n) {
+    uint32_t M = 2 * n, slots = n / 2;
+    uint32_t *e = (uint32_t *)malloc(sizeof(uint32_t) * slots);
+    uint64_t v = 1;
+    for (uint32_t j = 0; j < slots; j++) {
+        e[j] = (uint32_t)v;
+        v = (v * 5) % M;
+    }
+    return e;
+}
+
+size_t shm_encode_workspace_bytes(const shm_context *ctx, uint32_t n_vectors) {
+    (void)ctx;
+    (void)n_vectors;
+    return 0;
+}
+
+int shm_encode(const shm_context *ctx, const double *re, const double *im, uint32_t n_vectors, uint32_t n_values,
+               double scale, int64_t *coeffs, void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    const uint32_t n = ctx->c->n, M = 2 * n;
+    if (n_values > n / 2) return fail("more values than slots");
+    uint32_t *e = enc_exps(n);
+    double *ar = (double *)malloc(sizeof(double) * M), *ai = (double *)malloc(sizeof(double) * M);
+    const double f = 2.0 * scale / (double)n;
+    int bad = 0;
+    for (uint32_t p = 0; p < n_vectors && !bad; p++) {
+        memset(ar, 0, sizeof(double) * M);
+        memset(ai, 0, sizeof(double) * M);
+        for (uint32_t j = 0; j < n_values; j++) {
+            ar[e[j]] = re[(size_t)p * n_values + j];
+            ai[e[j]] = im[(size_t)p * n_values + j];
+        }
+        enc_fft(ar, ai, M, 1);
+        for (uint32_t k = 0; k < n; k++) {
+            const double r = nearbyint(f * ar[k]);
+            if (!(fabs(r) < 4611686018427387904.0)) {
+                bad = 1;
+                break;
+            }
+            coeffs[(size_t)p * n + k] = (int64_t)r;
+        }
+    }
+    free(ar);
+    free(ai);
+    free(e);
+    return bad ? fail("encoded values are too large") : SHM_OK;
+}
+
+int shm_decode(const shm_context *ctx, const double *coeffs, uint32_t n_vectors, double scale, double *re, double *im,
+               void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    const uint32_t n = ctx->c->n, M = 2 * n, slots = n / 2;
+    uint32_t *e = enc_exps(n);
+    double *br = (double *)malloc(sizeof(double) * M), *bi = (double *)malloc(sizeof(double) * M);
+    for (uint32_t p = 0; p < n_vectors; p++) {
+        memset(br, 0, sizeof(double) * M);
+        memset(bi, 0, sizeof(double) * M);
+        for (uint32_t k = 0; k < n; k++) br[k] = coeffs[(size_t)p * n + k];
+        enc_fft(br, bi, M, 0);
+        for (uint32_t j = 0; j < slots; j++) {
+            re[(size_t)p * slots + j] = br[e[j]] / scale;
+            im[(size_t)p * slots + j] = bi[e[j]] / scale;
+        }
+    }
+    free(br);
+    free(bi);
+    free(e);
     return SHM_OK;
 }
 

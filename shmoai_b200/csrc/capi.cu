@@ -34,6 +34,7 @@ void push4(std::vector<uint64_t> &v, uint64_t c, uint64_t psi_half_inv, uint64_t
 
 Context::~Context() {
     cudaSetDevice(device);
+    release_encode_tables(*this);
     for (void *p : {(void *)pc, (void *)tw, (void *)inv_scale_plain, (void *)moddown_scale, (void *)moddown_conv,
                     (void *)p_inv, (void *)p_mod, (void *)rescale_inv, arena})
         if (p) cudaFree(p);
@@ -1010,6 +1011,32 @@ int shm_sample_cbd(const shm_context *ctx, uint64_t *out, uint32_t n_polys, uint
         check_level(c, L);
         set_device(c);
         shm::sample_cbd(c, out, n_polys, L, seed, S(stream));
+    });
+}
+
+size_t shm_encode_workspace_bytes(const shm_context *ctx, uint32_t n_vectors) {
+    return ctx && ctx->c ? shm::encode_ws_bytes(*ctx->c, n_vectors) : 0;
+}
+
+int shm_encode(const shm_context *ctx, const double *re, const double *im, uint32_t n_vectors, uint32_t n_values,
+               double scale, int64_t *coeffs, void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        if (n_values && (!re || !im)) throw std::invalid_argument("null slot arrays");
+        set_device(c);
+        void *ws = ws_of(c, workspace, workspace_bytes, (shm::encode_ws_bytes(c, n_vectors) + 7) / 8);
+        if (!shm::encode(c, re, im, n_vectors, n_values, scale, coeffs, ws, S(stream)))
+            throw std::invalid_argument("encoded values are too large");
+    });
+}
+
+int shm_decode(const shm_context *ctx, const double *coeffs, uint32_t n_vectors, double scale, double *re, double *im,
+               void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        set_device(c);
+        void *ws = ws_of(c, workspace, workspace_bytes, (shm::encode_ws_bytes(c, n_vectors) + 7) / 8);
+        shm::decode(c, coeffs, n_vectors, scale, re, im, ws, S(stream));
     });
 }
 

@@ -163,6 +163,15 @@ void ctpt_matmul_cuda_core(const Context &c, const uint64_t *X, const int64_t *W
                            uint32_t n_out, uint32_t L, cudaStream_t st);
 size_t ctpt_tc_ws_bytes(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);
 
+// canonical-embedding encode / decode in FP64 (encode.cu); encode returns false when a
+// coefficient reaches 2^62
+size_t encode_ws_bytes(const Context &c, uint32_t n_pts);
+bool encode(const Context &c, const double *re, const double *im, uint32_t n_pts, uint32_t n_values, double scale,
+            int64_t *coeffs, void *ws, cudaStream_t st);
+void decode(const Context &c, const double *coeffs, uint32_t n_pts, double scale, double *re, double *im, void *ws,
+            cudaStream_t st);
+void release_encode_tables(const Context &c);
+
 // counter-based samplers and the signed lift (sampling.cu)
 void sample_uniform(const Context &c, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed, cudaStream_t st);
 void sample_cbd(const Context &c, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t seed, cudaStream_t st);

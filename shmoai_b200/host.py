@@ -86,6 +86,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_graph_kernels": (ctypes.c_uint64, [_P]),
         "shm_host_graph_destroy": (None, [_P]),
         "shm_ct_write": (i32, [_P, _P, u64p]),
+        "shm_host_encode": (i32, [_P, dp, dp, _U32, ctypes.c_double, ctypes.POINTER(ctypes.c_int64), i32]),
         "shm_slot_transform_selfcheck": (ctypes.c_double, [_U32]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
@@ -195,6 +196,16 @@ class Host:
         dp = ctypes.POINTER(ctypes.c_double)
         self._check(self.lib.shm_host_decrypt(self._h, ct._c, re.ctypes.data_as(dp), im.ctypes.data_as(dp)))
         return re + 1j * im
+
+    def encode_coeffs(self, z, scale: float, on_host: bool = False) -> np.ndarray:
+        """Integer coefficients of one slot vector: the device encoder, or the host FFT restatement."""
+        z = np.asarray(z, dtype=np.complex128)
+        re, im = np.ascontiguousarray(z.real), np.ascontiguousarray(z.imag)
+        out = np.empty(self.n, dtype=np.int64)
+        self._check(self.lib.shm_host_encode(self._h, re.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                             im.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(z), scale,
+                                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), int(on_host)))
+        return out
 
     def ct_from_host(self, data: np.ndarray, scale: float, shared: bool = False) -> "Ct":
         d = np.ascontiguousarray(data, dtype=np.uint64)

@@ -1,5 +1,6 @@
 // extern "C" entry points of include/shmoai_host.h over the C++ host classes.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -243,6 +244,29 @@ int shm_ct_info(const shm_ct *ct, uint32_t *count, uint32_t *size, uint32_t *L, 
         if (L) *L = c.L;
         if (scale) *scale = c.scale_;
         if (shared) *shared = c.shared ? 1 : 0;
+    });
+}
+
+int shm_host_encode(shm_host *h, const double *re, const double *im, uint32_t n_values, double scale,
+                    int64_t *coeffs, int on_host) {
+    return guard([&] {
+        auto &hh = H(h);
+        std::vector<cplx> z(n_values);
+        for (uint32_t j = 0; j < n_values; j++) z[j] = cplx(re[j], im[j]);
+        Encoder enc(*hh.ctx);
+        std::vector<int64_t> c;
+        if (on_host) {
+            std::vector<double> f = enc.encode_float(z.data(), z.size(), scale);
+            c.resize(f.size());
+            for (size_t k = 0; k < f.size(); k++) {
+                const double r = std::nearbyint(f[k]);
+                if (!(std::fabs(r) < 4611686018427387904.0)) throw Error("encoded values are too large");
+                c[k] = (int64_t)r;
+            }
+        } else {
+            c = enc.encode_coeffs(z.data(), z.size(), scale);
+        }
+        std::copy(c.begin(), c.end(), coeffs);
     });
 }
 

@@ -142,15 +142,49 @@ std::vector<double> Encoder::encode_float(const cplx *z, size_t len, double scal
     return out;
 }
 
-std::vector<int64_t> Encoder::encode_coeffs(const cplx *z, size_t len, double scale) const {
-    std::vector<double> f = encode_float(z, len, scale);
-    std::vector<int64_t> out(f.size());
-    for (size_t k = 0; k < f.size(); k++) {
-        const double r = std::nearbyint(f[k]);
-        if (!(std::fabs(r) < 4611686018427387904.0)) throw Error("encoded values are too large");
-        out[k] = (int64_t)r;
+void Encoder::encode_rows(const std::vector<std::vector<cplx>> &z, double scale, uint64_t *coeffs) const {
+    const uint32_t rows = (uint32_t)z.size(), slots = c_.n / 2;
+    size_t nv = 0;
+    for (auto &r : z) nv = std::max(nv, r.size());
+    if (nv > slots) throw Error("more values than slots");
+    shm_context *h = c_.handle();
+    DeviceBuffer dre, dim;
+    if (nv) {
+        std::vector<double> re(rows * nv, 0.0), im(rows * nv, 0.0);  // shorter rows padded with zero slots
+        for (uint32_t i = 0; i < rows; i++)
+            for (size_t j = 0; j < z[i].size(); j++) {
+                re[i * nv + j] = z[i][j].real();
+                im[i * nv + j] = z[i][j].imag();
+            }
+        dre = DeviceBuffer(c_, re.size());
+        dim = DeviceBuffer(c_, im.size());
+        c_.check(shm_memcpy(h, dre.data(), re.data(), re.size() * 8, SHM_COPY_H2D, c_.stream()));
+        c_.check(shm_memcpy(h, dim.data(), im.data(), im.size() * 8, SHM_COPY_H2D, c_.stream()));
     }
+    DeviceBuffer ws(c_, shm_encode_workspace_bytes(h, rows) / 8 + 1);
+    c_.check(shm_encode(h, reinterpret_cast<const double *>(dre.data()), reinterpret_cast<const double *>(dim.data()),
+                        rows, (uint32_t)nv, scale, reinterpret_cast<int64_t *>(coeffs), ws.data(), ws.words() * 8,
+                        c_.stream()));
+}
+
+std::vector<int64_t> Encoder::encode_coeffs(const cplx *z, size_t len, double scale) const {
+    DeviceBuffer d(c_, c_.n);
+    encode_rows({std::vector<cplx>(z, z + len)}, scale, d.data());
+    std::vector<int64_t> out(c_.n);
+    c_.check(shm_memcpy(c_.handle(), out.data(), d.data(), c_.n * 8, SHM_COPY_D2H, c_.stream()));
     return out;
+}
+
+void Encoder::lift(const uint64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const {
+    c_.check(shm_lift_signed(c_.handle(), reinterpret_cast<const int64_t *>(coeffs), out, (uint32_t)n_polys, L,
+                             c_.stream()));
+    c_.check(shm_ntt_forward(c_.handle(), out, (uint32_t)n_polys, L, c_.stream()));
+}
+
+void Encoder::lift_ext(const uint64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const {
+    c_.check(shm_lift_signed_ext(c_.handle(), reinterpret_cast<const int64_t *>(coeffs), out, (uint32_t)n_polys, L,
+                                 c_.stream()));
+    c_.check(shm_ntt_forward_ext(c_.handle(), out, (uint32_t)n_polys, L, c_.stream()));
 }
 
 void Encoder::upload(const int64_t *coeffs, size_t n_polys, uint32_t L, uint64_t *out) const {
@@ -170,22 +204,24 @@ void Encoder::upload_ext(const int64_t *coeffs, size_t n_polys, uint32_t L, uint
 }
 
 Plaintext Encoder::encode_ext(const std::vector<cplx> &z, uint32_t L, double scale) const {
-    std::vector<int64_t> coeffs = encode_coeffs(z.data(), z.size(), scale);
+    DeviceBuffer coeffs(c_, c_.n);
+    encode_rows({z}, scale, coeffs.data());
     Plaintext p;
     p.data = DeviceBuffer(c_, (size_t)(L + c_.np) * c_.n);
     p.L = L;
     p.scale = scale;
-    upload_ext(coeffs.data(), 1, L, p.data.data());
+    lift_ext(coeffs.data(), 1, L, p.data.data());
     return p;
 }
 
 Plaintext Encoder::encode(const std::vector<cplx> &z, uint32_t L, double scale) const {
-    std::vector<int64_t> coeffs = encode_coeffs(z.data(), z.size(), scale);
+    DeviceBuffer coeffs(c_, c_.n);
+    encode_rows({z}, scale, coeffs.data());
     Plaintext p;
     p.data = DeviceBuffer(c_, (size_t)L * c_.n);
     p.L = L;
     p.scale = scale;
-    upload(coeffs.data(), 1, L, p.data.data());
+    lift(coeffs.data(), 1, L, p.data.data());
     return p;
 }
 
@@ -202,14 +238,29 @@ Plaintext Encoder::encode(double value, uint32_t L, double scale) const {
     return p;
 }
 
+std::vector<std::vector<cplx>> Encoder::decode_rows(const std::vector<std::vector<double>> &coeffs,
+                                                     double scale) const {
+    const uint32_t rows = (uint32_t)coeffs.size(), N = c_.n, slots = N / 2;
+    shm_context *h = c_.handle();
+    std::vector<double> flat((size_t)rows * N, 0.0), re((size_t)rows * slots), im((size_t)rows * slots);
+    for (uint32_t r = 0; r < rows; r++)
+        for (uint32_t k = 0; k < N && k < coeffs[r].size(); k++) flat[(size_t)r * N + k] = coeffs[r][k];
+    DeviceBuffer dc(c_, flat.size()), dre(c_, re.size()), dim(c_, im.size());
+    DeviceBuffer ws(c_, shm_encode_workspace_bytes(h, rows) / 8 + 1);
+    c_.check(shm_memcpy(h, dc.data(), flat.data(), flat.size() * 8, SHM_COPY_H2D, c_.stream()));
+    c_.check(shm_decode(h, reinterpret_cast<const double *>(dc.data()), rows, scale,
+                        reinterpret_cast<double *>(dre.data()), reinterpret_cast<double *>(dim.data()), ws.data(),
+                        ws.words() * 8, c_.stream()));
+    c_.check(shm_memcpy(h, re.data(), dre.data(), re.size() * 8, SHM_COPY_D2H, c_.stream()));
+    c_.check(shm_memcpy(h, im.data(), dim.data(), im.size() * 8, SHM_COPY_D2H, c_.stream()));
+    std::vector<std::vector<cplx>> out(rows, std::vector<cplx>(slots));
+    for (uint32_t r = 0; r < rows; r++)
+        for (uint32_t j = 0; j < slots; j++) out[r][j] = cplx(re[(size_t)r * slots + j], im[(size_t)r * slots + j]);
+    return out;
+}
+
 std::vector<cplx> Encoder::decode(const std::vector<double> &coeffs, double scale) const {
-    const uint32_t N = c_.n, M = 2 * N, slots = N / 2;
-    std::vector<cplx> B(M, cplx(0, 0));
-    for (uint32_t k = 0; k < N && k < coeffs.size(); k++) B[k] = cplx(coeffs[k], 0);
-    fft(B, true);
-    std::vector<cplx> z(slots);
-    for (uint32_t j = 0; j < slots; j++) z[j] = B[exps_[j]] / scale;
-    return z;
+    return decode_rows({coeffs}, scale)[0];
 }
 
 // ------------------------------------------------------------------ KeyGenerator
@@ -379,14 +430,13 @@ Ciphertext KeyGenerator::encrypt(const std::vector<std::vector<cplx>> &z, double
     if (L < 1 || L > c_.nq) throw Error("level out of range");
     shm_context *h = c_.handle();
     void *st = c_.stream();
-    std::vector<int64_t> coeffs((size_t)count * N);
-    for (uint32_t i = 0; i < count; i++) {
-        std::vector<int64_t> m = enc_.encode_coeffs(z[i].data(), z[i].size(), scale);
-        std::copy(m.begin(), m.end(), coeffs.begin() + (size_t)i * N);
-    }
     const size_t ln = (size_t)L * N;
     DeviceBuffer m(c_, count * ln), a(c_, count * ln), e(c_, count * ln), t(c_, count * ln);
-    enc_.upload(coeffs.data(), count, L, m.data());
+    {
+        DeviceBuffer coeffs(c_, (size_t)count * N);  // every row encoded in one batch on the device
+        enc_.encode_rows(z, scale, coeffs.data());
+        enc_.lift(coeffs.data(), count, L, m.data());
+    }
     c_.check(shm_sample_uniform(h, a.data(), count, L, next_seed(), st));
     c_.check(shm_sample_cbd(h, e.data(), count, L, next_seed(), st));
     c_.check(shm_ntt_forward(h, e.data(), count, L, st));
@@ -449,11 +499,7 @@ std::vector<std::vector<double>> KeyGenerator::decrypt_coeffs(const Ciphertext &
 }
 
 std::vector<std::vector<cplx>> KeyGenerator::decrypt(const Ciphertext &ct) {
-    std::vector<std::vector<double>> c = decrypt_coeffs(ct);
-    std::vector<std::vector<cplx>> out;
-    out.reserve(c.size());
-    for (auto &row : c) out.push_back(enc_.decode(row, ct.scale_));
-    return out;
+    return enc_.decode_rows(decrypt_coeffs(ct), ct.scale_);
 }
 
 }  // namespace shmoai

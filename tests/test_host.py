@@ -235,3 +235,40 @@ def test_tuned_split_is_bit_exact_between_builds():
     og, oc = bg.run(g.encrypt(z, DELTA, 4), members=2), bc.run(c.encrypt(z, DELTA, 4), members=2)
     assert np.array_equal(og.to_host(), oc.to_host())
     assert np.abs(g.decrypt(og) - z).mean() < 2e-5
+
+
+def _encode_cases(h, rng):
+    n = h.n // 2
+    return [(_z(rng, 1, n)[0], DELTA), (_z(rng, 1, 100)[0], 2.0 ** 40),
+            (np.round(_z(rng, 1, n)[0] * 8) / 8, 2.0 ** 20), (np.zeros(0, dtype=np.complex128), DELTA)]
+
+
+def test_oracle_encoder_matches_host_fft_bit_for_bit():
+    """The oracle's shm_encode (the device encoder's C restatement) equals the host FFT
+    restatement (Encoder::encode_float + round half to even) bit for bit, and decoding
+    through shm_decode returns the slots."""
+    h = Host(12, _small_primes(), 5, hamming_weight=64, seed=17, lib=ORACLE_HOST)
+    rng = np.random.default_rng(31)
+    for z, scale in _encode_cases(h, rng):
+        assert np.array_equal(h.encode_coeffs(z, scale), h.encode_coeffs(z, scale, on_host=True))
+    z = _z(rng, 2, h.n // 2)
+    err = np.abs(h.decrypt(h.encrypt(z, DELTA, 4)) - z)
+    assert err.max() < 1e-6
+    with pytest.raises(HostError, match="too large"):
+        h.encode_coeffs(np.full(4, 1e6 + 0j), 2.0 ** 60)
+
+
+@pytest.mark.gpu
+def test_device_encoder_matches_host_fft_bit_for_bit():
+    """FP64 canonical embedding on the GPU (shm_encode / shm_decode): the same coefficients
+    as the host FFT restatement, bit for bit, at N = 2^12 and 2^16; encrypt / decrypt round
+    trip through the device encoder and decoder."""
+    rng = np.random.default_rng(32)
+    for log_n, bits in ((12, SMALL_BITS), (16, REF_BITS)):
+        h = Host(log_n, O.gen_primes(log_n, bits), 5, hamming_weight=64, seed=18)
+        for z, scale in _encode_cases(h, rng):
+            assert np.array_equal(h.encode_coeffs(z, scale), h.encode_coeffs(z, scale, on_host=True)), log_n
+        z = _z(rng, 3, h.n // 2)
+        err = np.abs(h.decrypt(h.encrypt(z, DELTA, 4)) - z)
+        assert err.max() < 1e-6
+        h.close()
