@@ -185,6 +185,13 @@ class KeyGenerator {
     std::vector<std::vector<double>> decrypt_coeffs(const Ciphertext &ct);
     std::vector<std::vector<cplx>> decrypt(const Ciphertext &ct);
 
+    // signed coefficients of the secret and of the auxiliary secrets of shared-a groups
+    const std::vector<int64_t> &secret_coeffs() const { return s_coeffs_; }
+    const std::vector<std::vector<int64_t>> &aux_secret_coeffs() const { return aux_coeffs_; }
+    // replace the secret and the auxiliary secrets (keys made earlier are not touched), e.g.
+    // with ones read from a key stream or the reference's secret-key text
+    void import_secrets(const std::vector<int64_t> &s, const std::vector<std::vector<int64_t>> &aux);
+
    private:
     uint64_t next_seed();
     std::vector<int64_t> ternary(uint32_t hamming_weight);

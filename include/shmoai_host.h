@@ -131,6 +131,37 @@ void shm_host_graph_destroy(shm_host_graph *g);
 /* self-check of the slot-transform factorisation at 2^log_slots slots (max error) */
 double shm_slot_transform_selfcheck(uint32_t log_slots);
 
+/* ---- binary records (include/shmoai/wire.hpp): an 80-byte header naming the kind, ring,
+ * prime-chain digest, shape and scale, the payload words, then the payload's digest.
+ * Loading checks the header against the host's context, every residue against its prime
+ * and the digest; a failure returns SHM_EINVAL and builds nothing.
+ * Ciphertext batches go to and from caller memory: shm_ct_serialized_bytes gives the size
+ * of the record, shm_ct_serialize writes it (cap must hold it), shm_ct_deserialize reads
+ * exactly one record of `len` bytes. */
+int shm_ct_serialized_bytes(shm_host *h, const shm_ct *ct, size_t *bytes);
+int shm_ct_serialize(shm_host *h, const shm_ct *ct, void *buf, size_t cap);
+int shm_ct_deserialize(shm_host *h, const void *buf, size_t len, shm_ct **out);
+/* The host's keys to and from a file: the secrets (with_secrets != 0: the secret and the
+ * auxiliary secrets of the last shm_host_gen_shared_keys), the relinearisation key, the
+ * Galois keys and every shared-a key set.  Loading replaces what the file holds and keeps
+ * the rest (a Galois key of another element stays). */
+int shm_host_save_keys(shm_host *h, const char *path, int with_secrets);
+int shm_host_load_keys(shm_host *h, const char *path);
+/* The secret as the reference's text file: Q*P*N decimal residues in NTT form, limb-major,
+ * one per line (PhantomSecretKey::load_secret_key,
+ * thirdparty/phantom-fhe/include/secretkey.h:290-307).  Import replaces the host's secret
+ * (keys generated afterwards use it; existing keys are kept); the residues must be one
+ * small integer polynomial. */
+int shm_host_import_secret_text(shm_host *h, const char *path);
+int shm_host_export_secret_text(shm_host *h, const char *path);
+/* Install an evaluation key from host words laid out as the reference's key digits,
+ * [dnum][2][QP][N] (b then a, NTT form; PhantomRelinKey / PhantomGaloisKey,
+ * thirdparty/phantom-fhe/src/secretkey.cu:328-373): kind 0 = relinearisation key,
+ * kind 1 = Galois key of element `elt`.  n_words must be dnum * 2 * QP * N. */
+#define SHM_KEY_RELIN 0
+#define SHM_KEY_GALOIS 1
+int shm_host_import_key(shm_host *h, int kind, uint32_t elt, const uint64_t *words, size_t n_words);
+
 /* ---- serving loop (shmoai::Server): jobs admitted by an HBM budget onto `slots`
  * concurrent streams, queued jobs of the same kind and shape batched together.  Submit
  * calls take ownership of the ciphertext handle (it is destroyed, the caller must not use

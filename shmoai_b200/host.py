@@ -88,6 +88,14 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_ct_write": (i32, [_P, _P, u64p]),
         "shm_host_encode": (i32, [_P, dp, dp, _U32, ctypes.c_double, ctypes.POINTER(ctypes.c_int64), i32]),
         "shm_slot_transform_selfcheck": (ctypes.c_double, [_U32]),
+        "shm_ct_serialized_bytes": (i32, [_P, _P, ctypes.POINTER(ctypes.c_size_t)]),
+        "shm_ct_serialize": (i32, [_P, _P, ctypes.c_void_p, ctypes.c_size_t]),
+        "shm_ct_deserialize": (i32, [_P, ctypes.c_void_p, ctypes.c_size_t, pp]),
+        "shm_host_save_keys": (i32, [_P, ctypes.c_char_p, i32]),
+        "shm_host_load_keys": (i32, [_P, ctypes.c_char_p]),
+        "shm_host_import_secret_text": (i32, [_P, ctypes.c_char_p]),
+        "shm_host_export_secret_text": (i32, [_P, ctypes.c_char_p]),
+        "shm_host_import_key": (i32, [_P, i32, _U32, u64p, ctypes.c_size_t]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
         "shm_server_submit_rotate": (i32, [_P, _P, i32, ctypes.POINTER(ctypes.c_uint64)]),
@@ -161,6 +169,31 @@ class Host:
     def gen_shared_keys(self, members: int, elts, hamming_weight: int = 192):
         e = (_U32 * len(elts))(*elts)
         self._check(self.lib.shm_host_gen_shared_keys(self._h, members, hamming_weight, e, len(elts)))
+
+    def save_keys(self, path: str, with_secrets: bool = True):
+        """Write the secrets (optional), relinearisation, Galois and shared-a keys as binary records."""
+        self._check(self.lib.shm_host_save_keys(self._h, os.fsencode(path), 1 if with_secrets else 0))
+
+    def load_keys(self, path: str):
+        self._check(self.lib.shm_host_load_keys(self._h, os.fsencode(path)))
+
+    def import_secret_text(self, path: str):
+        """Take the secret from the reference's text format (NTT residues over Q*P, one per line)."""
+        self._check(self.lib.shm_host_import_secret_text(self._h, os.fsencode(path)))
+
+    def export_secret_text(self, path: str):
+        self._check(self.lib.shm_host_export_secret_text(self._h, os.fsencode(path)))
+
+    def import_key(self, words: np.ndarray, elt: int | None = None):
+        """Install a key [dnum][2][QP][N]: the relinearisation key, or the Galois key of `elt`."""
+        w = np.ascontiguousarray(words, dtype=np.uint64)
+        self._check(self.lib.shm_host_import_key(self._h, 0 if elt is None else 1, elt or 0,
+                                                 w.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), w.size))
+
+    def deserialize(self, data: bytes) -> "Ct":
+        """A ciphertext batch from one binary record (Ct.serialize)."""
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        return self._out(self.lib.shm_ct_deserialize, ctypes.cast(buf, ctypes.c_void_p), len(data))
 
     def galois_elt(self, step: int) -> int:
         return int(self.lib.shm_host_galois_elt(self._h, step))
@@ -286,6 +319,15 @@ class Ct:
         """Overwrite the batch's residues from host memory at `ptr` (the to_ptr layout)."""
         self.host._check(self.host.lib.shm_ct_write(self.host._h, self._c,
                                                     ctypes.cast(ptr, ctypes.POINTER(ctypes.c_uint64))))
+
+    def serialize(self) -> bytes:
+        """The batch as one binary record (header, residues, digest)."""
+        n = ctypes.c_size_t()
+        self.host._check(self.host.lib.shm_ct_serialized_bytes(self.host._h, self._c, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        self.host._check(self.host.lib.shm_ct_serialize(self.host._h, self._c, ctypes.cast(buf, ctypes.c_void_p),
+                                                        n.value))
+        return buf.raw
 
     def device_ptr(self) -> int:
         return int(self.host.lib.shm_ct_device_data(self._c) or 0)

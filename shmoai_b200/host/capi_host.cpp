@@ -3,9 +3,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <memory>
 
 #include "../../include/shmoai_host.h"
+#include "../../include/shmoai/wire.hpp"
 #include "internal.hpp"
 
 using namespace shmoai;
@@ -233,6 +235,133 @@ int shm_ct_to_host(shm_host *h, const shm_ct *ct, uint64_t *data) {
         const Ciphertext &c = C(ct);
         hh.ctx->check(shm_memcpy(hh.ctx->handle(), data, c.data.data(), c.polys() * c.L * hh.ctx->n * 8,
                                  SHM_COPY_D2H, hh.ctx->stream()));
+    });
+}
+
+int shm_ct_serialized_bytes(shm_host *h, const shm_ct *ct, size_t *bytes) {
+    return guard([&] {
+        if (!bytes) throw Error("null argument");
+        *bytes = wire::serialized_bytes(*H(h).ctx, C(ct));
+    });
+}
+
+int shm_ct_serialize(shm_host *h, const shm_ct *ct, void *buf, size_t cap) {
+    return guard([&] {
+        auto &hh = H(h);
+        const size_t need = wire::serialized_bytes(*hh.ctx, C(ct));
+        if (!buf || cap < need) throw Error("buffer smaller than the record (" + std::to_string(need) + " bytes)");
+        uint8_t *p = static_cast<uint8_t *>(buf);
+        size_t used = 0;
+        wire::save([&](const void *src, size_t n) {
+            if (used + n > need) throw Error("record larger than its computed size", SHM_EINTERNAL);
+            std::memcpy(p + used, src, n);
+            used += n;
+        }, *hh.ctx, C(ct));
+    });
+}
+
+int shm_ct_deserialize(shm_host *h, const void *buf, size_t len, shm_ct **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!buf) throw Error("null argument");
+        const uint8_t *p = static_cast<const uint8_t *>(buf);
+        size_t used = 0;
+        Ciphertext ct = wire::load_ciphertext([&](void *dst, size_t n) {
+            if (n > len - used) throw Error("record truncated");
+            std::memcpy(dst, p + used, n);
+            used += n;
+        }, *hh.ctx);
+        if (used != len) throw Error("bytes after the record");
+        put(out, std::move(ct));
+    });
+}
+
+int shm_host_save_keys(shm_host *h, const char *path, int with_secrets) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!path) throw Error("null path");
+        std::ofstream f(path, std::ios::binary | std::ios::trunc);
+        if (!f) throw Error(std::string("cannot open ") + path);
+        wire::KeySet ks;
+        if (with_secrets) {
+            ks.secret = &hh.kg->secret_coeffs();
+            ks.aux = &hh.kg->aux_secret_coeffs();
+        }
+        ks.relin = &hh.relin;
+        ks.galois = &hh.galois;
+        ks.shared = &hh.shared;
+        wire::save_keys([&](const void *src, size_t n) {
+            f.write(static_cast<const char *>(src), (std::streamsize)n);
+            if (!f) throw Error(std::string("write failed: ") + path);
+        }, *hh.ctx, ks);
+        f.close();
+        if (!f) throw Error(std::string("write failed: ") + path);
+    });
+}
+
+int shm_host_load_keys(shm_host *h, const char *path) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!path) throw Error("null path");
+        std::ifstream f(path, std::ios::binary);
+        if (!f) throw Error(std::string("cannot open ") + path);
+        wire::LoadedKeys k = wire::load_keys([&](void *dst, size_t n) {
+            f.read(static_cast<char *>(dst), (std::streamsize)n);
+            if ((size_t)f.gcount() != n) throw Error("record truncated");
+        }, *hh.ctx);
+        if (f.peek() != std::char_traits<char>::eof()) throw Error("bytes after the end record");
+        // everything was read and checked: install it
+        if (k.has_secret) hh.kg->import_secrets(k.secret, k.aux);
+        if (k.relin.data()) hh.relin = std::move(k.relin);
+        for (auto &kv : k.galois) hh.galois[kv.first] = std::move(kv.second);
+        hh.ev->shared_keys = nullptr;
+        for (auto &kv : k.shared) {
+            hh.shared.erase(kv.first);
+            hh.shared.emplace(kv.first, std::move(kv.second));
+        }
+    });
+}
+
+int shm_host_import_secret_text(shm_host *h, const char *path) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!path) throw Error("null path");
+        std::ifstream f(path);
+        if (!f) throw Error(std::string("cannot open ") + path);
+        hh.kg->import_secrets(wire::import_secret_text(f, *hh.ctx), {});
+    });
+}
+
+int shm_host_export_secret_text(shm_host *h, const char *path) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!path) throw Error("null path");
+        std::ofstream f(path, std::ios::trunc);
+        if (!f) throw Error(std::string("cannot open ") + path);
+        wire::export_secret_text(f, *hh.ctx, hh.kg->secret_coeffs());
+        f.close();
+        if (!f) throw Error(std::string("write failed: ") + path);
+    });
+}
+
+int shm_host_import_key(shm_host *h, int kind, uint32_t elt, const uint64_t *words, size_t n_words) {
+    return guard([&] {
+        auto &hh = H(h);
+        const Context &c = *hh.ctx;
+        if (!words) throw Error("null argument");
+        if (kind != SHM_KEY_RELIN && kind != SHM_KEY_GALOIS) throw Error("unknown key kind");
+        const size_t QP = c.nq + c.np, want = (size_t)c.dnum * 2 * QP * c.n;
+        if (n_words != want) throw Error("key of " + std::to_string(n_words) + " words, expected " + std::to_string(want));
+        if (kind == SHM_KEY_GALOIS && (elt % 2 == 0 || elt >= 2 * c.n)) throw Error("invalid Galois element");
+        for (size_t r = 0; r < (size_t)c.dnum * 2 * QP; r++) {
+            const uint64_t q = c.primes[r % QP], *w = words + r * c.n;
+            for (size_t k = 0; k < c.n; k++)
+                if (w[k] >= q) throw Error("key residue not below its prime");
+        }
+        DeviceBuffer key(c, want);
+        c.check(shm_memcpy(c.handle(), key.data(), words, want * 8, SHM_COPY_H2D, c.stream()));
+        if (kind == SHM_KEY_RELIN) hh.relin = std::move(key);
+        else hh.galois[elt] = std::move(key);
     });
 }
 

@@ -271,6 +271,19 @@ KeyGenerator::KeyGenerator(const Context &c, uint32_t hamming_weight, uint64_t s
     s_ = ntt_qp(s_coeffs_);
 }
 
+void KeyGenerator::import_secrets(const std::vector<int64_t> &s, const std::vector<std::vector<int64_t>> &aux) {
+    if (s.size() != c_.n) throw Error("secret has the wrong length");
+    for (auto &a : aux)
+        if (a.size() != c_.n) throw Error("auxiliary secret has the wrong length");
+    DeviceBuffer s_ntt = ntt_qp(s);
+    std::vector<DeviceBuffer> aux_ntt;
+    for (auto &a : aux) aux_ntt.push_back(ntt_qp(a));
+    s_coeffs_ = s;
+    s_ = std::move(s_ntt);
+    aux_coeffs_ = aux;
+    aux_ = std::move(aux_ntt);
+}
+
 uint64_t KeyGenerator::next_seed() { return detail::mix64(seed_, ++ctr_); }
 
 // ternary secret with exactly h non-zero coefficients (gen_secretkey and the MOAI
