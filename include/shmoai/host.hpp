@@ -271,6 +271,9 @@ class Evaluator {
     // to (also to size-2 batches) and relinearised later
     Ciphertext multiply_lazy(const Ciphertext &a, const Ciphertext &b) const;
     Ciphertext relinearize(const Ciphertext &a) const;  // size 3 -> 2 (evaluate.cu:1358-1390)
+    // size 3 at L -> size 2 at L - 1 with one ModDown by q_{L-1} P (shm_relinearize_rescale):
+    // relinearize then rescale_to_next up to a few units per coefficient, one forward NTT fewer
+    Ciphertext relinearize_rescale(const Ciphertext &a) const;
     // sum_i w_i X_i + w0 (added to c0) at L primes in one pass, the X_i read at their first L
     // limbs; w_i and w0 are integers held exactly by doubles; the result is given `scale`
     // (the terms' common scale times the weights' factor)

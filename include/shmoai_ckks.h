@@ -124,6 +124,18 @@ int shm_keyswitch(const shm_context *ctx, const uint64_t *d, const uint64_t *key
 int shm_relinearize(const shm_context *ctx, const uint64_t *ct3, const uint64_t *relin_key, uint64_t *out,
                     uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
 
+/* Relinearize and rescale n_cts size-3 ciphertexts [n_cts][3][L][N] (2 <= L) into
+ * [n_cts][2][L-1][N] with one ModDown by S = q_{L-1} P instead of a ModDown by P and a
+ * rescale by q_{L-1}: out = floor((P c + <ModUp(c2), key>) / S), the conversion of the S
+ * limbs made exact by its overflow count.  Equal to shm_relinearize + shm_rescale (the
+ * reference's relinearize_inplace then rescale_to_next, evaluate.cu:1358-1443) except for
+ * a coefficient whose sum lies within n_p + 1 of a multiple of q_{L-1} P (probability about
+ * n_p / q_{L-1}; the result is then one less).  Saves the rescale's INTT and one forward NTT
+ * of 2 (L - 1) limbs.  Workspace as shm_keyswitch_workspace_bytes(n_cts, L); out must not
+ * overlap ct3. */
+int shm_relinearize_rescale(const shm_context *ctx, const uint64_t *ct3, const uint64_t *relin_key, uint64_t *out,
+                            uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
+
 /* Apply the automorphism X -> X^galois_elt with its key to n_cts ciphertexts.
  * Replaces apply_galois_inplace (evaluate.cu:1586-1647). */
 int shm_apply_galois(const shm_context *ctx, const uint64_t *ct, uint32_t galois_elt, const uint64_t *galois_key,

@@ -419,16 +419,13 @@ static void moddown_one(const orc_ctx *c, const uint64_t *cx, uint32_t L, uint64
     free(z);
 }
 
-/* Hybrid key switch of one polynomial d (NTT form, L limbs) with a key of
- * dnum digits over QP: returns (cx0, cx1), each [L][N], not yet added. */
-void orc_keyswitch(const orc_ctx *c, const uint64_t *d, uint32_t L, const uint64_t *key, uint32_t dnum,
-                   uint64_t *out) {
+/* The key switch's inner product: cx [2][L + np][N] = sum_b ModUp(d)_b * key_b over QlP,
+ * before the ModDown (keyswitch_inplace up to the inner product, eval_key_switch.cu:91-160). */
+static void keyswitch_acc(const orc_ctx *c, const uint64_t *d, uint32_t L, const uint64_t *key, uint64_t *cx) {
     size_t n = c->n;
     uint32_t alpha = c->np, beta = (L + alpha - 1) / alpha, LP = L + c->np, QP = c->nq + c->np;
-    (void)dnum;
     uint64_t *up = (uint64_t *)malloc(sizeof(uint64_t) * beta * LP * n);
     orc_modup(c, d, L, up);
-    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * 2 * LP * n);
 #pragma omp parallel for
     for (int j = 0; j < (int)LP; j++) {
         uint32_t pj = ext_prime(c, L, j);
@@ -447,11 +444,104 @@ void orc_keyswitch(const orc_ctx *c, const uint64_t *d, uint32_t L, const uint64
             cx[((size_t)LP + j) * n + k] = (uint64_t)a1;
         }
     }
+    free(up);
+}
+
+/* Hybrid key switch of one polynomial d (NTT form, L limbs) with a key of
+ * dnum digits over QP: returns (cx0, cx1), each [L][N], not yet added. */
+void orc_keyswitch(const orc_ctx *c, const uint64_t *d, uint32_t L, const uint64_t *key, uint32_t dnum,
+                   uint64_t *out) {
+    size_t n = c->n;
+    uint32_t LP = L + c->np;
+    (void)dnum;
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * 2 * LP * n);
+    keyswitch_acc(c, d, L, key, cx);
     moddown_one(c, cx, L, out);
     moddown_one(c, cx + (size_t)LP * n, L, out + (size_t)L * n);
     free(cx);
-    free(up);
 }
+
+/* ModDown of one extended polynomial y [L + np][N] (NTT form over QlP) by S = q_{L-1} P
+ * into out [L-1][N] = floor(y / S): z_k = INTT(y_{s_k}) (S/s_k)^-1 mod s_k for
+ * s = (q_{L-1}, p_0, ..), v = floor(sum_k z_k / s_k) in double precision (one unfused
+ * multiply and add per term, k in order), conv_j = (sum_k z_k (S/s_k) - v S) mod q_j = [y]_S
+ * mod q_j, out_j = (y_j - NTT(conv_j)) S^-1 mod q_j.  The conversion of moddown_from_NTT
+ * (rns_bconv.cu:776-828) with q_{L-1} counted among the special primes, made exact by
+ * the overflow count v. */
+static void moddown_s(const orc_ctx *c, const uint64_t *y, uint32_t L, uint64_t *out) {
+    size_t n = c->n;
+    uint32_t ns = c->np + 1;
+    uint32_t sidx[65];
+    sidx[0] = L - 1;
+    for (uint32_t k = 0; k < c->np; k++) sidx[1 + k] = c->nq + k;
+    uint64_t *z = (uint64_t *)malloc(sizeof(uint64_t) * ns * n);
+    for (uint32_t k = 0; k < ns; k++) {
+        uint64_t s = c->primes[sidx[k]], h = 1;
+        uint32_t row = k == 0 ? L - 1 : L + (k - 1);
+        memcpy(z + (size_t)k * n, y + (size_t)row * n, sizeof(uint64_t) * n);
+        orc_ntt_inv(z + (size_t)k * n, c->log_n, s, c->irp + (size_t)sidx[k] * n);
+        for (uint32_t k2 = 0; k2 < ns; k2++)
+            if (k2 != k) h = mulmod(h, c->primes[sidx[k2]] % s, s);
+        uint64_t hinv = orc_invmod(h, s);
+        for (size_t t = 0; t < n; t++) z[(size_t)k * n + t] = mulmod(z[(size_t)k * n + t], hinv, s);
+    }
+    uint8_t *v = (uint8_t *)malloc(n);
+    double inv_s[65];
+    for (uint32_t k = 0; k < ns; k++) inv_s[k] = 1.0 / (double)c->primes[sidx[k]];
+    for (size_t t = 0; t < n; t++) {
+        double f = 0.0;
+        for (uint32_t k = 0; k < ns; k++) {
+            double prod = (double)z[(size_t)k * n + t] * inv_s[k];
+            f = f + prod;
+        }
+        v[t] = (uint8_t)f;
+    }
+#pragma omp parallel for
+    for (int j = 0; j < (int)L - 1; j++) {
+        uint64_t q = c->primes[j];
+        uint64_t hm[65], S = 1;
+        for (uint32_t k = 0; k < ns; k++) {
+            uint64_t h = 1;
+            for (uint32_t k2 = 0; k2 < ns; k2++)
+                if (k2 != k) h = mulmod(h, c->primes[sidx[k2]] % q, q);
+            hm[k] = h;
+            S = mulmod(S, c->primes[sidx[k]] % q, q);
+        }
+        uint64_t sinv = orc_invmod(S, q);
+        uint64_t *o = out + (size_t)j * n;
+        for (size_t t = 0; t < n; t++) {
+            u128 acc = 0;
+            for (uint32_t k = 0; k < ns; k++) acc += (u128)z[(size_t)k * n + t] * hm[k];
+            o[t] = submod((uint64_t)(acc % q), mulmod(v[t], S, q), q);
+        }
+        orc_ntt_fwd(o, c->log_n, q, c->rp + (size_t)j * n);
+        const uint64_t *yi = y + (size_t)j * n;
+        for (size_t t = 0; t < n; t++) o[t] = mulmod(submod(yi[t], o[t], q), sinv, q);
+    }
+    free(v);
+    free(z);
+}
+
+/* Relinearize and rescale one size-3 ciphertext ct3 [3][L][N] (L >= 2) into out [2][L-1][N]
+ * in one ModDown: y_h = P c_h + cx_h over QlP, out_h = ModDown_S(y_h) with S = q_{L-1} P. */
+void orc_relin_rescale(const orc_ctx *c, const uint64_t *ct3, uint32_t L, const uint64_t *key, uint64_t *out) {
+    size_t n = c->n, ln = (size_t)L * n;
+    uint32_t LP = L + c->np;
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * 2 * LP * n);
+    keyswitch_acc(c, ct3 + 2 * ln, L, key, cx);
+    for (uint32_t h = 0; h < 2; h++) {
+        uint64_t *y = cx + (size_t)h * LP * n;
+        for (uint32_t j = 0; j < L; j++) {
+            uint64_t q = c->primes[j], P = 1;
+            for (uint32_t k = 0; k < c->np; k++) P = mulmod(P, c->primes[c->nq + k] % q, q);
+            const uint64_t *cj = ct3 + (size_t)h * ln + (size_t)j * n;
+            for (size_t t = 0; t < n; t++) y[(size_t)j * n + t] = addmod(y[(size_t)j * n + t], mulmod(P, cj[t], q), q);
+        }
+        moddown_s(c, y, L, out + (size_t)h * (L - 1) * n);
+    }
+    free(cx);
+}
+
 
 /* Hoisted Galois key switching (Halevi-Shoup): ModUp of c1 once, then for each
  * element g the automorphism is applied to the extended digits (an NTT-domain

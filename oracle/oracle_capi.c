@@ -770,6 +770,21 @@ int shm_relinearize(const shm_context *ctx, const uint64_t *ct3, const uint64_t 
     return SHM_OK;
 }
 
+int shm_relinearize_rescale(const shm_context *ctx, const uint64_t *ct3, const uint64_t *relin_key, uint64_t *out,
+                            uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ks_level(ctx, L) || L < 2) return fail("relinearize-rescale needs 2 <= L <= n_q");
+    if (!ct3 || !relin_key || !out) return fail("null argument");
+    size_t ln = (size_t)L * ctx->c->n;
+    const uint64_t *ae = ct3 + (size_t)n_cts * 3 * ln, *oe = out + (size_t)n_cts * 2 * (ln - ctx->c->n);
+    if (n_cts && (const uint64_t *)out < ae && ct3 < oe) return fail("relinearize-rescale output overlaps its input");
+    for (uint32_t i = 0; i < n_cts; i++)
+        orc_relin_rescale(ctx->c, ct3 + i * 3 * ln, L, relin_key, out + (size_t)i * 2 * (ln - ctx->c->n));
+    return SHM_OK;
+}
+
 int shm_apply_galois(const shm_context *ctx, const uint64_t *ct, uint32_t galois_elt, const uint64_t *galois_key,
                      uint64_t *out, uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes,
                      void *stream) {

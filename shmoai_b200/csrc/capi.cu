@@ -38,10 +38,10 @@ Context::~Context() {
     for (void *p : {(void *)pc, (void *)tw, (void *)inv_scale_plain, (void *)moddown_scale, (void *)moddown_conv,
                     (void *)p_inv, (void *)p_mod, (void *)rescale_inv, arena})
         if (p) cudaFree(p);
-    for (auto &l : ks) {
-        if (l.modup_scale) cudaFree(l.modup_scale);
-        if (l.modup_conv) cudaFree(l.modup_conv);
-    }
+    for (auto &l : ks)
+        for (void *p : {(void *)l.modup_scale, (void *)l.modup_conv, (void *)l.rr_scale, (void *)l.rr_conv,
+                        (void *)l.rr_sinv, (void *)l.rr_vs, (void *)l.rr_inv_s})
+            if (p) cudaFree(p);
     for (auto &kv : galois_perm) cudaFree(kv.second);
     for (auto &kv : ext_consts)
         for (void *p : kv.second) cudaFree(p);
@@ -176,6 +176,7 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
         c->moddown_conv = upload(mdc);
         c->p_inv = upload(pinv);
         c->p_mod = upload(pmod);
+        c->h_p_mod = pmod;
         // ModUp constants per level
         for (uint32_t L = 1; L <= nq; L++) {
             LevelKS &ks = c->ks[L];
@@ -199,6 +200,44 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
             }
             ks.modup_scale = upload(msc);
             ks.modup_conv = upload(conv);
+            if (L < 2) continue;
+            // ModDown by S = q_{L-1} P
+            std::vector<uint64_t> S{primes[L - 1]};
+            std::vector<uint32_t> sidx{L - 1};
+            for (uint32_t k = 0; k < np; k++) {
+                S.push_back(P[k]);
+                sidx.push_back(nq + k);
+            }
+            std::vector<uint64_t> rsc, rconv((size_t)(L - 1) * (np + 1)), rsinv((size_t)(L - 1) * 2);
+            for (uint32_t k = 0; k <= np; k++) {
+                const uint64_t s = S[k], h = host::partial_product(S, k, s);
+                push4(rsc, host::mulmod(host::invmod(h, s), c->h_pc[sidx[k]].n_inv, s), psi_half_inv[sidx[k]], s);
+            }
+            for (uint32_t j = 0; j + 1 < L; j++) {
+                const uint64_t q = primes[j];
+                uint64_t prod = 1;
+                for (uint32_t k = 0; k <= np; k++) {
+                    rconv[(size_t)j * (np + 1) + k] = host::partial_product(S, k, q);
+                    prod = host::mulmod(prod, S[k] % q, q);
+                }
+                const uint64_t v = host::invmod(prod, q);
+                rsinv[2 * j] = v;
+                rsinv[2 * j + 1] = host::shoup_of(v, q);
+            }
+            std::vector<uint64_t> rvs((size_t)(L - 1) * 16);
+            for (uint32_t j = 0; j + 1 < L; j++) {
+                const uint64_t q = primes[j];
+                uint64_t Sq = 1;
+                for (uint32_t k = 0; k <= np; k++) Sq = host::mulmod(Sq, S[k] % q, q);
+                for (uint32_t v = 0; v < 16; v++) rvs[(size_t)j * 16 + v] = host::mulmod(v, Sq, q);
+            }
+            std::vector<double> rinvs(np + 1);
+            for (uint32_t k = 0; k <= np; k++) rinvs[k] = 1.0 / (double)S[k];
+            ks.rr_scale = upload(rsc);
+            ks.rr_conv = upload(rconv);
+            ks.rr_sinv = upload(rsinv);
+            ks.rr_vs = upload(rvs);
+            ks.rr_inv_s = upload(rinvs);
         }
     }
     SHM_CUDA(cudaDeviceSynchronize());
@@ -431,6 +470,22 @@ int shm_relinearize(const shm_context *ctx, const uint64_t *ct3, const uint64_t 
             o.add1 = out + ln;
         }
         shm::keyswitch(c, ct3 + 2 * ln, 3 * ln, n_cts, L, relin_key, o, ws, S(stream));
+    });
+}
+
+int shm_relinearize_rescale(const shm_context *ctx, const uint64_t *ct3, const uint64_t *relin_key, uint64_t *out,
+                            uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        set_device(c);
+        if (!ct3 || !relin_key || !out) throw std::invalid_argument("null argument");
+        const size_t ln = (size_t)L * c.n;
+        const uint64_t *a = ct3, *ae = ct3 + (size_t)n_cts * 3 * ln;
+        const uint64_t *o = out, *oe = out + (size_t)n_cts * 2 * (ln - c.n);
+        if (n_cts && o < ae && a < oe) throw std::invalid_argument("relinearize-rescale output overlaps its input");
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, shm::keyswitch_ws_words(c, n_cts, L));
+        shm::relin_rescale(c, ct3, n_cts, L, relin_key, out, ws, S(stream));
     });
 }
 

@@ -37,6 +37,13 @@ struct LevelKS {
     uint32_t L = 0, beta = 0;
     uint64_t *modup_scale = nullptr;  // [L][4]: N^-1 * qhat_i^-1 (digit-relative), for the INTT's last stage
     uint64_t *modup_conv = nullptr;   // [beta][L+np][alpha]: qhat_i mod t_j (0 on the digit's own rows)
+    // ModDown by S = q_{L-1} P (relinearisation and rescale in one; L >= 2): s_0 = q_{L-1},
+    // s_{1+k} = p_k
+    uint64_t *rr_scale = nullptr;  // [np + 1][4]: N^-1 * (S / s_k)^-1 mod s_k, for the INTT's last stage
+    uint64_t *rr_conv = nullptr;   // [L - 1][np + 1]: (S / s_k) mod q_j
+    uint64_t *rr_sinv = nullptr;   // [L - 1][2]: S^-1 mod q_j and its Shoup companion
+    uint64_t *rr_vs = nullptr;     // [L - 1][16]: (v S) mod q_j for v < 16 (exact conversion)
+    double *rr_inv_s = nullptr;    // [np + 1]: 1 / s_k rounded to double
 };
 
 struct Context {
@@ -54,6 +61,7 @@ struct Context {
     uint64_t *moddown_conv = nullptr;   // [nq][np]: phat_k mod q_j
     uint64_t *p_inv = nullptr;          // [nq][2]: P^-1 mod q_j and Shoup companion
     uint64_t *p_mod = nullptr;          // [nq][2]: P mod q_j and Shoup companion (extended basis)
+    std::vector<uint64_t> h_p_mod;      // host copy
     uint64_t *rescale_inv = nullptr;    // [nq][nq][2]: q_{L-1}^-1 mod q_j (row L-1), Shoup
     std::vector<LevelKS> ks;            // index L (1..nq)
     std::map<uint32_t, uint32_t *> galois_perm;  // elt -> [N] permutation
@@ -119,6 +127,12 @@ struct KsOutput {
 void keyswitch(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n_cts, uint32_t L, const uint64_t *key,
                const KsOutput &o, uint64_t *ws, cudaStream_t st);
 size_t keyswitch_ws_words(const Context &c, uint32_t n_cts, uint32_t L);
+// Relinearisation and rescale of n_cts size-3 ciphertexts ct3 [n_cts][3][L][N] in one
+// ModDown by S = q_{L-1} P with an exact conversion: out [n_cts][2][L-1][N] =
+// floor((P c_h + ks_h) / S), which equals relinearize-then-rescale unless that sum lies
+// within n_p + 1 of a multiple of q_{L-1} P; workspace keyswitch_ws_words(c, n_cts, L).
+void relin_rescale(const Context &c, const uint64_t *ct3, uint32_t n_cts, uint32_t L, const uint64_t *key,
+                   uint64_t *out, uint64_t *ws, cudaStream_t st);
 // Hoisted automorphisms: one ModUp of the c1 of n_cts ciphertexts `ct` ([n_cts][2][L][N]),
 // then per element e: outs[e] = (sigma_e(c0) + cx0, cx1) with keys[e].
 void apply_galois_hoisted(const Context &c, const uint64_t *ct, uint32_t n_cts, uint32_t L, uint32_t n_elts,

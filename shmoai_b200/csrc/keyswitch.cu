@@ -164,7 +164,87 @@ ModDownIO moddown_io(const Context &c, const uint64_t *acc, const KsOutput &o) {
 }
 
 
+// acc[ct][h][row] += (P mod q) * ct3[ct][h][row] for h = 0, 1: the q_{L-1} limb of P c added
+// before that limb joins the special primes of the ModDown by q_{L-1} P
+__global__ void add_p_times_kernel(uint64_t *__restrict__ acc, const uint64_t *__restrict__ ct3, uint32_t L,
+                                   uint32_t LP, uint32_t row, uint64_t pm, uint64_t pms, uint64_t q, uint32_t log_n) {
+    const uint32_t k = blockIdx.x * kThreads + threadIdx.x, poly = blockIdx.y, ct = poly >> 1, h = poly & 1;
+    uint64_t *a = acc + (((size_t)poly * LP + row) << log_n) + k;
+    const uint64_t x = ct3[(((size_t)ct * 3 + h) * L + row << log_n) + k];
+    *a = add_mod(*a, shoup(x, pm, pms, q), q);
+}
+
+// v = floor(sum_k z_k / s_k) for the INTT'd limbs z_k of S (rows first .. first + ns - 1 of
+// each [LP][N] polynomial, z_k = [y (S/s_k)^-1]_{s_k}): sum_k z_k (S / s_k) = [y]_S + v S, so
+// subtracting v S makes the conversion exact.  The sum is formed in double precision, one
+// unfused multiply and add per term in k order (the oracle does the same); its error is
+// below 2^-49, so v is wrong only when [y]_S / S lies that close to 0 or 1.
+__global__ void overflow_count_kernel(const uint64_t *__restrict__ acc, uint8_t *__restrict__ v, uint32_t LP,
+                                      uint32_t first, uint32_t ns, const double *__restrict__ inv_s, uint32_t log_n) {
+    const uint32_t k = blockIdx.x * kThreads + threadIdx.x, poly = blockIdx.y;
+    const uint64_t *z = acc + (((size_t)poly * LP + first) << log_n) + k;
+    double f = 0.0;
+    for (uint32_t i = 0; i < ns; i++) f = __dadd_rn(f, __dmul_rn(__ull2double_rn(z[(size_t)i << log_n]), __ldg(inv_s + i)));
+    v[((size_t)poly << log_n) + k] = (uint8_t)f;
+}
+
 }  // namespace
+
+void relin_rescale(const Context &c, const uint64_t *ct3, uint32_t n_cts, uint32_t L, const uint64_t *key,
+                   uint64_t *out, uint64_t *ws, cudaStream_t st) {
+    if (n_cts == 0) return;
+    if (c.np == 0) throw std::invalid_argument("context has no special primes: key switching unavailable");
+    if (L < 2 || L > c.nq) throw std::invalid_argument("relinearize-rescale needs 2 <= L <= n_q");
+    const uint32_t np = c.np, beta = (L + np - 1) / np, LP = L + np;
+    if (beta > c.dnum) throw std::invalid_argument("level needs more key digits than the key holds");
+    if (np > kMaxAlpha || beta > kMaxBeta || LP > 64) throw std::invalid_argument("key-switching shape too large");
+    const size_t n = c.n, ln = (size_t)L * n;
+    uint64_t *x = ws;
+    uint64_t *up = x + (size_t)n_cts * L * n;
+    uint64_t *acc = up + (size_t)n_cts * beta * LP * n;
+    uint64_t *delta = up;
+    const LevelKS &ks = c.ks[L];
+
+    modup_into(c, ct3 + 2 * ln, 3 * ln, n_cts, L, x, up, st);
+    launch_ip(c, n_cts, L, up, key, acc, nullptr, st);
+    // y = P c + ks over QlP: P c vanishes mod every p_k; on the limbs j < L - 1 it is folded
+    // into the ModDown's store as c_j q_{L-1}^-1 (= P c_j S^-1); limb L - 1 gets it here
+    const uint64_t ql = c.primes[L - 1];
+    SHM_LAUNCHED(1);
+    add_p_times_kernel<<<dim3(c.n / kThreads, n_cts * 2), kThreads, 0, st>>>(
+        acc, ct3, L, LP, L - 1, c.h_p_mod[2 * (L - 1)], c.h_p_mod[2 * (L - 1) + 1], ql, c.log_n);
+    SHM_CUDA(cudaGetLastError());
+    // ModDown by S = q_{L-1} P: INTT of rows L-1 .. LP-1 scaled by (S / s_k)^-1, the overflow
+    // count of the conversion, exact conversion to the L - 1 remaining primes, NTT,
+    // (y_j - conv_j) S^-1 = floor(y / S)
+    LimbMap mp;
+    for (uint32_t r = 0; r < 512; r++)
+        mp.prime[r] = r == L - 1 ? (uint8_t)(L - 1) : (r >= L && r < LP) ? (uint8_t)(c.nq + (r - L)) : 255;
+    ntt_inverse(c, acc, n_cts * 2 * LP, LP, mp, ks.rr_scale, st, L - 1);
+    uint8_t *vrow = reinterpret_cast<uint8_t *>(x);  // x is free after the ModUp: [n_cts][2][N] bytes
+    SHM_LAUNCHED(1);
+    overflow_count_kernel<<<dim3(c.n / kThreads, n_cts * 2), kThreads, 0, st>>>(acc, vrow, LP, L - 1, np + 1,
+                                                                                ks.rr_inv_s, c.log_n);
+    SHM_CUDA(cudaGetLastError());
+    ModDownIO md;
+    md.acc = acc;
+    md.conv = ks.rr_conv;
+    md.pinv = ks.rr_sinv;
+    md.out = out;
+    md.out_ct = (long long)(2 * (L - 1) * n);
+    md.out_h = (long long)((L - 1) * n);
+    md.add = ct3;
+    md.add_ct = (long long)(3 * ln);
+    md.add_h = (long long)ln;
+    md.add_mul = c.rescale_inv + (size_t)(L - 1) * c.nq * 2;
+    md.n_add = 2;
+    md.H = 2;
+    md.np = np + 1;
+    md.s52 = c.s52 ? 1 : 0;
+    md.vrow = vrow;
+    md.vs = ks.rr_vs;
+    ntt_forward_moddown(c, md, delta, n_cts * 2, L - 1, st);
+}
 
 size_t keyswitch_ws_words(const Context &c, uint32_t n_cts, uint32_t L) {
     const uint32_t beta = (L + c.np - 1) / c.np, LP = L + c.np;

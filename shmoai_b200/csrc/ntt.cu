@@ -54,9 +54,10 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 #pragma unroll
         for (int m = 0; m < G::E; m++) a[m] = barrett({src[sig + (size_t)G::M * (lane + m * G::E)], 0}, p);
     } else if constexpr (IOK == kIoModDown) {
-        __shared__ uint64_t sconv[16];
+        __shared__ uint64_t sconv[16], svs[16];
         const uint32_t np = io.md.np, j = row % slots;
         if (threadIdx.x < np) sconv[threadIdx.x] = io.md.conv[(size_t)j * np + threadIdx.x];
+        if (io.md.vrow && threadIdx.x < 16) svs[threadIdx.x] = io.md.vs[(size_t)j * 16 + threadIdx.x];
         __syncthreads();
         const PrimeConst p = pc[pidx];
         const uint64_t *z = io.md.acc + ((size_t)((row / slots) * (slots + np) + slots) << G::LOGN) + chunk * S;
@@ -72,6 +73,11 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
                 for (uint32_t k = 0; k < np; k++) acc.add(z[((size_t)k << G::LOGN) + pos], sconv[k]);
                 a[m] = barrett(acc.get(), p);
             }
+        }
+        if (io.md.vrow) {
+            const uint8_t *vr = io.md.vrow + ((size_t)(row / slots) << G::LOGN) + chunk * S;
+#pragma unroll
+            for (int m = 0; m < G::E; m++) a[m] = sub_mod(a[m], svs[vr[sig + (size_t)G::M * (lane + m * G::E)] & 15], q);
         }
     } else {
 #pragma unroll
@@ -161,13 +167,25 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
         const uint64_t iw = md.pinv[2 * j], iws = md.pinv[2 * j + 1];
         const bool add = h < md.n_add, perm = add && h < md.n_perm && md.perm;
         const uint64_t *ad = add ? md.add + ct * md.add_ct + h * md.add_h + ((size_t)j << G::LOGN) : nullptr;
+        if (md.add_mul) {
+            const uint64_t mw = md.add_mul[2 * j], mws = md.add_mul[2 * j + 1];
 #pragma unroll
-        for (int i = 0; i < G::E; i++) {
-            uint32_t e = threadIdx.x + i * G::THREADS;
-            const uint64_t t = sm[(e / G::M) * G::PAD_M + padded(e % G::M)];
-            uint64_t r = shoup(sub_mod(ain[e], t, q), iw, iws, q);
-            if (add) r = add_mod(r, ad[perm ? __ldg(md.perm + off + e) : off + e], q);
-            o[e] = r;
+            for (int i = 0; i < G::E; i++) {
+                uint32_t e = threadIdx.x + i * G::THREADS;
+                const uint64_t t = sm[(e / G::M) * G::PAD_M + padded(e % G::M)];
+                uint64_t r = shoup(sub_mod(ain[e], t, q), iw, iws, q);
+                if (add) r = add_mod(r, shoup(ad[perm ? __ldg(md.perm + off + e) : off + e], mw, mws, q), q);
+                o[e] = r;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < G::E; i++) {
+                uint32_t e = threadIdx.x + i * G::THREADS;
+                const uint64_t t = sm[(e / G::M) * G::PAD_M + padded(e % G::M)];
+                uint64_t r = shoup(sub_mod(ain[e], t, q), iw, iws, q);
+                if (add) r = add_mod(r, ad[perm ? __ldg(md.perm + off + e) : off + e], q);
+                o[e] = r;
+            }
         }
     } else {
 #pragma unroll

@@ -46,7 +46,8 @@ struct RescaleIO {
 
 // The ModDown's forward NTT (ntt_forward_moddown): rows (poly, j < L) of the delta buffer are
 // read as the base conversion sum_k z_k (phat_k mod q_j) of the INTT'd special-prime limbs
-// z_k = acc[poly][L + k], and written as (acc[poly][j] - NTT(...)) P^-1 (+ add) into out;
+// z_k = acc[poly][L + k], and written as (acc[poly][j] - NTT(...)) P^-1 (+ add, or
+// + add * add_mul[j]) into out;
 // poly = ct * H + h.  The add term of rows h < n_add is read at perm[pos] for rows h < n_perm.
 struct ModDownIO {
     const uint64_t *acc = nullptr;   // [polys][L + np][N]
@@ -54,7 +55,12 @@ struct ModDownIO {
     const uint64_t *pinv = nullptr;  // [nq][2]: P^-1 mod q_j and its Shoup companion
     uint64_t *out = nullptr;
     const uint64_t *add = nullptr;
+    const uint64_t *add_mul = nullptr;  // [nq][2]: the add term times this per-limb constant; null: as is
     const uint32_t *perm = nullptr;
+    // exact conversion: the conversion sum minus vs[j][v] (v S mod q_j) with v = vrow[poly][k],
+    // the overflow count floor(sum_k z_k / s_k); null: the approximate conversion
+    const uint8_t *vrow = nullptr;
+    const uint64_t *vs = nullptr;  // [slots][16]
     long long out_ct = 0, out_h = 0, add_ct = 0, add_h = 0;  // word strides
     uint32_t H = 2, np = 0, n_add = 0, n_perm = 0;
     int s52 = 0;  // every prime below 2^52: Acc<true>

@@ -489,12 +489,13 @@ namespace {
 
 using Basis = std::map<int, Ciphertext>;
 
-// T_1 .. T_8 and T_16, T_32, ... by products 2 T_a T_b - T_{a-b}
+// T_1 .. T_8 and T_16, T_32, ... by products 2 T_a T_b - T_{a-b}; each product is
+// relinearised and rescaled in one ModDown by q_{L-1} P
 Basis cheb_basis(const Evaluator &ev, const Ciphertext &x, int deg) {
     Basis T;
     T.emplace(1, ev.adjust(x, x.L, x.scale_));
     auto prod = [&](int a, int b) {
-        Ciphertext p = ev.multiply_int(ev.multiply(T.at(a), T.at(b)), 2);
+        Ciphertext p = ev.multiply_int(ev.relinearize_rescale(ev.multiply_lazy(T.at(a), T.at(b))), 2);
         if (a == b) return ev.add_const(p, -1.0);
         return ev.sub(p, ev.adjust(T.at(a - b), p.L, p.scale_));
     };
@@ -579,7 +580,7 @@ Ciphertext BatchBootstrapper::evalmod(const Ciphertext &x, const Evaluator *evp)
     for (int i = p_.double_angles - 1; i >= 0; i--) s = std::sqrt(s * (double)c.primes[lvl - 1 - i]);
     Ciphertext y = cheb_eval(ev, T, cheb_, s, lvl);
     for (int i = 0; i < p_.double_angles; i++) {  // y = 2 y^2 - 1, the affine part in one pass
-        const Ciphertext sq = ev.square(y);
+        const Ciphertext sq = ev.relinearize_rescale(ev.multiply_lazy(y, y));
         y = ev.linear_combination({&sq}, {2.0}, std::nearbyint(-1.0 * sq.scale_), sq.L, sq.scale_);
     }
     y.scale_ /= c_fin_;

@@ -249,6 +249,21 @@ Ciphertext Evaluator::relinearize(const Ciphertext &a) const {
     return r;
 }
 
+Ciphertext Evaluator::relinearize_rescale(const Ciphertext &a) const {
+    if (a.shared || a.size != 3) throw Error("relinearize_rescale takes size-3 ciphertexts");
+    if (!relin_key) throw Error("no relinearisation key");
+    if (a.L < 2) throw Error("no prime left to rescale by");
+    Ciphertext r;
+    r.data = DeviceBuffer(c_, (size_t)a.count * 2 * (a.L - 1) * c_.n);
+    r.count = a.count;
+    r.L = a.L - 1;
+    r.scale_ = a.scale_ / (double)c_.primes[a.L - 1];
+    uint64_t *w = ws(shm_keyswitch_workspace_bytes(c_.handle(), a.count, a.L));
+    c_.check(shm_relinearize_rescale(c_.handle(), a.data.data(), relin_key->data(), r.data.data(), a.count, a.L, w,
+                                     ws_.words() * 8, c_.stream()));
+    return r;
+}
+
 Ciphertext Evaluator::multiply(const Ciphertext &a, const Ciphertext &b, bool rescale) const {
     if (a.shared || b.shared || a.size != 2 || b.size != 2) throw Error("multiply needs ordinary ciphertexts");
     if (a.count != b.count) throw Error("batches of different sizes");
