@@ -40,10 +40,12 @@ constexpr uint32_t kSmem = kStages * (kStageA + kStageB) + 1024;
 constexpr uint32_t kThreads = 256;  // two warpgroups: loads shared, epilogue split by output columns
 constexpr long long kSpinLimit = 1ll << 24;
 
+// The constants of every candidate modulus, and the CRT fractions for every modulus count T
+// (M = m_0 .. m_{T-1}): the table does not depend on the call, so concurrent calls that
+// write it write the same bytes; each kernel takes its T as an argument.
 struct ModTab {
-    uint32_t t;
     uint32_t m[kMaxMods];
-    uint32_t fracx[kMaxMods];  // [(M/m_t)^-1]_{m_t} / m_t as a 32-bit fixed-point fraction
+    uint32_t fracx[kMaxMods + 1][kMaxMods];  // [T][t]: [(M/m_t)^-1]_{m_t} / m_t, 32-bit fixed point
     uint32_t c24[kMaxMods];  // 2^20 mod m_t
     uint32_t c48[kMaxMods];  // 2^40 mod m_t
     uint32_t magic[kMaxMods];  // ceil(2^32 / m_t)
@@ -88,7 +90,7 @@ __device__ __forceinline__ uint32_t mod_acc(int a, uint32_t t) {
 
 // X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via a 64 x 64 shared-memory transpose
 __global__ void xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__ XP, uint32_t n_in, uint32_t Kp,
-                            uint64_t R, uint64_t r0) {
+                            uint64_t R, uint64_t r0, uint32_t T) {
     __shared__ uint64_t tile[64][65];
     const uint32_t i0 = blockIdx.y * 64;
     const uint64_t rb = (uint64_t)blockIdx.x * 64;
@@ -103,19 +105,19 @@ __global__ void xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__
         uint64_t x = tile[tx][rr];
 #pragma unroll
         for (uint32_t t = 0; t < kMaxMods; t++)
-            if (t < c_mods.t)
+            if (t < T)
                 XP[((uint64_t)t * chunk + rb + rr) * Kp + i0 + tx] = balanced(mod_small(x, t), c_mods.m[t]);
     }
 }
 
 // W [n_in][n_out] (int64) -> WP [t][Np][Kp] (int8)
 __global__ void wres_kernel(const int64_t *__restrict__ W, int8_t *__restrict__ WP, uint32_t n_in, uint32_t n_out,
-                            uint32_t Kp, uint32_t Np) {
+                            uint32_t Kp, uint32_t Np, uint32_t T) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // input index (K)
     const uint32_t o = blockIdx.y;
     if (i >= Kp) return;
     int64_t w = (i < n_in && o < n_out) ? W[(uint64_t)i * n_out + o] : 0;
-    for (uint32_t t = 0; t < c_mods.t; t++) {
+    for (uint32_t t = 0; t < T; t++) {
         int64_t m = c_mods.m[t];
         int64_t r = w % m;
         if (r < 0) r += m;
@@ -323,14 +325,13 @@ struct CrtLimb {
 // two 16-byte stores instead of byte loads and 8-byte stores
 __global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict__ Y, const CrtLimb *__restrict__ tab,
                            uint32_t n_out, uint64_t chunk, uint64_t r0, uint64_t R, uint32_t L, uint32_t log_n,
-                           const PrimeConst *__restrict__ pc) {
+                           const PrimeConst *__restrict__ pc, uint32_t T) {
     const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const uint32_t o = blockIdx.y;
     if (r >= chunk) return;
     const uint64_t rg = r0 + r;
     const uint32_t limb = (uint32_t)((rg >> log_n) % L);
     const CrtLimb &cl = tab[limb];
-    const uint32_t T = c_mods.t;
     uint32_t res[kMaxMods];
 #pragma unroll
     for (uint32_t t = 0; t < kMaxMods; t++)  // all loads in flight before any use
@@ -350,7 +351,7 @@ __global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict
                 const uint64_t c = cl.c[t];
                 lo += (uint64_t)rt * (uint32_t)c;
                 hi += (uint64_t)rt * (uint32_t)(c >> 32);
-                vx += (uint64_t)rt * c_mods.fracx[t];
+                vx += (uint64_t)rt * c_mods.fracx[T][t];
             }
         }
         u128 pos = {lo + (hi << 32), (hi >> 32) + ((lo + (hi << 32)) < lo ? 1ull : 0ull)};
@@ -370,13 +371,14 @@ namespace {
 
 struct Plan {
     ModTab mods;
+    uint32_t T = 0;
     std::vector<CrtLimb> limbs;
 };
 
 Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) {
     // |S| < n_in * max q * max|W|; the moduli product must exceed 8 |S| (CRT margin)
-    static const uint32_t cand[] = {251, 241, 239, 233, 229, 227, 223, 211, 199, 197, 193, 191, 181, 179, 173,
-                                    167, 163, 157, 151, 149};
+    static const uint32_t cand[kMaxMods] = {251, 241, 239, 233, 229, 227, 223, 211, 199, 197,
+                                            193, 191, 181, 179, 173, 167, 163, 157, 151, 149};
     uint64_t maxq = 0;
     for (uint32_t l = 0; l < L; l++) maxq = std::max(maxq, c.primes[l]);
     const double need = std::log2((double)n_in) + std::log2((double)maxq) + std::log2((double)std::max<uint64_t>(max_abs_w, 1)) + 4.0;
@@ -385,36 +387,42 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
     uint32_t T = 0;
     while (have < need) {
         if (T >= (uint32_t)kMaxMods) throw std::invalid_argument("ct-pt matmul: weights or inputs too large");
-        p.mods.m[T] = cand[T];
         have += std::log2((double)cand[T]);
         T++;
     }
-    p.mods.t = T;
-    // CRT constants: c_t = (M/m_t) * [(M/m_t)^-1 mod m_t]; per limb mod q_l
-    for (uint32_t t = 0; t < T; t++) {
-        uint32_t m = p.mods.m[t], Mt_mod_m = 1;
-        for (uint32_t u = 0; u < T; u++)
-            if (u != t) Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (p.mods.m[u] % m) % m);
-        uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);  // m prime
-        p.mods.fracx[t] = (uint32_t)std::llround((double)inv / (double)m * 4294967296.0);
+    p.T = T;
+    for (uint32_t t = 0; t < (uint32_t)kMaxMods; t++) {
+        const uint32_t m = cand[t];
+        p.mods.m[t] = m;
         p.mods.c24[t] = (1u << 20) % m;
         p.mods.c48[t] = (uint32_t)((uint64_t)p.mods.c24[t] * p.mods.c24[t] % m);
         p.mods.magic[t] = (uint32_t)(((1ull << 32) + m - 1) / m);
         p.mods.inv[t] = 1.0 / m;
         p.mods.invf[t] = 1.0f / (float)m;
     }
+    // CRT fractions [(M/m_t)^-1 mod m_t] / m_t for every modulus count
+    for (uint32_t n = 1; n <= (uint32_t)kMaxMods; n++)
+        for (uint32_t t = 0; t < n; t++) {
+            const uint32_t m = cand[t];
+            uint32_t Mt_mod_m = 1;
+            for (uint32_t u = 0; u < n; u++)
+                if (u != t) Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (cand[u] % m) % m);
+            const uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);  // m prime
+            p.mods.fracx[n][t] = (uint32_t)std::llround((double)inv / (double)m * 4294967296.0);
+        }
+    // CRT constants of the chosen T: c_t = (M/m_t) * [(M/m_t)^-1 mod m_t] mod q_l
     p.limbs.resize(L);
     for (uint32_t l = 0; l < L; l++) {
         uint64_t q = c.primes[l], M = 1;
-        for (uint32_t u = 0; u < T; u++) M = host::mulmod(M, p.mods.m[u], q);
+        for (uint32_t u = 0; u < T; u++) M = host::mulmod(M, cand[u], q);
         p.limbs[l].M = M;
         for (uint32_t t = 0; t < T; t++) {
-            uint32_t m = p.mods.m[t], Mt_mod_m = 1;
+            uint32_t m = cand[t], Mt_mod_m = 1;
             uint64_t Mt = 1;
             for (uint32_t u = 0; u < T; u++)
                 if (u != t) {
-                    Mt = host::mulmod(Mt, p.mods.m[u], q);
-                    Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (p.mods.m[u] % m) % m);
+                    Mt = host::mulmod(Mt, cand[u], q);
+                    Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (cand[u] % m) % m);
                 }
             uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);
             p.limbs[l].c[t] = host::mulmod(Mt, inv, q);
@@ -436,6 +444,9 @@ size_t ctpt_tc_ws_bytes(const Context &c, uint32_t n_in, uint32_t n_out, uint32_
            sizeof(CrtLimb) * 64;
 }
 
+// Chunks of 131,072 columns run one after the other on `st`.  (Alternating them over two
+// streams, so that one chunk's residue and CRT kernels could run beside the other's GEMM,
+// measured no faster: the GEMM's grid fills every SM.)
 void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
                     uint32_t L, void *ws, uint64_t max_abs_w, cudaStream_t st) {
     if (n_in == 0 || n_out == 0) return;
@@ -445,7 +456,7 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     if (R % chunk) throw std::invalid_argument("ct-pt matmul: column count not a multiple of the chunk");
     const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBM - 1) / kBM * kBM;
     Plan plan = make_plan(c, n_in, L, max_abs_w);
-    const uint32_t T = plan.mods.t;
+    const uint32_t T = plan.T;
     SHM_CUDA(cudaMemcpyToSymbolAsync(c_mods, &plan.mods, sizeof(ModTab), 0, cudaMemcpyHostToDevice, st));
     // workspace carve-up
     uint8_t *base = static_cast<uint8_t *>(ws);
@@ -459,13 +470,13 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     // zero-padded K tail of the X planes stays zero: clear once per call
     if (Kp != n_in) SHM_CUDA(cudaMemsetAsync(XP, 0, (size_t)T * chunk * Kp, st));
     SHM_LAUNCHED(1);
-    wres_kernel<<<dim3((Kp + 255) / 256, Np), 256, 0, st>>>(W, WP, n_in, n_out, Kp, Np);
+    wres_kernel<<<dim3((Kp + 255) / 256, Np), 256, 0, st>>>(W, WP, n_in, n_out, Kp, Np, T);
     SHM_CUDA(cudaGetLastError());
     SHM_CUDA(cudaFuncSetAttribute(mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
     const int acc24 = (uint64_t)Kp * 125 * 125 < (1ull << 24) ? 1 : 0;  // accumulators exact in float
     for (uint64_t r0 = 0; r0 < R; r0 += chunk) {
         SHM_LAUNCHED(1);
-        xres_kernel<<<dim3((uint32_t)(chunk / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0);
+        xres_kernel<<<dim3((uint32_t)(chunk / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0, T);
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
         mma_kernel<<<dim3(Np / kBM, (uint32_t)(chunk / kBN), T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
@@ -473,7 +484,7 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
         crt_kernel<<<dim3((uint32_t)((chunk / 4 + 255) / 256), n_out), 256, 0, st>>>(RES, Y, tab, n_out, chunk, r0, R,
-                                                                                    L, c.log_n, c.pc);
+                                                                                    L, c.log_n, c.pc, T);
         SHM_CUDA(cudaGetLastError());
     }
 }

@@ -40,3 +40,36 @@ def test_tc_matches_cuda_core_and_oracle(n_in, n_out, wbits):
     for k, c in enumerate(cols):
         assert np.array_equal(Y[c], ref[k])
     ctx.close()
+
+
+@pytest.mark.parametrize("L", [2, 3])
+def test_tc_over_several_column_chunks(L):
+    """N = 2^16: 2 L N columns are two or three chunks of 131,072 columns, each its own pass
+    of residues, GEMM and CRT (the weight planes and the CRT table shared)."""
+    import ctypes
+
+    import torch
+
+    from shmoai_b200._lib import check, lib
+    from shmoai_b200.ckks import CKKSContext, to_device, to_host
+
+    log_n, bits, np_ = O.PARAM_SETS["boot"]
+    primes = [int(p) for p in O.gen_primes(log_n, bits)]
+    ctx = CKKSContext(log_n, primes=primes, n_special=np_)
+    n, n_in, n_out = 1 << log_n, 24, 9
+    rng = np.random.default_rng(40 + L)
+    X = np.empty((n_in, 2, L, n), dtype=np.uint64)
+    for l in range(L):
+        X[:, :, l] = rng.integers(0, primes[l], size=(n_in, 2, n), dtype=np.uint64)
+    W = rng.integers(-(1 << 30), 1 << 30, size=(n_in, n_out), dtype=np.int64)
+    Xd, Wd = to_device(X), torch.from_numpy(W).cuda()
+    Y = to_host(ctx.ctpt_matmul(Xd, Wd))
+    Yc = torch.empty(n_out, 2, L, n, dtype=torch.int64, device="cuda")
+    check(lib().shm_ctpt_matmul_cuda_core(ctx._h, ctypes.c_void_p(Xd.data_ptr()), ctypes.c_void_p(Wd.data_ptr()),
+                                          ctypes.c_void_p(Yc.data_ptr()), n_in, n_out, L,
+                                          ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    assert np.array_equal(Y, to_host(Yc))
+    o = O.Oracle(log_n, primes, len(primes) - np_, np_)
+    ref = o.ctpt_matmul(X, np.ascontiguousarray(W[:, [0, n_out - 1]]))
+    assert np.array_equal(Y[0], ref[0]) and np.array_equal(Y[n_out - 1], ref[1])
+    ctx.close()
