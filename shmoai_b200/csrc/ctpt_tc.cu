@@ -89,7 +89,7 @@ __device__ __forceinline__ uint32_t mod_acc(int a, uint32_t t) {
 }
 
 // X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via a 64 x 64 shared-memory transpose
-__global__ void xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__ XP, uint32_t n_in, uint32_t Kp,
+__global__ void __launch_bounds__(256, 4) xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__ XP, uint32_t n_in, uint32_t Kp,
                             uint64_t R, uint64_t r0, uint32_t T) {
     __shared__ uint64_t tile[64][65];
     const uint32_t i0 = blockIdx.y * 64;
@@ -103,10 +103,8 @@ __global__ void xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__
     const uint64_t chunk = (uint64_t)gridDim.x * 64;
     for (uint32_t rr = ty; rr < 64; rr += 4) {
         uint64_t x = tile[tx][rr];
-#pragma unroll
-        for (uint32_t t = 0; t < kMaxMods; t++)
-            if (t < T)
-                XP[((uint64_t)t * chunk + rb + rr) * Kp + i0 + tx] = balanced(mod_small(x, t), c_mods.m[t]);
+        for (uint32_t t = 0; t < T; t++)
+            XP[((uint64_t)t * chunk + rb + rr) * Kp + i0 + tx] = balanced(mod_small(x, t), c_mods.m[t]);
     }
 }
 
