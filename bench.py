@@ -34,6 +34,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -699,6 +700,73 @@ def run_ctpt(args, rank, world, dist):
     return res
 
 
+GELU = dict(L=12, lo=-19.5, hi=12.5)  # input at 12 primes of the bootstrapping chain
+
+
+def run_gelu(args, rank, world, dist):
+    """The BERT layer's GELU stage: gelu_cheb's degree-24 Chebyshev series on [-19.5, 12.5]
+    (6 levels) over a batch of ciphertexts at 12 primes of the bootstrapping chain (N = 2^16,
+    scale 2^46), slot values uniform on the interval; step = one batch through the host API.
+    e2e adds the batch's upload from pinned host memory and the result's download."""
+    import torch
+
+    import shmoai_b200
+    from shmoai_b200.host import Host
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = shmoai_b200.lib()
+    h = Host(BOOT["log_n"], bits=BOOT["bits"], n_special=BOOT["n_special"], hamming_weight=BOOT["h"],
+             seed=0x5EED + rank, device=dev)
+    h.gen_relin_key()
+    B, L = args.batch, GELU["L"]
+    rng = np.random.default_rng(2000 + rank)
+    x = rng.uniform(GELU["lo"], GELU["hi"], (B, h.n // 2))
+    ct = h.encrypt(x, BOOT["scale"], L)
+    holder = {}
+
+    def step():
+        holder["out"] = h.gelu(ct)
+
+    clk = ClockSampler(dev).start()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    l0 = lib.shm_kernel_launches()
+    ms = timed_steps(torch, step, args.steps, dist, None)  # a batch at 12 primes is 805 MB > L2
+    launches = lib.shm_kernel_launches() - l0
+    out = holder["out"]
+    y = h.decrypt(out).real
+    gelu = 0.5 * x * (1.0 + np.vectorize(math.erf)(x / math.sqrt(2.0)))
+    err = np.abs(y - gelu)
+    # end to end: pinned host batch -> device, GELU, result -> pinned host memory
+    h_in = torch.from_numpy(ct.to_host().view(np.int64)).pin_memory()
+    h_out = torch.empty((out.count, out.size, out.level, h.n), dtype=torch.int64).pin_memory()
+
+    def e2e_step():
+        ct.write_from_ptr(h_in.data_ptr())
+        o = h.gelu(ct)
+        o.to_ptr(h_out.data_ptr())
+
+    e2e_ms = timed_steps(torch, e2e_step, args.steps, dist, None)
+    clocks = clk.summary()
+    return {
+        "metric": "GELU ciphertexts/s (gelu_cheb degree-24 series, N=2^16, input at 12 primes)",
+        "value": round(world * B * 1000.0 / ms, 2), "unit": "ciphertexts/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform slot values on [-19.5, 12.5])",
+        "config": {"workload": "gelu: the BERT layer's GELU stage on a batch per GPU per step", "batch_per_gpu": B,
+                   "N": h.n, "input_primes": L, "output_primes": out.level, "scale": BOOT["scale"],
+                   "err_vs_gelu_mean": float(err.mean()), "err_vs_gelu_max": float(err.max()),
+                   "reference_published": "GELU stage of one layer: 3072 ciphertexts in 30.2 s (101.7/s) on "
+                                          "RTX PRO 6000 (single_layer_results.csv)"},
+        "e2e": {"value": round(world * B * 1000.0 / e2e_ms, 2), "unit": "ciphertexts/s",
+                "h2d_bytes_per_step": int(h_in.numel() * 8), "d2h_bytes_per_step": int(h_out.numel() * 8)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+
+
 def run_kernel_case(args, rank, world, dist):
     """Profiling cases: 'ntt' = forward NTT of 4095 limbs (2 GB, > L2) at the bootstrap primes;
     'ks' = one hoisted-free rotation of 4 ciphertexts at 35 limbs (the C2S key switch)."""
@@ -749,7 +817,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks", "serve"])
+    ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks", "serve", "gelu"])
     ap.add_argument("--batch", type=int, default=None)
     ap.add_argument("--shared", type=int, default=8,
                     help="boot: shared-a group size n (0 = ordinary ciphertexts)")
@@ -764,7 +832,7 @@ def main():
     if args.small:
         CTPT.update(L=1)
     if args.batch is None:
-        args.batch = 32 if args.workload == "boot" else 1
+        args.batch = {"boot": 32, "gelu": 64}.get(args.workload, 1)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -805,7 +873,7 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
     runner = {"boot": run_boot, "prim": run_prim, "ctpt": run_ctpt, "serve": run_serve, "ntt": run_kernel_case,
-              "ks": run_kernel_case}[args.workload]
+              "ks": run_kernel_case, "gelu": run_gelu}[args.workload]
     res = runner(args, rank, world, dist)
     if rank == 0:
         if not args.no_cpu_baseline and args.workload in ("boot", "prim"):

@@ -317,6 +317,24 @@ class Evaluator {
     mutable Plaintext mono_;
 };
 
+// ---- polynomial operators on ciphertext batches (chebyshev.cpp): the BERT layer's
+// non-linear functions as Chebyshev series (src/include/source/non_linear_func/)
+
+// coefficients c_0 .. c_deg of the interpolant of f at the deg + 1 Chebyshev nodes of [lo, hi]
+std::vector<double> chebyshev_interpolant(const std::function<double(double)> &f, double lo, double hi, int deg);
+// sum_k c_k T_k(u), u = (2 x - hi - lo) / (hi - lo), at x's scale; one level for u, then the
+// basis and the baby-step giant-step tree (degree 24: 6 levels in all); approximates only on
+// [lo, hi]
+Ciphertext evaluate_chebyshev(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &c, double lo,
+                              double hi);
+double gelu_exact(double x);  // x Phi(x) = x (1 + erf(x / sqrt 2)) / 2
+// gelu_cheb's degree-24 near-minimax series on [-19.5, 12.5] (gelu_other.cuh:258-300), and
+// GELU by it: 6 levels (gelu_cheb takes 7); inputs outside the interval are not approximated.  The scales stay
+// near the primes when the levels it uses have primes of about the input scale's size
+// (the chain's 46-bit primes at scale 2^46).
+const std::vector<double> &gelu_series();
+Ciphertext gelu(const Evaluator &ev, const Ciphertext &x);
+
 struct BootstrapParams {
     double scale = 70368744177664.0;  // 2^46
     uint32_t input_level = 4;         // primes of the input (S2C-first)

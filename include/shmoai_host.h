@@ -92,6 +92,14 @@ int shm_host_multiply_i(shm_host *h, const shm_ct *a, int sign, shm_ct **out);
  * (|W| < 2^40) at w_scale; tensor_cores = 0 runs the CUDA-core kernel (the plain path) */
 int shm_host_ctpt_matmul(shm_host *h, const shm_ct *X, const int64_t *W, uint32_t n_out, double w_scale,
                          int tensor_cores, shm_ct **out);
+/* Polynomial operators (the BERT layer's non-linear functions, src/include/source/non_linear_func/):
+ * sum_k coeffs[k] T_k(u), u = (2 x - hi - lo) / (hi - lo), on every slot of an ordinary batch,
+ * output at the input's scale; and GELU by gelu_cheb's degree-24 series on [-19.5, 12.5]
+ * (non_linear_func/gelu_other.cuh:258-300).  They consume 1 + depth(series) levels (degree 24:
+ * 6, where gelu_cheb takes 7); SHM_EINVAL when the input has too few. */
+int shm_host_chebyshev(shm_host *h, const shm_ct *a, const double *coeffs, uint32_t n_coeffs, double lo, double hi,
+                       shm_ct **out);
+int shm_host_gelu(shm_host *h, const shm_ct *a, shm_ct **out);
 int shm_host_to_shared(shm_host *h, const shm_ct *a, uint32_t members, shm_ct **out);
 int shm_host_from_shared(shm_host *h, const shm_ct *a, shm_ct **out);
 

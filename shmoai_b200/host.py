@@ -96,6 +96,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_import_secret_text": (i32, [_P, ctypes.c_char_p]),
         "shm_host_export_secret_text": (i32, [_P, ctypes.c_char_p]),
         "shm_host_import_key": (i32, [_P, i32, _U32, u64p, ctypes.c_size_t]),
+        "shm_host_chebyshev": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp]),
+        "shm_host_gelu": (i32, [_P, _P, pp]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
         "shm_server_submit_rotate": (i32, [_P, _P, i32, ctypes.POINTER(ctypes.c_uint64)]),
@@ -283,6 +285,16 @@ class Host:
         W = np.ascontiguousarray(W, dtype=np.int64)
         return self._out(self.lib.shm_host_ctpt_matmul, X._c, W.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
                          W.shape[1], w_scale, 1 if tensor_cores else 0)
+
+    def chebyshev(self, a, coeffs, lo: float, hi: float):
+        """sum_k coeffs[k] T_k(u), u = (2 x - hi - lo) / (hi - lo), slot-wise, at the input's scale."""
+        c = np.ascontiguousarray(coeffs, dtype=np.float64)
+        return self._out(self.lib.shm_host_chebyshev, a._c, c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(c),
+                         lo, hi)
+
+    def gelu(self, a):
+        """GELU by the reference's degree-24 Chebyshev series on [-19.5, 12.5] (6 levels)."""
+        return self._out(self.lib.shm_host_gelu, a._c)
 
     def to_shared(self, a, members: int):
         return self._out(self.lib.shm_host_to_shared, a._c, members)

@@ -210,16 +210,6 @@ std::vector<double> cheb_interp(double (*f)(double, int), int r, double K, int d
 
 double evalmod_target(double t, int r) { return std::cos(2.0 * M_PI * (t - 0.25) / std::ldexp(1.0, r)); }
 
-// p = q T_m + r for Chebyshev coefficients c (degree < 2m)
-void cheb_divide(const std::vector<double> &c, int m, std::vector<double> &q, std::vector<double> &r) {
-    const int d = (int)c.size() - 1;
-    q.assign(1, c[m]);
-    for (int j = 1; j <= d - m; j++) q.push_back(2.0 * c[m + j]);
-    r.assign(c.begin(), c.begin() + m);
-    for (int j = 1; j <= d - m; j++) r[m - j] -= c[m + j];
-}
-
-int bitlen(uint32_t d) { return d ? 32 - __builtin_clz(d) : 0; }
 
 int64_t floordiv(int64_t a, int64_t b) {
     int64_t q = a / b;
@@ -485,82 +475,6 @@ SharedAKeys BatchBootstrapper::prepare_shared_keys(KeyGenerator &kg, uint32_t me
     return kg.shared_keys(members, galois_elts(), hw);
 }
 
-namespace {
-
-using Basis = std::map<int, Ciphertext>;
-
-// T_1 .. T_8 and T_16, T_32, ... by products 2 T_a T_b - T_{a-b}; each product is
-// relinearised and rescaled in one ModDown by q_{L-1} P
-Basis cheb_basis(const Evaluator &ev, const Ciphertext &x, int deg) {
-    Basis T;
-    T.emplace(1, ev.adjust(x, x.L, x.scale_));
-    auto prod = [&](int a, int b) {
-        Ciphertext p = ev.multiply_int(ev.relinearize_rescale(ev.multiply_lazy(T.at(a), T.at(b))), 2);
-        if (a == b) return ev.add_const(p, -1.0);
-        return ev.sub(p, ev.adjust(T.at(a - b), p.L, p.scale_));
-    };
-    const int g = 8;
-    for (int k = 2; k <= g && k <= deg; k++) {
-        if (k % 2 == 0) {
-            T.emplace(k, prod(k / 2, k / 2));
-        } else {
-            const int a = 1 << (bitlen((uint32_t)k) - 1);
-            T.emplace(k, prod(a, k - a));
-        }
-    }
-    for (int m = 2 * g; m <= deg; m *= 2) T.emplace(m, prod(m / 2, m / 2));
-    return T;
-}
-
-bool feasible(const Basis &T, int ncoef, uint32_t lvl) {
-    const int d = ncoef - 1;
-    if (d < 8) {
-        for (int i = 1; i <= d; i++)
-            if (T.at(i).L < lvl + 1) return false;
-        return true;
-    }
-    const int m = 1 << (bitlen((uint32_t)d) - 1);
-    return T.at(m).L >= lvl + 1 && feasible(T, d - m + 1, lvl + 1) && feasible(T, m, lvl);
-}
-
-// sum_i c_i T_i, output at exactly scale S and lvl primes (baby-step giant-step).  A
-// giant-step product is only added to, so it stays unrelinearised (size 3) through its
-// rescale and the sum; the sum is relinearised once, where it is needed as a multiplicand
-// or at the top (lazy = false), instead of every product on its own: two relinearisations
-// fewer at degree 47.
-Ciphertext cheb_eval(const Evaluator &ev, const Basis &T, const std::vector<double> &c, double S, uint32_t lvl,
-                     bool lazy = false) {
-    const Context &ctx = ev.context();
-    const int d = (int)c.size() - 1;
-    if (d < 1) throw Error("Chebyshev piece of degree 0");
-    if (d < 8) {
-        // c_0 + sum_i c_i T_i with each term at scale S q: weight round(c_i S q / scale(T_i)),
-        // one linear-combination pass (T_i read at their first lvl + 1 limbs), then the rescale
-        const double q = (double)ctx.primes[lvl];
-        std::vector<const Ciphertext *> X;
-        std::vector<double> w;
-        for (int i = 1; i <= d; i++) {
-            X.push_back(&T.at(i));
-            w.push_back(std::nearbyint(c[i] * (S * q / T.at(i).scale_)));
-        }
-        Ciphertext acc = ev.linear_combination(X, w, std::nearbyint(c[0] * (S * q)), lvl + 1, S * q);
-        Ciphertext out = ev.rescale_to_next(acc);
-        out.scale_ = S;
-        return out;
-    }
-    const int m = 1 << (bitlen((uint32_t)d) - 1);
-    std::vector<double> qc, rc;
-    cheb_divide(c, m, qc, rc);
-    Ciphertext Tm = ev.mod_switch_to(T.at(m), lvl + 1);
-    const double Sq = S * (double)ctx.primes[lvl] / Tm.scale_;
-    Ciphertext qct = cheb_eval(ev, T, qc, Sq, lvl + 1);  // a multiplicand: relinearised
-    Ciphertext prod = ev.rescale_to_next(ev.multiply_lazy(qct, Tm));
-    prod.scale_ = S;
-    Ciphertext sum = ev.add(prod, cheb_eval(ev, T, rc, S, lvl, true));
-    return lazy ? std::move(sum) : ev.relinearize(sum);
-}
-
-}  // namespace
 
 // x holds t / K; returns c_fin * sin(2 pi t) read at scale Delta.  Backward scale
 // targets: the i-th double angle squares at level lvl - i and drops prime lvl - 1 - i,
@@ -570,15 +484,15 @@ Ciphertext BatchBootstrapper::evalmod(const Ciphertext &x, const Evaluator *evp)
     const Evaluator &ev = evp ? *evp : ev_;
     const Context &c = ev.context();
     const int deg = (int)cheb_.size() - 1;
-    Basis T = cheb_basis(ev, x, deg);
+    detail::ChebBasis T = detail::cheb_basis(ev, x, deg);
     uint32_t lvl = x.L - 1;
-    while (!feasible(T, deg + 1, lvl)) {
+    while (!detail::cheb_feasible(T, deg + 1, lvl)) {
         if (lvl == 0) throw Error("not enough levels for EvalMod");
         lvl--;
     }
     double s = p_.scale * c_fin_;
     for (int i = p_.double_angles - 1; i >= 0; i--) s = std::sqrt(s * (double)c.primes[lvl - 1 - i]);
-    Ciphertext y = cheb_eval(ev, T, cheb_, s, lvl);
+    Ciphertext y = detail::cheb_eval(ev, T, cheb_, s, lvl);
     for (int i = 0; i < p_.double_angles; i++) {  // y = 2 y^2 - 1, the affine part in one pass
         const Ciphertext sq = ev.relinearize_rescale(ev.multiply_lazy(y, y));
         y = ev.linear_combination({&sq}, {2.0}, std::nearbyint(-1.0 * sq.scale_), sq.L, sq.scale_);

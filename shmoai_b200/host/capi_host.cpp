@@ -238,6 +238,19 @@ int shm_ct_to_host(shm_host *h, const shm_ct *ct, uint64_t *data) {
     });
 }
 
+int shm_host_chebyshev(shm_host *h, const shm_ct *a, const double *coeffs, uint32_t n_coeffs, double lo, double hi,
+                       shm_ct **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!coeffs) throw Error("null coefficients");
+        put(out, evaluate_chebyshev(*hh.ev, C(a), std::vector<double>(coeffs, coeffs + n_coeffs), lo, hi));
+    });
+}
+
+int shm_host_gelu(shm_host *h, const shm_ct *a, shm_ct **out) {
+    return guard([&] { put(out, gelu(*H(h).ev, C(a))); });
+}
+
 int shm_ct_serialized_bytes(shm_host *h, const shm_ct *ct, size_t *bytes) {
     return guard([&] {
         if (!bytes) throw Error("null argument");

@@ -35,5 +35,16 @@ inline uint64_t mix64(uint64_t seed, uint64_t idx) {
     return z ^ (z >> 31);
 }
 
+// Chebyshev series on ciphertexts (chebyshev.cpp): the basis T_1 .. T_8, T_16, T_32, .. up
+// to `deg`, whether a series of ncoef coefficients fits from level lvl, and its baby-step
+// giant-step evaluation at scale S and lvl primes
+using ChebBasis = std::map<int, Ciphertext>;
+void cheb_divide(const std::vector<double> &c, int m, std::vector<double> &q, std::vector<double> &r);
+int bitlen(uint32_t d);
+ChebBasis cheb_basis(const Evaluator &ev, const Ciphertext &x, int deg);
+bool cheb_feasible(const ChebBasis &T, int ncoef, uint32_t lvl);
+Ciphertext cheb_eval(const Evaluator &ev, const ChebBasis &T, const std::vector<double> &c, double S, uint32_t lvl,
+                     bool lazy = false);
+
 }  // namespace detail
 }  // namespace shmoai

@@ -1,0 +1,117 @@
+"""Polynomial operators of the BERT layer on ciphertext batches (shm_host_chebyshev,
+shm_host_gelu; the reference's non_linear_func/, gelu_cheb at gelu_other.cuh:258-300).
+
+CPU: the host library on the oracle's C ABI at N = 2^12.  A Chebyshev series evaluated on
+ciphertexts decrypts to numpy's evaluation of the same series (CKKS noise only); GELU
+decrypts to the reference's degree-24 series and, through it, to GELU within the series'
+fit error on [-19.5, 12.5] (0.037 in the reference's own comment; checked here against
+x Phi(x)); bad inputs are refused.  GPU: the CUDA build gives the oracle build's results
+bit for bit, and GELU at N = 2^16 on the bootstrapping chain has the same accuracy.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from shmoai_b200.host import Host, HostError
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_HOST = os.path.join(ROOT, "oracle", "_build", "libshmoai_host_oracle.so")
+SMALL_BITS = [51] + [46] * 8 + [51] * 11 + [51] * 5  # N = 2^12, nq = 20, np = 5
+REF_BITS = [51] + [46] * 20 + [51] * 14 + [51] * 5
+DELTA = 2.0 ** 46
+# gelu_cheb's series in u = (x + 3.5) / 16 (gelu_other.cuh:284-296), as the operator uses it
+GELU_D = [3.4550752799e+00, 5.7852067632e+00, 3.1727714170e+00, 7.0234932500e-01, -4.6200569546e-01,
+          -3.7817535966e-01, 8.4136420694e-02, 2.2427456987e-01, 2.9451916291e-02, -1.2928072669e-01,
+          -6.6659430283e-02, 6.4349502364e-02, 7.1733295078e-02, -1.9882581810e-02, -6.1145844240e-02,
+          -8.4827295421e-03, 4.3597254356e-02, 2.3373027950e-02, -2.4790187963e-02, -2.7940100474e-02,
+          8.8404026343e-03, 2.3776567058e-02, 8.8171887083e-03, -4.6290425955e-02, -9.7997267900e-03]
+
+
+def _gelu(x):
+    return 0.5 * x * (1.0 + np.vectorize(math.erf)(x / math.sqrt(2.0)))
+
+
+def _host(lib=ORACLE_HOST, seed=11, log_n=12, bits=SMALL_BITS, hw=64):
+    h = Host(log_n, O.gen_primes(log_n, bits), 5, hamming_weight=hw, seed=seed, lib=lib)
+    h.gen_relin_key()
+    return h
+
+
+@pytest.fixture(scope="module")
+def small():
+    return _host()
+
+
+@pytest.mark.parametrize("deg,L", [(5, 6), (12, 7), (24, 9)])
+def test_chebyshev_series_matches_numpy(small, deg, L):
+    h = small
+    rng = np.random.default_rng(deg)
+    lo, hi = -3.0, 5.0
+    c = rng.uniform(-1, 1, deg + 1) / (1 + np.arange(deg + 1))
+    x = rng.uniform(lo, hi, (2, h.n // 2))
+    out = h.chebyshev(h.encrypt(x, DELTA, L), c, lo, hi)
+    want = np.polynomial.chebyshev.chebval((2 * x - hi - lo) / (hi - lo), c)
+    assert out.scale == DELTA and out.level < L
+    assert np.abs(h.decrypt(out).real - want).max() < 1e-5
+
+
+def test_gelu_is_the_reference_series(small):
+    h = small
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-19.5, 12.5, (2, h.n // 2))
+    x[0, :4] = [-19.5, 12.5, 0.0, -3.5]
+    out = h.gelu(h.encrypt(x, DELTA, 9))
+    y = h.decrypt(out).real
+    series = np.polynomial.chebyshev.chebval((x + 3.5) / 16.0, GELU_D)
+    assert out.level == 9 - 6 and out.scale == DELTA  # one level fewer than gelu_cheb's 7
+    assert np.abs(y - series).max() < 1e-5
+    assert np.abs(y - _gelu(x)).max() < 0.04
+
+
+def test_polynomial_operators_refuse_bad_inputs(small):
+    h = small
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-1, 1, (2, 16))
+    with pytest.raises(HostError, match="not enough levels"):
+        h.gelu(h.encrypt(x, DELTA, 6))
+    with pytest.raises(HostError, match="not enough levels"):
+        h.chebyshev(h.encrypt(x, DELTA, 4), np.ones(6), -1.0, 1.0)
+    with pytest.raises(HostError, match="lo < hi"):
+        h.chebyshev(h.encrypt(x, DELTA, 6), [0.5, 1.0], 1.0, 1.0)
+    with pytest.raises(HostError, match="degree 0"):
+        h.chebyshev(h.encrypt(x, DELTA, 6), [0.5], -1.0, 1.0)
+
+
+@pytest.mark.gpu
+def test_cuda_polynomial_operators_match_oracle_build():
+    import shmoai_b200.host as H
+
+    g, c = _host(lib=H.PRODUCT_LIB, seed=21), _host(seed=21)
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-19.5, 12.5, (3, g.n // 2))
+    for h_cu, h_or in ((g, c),):
+        a, b = h_cu.encrypt(x, DELTA, 9), h_or.encrypt(x, DELTA, 9)
+        assert np.array_equal(a.to_host(), b.to_host())
+        assert np.array_equal(h_cu.gelu(a).to_host(), h_or.gelu(b).to_host())
+        coeffs = rng.uniform(-1, 1, 13)
+        assert np.array_equal(h_cu.chebyshev(a, coeffs, -20.0, 13.0).to_host(),
+                              h_or.chebyshev(b, coeffs, -20.0, 13.0).to_host())
+
+
+@pytest.mark.gpu
+def test_gelu_reference_parameters_on_b200():
+    """N = 2^16, the bootstrapping chain, scale 2^46, input at 12 primes, 4 full ciphertexts."""
+    import shmoai_b200.host as H
+
+    h = _host(lib=H.PRODUCT_LIB, seed=7, log_n=16, bits=REF_BITS, hw=192)
+    rng = np.random.default_rng(6)
+    x = rng.uniform(-19.5, 12.5, (4, h.n // 2))
+    out = h.gelu(h.encrypt(x, DELTA, 12))
+    y = h.decrypt(out).real
+    series = np.polynomial.chebyshev.chebval((x + 3.5) / 16.0, GELU_D)
+    assert out.level == 6
+    assert np.abs(y - series).max() < 1e-5
+    assert np.abs(y - _gelu(x)).max() < 0.04
