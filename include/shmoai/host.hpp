@@ -378,6 +378,11 @@ class Graph {
 
 // One autotuning decision: the candidates, their milliseconds (measured for the kernel
 // tiles, modelled from measured rotation costs for the BSGS splits) and the pick.
+// A CUDA graph of evaluate_chebyshev(ev, in, c, lo, hi) and the output batch every launch
+// rewrites (write the next input into `in` between launches; `in` must outlive the graph).
+std::unique_ptr<Graph> capture_chebyshev(const Evaluator &ev, const Ciphertext &in, const std::vector<double> &c,
+                                         double lo, double hi, Ciphertext &out);
+
 struct TuneRecord {
     std::string knob;
     std::vector<std::string> candidates;

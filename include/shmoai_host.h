@@ -28,6 +28,7 @@ extern "C" {
 typedef struct shm_host shm_host;
 typedef struct shm_ct shm_ct;
 typedef struct shm_boot shm_boot;
+typedef struct shm_host_graph shm_host_graph;
 
 const char *shm_host_last_error(void);
 
@@ -100,6 +101,10 @@ int shm_host_ctpt_matmul(shm_host *h, const shm_ct *X, const int64_t *W, uint32_
 int shm_host_chebyshev(shm_host *h, const shm_ct *a, const double *coeffs, uint32_t n_coeffs, double lo, double hi,
                        shm_ct **out);
 int shm_host_gelu(shm_host *h, const shm_ct *a, shm_ct **out);
+/* a CUDA graph of shm_host_chebyshev (coeffs = NULL: GELU) on `in`; *out is rewritten by every
+ * shm_host_graph_launch; write the next batch into `in` with shm_ct_write between launches */
+int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,
+                               double hi, shm_ct **out, shm_host_graph **graph);
 int shm_host_to_shared(shm_host *h, const shm_ct *a, uint32_t members, shm_ct **out);
 int shm_host_from_shared(shm_host *h, const shm_ct *a, shm_ct **out);
 
@@ -129,7 +134,6 @@ int shm_boot_set_split(shm_boot *b, const int *g1);
  * recorded; *out receives the output ciphertext, which every shm_host_graph_launch
  * rewrites.  Put the next batch into `in` with shm_ct_write between launches; `in` must
  * outlive the graph. */
-typedef struct shm_host_graph shm_host_graph;
 int shm_boot_capture(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out, shm_host_graph **graph);
 /* replay on the host's stream */
 int shm_host_graph_launch(shm_host_graph *g);

@@ -98,6 +98,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_import_key": (i32, [_P, i32, _U32, u64p, ctypes.c_size_t]),
         "shm_host_chebyshev": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp]),
         "shm_host_gelu": (i32, [_P, _P, pp]),
+        "shm_host_chebyshev_capture": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp, pp]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
         "shm_server_submit_rotate": (i32, [_P, _P, i32, ctypes.POINTER(ctypes.c_uint64)]),
@@ -295,6 +296,19 @@ class Host:
     def gelu(self, a):
         """GELU by the reference's degree-24 Chebyshev series on [-19.5, 12.5] (6 levels)."""
         return self._out(self.lib.shm_host_gelu, a._c)
+
+    def capture_chebyshev(self, ct, coeffs=None, lo: float = 0.0, hi: float = 0.0):
+        """A CUDA graph of chebyshev(ct, coeffs, lo, hi) (GELU when coeffs is None) and the output
+        batch every launch rewrites; write the next input into `ct` between launches."""
+        o, g = _P(), _P()
+        if coeffs is None:
+            cp, n = None, 0
+        else:
+            c = np.ascontiguousarray(coeffs, dtype=np.float64)
+            cp, n = c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(c)
+        self._check(self.lib.shm_host_chebyshev_capture(self._h, ct._c, cp, n, lo, hi, ctypes.byref(o),
+                                                        ctypes.byref(g)))
+        return Graph(self, g, keep=ct), Ct(self, o)
 
     def to_shared(self, a, members: int):
         return self._out(self.lib.shm_host_to_shared, a._c, members)

@@ -251,6 +251,23 @@ int shm_host_gelu(shm_host *h, const shm_ct *a, shm_ct **out) {
     return guard([&] { put(out, gelu(*H(h).ev, C(a))); });
 }
 
+int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,
+                               double hi, shm_ct **out, shm_host_graph **graph) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!graph || !out) throw Error("null output handle");
+        std::vector<double> c = coeffs ? std::vector<double>(coeffs, coeffs + n_coeffs) : gelu_series();
+        if (!coeffs) {
+            lo = -19.5;
+            hi = 12.5;
+        }
+        Ciphertext o;
+        std::unique_ptr<Graph> g = capture_chebyshev(*hh.ev, C(in), c, lo, hi, o);
+        *graph = new shm_host_graph{std::move(g)};
+        put(out, std::move(o));
+    });
+}
+
 int shm_ct_serialized_bytes(shm_host *h, const shm_ct *ct, size_t *bytes) {
     return guard([&] {
         if (!bytes) throw Error("null argument");

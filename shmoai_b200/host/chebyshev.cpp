@@ -155,3 +155,28 @@ const std::vector<double> &gelu_series() {
 Ciphertext gelu(const Evaluator &ev, const Ciphertext &x) { return evaluate_chebyshev(ev, x, gelu_series(), -19.5, 12.5); }
 
 }  // namespace shmoai
+
+namespace shmoai {
+
+std::unique_ptr<Graph> capture_chebyshev(const Evaluator &ev, const Ciphertext &in, const std::vector<double> &c,
+                                         double lo, double hi, Ciphertext &out) {
+    // the output's shape from one run on the base evaluator; the buffer belongs to the base context
+    Ciphertext shape = evaluate_chebyshev(ev, in, c, lo, hi);
+    const Context &ctx = ev.context();
+    out.data = DeviceBuffer(ctx, shape.data.words());
+    out.count = shape.count;
+    out.size = shape.size;
+    out.L = shape.L;
+    out.scale_ = shape.scale_;
+    out.shared = shape.shared;
+    ctx.synchronize();
+    uint64_t *dst = out.data.data();
+    const size_t bytes = shape.data.words() * 8;
+    return std::unique_ptr<Graph>(new Graph(ev, [&in, c, lo, hi, dst, bytes](const Evaluator &e) {
+        Ciphertext r = evaluate_chebyshev(e, in, c, lo, hi);
+        const Context &v = e.context();
+        v.check(shm_memcpy(v.handle(), dst, r.data.data(), bytes, SHM_COPY_D2D, v.stream()));
+    }));
+}
+
+}  // namespace shmoai

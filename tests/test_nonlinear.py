@@ -115,3 +115,27 @@ def test_gelu_reference_parameters_on_b200():
     assert out.level == 6
     assert np.abs(y - series).max() < 1e-5
     assert np.abs(y - _gelu(x)).max() < 0.04
+
+
+@pytest.mark.gpu
+def test_gelu_graph_replay_equals_eager():
+    """shm_host_chebyshev_capture: one CUDA graph of the GELU; a launch after writing the next
+    batch into the captured input gives that batch's eager result bit for bit."""
+    import shmoai_b200.host as H
+
+    h = _host(lib=H.PRODUCT_LIB, seed=31)
+    rng = np.random.default_rng(7)
+    x1, x2 = (rng.uniform(-19.5, 12.5, (2, h.n // 2)) for _ in range(2))
+    a = h.encrypt(x1, DELTA, 9)
+    nxt = h.encrypt(x2, DELTA, 9).to_host()
+    graph, out = h.capture_chebyshev(a)
+    assert graph.kernels > 0
+    graph.launch()
+    assert np.array_equal(out.to_host(), h.gelu(a).to_host())
+    a.write_from_ptr(nxt.ctypes.data)
+    graph.launch()
+    assert np.array_equal(out.to_host(), h.gelu(a).to_host())
+    coeffs = rng.uniform(-1, 1, 9)
+    g2, o2 = h.capture_chebyshev(a, coeffs, -20.0, 13.0)
+    g2.launch()
+    assert np.array_equal(o2.to_host(), h.chebyshev(a, coeffs, -20.0, 13.0).to_host())
