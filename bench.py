@@ -53,6 +53,7 @@ BOOT = dict(log_n=16, bits=[51] + [46] * 20 + [51] * 14 + [51] * 5, n_special=5,
 # key switches of one bootstrap (counted from the pipeline: rotations in the six linear
 # transforms + the conjugation, relinearisations of EvalMod on the re and im halves)
 BOOT_METRIC = "bootstraps/s (S2C-first, N=2^16, 35+5 primes, dnum 7, h=192, 2^15 slots, mean err <= 2e-5)"
+GELU_METRIC = "GELU ciphertexts/s (gelu_cheb degree-24 series, N=2^16, input at 12 primes)"
 PRIM_METRIC = "config-1 primitive chains/s (NTT inv+fwd, HRotate, mult+relin+rescale; N=2^16, L=24, dnum=3)"
 
 
@@ -642,6 +643,28 @@ def cpu_prim_chain():
     return 1.0 / (time.perf_counter() - t0), os.cpu_count()
 
 
+_GELU_CPU = {}
+
+
+def cpu_gelu_sample():
+    """GELU of one ciphertext at 12 primes (N = 2^16, the bootstrapping chain) through the host
+    library built on the CPU oracle (OpenMP over limbs); keys made once per process."""
+    from oracle import oracle as O
+    from shmoai_b200.host import Host
+
+    if "h" not in _GELU_CPU:
+        lib = os.path.join(ROOT, "oracle", "_build", "libshmoai_host_oracle.so")
+        h = Host(BOOT["log_n"], O.gen_primes(BOOT["log_n"], BOOT["bits"]), BOOT["n_special"],
+                 hamming_weight=BOOT["h"], seed=0x5EED, lib=lib)
+        h.gen_relin_key()
+        x = np.random.default_rng(2000).uniform(GELU["lo"], GELU["hi"], (1, h.n // 2))
+        _GELU_CPU.update(h=h, ct=h.encrypt(x, BOOT["scale"], GELU["L"]))
+    h, ct = _GELU_CPU["h"], _GELU_CPU["ct"]
+    t0 = time.perf_counter()
+    h.gelu(ct)
+    return 1.0 / (time.perf_counter() - t0), os.cpu_count()
+
+
 # ---------------------------------------------------------------------------
 # kernel workloads (config 2 and the profiling cases)
 
@@ -761,7 +784,7 @@ def run_gelu(args, rank, world, dist):
     e2e_ms = timed_steps(torch, e2e_step, args.steps, dist, None)
     clocks = clk.summary()
     return {
-        "metric": "GELU ciphertexts/s (gelu_cheb degree-24 series, N=2^16, input at 12 primes)",
+        "metric": GELU_METRIC,
         "value": round(world * B * 1000.0 / ms, 2), "unit": "ciphertexts/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform slot values on [-19.5, 12.5])",
@@ -852,19 +875,27 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        if args.workload not in ("boot", "prim", "gelu"):
+            print(json.dumps({"impl": "reference", "unavailable": "no CPU arm for the kernel workload "
+                              + args.workload + " (timed on the GPU only)"}))
+            return
         vals = []
         for i in range(args.warmup + args.steps):
             if args.workload == "boot":
                 v, cores, sample = cpu_boot_estimate(args.shared)
+            elif args.workload == "gelu":
+                v, cores = cpu_gelu_sample()
+                sample = "GELU of one ciphertext at 12 primes per step (host library on the oracle)"
             else:
                 v, cores = cpu_prim_chain()
                 sample = "one full config-1 chain per step"
             if i >= args.warmup:
                 vals.append(v)
         value = statistics.mean(vals)
-        unit = "bootstraps/s" if args.workload == "boot" else "chains/s"
+        unit = {"boot": "bootstraps/s", "gelu": "ciphertexts/s"}.get(args.workload, "chains/s")
+        metric = {"boot": BOOT_METRIC, "gelu": GELU_METRIC}.get(args.workload, PRIM_METRIC)
         print(json.dumps({
-            "impl": "reference", "metric": BOOT_METRIC if args.workload == "boot" else PRIM_METRIC,
+            "impl": "reference", "metric": metric,
             "value": round(value, 6), "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1000.0 / value, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
@@ -888,8 +919,12 @@ def main():
               "ks": run_kernel_case, "gelu": run_gelu}[args.workload]
     res = runner(args, rank, world, dist)
     if rank == 0:
-        if not args.no_cpu_baseline and args.workload in ("boot", "prim"):
-            if args.workload == "boot":
+        if not args.no_cpu_baseline and args.workload in ("boot", "prim", "gelu"):
+            if args.workload == "gelu":
+                v, cores = cpu_gelu_sample()
+                res["cpu_baseline"] = {"value": round(v, 4), "unit": "ciphertexts/s", "cores": cores, "kind": "port",
+                                       "sample": "GELU of one ciphertext at 12 primes (host library on the oracle)"}
+            elif args.workload == "boot":
                 v, cores, sample = cpu_boot_estimate(args.shared)
                 res["cpu_baseline"] = {"value": round(v, 6), "unit": "bootstraps/s", "cores": cores,
                                        "kind": "port", "sample": sample}
