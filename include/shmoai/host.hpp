@@ -378,6 +378,11 @@ class Graph {
 
 // One autotuning decision: the candidates, their milliseconds (measured for the kernel
 // tiles, modelled from measured rotation costs for the BSGS splits) and the pick.
+// the softmax's building blocks (softmax.cuh:23-118): exp(x) by (1 + x/128)^128 (8 levels) and
+// 1/x for x in (0, 2) by prod_{i <= iter} (1 + (1 - x)^(2^i)) (iter + 1 levels)
+Ciphertext exp_approx(const Evaluator &ev, const Ciphertext &x);
+Ciphertext inverse_approx(const Evaluator &ev, const Ciphertext &x, int iter);
+
 // A CUDA graph of evaluate_chebyshev(ev, in, c, lo, hi) and the output batch every launch
 // rewrites (write the next input into `in` between launches; `in` must outlive the graph).
 std::unique_ptr<Graph> capture_chebyshev(const Evaluator &ev, const Ciphertext &in, const std::vector<double> &c,

@@ -101,6 +101,10 @@ int shm_host_ctpt_matmul(shm_host *h, const shm_ct *X, const int64_t *W, uint32_
 int shm_host_chebyshev(shm_host *h, const shm_ct *a, const double *coeffs, uint32_t n_coeffs, double lo, double hi,
                        shm_ct **out);
 int shm_host_gelu(shm_host *h, const shm_ct *a, shm_ct **out);
+/* the softmax's building blocks (non_linear_func/softmax.cuh:23-118): exp(x) as (1 + x/128)^128
+ * (8 levels), and 1/x for x in (0, 2) as prod_{i <= iter} (1 + (1 - x)^(2^i)) (iter + 1 levels) */
+int shm_host_exp(shm_host *h, const shm_ct *a, shm_ct **out);
+int shm_host_inverse(shm_host *h, const shm_ct *a, uint32_t iter, shm_ct **out);
 /* a CUDA graph of shm_host_chebyshev (coeffs = NULL: GELU) on `in`; *out is rewritten by every
  * shm_host_graph_launch; write the next batch into `in` with shm_ct_write between launches */
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,

@@ -98,6 +98,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_import_key": (i32, [_P, i32, _U32, u64p, ctypes.c_size_t]),
         "shm_host_chebyshev": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp]),
         "shm_host_gelu": (i32, [_P, _P, pp]),
+        "shm_host_exp": (i32, [_P, _P, pp]),
+        "shm_host_inverse": (i32, [_P, _P, _U32, pp]),
         "shm_host_chebyshev_capture": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp, pp]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
@@ -296,6 +298,14 @@ class Host:
     def gelu(self, a):
         """GELU by the reference's degree-24 Chebyshev series on [-19.5, 12.5] (6 levels)."""
         return self._out(self.lib.shm_host_gelu, a._c)
+
+    def exp(self, a):
+        """exp(x) as (1 + x/128)^128 (the softmax's exp, 8 levels)."""
+        return self._out(self.lib.shm_host_exp, a._c)
+
+    def inverse(self, a, iter: int):
+        """1/x for x in (0, 2) as prod_{i <= iter} (1 + (1 - x)^(2^i)) (iter + 1 levels)."""
+        return self._out(self.lib.shm_host_inverse, a._c, iter)
 
     def capture_chebyshev(self, ct, coeffs=None, lo: float = 0.0, hi: float = 0.0):
         """A CUDA graph of chebyshev(ct, coeffs, lo, hi) (GELU when coeffs is None) and the output

@@ -251,6 +251,14 @@ int shm_host_gelu(shm_host *h, const shm_ct *a, shm_ct **out) {
     return guard([&] { put(out, gelu(*H(h).ev, C(a))); });
 }
 
+int shm_host_exp(shm_host *h, const shm_ct *a, shm_ct **out) {
+    return guard([&] { put(out, exp_approx(*H(h).ev, C(a))); });
+}
+
+int shm_host_inverse(shm_host *h, const shm_ct *a, uint32_t iter, shm_ct **out) {
+    return guard([&] { put(out, inverse_approx(*H(h).ev, C(a), (int)iter)); });
+}
+
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,
                                double hi, shm_ct **out, shm_host_graph **graph) {
     return guard([&] {

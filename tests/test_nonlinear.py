@@ -1,5 +1,6 @@
 """Polynomial operators of the BERT layer on ciphertext batches (shm_host_chebyshev,
-shm_host_gelu; the reference's non_linear_func/, gelu_cheb at gelu_other.cuh:258-300).
+shm_host_gelu, shm_host_exp, shm_host_inverse; the reference's non_linear_func/: gelu_cheb at
+gelu_other.cuh:258-300, exp and inverse at softmax.cuh:23-118).
 
 CPU: the host library on the oracle's C ABI at N = 2^12.  A Chebyshev series evaluated on
 ciphertexts decrypts to numpy's evaluation of the same series (CKKS noise only); GELU
@@ -71,6 +72,30 @@ def test_gelu_is_the_reference_series(small):
     assert np.abs(y - _gelu(x)).max() < 0.04
 
 
+def test_exp_and_inverse_are_the_reference_formulas(small):
+    """exp as (1 + x/128)^128 and 1/x as prod (1 + (1 - x)^(2^i)) (softmax.cuh:23-118):
+    decryptions equal numpy's evaluation of the same formulas; levels 8 and iter + 1."""
+    h = small
+    rng = np.random.default_rng(8)
+    x = rng.uniform(-8.0, 1.0, (2, h.n // 2))
+    out = h.exp(h.encrypt(x, DELTA, 10))
+    assert out.level == 2
+    assert np.abs(h.decrypt(out).real - (1 + x / 128) ** 128).max() < 1e-6
+    x = rng.uniform(0.05, 1.95, (2, h.n // 2))
+    for it in (3, 7):
+        out = h.inverse(h.encrypt(x, DELTA, 9), it)
+        y, r = 1 - x, 2 - x
+        for _ in range(it):
+            y = y * y
+            r = r * (1 + y)
+        assert out.level == 9 - it - 1
+        assert np.abs(h.decrypt(out).real - r).max() < 1e-6
+    with pytest.raises(HostError, match="levels"):
+        h.exp(h.encrypt(x, DELTA, 9))
+    with pytest.raises(HostError, match="levels"):
+        h.inverse(h.encrypt(x, DELTA, 5), 4)
+
+
 def test_polynomial_operators_refuse_bad_inputs(small):
     h = small
     rng = np.random.default_rng(4)
@@ -99,6 +124,10 @@ def test_cuda_polynomial_operators_match_oracle_build():
         coeffs = rng.uniform(-1, 1, 13)
         assert np.array_equal(h_cu.chebyshev(a, coeffs, -20.0, 13.0).to_host(),
                               h_or.chebyshev(b, coeffs, -20.0, 13.0).to_host())
+        assert np.array_equal(h_cu.inverse(h_cu.encrypt(x / 20.0 + 1.0, DELTA, 9), 6).to_host(),
+                              h_or.inverse(h_or.encrypt(x / 20.0 + 1.0, DELTA, 9), 6).to_host())
+        e1, e2 = h_cu.encrypt(x / 4.0, DELTA, 10), h_or.encrypt(x / 4.0, DELTA, 10)
+        assert np.array_equal(h_cu.exp(e1).to_host(), h_or.exp(e2).to_host())
 
 
 @pytest.mark.gpu
