@@ -382,6 +382,9 @@ class Graph {
 // 1/x for x in (0, 2) by prod_{i <= iter} (1 + (1 - x)^(2^i)) (iter + 1 levels)
 Ciphertext exp_approx(const Evaluator &ev, const Ciphertext &x);
 Ciphertext inverse_approx(const Evaluator &ev, const Ciphertext &x, int iter);
+// 1/sqrt(x) for LayerNorm (invert_sqrt, layernorm.cuh:708-897): a linear first guess,
+// d_newt Newton steps and d_gold Goldschmidt steps (the reference uses 4 and 2)
+Ciphertext inv_sqrt_approx(const Evaluator &ev, const Ciphertext &x, int d_newt = 4, int d_gold = 2);
 
 // A CUDA graph of evaluate_chebyshev(ev, in, c, lo, hi) and the output batch every launch
 // rewrites (write the next input into `in` between launches; `in` must outlive the graph).

@@ -105,6 +105,9 @@ int shm_host_gelu(shm_host *h, const shm_ct *a, shm_ct **out);
  * (8 levels), and 1/x for x in (0, 2) as prod_{i <= iter} (1 + (1 - x)^(2^i)) (iter + 1 levels) */
 int shm_host_exp(shm_host *h, const shm_ct *a, shm_ct **out);
 int shm_host_inverse(shm_host *h, const shm_ct *a, uint32_t iter, shm_ct **out);
+/* 1/sqrt(x) for LayerNorm (invert_sqrt, non_linear_func/layernorm.cuh:708-897): the first
+ * guess -1.29054537e-4 x + 0.129054537, d_newt Newton and d_gold Goldschmidt steps */
+int shm_host_inv_sqrt(shm_host *h, const shm_ct *a, uint32_t d_newt, uint32_t d_gold, shm_ct **out);
 /* a CUDA graph of shm_host_chebyshev (coeffs = NULL: GELU) on `in`; *out is rewritten by every
  * shm_host_graph_launch; write the next batch into `in` with shm_ct_write between launches */
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,

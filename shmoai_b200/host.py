@@ -100,6 +100,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_gelu": (i32, [_P, _P, pp]),
         "shm_host_exp": (i32, [_P, _P, pp]),
         "shm_host_inverse": (i32, [_P, _P, _U32, pp]),
+        "shm_host_inv_sqrt": (i32, [_P, _P, _U32, _U32, pp]),
         "shm_host_chebyshev_capture": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp, pp]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
@@ -306,6 +307,10 @@ class Host:
     def inverse(self, a, iter: int):
         """1/x for x in (0, 2) as prod_{i <= iter} (1 + (1 - x)^(2^i)) (iter + 1 levels)."""
         return self._out(self.lib.shm_host_inverse, a._c, iter)
+
+    def inv_sqrt(self, a, d_newt: int = 4, d_gold: int = 2):
+        """1/sqrt(x) as LayerNorm's invert_sqrt: linear guess, Newton then Goldschmidt steps."""
+        return self._out(self.lib.shm_host_inv_sqrt, a._c, d_newt, d_gold)
 
     def capture_chebyshev(self, ct, coeffs=None, lo: float = 0.0, hi: float = 0.0):
         """A CUDA graph of chebyshev(ct, coeffs, lo, hi) (GELU when coeffs is None) and the output

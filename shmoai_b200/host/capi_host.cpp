@@ -259,6 +259,10 @@ int shm_host_inverse(shm_host *h, const shm_ct *a, uint32_t iter, shm_ct **out) 
     return guard([&] { put(out, inverse_approx(*H(h).ev, C(a), (int)iter)); });
 }
 
+int shm_host_inv_sqrt(shm_host *h, const shm_ct *a, uint32_t d_newt, uint32_t d_gold, shm_ct **out) {
+    return guard([&] { put(out, inv_sqrt_approx(*H(h).ev, C(a), (int)d_newt, (int)d_gold)); });
+}
+
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,
                                double hi, shm_ct **out, shm_host_graph **graph) {
     return guard([&] {

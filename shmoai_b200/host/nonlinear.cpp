@@ -1,6 +1,9 @@
 // The softmax's building blocks on ciphertext batches (src/include/source/non_linear_func/
 // softmax.cuh:23-118): exp by (1 + x/128)^128 and 1/x by the product prod_i (1 + y^(2^i)),
 // y = 1 - x.  Products are relinearised and rescaled in one ModDown (relinearize_rescale).
+#include <algorithm>
+#include <cmath>
+
 #include "internal.hpp"
 
 namespace shmoai {
@@ -44,6 +47,48 @@ Ciphertext inverse_approx(const Evaluator &ev, const Ciphertext &x, int iter) {
         r = product(ev, r, ev.add_const(y, 1.0));
     }
     return r;
+}
+
+// a + b after bringing both to the lower level and b to a's scale (b is scaled by one exact
+// constant multiply when the scales differ, which needs a spare level on b)
+static Ciphertext add_aligned(const Evaluator &ev, const Ciphertext &a, const Ciphertext &b) {
+    const uint32_t L = std::min(a.L, b.L);
+    const bool same = std::fabs(a.scale_ / b.scale_ - 1.0) < 1e-12;
+    if (same) return ev.add(ev.mod_switch_to(a, L), ev.mod_switch_to(b, L));
+    // the rescaled copy of b lands one level lower: bring a there too
+    const uint32_t Lb = std::min(L + 1, b.L);
+    Ciphertext bs = ev.multiply_const(ev.mod_switch_to(b, Lb), 1.0, a.scale_);
+    const uint32_t Lo = std::min(bs.L, L);
+    Ciphertext ao = ev.mod_switch_to(a, Lo);
+    return ev.add(ao, ev.mod_switch_to(bs, Lo));
+}
+
+// 1/sqrt(x) (invert_sqrt, layernorm.cuh:708-897): the line -1.29054537e-4 x + 0.129054537 as
+// the first guess, d_newt Newton steps r <- r (3/2 - x r^2 / 2), then d_gold Goldschmidt steps
+// on (g, h) = (x r, r / 2): s = 1/2 - g h, g <- g + g s, h <- h + h s; the result is 2 h
+Ciphertext inv_sqrt_approx(const Evaluator &ev, const Ciphertext &x, int d_newt, int d_gold) {
+    need_ordinary(x, "inverse square root");
+    if (d_newt < 0 || d_gold < 0) throw Error("iteration counts must be non-negative");
+    const uint32_t need = 2 * (uint32_t)(d_newt + d_gold) + 4;  // levels used + the output prime
+    if (x.L < need) throw Error("inverse square root needs " + std::to_string(need) + " primes");
+    const Context &c = ev.context();
+    const double S = x.scale_;
+    Ciphertext r = ev.add_const(ev.multiply_const(x, -1.29054537e-4, (double)c.primes[x.L - 2]), 1.29054537e-1);
+    const Ciphertext xh = ev.multiply_const(x, -0.5, (double)c.primes[x.L - 2]);  // -x / 2
+    for (int i = 0; i < d_newt; i++) {
+        Ciphertext t = product(ev, product(ev, xh, r), square(ev, r));  // -x r^3 / 2
+        r = add_aligned(ev, t, ev.multiply_const(r, 1.5, (double)c.primes[r.L - 2]));
+    }
+    Ciphertext g = product(ev, x, r);
+    Ciphertext h = ev.multiply_const(r, 0.5, (double)c.primes[r.L - 2]);
+    for (int i = 0; i < d_gold; i++) {
+        Ciphertext s = ev.add_const(ev.multiply_int(product(ev, g, h), -1), 0.5);
+        Ciphertext g2 = product(ev, g, s), h2 = product(ev, h, s);
+        g = add_aligned(ev, g2, g);
+        h = add_aligned(ev, h2, h);
+    }
+    Ciphertext out = ev.multiply_const(h, 2.0, S);
+    return out;
 }
 
 }  // namespace shmoai

@@ -96,6 +96,34 @@ def test_exp_and_inverse_are_the_reference_formulas(small):
         h.inverse(h.encrypt(x, DELTA, 5), 4)
 
 
+def _inv_sqrt_reference(x, d_newt=4, d_gold=2):
+    """invert_sqrt's arithmetic in numpy (layernorm.cuh:708-897)."""
+    r = -1.29054537e-4 * x + 1.29054537e-1
+    for _ in range(d_newt):
+        r = r * (1.5 - 0.5 * x * r * r)
+    g, h = x * r, 0.5 * r
+    for _ in range(d_gold):
+        s = 0.5 - g * h
+        g, h = g + g * s, h + h * s
+    return 2 * h
+
+
+def test_inv_sqrt_is_the_reference_iteration():
+    """LayerNorm's inverse square root: a linear guess, 4 Newton and 2 Goldschmidt steps,
+    2 (d_newt + d_gold) + 3 levels; decryptions equal numpy's run of the same iteration."""
+    h = _host(bits=[51] + [46] * 19 + [51] + [51] * 5)
+    rng = np.random.default_rng(9)
+    x = rng.uniform(1.0, 800.0, (2, h.n // 2))
+    out = h.inv_sqrt(h.encrypt(x, DELTA, 21))
+    assert out.level == 21 - 15 and out.scale == DELTA
+    assert np.abs(h.decrypt(out).real - _inv_sqrt_reference(x)).max() < 1e-7
+    out = h.inv_sqrt(h.encrypt(x, DELTA, 16), 2, 1)
+    assert out.level == 16 - 9
+    assert np.abs(h.decrypt(out).real - _inv_sqrt_reference(x, 2, 1)).max() < 1e-7
+    with pytest.raises(HostError, match="needs 16 primes"):
+        h.inv_sqrt(h.encrypt(x, DELTA, 15))
+
+
 def test_polynomial_operators_refuse_bad_inputs(small):
     h = small
     rng = np.random.default_rng(4)
@@ -128,6 +156,8 @@ def test_cuda_polynomial_operators_match_oracle_build():
                               h_or.inverse(h_or.encrypt(x / 20.0 + 1.0, DELTA, 9), 6).to_host())
         e1, e2 = h_cu.encrypt(x / 4.0, DELTA, 10), h_or.encrypt(x / 4.0, DELTA, 10)
         assert np.array_equal(h_cu.exp(e1).to_host(), h_or.exp(e2).to_host())
+        v1, v2 = h_cu.encrypt(x * 20.0 + 400.0, DELTA, 12), h_or.encrypt(x * 20.0 + 400.0, DELTA, 12)
+        assert np.array_equal(h_cu.inv_sqrt(v1, 2, 1).to_host(), h_or.inv_sqrt(v2, 2, 1).to_host())
 
 
 @pytest.mark.gpu
