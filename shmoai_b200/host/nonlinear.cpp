@@ -1,6 +1,7 @@
-// The softmax's building blocks on ciphertext batches (src/include/source/non_linear_func/
-// softmax.cuh:23-118): exp by (1 + x/128)^128 and 1/x by the product prod_i (1 + y^(2^i)),
-// y = 1 - x.  Products are relinearised and rescaled in one ModDown (relinearize_rescale).
+// The softmax's and LayerNorm's building blocks on ciphertext batches (src/include/source/
+// non_linear_func/softmax.cuh:23-118, layernorm.cuh:708-897): exp by (1 + x/128)^128, 1/x by
+// the product prod_i (1 + y^(2^i)), y = 1 - x, and 1/sqrt(x) by Newton and Goldschmidt steps.
+// Products are relinearised and rescaled in one ModDown (relinearize_rescale).
 #include <algorithm>
 #include <cmath>
 
@@ -26,7 +27,7 @@ void need_ordinary(const Ciphertext &x, const char *what) {
 // prime the first square divides by), then seven squarings: 8 levels
 Ciphertext exp_approx(const Evaluator &ev, const Ciphertext &x) {
     need_ordinary(x, "exp");
-    if (x.L < 10) throw Error("exp needs 8 levels and one prime for its output");
+    if (x.L < 9) throw Error("exp needs 8 levels and one prime for its output");
     const Context &c = ev.context();
     Ciphertext y = ev.add_const(ev.multiply_const(x, 1.0 / 128.0, (double)c.primes[x.L - 2]), 1.0);
     for (int i = 0; i < 7; i++) y = square(ev, y);

@@ -90,8 +90,9 @@ def test_exp_and_inverse_are_the_reference_formulas(small):
             r = r * (1 + y)
         assert out.level == 9 - it - 1
         assert np.abs(h.decrypt(out).real - r).max() < 1e-6
+    assert h.exp(h.encrypt(x - 1.0, DELTA, 9)).level == 1
     with pytest.raises(HostError, match="levels"):
-        h.exp(h.encrypt(x, DELTA, 9))
+        h.exp(h.encrypt(x, DELTA, 8))
     with pytest.raises(HostError, match="levels"):
         h.inverse(h.encrypt(x, DELTA, 5), 4)
 
