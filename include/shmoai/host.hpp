@@ -385,6 +385,14 @@ Ciphertext inverse_approx(const Evaluator &ev, const Ciphertext &x, int iter);
 // 1/sqrt(x) for LayerNorm (invert_sqrt, layernorm.cuh:708-897): a linear first guess,
 // d_newt Newton steps and d_gold Goldschmidt steps (the reference uses 4 and 2)
 Ciphertext inv_sqrt_approx(const Evaluator &ev, const Ciphertext &x, int d_newt = 4, int d_gold = 2);
+// the sum of a batch's ciphertexts (one ciphertext), and one batch made of several
+Ciphertext batch_sum(const Evaluator &ev, const Ciphertext &x);
+Ciphertext batch_gather(const Evaluator &ev, const std::vector<Ciphertext> &parts);
+// LayerNorm over the hidden columns of the column packing, one column per ciphertext of the
+// batch (layernorm, layernorm.cuh:899-): gamma_i (x_i - mean) / sqrt(var) + beta_i with the
+// inverse square root above; 2 (d_newt + d_gold) + 8 levels
+Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &gamma,
+                     const std::vector<double> &beta, int d_newt = 4, int d_gold = 2);
 
 // A CUDA graph of evaluate_chebyshev(ev, in, c, lo, hi) and the output batch every launch
 // rewrites (write the next input into `in` between launches; `in` must outlive the graph).

@@ -108,6 +108,12 @@ int shm_host_inverse(shm_host *h, const shm_ct *a, uint32_t iter, shm_ct **out);
 /* 1/sqrt(x) for LayerNorm (invert_sqrt, non_linear_func/layernorm.cuh:708-897): the first
  * guess -1.29054537e-4 x + 0.129054537, d_newt Newton and d_gold Goldschmidt steps */
 int shm_host_inv_sqrt(shm_host *h, const shm_ct *a, uint32_t d_newt, uint32_t d_gold, shm_ct **out);
+/* LayerNorm over the hidden columns of the column packing, one column per ciphertext of the
+ * batch `a` (layernorm, non_linear_func/layernorm.cuh:899-): gamma[i] (x_i - mean) / sqrt(var)
+ * + beta[i] with the inverse square root above (gamma, beta: one value per ciphertext);
+ * 2 (d_newt + d_gold) + 8 levels */
+int shm_host_layernorm(shm_host *h, const shm_ct *a, const double *gamma, const double *beta, uint32_t d_newt,
+                       uint32_t d_gold, shm_ct **out);
 /* a CUDA graph of shm_host_chebyshev (coeffs = NULL: GELU) on `in`; *out is rewritten by every
  * shm_host_graph_launch; write the next batch into `in` with shm_ct_write between launches */
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,

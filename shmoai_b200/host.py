@@ -101,6 +101,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_exp": (i32, [_P, _P, pp]),
         "shm_host_inverse": (i32, [_P, _P, _U32, pp]),
         "shm_host_inv_sqrt": (i32, [_P, _P, _U32, _U32, pp]),
+        "shm_host_layernorm": (i32, [_P, _P, dp, dp, _U32, _U32, pp]),
         "shm_host_chebyshev_capture": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp, pp]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
@@ -311,6 +312,15 @@ class Host:
     def inv_sqrt(self, a, d_newt: int = 4, d_gold: int = 2):
         """1/sqrt(x) as LayerNorm's invert_sqrt: linear guess, Newton then Goldschmidt steps."""
         return self._out(self.lib.shm_host_inv_sqrt, a._c, d_newt, d_gold)
+
+    def layernorm(self, a, gamma, beta, d_newt: int = 4, d_gold: int = 2):
+        """LayerNorm over the batch's ciphertexts (one hidden column each): gamma_i (x_i - mean) / sqrt(var) + beta_i."""
+        g = np.ascontiguousarray(gamma, dtype=np.float64)
+        b = np.ascontiguousarray(beta, dtype=np.float64)
+        if len(g) != a.count or len(b) != a.count:
+            raise ValueError("gamma and beta need one value per ciphertext")
+        dp = ctypes.POINTER(ctypes.c_double)
+        return self._out(self.lib.shm_host_layernorm, a._c, g.ctypes.data_as(dp), b.ctypes.data_as(dp), d_newt, d_gold)
 
     def capture_chebyshev(self, ct, coeffs=None, lo: float = 0.0, hi: float = 0.0):
         """A CUDA graph of chebyshev(ct, coeffs, lo, hi) (GELU when coeffs is None) and the output

@@ -263,6 +263,17 @@ int shm_host_inv_sqrt(shm_host *h, const shm_ct *a, uint32_t d_newt, uint32_t d_
     return guard([&] { put(out, inv_sqrt_approx(*H(h).ev, C(a), (int)d_newt, (int)d_gold)); });
 }
 
+int shm_host_layernorm(shm_host *h, const shm_ct *a, const double *gamma, const double *beta, uint32_t d_newt,
+                       uint32_t d_gold, shm_ct **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        const Ciphertext &x = C(a);
+        if (!gamma || !beta) throw Error("null gamma or beta");
+        put(out, layernorm(*hh.ev, x, std::vector<double>(gamma, gamma + x.count),
+                           std::vector<double>(beta, beta + x.count), (int)d_newt, (int)d_gold));
+    });
+}
+
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,
                                double hi, shm_ct **out, shm_host_graph **graph) {
     return guard([&] {

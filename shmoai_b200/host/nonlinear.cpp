@@ -92,4 +92,77 @@ Ciphertext inv_sqrt_approx(const Evaluator &ev, const Ciphertext &x, int d_newt,
     return out;
 }
 
+Ciphertext batch_sum(const Evaluator &ev, const Ciphertext &x) {
+    need_ordinary(x, "batch_sum");
+    if (x.count == 0) throw Error("empty batch");
+    Ciphertext cur = ev.slice(x, 0, x.count);
+    while (cur.count > 1) {  // halves added pairwise; an odd last member is carried
+        const uint32_t h = cur.count / 2;
+        Ciphertext s = ev.add(ev.slice(cur, 0, h), ev.slice(cur, h, h));
+        if (cur.count & 1) s = ev.concat(s, ev.slice(cur, 2 * h, 1));
+        cur = std::move(s);
+    }
+    return cur;
+}
+
+static Ciphertext gather_ptrs(const Evaluator &ev, const std::vector<const Ciphertext *> &parts) {
+    if (parts.empty()) throw Error("nothing to gather");
+    const Ciphertext &p0 = *parts[0];
+    const Context &c = ev.context();
+    size_t words = 0;
+    uint32_t count = 0;
+    for (const Ciphertext *p : parts) {
+        if (p->L != p0.L || p->size != p0.size || p->shared != p0.shared ||
+            std::fabs(p->scale_ / p0.scale_ - 1.0) > 1e-12)
+            throw Error("gather: parts differ in level, size or scale");
+        words += p->polys() * p->L * c.n;
+        count += p->count;
+    }
+    Ciphertext o;
+    o.data = DeviceBuffer(c, words);
+    o.count = count;
+    o.size = p0.size;
+    o.L = p0.L;
+    o.scale_ = p0.scale_;
+    o.shared = p0.shared;
+    size_t off = 0;
+    for (const Ciphertext *p : parts) {
+        const size_t w = p->polys() * p->L * c.n;
+        c.check(shm_memcpy(c.handle(), o.data.data() + off, p->data.data(), w * 8, SHM_COPY_D2D, c.stream()));
+        off += w;
+    }
+    return o;
+}
+
+Ciphertext batch_gather(const Evaluator &ev, const std::vector<Ciphertext> &parts) {
+    std::vector<const Ciphertext *> p;
+    for (const Ciphertext &x : parts) p.push_back(&x);
+    return gather_ptrs(ev, p);
+}
+
+// LayerNorm over hidden columns packed one per ciphertext (layernorm, layernorm.cuh:899-):
+// mean and variance are sums over the batch, the inverse square root is inv_sqrt_approx, and
+// column i gets gamma_i (x_i - mean) / sqrt(var) + beta_i; 2 (d_newt + d_gold) + 8 levels
+Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &gamma,
+                     const std::vector<double> &beta, int d_newt, int d_gold) {
+    need_ordinary(x, "layernorm");
+    const uint32_t d = x.count;
+    if (d == 0 || gamma.size() != d || beta.size() != d) throw Error("layernorm: gamma and beta need one value per column");
+    const uint32_t need = 2 * (uint32_t)(d_newt + d_gold) + 9;
+    if (x.L < need) throw Error("layernorm needs " + std::to_string(need) + " primes");
+    const Context &c = ev.context();
+    const double S = x.scale_;
+    auto broadcast = [&](const Ciphertext &one) { return gather_ptrs(ev, std::vector<const Ciphertext *>(d, &one)); };
+    const Ciphertext mean = ev.multiply_const(batch_sum(ev, x), 1.0 / d, S);
+    const Ciphertext xc = ev.sub(ev.mod_switch_to(x, mean.L), broadcast(mean));
+    const Ciphertext sq = square(ev, xc);
+    const Ciphertext var = ev.multiply_const(batch_sum(ev, sq), 1.0 / d, (double)c.primes[sq.L - 2]);
+    const Ciphertext inv = inv_sqrt_approx(ev, var, d_newt, d_gold);
+    const Ciphertext y = product(ev, xc, broadcast(inv));
+    std::vector<Ciphertext> cols;
+    cols.reserve(d);
+    for (uint32_t i = 0; i < d; i++) cols.push_back(ev.add_const(ev.multiply_const(ev.slice(y, i, 1), gamma[i], S), beta[i]));
+    return batch_gather(ev, cols);
+}
+
 }  // namespace shmoai

@@ -1,6 +1,7 @@
 """Polynomial operators of the BERT layer on ciphertext batches (shm_host_chebyshev,
-shm_host_gelu, shm_host_exp, shm_host_inverse; the reference's non_linear_func/: gelu_cheb at
-gelu_other.cuh:258-300, exp and inverse at softmax.cuh:23-118).
+shm_host_gelu, shm_host_exp, shm_host_inverse, shm_host_inv_sqrt, shm_host_layernorm; the
+reference's non_linear_func/: gelu_cheb at gelu_other.cuh:258-300, exp and inverse at
+softmax.cuh:23-118, invert_sqrt and layernorm in layernorm.cuh).
 
 CPU: the host library on the oracle's C ABI at N = 2^12.  A Chebyshev series evaluated on
 ciphertexts decrypts to numpy's evaluation of the same series (CKKS noise only); GELU
@@ -125,6 +126,28 @@ def test_inv_sqrt_is_the_reference_iteration():
         h.inv_sqrt(h.encrypt(x, DELTA, 15))
 
 
+def test_layernorm_over_the_hidden_columns():
+    """LayerNorm of 8 hidden columns (one per ciphertext): mean and variance over the batch,
+    the reference's inverse square root, gamma and beta per column; decryptions equal numpy's
+    run of the same arithmetic; 2 (4 + 2) + 8 = 20 levels."""
+    h = _host(bits=[51] + [46] * 19 + [51] + [51] * 5)
+    rng = np.random.default_rng(10)
+    d, n = 8, h.n // 2
+    z = rng.standard_normal((d, n))
+    z = (z - z.mean(axis=0)) / z.std(axis=0)  # per slot: mean 0, variance 1 over the columns
+    sigma = rng.uniform(2.0, 20.0, n)  # so that var = sigma^2 lies in [4, 400], inside the guess's range
+    x = rng.uniform(-3, 3, n) + sigma * z
+    gamma, beta = rng.uniform(0.5, 1.5, d), rng.uniform(-0.5, 0.5, d)
+    out = h.layernorm(h.encrypt(x, DELTA, 21), gamma, beta)
+    mean = x.mean(axis=0)
+    var = ((x - mean) ** 2).mean(axis=0)
+    want = gamma[:, None] * (x - mean) * _inv_sqrt_reference(var) + beta[:, None]
+    assert out.count == d and out.level == 1 and out.scale == DELTA
+    assert np.abs(h.decrypt(out).real - want).max() < 1e-5
+    with pytest.raises(HostError, match="needs 21 primes"):
+        h.layernorm(h.encrypt(x, DELTA, 20), gamma, beta)
+
+
 def test_polynomial_operators_refuse_bad_inputs(small):
     h = small
     rng = np.random.default_rng(4)
@@ -159,6 +182,11 @@ def test_cuda_polynomial_operators_match_oracle_build():
         assert np.array_equal(h_cu.exp(e1).to_host(), h_or.exp(e2).to_host())
         v1, v2 = h_cu.encrypt(x * 20.0 + 400.0, DELTA, 12), h_or.encrypt(x * 20.0 + 400.0, DELTA, 12)
         assert np.array_equal(h_cu.inv_sqrt(v1, 2, 1).to_host(), h_or.inv_sqrt(v2, 2, 1).to_host())
+        z = rng.standard_normal((3, g.n // 2))
+        cols = 5.0 * (z - z.mean(axis=0)) / z.std(axis=0)
+        w1, w2 = h_cu.encrypt(cols, DELTA, 16), h_or.encrypt(cols, DELTA, 16)
+        gm, bt = [1.0, 0.5, 2.0], [0.0, 0.25, -0.5]
+        assert np.array_equal(h_cu.layernorm(w1, gm, bt, 2, 1).to_host(), h_or.layernorm(w2, gm, bt, 2, 1).to_host())
 
 
 @pytest.mark.gpu
