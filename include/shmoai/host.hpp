@@ -393,6 +393,10 @@ Ciphertext batch_gather(const Evaluator &ev, const std::vector<Ciphertext> &part
 // inverse square root above; 2 (d_newt + d_gold) + 8 levels
 Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &gamma,
                      const std::vector<double> &beta, int d_newt = 4, int d_gold = 2);
+// softmax over the members of a batch (softmax.cuh:119-, without the attention layout's masks):
+// e_i / sum_j e_j with e_i = exp_approx(x_i - shift) and the sum's inverse by inverse_approx on
+// sum_scale * sum_j e_j, which the caller brings into (0, 2); iter + 12 levels
+Ciphertext softmax_batch(const Evaluator &ev, const Ciphertext &x, double shift, double sum_scale, int iter);
 
 // A CUDA graph of evaluate_chebyshev(ev, in, c, lo, hi) and the output batch every launch
 // rewrites (write the next input into `in` between launches; `in` must outlive the graph).

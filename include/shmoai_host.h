@@ -114,6 +114,11 @@ int shm_host_inv_sqrt(shm_host *h, const shm_ct *a, uint32_t d_newt, uint32_t d_
  * 2 (d_newt + d_gold) + 8 levels */
 int shm_host_layernorm(shm_host *h, const shm_ct *a, const double *gamma, const double *beta, uint32_t d_newt,
                        uint32_t d_gold, shm_ct **out);
+/* softmax over the ciphertexts of a batch (softmax, non_linear_func/softmax.cuh:119-, without
+ * the attention layout's masks): e_i / sum_j e_j, e_i = exp(x_i - shift) as above, the sum's
+ * inverse by shm_host_inverse on sum_scale * sum_j e_j (the caller keeps it in (0, 2));
+ * iter + 12 levels */
+int shm_host_softmax(shm_host *h, const shm_ct *a, double shift, double sum_scale, uint32_t iter, shm_ct **out);
 /* a CUDA graph of shm_host_chebyshev (coeffs = NULL: GELU) on `in`; *out is rewritten by every
  * shm_host_graph_launch; write the next batch into `in` with shm_ct_write between launches */
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,

@@ -274,6 +274,10 @@ int shm_host_layernorm(shm_host *h, const shm_ct *a, const double *gamma, const 
     });
 }
 
+int shm_host_softmax(shm_host *h, const shm_ct *a, double shift, double sum_scale, uint32_t iter, shm_ct **out) {
+    return guard([&] { put(out, softmax_batch(*H(h).ev, C(a), shift, sum_scale, (int)iter)); });
+}
+
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,
                                double hi, shm_ct **out, shm_host_graph **graph) {
     return guard([&] {

@@ -165,4 +165,22 @@ Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector
     return batch_gather(ev, cols);
 }
 
+// softmax over the members of a batch (softmax.cuh:119-, without the attention layout's
+// masks): e_i = exp_approx(x_i - shift), s = sum_scale * sum_i e_i brought into (0, 2) by the
+// caller's sum_scale, y_i = sum_scale * e_i * inverse_approx(s, iter) = e_i / sum_j e_j;
+// iter + 12 levels
+Ciphertext softmax_batch(const Evaluator &ev, const Ciphertext &x, double shift, double sum_scale, int iter) {
+    need_ordinary(x, "softmax");
+    if (!(sum_scale > 0)) throw Error("softmax: sum_scale must be positive");
+    const uint32_t need = (uint32_t)iter + 13;
+    if (x.L < need) throw Error("softmax needs " + std::to_string(need) + " primes");
+    const Context &c = ev.context();
+    const double S = x.scale_;
+    const Ciphertext e = exp_approx(ev, ev.add_const(x, -shift));
+    const Ciphertext s = ev.multiply_const(batch_sum(ev, e), sum_scale, (double)c.primes[e.L - 2]);
+    const Ciphertext inv = inverse_approx(ev, s, iter);
+    const Ciphertext y = product(ev, e, gather_ptrs(ev, std::vector<const Ciphertext *>(x.count, &inv)));
+    return ev.multiply_const(y, sum_scale, S);
+}
+
 }  // namespace shmoai

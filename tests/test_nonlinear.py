@@ -1,5 +1,6 @@
 """Polynomial operators of the BERT layer on ciphertext batches (shm_host_chebyshev,
-shm_host_gelu, shm_host_exp, shm_host_inverse, shm_host_inv_sqrt, shm_host_layernorm; the
+shm_host_gelu, shm_host_exp, shm_host_inverse, shm_host_inv_sqrt, shm_host_layernorm,
+shm_host_softmax; the
 reference's non_linear_func/: gelu_cheb at gelu_other.cuh:258-300, exp and inverse at
 softmax.cuh:23-118, invert_sqrt and layernorm in layernorm.cuh).
 
@@ -148,6 +149,28 @@ def test_layernorm_over_the_hidden_columns():
         h.layernorm(h.encrypt(x, DELTA, 20), gamma, beta)
 
 
+def test_softmax_over_the_batch():
+    """softmax over 6 ciphertexts: the reference's exp, a batch sum scaled into (0, 2), its
+    Goldschmidt inverse and the product; decryptions equal numpy's run of the same formulas."""
+    h = _host(bits=[51] + [46] * 19 + [51] + [51] * 5)
+    rng = np.random.default_rng(12)
+    x = rng.uniform(-2.0, 2.0, (6, h.n // 2))
+    shift, sum_scale, it = 0.5, 1.0 / 32.0, 7
+    out = h.softmax(h.encrypt(x, DELTA, 21), shift, sum_scale, it)
+    e = (1 + (x - shift) / 128) ** 128
+    s = sum_scale * e.sum(axis=0)
+    y, r = 1 - s, 2 - s
+    for _ in range(it):
+        y = y * y
+        r = r * (1 + y)
+    want = sum_scale * e * r
+    assert out.count == 6 and out.level == 21 - it - 12 and out.scale == DELTA
+    assert np.abs(h.decrypt(out).real - want).max() < 1e-5
+    assert np.abs(want - np.exp(x) / np.exp(x).sum(axis=0)).max() < 0.05  # the formulas approximate softmax
+    with pytest.raises(HostError, match="needs 20 primes"):
+        h.softmax(h.encrypt(x, DELTA, 19), shift, sum_scale, it)
+
+
 def test_polynomial_operators_refuse_bad_inputs(small):
     h = small
     rng = np.random.default_rng(4)
@@ -187,6 +210,8 @@ def test_cuda_polynomial_operators_match_oracle_build():
         w1, w2 = h_cu.encrypt(cols, DELTA, 16), h_or.encrypt(cols, DELTA, 16)
         gm, bt = [1.0, 0.5, 2.0], [0.0, 0.25, -0.5]
         assert np.array_equal(h_cu.layernorm(w1, gm, bt, 2, 1).to_host(), h_or.layernorm(w2, gm, bt, 2, 1).to_host())
+        s1, s2 = h_cu.encrypt(x / 10.0, DELTA, 19), h_or.encrypt(x / 10.0, DELTA, 19)
+        assert np.array_equal(h_cu.softmax(s1, 0.5, 1.0 / 8.0, 5).to_host(), h_or.softmax(s2, 0.5, 1.0 / 8.0, 5).to_host())
 
 
 @pytest.mark.gpu
