@@ -8,13 +8,14 @@
 // prime order are the reference's, so a secret moves either way unchanged.
 //
 // A record is an 80-byte header, the payload as little-endian 64-bit words, and the
-// payload's digest (8 bytes).  Header, in order:
+// record's digest (8 bytes).  Header, in order:
 //   magic "SHMOAIW\0" (8 bytes), version (u16, 1), kind (u16, Kind),
 //   log N (u32), n_q (u32), n_p (u32), digest of the prime chain Q then P (u64),
 //   shape d0, d1, d2 (u32 each), flags (u32: bit 0 shared-a groups),
 //   tag (u32: Galois element or member index), group (u32: members of a shared-a key set,
 //   or the number of auxiliary secrets), scale (f64), payload words (u64), reserved (u64, 0).
-// The payload holds d0 * d1 * d2 * N words.  Digests are 64-bit FNV-1a over words:
+// The payload holds d0 * d1 * d2 * N words.  The digest covers the header (its 80 bytes as
+// ten little-endian words) and then the payload: 64-bit FNV-1a over words,
 // h = (h ^ w) * 0x100000001b3, starting from 0xcbf29ce484222325.
 //
 // Loading checks every header field against the context, every residue against its prime

@@ -162,7 +162,7 @@ void shm_host_graph_destroy(shm_host_graph *g);
 double shm_slot_transform_selfcheck(uint32_t log_slots);
 
 /* ---- binary records (include/shmoai/wire.hpp): an 80-byte header naming the kind, ring,
- * prime-chain digest, shape and scale, the payload words, then the payload's digest.
+ * prime-chain digest, shape and scale, the payload words, then a digest of header and payload.
  * Loading checks the header against the host's context, every residue against its prime
  * and the digest; a failure returns SHM_EINVAL and builds nothing.
  * Ciphertext batches go to and from caller memory: shm_ct_serialized_bytes gives the size

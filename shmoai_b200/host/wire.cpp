@@ -33,7 +33,14 @@ struct Header {
     uint32_t d0 = 0, d1 = 0, d2 = 0, flags = 0, tag = 0, group = 0;
     double scale = 1.0;
     uint64_t words = 0;
+    uint64_t digest = 0;  // of the header's bytes: the record's digest continues from it
 };
+
+uint64_t header_digest(const uint8_t *b) {
+    uint64_t w[kHeaderBytes / 8];
+    std::memcpy(w, b, kHeaderBytes);
+    return fnv(kFnvBasis, w, kHeaderBytes / 8);
+}
 
 template <typename T>
 void put(uint8_t *&p, T v) {
@@ -48,7 +55,7 @@ T get(const uint8_t *&p) {
     return v;
 }
 
-void write_header(const Sink &out, const Header &h) {
+uint64_t write_header(const Sink &out, const Header &h) {
     uint8_t b[kHeaderBytes] = {}, *p = b;
     std::memcpy(p, kMagic, 8);
     p += 8;
@@ -68,6 +75,7 @@ void write_header(const Sink &out, const Header &h) {
     put(p, h.words);
     put<uint64_t>(p, 0);  // reserved
     out(b, kHeaderBytes);
+    return header_digest(b);
 }
 
 Header read_header(const Source &in, const Context &c) {
@@ -76,6 +84,7 @@ Header read_header(const Source &in, const Context &c) {
     if (std::memcmp(b, kMagic, 8) != 0) throw Error("not a record: bad magic");
     const uint8_t *p = b + 8;
     Header h;
+    h.digest = header_digest(b);
     const uint16_t version = get<uint16_t>(p);
     if (version != kVersion) throw Error("record version " + std::to_string(version) + " is not supported");
     const uint16_t kind = get<uint16_t>(p);
@@ -111,10 +120,9 @@ Header base(const Context &c, Kind k) {
     return h;
 }
 
-// device words -> sink, in chunks, then the digest
-void write_device(const Sink &out, const Context &c, const uint64_t *dev, size_t words) {
+// device words -> sink, in chunks, then the digest (continued from the header's)
+void write_device(const Sink &out, const Context &c, const uint64_t *dev, size_t words, uint64_t h) {
     std::vector<uint64_t> buf(std::min(words, kChunkWords));
-    uint64_t h = kFnvBasis;
     for (size_t off = 0; off < words; off += buf.size()) {
         const size_t n = std::min(buf.size(), words - off);
         c.check(shm_memcpy(c.handle(), buf.data(), dev + off, n * 8, SHM_COPY_D2H, c.stream()));
@@ -126,10 +134,9 @@ void write_device(const Sink &out, const Context &c, const uint64_t *dev, size_t
 
 // source -> device words, in chunks; limb j of every [d2][N] block must be below primes[j]
 void read_device(const Source &in, const Context &c, uint64_t *dev, size_t words,
-                 const std::vector<uint64_t> &limb_primes) {
+                 const std::vector<uint64_t> &limb_primes, uint64_t h) {
     const size_t N = c.n, d2 = limb_primes.size();
     std::vector<uint64_t> buf(std::min(words, (kChunkWords / N) * N));
-    uint64_t h = kFnvBasis;
     for (size_t off = 0; off < words; off += buf.size()) {
         const size_t n = std::min(buf.size(), words - off);
         in(buf.data(), n * 8);
@@ -146,7 +153,7 @@ void read_device(const Source &in, const Context &c, uint64_t *dev, size_t words
     }
     uint64_t stored;
     in(&stored, 8);
-    if (stored != h) throw Error("payload digest mismatch: the record is corrupt");
+    if (stored != h) throw Error("digest mismatch: the record is corrupt");
 }
 
 std::vector<uint64_t> q_primes(const Context &c, uint32_t L) {
@@ -173,14 +180,13 @@ void key_record(const Sink &out, const Context &c, Kind k, const DeviceBuffer &k
     h.tag = tag;
     h.group = group;
     h.words = key.words();
-    write_header(out, h);
-    write_device(out, c, key.data(), key.words());
+    write_device(out, c, key.data(), key.words(), write_header(out, h));
 }
 
 DeviceBuffer key_payload(const Source &in, const Context &c, const Header &h, uint32_t d0, uint32_t d1) {
     if (h.d0 != d0 || h.d1 != d1 || h.d2 != c.nq + c.np) throw Error("key record has the wrong shape");
     DeviceBuffer key(c, h.words);
-    read_device(in, c, key.data(), h.words, qp_primes(c));
+    read_device(in, c, key.data(), h.words, qp_primes(c), h.digest);
     return key;
 }
 
@@ -208,8 +214,7 @@ void save(const Sink &out, const Context &c, const Ciphertext &ct) {
     h.scale = ct.scale_;
     h.words = ct.polys() * ct.L * c.n;
     if (ct.data.words() < h.words) throw Error("ciphertext buffer smaller than its shape");
-    write_header(out, h);
-    write_device(out, c, ct.data.data(), h.words);
+    write_device(out, c, ct.data.data(), h.words, write_header(out, h));
 }
 
 Ciphertext load_ciphertext(const Source &in, const Context &c) {
@@ -220,7 +225,7 @@ Ciphertext load_ciphertext(const Source &in, const Context &c) {
     if (!(h.flags & kFlagShared) && h.d1 > 3) throw Error("ciphertext size above 3");
     Ciphertext ct;
     ct.data = DeviceBuffer(c, h.words);
-    read_device(in, c, ct.data.data(), h.words, q_primes(c, h.d2));
+    read_device(in, c, ct.data.data(), h.words, q_primes(c, h.d2), h.digest);
     ct.count = h.d0;
     ct.size = h.d1;
     ct.L = h.d2;
@@ -239,8 +244,7 @@ void save_keys(const Sink &out, const Context &c, const KeySet &keys) {
         h.d1 = h.d2 = 1;
         h.group = (uint32_t)rows.size() - 1;
         h.words = rows.size() * c.n;
-        write_header(out, h);
-        uint64_t d = kFnvBasis;
+        uint64_t d = write_header(out, h);
         for (auto *r : rows) {
             if (r->size() != c.n) throw Error("secret has the wrong length");
             d = fnv(d, reinterpret_cast<const uint64_t *>(r->data()), c.n);
@@ -261,8 +265,7 @@ void save_keys(const Sink &out, const Context &c, const KeySet &keys) {
             for (auto &g : s.galois) key_record(out, c, Kind::SharedGaloisKey, g.second, c.dnum, m + 1, g.first, m);
         }
     Header end = base(c, Kind::End);
-    write_header(out, end);
-    const uint64_t d = kFnvBasis;
+    const uint64_t d = write_header(out, end);
     out(&d, 8);
 }
 
@@ -276,7 +279,7 @@ LoadedKeys load_keys(const Source &in, const Context &c) {
             case Kind::End: {
                 uint64_t d;
                 in(&d, 8);
-                if (d != kFnvBasis || h.words) throw Error("malformed end record");
+                if (d != h.digest || h.words) throw Error("malformed end record");
                 for (auto &kv : k.shared) {
                     bool complete = have_format[kv.first];
                     for (bool b : have_backward[kv.first]) complete = complete && b;
@@ -292,7 +295,7 @@ LoadedKeys load_keys(const Source &in, const Context &c) {
                 in(w.data(), h.words * 8);
                 uint64_t d;
                 in(&d, 8);
-                if (d != fnv(kFnvBasis, w.data(), w.size())) throw Error("payload digest mismatch: the record is corrupt");
+                if (d != fnv(h.digest, w.data(), w.size())) throw Error("digest mismatch: the record is corrupt");
                 auto row = [&](uint32_t r) {
                     std::vector<int64_t> s(c.n);
                     std::memcpy(s.data(), w.data() + (size_t)r * c.n, c.n * 8);

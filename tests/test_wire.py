@@ -82,7 +82,7 @@ def test_ciphertext_record_round_trip_and_layout():
     assert chain == _fnv(h.primes)
     assert (d0, d1, d2, flags, scale, words) == (2, 2, 4, 0, 2.0 ** 40, 2 * 2 * 4 * h.n)
     assert np.array_equal(payload.reshape(2, 2, 4, h.n), ct.to_host())
-    assert digest == _fnv(payload)
+    assert digest == _fnv(np.concatenate([np.frombuffer(blob[:HEADER.size], dtype=np.uint64), payload]))
     back = h.deserialize(blob)
     assert (back.count, back.size, back.level, back.scale, back.shared) == (2, 2, 4, 2.0 ** 40, False)
     assert np.array_equal(back.to_host(), ct.to_host())
@@ -100,7 +100,8 @@ def test_ciphertext_record_round_trip_and_layout():
 def _forge(blob, payload):
     """The record with `payload` in place of its own and the digest recomputed."""
     head = blob[:HEADER.size]
-    return head + payload.tobytes() + struct.pack("<Q", _fnv(payload))
+    words = np.concatenate([np.frombuffer(head, dtype=np.uint64), payload])
+    return head + payload.tobytes() + struct.pack("<Q", _fnv(words))
 
 
 def test_damaged_records_are_refused():
@@ -113,6 +114,11 @@ def test_damaged_records_are_refused():
         h.deserialize(bytes(bad))
     with pytest.raises(HostError, match="truncated"):
         h.deserialize(bytes(blob[:-9]))
+    for off in (48, 56, 63):  # tag, scale: fields no shape check reads are covered by the digest
+        bad = bytearray(blob)
+        bad[off] ^= 4
+        with pytest.raises(HostError, match="digest"):
+            h.deserialize(bytes(bad))
     with pytest.raises(HostError, match="bytes after"):
         h.deserialize(bytes(blob) + b"\0")
     bad = bytearray(blob)
