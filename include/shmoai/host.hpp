@@ -393,6 +393,13 @@ Ciphertext batch_gather(const Evaluator &ev, const std::vector<Ciphertext> &part
 // inverse square root above; 2 (d_newt + d_gold) + 8 levels
 Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &gamma,
                      const std::vector<double> &beta, int d_newt = 4, int d_gold = 2);
+// attention's ciphertext-ciphertext product in the column packing (ct_ct_matrix_mul_colpacking,
+// Ct_ct_matrix_mul.cuh:10-120): X and W batches of the same count; output batch of `rows`,
+// out_i = sum_j X_j * rot(W_j, i * num_batch) relinearised and rescaled (1 level); needs the
+// Galois keys of the steps i * num_batch
+Ciphertext ct_ct_matmul_colpacking(const Evaluator &ev, const Ciphertext &X, const Ciphertext &W, uint32_t rows,
+                                   uint32_t num_batch);
+
 // softmax over the members of a batch (softmax.cuh:119-, without the attention layout's masks):
 // e_i / sum_j e_j with e_i = exp_approx(x_i - shift) and the sum's inverse by inverse_approx on
 // sum_scale * sum_j e_j, which the caller brings into (0, 2); iter + 12 levels

@@ -119,6 +119,12 @@ int shm_host_layernorm(shm_host *h, const shm_ct *a, const double *gamma, const 
  * inverse by shm_host_inverse on sum_scale * sum_j e_j (the caller keeps it in (0, 2));
  * iter + 12 levels */
 int shm_host_softmax(shm_host *h, const shm_ct *a, double shift, double sum_scale, uint32_t iter, shm_ct **out);
+/* attention's ct-ct product in the column packing (ct_ct_matrix_mul_colpacking,
+ * matrix_mul/Ct_ct_matrix_mul.cuh:10-120): X and W batches of the same count, output batch of
+ * `rows` ciphertexts out_i = sum_j X_j * rot(W_j, i * num_batch), relinearised and rescaled;
+ * the Galois keys of the steps i * num_batch must have been generated */
+int shm_host_ct_ct_matmul(shm_host *h, const shm_ct *X, const shm_ct *W, uint32_t rows, uint32_t num_batch,
+                          shm_ct **out);
 /* a CUDA graph of shm_host_chebyshev (coeffs = NULL: GELU) on `in`; *out is rewritten by every
  * shm_host_graph_launch; write the next batch into `in` with shm_ct_write between launches */
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,

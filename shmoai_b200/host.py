@@ -103,6 +103,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_inv_sqrt": (i32, [_P, _P, _U32, _U32, pp]),
         "shm_host_layernorm": (i32, [_P, _P, dp, dp, _U32, _U32, pp]),
         "shm_host_softmax": (i32, [_P, _P, ctypes.c_double, ctypes.c_double, _U32, pp]),
+        "shm_host_ct_ct_matmul": (i32, [_P, _P, _P, _U32, _U32, pp]),
         "shm_host_chebyshev_capture": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp, pp]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
@@ -326,6 +327,10 @@ class Host:
     def softmax(self, a, shift: float, sum_scale: float, iter: int):
         """e_i / sum_j e_j over the batch's ciphertexts, e_i = exp(x_i - shift) as (1 + (x_i - shift)/128)^128."""
         return self._out(self.lib.shm_host_softmax, a._c, shift, sum_scale, iter)
+
+    def ct_ct_matmul(self, X, W, rows: int, num_batch: int):
+        """Column-packed ct-ct product: out_i = sum_j X_j * rot(W_j, i * num_batch), i < rows."""
+        return self._out(self.lib.shm_host_ct_ct_matmul, X._c, W._c, rows, num_batch)
 
     def capture_chebyshev(self, ct, coeffs=None, lo: float = 0.0, hi: float = 0.0):
         """A CUDA graph of chebyshev(ct, coeffs, lo, hi) (GELU when coeffs is None) and the output

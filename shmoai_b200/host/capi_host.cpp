@@ -278,6 +278,11 @@ int shm_host_softmax(shm_host *h, const shm_ct *a, double shift, double sum_scal
     return guard([&] { put(out, softmax_batch(*H(h).ev, C(a), shift, sum_scale, (int)iter)); });
 }
 
+int shm_host_ct_ct_matmul(shm_host *h, const shm_ct *X, const shm_ct *W, uint32_t rows, uint32_t num_batch,
+                          shm_ct **out) {
+    return guard([&] { put(out, ct_ct_matmul_colpacking(*H(h).ev, C(X), C(W), rows, num_batch)); });
+}
+
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,
                                double hi, shm_ct **out, shm_host_graph **graph) {
     return guard([&] {
