@@ -388,6 +388,7 @@ Ciphertext inv_sqrt_approx(const Evaluator &ev, const Ciphertext &x, int d_newt 
 // the sum of a batch's ciphertexts (one ciphertext), and one batch made of several
 Ciphertext batch_sum(const Evaluator &ev, const Ciphertext &x);
 Ciphertext batch_gather(const Evaluator &ev, const std::vector<Ciphertext> &parts);
+Ciphertext batch_broadcast(const Evaluator &ev, const Ciphertext &one, uint32_t count);  // count copies
 // LayerNorm over the hidden columns of the column packing, one column per ciphertext of the
 // batch (layernorm, layernorm.cuh:899-): gamma_i (x_i - mean) / sqrt(var) + beta_i with the
 // inverse square root above; 2 (d_newt + d_gold) + 8 levels
@@ -399,6 +400,15 @@ Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector
 // Galois keys of the steps i * num_batch
 Ciphertext ct_ct_matmul_colpacking(const Evaluator &ev, const Ciphertext &X, const Ciphertext &W, uint32_t rows,
                                    uint32_t num_batch);
+
+// attention's ct-ct product in the diagonal packing (ct_ct_matrix_mul_diagpacking,
+// Ct_ct_matrix_mul.cuh:182-): X holds the col_X = X.count diagonals, W the col_W = W.count
+// columns; baby-step giant-step with g = ceil(sqrt(col_X)), b = ceil(col_X / g): X's members
+// rotated by (col_X - i g) num_batch per giant step i, W's by j num_batch per baby step j,
+// products summed and relinearised-rescaled per giant step, giant-step results rotated by
+// j g num_batch and added (1 level); needs the Galois keys of those steps
+Ciphertext ct_ct_matmul_diagpacking(const Evaluator &ev, const Ciphertext &X, const Ciphertext &W,
+                                    uint32_t num_batch);
 
 // softmax over the members of a batch (softmax.cuh:119-, without the attention layout's masks):
 // e_i / sum_j e_j with e_i = exp_approx(x_i - shift) and the sum's inverse by inverse_approx on

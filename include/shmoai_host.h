@@ -125,6 +125,9 @@ int shm_host_softmax(shm_host *h, const shm_ct *a, double shift, double sum_scal
  * the Galois keys of the steps i * num_batch must have been generated */
 int shm_host_ct_ct_matmul(shm_host *h, const shm_ct *X, const shm_ct *W, uint32_t rows, uint32_t num_batch,
                           shm_ct **out);
+/* the diagonal-packed ct-ct product (ct_ct_matrix_mul_diagpacking, Ct_ct_matrix_mul.cuh:182-):
+ * X holds the diagonals, W the columns; output batch of W.count ciphertexts (1 level) */
+int shm_host_ct_ct_matmul_diag(shm_host *h, const shm_ct *X, const shm_ct *W, uint32_t num_batch, shm_ct **out);
 /* a CUDA graph of shm_host_chebyshev (coeffs = NULL: GELU) on `in`; *out is rewritten by every
  * shm_host_graph_launch; write the next batch into `in` with shm_ct_write between launches */
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,

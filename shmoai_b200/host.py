@@ -104,6 +104,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_layernorm": (i32, [_P, _P, dp, dp, _U32, _U32, pp]),
         "shm_host_softmax": (i32, [_P, _P, ctypes.c_double, ctypes.c_double, _U32, pp]),
         "shm_host_ct_ct_matmul": (i32, [_P, _P, _P, _U32, _U32, pp]),
+        "shm_host_ct_ct_matmul_diag": (i32, [_P, _P, _P, _U32, pp]),
         "shm_host_chebyshev_capture": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp, pp]),
         "shm_server_create": (i32, [_P, _P, ctypes.c_size_t, _U32, _U32, pp]),
         "shm_server_destroy": (None, [_P]),
@@ -331,6 +332,10 @@ class Host:
     def ct_ct_matmul(self, X, W, rows: int, num_batch: int):
         """Column-packed ct-ct product: out_i = sum_j X_j * rot(W_j, i * num_batch), i < rows."""
         return self._out(self.lib.shm_host_ct_ct_matmul, X._c, W._c, rows, num_batch)
+
+    def ct_ct_matmul_diag(self, X, W, num_batch: int):
+        """Diagonal-packed ct-ct product (baby-step giant-step over X's diagonals), W.count outputs."""
+        return self._out(self.lib.shm_host_ct_ct_matmul_diag, X._c, W._c, num_batch)
 
     def capture_chebyshev(self, ct, coeffs=None, lo: float = 0.0, hi: float = 0.0):
         """A CUDA graph of chebyshev(ct, coeffs, lo, hi) (GELU when coeffs is None) and the output

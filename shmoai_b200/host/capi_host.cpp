@@ -283,6 +283,10 @@ int shm_host_ct_ct_matmul(shm_host *h, const shm_ct *X, const shm_ct *W, uint32_
     return guard([&] { put(out, ct_ct_matmul_colpacking(*H(h).ev, C(X), C(W), rows, num_batch)); });
 }
 
+int shm_host_ct_ct_matmul_diag(shm_host *h, const shm_ct *X, const shm_ct *W, uint32_t num_batch, shm_ct **out) {
+    return guard([&] { put(out, ct_ct_matmul_diagpacking(*H(h).ev, C(X), C(W), num_batch)); });
+}
+
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,
                                double hi, shm_ct **out, shm_host_graph **graph) {
     return guard([&] {

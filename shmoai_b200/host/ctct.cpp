@@ -1,8 +1,11 @@
-// Ciphertext-ciphertext matrix product of the attention block in the column packing
+// Ciphertext-ciphertext matrix products of the attention block.  Column packing
 // (ct_ct_matrix_mul_colpacking, src/include/source/matrix_mul/Ct_ct_matrix_mul.cuh:10-120):
 // out_i = sum_j X_j * rot(W_j, i * num_batch), one relinearisation and rescale per output.
 // The rotations of W are hoisted (one ModUp of the whole W batch for every step) and the
 // products are summed unrelinearised (size 3), as the reference sums before relinearising.
+#include <algorithm>
+#include <cmath>
+
 #include "internal.hpp"
 
 namespace shmoai {
@@ -39,6 +42,55 @@ Ciphertext ct_ct_matmul_colpacking(const Evaluator &ev, const Ciphertext &X, con
         outs.push_back(ev.relinearize_rescale(sum_members(ev, ev.multiply_lazy(X, Wi))));
     }
     return batch_gather(ev, outs);
+}
+
+Ciphertext ct_ct_matmul_diagpacking(const Evaluator &ev, const Ciphertext &X, const Ciphertext &W,
+                                    uint32_t num_batch) {
+    if (X.shared || W.shared || X.size != 2 || W.size != 2) throw Error("ct-ct matmul takes ordinary ciphertexts");
+    const uint32_t col = X.count, cw = W.count;
+    if (col == 0 || cw == 0) throw Error("ct-ct matmul: empty batch");
+    const int64_t slots = ev.context().n / 2;
+    auto norm = [&](int64_t k) { return (int)(((k % slots) + slots) % slots); };
+    uint32_t g = (uint32_t)std::sqrt((double)col);
+    if (g * g < col) g++;
+    uint32_t b = col / g;
+    if (b * g < col) b++;
+    // giant-step groups of X: members i g .. i g + g - 1 rotated by (col - i g) num_batch
+    std::vector<Ciphertext> rx;  // one batch per giant step
+    for (uint32_t i = 0; i < b; i++) {
+        const uint32_t lo = i * g, cnt = std::min(g, col - lo);
+        Ciphertext grp = ev.slice(X, lo, cnt);
+        const int step = norm((int64_t)(col - i * g) * num_batch);
+        if (i == 0 || step == 0) {
+            rx.push_back(std::move(grp));
+        } else {
+            auto r = ev.rotate_many(grp, {step});
+            rx.push_back(std::move(r.at(step)));
+        }
+    }
+    // baby steps of W: rot(W, j num_batch), j < g, hoisted over the whole W batch
+    std::vector<int> bsteps;
+    for (uint32_t j = 1; j < g; j++) bsteps.push_back(norm((int64_t)j * num_batch));
+    const std::map<int, Ciphertext> wr = ev.rotate_many(W, bsteps);
+    auto baby = [&](uint32_t j) -> const Ciphertext & {
+        const int st = j ? norm((int64_t)j * num_batch) : 0;
+        auto it = wr.find(st);
+        return (j == 0 || it == wr.end()) ? W : it->second;
+    };
+    Ciphertext total;
+    for (uint32_t i = 0; i < b; i++) {
+        Ciphertext acc;
+        for (uint32_t k = 0; k < g && i * g + k < col; k++) {
+            const Ciphertext xk = ev.slice(rx[i], k, 1);
+            Ciphertext p = ev.multiply_lazy(baby(k), batch_broadcast(ev, xk, cw));
+            acc = acc.count ? ev.add(acc, p) : std::move(p);
+        }
+        Ciphertext o = ev.relinearize_rescale(acc);
+        const int gs = norm((int64_t)i * g * num_batch);
+        if (i > 0 && gs != 0) o = std::move(ev.rotate_many(o, {gs}).at(gs));
+        total = total.count ? ev.add(total, o) : std::move(o);
+    }
+    return total;
 }
 
 }  // namespace shmoai

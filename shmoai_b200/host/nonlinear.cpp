@@ -134,6 +134,11 @@ static Ciphertext gather_ptrs(const Evaluator &ev, const std::vector<const Ciphe
     return o;
 }
 
+Ciphertext batch_broadcast(const Evaluator &ev, const Ciphertext &one, uint32_t count) {
+    if (count == 0) throw Error("broadcast to an empty batch");
+    return gather_ptrs(ev, std::vector<const Ciphertext *>(count, &one));
+}
+
 Ciphertext batch_gather(const Evaluator &ev, const std::vector<Ciphertext> &parts) {
     std::vector<const Ciphertext *> p;
     for (const Ciphertext &x : parts) p.push_back(&x);
