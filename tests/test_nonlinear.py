@@ -127,13 +127,15 @@ def test_inv_sqrt_is_the_reference_iteration():
         h.inv_sqrt(h.encrypt(x, DELTA, 15))
 
 
-def test_layernorm_over_the_hidden_columns():
-    """LayerNorm of 8 hidden columns (one per ciphertext): mean and variance over the batch,
-    the reference's inverse square root, gamma and beta per column; decryptions equal numpy's
-    run of the same arithmetic; 2 (4 + 2) + 8 = 20 levels."""
+@pytest.mark.parametrize("d", [5, 8])
+def test_layernorm_over_the_hidden_columns(d):
+    """LayerNorm of d hidden columns (one per ciphertext; an odd d exercises the batch sum's
+    carried member): mean and variance over the batch, the reference's inverse square root,
+    gamma and beta per column; decryptions equal numpy's run of the same arithmetic;
+    2 (4 + 2) + 8 = 20 levels."""
     h = _host(bits=[51] + [46] * 19 + [51] + [51] * 5)
-    rng = np.random.default_rng(10)
-    d, n = 8, h.n // 2
+    rng = np.random.default_rng(10 + d)
+    n = h.n // 2
     z = rng.standard_normal((d, n))
     z = (z - z.mean(axis=0)) / z.std(axis=0)  # per slot: mean 0, variance 1 over the columns
     sigma = rng.uniform(2.0, 20.0, n)  # so that var = sigma^2 lies in [4, 400], inside the guess's range
