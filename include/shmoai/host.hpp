@@ -410,6 +410,12 @@ Ciphertext ct_ct_matmul_colpacking(const Evaluator &ev, const Ciphertext &X, con
 Ciphertext ct_ct_matmul_diagpacking(const Evaluator &ev, const Ciphertext &X, const Ciphertext &W,
                                     uint32_t num_batch);
 
+// the attention block's softmax with its masks (softmax, softmax.cuh:119-): the batch's members
+// are the diagonals, bias_vec (one 0/1 per slot) marks the valid token slots, input_num the
+// reference's band; shifts by -8.1, exp, mask subtraction, the inverse of the sum (iter
+// steps) times each member; iter + 10 levels
+Ciphertext softmax_attention(const Evaluator &ev, const Ciphertext &x, const std::vector<int> &bias_vec,
+                             int input_num, int iter);
 // softmax over the members of a batch (softmax.cuh:119-, without the attention layout's masks):
 // e_i / sum_j e_j with e_i = exp_approx(x_i - shift) and the sum's inverse by inverse_approx on
 // sum_scale * sum_j e_j, which the caller brings into (0, 2); iter + 12 levels

@@ -119,6 +119,11 @@ int shm_host_layernorm(shm_host *h, const shm_ct *a, const double *gamma, const 
  * inverse by shm_host_inverse on sum_scale * sum_j e_j (the caller keeps it in (0, 2));
  * iter + 12 levels */
 int shm_host_softmax(shm_host *h, const shm_ct *a, double shift, double sum_scale, uint32_t iter, shm_ct **out);
+/* the attention block's softmax with its masks (softmax, non_linear_func/softmax.cuh:119-):
+ * bias_vec has one 0/1 entry per slot (N/2), input_num is the reference's band of diagonals;
+ * iter + 10 levels */
+int shm_host_softmax_attention(shm_host *h, const shm_ct *a, const int *bias_vec, int input_num, uint32_t iter,
+                               shm_ct **out);
 /* attention's ct-ct product in the column packing (ct_ct_matrix_mul_colpacking,
  * matrix_mul/Ct_ct_matrix_mul.cuh:10-120): X and W batches of the same count, output batch of
  * `rows` ciphertexts out_i = sum_j X_j * rot(W_j, i * num_batch), relinearised and rescaled;

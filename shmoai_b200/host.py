@@ -103,6 +103,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_inv_sqrt": (i32, [_P, _P, _U32, _U32, pp]),
         "shm_host_layernorm": (i32, [_P, _P, dp, dp, _U32, _U32, pp]),
         "shm_host_softmax": (i32, [_P, _P, ctypes.c_double, ctypes.c_double, _U32, pp]),
+        "shm_host_softmax_attention": (i32, [_P, _P, ctypes.POINTER(ctypes.c_int), i32, _U32, pp]),
         "shm_host_ct_ct_matmul": (i32, [_P, _P, _P, _U32, _U32, pp]),
         "shm_host_ct_ct_matmul_diag": (i32, [_P, _P, _P, _U32, pp]),
         "shm_host_chebyshev_capture": (i32, [_P, _P, dp, _U32, ctypes.c_double, ctypes.c_double, pp, pp]),
@@ -328,6 +329,14 @@ class Host:
     def softmax(self, a, shift: float, sum_scale: float, iter: int):
         """e_i / sum_j e_j over the batch's ciphertexts, e_i = exp(x_i - shift) as (1 + (x_i - shift)/128)^128."""
         return self._out(self.lib.shm_host_softmax, a._c, shift, sum_scale, iter)
+
+    def softmax_attention(self, a, bias_vec, input_num: int, iter: int):
+        """The attention block's softmax with the reference's masks (bias_vec: one 0/1 per slot)."""
+        b = np.ascontiguousarray(bias_vec, dtype=np.int32)
+        if b.size != self.n // 2:
+            raise ValueError("bias_vec needs one entry per slot")
+        return self._out(self.lib.shm_host_softmax_attention, a._c, b.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                         input_num, iter)
 
     def ct_ct_matmul(self, X, W, rows: int, num_batch: int):
         """Column-packed ct-ct product: out_i = sum_j X_j * rot(W_j, i * num_batch), i < rows."""

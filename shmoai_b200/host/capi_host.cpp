@@ -287,6 +287,16 @@ int shm_host_ct_ct_matmul_diag(shm_host *h, const shm_ct *X, const shm_ct *W, ui
     return guard([&] { put(out, ct_ct_matmul_diagpacking(*H(h).ev, C(X), C(W), num_batch)); });
 }
 
+int shm_host_softmax_attention(shm_host *h, const shm_ct *a, const int *bias_vec, int input_num, uint32_t iter,
+                               shm_ct **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!bias_vec) throw Error("null bias_vec");
+        put(out, softmax_attention(*hh.ev, C(a), std::vector<int>(bias_vec, bias_vec + hh.ctx->n / 2), input_num,
+                                   (int)iter));
+    });
+}
+
 int shm_host_chebyshev_capture(shm_host *h, const shm_ct *in, const double *coeffs, uint32_t n_coeffs, double lo,
                                double hi, shm_ct **out, shm_host_graph **graph) {
     return guard([&] {

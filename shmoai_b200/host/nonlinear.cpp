@@ -188,4 +188,65 @@ Ciphertext softmax_batch(const Evaluator &ev, const Ciphertext &x, double shift,
     return ev.multiply_const(y, sum_scale, S);
 }
 
+namespace {
+
+// member i of the batch gets the slot vector v_i added (encoded at the batch's level and scale;
+// an empty vector adds nothing): c0 += encode(v_i) on every limb
+Ciphertext add_slot_vectors(const Evaluator &ev, const Ciphertext &a, const std::vector<std::vector<double>> &v) {
+    const Context &c = ev.context();
+    Ciphertext o = ev.slice(a, 0, a.count);
+    const size_t per = (size_t)a.size * a.L * c.n;
+    for (uint32_t i = 0; i < a.count; i++) {
+        if (v[i].empty()) continue;
+        std::vector<cplx> z(v[i].begin(), v[i].end());
+        const Plaintext p = ev.encoder().encode(z, a.L, a.scale_);
+        uint64_t *c0 = o.data.data() + i * per;
+        c.check(shm_add(c.handle(), c0, p.data.data(), c0, 1, a.L, c.stream()));
+    }
+    return o;
+}
+
+}  // namespace
+
+// softmax of the attention block (softmax, softmax.cuh:119-): member i of the batch is shifted
+// by -8.1 on the bias slots its position selects (all of them for i = 0; slots below
+// num_batch (input_num - i) for 1 <= i <= input_num; none in the middle; slots from
+// num_batch (num - i) on for i > num - input_num), exponentiated, and has 1 taken off every
+// slot except those same bias slots; the members' sum is inverted (inverse_approx, iter) and
+// multiplies each member.  num_batch = slots / 128.  iter + 10 levels.
+Ciphertext softmax_attention(const Evaluator &ev, const Ciphertext &x, const std::vector<int> &bias_vec,
+                             int input_num, int iter) {
+    need_ordinary(x, "softmax");
+    const Context &c = ev.context();
+    const size_t slots = c.n / 2;
+    if (bias_vec.size() != slots) throw Error("softmax: bias_vec needs one entry per slot");
+    const uint32_t need = (uint32_t)iter + 11;
+    if (x.L < need) throw Error("softmax needs " + std::to_string(need) + " primes");
+    const int num = (int)x.count, nb = (int)(slots / 128);
+    // which bias slots member i treats as its own: all (i = 0), a prefix, none, or a suffix
+    auto selected = [&](int i, size_t s) {
+        if (bias_vec[s] != 1) return false;
+        if (i == 0) return true;
+        if (i > input_num && i <= num - input_num) return false;
+        if (i <= input_num) return (long long)s < (long long)nb * (input_num - i);
+        return (long long)s >= (long long)(num - i) * nb;
+    };
+    std::vector<std::vector<double>> shift(num), sub(num);
+    for (int i = 0; i < num; i++) {
+        std::vector<double> sh(slots, 0.0), sb(slots, -1.0);
+        bool any = false;
+        for (size_t s = 0; s < slots; s++)
+            if (selected(i, s)) {
+                sh[s] = -8.1;
+                sb[s] = 0.0;
+                any = true;
+            }
+        if (any) shift[i] = std::move(sh);
+        sub[i] = std::move(sb);
+    }
+    const Ciphertext e = add_slot_vectors(ev, exp_approx(ev, add_slot_vectors(ev, x, shift)), sub);
+    const Ciphertext inv = inverse_approx(ev, batch_sum(ev, e), iter);
+    return product(ev, e, gather_ptrs(ev, std::vector<const Ciphertext *>(x.count, &inv)));
+}
+
 }  // namespace shmoai

@@ -173,6 +173,57 @@ def test_softmax_over_the_batch():
         h.softmax(h.encrypt(x, DELTA, 19), shift, sum_scale, it)
 
 
+def _softmax_attention_reference(x, bias, input_num, it):
+    """softmax.cuh:119-'s masks and arithmetic on slot vectors."""
+    num, slots = x.shape
+    nb = slots // 128
+    idx = np.arange(slots)
+
+    def selected(i):
+        if i == 0:
+            return bias == 1
+        if input_num < i <= num - input_num:
+            return np.zeros(slots, dtype=bool)
+        if i <= input_num:
+            return (bias == 1) & (idx < nb * (input_num - i))
+        return (bias == 1) & (idx >= (num - i) * nb)
+
+    e = []
+    for i in range(num):
+        sel = selected(i)
+        v = x[i] - 8.1 * sel
+        e.append((1 + v / 128) ** 128 - np.where(sel, 0.0, 1.0))
+    e = np.stack(e)
+    s = e.sum(axis=0)
+    y, r = 1 - s, 2 - s
+    for _ in range(it):
+        y = y * y
+        r = r * (1 + y)
+    return e * r
+
+
+def test_softmax_attention_is_the_reference_arithmetic():
+    """The attention block's softmax with its masks: 6 diagonals, input_num 2, valid token
+    slots marked by bias_vec (padding slots hold 0); decryptions equal numpy's run of the
+    reference's masks and formulas; iter + 10 levels."""
+    h = _host(bits=[51] + [46] * 23 + [51] + [51] * 5)
+    rng = np.random.default_rng(13)
+    slots, num, it = h.n // 2, 6, 13
+    bias = (np.arange(slots) < 1500).astype(np.int32)
+    # scores in [0, 0.05] keep every slot's sum in (0, 2), where the inverse converges
+    x = np.where(bias == 1, rng.uniform(0.0, 0.05, (num, slots)), 0.0)
+    out = h.softmax_attention(h.encrypt(x, DELTA, 25), bias, 2, it)
+    assert out.count == num and out.level == 25 - it - 10
+    want = _softmax_attention_reference(x, bias, 2, it)
+    err = np.abs(h.decrypt(out).real - want)
+    assert err[:, bias == 1].max() < 1e-6
+    # padding slots: their sum is 0, so the inverse is 2^(iter + 1) and scales the noise of
+    # values that are 0 (the reference's caller masks these slots out)
+    assert err[:, bias == 0].max() < 1e-3
+    with pytest.raises(HostError, match="needs 24 primes"):
+        h.softmax_attention(h.encrypt(x, DELTA, 23), bias, 2, it)
+
+
 def test_polynomial_operators_refuse_bad_inputs(small):
     h = small
     rng = np.random.default_rng(4)
