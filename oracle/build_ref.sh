@@ -14,8 +14,9 @@
 # elsewhere the script does nothing.  Set SHMOAI_REF_GPU=0 to skip the
 # (slow, ~minutes) GPU build.
 set -euo pipefail
-REF=${SHMOAI_REFERENCE:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+# the reference tree: $SHMOAI_REFERENCE, else a checkout named "reference" beside the repository
+REF=${SHMOAI_REFERENCE:-$(cd "$HERE/../.." && pwd)/reference}
 OUT=$HERE/_ref
 PH=$REF/thirdparty/phantom-fhe
 if [ ! -d "$PH" ]; then

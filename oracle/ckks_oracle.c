@@ -719,7 +719,9 @@ void orc_shared_rotate_ext(const orc_ctx *c, const uint64_t *in, int in_ext, uin
 
 /* Exact extension of a (NTT form, L limbs) to QlP: the Ql rows keep a, the P rows get
  * (sum_i y_i qhat_i - v Q) mod p_k with y_i = [x_i qhat_i^-1]_{q_i} (x = INTT(a)) and
- * v = floor(sum_i y_i / q_i) in double arithmetic (FmtSwitch.cu:82-108). */
+ * v = floor(sum_i y_i / q_i) in double arithmetic as FmtSwitch.cu:86-106 computes it: the
+ * quotients y_i / q_i summed in limb order, truncated, and raised by one where the sum is
+ * within 1e-9 below the next integer. */
 static void exact_extend(const orc_ctx *c, const uint64_t *a, uint32_t L, uint64_t *ext) {
     size_t n = c->n;
     uint32_t LP = L + c->np;
@@ -751,17 +753,25 @@ static void exact_extend(const orc_ctx *c, const uint64_t *a, uint32_t L, uint64
             u128 acc = 0;
             for (uint32_t i = 0; i < L; i++) {
                 uint64_t yi = y[(size_t)i * n + t];
-                double prod = (double)yi * (1.0 / (double)c->primes[i]);
-                frac = frac + prod;
+                frac = frac + (double)yi / (double)c->primes[i];
                 acc += (u128)yi * hm[i];
             }
             uint64_t v = (uint64_t)frac;
+            if (frac - (double)v > 1.0 - 1e-9) v += 1;
             o[t] = submod((uint64_t)(acc % p), mulmod(v, Qm, p), p);
         }
         orc_ntt_fwd(o, c->log_n, p, c->rp + (size_t)pk * n);
     }
     (void)LP;
     free(y);
+}
+
+/* The exact extension alone, for n_polys polynomials [n_polys][L][N] (NTT form) into
+ * [n_polys][L + np][N] (the extension step of FmtSwitch.cu:317-329). */
+void orc_exact_extend(const orc_ctx *c, const uint64_t *a, uint32_t n_polys, uint32_t L, uint64_t *ext) {
+    size_t n = c->n;
+    for (uint32_t p = 0; p < n_polys; p++)
+        exact_extend(c, a + (size_t)p * L * n, L, ext + (size_t)p * (L + c->np) * n);
 }
 
 /* FmtSwitch forward (FmtSwitch.cu:276-394) of one group: cts [n][2][L][N] under s ->

@@ -72,6 +72,7 @@ def lib():
         L.orc_shared_rotate_hoisted.argtypes = [vp, _u64p, u32, u32, u32, ctypes.POINTER(ctypes.c_uint32),
                                                 ctypes.POINTER(_u64p), ctypes.POINTER(_u64p)]
         L.orc_fmt_forward.argtypes = [vp, _u64p, u32, u32, _u64p, _u64p]
+        L.orc_exact_extend.argtypes = [vp, _u64p, u32, u32, _u64p]
         L.orc_fmt_backward.argtypes = [vp, _u64p, u32, u32, ctypes.POINTER(_u64p), _u64p]
         L.orc_signed_residue.argtypes = [ctypes.c_int64, u64]
         L.orc_signed_residue.restype = u64
@@ -223,6 +224,16 @@ class Oracle:
         op = (_u64p * len(outs))(*[_p(o) for o in outs])
         lib().orc_shared_rotate_hoisted(self._h, _p(sh), H - 1, L, len(elts), e, kp, op)
         return outs
+
+    def exact_extend(self, a):
+        """[..][L][N] NTT-form polynomials -> [..][L + np][N]: the Ql rows copied, the P rows
+        the floor-corrected CRT extension of FmtSwitch.cu:86-106 (NTT form)."""
+        L = a.shape[-2]
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        m = int(np.prod(a.shape[:-2], dtype=np.int64))
+        out = np.empty(a.shape[:-2] + (L + self.np, self.n), dtype=np.uint64)
+        lib().orc_exact_extend(self._h, _p(a), m, L, _p(out))
+        return out
 
     def fmt_forward(self, cts, key):
         """[n][2][L][N] ciphertexts under s -> one shared-a group [n+1][L][N]."""

@@ -142,9 +142,11 @@ size_t rescale_ws_words(const Context &c, uint32_t n_polys, uint32_t L) {
 void rescale(const Context &c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L, uint64_t *ws,
              cudaStream_t st) {
     if (L < 2) throw std::invalid_argument("rescale needs at least two limbs");
+    if (n_polys == 0) return;  // nothing to do; a grid with y = 0 would be an invalid launch
     uint64_t *last = ws, *t = ws + ((size_t)n_polys << c.log_n);
     const uint32_t chunks = c.n / kEwThreads;
     SHM_LAUNCHED(1); gather_last<<<dim3(chunks, n_polys), kEwThreads, 0, st>>>(in, last, L, c.log_n);
+    SHM_CUDA(cudaGetLastError());
     LimbMap m;
     for (int i = 0; i < 512; i++) m.prime[i] = 255;
     m.prime[0] = (uint8_t)(L - 1);

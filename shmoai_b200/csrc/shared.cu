@@ -86,9 +86,12 @@ struct Target {
 };
 
 // exact Ql -> P extension (floor-corrected CRT): x = sum_i y_i qhat_i - v Q, v = floor(sum_i y_i / q_i),
-// y_i = [x_i qhat_i^-1]_{q_i} already in the coefficient buffer; writes the P rows of ext
+// y_i = [x_i qhat_i^-1]_{q_i} already in the coefficient buffer; writes the P rows of ext.
+// v follows FmtSwitch.cu:86-106 operation for operation: the double sum of the correctly rounded
+// quotients y_i / q_i in limb order (no contraction), truncated, plus one where the sum lies
+// within 1e-9 below the next integer.
 __global__ void exact_ext_kernel(const uint64_t *__restrict__ y, uint64_t *__restrict__ ext, const uint64_t *__restrict__ tab,
-                                 const double *__restrict__ qinv, uint32_t L, uint32_t np, uint32_t nq, uint32_t log_n,
+                                 const double *__restrict__ qd, uint32_t L, uint32_t np, uint32_t nq, uint32_t log_n,
                                  const PrimeConst *__restrict__ pc) {
     const uint32_t poly = blockIdx.y;
     const uint32_t k = blockIdx.x * kT + threadIdx.x;
@@ -98,9 +101,10 @@ __global__ void exact_ext_kernel(const uint64_t *__restrict__ y, uint64_t *__res
     double frac = 0.0;
     for (uint32_t i = 0; i < L; i++) {
         yv[i] = yp[(size_t)i * n];
-        frac = __dadd_rn(frac, __dmul_rn((double)yv[i], qinv[i]));  // no contraction: reproducible
+        frac = __dadd_rn(frac, __ddiv_rn((double)yv[i], qd[i]));  // no contraction: reproducible
     }
-    const uint64_t v = (uint64_t)frac;
+    uint64_t v = (uint64_t)frac;
+    if (__dsub_rn(frac, (double)v) > 1.0 - 1e-9) v += 1;
     uint64_t *o = ext + (size_t)poly * (L + np) * n + (size_t)L * n + k;
     for (uint32_t kk = 0; kk < np; kk++) {
         const uint64_t *row = tab + (size_t)kk * (L + 1);  // qhat_i mod p_k (L values), Q mod p_k
@@ -120,7 +124,7 @@ namespace {
 struct ExtConsts {
     uint64_t *scale = nullptr;  // [L][4] inverse-NTT last-stage constants with qhat_i^-1 folded
     uint64_t *tab = nullptr;    // [np][L+1]
-    double *qinv = nullptr;     // [L]
+    double *qd = nullptr;       // [L] the primes as doubles
 };
 
 ExtConsts ext_consts(Context &c, uint32_t L) {
@@ -139,7 +143,7 @@ ExtConsts ext_consts(Context &c, uint32_t L) {
         SHM_CUDA(cudaMemcpy(&psi_half_inv, c.tw + (size_t)i * 4 * c.n + 2 * c.n + 1, 8, cudaMemcpyDeviceToHost));
         uint64_t c1 = host::mulmod(cc, psi_half_inv, q);
         sc.insert(sc.end(), {cc, host::shoup_of(cc, q), c1, host::shoup_of(c1, q)});
-        qi[i] = 1.0 / (double)q;
+        qi[i] = (double)q;
     }
     for (uint32_t k = 0; k < c.np; k++) {
         uint64_t p = c.primes[c.nq + k], Qm = 1;
@@ -153,9 +157,9 @@ ExtConsts ext_consts(Context &c, uint32_t L) {
     SHM_CUDA(cudaMemcpy(e.scale, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice));
     SHM_CUDA(cudaMalloc(&e.tab, tab.size() * 8));
     SHM_CUDA(cudaMemcpy(e.tab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice));
-    SHM_CUDA(cudaMalloc(&e.qinv, qi.size() * 8));
-    SHM_CUDA(cudaMemcpy(e.qinv, qi.data(), qi.size() * 8, cudaMemcpyHostToDevice));
-    c.ext_consts[L] = {e.scale, e.tab, e.qinv};
+    SHM_CUDA(cudaMalloc(&e.qd, qi.size() * 8));
+    SHM_CUDA(cudaMemcpy(e.qd, qi.data(), qi.size() * 8, cudaMemcpyHostToDevice));
+    c.ext_consts[L] = {e.scale, e.tab, e.qd};
     return e;
 }
 
@@ -265,7 +269,7 @@ void fmt_forward(const Context &c, const uint64_t *cts, uint32_t n_groups, uint3
     ntt_inverse(c, y, m * L, L, q_map(L), e.scale, st);
     SHM_CUDA(cudaMemcpy2DAsync(ext, LP * N * 8, cts + ln, 2 * ln * 8, ln * 8, m, cudaMemcpyDeviceToDevice, st));
     SHM_LAUNCHED(1);
-    exact_ext_kernel<<<dim3(N / kT, m), kT, 0, st>>>(y, ext, e.tab, e.qinv, L, c.np, c.nq, c.log_n, c.pc);
+    exact_ext_kernel<<<dim3(N / kT, m), kT, 0, st>>>(y, ext, e.tab, e.qd, L, c.np, c.nq, c.log_n, c.pc);
     SHM_CUDA(cudaGetLastError());
     LimbMap mp;
     for (uint32_t s = 0; s < 512; s++) mp.prime[s] = (s >= L && s < LP) ? (uint8_t)(c.nq + (s - L)) : 255;
