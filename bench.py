@@ -26,9 +26,14 @@ Multi-GPU: ciphertexts are independent, so each rank bootstraps its own batch
 
 --impl reference: the reference has no CPU implementation of these operations,
 so the CPU arm is the oracle (oracle/ckks_oracle.c, a scalar OpenMP restatement
-of the reference's arithmetic) on all host cores: for boot, one (Sh-)rotation at the
-C2S level and at the S2C level and one relinearisation at the EvalMod level per
-step, scaled by the bootstrap's own count of rotations and relinearisations.
+of the reference's arithmetic) on all host cores: for boot, the C++ host library
+built on the oracle runs one full bootstrap of the configured form (a shared-a
+group of n, or one ordinary ciphertext), timed once and reported as one step.
+
+The boot line also carries, after its timed region, the reference's own GPU build
+(PhantomFHE + moai adapter for sm_100a, oracle/_ref/ref_golden) timed on the same
+GPU on single-ciphertext calls and its per-ciphertext ct-pt loop, beside this
+library's kernels on the same calls ("reference_gpu", "ours_same_calls").
 """
 from __future__ import annotations
 
@@ -175,15 +180,121 @@ def ntt_roofline(torch, ctx, L, limbs_target=4096):
     torch.cuda.synchronize()
     ms = s.elapsed_time(e) / reps
     limbs = rows * L
-    algo = limbs * n * 8 * 2 * 2  # two phase kernels, each reads and writes every word once
+    algo = limbs * n * 8 * 2  # one transform reads and writes every word of every limb once: 16N bytes per limb
     peak, kind = measured_peaks()
     achieved = algo / (ms * 1e-3) / 1e9
     tr = traffic_from_profiles("ntt_forward_pair_bytes_per_limb")
+    traffic = None if tr is None else round(tr * limbs)
     return {"kernel": "ntt forward (fwd_col + fwd_blk launch pair), batched limbs", "bound": "hbm",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "peak_source": kind, "traffic": None if tr is None else round(tr * limbs),
-            "algorithmic_bytes_per_launch_pair": algo, "limbs_per_launch": limbs,
-            "launch_pair_ms": round(ms, 4)}
+            "peak_source": kind, "traffic": traffic,
+            "traffic_over_algorithmic": None if traffic is None else round(traffic / algo, 3),
+            "algorithmic_bytes_per_launch_pair": algo, "algorithmic_bytes_per_limb": n * 16,
+            "limbs_per_launch": limbs, "launch_pair_ms": round(ms, 4)}
+
+
+# ---------------------------------------------------------------------------
+# the reference's own GPU build on this GPU, beside the same calls of this library
+
+REF_GOLDEN = os.path.join(ROOT, "oracle", "_ref", "ref_golden")
+
+
+def _json_doc(text: str):
+    """The JSON document in a harness output (the reference prints a debug line of its own)."""
+    keep = [ln for ln in text.splitlines() if ln[:1] in ("{", "}", " ") or ln == ""]
+    return json.loads("\n".join(keep))
+
+
+def reference_gpu_leg(ctpt_cols: int = 64):
+    """Times the reference's PhantomFHE + moai adapter built for sm_100a from the reference sources
+    (oracle/_ref/ref_golden, mode `time`) on this GPU with CUDA events: at the config-1 chain (N = 2^16,
+    [60] + 23 x [50] + 8 x [60], dnum 3) one ciphertext's inverse + forward NTT, HRotate by one slot and
+    multiply + relinearize + rescale; the same calls at the bootstrapping chain's top level (35 primes,
+    dnum 7); and the per-ciphertext ct-pt loop of Ct_pt_matrix_mul.cuh:85-158 for 768 inputs at 13 limbs
+    and the first `ctpt_cols` output columns (OpenMP over columns, one stream per thread)."""
+    if not os.path.exists(REF_GOLDEN):
+        return {"unavailable": "oracle/_ref/ref_golden was not built (no reference tree at build time)"}
+    out = {"build": "reference PhantomFHE + moai adapter, nvcc -arch sm_100a -rdc (oracle/build_ref.sh)",
+           "timing": "CUDA events on the reference's stream, 3 warm-up + 20 calls; ct-pt loop by wall clock "
+                     "around a device synchronize"}
+    for name, cols in (("prim", 0), ("boot", ctpt_cols)):
+        try:
+            r = subprocess.run([REF_GOLDEN, name, "time", str(cols)], capture_output=True, text=True, timeout=900)
+            if r.returncode != 0:
+                out[name] = {"error": (r.stderr or r.stdout)[-300:]}
+                continue
+            out[name] = _json_doc(r.stdout)["time"]
+        except Exception as e:  # reported, not fatal: the leg is a side measurement
+            out[name] = {"error": repr(e)[:300]}
+    c = out.get("boot", {}).get("ctpt_loop")
+    if c:
+        c["output_cts_per_s"] = round(c["n_out"] * 1000.0 / c["ms"], 3)
+    return out
+
+
+def ours_per_ct_leg(dev: int, ctpt_cols: int = 64):
+    """This library's kernels on the calls the reference leg times, one ciphertext per call (eager, CUDA
+    events, 3 warm-up + 20 calls): inverse + forward NTT, HRotate by one slot, multiply + relinearize +
+    rescale at the config-1 chain and at the bootstrapping chain's top level; and the ct-pt matmul of 768
+    inputs at 13 limbs into `ctpt_cols` outputs on the INT8 tensor cores."""
+    import torch
+
+    from shmoai_b200.ckks import CKKSContext
+
+    res = {}
+    for name, P in (("prim", PRIM), ("boot", BOOT)):
+        ctx = CKKSContext(P["log_n"], bits=P["bits"], n_special=P["n_special"], device=dev)
+        n, L, QP, dnum = ctx.n, ctx.nq, ctx.nq + ctx.np, ctx.dnum
+        g = torch.Generator(device="cuda").manual_seed(77)
+        pt = torch.tensor(ctx.primes.astype(np.int64), device="cuda")
+
+        def residues(shape, primes):
+            x = torch.randint(0, 2 ** 62, shape, device="cuda", generator=g, dtype=torch.int64)
+            return torch.remainder(x, primes.view(*([1] * (len(shape) - 2)), -1, 1))
+
+        A, B = residues((2, L, n), pt[:L]), residues((2, L, n), pt[:L])
+        gk, rk = residues((dnum, 2, QP, n), pt), residues((dnum, 2, QP, n), pt)
+        ws = torch.empty(max(ctx.workspace_bytes("keyswitch", 1, L) // 8 + 2 * L * n,
+                             ctx.workspace_bytes("rescale", 2, L) // 8), dtype=torch.int64, device="cuda")
+        rot, rel = torch.empty_like(A), torch.empty_like(A)
+        m = torch.empty(3, L, n, dtype=torch.int64, device="cuda")
+        outr = torch.empty(2, L - 1, n, dtype=torch.int64, device="cuda")
+
+        def ntt():
+            ctx.ntt_inverse_(A)
+            ctx.ntt_forward_(A)
+
+        def mrr():
+            ctx.multiply(A, B, out=m)
+            ctx.relinearize(m, rk, out=rel, workspace=ws)
+            ctx.rescale(rel, out=outr, workspace=ws)
+
+        t = {"limbs": L}
+        for key, fn in (("ntt_inv_fwd_ms", ntt), ("rotate1_ms", lambda: ctx.rotate(A, 1, gk, out=rot, workspace=ws)),
+                        ("mul_relin_rescale_ms", mrr)):
+            for _ in range(3):
+                fn()
+            t[key] = round(timed_steps(torch, fn, 20, None, None), 4)
+        t["chain_ms"] = round(t["ntt_inv_fwd_ms"] + t["rotate1_ms"] + t["mul_relin_rescale_ms"], 4)
+        if name == "boot" and ctpt_cols:
+            Lc = CTPT["L"]
+            X = residues((CTPT["n_in"], 2, Lc, n), pt[:Lc])
+            W = torch.round(torch.randn(CTPT["n_in"], ctpt_cols, device="cuda", generator=g, dtype=torch.float64)
+                            * 0.02 * 2 ** 40).to(torch.int64)
+            wsm = torch.empty(ctx.workspace_bytes("ctpt", CTPT["n_in"], Lc, ctpt_cols) // 8 + 1, dtype=torch.int64,
+                              device="cuda")
+            Y = torch.empty(ctpt_cols, 2, Lc, n, dtype=torch.int64, device="cuda")
+            mm = lambda: ctx.ctpt_matmul(X, W, out=Y, workspace=wsm)  # noqa: E731
+            for _ in range(3):
+                mm()
+            ms = timed_steps(torch, mm, 5, None, None)
+            t["ctpt"] = {"n_in": CTPT["n_in"], "n_out": ctpt_cols, "limbs": Lc, "ms": round(ms, 3),
+                         "output_cts_per_s": round(ctpt_cols * 1000.0 / ms, 3)}
+            del X, Y, wsm
+        res[name] = t
+        ctx.close()
+        torch.cuda.empty_cache()
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -278,6 +389,12 @@ def run_boot(args, rank, world, dist):
     graph_kernels = graph.kernels
     graph.close()
     clocks = clk.summary()
+    side = {}
+    if not args.no_extras and world == 1:
+        # after the timed region: the same single-ciphertext calls on this library and on the reference's
+        # own GPU build, one after the other on this GPU
+        side["ours_same_calls"] = ours_per_ct_leg(dev)
+        side["reference_gpu"] = reference_gpu_leg()
     return {
         "metric": BOOT_METRIC, "value": round(world * B * 1000.0 / ms, 3), "unit": "bootstraps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
@@ -305,61 +422,52 @@ def run_boot(args, rank, world, dist):
         "gpu_launches": int(launches),
         "roofline": roof,
         "clocks": clocks,
+        **side,
     }
 
 
-# key switches per bootstrapped ciphertext in this pipeline at N = 2^16: C2S 7+7, 7+7, 7+4
-# rotations at 35/34/33 primes plus the conjugation; S2C the same 39 at 4/3/2 primes;
-# EvalMod 17 relinearisations on each of the two halves (7 baby + 2 giant basis products,
-# 5 split products, 3 double angles) at 32..23 primes.
-BOOT_OPS = {"rot_high": 40, "rot_low": 39, "relin": 34}
+def cpu_boot_run(shared: int = 0):
+    """One full S2C-first bootstrap on the host cores: the C++ host library built on the CPU oracle
+    (oracle/_build/libshmoai_host_oracle.so, OpenMP over limbs) at the reference parameters, keys generated
+    before the timed call.  shared = n: one shared-a group of n ciphertexts; 0: one ordinary ciphertext.
+    Returns (bootstraps/s, seconds of the timed bootstrap, seconds of set-up, mean decryption error)."""
+    from shmoai_b200.host import Bootstrapper, Host
 
-
-def cpu_boot_estimate(shared: int = 0):
-    """CPU oracle on all host cores (N = 2^16) -> bootstraps/s.  Ordinary: one HRotate at 34
-    primes, one at 3 primes and one relinearisation at 27 primes, scaled by BOOT_OPS.
-    Shared-a groups of n: one Sh-Rot of a group at 34 and at 3 primes and one FmtSwitch
-    backward of a group at 33 primes, per ciphertext (/ n), plus the EvalMod
-    relinearisations (ordinary ciphertexts)."""
-    from oracle import oracle as O
-
-    o = O.Oracle.from_bits(BOOT["log_n"], BOOT["bits"], BOOT["n_special"])
-    n, QP = o.n, o.nq + o.np
-    key = np.stack([O.fill(900 + d, (2, QP, n), list(o.primes) * 2) for d in range(o.dnum)])
-    t = {}
-    if shared:
-        H = shared + 1
-        shkey = np.stack([O.fill(910 + d, (H, QP, n), list(o.primes) * H) for d in range(o.dnum)])
-        cases = (("rot_high", 34), ("rot_low", 3), ("bwd", 33))
-        for name, L in cases:
-            g = O.fill(911, (H, L, n), list(o.primes[:L]) * H)
-            t0 = time.perf_counter()
-            if name == "bwd":
-                o.fmt_backward(g, [key] * shared)
-            else:
-                o.shared_rotate_hoisted(g, [5], [shkey])
-            t[name] = (time.perf_counter() - t0) / shared
-    else:
-        for name, L in (("rot_high", 34), ("rot_low", 3)):
-            x = O.fill(901, (2, L, n), list(o.primes[:L]) * 2)
-            t0 = time.perf_counter()
-            o.apply_galois_ct(x, 5, key)
-            t[name] = time.perf_counter() - t0
-        t["bwd"] = 0.0
-    x = O.fill(902, (3, 27, n), list(o.primes[:27]) * 3)
+    lib = os.path.join(ROOT, "oracle", "_build", "libshmoai_host_oracle.so")
     t0 = time.perf_counter()
-    o.relinearize(x, key)
-    t["relin"] = time.perf_counter() - t0
-    per_boot = sum(BOOT_OPS[k] * t[k] for k in BOOT_OPS) + 2 * t["bwd"]
-    what = (f"one Sh-Rot of a group of {shared} at 34 primes ({t['rot_high'] * shared:.2f} s), one at 3 primes "
-            f"({t['rot_low'] * shared:.2f} s), one FmtSwitch backward of the group at 33 primes "
-            f"({t['bwd'] * shared:.2f} s), each / {shared} per ciphertext" if shared else
-            f"one HRotate at 34 primes ({t['rot_high']:.2f} s), one at 3 primes ({t['rot_low']:.2f} s)")
-    sample = (f"{what}, and one relinearisation at 27 primes ({t['relin']:.2f} s) on the CPU oracle (OpenMP "
-              f"over limbs), scaled by {BOOT_OPS['rot_high']} + {BOOT_OPS['rot_low']} rotations"
-              f"{' + 2 backward switches' if shared else ''} and {BOOT_OPS['relin']} relinearisations per "
-              "bootstrapped ciphertext")
-    return 1.0 / per_boot, os.cpu_count(), sample
+    h = Host(BOOT["log_n"], bits=BOOT["bits"], n_special=BOOT["n_special"], hamming_weight=BOOT["h"], seed=0x5EED,
+             lib=lib)
+    h.gen_relin_key()
+    bs = Bootstrapper(h, BOOT["scale"], BOOT["input_level"])
+    if shared:
+        h.gen_shared_keys(shared, bs.galois_elts(), hamming_weight=BOOT["h"])
+    else:
+        h.gen_galois_keys(bs.galois_elts())
+    count = shared or 1
+    rng = np.random.default_rng(3000)
+    z = rng.uniform(-1, 1, (count, h.n // 2)) + 1j * rng.uniform(-1, 1, (count, h.n // 2))
+    ct = h.encrypt(z, BOOT["scale"], BOOT["input_level"])
+    setup = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    out = bs.run(ct, shared)
+    secs = time.perf_counter() - t1
+    err = float(np.abs(h.decrypt(out) - z).mean())
+    out.close()
+    ct.close()
+    bs.close()
+    h.close()
+    return count / secs, secs, setup, err
+
+
+def cpu_boot_sample(shared: int = 0):
+    """cpu_boot_run with the sample described for the JSON line."""
+    v, secs, setup, err = cpu_boot_run(shared)
+    what = (f"one full shared-a S2C-first bootstrap of a group of {shared} ciphertexts" if shared else
+            "one full S2C-first bootstrap of one ordinary ciphertext")
+    sample = (f"{what} at N = 2^16, 35 + 5 primes, input at 4 primes ({secs:.1f} s; mean error {err:.2e}), "
+              f"through the C++ host library built on the CPU oracle (OpenMP over limbs); key generation and "
+              f"set-up ({setup:.1f} s) before the timed call")
+    return v, os.cpu_count(), sample, secs
 
 
 # ---------------------------------------------------------------------------
@@ -879,11 +987,41 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": "no CPU arm for the kernel workload "
                               + args.workload + " (timed on the GPU only)"}))
             return
+        if args.workload == "boot":
+            # one full bootstrap of the configured form (a shared-a group of n, or one ordinary
+            # ciphertext) is minutes of CPU work: the arm runs it once and reports that one step
+            shared = args.shared
+            need = (7 * (shared + 1) if shared else 14) * 40 * 2 ** 16 * 8 * 42 + (24 << 30)
+            try:
+                import psutil
+
+                avail = psutil.virtual_memory().available
+            except Exception:
+                avail = need
+            note = None
+            if shared and avail < need:
+                note = (f"host memory {avail >> 30} GiB is below the ~{need >> 30} GiB the shared-a keys of a "
+                        f"group of {shared} need on the CPU: one ordinary ciphertext was bootstrapped instead")
+                shared = 0
+            v, cores, sample, secs = cpu_boot_sample(shared)
+            print(json.dumps({
+                "impl": "reference", "metric": BOOT_METRIC, "value": round(v, 6), "unit": "bootstraps/s",
+                "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": round(secs * 1000.0, 1),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                "data": "synthetic (seeded uniform slot values in [-1,1]^2)",
+                "config": {"workload": "boot (reference CPU arm: the reference has no host-side CKKS path; the host "
+                                       "library on the oracle restatement, one full bootstrap)",
+                           "shared_a_group": shared or None, "steps_requested": args.steps,
+                           "warmup_requested": args.warmup, "note": note},
+                "cpu_baseline": {"value": round(v, 6), "unit": "bootstraps/s", "cores": cores, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": round(v, 6), "unit": "bootstraps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+            }))
+            return
         vals = []
         for i in range(args.warmup + args.steps):
-            if args.workload == "boot":
-                v, cores, sample = cpu_boot_estimate(args.shared)
-            elif args.workload == "gelu":
+            if args.workload == "gelu":
                 v, cores = cpu_gelu_sample()
                 sample = "GELU of one ciphertext at 12 primes per step (host library on the oracle)"
             else:
@@ -925,7 +1063,9 @@ def main():
                 res["cpu_baseline"] = {"value": round(v, 4), "unit": "ciphertexts/s", "cores": cores, "kind": "port",
                                        "sample": "GELU of one ciphertext at 12 primes (host library on the oracle)"}
             elif args.workload == "boot":
-                v, cores, sample = cpu_boot_estimate(args.shared)
+                # bounded: one ordinary ciphertext's full bootstrap (a shared-a group is the
+                # --impl reference arm's sample)
+                v, cores, sample, _ = cpu_boot_sample(0)
                 res["cpu_baseline"] = {"value": round(v, 6), "unit": "bootstraps/s", "cores": cores,
                                        "kind": "port", "sample": sample}
             else:

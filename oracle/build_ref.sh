@@ -5,10 +5,11 @@
 #   _ref/libref_host.so  host number theory (primes, NTT tables, RNS constants)
 #                        of the vendored PhantomFHE, compiled by g++, behind
 #                        the extern "C" face in ref_host_shim.cpp
-#   _ref/ref_golden      the reference GPU evaluator (all PhantomFHE .cu files
-#                        + the moai:: adapter ckks_evaluator_parallel.cu) for
-#                        sm_100a, linked with the golden-vector generator
-#                        ref_golden.cu
+#   _ref/ref_golden      the reference GPU evaluator (all PhantomFHE .cu files,
+#                        the moai:: adapter ckks_evaluator_parallel.cu and the
+#                        shared-a files FmtSwitch.cu, ShRotate.cu and
+#                        SharedABatchOps.cu) for sm_100a, linked with the
+#                        golden-vector and timing harness ref_golden.cu
 #
 # The outputs are test infrastructure.  Run where the reference tree exists;
 # elsewhere the script does nothing.  Set SHMOAI_REF_GPU=0 to skip the
@@ -39,8 +40,11 @@ if [ "${SHMOAI_REF_GPU:-1}" = "0" ]; then exit 0; fi
 if [ -f "$OUT/ref_golden" ] && [ "$OUT/ref_golden" -nt "$HERE/ref_golden.cu" ]; then exit 0; fi
 
 NVFLAGS=(-std=c++17 -O3 -rdc=true -Xcompiler -fPIC,-fopenmp --default-stream per-thread -DPHANTOM_USE_CUDA_PTX
-         -gencode arch=compute_100a,code=sm_100a -I"$PH/include" -I"$REF/src/include/source" -w)
-SRCS=("$PH"/src/*.cu "$PH"/src/ntt/*.cu "$PH"/src/util/*.cu "$REF/src/include/source/ckks_evaluator_parallel.cu")
+         -gencode arch=compute_100a,code=sm_100a -I"$PH/include" -I"$REF/src/include/source"
+         -I"$REF/src/include/source/bootstrapping" -w)
+BOOT=$REF/src/include/source/bootstrapping
+SRCS=("$PH"/src/*.cu "$PH"/src/ntt/*.cu "$PH"/src/util/*.cu "$REF/src/include/source/ckks_evaluator_parallel.cu"
+      "$BOOT/FmtSwitch.cu" "$BOOT/ShRotate.cu" "$BOOT/SharedABatchOps.cu")
 pids=()
 for src in "${SRCS[@]}"; do
     rel=${src#"$REF"/}

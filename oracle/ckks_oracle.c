@@ -766,6 +766,24 @@ static void exact_extend(const orc_ctx *c, const uint64_t *a, uint32_t L, uint64
     free(y);
 }
 
+/* ModRaise (Bootstrapper.cu:3271-3356, SharedABatchOps.cu:15-25, 128-166): one-limb polynomials
+ * [n_polys][N] (mod q0, NTT form) -> [n_polys][L][N] (NTT form) by the centred lift: the residue x
+ * mod q0 goes to every prime as x, or as x - q0 when x > floor(q0 / 2). */
+void orc_modraise(const orc_ctx *c, const uint64_t *in, uint64_t *out, uint32_t n_polys, uint32_t L) {
+    size_t n = c->n;
+    uint64_t q0 = c->primes[0], *x = (uint64_t *)malloc(n * 8);
+    for (uint32_t p = 0; p < n_polys; p++) {
+        memcpy(x, in + (size_t)p * n, n * 8);
+        orc_ntt_inv(x, c->log_n, q0, c->irp);
+        for (uint32_t j = 0; j < L; j++) {
+            uint64_t qj = c->primes[j], *o = out + ((size_t)p * L + j) * n;
+            for (size_t k = 0; k < n; k++) o[k] = x[k] > q0 / 2 ? submod(x[k] % qj, q0 % qj, qj) : x[k] % qj;
+        }
+    }
+    free(x);
+    orc_ntt(c, out, n_polys, L, 0);
+}
+
 /* The exact extension alone, for n_polys polynomials [n_polys][L][N] (NTT form) into
  * [n_polys][L + np][N] (the extension step of FmtSwitch.cu:317-329). */
 void orc_exact_extend(const orc_ctx *c, const uint64_t *a, uint32_t n_polys, uint32_t L, uint64_t *ext) {

@@ -73,6 +73,7 @@ def lib():
                                                 ctypes.POINTER(_u64p), ctypes.POINTER(_u64p)]
         L.orc_fmt_forward.argtypes = [vp, _u64p, u32, u32, _u64p, _u64p]
         L.orc_exact_extend.argtypes = [vp, _u64p, u32, u32, _u64p]
+        L.orc_modraise.argtypes = [vp, _u64p, _u64p, u32, u32]
         L.orc_fmt_backward.argtypes = [vp, _u64p, u32, u32, ctypes.POINTER(_u64p), _u64p]
         L.orc_signed_residue.argtypes = [ctypes.c_int64, u64]
         L.orc_signed_residue.restype = u64
@@ -224,6 +225,14 @@ class Oracle:
         op = (_u64p * len(outs))(*[_p(o) for o in outs])
         lib().orc_shared_rotate_hoisted(self._h, _p(sh), H - 1, L, len(elts), e, kp, op)
         return outs
+
+    def modraise(self, a, L: int):
+        """[..][1][N] polynomials mod q0 (NTT form) -> [..][L][N] by the centred lift."""
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        m = a.size // self.n
+        out = np.empty(a.shape[:-2] + (L, self.n), dtype=np.uint64)
+        lib().orc_modraise(self._h, _p(a), _p(out), m, L)
+        return out
 
     def exact_extend(self, a):
         """[..][L][N] NTT-form polynomials -> [..][L + np][N]: the Ql rows copied, the P rows

@@ -688,18 +688,7 @@ int shm_modraise(const shm_context *ctx, const uint64_t *in, uint64_t *out, uint
     (void)stream;
     const orc_ctx *c = ctx->c;
     if (L < 1 || L > c->nq) return fail("level out of range");
-    size_t n = c->n;
-    uint64_t q0 = c->primes[0], *x = (uint64_t *)malloc(n * 8);
-    for (uint32_t p = 0; p < n_polys; p++) {
-        memcpy(x, in + (size_t)p * n, n * 8);
-        orc_ntt_inv(x, c->log_n, q0, c->irp);
-        for (uint32_t j = 0; j < L; j++) {
-            uint64_t qj = c->primes[j], *o = out + ((size_t)p * L + j) * n;
-            for (size_t k = 0; k < n; k++) o[k] = x[k] > q0 / 2 ? submod(x[k] % qj, q0 % qj, qj) : x[k] % qj;
-        }
-    }
-    free(x);
-    orc_ntt(c, out, n_polys, L, 0);
+    orc_modraise(c, in, out, n_polys, L);
     return SHM_OK;
 }
 

@@ -7,15 +7,33 @@
 // reference: they are filled from the counter generator below, which the
 // Python tests regenerate bit for bit, so no large arrays have to be stored.
 //
-//   usage: ref_golden <tiny|prim|boot> > golden.json
+//   usage: ref_golden <tiny|prim|boot> [golden|shared|time] > out.json
+//
+//   golden  the evaluator records (NTT, add, multiply_plain, rescale, rotate,
+//           conjugate, multiply, relinearize, constant encodes, ct-pt loop)
+//   shared  the shared-a records (FmtSwitch forward / backward, Sh-Rot, the
+//           shared batch rescale / modraise / multiply_plain / add) and a
+//           complex slot-vector encode; params.name is "shared_<set>"
+//   time    CUDA-event timings of the reference's own calls on this GPU (the
+//           config-1 primitives, per-ciphertext HRotate and multiply +
+//           relinearize + rescale, the per-ciphertext ct-pt loop)
+#include <omp.h>
+
+#include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
+#include <functional>
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "phantom.h"
 #include "ckks_evaluator_parallel.cuh"
+#include "FmtSwitch.cuh"
+#include "ShRotate.cuh"
+#include "SharedABatchOps.cuh"
 
 using namespace phantom;
 using namespace phantom::arith;
@@ -71,8 +89,345 @@ static double weight(uint64_t tag, uint64_t i) {
     return (double)m * (0.08 / 4503599627370496.0);
 }
 
+// slot value in [-1, 1): a 53-bit integer times 2^-52 minus one, exactly reproducible in numpy
+static double unit(uint64_t tag, uint64_t i) {
+    return (double)(sm64((tag << 40) + i) >> 11) * (1.0 / 4503599627370496.0) - 1.0;
+}
+
+struct Env {
+    PhantomContext &context;
+    PhantomCKKSEncoder &encoder;
+    moai::Encoder &enc;
+    moai::Evaluator &ev;
+    PhantomSecretKey &sk;
+    PhantomRelinKey &rk;
+    PhantomGaloisKey &gk;
+    std::vector<uint64_t> primes;
+    size_t N, nq, np, dnum, QP;
+    int log_n;
+    cudaStream_t s;
+};
+
+// rows of a tag-filled array: `reps` copies of the given prime list
+static std::vector<uint64_t> rows_of(const std::vector<uint64_t> &ps, size_t reps) {
+    std::vector<uint64_t> r;
+    for (size_t k = 0; k < reps; k++) r.insert(r.end(), ps.begin(), ps.end());
+    return r;
+}
+
+static std::vector<uint64_t> first_primes(const Env &E, size_t L) {
+    return std::vector<uint64_t>(E.primes.begin(), E.primes.begin() + L);
+}
+
+// a shared-a batch of n members at L limbs, b_i filled with tag + i and a with tag + 9
+static void fill_batch(const Env &E, moai::SharedACiphertextBatch &b, size_t n, size_t L, uint64_t tag) {
+    b.allocate(E.context, 1 + (E.nq - L), n, std::pow(2.0, 40), E.s);
+    std::vector<uint64_t> v(L * E.N);
+    for (size_t i = 0; i < n; i++) {
+        fill(v, tag + i, E.N, first_primes(E, L));
+        h2d(b.b_[i].get(), v);
+    }
+    fill(v, tag + 9, E.N, first_primes(E, L));
+    h2d(b.a_.get(), v);
+}
+
+// a shared-a batch in the layout [n + 1][L][N] = (b_0 .. b_{n-1}, a)
+static void dump_batch(const Env &E, const char *name, const moai::SharedACiphertextBatch &b) {
+    const size_t L = b.size_Ql_, w = L * E.N;
+    std::vector<uint64_t> all;
+    all.reserve((b.n_ + 1) * w);
+    for (size_t i = 0; i < b.n_; i++) {
+        auto v = d2h(b.b_[i].get(), w);
+        all.insert(all.end(), v.begin(), v.end());
+    }
+    auto a = d2h(b.a_.get(), w);
+    all.insert(all.end(), a.begin(), a.end());
+    emit(name, all, (b.n_ + 1) * L, E.N);
+}
+
+static PhantomCiphertext make_ct_env(const Env &E, uint64_t tag, size_t limbs) {
+    PhantomCiphertext ct;
+    ct.resize(E.context, 1 + (E.nq - limbs), 2, E.s);
+    ct.set_scale(std::pow(2.0, 40));
+    ct.set_ntt_form(true);
+    std::vector<uint64_t> v(2 * limbs * E.N);
+    fill(v, tag, E.N, rows_of(first_primes(E, limbs), 2));
+    h2d(ct.data(), v);
+    return ct;
+}
+
+static void load_key_env(const Env &E, const PhantomRelinKey &key, uint64_t tag) {
+    std::vector<uint64_t *> ptrs(E.dnum);
+    cudaDeviceSynchronize();
+    cudaMemcpy(ptrs.data(), key.public_keys_ptr(), E.dnum * sizeof(uint64_t *), cudaMemcpyDeviceToHost);
+    for (size_t d = 0; d < E.dnum; d++) {
+        std::vector<uint64_t> v(2 * E.QP * E.N);
+        fill(v, tag + d, E.N, rows_of(E.primes, 2));
+        h2d(ptrs[d], v);
+    }
+}
+
+// FmtSwitch forward and backward for groups of n at L limbs.  The format key rows live in the QlP
+// basis (FmtSwitch.cuh:31-40): a_fmt[j] tag 400 + j, B_fmt[j][i] tag 500 + j n + i; backward key i
+// digit d tag 600 + 10 i + d.  Inputs: ciphertext j tag 30 + j; the backward batch tags 50.. (fill_batch).
+static void shared_fmt_records(const Env &E, size_t n, size_t L) {
+    const size_t chain = 1 + (E.nq - L), QlP = L + E.np, pc = QlP * E.N;
+    std::vector<uint64_t> qlp_rows = first_primes(E, L);
+    qlp_rows.insert(qlp_rows.end(), E.primes.begin() + E.nq, E.primes.end());
+    moai::SharedAFormatKey fk;
+    fk.n_ = n;
+    fk.chain_index_ = chain;
+    fk.size_Ql_ = L;
+    fk.size_P_ = E.np;
+    fk.a_fmt_ = make_cuda_auto_ptr<uint64_t>(n * pc, E.s);
+    fk.B_fmt_ = make_cuda_auto_ptr<uint64_t>(n * n * pc, E.s);
+    std::vector<uint64_t> v(pc);
+    for (size_t j = 0; j < n; j++) {
+        fill(v, 400 + j, E.N, qlp_rows);
+        h2d(fk.a_fmt_.get() + j * pc, v);
+        for (size_t i = 0; i < n; i++) {
+            fill(v, 500 + j * n + i, E.N, qlp_rows);
+            h2d(fk.B_fmt_.get() + (j * n + i) * pc, v);
+        }
+    }
+    for (size_t i = 0; i < n; i++) {
+        fk.backward_keys_.emplace_back(E.sk.gen_relinkey(E.context));
+        load_key_env(E, fk.backward_keys_[i], 600 + 10 * i);
+    }
+    std::vector<PhantomCiphertext> cts;
+    for (size_t j = 0; j < n; j++) cts.push_back(make_ct_env(E, 30 + j, L));
+    moai::SharedACiphertextBatch out;
+    moai::fmt_switch_forward(E.context, cts, fk, out, E.s);
+    char nm[64];
+    snprintf(nm, sizeof nm, "fmt_fwd_n%zu_L%zu", n, L);
+    dump_batch(E, nm, out);
+
+    moai::SharedACiphertextBatch in;
+    fill_batch(E, in, n, L, 50);
+    std::vector<PhantomCiphertext> back;
+    moai::fmt_switch_backward(E.context, in, fk, back, E.s);
+    std::vector<uint64_t> all;
+    for (auto &ct : back) {
+        auto w = d2h(ct.data(), 2 * L * E.N);
+        all.insert(all.end(), w.begin(), w.end());
+    }
+    snprintf(nm, sizeof nm, "fmt_bwd_n%zu_L%zu", n, L);
+    emit(nm, all, n * 2 * L, E.N);
+}
+
+// Sh-Rot of a group of n at L limbs by `step` with a Sh-Galois key whose A_g has tag 700 + g and
+// B_{g,i} tag 800 + g n + i (ShRotate.cuh:25-36); input batch tags 60.. (fill_batch)
+static void shared_rot_record(const Env &E, size_t n, size_t L, int step) {
+    moai::SharedAGaloisKey key;
+    key.step_ = step;
+    key.n_ = n;
+    key.dnum_ = E.dnum;
+    auto elts = get_elts_from_steps(std::vector<int>{step}, E.N);
+    key.galois_elt_ = elts[0];
+    key.tool_ = std::make_unique<PhantomGaloisTool>(elts, E.log_n, E.s, false);
+    const size_t pc = E.QP * E.N;
+    key.A_ = make_cuda_auto_ptr<uint64_t>(E.dnum * pc, E.s);
+    key.B_ = make_cuda_auto_ptr<uint64_t>(E.dnum * n * pc, E.s);
+    std::vector<uint64_t> v(pc);
+    for (size_t g = 0; g < E.dnum; g++) {
+        fill(v, 700 + g, E.N, E.primes);
+        h2d(key.A_.get() + g * pc, v);
+        for (size_t i = 0; i < n; i++) {
+            fill(v, 800 + g * n + i, E.N, E.primes);
+            h2d(key.B_.get() + (g * n + i) * pc, v);
+        }
+    }
+    moai::SharedACiphertextBatch in, out;
+    fill_batch(E, in, n, L, 60);
+    moai::shared_a_rotate(E.context, in, key, out, E.s);
+    char nm[64];
+    snprintf(nm, sizeof nm, "shrot_n%zu_L%zu_s%d", n, L, step);
+    printf(",\n  \"%s_elt\": %u", nm, (unsigned)elts[0]);
+    dump_batch(E, nm, out);
+}
+
+static int run_shared(const Env &E, const std::string &which) {
+    const bool tiny = which == "tiny";
+    const size_t n = 4;
+    // FmtSwitch at the bootstrap's input level (4 primes; 2 at N = 2^12), groups of 4 and 8
+    const size_t L_fmt = tiny ? 2 : 4;
+    shared_fmt_records(E, n, L_fmt);
+    shared_fmt_records(E, 8, L_fmt);
+    // Sh-Rot at the top level, one level below it (a short last digit) and at 3 primes
+    shared_rot_record(E, n, E.nq, 1);
+    shared_rot_record(E, n, E.nq - 1, 1);
+    shared_rot_record(E, n, 3, -3);
+    {   // shared_a_rescale_to_next_inplace at L = nq - 1 (tags 70..)
+        moai::SharedACiphertextBatch b;
+        fill_batch(E, b, n, E.nq - 1, 70);
+        moai::shared_a_rescale_to_next_inplace(E.context, b, E.s);
+        dump_batch(E, "shared_rescale", b);
+    }
+    {   // shared_a_modraise_inplace from one prime (tags 80..)
+        moai::SharedACiphertextBatch b;
+        fill_batch(E, b, n, 1, 80);
+        moai::shared_a_modraise_inplace(E.context, b, E.s);
+        dump_batch(E, "shared_modraise", b);
+    }
+    {   // shared_a_multiply_plain_inplace at 3 limbs (batch tags 90.., plaintext tag 98) and
+        // shared_a_add_inplace of two batches (tags 110.. and 120..)
+        const size_t L = 3;
+        moai::SharedACiphertextBatch b;
+        fill_batch(E, b, n, L, 90);
+        PhantomPlaintext pt;
+        pt.resize(L, E.N, E.s);
+        pt.set_chain_index(1 + (E.nq - L));
+        std::vector<uint64_t> v(L * E.N);
+        fill(v, 98, E.N, first_primes(E, L));
+        h2d(pt.data(), v);
+        moai::shared_a_multiply_plain_inplace(E.context, b, pt, E.s);
+        dump_batch(E, "shared_mulplain", b);
+        moai::SharedACiphertextBatch x, y;
+        fill_batch(E, x, n, L, 110);
+        fill_batch(E, y, n, L, 120);
+        moai::shared_a_add_inplace(E.context, x, y, E.s);
+        dump_batch(E, "shared_add", x);
+    }
+    {   // complex slot-vector encode at the top level: slot j = unit(12, j) + i unit(13, j); the
+        // record holds the NTT-form plaintext and the integer coefficients (the reference's own INTT
+        // of limb 0, centred), all of them at N = 2^12, every 8th at N = 2^16
+        const double scale = std::pow(2.0, tiny ? 40 : 46);
+        std::vector<std::complex<double>> z(E.N / 2);
+        for (size_t j = 0; j < z.size(); j++) z[j] = std::complex<double>(unit(12, j), unit(13, j));
+        PhantomPlaintext pt;
+        E.encoder.encode(E.context, z, scale, pt, 1, *global_variables::default_stream);
+        auto v = d2h(pt.data(), E.nq * E.N);
+        emit("encode_z", v, E.nq, E.N);
+        auto c = make_cuda_auto_ptr<uint64_t>(E.N, E.s);
+        cudaMemcpyAsync(c.get(), pt.data(), E.N * 8, cudaMemcpyDeviceToDevice, E.s);
+        nwt_2d_radix8_backward_inplace(c.get(), E.context.gpu_rns_tables(), 1, 0, E.s);
+        auto co = d2h(c.get(), E.N);
+        const size_t stride = tiny ? 1 : 8;
+        printf(",\n  \"encode_z_coeffs\": {\"scale_log2\": %d, \"stride\": %zu, \"values\": [", tiny ? 40 : 46, stride);
+        for (size_t k = 0; k < E.N; k += stride) {
+            int64_t x = co[k] > E.primes[0] / 2 ? -(int64_t)(E.primes[0] - co[k]) : (int64_t)co[k];
+            printf("%s\"%lld\"", k ? ", " : "", (long long)x);
+        }
+        printf("]}");
+    }
+    printf("\n}\n");
+    cudaDeviceSynchronize();
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// ---- timing of the reference's own calls (CUDA events on the evaluator's stream)
+
+static double time_ms(cudaStream_t s, int warm, int reps, const std::function<void()> &fn) {
+    for (int i = 0; i < warm; i++) fn();
+    cudaDeviceSynchronize();
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+    for (int i = 0; i < reps; i++) fn();
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    cudaDeviceSynchronize();
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms / reps;
+}
+
+// the per-ciphertext ct-pt loop of Ct_pt_matrix_mul.cuh:85-158 (OpenMP over output columns, one
+// encoder, evaluator and stream per thread; per weight: scalar encode, deep copy of the input,
+// multiply_plain_inplace, add_inplace; then rescale), restated over the reference's calls for
+// n_in inputs at L limbs and the first n_out output columns
+static double ctpt_loop_ms(const Env &E, size_t n_in, size_t n_out, size_t L, int threads) {
+    std::vector<PhantomCiphertext> X;
+    X.reserve(n_in);
+    const size_t words = 2 * L * E.N;
+    for (size_t j = 0; j < n_in; j++) {
+        if (j < 4) {
+            X.push_back(make_ct_env(E, 20 + j, L));
+        } else {  // distinct buffers, contents copied on the device
+            PhantomCiphertext ct;
+            ct.resize(E.context, X[0].chain_index(), 2, E.s);
+            ct.set_scale(X[0].scale());
+            ct.set_ntt_form(true);
+            cudaMemcpyAsync(ct.data(), X[j % 4].data(), words * 8, cudaMemcpyDeviceToDevice, E.s);
+            X.push_back(std::move(ct));
+        }
+    }
+    cudaDeviceSynchronize();
+    std::vector<std::unique_ptr<cuda_stream_wrapper>> streams;
+    for (int t = 0; t < threads; t++) streams.push_back(std::make_unique<cuda_stream_wrapper>());
+    auto run = [&](size_t cols) {
+#pragma omp parallel num_threads(threads)
+        {
+            PhantomCKKSEncoder penc(E.context);
+            moai::Encoder enc(&E.context, &penc);
+            moai::Evaluator ev(&E.context, &penc);
+            auto &st = *streams[omp_get_thread_num()];
+            const cudaStream_t cs = st.get_stream();
+#pragma omp for schedule(static)
+            for (int i = 0; i < (int)cols; i++) {
+                PhantomCiphertext acc;
+                for (size_t j = 0; j < n_in; j++) {
+                    PhantomPlaintext pt;
+                    enc.encode(weight(8, j * 768 + i), X[j].chain_index(), X[j].scale(), pt, st);
+                    PhantomCiphertext tmp;
+                    tmp.resize(E.context, X[j].chain_index(), 2, cs);
+                    tmp.set_scale(X[j].scale());
+                    tmp.set_ntt_form(true);
+                    cudaMemcpyAsync(tmp.data(), X[j].data(), words * 8, cudaMemcpyDeviceToDevice, cs);
+                    ev.multiply_plain_inplace(tmp, pt, st);
+                    if (j == 0) acc = std::move(tmp);
+                    else ev.add_inplace(acc, tmp, st);
+                }
+                ev.rescale_to_next_inplace(acc, st);
+            }
+            cudaStreamSynchronize(cs);
+        }
+    };
+    run(threads);  // warm-up: one column per thread
+    cudaDeviceSynchronize();
+    auto t0 = std::chrono::steady_clock::now();
+    run(n_out);
+    cudaDeviceSynchronize();
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+static int run_time(const Env &E, const std::string &which, int ctpt_cols) {
+    PhantomCiphertext A = make_ct_env(E, 1, E.nq), B = make_ct_env(E, 2, E.nq);
+    const int warm = 3, reps = 20;
+    const cudaStream_t s = E.s;
+    double ntt = time_ms(s, warm, reps, [&] {
+        E.ev.transform_from_ntt_inplace(A);
+        E.ev.transform_to_ntt_inplace(A);
+    });
+    double rot = time_ms(s, warm, reps, [&] { E.ev.rotate_vector_inplace(A, 1, E.gk); });
+    double mrr = time_ms(s, warm, reps, [&] {
+        PhantomCiphertext t;
+        E.ev.multiply(A, B, t);
+        E.ev.relinearize_inplace(t, E.rk);
+        E.ev.rescale_to_next_inplace(t);
+    });
+    printf(",\n  \"time\": {\"limbs\": %zu, \"warmup\": %d, \"reps\": %d, \"ntt_inv_fwd_ms\": %.4f, "
+           "\"rotate1_ms\": %.4f, \"mul_relin_rescale_ms\": %.4f, \"chain_ms\": %.4f",
+           E.nq, warm, reps, ntt, rot, mrr, ntt + rot + mrr);
+    if (ctpt_cols > 0) {
+        const int threads = std::max(1, std::min(omp_get_max_threads(), 32));
+        const size_t n_in = 768, L = 13;
+        double ms = ctpt_loop_ms(E, n_in, (size_t)ctpt_cols, L, threads);
+        printf(", \"ctpt_loop\": {\"n_in\": %zu, \"n_out\": %d, \"limbs\": %zu, \"threads\": %d, \"ms\": %.3f}",
+               n_in, ctpt_cols, L, threads, ms);
+    }
+    printf("}\n}\n");
+    cudaDeviceSynchronize();
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
 int main(int argc, char **argv) {
     std::string which = argc > 1 ? argv[1] : "tiny";
+    std::string mode = argc > 2 ? argv[2] : "golden";
+    const int ctpt_cols = argc > 3 ? atoi(argv[3]) : 0;
     int log_n;
     std::vector<int> bits;
     size_t np;
@@ -112,8 +467,9 @@ int main(int argc, char **argv) {
     std::vector<uint64_t> primes(QP);
     for (size_t i = 0; i < QP; i++) primes[i] = parms.coeff_modulus()[i].value();
 
+    const std::string set_name = mode == "shared" ? "shared_" + which : which;
     printf("{\n  \"params\": {\"name\": \"%s\", \"log_n\": %d, \"nq\": %zu, \"np\": %zu, \"dnum\": %zu, \"primes\": [",
-           which.c_str(), log_n, nq, np, dnum);
+           set_name.c_str(), log_n, nq, np, dnum);
     for (size_t i = 0; i < QP; i++) printf("%s\"%llu\"", i ? ", " : "", (unsigned long long)primes[i]);
     printf("]}");
     first_record = false;
@@ -140,6 +496,11 @@ int main(int argc, char **argv) {
     {
         auto &elts = context.key_galois_tool_->galois_elts();
         for (size_t idx = 0; idx < elts.size(); idx++) load_key(gk.get_relin_keys(idx), elts[idx] == 5 ? 300 : 200);
+    }
+
+    if (mode == "shared" || mode == "time") {
+        Env E{context, encoder, enc, ev, sk, rk, gk, primes, N, nq, np, dnum, QP, log_n, s};
+        return mode == "shared" ? run_shared(E, which) : run_time(E, which, ctpt_cols);
     }
 
     std::vector<uint64_t> qrows;

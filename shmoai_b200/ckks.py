@@ -190,6 +190,14 @@ class CKKSContext:
         check(lib().shm_rescale(self._h, _ptr(a), _ptr(out), p, L, ws, wsb, _stream(stream)))
         return out
 
+    def modraise(self, a, L: int, workspace=None, stream=None):
+        """[..][1][N] one-limb polynomials (mod q0, NTT form) -> [..][L][N] by the centred lift."""
+        p = a.numel() // self.n
+        out = self.empty(*(a.shape[:-2] + (L, self.n)))
+        ws, wsb = self._ws(workspace)
+        check(lib().shm_modraise(self._h, _ptr(a), _ptr(out), p, L, ws, wsb, _stream(stream)))
+        return out
+
     def keyswitch(self, d, key, workspace=None, stream=None):
         p, L = self._levels(d)
         out = self.empty(p, 2, L, self.n)
