@@ -170,6 +170,8 @@ class KeyGenerator {
     const DeviceBuffer &secret() const { return s_; }  // [QP][N] NTT form
     DeviceBuffer switching_key(const DeviceBuffer &s_new);  // [dnum][2][QP][N]: s_new -> s
     DeviceBuffer relin_key();
+    // [2][QP][N] = (e - a s, a) in NTT form (gen_publickey, secretkey.cu:524-537)
+    DeviceBuffer public_key();
     DeviceBuffer galois_key(uint32_t elt);
     std::map<uint32_t, DeviceBuffer> galois_keys(const std::vector<uint32_t> &elts);
 
@@ -215,6 +217,43 @@ class KeyGenerator {
     std::vector<std::vector<int64_t>> aux_coeffs_;
     std::vector<DeviceBuffer> aux_;
 };
+
+// Public-key encryption (PhantomPublicKey::encrypt_asymmetric and
+// encrypt_zero_asymmetric_internal, thirdparty/phantom-fhe/src/secretkey.cu:15-217): with
+// pk = (e - a s, a) over QP, a ternary u and CBD errors e0, e1 over QP, the ciphertext is the
+// ModDown to Q of u pk + (e0, e1), limbs dropped to L, plus the encoded message on c0.  The
+// reference runs the ModDown only from the key level to the top data level (chain index 1) and
+// encrypts only there in practice; below the top level this class drops limbs after it.
+// Deterministic in `seed` (counter-based samplers, like KeyGenerator).
+class PublicEncryptor {
+   public:
+    PublicEncryptor(const Context &c, DeviceBuffer pk, uint64_t seed = 0xE0C0);
+    Ciphertext encrypt(const std::vector<std::vector<cplx>> &z, double scale, uint32_t L);
+    // an encoded plaintext (moai::Encryptor::encrypt(plain, ct)): one ciphertext at pt.L, pt.scale
+    Ciphertext encrypt(const Plaintext &pt);
+    // count encryptions of zero at L primes
+    Ciphertext encrypt_zero(uint32_t count, uint32_t L, double scale);
+    const DeviceBuffer &public_key() const { return pk_; }
+
+   private:
+    const Context &c_;
+    Encoder enc_;
+    DeviceBuffer pk_;  // [2][QP][N] NTT form
+    uint64_t seed_, ctr_ = 0;
+};
+
+// ---- the MOAI packing of a batch of inputs (src/include/source/matrix_mul/Batch_encode_encrypt.cuh)
+
+// Column-interleaved packing (batch_input, Batch_encode_encrypt.cuh:12-43): X holds num_X
+// matrices of num_row x num_col values, X[(j * num_row + k) * num_col + i] = input j, row k,
+// column i; column i becomes one ciphertext whose slot num_X * k + j holds X_j[k][i] (num_X *
+// num_row <= N / 2, the other slots 0).  All columns are encoded in one batch on the device and
+// encrypted with the public key at L primes; the result is a batch of num_col ciphertexts.
+Ciphertext batch_input(PublicEncryptor &enc, const std::vector<double> &X, uint32_t num_X, uint32_t num_row,
+                       uint32_t num_col, double scale, uint32_t L);
+// The matching slot mask (bias_vec, Batch_encode_encrypt.cuh:45-56): slot j * num_X + i is 1 for
+// the first lengths[i] rows of input i, 0 elsewhere.
+std::vector<int> bias_vec(const std::vector<int> &lengths, uint32_t num_X, uint32_t num_row);
 
 // moai::Encryptor / moai::Decryptor names over the key generator's secret.
 class Encryptor {

@@ -59,6 +59,22 @@ uint32_t shm_host_galois_elt(const shm_host *h, int step);
  * primes and `scale`. */
 int shm_host_encrypt(shm_host *h, const double *re, const double *im, uint32_t count, uint32_t n_values, uint32_t L,
                      double scale, shm_ct **out);
+/* Public-key encryption (PhantomPublicKey::encrypt_asymmetric, secretkey.cu:15-217):
+ * shm_host_gen_public_key makes pk = (e - a s, a) over QP from the host's secret
+ * (gen_publickey, secretkey.cu:524-537) and a public-key encryptor whose samplers start at
+ * `seed`; shm_host_encrypt_public then encrypts like shm_host_encrypt with u pk + (e0, e1)
+ * brought down from QP to Q (the first L limbs kept) in place of the secret key. */
+int shm_host_gen_public_key(shm_host *h, uint64_t seed);
+int shm_host_encrypt_public(shm_host *h, const double *re, const double *im, uint32_t count, uint32_t n_values,
+                            uint32_t L, double scale, shm_ct **out);
+/* The MOAI packing (src/include/source/matrix_mul/Batch_encode_encrypt.cuh):
+ * shm_host_batch_input replaces batch_input (:12-43): X [num_X][num_row][num_col] doubles ->
+ * num_col ciphertexts, column i with slot num_X * k + j = X[j][k][i], encrypted with the
+ * public key at L primes and `scale`.  shm_host_bias_vec replaces bias_vec (:45-56): out
+ * [num_X * num_row] with slot j * num_X + i = 1 for j < lengths[i]. */
+int shm_host_batch_input(shm_host *h, const double *X, uint32_t num_X, uint32_t num_row, uint32_t num_col,
+                         double scale, uint32_t L, shm_ct **out);
+int shm_host_bias_vec(const int *lengths, uint32_t num_X, uint32_t num_row, int *out);
 /* Decrypt to [members in the batch][N/2] slot values (shared-a groups: member i of group
  * g is row g * members + i). */
 int shm_host_decrypt(shm_host *h, const shm_ct *ct, double *re, double *im);

@@ -55,6 +55,10 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_gen_shared_keys": (i32, [_P, _U32, _U32, ctypes.POINTER(_U32), _U32]),
         "shm_host_galois_elt": (_U32, [_P, i32]),
         "shm_host_encrypt": (i32, [_P, dp, dp, _U32, _U32, _U32, ctypes.c_double, pp]),
+        "shm_host_gen_public_key": (i32, [_P, ctypes.c_uint64]),
+        "shm_host_encrypt_public": (i32, [_P, dp, dp, _U32, _U32, _U32, ctypes.c_double, pp]),
+        "shm_host_batch_input": (i32, [_P, dp, _U32, _U32, _U32, ctypes.c_double, _U32, pp]),
+        "shm_host_bias_vec": (i32, [ctypes.POINTER(ctypes.c_int), _U32, _U32, ctypes.POINTER(ctypes.c_int)]),
         "shm_host_decrypt": (i32, [_P, _P, dp, dp]),
         "shm_ct_from_host": (i32, [_P, u64p, _U32, _U32, _U32, ctypes.c_double, i32, pp]),
         "shm_ct_to_host": (i32, [_P, _P, u64p]),
@@ -232,6 +236,25 @@ class Host:
         dp = ctypes.POINTER(ctypes.c_double)
         return self._out(self.lib.shm_host_encrypt, re.ctypes.data_as(dp), im.ctypes.data_as(dp), z.shape[0],
                          z.shape[1], L, scale)
+
+    def gen_public_key(self, seed: int = 0xE0C0):
+        self._check(self.lib.shm_host_gen_public_key(self._h, seed))
+
+    def encrypt_public(self, z, scale: float, L: int) -> "Ct":
+        """Public-key encryption (encrypt_asymmetric); gen_public_key first."""
+        z = np.atleast_2d(np.asarray(z, dtype=np.complex128))
+        re = np.ascontiguousarray(z.real)
+        im = np.ascontiguousarray(z.imag)
+        dp = ctypes.POINTER(ctypes.c_double)
+        return self._out(self.lib.shm_host_encrypt_public, re.ctypes.data_as(dp), im.ctypes.data_as(dp),
+                         z.shape[0], z.shape[1], L, scale)
+
+    def batch_input(self, X, scale: float, L: int) -> "Ct":
+        """X [num_X][num_row][num_col] -> num_col ciphertexts in the column-interleaved packing (public key)."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        nx, nr, nc = X.shape
+        dp = ctypes.POINTER(ctypes.c_double)
+        return self._out(self.lib.shm_host_batch_input, X.ctypes.data_as(dp), nx, nr, nc, scale, L)
 
     def decrypt(self, ct: "Ct") -> np.ndarray:
         rows = ct.count * ct.members
@@ -566,3 +589,14 @@ class Server:
 
 def slot_transform_selfcheck(log_slots: int, lib: str | None = None) -> float:
     return float(load(lib).shm_slot_transform_selfcheck(log_slots))
+
+
+def bias_vec(lengths, num_X: int, num_row: int, lib: str | None = None) -> np.ndarray:
+    """The valid-slot mask of the column-interleaved packing (Batch_encode_encrypt.cuh:45-56)."""
+    ln = np.ascontiguousarray(lengths, dtype=np.int32)
+    out = np.zeros(num_X * num_row, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    L = load(lib)
+    if L.shm_host_bias_vec(ln.ctypes.data_as(ip), num_X, num_row, out.ctypes.data_as(ip)) != 0:
+        raise HostError(L.shm_host_last_error().decode())
+    return out

@@ -18,6 +18,7 @@ struct shm_host {
     std::unique_ptr<KeyGenerator> kg;
     std::unique_ptr<Evaluator> ev;
     DeviceBuffer relin;
+    std::unique_ptr<PublicEncryptor> pub;  // shm_host_gen_public_key
     std::map<uint32_t, DeviceBuffer> galois;
     std::map<uint32_t, SharedAKeys> shared;  // group size -> keys
 
@@ -194,6 +195,43 @@ int shm_host_encrypt(shm_host *h, const double *re, const double *im, uint32_t c
             for (uint32_t j = 0; j < n_values; j++)
                 z[i][j] = cplx(re[(size_t)i * n_values + j], im ? im[(size_t)i * n_values + j] : 0.0);
         put(out, hh.kg->encrypt(z, scale, L));
+    });
+}
+
+int shm_host_gen_public_key(shm_host *h, uint64_t seed) {
+    return guard([&] {
+        auto &hh = H(h);
+        hh.pub = std::make_unique<PublicEncryptor>(*hh.ctx, hh.kg->public_key(), seed);
+    });
+}
+
+int shm_host_encrypt_public(shm_host *h, const double *re, const double *im, uint32_t count, uint32_t n_values,
+                            uint32_t L, double scale, shm_ct **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!hh.pub) throw Error("no public key: call shm_host_gen_public_key first");
+        std::vector<std::vector<cplx>> z(count, std::vector<cplx>(n_values));
+        for (uint32_t i = 0; i < count; i++)
+            for (uint32_t j = 0; j < n_values; j++)
+                z[i][j] = cplx(re[(size_t)i * n_values + j], im ? im[(size_t)i * n_values + j] : 0.0);
+        put(out, hh.pub->encrypt(z, scale, L));
+    });
+}
+
+int shm_host_batch_input(shm_host *h, const double *X, uint32_t num_X, uint32_t num_row, uint32_t num_col,
+                         double scale, uint32_t L, shm_ct **out) {
+    return guard([&] {
+        auto &hh = H(h);
+        if (!hh.pub) throw Error("no public key: call shm_host_gen_public_key first");
+        std::vector<double> x(X, X + (size_t)num_X * num_row * num_col);
+        put(out, batch_input(*hh.pub, x, num_X, num_row, num_col, scale, L));
+    });
+}
+
+int shm_host_bias_vec(const int *lengths, uint32_t num_X, uint32_t num_row, int *out) {
+    return guard([&] {
+        std::vector<int> v = bias_vec(std::vector<int>(lengths, lengths + num_X), num_X, num_row);
+        std::copy(v.begin(), v.end(), out);
     });
 }
 

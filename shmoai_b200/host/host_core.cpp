@@ -380,6 +380,79 @@ DeviceBuffer KeyGenerator::relin_key() {
     return switching_key(s2);
 }
 
+DeviceBuffer KeyGenerator::public_key() { return multi_key({&s_}, {{}}); }
+
+PublicEncryptor::PublicEncryptor(const Context &c, DeviceBuffer pk, uint64_t seed)
+    : c_(c), enc_(c), pk_(std::move(pk)), seed_(seed) {
+    if (pk_.words() != 2 * (size_t)(c_.nq + c_.np) * c_.n) throw Error("public key: expected [2][QP][N] words");
+}
+
+Ciphertext PublicEncryptor::encrypt_zero(uint32_t count, uint32_t L, double scale) {
+    const uint32_t N = c_.n, nq = c_.nq, QP = c_.nq + c_.np;
+    if (L < 1 || L > nq) throw Error("level out of range");
+    if (!count) throw Error("nothing to encrypt");
+    shm_context *h = c_.handle();
+    void *st = c_.stream();
+    const size_t row = (size_t)QP * N;
+    // u: uniform ternary coefficients, one polynomial per ciphertext (sample_ternary_poly)
+    std::vector<int64_t> uc((size_t)count * N);
+    const uint64_t su = detail::mix64(seed_, ++ctr_);
+    for (size_t j = 0; j < uc.size(); j++) uc[j] = (int64_t)(detail::mix64(su, j) % 3) - 1;
+    DeviceBuffer u(c_, count * row), x(c_, 2 * count * row), t(c_, row);
+    enc_.upload(uc.data(), count, QP, u.data());
+    // (e0, e1) over QP, NTT form, then + u * pk
+    c_.check(shm_sample_cbd(h, x.data(), 2 * count, QP, detail::mix64(seed_, ++ctr_), st));
+    c_.check(shm_ntt_forward(h, x.data(), 2 * count, QP, st));
+    for (uint32_t i = 0; i < count; i++)
+        for (uint32_t k = 0; k < 2; k++) {
+            uint64_t *xi = x.data() + (2 * (size_t)i + k) * row;
+            c_.check(shm_multiply_plain(h, u.data() + i * row, pk_.data() + k * row, t.data(), 1, QP, st));
+            c_.check(shm_add(h, xi, t.data(), xi, 1, QP, st));
+        }
+    // ModDown QP -> Q (divide by P), then the first L limbs
+    DeviceBuffer q(c_, 2 * (size_t)count * nq * N);
+    {
+        DeviceBuffer ws(c_, shm_moddown_ext_workspace_bytes(h, 2 * count, nq) / 8 + 1);
+        c_.check(shm_moddown_ext(h, x.data(), q.data(), 2 * count, nq, ws.data(), ws.words() * 8, st));
+    }
+    Ciphertext ct;
+    ct.count = count;
+    ct.size = 2;
+    ct.L = L;
+    ct.scale_ = scale;
+    if (L == nq) {
+        ct.data = std::move(q);
+    } else {
+        ct.data = DeviceBuffer(c_, 2 * (size_t)count * L * N);
+        c_.check(shm_drop_limbs(h, q.data(), ct.data.data(), 2 * count, nq, L, st));
+    }
+    return ct;
+}
+
+Ciphertext PublicEncryptor::encrypt(const std::vector<std::vector<cplx>> &z, double scale, uint32_t L) {
+    const uint32_t count = (uint32_t)z.size();
+    Ciphertext ct = encrypt_zero(count, L, scale);
+    // + the message on c0
+    const size_t ln = (size_t)L * c_.n;
+    DeviceBuffer m(c_, count * ln);
+    {
+        DeviceBuffer coeffs(c_, (size_t)count * c_.n);
+        enc_.encode_rows(z, scale, coeffs.data());
+        enc_.lift(coeffs.data(), count, L, m.data());
+    }
+    for (uint32_t i = 0; i < count; i++) {
+        uint64_t *c0 = ct.data.data() + 2 * i * ln;
+        c_.check(shm_add(c_.handle(), c0, m.data() + i * ln, c0, 1, L, c_.stream()));
+    }
+    return ct;
+}
+
+Ciphertext PublicEncryptor::encrypt(const Plaintext &pt) {
+    Ciphertext ct = encrypt_zero(1, pt.L, pt.scale);
+    c_.check(shm_add(c_.handle(), ct.data.data(), pt.data.data(), ct.data.data(), 1, pt.L, c_.stream()));
+    return ct;
+}
+
 DeviceBuffer KeyGenerator::galois_key(uint32_t elt) { return switching_key(automorph(s_coeffs_, elt)); }
 
 std::map<uint32_t, DeviceBuffer> KeyGenerator::galois_keys(const std::vector<uint32_t> &elts) {

@@ -272,3 +272,35 @@ def test_device_encoder_matches_host_fft_bit_for_bit():
         err = np.abs(h.decrypt(h.encrypt(z, DELTA, 4)) - z)
         assert err.max() < 1e-6
         h.close()
+
+
+def _public_encrypt_roundtrip(lib):
+    h = Host(12, _small_primes(), 5, hamming_weight=64, seed=21, lib=lib)
+    h.gen_public_key(9)
+    rng = np.random.default_rng(4)
+    z = _z(rng, 3, h.n // 2)
+    outs = []
+    for L in (h.nq, 5):
+        c = h.encrypt_public(z, 2.0 ** 40, L)
+        assert (c.count, c.size, c.level, c.scale) == (3, 2, L, 2.0 ** 40)
+        # fresh public-key noise u e + e0 + e1 s, divided by P: within 1e-7 of the slots at 2^40
+        assert np.abs(h.decrypt(c) - z).max() < 1e-7
+        outs.append(c.to_host())
+    # a second encryption of the same message draws new randomness
+    assert not np.array_equal(h.encrypt_public(z, 2.0 ** 40, h.nq).to_host(), outs[0])
+    return outs
+
+
+def test_public_key_encryption_on_oracle():
+    """encrypt_asymmetric's form (secretkey.cu:15-217): u pk + (e0, e1) over QP, ModDown to Q, message added;
+    decrypts to the slots at the top level and below it."""
+    _public_encrypt_roundtrip(ORACLE_HOST)
+
+
+@pytest.mark.gpu
+def test_public_key_encryption_cuda_matches_oracle_build():
+    """The CUDA build draws the same keys and ciphertexts as the oracle build (counter-based samplers)."""
+    a = _public_encrypt_roundtrip(None)
+    b = _public_encrypt_roundtrip(ORACLE_HOST)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
