@@ -342,6 +342,14 @@ class Evaluator {
     // cores (exact residue GEMMs) or the CUDA-core kernel; both exact.
     Ciphertext ctpt_matmul(const Ciphertext &X, const std::vector<int64_t> &W, uint32_t n_out, double w_scale,
                            bool tensor_cores = true) const;
+    // The masked projection (ct_pt_matrix_mul_wo_pre_w_mask, Ct_pt_matrix_mul.cuh:846-986):
+    // Y[o] = mask * sum_i X[i] W[i][o] slot-wise.  The reference encodes W[i][o] * mask as its own
+    // slot-vector plaintext for every (i, o) (n_in * n_out encodes, one level); here the weights
+    // stay scalars (ctpt_matmul, one level) and the mask is encoded once, at the product's level
+    // with the next prime as its scale, and multiplies every output before a second rescale
+    // (two levels, output scale X.scale * w_scale / q exactly as ctpt_matmul's).  mask: N/2 slots.
+    Ciphertext ctpt_matmul_masked(const Ciphertext &X, const std::vector<int64_t> &W, uint32_t n_out,
+                                  double w_scale, const std::vector<double> &mask, bool tensor_cores = true) const;
 
    private:
     std::vector<uint64_t> residues(double integral, uint32_t L) const;

@@ -109,6 +109,11 @@ int shm_host_multiply_i(shm_host *h, const shm_ct *a, int sign, shm_ct **out);
  * (|W| < 2^40) at w_scale; tensor_cores = 0 runs the CUDA-core kernel (the plain path) */
 int shm_host_ctpt_matmul(shm_host *h, const shm_ct *X, const int64_t *W, uint32_t n_out, double w_scale,
                          int tensor_cores, shm_ct **out);
+/* the masked projection (ct_pt_matrix_mul_wo_pre_w_mask, Ct_pt_matrix_mul.cuh:846-986):
+ * mask [N/2] slot values multiply every output of the ct-pt matmul; one mask plaintext, two
+ * levels (the reference: n_in * n_out masked-weight plaintexts, one level) */
+int shm_host_ctpt_matmul_masked(shm_host *h, const shm_ct *X, const int64_t *W, uint32_t n_out, double w_scale,
+                                const double *mask, int tensor_cores, shm_ct **out);
 /* Polynomial operators (the BERT layer's non-linear functions, src/include/source/non_linear_func/):
  * sum_k coeffs[k] T_k(u), u = (2 x - hi - lo) / (hi - lo), on every slot of an ordinary batch,
  * output at the input's scale; and GELU by gelu_cheb's degree-24 series on [-19.5, 12.5]

@@ -77,6 +77,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_host_to_shared": (i32, [_P, _P, _U32, pp]),
         "shm_host_slice": (i32, [_P, _P, _U32, _U32, pp]),
         "shm_host_ctpt_matmul": (i32, [_P, _P, ctypes.POINTER(ctypes.c_int64), _U32, ctypes.c_double, i32, pp]),
+        "shm_host_ctpt_matmul_masked": (i32, [_P, _P, ctypes.POINTER(ctypes.c_int64), _U32, ctypes.c_double, dp, i32,
+                                              pp]),
         "shm_host_from_shared": (i32, [_P, _P, pp]),
         "shm_boot_create": (i32, [_P, ctypes.c_double, _U32, pp]),
         "shm_boot_destroy": (None, [_P]),
@@ -317,6 +319,16 @@ class Host:
         W = np.ascontiguousarray(W, dtype=np.int64)
         return self._out(self.lib.shm_host_ctpt_matmul, X._c, W.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
                          W.shape[1], w_scale, 1 if tensor_cores else 0)
+
+    def ctpt_matmul_masked(self, X, W: np.ndarray, w_scale: float, mask, tensor_cores: bool = True):
+        """mask (N/2 slot values) times the ct-pt matmul X W: the masked projection, two levels."""
+        W = np.ascontiguousarray(W, dtype=np.int64)
+        m = np.ascontiguousarray(mask, dtype=np.float64)
+        if m.shape != (self.n // 2,):
+            raise ValueError("mask needs N/2 slot values")
+        return self._out(self.lib.shm_host_ctpt_matmul_masked, X._c,
+                         W.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), W.shape[1], w_scale,
+                         m.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1 if tensor_cores else 0)
 
     def chebyshev(self, a, coeffs, lo: float, hi: float):
         """sum_k coeffs[k] T_k(u), u = (2 x - hi - lo) / (hi - lo), slot-wise, at the input's scale."""

@@ -579,6 +579,16 @@ int shm_host_ctpt_matmul(shm_host *h, const shm_ct *X, const int64_t *W, uint32_
     });
 }
 
+int shm_host_ctpt_matmul_masked(shm_host *h, const shm_ct *X, const int64_t *W, uint32_t n_out, double w_scale,
+                                const double *mask, int tensor_cores, shm_ct **out) {
+    return guard([&] {
+        const Ciphertext &x = C(X);
+        if (!W || !mask) throw Error("null weights or mask");
+        put(out, H(h).ev->ctpt_matmul_masked(x, std::vector<int64_t>(W, W + (size_t)x.count * n_out), n_out, w_scale,
+                                             std::vector<double>(mask, mask + H(h).ctx->n / 2), tensor_cores != 0));
+    });
+}
+
 int shm_host_to_shared(shm_host *h, const shm_ct *a, uint32_t members, shm_ct **out) {
     return guard([&] {
         H(h).use_shared(members);

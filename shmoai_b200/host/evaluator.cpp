@@ -466,6 +466,16 @@ Ciphertext Evaluator::ctpt_matmul(const Ciphertext &X, const std::vector<int64_t
     return rescale_to_next(Y);
 }
 
+Ciphertext Evaluator::ctpt_matmul_masked(const Ciphertext &X, const std::vector<int64_t> &W, uint32_t n_out,
+                                         double w_scale, const std::vector<double> &mask, bool tensor_cores) const {
+    if (mask.size() != c_.n / 2) throw Error("mask needs one value per slot");
+    if (X.L < 3) throw Error("masked ct-pt matmul needs two levels and one prime for its output");
+    Ciphertext Z = ctpt_matmul(X, W, n_out, w_scale, tensor_cores);
+    const std::vector<cplx> m(mask.begin(), mask.end());
+    const Plaintext M = enc_.encode(m, Z.L, (double)c_.primes[Z.L - 1]);
+    return rescale_to_next(multiply_plain(Z, M));
+}
+
 Ciphertext Evaluator::to_shared(const Ciphertext &a, uint32_t members) const {
     if (a.shared || a.size != 2) throw Error("to_shared takes ordinary ciphertexts");
     if (!members || a.count % members) throw Error("batch is not a multiple of the group size");

@@ -63,3 +63,35 @@ def test_bias_vec_matches_reference():
 @pytest.mark.gpu
 def test_batch_input_cuda_matches_oracle_build():
     assert np.array_equal(_packing_case(None), _packing_case(ORACLE_HOST))
+
+
+def _masked_case(lib):
+    """The masked projection (ct_pt_matrix_mul_wo_pre_w_mask, Ct_pt_matrix_mul.cuh:846-986) on the packing:
+    Y[o] = bias_vec * sum_i X[i] W[i][o], slot-wise."""
+    log_n, bits, n_sp = O.PARAM_SETS["tiny"]
+    h = Host(log_n, bits=bits, n_special=n_sp, hamming_weight=64, seed=6, lib=lib)
+    h.gen_public_key(4)
+    rng = np.random.default_rng(10)
+    nx, nr, n_in, n_out = 16, 128, 12, 5
+    X = np.clip(rng.normal(size=(nx, nr, n_in)), -4, 4)
+    ct = h.batch_input(X, 2.0 ** 50, h.nq)  # x 2^40 weights / a 50-bit prime: products at 2^40
+    w_scale = 2.0 ** 40
+    W = np.round(rng.normal(0, 0.02, (n_in, n_out)) * w_scale).astype(np.int64)
+    lengths = rng.integers(1, nr + 1, nx)
+    mask = bias_vec(lengths, nx, nr, lib).astype(np.float64)
+    Y = h.ctpt_matmul_masked(ct, W, w_scale, mask)
+    assert (Y.count, Y.level) == (n_out, h.nq - 2)
+    xs = _reference_packing(X)  # [n_in][slots]
+    want = mask[None, :] * ((W.astype(np.float64) / w_scale).T @ xs)
+    got = h.decrypt(Y)[:, : nx * nr]
+    assert np.abs(got - want).max() < 1e-6
+    return Y.to_host()
+
+
+def test_masked_projection_on_oracle():
+    _masked_case(ORACLE_HOST)
+
+
+@pytest.mark.gpu
+def test_masked_projection_cuda_matches_oracle_build():
+    assert np.array_equal(_masked_case(None), _masked_case(ORACLE_HOST))
