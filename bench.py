@@ -391,9 +391,14 @@ def run_boot(args, rank, world, dist):
     clocks = clk.summary()
     side = {}
     if not args.no_extras and world == 1:
-        # after the timed region: the same single-ciphertext calls on this library and on the reference's
-        # own GPU build, one after the other on this GPU
+        # after the timed region, with the bootstrapper's keys and memory pool released: the same
+        # single-ciphertext calls on this library and on the reference's own GPU build, one after the
+        # other on this GPU
+        for obj in (out, ct, bs, h):
+            obj.close()
+        torch.cuda.empty_cache()
         side["ours_same_calls"] = ours_per_ct_leg(dev)
+        torch.cuda.empty_cache()
         side["reference_gpu"] = reference_gpu_leg()
     return {
         "metric": BOOT_METRIC, "value": round(world * B * 1000.0 / ms, 3), "unit": "bootstraps/s",
@@ -774,6 +779,111 @@ def cpu_gelu_sample():
 
 
 # ---------------------------------------------------------------------------
+# config 4: one full-width BERT-base layer (shm_boot_bert_layer)
+
+# the reference's layer chain for the shared-a form (test_single_layer.cuh:503-530): three 46-bit
+# primes where the bootstrap region starts, so every rescale after a bootstrap is by a 46-bit prime
+LAYER_BITS = [51] + [46] * 23 + [51] * 11 + [51] * 5
+LAYER = dict(hidden=768, heads=12, ffn=3072, num_X=256, tokens=128, input_num=128, softmax_iter=13, ln_newt=3,
+             ln_gold=2, gelu_input_level=13, ffn_chunk=256, boot_batch=16, w_scale=2.0 ** 40, ln_var_scale=64.0)
+LAYER_METRIC = "BERT-base layer amortized seconds per input (256 inputs x 128 tokens, hidden 768, 12 heads, FFN 3072)"
+
+
+def run_layer(args, rank, world, dist):
+    """One BERT-base encoder layer per step on 256 inputs x 128 tokens (the column packing fills the 2^15
+    slots): attention (12 heads), SelfOutput, four bootstrap segments of 768 ciphertexts, two LayerNorms,
+    Intermediate, GELU and the masked Final projection.  --shared n: shared-a bootstrap segments
+    (the reference's "sham" form); --shared 0: one ordinary bootstrap per ciphertext (its "orig"
+    form).  Unit: seconds per input (the step's time / 256), lower is better."""
+    import torch
+
+    import shmoai_b200
+    from shmoai_b200 import plain_layer as PL
+    from shmoai_b200.host import Bootstrapper, Host
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = shmoai_b200.lib()
+    S = args.shared
+    cfg = dict(LAYER, members=S, boot_batch=LAYER["boot_batch"] if S else 1)
+    t_setup = time.perf_counter()
+    h = Host(16, bits=LAYER_BITS, n_special=5, hamming_weight=BOOT["h"], seed=0x5EED + rank, device=dev)
+    h.gen_relin_key()
+    h.gen_public_key(0xE0C0 + rank)
+    bs = Bootstrapper(h, BOOT["scale"], BOOT["input_level"])
+    if S:
+        h.gen_shared_keys(S, bs.galois_elts(), hamming_weight=BOOT["h"])
+    else:
+        h.gen_galois_keys(bs.galois_elts())
+    # the attention's 127 rotation keys are made inside each layer call and released after its attention
+    rng = np.random.default_rng(4000 + rank)
+    X = rng.normal(0.0, 1.0, (cfg["num_X"], cfg["tokens"], cfg["hidden"]))
+    w = PL.random_weights(rng, cfg["hidden"], cfg["ffn"])
+    mask = np.ones(h.n // 2, dtype=np.int32)
+    ct = h.batch_input(X, BOOT["scale"], 23)
+    setup_s = time.perf_counter() - t_setup
+    holder = {}
+
+    def step():
+        holder["out"], holder["times"] = bs.bert_layer(ct, w, cfg, mask)
+
+    clk = ClockSampler(dev).start()
+    for _ in range(args.warmup):
+        step()
+        holder["out"].close()
+    torch.cuda.synchronize()
+    _, _ = h.device_memory(reset_peak=True)
+    l0 = lib.shm_kernel_launches()
+    stage_sum = {}
+    ms = timed_steps(torch, lambda: (step(), [stage_sum.__setitem__(k, stage_sum.get(k, 0.0) + v)
+                                              for k, v in holder["times"].items()]), args.steps, dist, None)
+    launches = lib.shm_kernel_launches() - l0
+    _, peak = h.device_memory()
+    out = holder["out"]
+    got = h.decrypt(out).real
+    # end to end: the ciphertext batch written from pinned host memory, the layer, the output read back
+    h_in = torch.from_numpy(ct.to_host().view(np.int64)).pin_memory()
+    h_out = torch.empty((out.count, out.size, out.level, h.n), dtype=torch.int64).pin_memory()
+
+    def e2e_step():
+        ct.write_from_ptr(h_in.data_ptr())
+        step()
+        holder["out"].to_ptr(h_out.data_ptr())
+        holder["out"].close()
+
+    e2e_ms = timed_steps(torch, e2e_step, 1, dist, None) if not args.no_extras else ms
+    clocks = clk.summary()
+    cols = PL.pack_columns(X)
+    approx = PL.layer(cols, w, cfg, mask, approx=True)
+    exact = PL.layer(cols, w, cfg, mask, approx=False)
+    e_a, e_x = np.abs(got - approx), np.abs(got - exact)
+    n_in = cfg["num_X"]
+    stages = {k: round(v / args.steps, 3) for k, v in stage_sum.items()}
+    ref = {"orig": 10.34, "sham": 6.85}
+    return {
+        "metric": LAYER_METRIC, "value": round(ms / 1000.0 / n_in, 5), "unit": "s/input", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (inputs N(0,1); weights N(0, 0.02^2), LayerNorm gamma 1 beta 0; every token valid)",
+        "config": {"workload": "layer: one BERT-base encoder layer per GPU per step ("
+                               + ("shared-a bootstrap segments, groups of %d" % S if S else
+                                  "one ordinary bootstrap per ciphertext") + ")",
+                   "form": "sham" if S else "orig", "N": h.n, "Q": "[51]+23x[46]+11x[51]", "P": "5x[51]",
+                   "inputs": n_in, "tokens": cfg["tokens"], "hidden": cfg["hidden"], "heads": cfg["heads"],
+                   "ffn": cfg["ffn"], "stage_seconds": stages, "total_seconds": round(ms / 1000.0, 2),
+                   "setup_seconds": round(setup_s, 1),
+                   "error_vs_fp64_same_approximations": {"mean": float(e_a.mean()), "max": float(e_a.max())},
+                   "error_vs_fp64_exact_layer": {"mean": float(e_x.mean()), "max": float(e_x.max())},
+                   "device_gb_peak": round(peak / 2 ** 30, 2),
+                   "reference_published_s_per_input": ref["sham" if S else "orig"],
+                   "l2": "not flushed: every stage's live data exceeds the 126 MB L2"},
+        "e2e": {"value": round(e2e_ms / 1000.0 / n_in, 5), "unit": "s/input",
+                "h2d_bytes_per_step": int(h_in.numel() * 8), "d2h_bytes_per_step": int(h_out.numel() * 8)},
+        "gpu_launches": int(launches), "roofline": None, "clocks": clocks,
+    }
+
+
+# ---------------------------------------------------------------------------
 # kernel workloads (config 2 and the profiling cases)
 
 CTPT = dict(n_in=768, n_out=768, L=13)  # config 2: one BERT-base projection at level 12
@@ -960,7 +1070,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks", "serve", "gelu"])
+    ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks", "serve", "gelu",
+                                                            "layer"])
     ap.add_argument("--batch", type=int, default=None)
     ap.add_argument("--shared", type=int, default=8,
                     help="boot: shared-a group size n (0 = ordinary ciphertexts)")
@@ -1054,7 +1165,7 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
     runner = {"boot": run_boot, "prim": run_prim, "ctpt": run_ctpt, "serve": run_serve, "ntt": run_kernel_case,
-              "ks": run_kernel_case, "gelu": run_gelu}[args.workload]
+              "ks": run_kernel_case, "gelu": run_gelu, "layer": run_layer}[args.workload]
     res = runner(args, rank, world, dist)
     if rank == 0:
         if not args.no_cpu_baseline and args.workload in ("boot", "prim", "gelu"):

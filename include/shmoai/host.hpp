@@ -439,8 +439,11 @@ Ciphertext batch_broadcast(const Evaluator &ev, const Ciphertext &one, uint32_t 
 // LayerNorm over the hidden columns of the column packing, one column per ciphertext of the
 // batch (layernorm, layernorm.cuh:899-): gamma_i (x_i - mean) / sqrt(var) + beta_i with the
 // inverse square root above; 2 (d_newt + d_gold) + 8 levels
+// var_scale c > 0 brings the variance into the inverse square root's first-guess range: the
+// iteration runs on c var (the factor joins the 1/d of the mean of squares) and sqrt(c) joins
+// gamma, so no level is added (the reference's guess line suits variances of about 10..1000)
 Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &gamma,
-                     const std::vector<double> &beta, int d_newt = 4, int d_gold = 2);
+                     const std::vector<double> &beta, int d_newt = 4, int d_gold = 2, double var_scale = 1.0);
 // attention's ciphertext-ciphertext product in the column packing (ct_ct_matrix_mul_colpacking,
 // Ct_ct_matrix_mul.cuh:10-120): X and W batches of the same count; output batch of `rows`,
 // out_i = sum_j X_j * rot(W_j, i * num_batch) relinearised and rescaled (1 level); needs the
@@ -463,6 +466,12 @@ Ciphertext ct_ct_matmul_diagpacking(const Evaluator &ev, const Ciphertext &X, co
 // steps) times each member; iter + 10 levels
 Ciphertext softmax_attention(const Evaluator &ev, const Ciphertext &x, const std::vector<int> &bias_vec,
                              int input_num, int iter);
+// the same softmax in two parts around a bootstrap of the members' sum (softmax_boot,
+// softmax.cuh:512-): the shifted, exponentiated and masked members (8 levels), then, given the
+// sum (refreshed by the caller), its inverse times every member (iter + 2 levels of the sum)
+Ciphertext softmax_attention_numerators(const Evaluator &ev, const Ciphertext &x, const std::vector<int> &bias_vec,
+                                        int input_num);
+Ciphertext softmax_attention_finish(const Evaluator &ev, const Ciphertext &e, const Ciphertext &sum, int iter);
 // softmax over the members of a batch (softmax.cuh:119-, without the attention layout's masks):
 // e_i / sum_j e_j with e_i = exp_approx(x_i - shift) and the sum's inverse by inverse_approx on
 // sum_scale * sum_j e_j, which the caller brings into (0, 2); iter + 12 levels
@@ -525,6 +534,54 @@ class BatchBootstrapper {
     double q0_ = 0, c_fin_ = 0;
     uint32_t top_ = 0;
 };
+
+// ---- one BERT encoder layer (layer.cpp; src/include/test/test_single_layer.cuh:422-2062)
+
+struct BertLayerConfig {
+    uint32_t hidden = 768, heads = 12, ffn = 3072;
+    uint32_t num_X = 256, tokens = 128;  // inputs x tokens fill the N/2 slots (column packing)
+    uint32_t input_num = 128;            // the softmax masks' band (softmax.cuh): valid tokens per input
+    int softmax_iter = 13;               // inverse iterations of the softmax's sum
+    int ln_newt = 3, ln_gold = 2;        // LayerNorm's inverse square root: 2 (newt + gold) + 8 levels
+    double ln_var_scale = 64.0;          // see layernorm
+    double w_scale = 1099511627776.0;    // 2^40: integer weights of the exact contractions
+    uint32_t gelu_input_level = 13;      // GELU (6 levels) then the masked Final (2) and one to adjust
+    uint32_t ffn_chunk = 256;            // Intermediate + GELU columns per pass (bounds the working set)
+    uint32_t members = 0;                // shared-a group size of the bootstrap segments; 0 = ordinary
+    uint32_t boot_batch = 16;            // ciphertexts per bootstrap call (1 = one per call)
+};
+
+// row-major [in][out] weight matrices and per-column vectors
+struct BertLayerWeights {
+    std::vector<double> Wq, Wk, Wv, Wo;  // [hidden][hidden]
+    std::vector<double> bq, bk, bv, bo, ln1_gamma, ln1_beta, ln2_gamma, ln2_beta, bf;  // [hidden]
+    std::vector<double> Wi, bi;  // [hidden][ffn], [ffn]
+    std::vector<double> Wf;      // [ffn][hidden]
+};
+
+struct StageTime {
+    std::string name;
+    double seconds;
+};
+
+// the steps of the attention's rotations (multiples of N/2 / tokens); generate their Galois keys
+std::vector<int> bert_layer_rotation_steps(const BertLayerConfig &cfg, uint32_t slots);
+// column o of Y plus b[o] on the slots marked 1 by mask (all slots when mask is empty)
+Ciphertext add_column_bias(const Evaluator &ev, const Ciphertext &Y, const std::vector<double> &b,
+                           const std::vector<int> &mask);
+// x brought to the bootstrap's input level and scale, then bootstrapped in calls of `batch`
+// ciphertexts (shared-a groups of `members`, a short last group padded; 0 = ordinary)
+Ciphertext bootstrap_segment(const Evaluator &ev, const BatchBootstrapper &boot, const Ciphertext &x,
+                             uint32_t members, uint32_t batch);
+// One layer on X (hidden columns at the bootstrap's output level and scale); the output has X's
+// level and scale.  ev needs the relinearisation key, the Galois keys of the bootstrap (ordinary)
+// or the shared-a keys of `members`, and the Galois keys of bert_layer_rotation_steps: either in
+// ev.galois_keys or, with attention_keys, made from that key generator for the attention block
+// and released after it (their time counts in the block).  times receives the 11 stages in the
+// reference's names and order.
+Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const Ciphertext &X,
+                      const BertLayerWeights &w, const BertLayerConfig &cfg, const std::vector<int> &bias_vec,
+                      std::vector<StageTime> *times = nullptr, KeyGenerator *attention_keys = nullptr);
 
 // max |V w - layers(w)| / max |V w| of the slot-transform factorisation at n slots
 // (a self-check of the planning code on random input)

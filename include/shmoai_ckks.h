@@ -165,6 +165,17 @@ size_t shm_shared_rotate_workspace_bytes(const shm_context *ctx, uint32_t n_grou
 int shm_shared_rotate_hoisted(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members,
                               uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs,
                               uint32_t L, void *workspace, size_t workspace_bytes, void *stream);
+/* Sh-Rot of every group by one Galois element in the reference's order: the automorphism
+ * on a and every b first, then one ModUp of the rotated a, the n + 1 inner products and
+ * ModDowns (shared_a_rotate, ShRotate.cu:201-257; bit for bit the reference's limbs).  The
+ * hoisted entry point above applies the automorphism to the extended digits after the
+ * ModUp instead (one ModUp for every element): the same rotation up to the base
+ * conversion's overflow multiples of Q, so it decrypts the same but its limbs differ. */
+size_t shm_shared_rotate_one_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                             uint32_t L);
+int shm_shared_rotate(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members, uint32_t elt,
+                      const uint64_t *key, uint64_t *out, uint32_t L, void *workspace, size_t workspace_bytes,
+                      void *stream);
 /* FmtSwitch forward: n_groups * n_members ordinary ciphertexts [.][2][L][N] under s
  * -> shared-a batch [n_groups][n_members + 1][L][N] under s'_i, with the format key
  * [n_members][n_members + 1][QP][N] (halves B_fmt[j][0..n-1], a_fmt[j]); the a_j are

@@ -171,6 +171,21 @@ int shm_boot_galois_elts(const shm_boot *b, uint32_t *out, uint32_t cap, uint32_
  * members = n: shared-a groups of n consecutive ciphertexts (keys from
  * shm_host_gen_shared_keys) */
 int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out);
+/* One BERT encoder layer (src/include/test/test_single_layer.cuh:422-2062) on X: hidden
+ * columns in the column packing at the bootstrap's output level and scale.
+ * dims: hidden, heads, ffn, num_X, tokens, input_num, softmax_iter, ln_newt, ln_gold,
+ *       gelu_input_level, ffn_chunk, members (shared-a group size of the bootstrap segments,
+ *       0 = ordinary), boot_batch (ciphertexts per bootstrap call);
+ * reals: w_scale (integer weights of the contractions), ln_var_scale;
+ * weights: Wq [d][d], bq [d], Wk, bk, Wv, bv, Wo, bo, ln1_gamma [d], ln1_beta [d],
+ *          Wi [d][ffn], bi [ffn], Wf [ffn][d], bf [d], ln2_gamma, ln2_beta, concatenated;
+ * bias_vec: N/2 ints (1 = valid token slot).  The host needs the relinearisation key, the Galois
+ * keys of the attention's rotation steps (multiples of N/2 / tokens) and, for members = 0, of the
+ * bootstrap, else the shared-a keys of groups of `members`.  stage_seconds receives 11 wall
+ * times: Attention Block, SelfOutput, 1st Bootstrapping, LayerNorm1, 2nd Bootstrapping,
+ * Intermediate Linear, GELU, Final Linear, 3rd Bootstrapping, LayerNorm2, 4th Bootstrapping. */
+int shm_boot_bert_layer(shm_boot *b, const shm_ct *X, const uint32_t *dims, const double *reals, const double *weights,
+                        const int *bias_vec, shm_ct **out, double *stage_seconds);
 /* autotuning for batches of `count` (shmoai::BatchBootstrapper::tune): NTT tile, Sh-Rot
  * inner-product chunk, BSGS split per slot-transform layer; call before generating the
  * Galois / Sh-Galois keys (shm_boot_galois_elts changes with the split).  Writes a JSON

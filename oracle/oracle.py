@@ -244,6 +244,11 @@ class Oracle:
         lib().orc_exact_extend(self._h, _p(a), m, L, _p(out))
         return out
 
+    def shared_rotate(self, sh, elt, key):
+        """Sh-Rot of one group [n+1][L][N] in the reference's order (ShRotate.cu:218-256): the automorphism on
+        every row first, then one ModUp of the rotated a and the key switch."""
+        return self.shared_rotate_hoisted(self.apply_galois(sh, elt), [1], [key])[0]
+
     def fmt_forward(self, cts, key):
         """[n][2][L][N] ciphertexts under s -> one shared-a group [n+1][L][N]."""
         m, _, L, _ = cts.shape

@@ -820,6 +820,39 @@ size_t shm_shared_rotate_workspace_bytes(const shm_context *ctx, uint32_t n_grou
     return 0;
 }
 
+size_t shm_shared_rotate_one_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                             uint32_t L) {
+    (void)ctx;
+    (void)n_groups;
+    (void)n_members;
+    (void)L;
+    return 0;
+}
+
+/* the reference's order (ShRotate.cu:218-256): the automorphism on every row, then the
+ * hoisted key switch with the identity element */
+int shm_shared_rotate(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members, uint32_t elt,
+                      const uint64_t *key, uint64_t *out, uint32_t L, void *workspace, size_t workspace_bytes,
+                      void *stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    (void)stream;
+    if (!ks_level(ctx, L)) return fail("level out of range for key switching");
+    if (!key || !out || !n_members || out == sh) return fail("bad shared-a rotation arguments");
+    if (elt % 2 == 0 || elt >= 2 * ctx->c->n) return fail("Galois element must be odd and below 2N");
+    size_t gl = (size_t)(n_members + 1) * L * ctx->c->n;
+    uint64_t *rot = (uint64_t *)malloc(gl * 8);
+    const uint32_t one = 1;
+    const uint64_t *k = key;
+    for (uint32_t g = 0; g < n_groups; g++) {
+        orc_apply_galois(ctx->c, sh + g * gl, rot, n_members + 1, L, elt);
+        uint64_t *o = out + g * gl;
+        orc_shared_rotate_hoisted(ctx->c, rot, n_members, L, 1, &one, &k, (uint64_t *const *)&o);
+    }
+    free(rot);
+    return SHM_OK;
+}
+
 int shm_shared_rotate_hoisted(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members,
                               uint32_t n_elts, const uint32_t *elts, const uint64_t *const *keys, uint64_t *const *outs,
                               uint32_t L, void *workspace, size_t workspace_bytes, void *stream) {

@@ -69,6 +69,8 @@ def _declare(L):
         "shm_ctpt_matmul_cuda_core": (ctypes.c_int, [_P, _P, _P, _P, _U32, _U32, _U32, _P]),
         "shm_ctpt_matmul": (ctypes.c_int, [_P, _P, _P, _P, _U32, _U32, _U32, _P, _SZ, _P]),
         "shm_shared_rotate_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),
+        "shm_shared_rotate_one_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),
+        "shm_shared_rotate": (ctypes.c_int, [_P, _P, _U32, _U32, _U32, _P, _P, _U32, _P, _SZ, _P]),
         "shm_shared_rotate_hoisted": (ctypes.c_int, [_P, _P, _U32, _U32, _U32, ctypes.POINTER(_U32),
                                                      ctypes.POINTER(_P), ctypes.POINTER(_P), _U32, _P, _SZ, _P]),
         "shm_fmt_switch_forward_workspace_bytes": (_SZ, [_P, _U32, _U32, _U32]),

@@ -280,6 +280,16 @@ class CKKSContext:
                                               _stream(stream)))
         return outs
 
+    def shared_rotate(self, sh, elt: int, key, stream=None):
+        """Shared-a groups [G][n + 1][L][N]: Sh-Rot by one element in the reference's order
+        (automorphism, then ModUp of a; ShRotate.cu:201-257)."""
+        G, H, L = sh.shape[0], sh.shape[1], sh.shape[2]
+        out = torch.empty_like(sh)
+        ws = self.empty(max(1, lib().shm_shared_rotate_one_workspace_bytes(self._h, G, H - 1, L) // 8))
+        check(lib().shm_shared_rotate(self._h, _ptr(sh), G, H - 1, elt, _ptr(key), _ptr(out), L, _ptr(ws),
+                                      ws.numel() * 8, _stream(stream)))
+        return out
+
     def fmt_forward(self, cts, n, key, stream=None):
         """[G * n][2][L][N] ciphertexts under s -> [G][n + 1][L][N] shared-a groups."""
         m, L = cts.shape[0], cts.shape[2]

@@ -558,6 +558,36 @@ int shm_shared_rotate_hoisted(const shm_context *ctx, const uint64_t *sh, uint32
     });
 }
 
+size_t shm_shared_rotate_one_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
+                                             uint32_t L) {
+    if (!ctx || !ctx->c) return 0;
+    const size_t rot = (size_t)n_groups * (n_members + 1) * L * ctx->c->n;
+    return (rot + shm::shared_rotate_ws_words(*ctx->c, n_groups, n_members, L)) * 8;
+}
+
+// the reference's order (ShRotate.cu:218-256): the automorphism on a and every b first, then
+// ModUp of the rotated a, the inner products and ModDown; the hoisted entry point with the
+// identity element runs the key-switch half
+int shm_shared_rotate(const shm_context *ctx, const uint64_t *sh, uint32_t n_groups, uint32_t n_members, uint32_t elt,
+                      const uint64_t *key, uint64_t *out, uint32_t L, void *workspace, size_t workspace_bytes,
+                      void *stream) {
+    return guard([&] {
+        auto &c = const_cast<shm::Context &>(ctx_of(ctx));
+        check_level(c, L);
+        if (!key || !out || n_members == 0) throw std::invalid_argument("bad shared-a rotation arguments");
+        if (out == sh) throw std::invalid_argument("the output must not alias the input");
+        if (elt % 2 == 0 || elt >= 2 * c.n) throw std::invalid_argument("Galois element must be odd and below 2N");
+        set_device(c);
+        const size_t rot = (size_t)n_groups * (n_members + 1) * L * c.n;
+        uint64_t *ws = ws_of(c, workspace, workspace_bytes, rot + shm::shared_rotate_ws_words(c, n_groups, n_members, L));
+        shm::apply_galois(c, sh, ws, (uint32_t)((size_t)n_groups * (n_members + 1) * L), elt, S(stream));
+        const uint32_t one = 1;
+        const uint64_t *k = key;
+        uint64_t *o = out;
+        shm::shared_rotate_hoisted(c, ws, n_groups, n_members, L, 1, &one, &k, &o, ws + rot, S(stream));
+    });
+}
+
 size_t shm_fmt_switch_forward_workspace_bytes(const shm_context *ctx, uint32_t n_groups, uint32_t n_members,
                                               uint32_t L) {
     return ctx && ctx->c ? shm::fmt_forward_ws_words(*ctx->c, n_groups, n_members, L) * 8 : 0;

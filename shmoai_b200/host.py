@@ -84,6 +84,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_boot_destroy": (None, [_P]),
         "shm_boot_galois_elts": (i32, [_P, ctypes.POINTER(_U32), _U32, ctypes.POINTER(_U32)]),
         "shm_boot_run": (i32, [_P, _P, _U32, pp]),
+        "shm_boot_bert_layer": (i32, [_P, _P, ctypes.POINTER(_U32), dp, dp, ctypes.POINTER(ctypes.c_int), pp, dp]),
         "shm_boot_capture": (i32, [_P, _P, _U32, pp, pp]),
         "shm_boot_tune": (i32, [_P, _U32, _U32, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
         "shm_boot_get_split": (i32, [_P, ctypes.POINTER(ctypes.c_int)]),
@@ -131,6 +132,10 @@ def load(path: str | None = None) -> ctypes.CDLL:
         f.argtypes = args
     _libs[path] = L
     return L
+
+
+BERT_STAGES = ["Attention Block", "SelfOutput", "1st Bootstrapping", "LayerNorm1", "2nd Bootstrapping",
+               "Intermediate Linear", "GELU", "Final Linear", "3rd Bootstrapping", "LayerNorm2", "4th Bootstrapping"]
 
 
 class HostError(RuntimeError):
@@ -472,6 +477,27 @@ class Bootstrapper:
         o = _P()
         self.host._check(self.host.lib.shm_boot_run(self._b, ct._c, members, ctypes.byref(o)))
         return Ct(self.host, o)
+
+    def bert_layer(self, X: Ct, weights: dict, cfg: dict, bias_vec) -> tuple[Ct, dict]:
+        """One BERT encoder layer (shm_boot_bert_layer) -> (output, {stage: seconds})."""
+        d, F = cfg["hidden"], cfg["ffn"]
+        order = [("Wq", d * d), ("bq", d), ("Wk", d * d), ("bk", d), ("Wv", d * d), ("bv", d), ("Wo", d * d),
+                 ("bo", d), ("ln1_gamma", d), ("ln1_beta", d), ("Wi", d * F), ("bi", F), ("Wf", F * d), ("bf", d),
+                 ("ln2_gamma", d), ("ln2_beta", d)]
+        flat = np.concatenate([np.ascontiguousarray(weights[k], dtype=np.float64).reshape(-1) for k, n in order])
+        assert flat.size == sum(n for _, n in order), "weight shapes"
+        keys = ["hidden", "heads", "ffn", "num_X", "tokens", "input_num", "softmax_iter", "ln_newt", "ln_gold",
+                "gelu_input_level", "ffn_chunk", "members", "boot_batch"]
+        dims = (_U32 * len(keys))(*[int(cfg[k]) for k in keys])
+        reals = np.array([cfg.get("w_scale", 2.0 ** 40), cfg.get("ln_var_scale", 64.0)], dtype=np.float64)
+        bv = np.ascontiguousarray(bias_vec, dtype=np.int32)
+        secs = np.zeros(11, dtype=np.float64)
+        dp = ctypes.POINTER(ctypes.c_double)
+        o = _P()
+        self.host._check(self.host.lib.shm_boot_bert_layer(
+            self._b, X._c, dims, reals.ctypes.data_as(dp), flat.ctypes.data_as(dp),
+            bv.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(o), secs.ctypes.data_as(dp)))
+        return Ct(self.host, o), dict(zip(BERT_STAGES, secs.tolist()))
 
     def tune(self, count: int, members: int = 0) -> list[dict]:
         """Autotune for batches of `count` (shm_boot_tune); generate Galois keys afterwards."""

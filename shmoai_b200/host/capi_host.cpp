@@ -639,6 +639,67 @@ int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out) 
     });
 }
 
+int shm_boot_bert_layer(shm_boot *b, const shm_ct *X, const uint32_t *dims, const double *reals, const double *weights,
+                        const int *bias_vec, shm_ct **out, double *stage_seconds) {
+    return guard([&] {
+        if (!b || !dims || !reals || !weights || !bias_vec) throw Error("null argument");
+        BertLayerConfig cfg;
+        cfg.hidden = dims[0];
+        cfg.heads = dims[1];
+        cfg.ffn = dims[2];
+        cfg.num_X = dims[3];
+        cfg.tokens = dims[4];
+        cfg.input_num = dims[5];
+        cfg.softmax_iter = (int)dims[6];
+        cfg.ln_newt = (int)dims[7];
+        cfg.ln_gold = (int)dims[8];
+        cfg.gelu_input_level = dims[9];
+        cfg.ffn_chunk = dims[10];
+        cfg.members = dims[11];
+        cfg.boot_batch = dims[12];
+        cfg.w_scale = reals[0];
+        cfg.ln_var_scale = reals[1];
+        const size_t d = cfg.hidden, F = cfg.ffn;
+        const double *p = weights;
+        auto take = [&](size_t n) {
+            std::vector<double> v(p, p + n);
+            p += n;
+            return v;
+        };
+        BertLayerWeights w;
+        w.Wq = take(d * d);
+        w.bq = take(d);
+        w.Wk = take(d * d);
+        w.bk = take(d);
+        w.Wv = take(d * d);
+        w.bv = take(d);
+        w.Wo = take(d * d);
+        w.bo = take(d);
+        w.ln1_gamma = take(d);
+        w.ln1_beta = take(d);
+        w.Wi = take(d * F);
+        w.bi = take(F);
+        w.Wf = take(F * d);
+        w.bf = take(d);
+        w.ln2_gamma = take(d);
+        w.ln2_beta = take(d);
+        if (cfg.members) b->h->use_shared(cfg.members);
+        Evaluator &ev = *b->h->ev;
+        ev.galois_keys = &b->h->galois;
+        std::vector<StageTime> t;
+        const size_t slots = b->h->ctx->n / 2;
+        // the attention's rotation keys: the host's own where it has them all, else made for the
+        // attention block and released after it
+        bool have_all = true;
+        for (int st : bert_layer_rotation_steps(cfg, (uint32_t)slots))
+            if (!b->h->galois.count(ev.galois_elt(st))) have_all = false;
+        put(out, bert_layer(ev, *b->b, C(X), w, cfg, std::vector<int>(bias_vec, bias_vec + slots), &t,
+                            have_all ? nullptr : b->h->kg.get()));
+        if (stage_seconds)
+            for (size_t i = 0; i < t.size(); i++) stage_seconds[i] = t[i].seconds;
+    });
+}
+
 namespace {
 
 std::string json_str(const std::string &v) {

@@ -30,16 +30,24 @@ Ciphertext ct_ct_matmul_colpacking(const Evaluator &ev, const Ciphertext &X, con
     if (X.shared || W.shared || X.size != 2 || W.size != 2) throw Error("ct-ct matmul takes ordinary ciphertexts");
     if (X.count != W.count || X.count == 0) throw Error("ct-ct matmul: X and W need the same number of columns");
     if (rows == 0) throw Error("ct-ct matmul: no output rows");
-    std::vector<int> steps;
-    for (uint32_t i = 1; i < rows; i++) steps.push_back((int)(i * num_batch));
-    const std::map<int, Ciphertext> rot = ev.rotate_many(W, steps);
+    // the rotated copies of W are made a chunk of steps at a time (one hoisted ModUp per chunk), so
+    // at most ~8 GB of them are live: at full width a head's 127 rotations of 64 ciphertexts would
+    // otherwise hold 170 GB
+    const size_t w_bytes = W.polys() * W.L * ev.context().n * 8;
+    const uint32_t chunk = (uint32_t)std::max<size_t>(1, (size_t(8) << 30) / std::max<size_t>(w_bytes, 1));
     std::vector<Ciphertext> outs;
     outs.reserve(rows);
-    for (uint32_t i = 0; i < rows; i++) {
-        const int step = (int)(i * num_batch);
-        auto it = rot.find(step);
-        const Ciphertext &Wi = (i == 0 || it == rot.end()) ? W : it->second;  // a full turn is W itself
-        outs.push_back(ev.relinearize_rescale(sum_members(ev, ev.multiply_lazy(X, Wi))));
+    for (uint32_t lo = 0; lo < rows; lo += chunk) {
+        const uint32_t hi = std::min(rows, lo + chunk);
+        std::vector<int> steps;
+        for (uint32_t i = std::max(lo, 1u); i < hi; i++) steps.push_back((int)(i * num_batch));
+        const std::map<int, Ciphertext> rot = ev.rotate_many(W, steps);
+        for (uint32_t i = lo; i < hi; i++) {
+            const int step = (int)(i * num_batch);
+            auto it = rot.find(step);
+            const Ciphertext &Wi = (i == 0 || it == rot.end()) ? W : it->second;  // a full turn is W itself
+            outs.push_back(ev.relinearize_rescale(sum_members(ev, ev.multiply_lazy(X, Wi))));
+        }
     }
     return batch_gather(ev, outs);
 }

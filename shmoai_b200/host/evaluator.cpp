@@ -35,7 +35,7 @@ Ciphertext Evaluator::like(const Ciphertext &a, uint32_t L) const {
 std::vector<uint64_t> Evaluator::residues(double v, uint32_t L) const {
     std::vector<uint64_t> r(L, 0);
     if (v == 0.0) return r;
-    if (!std::isfinite(v) || v != std::nearbyint(v)) throw Error("constant is not an integer");
+    if (!std::isfinite(v) || v != std::nearbyint(v)) throw Error("constant is not an integer: " + std::to_string(v));
     const bool neg = v < 0;
     int e = 0;
     const double m = std::frexp(std::fabs(v), &e);

@@ -149,24 +149,39 @@ Ciphertext batch_gather(const Evaluator &ev, const std::vector<Ciphertext> &part
 // mean and variance are sums over the batch, the inverse square root is inv_sqrt_approx, and
 // column i gets gamma_i (x_i - mean) / sqrt(var) + beta_i; 2 (d_newt + d_gold) + 8 levels
 Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &gamma,
-                     const std::vector<double> &beta, int d_newt, int d_gold) {
+                     const std::vector<double> &beta, int d_newt, int d_gold, double var_scale) {
     need_ordinary(x, "layernorm");
+    if (!(var_scale > 0)) throw Error("layernorm: var_scale must be positive");
     const uint32_t d = x.count;
     if (d == 0 || gamma.size() != d || beta.size() != d) throw Error("layernorm: gamma and beta need one value per column");
     const uint32_t need = 2 * (uint32_t)(d_newt + d_gold) + 9;
     if (x.L < need) throw Error("layernorm needs " + std::to_string(need) + " primes");
     const Context &c = ev.context();
     const double S = x.scale_;
-    auto broadcast = [&](const Ciphertext &one) { return gather_ptrs(ev, std::vector<const Ciphertext *>(d, &one)); };
+    auto broadcast = [&](const Ciphertext &one, uint32_t k) {
+        return gather_ptrs(ev, std::vector<const Ciphertext *>(k, &one));
+    };
+    // columns are squared and normalised in chunks so that at most a chunk's temporaries sit beside the
+    // centred batch (at full width a whole-batch temporary is ~15 GB); the modular sums are the same
+    const uint32_t chunk = std::min<uint32_t>(d, 128);
     const Ciphertext mean = ev.multiply_const(batch_sum(ev, x), 1.0 / d, S);
-    const Ciphertext xc = ev.sub(ev.mod_switch_to(x, mean.L), broadcast(mean));
-    const Ciphertext sq = square(ev, xc);
-    const Ciphertext var = ev.multiply_const(batch_sum(ev, sq), 1.0 / d, (double)c.primes[sq.L - 2]);
+    const Ciphertext xc = ev.sub(ev.mod_switch_to(x, mean.L), broadcast(mean, d));
+    Ciphertext sq_sum;
+    for (uint32_t lo = 0; lo < d; lo += chunk) {
+        Ciphertext part = batch_sum(ev, square(ev, ev.slice(xc, lo, std::min(chunk, d - lo))));
+        sq_sum = sq_sum.count ? ev.add(sq_sum, part) : std::move(part);
+    }
+    const Ciphertext var = ev.multiply_const(sq_sum, var_scale / d, (double)c.primes[sq_sum.L - 2]);
     const Ciphertext inv = inv_sqrt_approx(ev, var, d_newt, d_gold);
-    const Ciphertext y = product(ev, xc, broadcast(inv));
+    const double rs = std::sqrt(var_scale);
     std::vector<Ciphertext> cols;
     cols.reserve(d);
-    for (uint32_t i = 0; i < d; i++) cols.push_back(ev.add_const(ev.multiply_const(ev.slice(y, i, 1), gamma[i], S), beta[i]));
+    for (uint32_t lo = 0; lo < d; lo += chunk) {
+        const uint32_t k = std::min(chunk, d - lo);
+        const Ciphertext y = product(ev, ev.slice(xc, lo, k), broadcast(inv, k));
+        for (uint32_t i = 0; i < k; i++)
+            cols.push_back(ev.add_const(ev.multiply_const(ev.slice(y, i, 1), gamma[lo + i] * rs, S), beta[lo + i]));
+    }
     return batch_gather(ev, cols);
 }
 
@@ -217,11 +232,27 @@ Ciphertext add_slot_vectors(const Evaluator &ev, const Ciphertext &a, const std:
 Ciphertext softmax_attention(const Evaluator &ev, const Ciphertext &x, const std::vector<int> &bias_vec,
                              int input_num, int iter) {
     need_ordinary(x, "softmax");
+    const uint32_t need = (uint32_t)iter + 11;
+    if (x.L < need) throw Error("softmax needs " + std::to_string(need) + " primes");
+    const Ciphertext e = softmax_attention_numerators(ev, x, bias_vec, input_num);
+    return softmax_attention_finish(ev, e, batch_sum(ev, e), iter);
+}
+
+// the members' sum inverted (inverse_approx, iter steps) and multiplied into every member
+Ciphertext softmax_attention_finish(const Evaluator &ev, const Ciphertext &e, const Ciphertext &sum, int iter) {
+    need_ordinary(e, "softmax");
+    if (sum.count != 1) throw Error("softmax: one sum ciphertext");
+    const Ciphertext inv = inverse_approx(ev, sum, iter);
+    return product(ev, e, gather_ptrs(ev, std::vector<const Ciphertext *>(e.count, &inv)));
+}
+
+Ciphertext softmax_attention_numerators(const Evaluator &ev, const Ciphertext &x, const std::vector<int> &bias_vec,
+                                        int input_num) {
+    need_ordinary(x, "softmax");
     const Context &c = ev.context();
     const size_t slots = c.n / 2;
     if (bias_vec.size() != slots) throw Error("softmax: bias_vec needs one entry per slot");
-    const uint32_t need = (uint32_t)iter + 11;
-    if (x.L < need) throw Error("softmax needs " + std::to_string(need) + " primes");
+    if (x.L < 9) throw Error("softmax's exp needs 8 levels and one prime for its output");
     const int num = (int)x.count, nb = (int)(slots / 128);
     // which bias slots member i treats as its own: all (i = 0), a prefix, none, or a suffix
     auto selected = [&](int i, size_t s) {
@@ -244,9 +275,7 @@ Ciphertext softmax_attention(const Evaluator &ev, const Ciphertext &x, const std
         if (any) shift[i] = std::move(sh);
         sub[i] = std::move(sb);
     }
-    const Ciphertext e = add_slot_vectors(ev, exp_approx(ev, add_slot_vectors(ev, x, shift)), sub);
-    const Ciphertext inv = inverse_approx(ev, batch_sum(ev, e), iter);
-    return product(ev, e, gather_ptrs(ev, std::vector<const Ciphertext *>(x.count, &inv)));
+    return add_slot_vectors(ev, exp_approx(ev, add_slot_vectors(ev, x, shift)), sub);
 }
 
 }  // namespace shmoai

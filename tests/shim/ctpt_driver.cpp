@@ -58,10 +58,10 @@ int main(int argc, char **argv) {
         for (size_t ind = 0; ind < slot_count; ++ind) {
             const int j = (int)(ind / num_X);  // token row of slot num_X * j + input
             const double want = j < num_row ? (j + 1.0) * num_col / 128.0 : 0.0;
-            max_err = fmax(max_err, fabs(result[ind] - want));
+            max_err = fmax(max_err, fabs(result[ind] - want) / fmax(1.0, fabs(want)));
         }
     }
-    printf("outputs %d chain_index %zu coeff_modulus_size %zu scale_log2 %.3f max_err %.3e\n", col_W,
+    printf("outputs %d chain_index %zu coeff_modulus_size %zu scale_log2 %.3f max_rel_err %.3e\n", col_W,
            ct_pt_mul[0].chain_index(), ct_pt_mul[0].coeff_modulus_size(), log2(ct_pt_mul[0].scale()), max_err);
-    return max_err < 1e-3 ? 0 : 1;
+    return max_err < 1e-5 ? 0 : 1;
 }
