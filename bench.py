@@ -221,7 +221,7 @@ def reference_gpu_leg(ctpt_cols: int = 64):
         try:
             r = subprocess.run([REF_GOLDEN, name, "time", str(cols)], capture_output=True, text=True, timeout=900)
             if r.returncode != 0:
-                out[name] = {"error": (r.stderr or r.stdout)[-300:]}
+                out[name] = {"error": "rc %d: %s | %s" % (r.returncode, r.stderr[-300:], r.stdout[-300:])}
                 continue
             out[name] = _json_doc(r.stdout)["time"]
         except Exception as e:  # reported, not fatal: the leg is a side measurement

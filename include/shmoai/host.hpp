@@ -22,6 +22,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -448,8 +449,10 @@ Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector
 // Ct_ct_matrix_mul.cuh:10-120): X and W batches of the same count; output batch of `rows`,
 // out_i = sum_j X_j * rot(W_j, i * num_batch) relinearised and rescaled (1 level); needs the
 // Galois keys of the steps i * num_batch
+// (with keys: the Galois keys are made from that generator a chunk of steps at a time and
+// released, instead of read from ev.galois_keys)
 Ciphertext ct_ct_matmul_colpacking(const Evaluator &ev, const Ciphertext &X, const Ciphertext &W, uint32_t rows,
-                                   uint32_t num_batch);
+                                   uint32_t num_batch, KeyGenerator *keys = nullptr);
 
 // attention's ct-ct product in the diagonal packing (ct_ct_matrix_mul_diagpacking,
 // Ct_ct_matrix_mul.cuh:182-): X holds the col_X = X.count diagonals, W the col_W = W.count
@@ -507,6 +510,12 @@ class BatchBootstrapper {
     // groups of `members` consecutive ciphertexts; needs ev.shared_keys for that size
     Ciphertext bootstrap_shared_a_s2c_first(const Ciphertext &ct, uint32_t members,
                                             const Evaluator *ev = nullptr) const;
+    // The original per-ciphertext C2S-first form (Bootstrapper::bootstrap_3 / bootstrap_full_3,
+    // Bootstrapper.cu:3606-3627, 3889-3903): input at one prime (or brought there; scale Delta),
+    // ModRaise to the top, CoeffToSlot, EvalMod, then SlotToCoeff at EvalMod's output level (its
+    // diagonals are encoded there on the first call; make that call before any graph capture).
+    // Ordinary ciphertexts, any batch size; the output has the input's slots at scale Delta.
+    Ciphertext bootstrap_c2s_first(const Ciphertext &ct, const Evaluator *ev = nullptr) const;
     // EvalMod of ciphertexts holding t / K: c_fin * sin(2 pi t) read at scale Delta
     Ciphertext evalmod(const Ciphertext &x, const Evaluator *ev = nullptr) const;
     // Autotuning for batches of `count` ciphertexts (members per shared-a group, 0 =
@@ -530,6 +539,9 @@ class BatchBootstrapper {
     Evaluator &ev_;
     BootstrapParams p_;
     std::vector<LinearTransform *> s2c_, c2s_;
+    mutable std::vector<LinearTransform *> s2c_late_;  // SlotToCoeff after EvalMod (C2S-first)
+    mutable uint32_t late_level_ = 0;
+    mutable std::mutex late_mu_;
     std::vector<double> cheb_;
     double q0_ = 0, c_fin_ = 0;
     uint32_t top_ = 0;

@@ -171,6 +171,11 @@ int shm_boot_galois_elts(const shm_boot *b, uint32_t *out, uint32_t cap, uint32_
  * members = n: shared-a groups of n consecutive ciphertexts (keys from
  * shm_host_gen_shared_keys) */
 int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out);
+/* The original per-ciphertext C2S-first bootstrap (Bootstrapper::bootstrap_3,
+ * Bootstrapper.cu:3606-3627, 3889-3903): ordinary ciphertexts at one prime (or brought there
+ * at scale Delta), ModRaise, CoeffToSlot, EvalMod, SlotToCoeff; the first call encodes the
+ * late SlotToCoeff diagonals. */
+int shm_boot_run_c2s_first(shm_boot *b, const shm_ct *in, shm_ct **out);
 /* One BERT encoder layer (src/include/test/test_single_layer.cuh:422-2062) on X: hidden
  * columns in the column packing at the bootstrap's output level and scale.
  * dims: hidden, heads, ffn, num_X, tokens, input_num, softmax_iter, ln_newt, ln_gold,

@@ -358,9 +358,10 @@ static double ctpt_loop_ms(const Env &E, size_t n_in, size_t n_out, size_t L, in
     cudaDeviceSynchronize();
     std::vector<std::unique_ptr<cuda_stream_wrapper>> streams;
     for (int t = 0; t < threads; t++) streams.push_back(std::make_unique<cuda_stream_wrapper>());
+    std::string failure;
     auto run = [&](size_t cols) {
 #pragma omp parallel num_threads(threads)
-        {
+        try {
             PhantomCKKSEncoder penc(E.context);
             moai::Encoder enc(&E.context, &penc);
             moai::Evaluator ev(&E.context, &penc);
@@ -384,7 +385,11 @@ static double ctpt_loop_ms(const Env &E, size_t n_in, size_t n_out, size_t L, in
                 ev.rescale_to_next_inplace(acc, st);
             }
             cudaStreamSynchronize(cs);
+        } catch (const std::exception &e) {  // an exception may not leave an OpenMP region
+#pragma omp critical
+            failure = e.what();
         }
+        if (!failure.empty()) throw std::runtime_error("ct-pt loop: " + failure);
     };
     run(threads);  // warm-up: one column per thread
     cudaDeviceSynchronize();
@@ -425,6 +430,7 @@ static int run_time(const Env &E, const std::string &which, int ctpt_cols) {
 }
 
 int main(int argc, char **argv) {
+    setvbuf(stdout, nullptr, _IONBF, 0);  // a failure late in a run keeps the records printed before it
     std::string which = argc > 1 ? argv[1] : "tiny";
     std::string mode = argc > 2 ? argv[2] : "golden";
     const int ctpt_cols = argc > 3 ? atoi(argv[3]) : 0;
@@ -500,7 +506,12 @@ int main(int argc, char **argv) {
 
     if (mode == "shared" || mode == "time") {
         Env E{context, encoder, enc, ev, sk, rk, gk, primes, N, nq, np, dnum, QP, log_n, s};
-        return mode == "shared" ? run_shared(E, which) : run_time(E, which, ctpt_cols);
+        try {
+            return mode == "shared" ? run_shared(E, which) : run_time(E, which, ctpt_cols);
+        } catch (const std::exception &e) {
+            fprintf(stderr, "ref_golden %s %s: %s\n", which.c_str(), mode.c_str(), e.what());
+            return 2;
+        }
     }
 
     std::vector<uint64_t> qrows;

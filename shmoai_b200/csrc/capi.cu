@@ -49,6 +49,7 @@ Context::~Context() {
         cudaDeviceSynchronize();
         cudaMemPoolDestroy(pool);
     }
+    (void)cudaGetLastError();  // the frees above report nothing a caller could act on
 }
 
 cudaMemPool_t Context::mempool() {
@@ -259,6 +260,10 @@ thread_local std::string g_err;
 
 template <typename F>
 int guard(F &&f) {
+    // the runtime's last-error slot may hold a non-sticky error left by a call outside this library
+    // (or ignored in a destructor); it is not this call's, so it is cleared before the call's own
+    // launch checks read the slot.  Sticky errors (a faulted context) survive this and still fail.
+    (void)cudaGetLastError();
     try {
         f();
         return SHM_OK;
@@ -1075,6 +1080,7 @@ void shm_graph_destroy(shm_graph *g) {
     if (g->graph) cudaGraphDestroy(g->graph);
     cudaDeviceGraphMemTrim(g->device);
     delete g;
+    (void)cudaGetLastError();
 }
 
 // ---- sampling and lifting

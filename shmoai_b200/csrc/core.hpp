@@ -100,6 +100,10 @@ void ntt_forward_rescale(const Context &c, const RescaleIO &io, uint64_t *t, uin
                          cudaStream_t st);
 // ModDown's conversion, forward NTT and combine in one launch pair (ModDownIO); delta:
 // [n_polys][L][N] scratch between the two phases
+// ModUp's base conversion, forward NTT and the digit copies in one launch pair (ModUpIO): up
+// [n_cts][beta][LP][N] with map = the prime of every converted row, 255 on the digits' own rows
+void ntt_forward_modup(const Context &c, const ModUpIO &mu, uint64_t *up, uint32_t n_cts, uint32_t beta,
+                       const LimbMap &map, cudaStream_t st);
 void ntt_forward_moddown(const Context &c, const ModDownIO &md, uint64_t *delta, uint32_t n_polys, uint32_t L,
                          cudaStream_t st);
 

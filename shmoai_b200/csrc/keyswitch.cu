@@ -21,41 +21,6 @@ constexpr int kThreads = 256;
 constexpr int kMaxAlpha = 16;
 constexpr int kMaxBeta = 16;
 
-// up[ct][b][j][k] for j outside digit b; digit rows copy d (NTT form).
-template <bool S52>
-__global__ void modup_conv_kernel(const uint64_t *__restrict__ x, const uint64_t *__restrict__ d, size_t d_stride,
-                                  uint64_t *__restrict__ up, const uint64_t *__restrict__ conv, uint32_t L,
-                                  uint32_t np, uint32_t nq, uint32_t log_n, const PrimeConst *__restrict__ pc) {
-    __shared__ uint64_t s_conv[64 * kMaxAlpha];
-    const uint32_t b = blockIdx.y, ct = blockIdx.z;
-    const uint32_t alpha = np, LP = L + np, beta = gridDim.y;
-    const uint32_t s = b * alpha, e = min(s + alpha, L), na = e - s;
-    for (uint32_t i = threadIdx.x; i < LP * alpha; i += blockDim.x) s_conv[i] = conv[(size_t)b * LP * alpha + i];
-    __syncthreads();
-    const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
-    const size_t n = (size_t)1 << log_n;
-    uint64_t y[kMaxAlpha];
-    const uint64_t *xc = x + (size_t)ct * L * n;
-#pragma unroll
-    for (int i = 0; i < kMaxAlpha; i++)
-        if (i < (int)na) y[i] = xc[(size_t)(s + i) * n + k];
-    uint64_t *o = up + ((size_t)ct * beta + b) * LP * n;
-    const uint64_t *dc = d + (size_t)ct * d_stride;
-    for (uint32_t j = 0; j < LP; j++) {
-        if (j >= s && j < e) {
-            o[(size_t)j * n + k] = dc[(size_t)j * n + k];
-            continue;
-        }
-        const PrimeConst &p = pc[j < L ? j : nq + (j - L)];
-        const uint64_t *cj = s_conv + j * alpha;
-        Acc<S52> acc;
-#pragma unroll
-        for (int i = 0; i < kMaxAlpha; i++)
-            if (i < (int)na) acc.add(y[i], cj[i]);
-        o[(size_t)j * n + k] = barrett(acc.get(), p);
-    }
-}
-
 // acc[ct][h][j][k] = sum_b up[ct][b][j][perm[k]] * key[b][h][prime(j)][k]   (perm = identity if null)
 // An NTT-domain automorphism maps every aligned block of 32 slots onto an aligned block
 // of 32 slots, so the permuted read of a warp stays within one 256-byte segment.
@@ -115,20 +80,7 @@ void launch_inner_product(dim3 grid, cudaStream_t st, const uint64_t *up, const 
 #undef SHM_IP_CASE
 }
 
-// the kernels above for one context: Acc<true> when every prime is below 2^52
-void launch_modup_conv(const Context &c, uint32_t n_cts, uint32_t L, const uint64_t *x, const uint64_t *d,
-                       size_t d_stride, uint64_t *up, cudaStream_t st) {
-    const uint32_t np = c.np, beta = (L + np - 1) / np;
-    const dim3 grid(c.n / kThreads, beta, n_cts);
-    const uint64_t *conv = c.ks[L].modup_conv;
-    SHM_LAUNCHED(1);
-    if (c.s52)
-        modup_conv_kernel<true><<<grid, kThreads, 0, st>>>(x, d, d_stride, up, conv, L, np, c.nq, c.log_n, c.pc);
-    else
-        modup_conv_kernel<false><<<grid, kThreads, 0, st>>>(x, d, d_stride, up, conv, L, np, c.nq, c.log_n, c.pc);
-    SHM_CUDA(cudaGetLastError());
-}
-
+// the inner product for one context: Acc<true> when every prime is below 2^52
 void launch_ip(const Context &c, uint32_t n_cts, uint32_t L, const uint64_t *up, const uint64_t *key, uint64_t *acc,
                const uint32_t *perm, cudaStream_t st) {
     const uint32_t np = c.np, beta = (L + np - 1) / np, LP = L + np;
@@ -287,7 +239,6 @@ void modup_into(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n
     const LevelKS &ks = c.ks[L];
     SHM_CUDA(cudaMemcpy2DAsync(x, ln * 8, d, d_stride * 8, ln * 8, n_cts, cudaMemcpyDeviceToDevice, st));
     ntt_inverse(c, x, n_cts * L, L, q_map(L), ks.modup_scale, st);
-    launch_modup_conv(c, n_cts, L, x, d, d_stride, up, st);
     LimbMap m;
     for (uint32_t s = 0; s < 512; s++) {
         if (s >= beta * LP) {
@@ -298,7 +249,18 @@ void modup_into(const Context &c, const uint64_t *d, size_t d_stride, uint32_t n
         bool own = j >= b * np && j < std::min((b + 1) * np, L);
         m.prime[s] = own ? 255 : (uint8_t)(j < L ? j : c.nq + (j - L));
     }
-    ntt_forward(c, up, n_cts * beta * LP, beta * LP, m, st);
+    // the conversion is computed in the forward NTT's load and the digits' own rows are copied by
+    // the same launch: the converted limbs never go through HBM in coefficient form
+    ModUpIO mu;
+    mu.x = x;
+    mu.d = d;
+    mu.d_stride = (long long)d_stride;
+    mu.conv = ks.modup_conv;
+    mu.L = L;
+    mu.np = np;
+    mu.LP = LP;
+    mu.s52 = c.s52 ? 1 : 0;
+    ntt_forward_modup(c, mu, up, n_cts, beta, m, st);
 }
 
 size_t hoisted_ws_words(const Context &c, uint32_t n_cts, uint32_t L) {

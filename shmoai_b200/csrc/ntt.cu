@@ -40,15 +40,52 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
     const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t pidx = map.prime[row % slots];
+    const uint32_t sig = threadIdx.x % S, lane = threadIdx.x / S;
+    if constexpr (IOK == kIoModUp) {
+        if (pidx == 255) {  // a limb of the digit itself: the NTT-form input, copied
+            const ModUpIO &mu = io.mu;
+            const uint32_t ct = row / slots, j = (row % slots) % mu.LP;
+            if (j >= mu.L) return;  // rows past the extended basis (none in a ModUp map)
+            const uint64_t *src = mu.d + ct * mu.d_stride + ((size_t)j << G::LOGN) + chunk * S;
+            uint64_t *dst = data + ((size_t)row << G::LOGN) + chunk * S;
+#pragma unroll
+            for (int m = 0; m < G::E; m++) {
+                const size_t pos = sig + (size_t)G::M * (lane + m * G::E);
+                dst[pos] = src[pos];
+            }
+            return;
+        }
+    }
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN), *ws = w + G::N;
     uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * S;
-    const uint32_t sig = threadIdx.x % S, lane = threadIdx.x / S;
 
     const bool grow = q < kGrowPrimeLimit;  // uniform per CTA (one limb)
     uint64_t a[G::E];
-    if constexpr (IOK == kIoRescale) {
+    if constexpr (IOK == kIoModUp) {
+        const ModUpIO &mu = io.mu;
+        __shared__ uint64_t sconv[16];
+        const uint32_t ct = row / slots, slot = row % slots, b = slot / mu.LP, j = slot % mu.LP;
+        const uint32_t s0 = b * mu.np, na = min(mu.np, mu.L - s0);
+        if (threadIdx.x < na) sconv[threadIdx.x] = mu.conv[((size_t)b * mu.LP + j) * mu.np + threadIdx.x];
+        __syncthreads();
+        const PrimeConst p = pc[pidx];
+        const uint64_t *y = mu.x + (((size_t)ct * mu.L + s0) << G::LOGN) + chunk * S;
+#pragma unroll
+        for (int m = 0; m < G::E; m++) {
+            const size_t pos = sig + (size_t)G::M * (lane + m * G::E);
+            if (mu.s52) {
+                Acc<true> acc;
+                for (uint32_t i = 0; i < na; i++) acc.add(y[((size_t)i << G::LOGN) + pos], sconv[i]);
+                a[m] = barrett(acc.get(), p);
+            } else {
+                Acc<false> acc;
+                for (uint32_t i = 0; i < na; i++) acc.add(y[((size_t)i << G::LOGN) + pos], sconv[i]);
+                a[m] = barrett(acc.get(), p);
+            }
+        }
+    } else if constexpr (IOK == kIoRescale) {
         const PrimeConst p = pc[pidx];
         const uint64_t *src = io.rs.last + ((size_t)(row / slots) << G::LOGN) + chunk * S;
 #pragma unroll
@@ -296,10 +333,11 @@ void launch_fwd_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slot
                   cudaStream_t st, const NttIO &io = NttIO{}) {
     using G = Geo<R, S>;
     dim3 grid(rows * G::CHUNKS);
+    constexpr int BLK = IOK == kIoModUp ? kIoPlain : IOK;  // ModUp's block phase is a plain one
     SHM_LAUNCHED(1);
     fwd_col<R, S, MINB, IOK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
     SHM_LAUNCHED(1);
-    fwd_blk<R, S, MINB, IOK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
+    fwd_blk<R, S, MINB, BLK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
 }
 
 template <int R, int S, int MINB>
@@ -373,6 +411,19 @@ void ntt_forward_moddown(const Context &c, const ModDownIO &md, uint64_t *delta,
     io.md = md;
     if (c.log_n == 16) launch_fwd<4, kIoModDown>(c, delta, n_polys * L, L, q_map(L), st, io);
     else if (c.log_n == 12) launch_fwd<3, kIoModDown>(c, delta, n_polys * L, L, q_map(L), st, io);
+    else throw std::invalid_argument("NTT supports N = 2^12 and 2^16");
+    SHM_CUDA(cudaGetLastError());
+}
+
+void ntt_forward_modup(const Context &c, const ModUpIO &mu, uint64_t *up, uint32_t n_cts, uint32_t beta,
+                       const LimbMap &map, cudaStream_t st) {
+    if (n_cts == 0) return;
+    if (mu.np > 16 || mu.np == 0 || mu.LP != mu.L + mu.np) throw std::invalid_argument("ModUp: shape out of range");
+    NttIO io;
+    io.mu = mu;
+    const uint32_t slots = beta * mu.LP;
+    if (c.log_n == 16) launch_fwd<4, kIoModUp>(c, up, n_cts * slots, slots, map, st, io);
+    else if (c.log_n == 12) launch_fwd<3, kIoModUp>(c, up, n_cts * slots, slots, map, st, io);
     else throw std::invalid_argument("NTT supports N = 2^12 and 2^16");
     SHM_CUDA(cudaGetLastError());
 }

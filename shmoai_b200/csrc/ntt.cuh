@@ -66,12 +66,28 @@ struct ModDownIO {
     int s52 = 0;  // every prime below 2^52: Acc<true>
 };
 
+// ModUp's forward NTT (ntt_forward_modup): row (ct, b, j) of up [n_cts][beta][LP][N].  For j
+// outside digit b (limbs [b alpha, min((b+1) alpha, L))) the column kernel reads the base
+// conversion sum_i y_i (qhat_i mod t_j) of the digit's INTT'd, qhat^-1-scaled limbs
+// y = x[ct][b alpha ..] (coefficient form) and the row is transformed; for j inside the digit it
+// copies d[ct][j] (already NTT form) and the block kernel leaves the row alone (map 255).  The
+// converted digits are never stored in coefficient form.
+struct ModUpIO {
+    const uint64_t *x = nullptr;     // [n_cts][L][N]
+    const uint64_t *d = nullptr;     // ciphertext ct's polynomial at d + ct * d_stride, [L][N]
+    const uint64_t *conv = nullptr;  // [beta][LP][np]: qhat_i mod t_j of the level's digits
+    long long d_stride = 0;
+    uint32_t L = 0, np = 0, LP = 0;
+    int s52 = 0;
+};
+
 // the optional load / store transforms of the forward NTT kernels
 struct NttIO {
     RescaleIO rs;
     ModDownIO md;
+    ModUpIO mu;
 };
-constexpr int kIoPlain = 0, kIoRescale = 1, kIoModDown = 2;
+constexpr int kIoPlain = 0, kIoRescale = 1, kIoModDown = 2, kIoModUp = 3;
 
 // scale constants of the inverse's last stage, per limb slot: c, c', c*psi^-(N/2), (c*psi^-(N/2))'
 struct InvScale {

@@ -84,6 +84,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "shm_boot_destroy": (None, [_P]),
         "shm_boot_galois_elts": (i32, [_P, ctypes.POINTER(_U32), _U32, ctypes.POINTER(_U32)]),
         "shm_boot_run": (i32, [_P, _P, _U32, pp]),
+        "shm_boot_run_c2s_first": (i32, [_P, _P, pp]),
         "shm_boot_bert_layer": (i32, [_P, _P, ctypes.POINTER(_U32), dp, dp, ctypes.POINTER(ctypes.c_int), pp, dp]),
         "shm_boot_capture": (i32, [_P, _P, _U32, pp, pp]),
         "shm_boot_tune": (i32, [_P, _U32, _U32, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
@@ -476,6 +477,12 @@ class Bootstrapper:
     def run(self, ct: Ct, members: int = 0) -> Ct:
         o = _P()
         self.host._check(self.host.lib.shm_boot_run(self._b, ct._c, members, ctypes.byref(o)))
+        return Ct(self.host, o)
+
+    def run_c2s_first(self, ct: Ct) -> Ct:
+        """The original per-ciphertext C2S-first bootstrap (bootstrap_3)."""
+        o = _P()
+        self.host._check(self.host.lib.shm_boot_run_c2s_first(self._b, ct._c, ctypes.byref(o)))
         return Ct(self.host, o)
 
     def bert_layer(self, X: Ct, weights: dict, cfg: dict, bias_vec) -> tuple[Ct, dict]:

@@ -426,6 +426,7 @@ BatchBootstrapper::BatchBootstrapper(Evaluator &ev, BootstrapParams p) : ev_(ev)
 BatchBootstrapper::~BatchBootstrapper() {
     for (auto *lt : s2c_) delete lt;
     for (auto *lt : c2s_) delete lt;
+    for (auto *lt : s2c_late_) delete lt;
 }
 
 void BatchBootstrapper::prepare() {
@@ -433,6 +434,11 @@ void BatchBootstrapper::prepare() {
     if (p_.input_level < 4 || p_.input_level > c.nq) throw Error("input level must be in [4, nq]");
     for (auto *lt : s2c_) delete lt;
     for (auto *lt : c2s_) delete lt;
+    {
+        std::lock_guard<std::mutex> g(late_mu_);
+        for (auto *lt : s2c_late_) delete lt;
+        s2c_late_.clear();
+    }
     s2c_.clear();
     c2s_.clear();
     const Twiddles tw(c.n / 2);
@@ -527,6 +533,41 @@ Ciphertext BatchBootstrapper::bootstrap_ordinary_s2c_first(const Ciphertext &ct,
     Ciphertext re, im;
     slots_to_re_im(ev, ev.adjust(ct, ct.L, ct.scale_), re, im);
     return finish(ev, re, im);
+}
+
+// C2S-first: the input's coefficients t = Delta c / q0 (c = the encoding of its slots) after ModRaise;
+// CoeffToSlot and EvalMod leave c / F in the slots (EvalMod's c_fin assumes SlotToCoeff's factor F),
+// and SlotToCoeff with F on its last layer puts Delta c back into the coefficients
+Ciphertext BatchBootstrapper::bootstrap_c2s_first(const Ciphertext &ct, const Evaluator *evp) const {
+    const Evaluator &ev = evp ? *evp : ev_;
+    if (c2s_.empty()) throw Error("call prepare() first");
+    if (ct.shared || ct.size != 2) throw Error("bootstrap takes ordinary size-2 ciphertexts");
+    const Ciphertext x1 = ev.adjust(ct, 1, p_.scale);
+    Ciphertext w = ev.mod_raise(x1, top_);
+    w.scale_ = q0_;
+    w = c2s_[0]->apply(ev, w);
+    w = c2s_[1]->apply(ev, w);
+    w = c2s_[2]->apply(ev, w, false);
+    const Ciphertext wc = ev.complex_conjugate(w);
+    Ciphertext y = finish(ev, ev.add(w, wc), ev.multiply_i(ev.sub(w, wc), -1));
+    {
+        std::lock_guard<std::mutex> g(late_mu_);
+        if (s2c_late_.empty() || y.L != late_level_) {
+            if (y.L < 4) throw Error("not enough levels left for SlotToCoeff after EvalMod");
+            for (auto *lt : s2c_late_) delete lt;
+            s2c_late_.clear();
+            const Twiddles tw(ev.context().n / 2);
+            std::vector<Diags> s = s2c_layers(tw);
+            for (auto &kv : s[2])
+                for (auto &z : kv.second) z *= p_.F;
+            for (uint32_t i = 0; i < 3; i++)
+                s2c_late_.push_back(new LinearTransform(ev_, s[i], y.L - i, p_.bsgs_g1[i]));
+            late_level_ = y.L;
+            ev_.context().synchronize();
+        }
+    }
+    for (auto *lt : s2c_late_) y = lt->apply(ev, y);
+    return y;
 }
 
 Ciphertext BatchBootstrapper::bootstrap_shared_a_s2c_first(const Ciphertext &ct, uint32_t members,

@@ -639,6 +639,13 @@ int shm_boot_run(shm_boot *b, const shm_ct *in, uint32_t members, shm_ct **out) 
     });
 }
 
+int shm_boot_run_c2s_first(shm_boot *b, const shm_ct *in, shm_ct **out) {
+    return guard([&] {
+        if (!b) throw Error("null bootstrapper");
+        put(out, b->b->bootstrap_c2s_first(C(in)));
+    });
+}
+
 int shm_boot_bert_layer(shm_boot *b, const shm_ct *X, const uint32_t *dims, const double *reals, const double *weights,
                         const int *bias_vec, shm_ct **out, double *stage_seconds) {
     return guard([&] {

@@ -26,22 +26,33 @@ Ciphertext sum_members(const Evaluator &ev, Ciphertext cur) {
 }  // namespace
 
 Ciphertext ct_ct_matmul_colpacking(const Evaluator &ev, const Ciphertext &X, const Ciphertext &W, uint32_t rows,
-                                   uint32_t num_batch) {
+                                   uint32_t num_batch, KeyGenerator *keys) {
     if (X.shared || W.shared || X.size != 2 || W.size != 2) throw Error("ct-ct matmul takes ordinary ciphertexts");
     if (X.count != W.count || X.count == 0) throw Error("ct-ct matmul: X and W need the same number of columns");
     if (rows == 0) throw Error("ct-ct matmul: no output rows");
     // the rotated copies of W are made a chunk of steps at a time (one hoisted ModUp per chunk), so
-    // at most ~8 GB of them are live: at full width a head's 127 rotations of 64 ciphertexts would
+    // at most ~12 GB of them are live: at full width a head's 127 rotations of 64 ciphertexts would
     // otherwise hold 170 GB
+    // With `keys`, the Galois keys of a chunk's steps are made for that chunk and released after
+    // it (at full width the 127 keys would hold ~36 GB for the whole product).
     const size_t w_bytes = W.polys() * W.L * ev.context().n * 8;
-    const uint32_t chunk = (uint32_t)std::max<size_t>(1, (size_t(8) << 30) / std::max<size_t>(w_bytes, 1));
+    const uint32_t chunk = (uint32_t)std::max<size_t>(1, (size_t(12) << 30) / std::max<size_t>(w_bytes, 1));
     std::vector<Ciphertext> outs;
     outs.reserve(rows);
     for (uint32_t lo = 0; lo < rows; lo += chunk) {
         const uint32_t hi = std::min(rows, lo + chunk);
         std::vector<int> steps;
         for (uint32_t i = std::max(lo, 1u); i < hi; i++) steps.push_back((int)(i * num_batch));
-        const std::map<int, Ciphertext> rot = ev.rotate_many(W, steps);
+        std::map<uint32_t, DeviceBuffer> chunk_keys;
+        Evaluator kev(ev.context(), ev.encoder());
+        kev.relin_key = ev.relin_key;
+        kev.galois_keys = &chunk_keys;
+        if (keys)
+            for (int st : steps) {
+                const uint32_t e = ev.galois_elt(st);
+                if (!chunk_keys.count(e)) chunk_keys.emplace(e, keys->galois_key(e));
+            }
+        const std::map<int, Ciphertext> rot = (keys ? kev : ev).rotate_many(W, steps);
         for (uint32_t i = lo; i < hi; i++) {
             const int step = (int)(i * num_batch);
             auto it = rot.find(step);

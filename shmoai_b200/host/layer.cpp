@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <set>
 
 #include "internal.hpp"
 
@@ -147,10 +148,22 @@ Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const 
     att_ev.shared_keys = ev.shared_keys;
     att_ev.galois_keys = ev.galois_keys;
     if (attention_keys) {
-        for (int st : bert_layer_rotation_steps(cfg, slots)) {
-            const uint32_t e = ev.galois_elt(st);
-            if (!att_keys.count(e)) att_keys.emplace(e, attention_keys->galois_key(e));
+        // the diagonal packing's baby and giant steps (about 3 sqrt(tokens) of them) stay for the
+        // block; the column packing makes its 127 keys a chunk at a time
+        uint32_t g = (uint32_t)std::sqrt((double)cfg.tokens);
+        if (g * g < cfg.tokens) g++;
+        const uint32_t bsteps = (cfg.tokens + g - 1) / g;
+        std::set<int> need;
+        for (uint32_t j = 1; j < g; j++) need.insert((int)((j * nb) % slots));
+        for (uint32_t i = 1; i < bsteps; i++) {
+            need.insert((int)(((cfg.tokens - i * g) * nb) % slots));
+            need.insert((int)((i * g * nb) % slots));
         }
+        for (int st : need)
+            if (st) {
+                const uint32_t e = ev.galois_elt(st);
+                if (!att_keys.count(e)) att_keys.emplace(e, attention_keys->galois_key(e));
+            }
         att_ev.galois_keys = &att_keys;
     }
     const Evaluator &aev = attention_keys ? att_ev : ev;
@@ -176,7 +189,8 @@ Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const 
             b[2 * dh + j] = w.bv[h * dh + j];
         }
         const Ciphertext qkv = add_column_bias(ev, ev.ctpt_matmul(X, Wqkv, 3 * dh, ws), b, bias_vec);
-        const Ciphertext S = ct_ct_matmul_colpacking(aev, ev.slice(qkv, 0, dh), ev.slice(qkv, dh, dh), cfg.tokens, nb);
+        const Ciphertext S = ct_ct_matmul_colpacking(aev, ev.slice(qkv, 0, dh), ev.slice(qkv, dh, dh), cfg.tokens, nb,
+                                                     attention_keys);
         // full rows (every token valid): each cyclic diagonal entry is a valid (query, key) pair, so
         // every slot takes the shift; the reference's band masks assume input_num <= tokens / 2
         numer[h] = cfg.input_num >= cfg.tokens ? exp_approx(ev, ev.add_const(S, kSoftmaxShift))

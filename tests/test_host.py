@@ -128,6 +128,22 @@ def test_bootstrap_shared_on_oracle(small):
         bs.run(h.encrypt(z[:2], DELTA, 5))
 
 
+def test_bootstrap_c2s_first_on_oracle(small):
+    """The original per-ciphertext C2S-first form (Bootstrapper::bootstrap_3): input at one prime,
+    ModRaise, CoeffToSlot, EvalMod, SlotToCoeff (three more levels than the S2C-first output)."""
+    h, bs = small
+    rng = np.random.default_rng(6)
+    z = _z(rng, 2, h.n // 2)
+    out = bs.run_c2s_first(h.encrypt(z, DELTA, 1))
+    err = np.abs(h.decrypt(out) - z)
+    assert out.level == 20 - 3 - 9 - 3 and abs(out.scale - DELTA) < 1e-6 * DELTA
+    assert err.mean() < 2e-5, err.mean()
+    assert err.max() < 1e-4, err.max()
+    # an input above one prime at scale Delta is brought down first
+    out2 = bs.run_c2s_first(h.encrypt(z, DELTA, 3))
+    assert np.abs(h.decrypt(out2) - z).mean() < 2e-5
+
+
 # ------------------------------------------------------------------ GPU
 
 
@@ -163,6 +179,26 @@ def test_host_cuda_matches_oracle_build_bit_for_bit():
     assert np.array_equal(sg.to_host(), sc.to_host()), "shared-a bootstrap"
     err = np.abs(g.decrypt(sg) - z)
     assert err.mean() < 2e-5
+    c1g, c1c = g.encrypt(z[:2], DELTA, 1), c.encrypt(z[:2], DELTA, 1)
+    fg, fc = bg.run_c2s_first(c1g), bc.run_c2s_first(c1c)
+    assert np.array_equal(fg.to_host(), fc.to_host()), "C2S-first bootstrap"
+    assert np.abs(g.decrypt(fg) - z[:2]).mean() < 2e-5
+
+
+@pytest.mark.gpu
+def test_bootstrap_c2s_first_reference_parameters_on_b200():
+    """The original per-ciphertext C2S-first form at N = 2^16 with the reference's parameters: input at
+    one prime, output three primes below the S2C-first output, mean error within 2e-5."""
+    primes = O.gen_primes(16, REF_BITS)
+    h = Host(16, primes, 5, hamming_weight=192, seed=8)
+    h.gen_relin_key()
+    bs = Bootstrapper(h, DELTA, 4)
+    h.gen_galois_keys(bs.galois_elts())
+    rng = np.random.default_rng(12)
+    z = _z(rng, 2, h.n // 2)
+    out = bs.run_c2s_first(h.encrypt(z, DELTA, 1))
+    err = np.abs(h.decrypt(out) - z)
+    assert out.level == 20 and err.mean() < 2e-5, (out.level, err.mean(), err.max())
 
 
 @pytest.mark.gpu
