@@ -479,7 +479,7 @@ def cpu_boot_sample(shared: int = 0):
 # serving workload: a Poisson stream of mixed jobs through the serving loop, against
 # the same jobs executed one after the other on the plain per-ciphertext path
 
-SERVE = dict(n_jobs=24, rate=3.0, seed=5, p_rot=0.65, p_mm=0.15, members=8, boot_batch=32, mm_n=192, mm_L=13,
+SERVE = dict(n_jobs=200, rate=3.0, seed=5, p_rot=0.65, p_mm=0.15, members=8, boot_batch=32, mm_n=192, mm_L=13,
              rot_steps=(1, 2, 4, 8), rot_max=32, rot_levels=(4, 24), slots=3, budget_gb=80)
 
 
@@ -522,15 +522,26 @@ def run_serve(args, rank, world, dist):
     rng = np.random.default_rng(77 + rank)
     w_scale = 2.0 ** 20
     W = np.rint(rng.normal(0, 0.02, (S["mm_n"], S["mm_n"])) * w_scale).astype(np.int64)
+    # one encrypted batch per (kind, level) with the largest count any job of that shape asks for;
+    # a job's input is a device copy of its first `count` ciphertexts (200 distinct inputs would not
+    # fit beside the keys)
+    masters = {}
+    for kind, count, L, _, _ in jobs:
+        key = (kind, L)
+        masters[key] = max(masters.get(key, 0), count)
+    for key, count in list(masters.items()):
+        kind, L = key
+        z = rng.uniform(-1, 1, (count, h.n // 2)) + 1j * rng.uniform(-1, 1, (count, h.n // 2))
+        masters[key] = (z, h.encrypt(z, BOOT["scale"] if kind != "rot" else 2.0 ** 40, L))
     inputs = []
     for kind, count, L, _, _ in jobs:
-        z = rng.uniform(-1, 1, (count, h.n // 2)) + 1j * rng.uniform(-1, 1, (count, h.n // 2))
-        inputs.append((z, h.encrypt(z, BOOT["scale"] if kind != "rot" else 2.0 ** 40, L)))
+        z, master = masters[(kind, L)]
+        inputs.append((z[:count], master))
     h.synchronize()
 
     def submit(srv, i):
         kind, count, L, arg, _ = jobs[i]
-        ct = h.slice(inputs[i][1])
+        ct = h.slice(inputs[i][1], 0, count)
         if kind == "rot":
             return srv.submit_rotate(ct, arg)
         if kind == "mm":
@@ -599,7 +610,7 @@ def run_serve(args, rank, world, dist):
     # ordinary bootstrapping, the CUDA-core matmul; latency from the measured service times
     service, plain = [], []
     for i, (kind, count, L, arg, _) in enumerate(jobs):
-        x = inputs[i][1]
+        x = h.slice(inputs[i][1], 0, count)
         torch.cuda.synchronize()
         t = time.perf_counter()
         if kind == "mm":
@@ -626,6 +637,12 @@ def run_serve(args, rank, world, dist):
     n_cts = sum(j[1] for j in jobs)
     kinds = {k: sum(1 for j in jobs if j[0] == k) for k in ("rot", "mm", "boot")}
     ms = lambda a, q: round(float(np.percentile(a, q)) * 1000.0, 2)  # noqa: E731
+    by_kind = {}
+    for k in ("rot", "mm", "boot"):
+        sel = [i for i, j in enumerate(jobs) if j[0] == k]
+        if sel:
+            by_kind[k] = {"p50_ms": ms(lat[sel], 50), "p99_ms": ms(lat[sel], 99),
+                          "plain_p50_ms": ms(plat[sel], 50), "plain_p99_ms": ms(plat[sel], 99)}
     return {
         "metric": "serving throughput, jobs/s with every job queued (rotation batches, ct-pt matmuls, shared-a "
                   "bootstraps); p50/p99 latency at Poisson arrivals",
@@ -637,7 +654,10 @@ def run_serve(args, rank, world, dist):
                    "budget_gb": S["budget_gb"], "rotation_batches": f"1-{S['rot_max']} cts at {S['rot_levels']} limbs",
                    "matmul": f"{S['mm_n']}x{S['mm_n']} at {S['mm_L']} limbs",
                    "bootstrap": f"{S['boot_batch']} cts, shared-a n={S['members']}"},
-        "serving": {"p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99), "poisson_jobs_per_s": round(len(jobs) / span, 3),
+        "serving": {"p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99), "by_kind": by_kind,
+                    "admission": "head of the queue when it fits the budget, else a later job that fits until the "
+                                 "head has waited 0.5 s, then the released budget is kept for the head",
+                    "poisson_jobs_per_s": round(len(jobs) / span, 3),
                     "capacity_jobs_per_s": round(len(jobs) / cap_span, 3),
                     "capacity_cts_per_s": round(n_cts / cap_span, 2), "capacity_batches": cap_stats["batches"],
                     "peak_admitted_gb": round(stats["peak_admitted"] / 2**30, 2),
@@ -889,6 +909,29 @@ def run_layer(args, rank, world, dist):
 CTPT = dict(n_in=768, n_out=768, L=13)  # config 2: one BERT-base projection at level 12
 
 
+def int8_peak_tops(torch):
+    """Dense INT8 tensor throughput of this GPU, measured: torch._int_mm (a cuBLASLt int8 GEMM with
+    int32 accumulation) on 8192 x 8192 x 8192, best of 10 after warm-up, CUDA events."""
+    try:
+        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        for _ in range(3):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(10):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch._int_mm(a, b)
+            e.record()
+            torch.cuda.synchronize()
+            best = min(best, s.elapsed_time(e))
+        del a, b
+        return round(2 * 8192 ** 3 / (best * 1e-3) / 1e12, 1), "measured: torch._int_mm int8 8192^3, best of 10"
+    except Exception as ex:  # reported, the datasheet figure stands in
+        return 4500.0, "datasheet dense INT8 (measurement failed: %s)" % repr(ex)[:120]
+
+
 def run_ctpt(args, rank, world, dist):
     """Config 2: 768 ciphertexts at 13 limbs (N = 2^16) times a 768 x 768 integer weight
     matrix (N(0, 0.02^2) at scale 2^40) on the INT8 tensor cores; step = the whole projection."""
@@ -921,7 +964,7 @@ def run_ctpt(args, rank, world, dist):
     ms = timed_steps(torch, step, args.steps, dist, None)  # X and Y (20 GB) exceed L2
     launches = lib.shm_kernel_launches() - l0
     macs = n_in * n_out * 2 * L * n
-    peak_i8 = 4500.0  # dense INT8 TOPS, datasheet (not measured on this pool)
+    peak_i8, peak_src = int8_peak_tops(torch)
     res = {
         "metric": "ct-pt matmul output ciphertexts/s (768 -> 768, 13 limbs, N=2^16, exact)",
         "value": round(world * n_out * 1000.0 / ms, 2), "unit": "output ciphertexts/s", "n_gpus": world,
@@ -935,7 +978,7 @@ def run_ctpt(args, rank, world, dist):
                      "achieved": round(macs * 13 * 2 / (ms * 1e-3) / 1e12, 1), "peak": peak_i8,
                      "unit": "TOPS (int8, 13 residue GEMMs)",
                      "frac": round(macs * 13 * 2 / (ms * 1e-3) / 1e12 / peak_i8, 4),
-                     "peak_source": "datasheet dense INT8 (no measured INT8 peak)", "traffic": None},
+                     "peak_source": peak_src, "traffic": None},
         "clocks": clk.summary(),
     }
     return res
@@ -1039,6 +1082,49 @@ def run_kernel_case(args, rank, world, dist):
         def step():
             ctx.ntt_forward_(x)
         unit, per = "limbs/s", 117 * L
+    elif args.workload == "zoo":
+        # the bootstrap's other hot kernels on a few GB: Sh-Rot of one group of 8 at 34 limbs
+        # (ip_multi_kernel, the ModUp- and ModDown-fused NTTs), a multiply-plain-accumulate of 8 terms over
+        # 16 ciphertexts at 33 limbs (the BSGS inner sums), a 4-term linear combination of 8 ciphertexts at
+        # 28 limbs (EvalMod's leaves) and the tensor product of 8 ciphertext pairs at 30 limbs
+        import ctypes
+
+        import shmoai_b200
+
+        lib = shmoai_b200.lib()
+
+        def res(shape, limbs):
+            return torch.remainder(torch.randint(0, 2 ** 62, shape, device="cuda", generator=g),
+                                   pr[:limbs].view(*([1] * (len(shape) - 2)), limbs, 1))
+
+        qp_rows = pr.view(1, 1, QP, 1)
+        sh = res((1, 9, 34, n), 34)
+        shkey = torch.remainder(torch.randint(0, 2 ** 62, (7, 9, QP, n), device="cuda", generator=g), qp_rows)
+        elt = ctx.galois_elt(5)
+        Xm = res((16, 2, 33, n), 33)
+        Pm = [res((33, n), 33) for _ in range(8)]
+        Xs = [Xm] * 8
+        mp_out = torch.empty_like(Xm)
+        Xl = [res((8, 2, 28, n), 28) for _ in range(4)]
+        w = np.ascontiguousarray(np.random.default_rng(4).integers(0, 2 ** 40, (4, 28)).astype(np.uint64))
+        w0 = np.ascontiguousarray(np.random.default_rng(5).integers(0, 2 ** 40, 28).astype(np.uint64))
+        lc_out = torch.empty_like(Xl[0])
+        A, B = res((8, 2, 30, n), 30), res((8, 2, 30, n), 30)
+        T = torch.empty(8, 3, 30, n, dtype=torch.int64, device="cuda")
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+
+        def step():
+            ctx.shared_rotate_hoisted(sh, [elt], [shkey])
+            xp = (ctypes.c_void_p * 8)(*[t.data_ptr() for t in Xs])
+            pp = (ctypes.c_void_p * 8)(*[t.data_ptr() for t in Pm])
+            assert lib.shm_multiply_plain_accumulate(ctx._h, xp, pp, 8, ctypes.c_void_p(mp_out.data_ptr()), 32, 33,
+                                                     0, None) == 0
+            lp = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in Xl])
+            lv = (ctypes.c_uint32 * 4)(28, 28, 28, 28)
+            assert lib.shm_linear_combination(ctx._h, lp, lv, w.ctypes.data_as(u64p), 4, w0.ctypes.data_as(u64p),
+                                              ctypes.c_void_p(lc_out.data_ptr()), 8, 28, None) == 0
+            ctx.multiply(A, B, out=T)
+        unit, per = "kernel-zoo passes/s", 1
     else:
         ct = torch.remainder(torch.randint(0, 2 ** 62, (4, 2, L, n), device="cuda", generator=g),
                              pr[:L].view(1, 1, L, 1))
@@ -1070,8 +1156,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks", "serve", "gelu",
-                                                            "layer"])
+    ap.add_argument("--workload", default="boot", choices=["boot", "prim", "ctpt", "ntt", "ks", "zoo", "serve",
+                                                            "gelu", "layer"])
     ap.add_argument("--batch", type=int, default=None)
     ap.add_argument("--shared", type=int, default=8,
                     help="boot: shared-a group size n (0 = ordinary ciphertexts)")
@@ -1165,7 +1251,7 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
     runner = {"boot": run_boot, "prim": run_prim, "ctpt": run_ctpt, "serve": run_serve, "ntt": run_kernel_case,
-              "ks": run_kernel_case, "gelu": run_gelu, "layer": run_layer}[args.workload]
+              "ks": run_kernel_case, "zoo": run_kernel_case, "gelu": run_gelu, "layer": run_layer}[args.workload]
     res = runner(args, rank, world, dist)
     if rank == 0:
         if not args.no_cpu_baseline and args.workload in ("boot", "prim", "gelu"):

@@ -62,6 +62,9 @@ def _declare(L):
         "shm_add_scalar": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint64), _P, _U32, _U32, _P]),
         "shm_multiply_plain_accumulate": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _U32, _P, _U32,
                                                          _U32, ctypes.c_int, _P]),
+        "shm_linear_combination": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_U32),
+                                                  ctypes.POINTER(ctypes.c_uint64), _U32, ctypes.POINTER(ctypes.c_uint64),
+                                                  _P, _U32, _U32, _P]),
         "shm_modraise_workspace_bytes": (_SZ, [_P, _U32]),
         "shm_modraise": (ctypes.c_int, [_P, _P, _P, _U32, _U32, _P, _SZ, _P]),
         "shm_drop_limbs": (ctypes.c_int, [_P, _P, _P, _U32, _U32, _U32, _P]),

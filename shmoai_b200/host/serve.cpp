@@ -172,6 +172,8 @@ uint64_t Server::submit_bootstrap(Ciphertext &&ct, uint32_t members) {
 
 namespace {
 
+constexpr double kReserveAfter = 0.5;  // seconds the head may be passed by smaller jobs
+
 bool mergeable(const Ciphertext &a, const Ciphertext &b) {
     return a.L == b.L && a.size == b.size && a.shared == b.shared && Evaluator::same_scale(a.scale_, b.scale_);
 }
@@ -184,14 +186,30 @@ void Server::worker(uint32_t slot) {
         std::vector<Job *> batch;
         {
             std::unique_lock<std::mutex> lk(S.mu);
-            S.work.wait(lk, [&] {
-                return (S.stop && S.queue.empty()) ||
-                       (!S.paused && !S.queue.empty() && S.admitted + S.queue.front()->bytes <= budget_);
-            });
-            if (S.queue.empty()) return;  // stopping and drained
-            // FIFO admission of the head; queued jobs of the same kind and shape join it
-            Job *head = S.queue.front();
-            S.queue.pop_front();
+            // Admission: the head of the queue when it fits the budget; while it does not, a later
+            // job that fits may start in its place (backfill), until the head has waited
+            // kReserveAfter seconds: from then on nothing else starts, so the budget the running
+            // jobs release is kept for the head (a large bootstrap is not starved by small jobs)
+            auto pick = [&]() -> std::deque<Job *>::iterator {
+                if (S.paused || S.queue.empty()) return S.queue.end();
+                Job *h0 = S.queue.front();
+                if (S.admitted + h0->bytes <= budget_) return S.queue.begin();
+                if (now() - h0->result.t_submit >= kReserveAfter) return S.queue.end();
+                for (auto it = S.queue.begin() + 1; it != S.queue.end(); ++it)
+                    if (S.admitted + (*it)->bytes <= budget_) return it;
+                return S.queue.end();
+            };
+            auto it = S.queue.end();
+            for (;;) {
+                if (S.stop && S.queue.empty()) return;  // stopping and drained
+                it = pick();
+                if (it != S.queue.end()) break;
+                // aging changes the answer without a notification: look again after a while
+                S.work.wait_for(lk, std::chrono::milliseconds(20));
+            }
+            // queued jobs of the same kind and shape join the picked one
+            Job *head = *it;
+            S.queue.erase(it);
             batch.push_back(head);
             S.admitted += head->bytes;
             if (head->kind != JobKind::Matmul)
