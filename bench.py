@@ -301,7 +301,7 @@ def ours_per_ct_leg(dev: int, ctpt_cols: int = 64):
 # bootstrapping workload
 
 
-def setup_boot(dev, rank, shared=0, tune_batch=0):
+def setup_boot(dev, rank, shared=0, tune_batch=0, g1=0):
     """C++ host (context, secret key, relinearisation key) and bootstrapper at the
     reference parameters; with shared = n the Sh-Galois, format and backward keys of
     shared-a groups of n replace the Galois keys.  tune_batch > 0 autotunes the kernel tiles
@@ -313,6 +313,8 @@ def setup_boot(dev, rank, shared=0, tune_batch=0):
     h.gen_relin_key()
     bs = Bootstrapper(h, BOOT["scale"], BOOT["input_level"])
     bs.tuning = bs.tune(tune_batch, shared) if tune_batch else []
+    if g1:  # a fixed BSGS split for every slot-transform layer (the tuned kernel tiles are kept)
+        bs.split = [g1] * 6
     if shared:
         h.gen_shared_keys(shared, bs.galois_elts(), hamming_weight=BOOT["h"])
     else:
@@ -333,7 +335,7 @@ def run_boot(args, rank, world, dist):
     B = args.batch
     if S and B % S:
         raise SystemExit("--batch must be a multiple of --shared")
-    h, bs = setup_boot(dev, rank, S, tune_batch=0 if args.no_tune else B)
+    h, bs = setup_boot(dev, rank, S, tune_batch=0 if args.no_tune else B, g1=args.g1)
     rng = np.random.default_rng(1000 + rank)
     n = h.n // 2
     z = rng.uniform(-1, 1, (B, n)) + 1j * rng.uniform(-1, 1, (B, n))
@@ -805,7 +807,7 @@ def cpu_gelu_sample():
 # primes where the bootstrap region starts, so every rescale after a bootstrap is by a 46-bit prime
 LAYER_BITS = [51] + [46] * 23 + [51] * 11 + [51] * 5
 LAYER = dict(hidden=768, heads=12, ffn=3072, num_X=256, tokens=128, input_num=128, softmax_iter=13, ln_newt=3,
-             ln_gold=2, gelu_input_level=13, ffn_chunk=256, boot_batch=16, w_scale=2.0 ** 40, ln_var_scale=64.0)
+             ln_gold=2, gelu_input_level=13, ffn_chunk=128, boot_batch=8, w_scale=2.0 ** 40, ln_var_scale=64.0)
 LAYER_METRIC = "BERT-base layer amortized seconds per input (256 inputs x 128 tokens, hidden 768, 12 heads, FFN 3072)"
 
 
@@ -895,6 +897,7 @@ def run_layer(args, rank, world, dist):
                    "error_vs_fp64_same_approximations": {"mean": float(e_a.mean()), "max": float(e_a.max())},
                    "error_vs_fp64_exact_layer": {"mean": float(e_x.mean()), "max": float(e_x.max())},
                    "device_gb_peak": round(peak / 2 ** 30, 2),
+                   "stage_device_gb_peak": {k: round(v, 1) for k, v in bs.last_stage_peak_gb.items()},
                    "reference_published_s_per_input": ref["sham" if S else "orig"],
                    "l2": "not flushed: every stage's live data exceeds the 126 MB L2"},
         "e2e": {"value": round(e2e_ms / 1000.0 / n_in, 5), "unit": "s/input",
@@ -1163,6 +1166,7 @@ def main():
                     help="boot: shared-a group size n (0 = ordinary ciphertexts)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="boot: skip the autotuner (default tiles and BSGS split)")
+    ap.add_argument("--g1", type=int, default=0, help="boot: baby steps of every slot-transform layer (0 = tuned)")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the step only (no e2e, roofline or CPU legs): used for ncu launch lists")
     ap.add_argument("--small", action="store_true",

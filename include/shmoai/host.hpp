@@ -574,6 +574,7 @@ struct BertLayerWeights {
 struct StageTime {
     std::string name;
     double seconds;
+    size_t peak_bytes = 0;  // the context pool's high-water mark of device memory in use during the stage
 };
 
 // the steps of the attention's rotations (multiples of N/2 / tokens); generate their Galois keys

@@ -186,9 +186,10 @@ int shm_boot_run_c2s_first(shm_boot *b, const shm_ct *in, shm_ct **out);
  *          Wi [d][ffn], bi [ffn], Wf [ffn][d], bf [d], ln2_gamma, ln2_beta, concatenated;
  * bias_vec: N/2 ints (1 = valid token slot).  The host needs the relinearisation key, the Galois
  * keys of the attention's rotation steps (multiples of N/2 / tokens) and, for members = 0, of the
- * bootstrap, else the shared-a keys of groups of `members`.  stage_seconds receives 11 wall
- * times: Attention Block, SelfOutput, 1st Bootstrapping, LayerNorm1, 2nd Bootstrapping,
- * Intermediate Linear, GELU, Final Linear, 3rd Bootstrapping, LayerNorm2, 4th Bootstrapping. */
+ * bootstrap, else the shared-a keys of groups of `members`.  stage_seconds receives 22 values:
+ * the wall times of Attention Block, SelfOutput, 1st Bootstrapping, LayerNorm1, 2nd
+ * Bootstrapping, Intermediate Linear, GELU, Final Linear, 3rd Bootstrapping, LayerNorm2, 4th
+ * Bootstrapping, then the device memory high-water mark (GiB, the context pool) of each stage. */
 int shm_boot_bert_layer(shm_boot *b, const shm_ct *X, const uint32_t *dims, const double *reals, const double *weights,
                         const int *bias_vec, shm_ct **out, double *stage_seconds);
 /* autotuning for batches of `count` (shmoai::BatchBootstrapper::tune): NTT tile, Sh-Rot

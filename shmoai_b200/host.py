@@ -498,13 +498,14 @@ class Bootstrapper:
         dims = (_U32 * len(keys))(*[int(cfg[k]) for k in keys])
         reals = np.array([cfg.get("w_scale", 2.0 ** 40), cfg.get("ln_var_scale", 64.0)], dtype=np.float64)
         bv = np.ascontiguousarray(bias_vec, dtype=np.int32)
-        secs = np.zeros(11, dtype=np.float64)
+        secs = np.zeros(22, dtype=np.float64)
         dp = ctypes.POINTER(ctypes.c_double)
         o = _P()
         self.host._check(self.host.lib.shm_boot_bert_layer(
             self._b, X._c, dims, reals.ctypes.data_as(dp), flat.ctypes.data_as(dp),
             bv.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(o), secs.ctypes.data_as(dp)))
-        return Ct(self.host, o), dict(zip(BERT_STAGES, secs.tolist()))
+        self.last_stage_peak_gb = dict(zip(BERT_STAGES, secs[11:].tolist()))
+        return Ct(self.host, o), dict(zip(BERT_STAGES, secs[:11].tolist()))
 
     def tune(self, count: int, members: int = 0) -> list[dict]:
         """Autotune for batches of `count` (shm_boot_tune); generate Galois keys afterwards."""

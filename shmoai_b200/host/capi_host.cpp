@@ -129,6 +129,7 @@ void shm_host_destroy(shm_host *h) {
     if (!h) return;
     // keys and buffers are returned to the context's pool before the context goes
     h->ev.reset();
+    h->pub.reset();
     h->kg.reset();
     h->shared.clear();
     h->galois.clear();
@@ -703,7 +704,10 @@ int shm_boot_bert_layer(shm_boot *b, const shm_ct *X, const uint32_t *dims, cons
         put(out, bert_layer(ev, *b->b, C(X), w, cfg, std::vector<int>(bias_vec, bias_vec + slots), &t,
                             have_all ? nullptr : b->h->kg.get()));
         if (stage_seconds)
-            for (size_t i = 0; i < t.size(); i++) stage_seconds[i] = t[i].seconds;
+            for (size_t i = 0; i < t.size(); i++) {
+                stage_seconds[i] = t[i].seconds;
+                stage_seconds[t.size() + i] = (double)t[i].peak_bytes / (double)(1ull << 30);
+            }
     });
 }
 

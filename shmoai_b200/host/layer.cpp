@@ -131,10 +131,16 @@ Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const 
     const uint32_t top = X.L;
     const double ws = cfg.w_scale;
     double t0 = now_s();
+    auto pool_peak = [&](bool reset) {
+        size_t high = 0;
+        c.check(shm_pool_usage(c.handle(), nullptr, nullptr, &high, reset ? 1 : 0));
+        return high;
+    };
+    pool_peak(true);
     auto stage = [&](const char *name) {
         c.synchronize();
         const double t1 = now_s();
-        if (times) times->push_back(StageTime{name, t1 - t0});
+        if (times) times->push_back(StageTime{name, t1 - t0, pool_peak(true)});
         t0 = t1;
     };
 
@@ -250,8 +256,9 @@ Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const 
         t_gelu += now_s() - tb;
     }
     if (times) {
-        times->push_back(StageTime{"Intermediate Linear", t_inter});
-        times->push_back(StageTime{"GELU", t_gelu});
+        const size_t high = pool_peak(true);
+        times->push_back(StageTime{"Intermediate Linear", t_inter, high});
+        times->push_back(StageTime{"GELU", t_gelu, high});
     }
     t0 = now_s();
 
