@@ -205,13 +205,13 @@ def _json_doc(text: str):
     return json.loads("\n".join(keep))
 
 
-def reference_gpu_leg(ctpt_cols: int = 64):
+def reference_gpu_leg(ctpt_cols: int = 16):
     """Times the reference's PhantomFHE + moai adapter built for sm_100a from the reference sources
     (oracle/_ref/ref_golden, mode `time`) on this GPU with CUDA events: at the config-1 chain (N = 2^16,
     [60] + 23 x [50] + 8 x [60], dnum 3) one ciphertext's inverse + forward NTT, HRotate by one slot and
     multiply + relinearize + rescale; the same calls at the bootstrapping chain's top level (35 primes,
-    dnum 7); and the per-ciphertext ct-pt loop of Ct_pt_matrix_mul.cuh:85-158 for 768 inputs at 13 limbs
-    and the first `ctpt_cols` output columns (OpenMP over columns, one stream per thread)."""
+    dnum 7); and the per-ciphertext ct-pt loop of ct_pt_matrix_mul_wo_pre_single (Ct_pt_matrix_mul.cuh:188-303,
+    one stream) for 768 inputs at 13 limbs and the first `ctpt_cols` output columns."""
     if not os.path.exists(REF_GOLDEN):
         return {"unavailable": "oracle/_ref/ref_golden was not built (no reference tree at build time)"}
     out = {"build": "reference PhantomFHE + moai adapter, nvcc -arch sm_100a -rdc (oracle/build_ref.sh)",
@@ -232,7 +232,7 @@ def reference_gpu_leg(ctpt_cols: int = 64):
     return out
 
 
-def ours_per_ct_leg(dev: int, ctpt_cols: int = 64):
+def ours_per_ct_leg(dev: int, ctpt_cols: int = 16):
     """This library's kernels on the calls the reference leg times, one ciphertext per call (eager, CUDA
     events, 3 warm-up + 20 calls): inverse + forward NTT, HRotate by one slot, multiply + relinearize +
     rescale at the config-1 chain and at the bootstrapping chain's top level; and the ct-pt matmul of 768
@@ -844,6 +844,8 @@ def run_layer(args, rank, world, dist):
     mask = np.ones(h.n // 2, dtype=np.int32)
     ct = h.batch_input(X, BOOT["scale"], 23)
     setup_s = time.perf_counter() - t_setup
+    resident, _ = h.device_memory()
+    print("layer: %.2f GB resident before the first call (keys, input)" % (resident / 2 ** 30), file=sys.stderr)
     holder = {}
 
     def step():
@@ -897,6 +899,7 @@ def run_layer(args, rank, world, dist):
                    "error_vs_fp64_same_approximations": {"mean": float(e_a.mean()), "max": float(e_a.max())},
                    "error_vs_fp64_exact_layer": {"mean": float(e_x.mean()), "max": float(e_x.max())},
                    "device_gb_peak": round(peak / 2 ** 30, 2),
+                   "device_gb_resident_keys_input": round(resident / 2 ** 30, 2),
                    "stage_device_gb_peak": {k: round(v, 1) for k, v in bs.last_stage_peak_gb.items()},
                    "reference_published_s_per_input": ref["sham" if S else "orig"],
                    "l2": "not flushed: every stage's live data exceeds the 126 MB L2"},

@@ -436,6 +436,8 @@ Ciphertext inv_sqrt_approx(const Evaluator &ev, const Ciphertext &x, int d_newt 
 // the sum of a batch's ciphertexts (one ciphertext), and one batch made of several
 Ciphertext batch_sum(const Evaluator &ev, const Ciphertext &x);
 Ciphertext batch_gather(const Evaluator &ev, const std::vector<Ciphertext> &parts);
+// the same, releasing each part once it is copied (parts is left empty)
+Ciphertext batch_gather(const Evaluator &ev, std::vector<Ciphertext> &&parts);
 Ciphertext batch_broadcast(const Evaluator &ev, const Ciphertext &one, uint32_t count);  // count copies
 // LayerNorm over the hidden columns of the column packing, one column per ciphertext of the
 // batch (layernorm, layernorm.cuh:899-): gamma_i (x_i - mean) / sqrt(var) + beta_i with the

@@ -335,10 +335,11 @@ static double time_ms(cudaStream_t s, int warm, int reps, const std::function<vo
     return ms / reps;
 }
 
-// the per-ciphertext ct-pt loop of Ct_pt_matrix_mul.cuh:85-158 (OpenMP over output columns, one
-// encoder, evaluator and stream per thread; per weight: scalar encode, deep copy of the input,
-// multiply_plain_inplace, add_inplace; then rescale), restated over the reference's calls for
-// n_in inputs at L limbs and the first n_out output columns
+// the per-ciphertext ct-pt loop of Ct_pt_matrix_mul.cuh:85-158 / its single-stream form
+// ct_pt_matrix_mul_wo_pre_single (:188-303) (per weight: scalar encode, deep copy of the input,
+// multiply_plain_inplace, add_inplace; then rescale; `threads` > 1 runs output columns in OpenMP
+// threads, one encoder, evaluator and stream each), restated over the reference's calls for n_in
+// inputs at L limbs and the first n_out output columns
 static double ctpt_loop_ms(const Env &E, size_t n_in, size_t n_out, size_t L, int threads) {
     std::vector<PhantomCiphertext> X;
     X.reserve(n_in);
@@ -418,7 +419,7 @@ static int run_time(const Env &E, const std::string &which, int ctpt_cols) {
            "\"rotate1_ms\": %.4f, \"mul_relin_rescale_ms\": %.4f, \"chain_ms\": %.4f",
            E.nq, warm, reps, ntt, rot, mrr, ntt + rot + mrr);
     if (ctpt_cols > 0) {
-        const int threads = std::max(1, std::min(omp_get_max_threads(), 32));
+        const int threads = 1;  // the single-stream form: several encoders built in parallel crashed here
         const size_t n_in = 768, L = 13;
         double ms = ctpt_loop_ms(E, n_in, (size_t)ctpt_cols, L, threads);
         printf(", \"ctpt_loop\": {\"n_in\": %zu, \"n_out\": %d, \"limbs\": %zu, \"threads\": %d, \"ms\": %.3f}",

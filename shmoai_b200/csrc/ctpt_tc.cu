@@ -451,7 +451,6 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     const uint64_t R = 2ull * L * c.n;
     if (R % kBN) throw std::invalid_argument("ct-pt matmul: 2 L N must be a multiple of 256");
     const uint64_t chunk = std::min<uint64_t>(R, kChunkCols);
-    if (R % chunk) throw std::invalid_argument("ct-pt matmul: column count not a multiple of the chunk");
     const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBM - 1) / kBM * kBM;
     Plan plan = make_plan(c, n_in, L, max_abs_w);
     const uint32_t T = plan.T;
@@ -473,16 +472,19 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     SHM_CUDA(cudaFuncSetAttribute(mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
     const int acc24 = (uint64_t)Kp * 125 * 125 < (1ull << 24) ? 1 : 0;  // accumulators exact in float
     for (uint64_t r0 = 0; r0 < R; r0 += chunk) {
+        // a shorter last pass (2 L N not a multiple of the chunk, e.g. at N = 2^12) lays its planes out
+        // with its own column count; every count here is a multiple of 256
+        const uint64_t cur = std::min<uint64_t>(chunk, R - r0);
         SHM_LAUNCHED(1);
-        xres_kernel<<<dim3((uint32_t)(chunk / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0, T);
+        xres_kernel<<<dim3((uint32_t)(cur / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0, T);
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
-        mma_kernel<<<dim3(Np / kBM, (uint32_t)(chunk / kBN), T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
-                                                                                       chunk, err, acc24);
+        mma_kernel<<<dim3(Np / kBM, (uint32_t)(cur / kBN), T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
+                                                                                     cur, err, acc24);
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
-        crt_kernel<<<dim3((uint32_t)((chunk / 4 + 255) / 256), n_out), 256, 0, st>>>(RES, Y, tab, n_out, chunk, r0, R,
-                                                                                    L, c.log_n, c.pc, T);
+        crt_kernel<<<dim3((uint32_t)((cur / 4 + 255) / 256), n_out), 256, 0, st>>>(RES, Y, tab, n_out, cur, r0, R, L,
+                                                                                  c.log_n, c.pc, T);
         SHM_CUDA(cudaGetLastError());
     }
 }

@@ -38,7 +38,10 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
     using G = Geo<R, S>;
     __shared__ uint64_t sm[G::M * S];
     const uint32_t chunk = blockIdx.x % G::CHUNKS;
-    const uint32_t row = limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
+    // ModUp rows go ct-major instead: the rows of one digit are consecutive CTAs, so the digit's
+    // coefficient-form limbs that every one of its rows reads stay in L2 while they run
+    const uint32_t row = IOK == kIoModUp ? blockIdx.x / G::CHUNKS
+                                         : limb_major_row(blockIdx.x / G::CHUNKS, slots, gridDim.x / G::CHUNKS);
     const uint32_t pidx = map.prime[row % slots];
     const uint32_t sig = threadIdx.x % S, lane = threadIdx.x / S;
     if constexpr (IOK == kIoModUp) {

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <set>
 
 #include "internal.hpp"
@@ -104,12 +105,54 @@ Ciphertext bootstrap_segment(const Evaluator &ev, const BatchBootstrapper &boot,
             parts.push_back(boot.bootstrap_ordinary_s2c_first(ev.slice(in, lo, n), &ev));
         }
     }
-    return parts.size() == 1 ? std::move(parts[0]) : batch_gather(ev, parts);
+    return batch_gather(ev, std::move(parts));
 }
+
+namespace {
+
+Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot, const Ciphertext &X,
+                             const BertLayerWeights &w, const BertLayerConfig &cfg, const std::vector<int> &bias_vec,
+                             std::vector<StageTime> *times, KeyGenerator *attention_keys, int &stage_no);
+
+const char *const kStageNames[] = {"Attention Block", "SelfOutput", "1st Bootstrapping", "LayerNorm1",
+                                   "2nd Bootstrapping", "Intermediate Linear / GELU", "Intermediate Linear / GELU",
+                                   "Final Linear", "3rd Bootstrapping", "LayerNorm2", "4th Bootstrapping"};
+
+}  // namespace
 
 Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const Ciphertext &X,
                       const BertLayerWeights &w, const BertLayerConfig &cfg, const std::vector<int> &bias_vec,
                       std::vector<StageTime> *times, KeyGenerator *attention_keys) {
+    int stage_no = 0;
+    std::vector<StageTime> local;
+    std::vector<StageTime> *tv = times ? times : &local;
+    const size_t done0 = tv->size();
+    try {
+        return bert_layer_stages(ev, boot, X, w, cfg, bias_vec, tv, attention_keys, stage_no);
+    } catch (const Error &e) {
+        // which stage failed (an allocation failure names only its call site), the device memory in
+        // use then and the high-water mark of every finished stage
+        std::string msg = std::string(e.what()) + " [bert_layer, stage " + kStageNames[std::min(stage_no, 10)];
+        size_t used = 0, reserved = 0;
+        if (shm_pool_usage(ev.context().handle(), &reserved, &used, nullptr, 0) == 0) {
+            char buf[96];
+            std::snprintf(buf, sizeof buf, "; pool %.2f GB used, %.2f GB reserved", used / 1e9, reserved / 1e9);
+            msg += buf;
+        }
+        for (size_t i = done0; i < tv->size(); i++) {
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "; %s peak %.2f GB", (*tv)[i].name.c_str(), (*tv)[i].peak_bytes / 1e9);
+            msg += buf;
+        }
+        throw Error(msg + "]", e.code);
+    }
+}
+
+namespace {
+
+Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot, const Ciphertext &X,
+                             const BertLayerWeights &w, const BertLayerConfig &cfg, const std::vector<int> &bias_vec,
+                             std::vector<StageTime> *times, KeyGenerator *attention_keys, int &stage_no) {
     const Context &c = ev.context();
     const uint32_t d = cfg.hidden, H = cfg.heads, dh = d / H, F = cfg.ffn, slots = c.n / 2;
     const uint32_t nb = slots / cfg.tokens;
@@ -142,6 +185,7 @@ Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const 
         const double t1 = now_s();
         if (times) times->push_back(StageTime{name, t1 - t0, pool_peak(true)});
         t0 = t1;
+        stage_no++;
     };
 
     // ---- Attention Block: per head QKV (one contraction of 3 * dh outputs), QK^T, softmax
@@ -215,7 +259,7 @@ Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const 
         heads[h] = ct_ct_matmul_diagpacking(aev, sm, ev.mod_switch_to(vals[h], sm.L), nb);
         vals[h] = Ciphertext();
     }
-    Ciphertext att = batch_gather(ev, heads);
+    Ciphertext att = batch_gather(ev, std::move(heads));
     heads.clear();
     att_keys.clear();
     stage("Attention Block");
@@ -239,7 +283,7 @@ Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const 
 
     // ---- Intermediate + GELU in column chunks (each chunk's GELU working set stays bounded)
     const uint32_t l_inter = std::min(H1.L, cfg.gelu_input_level + 1);
-    const Ciphertext h1i = ev.mod_switch_to(H1, l_inter);
+    Ciphertext h1i = ev.mod_switch_to(H1, l_inter);
     std::vector<Ciphertext> g;
     double t_inter = 0, t_gelu = 0;
     for (uint32_t lo = 0; lo < F; lo += cfg.ffn_chunk) {
@@ -255,16 +299,17 @@ Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const 
         t_inter += tb - ta;
         t_gelu += now_s() - tb;
     }
+    h1i = Ciphertext();
     if (times) {
         const size_t high = pool_peak(true);
         times->push_back(StageTime{"Intermediate Linear", t_inter, high});
         times->push_back(StageTime{"GELU", t_gelu, high});
     }
+    stage_no += 2;
     t0 = now_s();
 
     // ---- Final (masked by bias_vec: the padding slots GELU left non-zero are cleared)
-    Ciphertext G = batch_gather(ev, g);
-    g.clear();
+    Ciphertext G = batch_gather(ev, std::move(g));
     std::vector<double> mask(bias_vec.begin(), bias_vec.end());
     Ciphertext fin = add_column_bias(ev, ev.ctpt_matmul_masked(G, int_weights(w.Wf, F, d, 0, d, ws), d, ws, mask),
                                      w.bf, bias_vec);
@@ -284,5 +329,7 @@ Ciphertext bert_layer(const Evaluator &ev, const BatchBootstrapper &boot, const 
     (void)top;
     return out;
 }
+
+}  // namespace
 
 }  // namespace shmoai

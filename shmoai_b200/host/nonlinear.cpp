@@ -145,6 +145,49 @@ Ciphertext batch_gather(const Evaluator &ev, const std::vector<Ciphertext> &part
     return gather_ptrs(ev, p);
 }
 
+// each part is released (stream-ordered, after its copy) as soon as it is copied, so the gathered
+// batch and the parts together never take much more than one batch of device memory
+Ciphertext batch_gather(const Evaluator &ev, std::vector<Ciphertext> &&parts) {
+    if (parts.size() == 1) {
+        Ciphertext o = std::move(parts[0]);
+        parts.clear();
+        return o;
+    }
+    Ciphertext o;
+    {
+        std::vector<const Ciphertext *> p;
+        for (const Ciphertext &x : parts) p.push_back(&x);
+        // checks and the allocation of the whole batch, copies of nothing yet
+        const Ciphertext &p0 = *p.at(0);
+        const Context &c = ev.context();
+        size_t words = 0;
+        uint32_t count = 0;
+        for (const Ciphertext *q : p) {
+            if (q->L != p0.L || q->size != p0.size || q->shared != p0.shared ||
+                std::fabs(q->scale_ / p0.scale_ - 1.0) > 1e-12)
+                throw Error("gather: parts differ in level, size or scale");
+            words += q->polys() * q->L * c.n;
+            count += q->count;
+        }
+        o.data = DeviceBuffer(c, words);
+        o.count = count;
+        o.size = p0.size;
+        o.L = p0.L;
+        o.scale_ = p0.scale_;
+        o.shared = p0.shared;
+    }
+    const Context &c = ev.context();
+    size_t off = 0;
+    for (Ciphertext &x : parts) {
+        const size_t w = x.polys() * x.L * c.n;
+        c.check(shm_memcpy(c.handle(), o.data.data() + off, x.data.data(), w * 8, SHM_COPY_D2D, c.stream()));
+        off += w;
+        x = Ciphertext();
+    }
+    parts.clear();
+    return o;
+}
+
 // LayerNorm over hidden columns packed one per ciphertext (layernorm, layernorm.cuh:899-):
 // mean and variance are sums over the batch, the inverse square root is inv_sqrt_approx, and
 // column i gets gamma_i (x_i - mean) / sqrt(var) + beta_i; 2 (d_newt + d_gold) + 8 levels
