@@ -352,6 +352,10 @@ class Evaluator {
     Ciphertext ctpt_matmul_masked(const Ciphertext &X, const std::vector<int64_t> &W, uint32_t n_out,
                                   double w_scale, const std::vector<double> &mask, bool tensor_cores = true) const;
 
+    // frees the scratch buffer that key switches, rescales and matmuls share (it grows to the
+    // largest request and is kept); the next such call allocates it again
+    void release_workspace() const;
+
    private:
     std::vector<uint64_t> residues(double integral, uint32_t L) const;
     std::vector<Ciphertext> automorphisms(const Ciphertext &a, const std::vector<uint32_t> &elts) const;

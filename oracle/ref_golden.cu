@@ -335,12 +335,12 @@ static double time_ms(cudaStream_t s, int warm, int reps, const std::function<vo
     return ms / reps;
 }
 
-// the per-ciphertext ct-pt loop of Ct_pt_matrix_mul.cuh:85-158 / its single-stream form
-// ct_pt_matrix_mul_wo_pre_single (:188-303) (per weight: scalar encode, deep copy of the input,
-// multiply_plain_inplace, add_inplace; then rescale; `threads` > 1 runs output columns in OpenMP
-// threads, one encoder, evaluator and stream each), restated over the reference's calls for n_in
-// inputs at L limbs and the first n_out output columns
-static double ctpt_loop_ms(const Env &E, size_t n_in, size_t n_out, size_t L, int threads) {
+// the per-ciphertext ct-pt loop of ct_pt_matrix_mul_wo_pre_single (Ct_pt_matrix_mul.cuh:188-303),
+// call for call on the default stream: per output column, a scalar encode of each weight at the
+// input's level and scale, multiply_plain into a new ciphertext, add_inplace into the accumulator,
+// then rescale_to_next_inplace; one encoder and evaluator for the whole loop (the reference's
+// single-thread region).  n_in inputs at L limbs, the first n_out output columns.
+static double ctpt_loop_ms(const Env &E, size_t n_in, size_t n_out, size_t L) {
     std::vector<PhantomCiphertext> X;
     X.reserve(n_in);
     const size_t words = 2 * L * E.N;
@@ -357,42 +357,29 @@ static double ctpt_loop_ms(const Env &E, size_t n_in, size_t n_out, size_t L, in
         }
     }
     cudaDeviceSynchronize();
-    std::vector<std::unique_ptr<cuda_stream_wrapper>> streams;
-    for (int t = 0; t < threads; t++) streams.push_back(std::make_unique<cuda_stream_wrapper>());
-    std::string failure;
+    PhantomCKKSEncoder penc(E.context);
+    moai::Encoder enc(&E.context, &penc);
+    moai::Evaluator ev(&E.context, &penc);
+    std::vector<PhantomCiphertext> out;
     auto run = [&](size_t cols) {
-#pragma omp parallel num_threads(threads)
-        try {
-            PhantomCKKSEncoder penc(E.context);
-            moai::Encoder enc(&E.context, &penc);
-            moai::Evaluator ev(&E.context, &penc);
-            auto &st = *streams[omp_get_thread_num()];
-            const cudaStream_t cs = st.get_stream();
-#pragma omp for schedule(static)
-            for (int i = 0; i < (int)cols; i++) {
-                PhantomCiphertext acc;
-                for (size_t j = 0; j < n_in; j++) {
-                    PhantomPlaintext pt;
-                    enc.encode(weight(8, j * 768 + i), X[j].chain_index(), X[j].scale(), pt, st);
-                    PhantomCiphertext tmp;
-                    tmp.resize(E.context, X[j].chain_index(), 2, cs);
-                    tmp.set_scale(X[j].scale());
-                    tmp.set_ntt_form(true);
-                    cudaMemcpyAsync(tmp.data(), X[j].data(), words * 8, cudaMemcpyDeviceToDevice, cs);
-                    ev.multiply_plain_inplace(tmp, pt, st);
-                    if (j == 0) acc = std::move(tmp);
-                    else ev.add_inplace(acc, tmp, st);
-                }
-                ev.rescale_to_next_inplace(acc, st);
+        out.clear();
+        for (size_t i = 0; i < cols; i++) {
+            PhantomPlaintext p0;
+            enc.encode(weight(8, i), X[0].chain_index(), X[0].scale(), p0);
+            PhantomCiphertext acc;
+            ev.multiply_plain(X[0], p0, acc);
+            for (size_t j = 1; j < n_in; j++) {
+                PhantomPlaintext pj;
+                enc.encode(weight(8, j * 768 + i), X[j].chain_index(), X[j].scale(), pj);
+                PhantomCiphertext tmp;
+                ev.multiply_plain(X[j], pj, tmp);
+                ev.add_inplace(acc, tmp);
             }
-            cudaStreamSynchronize(cs);
-        } catch (const std::exception &e) {  // an exception may not leave an OpenMP region
-#pragma omp critical
-            failure = e.what();
+            ev.rescale_to_next_inplace(acc);
+            out.push_back(std::move(acc));
         }
-        if (!failure.empty()) throw std::runtime_error("ct-pt loop: " + failure);
     };
-    run(threads);  // warm-up: one column per thread
+    run(1);  // warm-up: one column
     cudaDeviceSynchronize();
     auto t0 = std::chrono::steady_clock::now();
     run(n_out);
@@ -419,11 +406,10 @@ static int run_time(const Env &E, const std::string &which, int ctpt_cols) {
            "\"rotate1_ms\": %.4f, \"mul_relin_rescale_ms\": %.4f, \"chain_ms\": %.4f",
            E.nq, warm, reps, ntt, rot, mrr, ntt + rot + mrr);
     if (ctpt_cols > 0) {
-        const int threads = 1;  // the single-stream form: several encoders built in parallel crashed here
         const size_t n_in = 768, L = 13;
-        double ms = ctpt_loop_ms(E, n_in, (size_t)ctpt_cols, L, threads);
-        printf(", \"ctpt_loop\": {\"n_in\": %zu, \"n_out\": %d, \"limbs\": %zu, \"threads\": %d, \"ms\": %.3f}",
-               n_in, ctpt_cols, L, threads, ms);
+        double ms = ctpt_loop_ms(E, n_in, (size_t)ctpt_cols, L);
+        printf(", \"ctpt_loop\": {\"n_in\": %zu, \"n_out\": %d, \"limbs\": %zu, \"threads\": 1, \"ms\": %.3f}",
+               n_in, ctpt_cols, L, ms);
     }
     printf("}\n}\n");
     cudaDeviceSynchronize();

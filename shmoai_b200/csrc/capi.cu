@@ -885,6 +885,13 @@ int shm_malloc(const shm_context *ctx, size_t bytes, void **out, void *stream) {
             SHM_CUDA(cudaDeviceSynchronize());
             e = cudaMallocFromPoolAsync(out, bytes, pool, S(stream));
         }
+        if (e == cudaErrorMemoryAllocation) {
+            // the free blocks may be scattered over the pool's chunks with none large enough:
+            // give every wholly free chunk back to the device and try once more
+            cudaGetLastError();
+            SHM_CUDA(cudaMemPoolTrimTo(pool, 0));
+            e = cudaMallocFromPoolAsync(out, bytes, pool, S(stream));
+        }
         SHM_CUDA(e);
     });
 }

@@ -20,6 +20,8 @@ uint64_t *Evaluator::ws(size_t bytes) const {
     return ws_.data();
 }
 
+void Evaluator::release_workspace() const { ws_ = DeviceBuffer(); }
+
 Ciphertext Evaluator::like(const Ciphertext &a, uint32_t L) const {
     Ciphertext o;
     o.data = DeviceBuffer(c_, a.polys() * L * c_.n);

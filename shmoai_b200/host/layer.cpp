@@ -181,6 +181,7 @@ Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot,
     };
     pool_peak(true);
     auto stage = [&](const char *name) {
+        ev.release_workspace();  // each stage's scratch peak is its own, not the largest so far
         c.synchronize();
         const double t1 = now_s();
         if (times) times->push_back(StageTime{name, t1 - t0, pool_peak(true)});
@@ -262,6 +263,7 @@ Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot,
     Ciphertext att = batch_gather(ev, std::move(heads));
     heads.clear();
     att_keys.clear();
+    att_ev.release_workspace();
     stage("Attention Block");
 
     // ---- SelfOutput
