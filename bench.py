@@ -342,8 +342,12 @@ def run_boot(args, rank, world, dist):
     ct = h.encrypt(z, BOOT["scale"], BOOT["input_level"])
     holder = {}
 
+    c2s = args.form == "c2s"
+    if c2s and S:
+        raise SystemExit("--form c2s is the ordinary per-ciphertext bootstrap: use --shared 0")
+
     def step():
-        holder["out"] = bs.run(ct, S)
+        holder["out"] = bs.run_c2s_first(ct) if c2s else bs.run(ct, S)
 
     resident, _ = h.device_memory(reset_peak=True)  # keys, diagonals, the input batch
     clk = ClockSampler(dev).start()
@@ -355,17 +359,45 @@ def run_boot(args, rank, world, dist):
     eager_ms = timed_steps(torch, step, args.steps, dist, None)
     eager_out = holder.pop("out").to_host()
 
-    # the timed path: the same bootstrap recorded once as a CUDA graph (BatchBootstrapper::capture)
-    # and replayed; its output must equal the eager one bit for bit
-    graph, out = bs.capture(ct, S)
-    for _ in range(args.warmup):
+    if c2s:
+        # the original C2S-first form, eager (one shm_boot_run_c2s_first per step), as the plain path runs
+        class _Eager:
+            kernels = 0
+
+            def __init__(self):
+                self.out = None
+
+            def launch(self):
+                if self.out is not None:
+                    self.out.close()
+                self.out = bs.run_c2s_first(ct)
+
+            def close(self):
+                pass
+
+        graph = _Eager()
         graph.launch()
-    torch.cuda.synchronize()
-    if not np.array_equal(out.to_host(), eager_out):
-        raise SystemExit("graph replay differs from the eager bootstrap")
-    l0 = lib.shm_kernel_launches()
-    ms = timed_steps(torch, graph.launch, args.steps, dist, None)  # a batch is ~1 GB of live data > L2
-    launches = lib.shm_kernel_launches() - l0
+        out = graph.out
+        torch.cuda.synchronize()
+        if not np.array_equal(out.to_host(), eager_out):
+            raise SystemExit("repeated C2S-first bootstrap differs from the first")
+        l0 = lib.shm_kernel_launches()
+        ms = timed_steps(torch, graph.launch, args.steps, dist, None)
+        launches = lib.shm_kernel_launches() - l0
+        out = graph.out
+        graph.kernels = launches // max(1, args.steps)
+    else:
+        # the timed path: the same bootstrap recorded once as a CUDA graph (BatchBootstrapper::capture)
+        # and replayed; its output must equal the eager one bit for bit
+        graph, out = bs.capture(ct, S)
+        for _ in range(args.warmup):
+            graph.launch()
+        torch.cuda.synchronize()
+        if not np.array_equal(out.to_host(), eager_out):
+            raise SystemExit("graph replay differs from the eager bootstrap")
+        l0 = lib.shm_kernel_launches()
+        ms = timed_steps(torch, graph.launch, args.steps, dist, None)  # a batch is ~1 GB of live data > L2
+        launches = lib.shm_kernel_launches() - l0
     err = np.abs(h.decrypt(out) - z)
     out_level = out.level
 
@@ -377,7 +409,7 @@ def run_boot(args, rank, world, dist):
     def e2e_step():
         ct.write_from_ptr(h_in.data_ptr())
         graph.launch()
-        out.to_ptr(h_out.data_ptr())
+        (graph.out if c2s else out).to_ptr(h_out.data_ptr())
 
     if args.no_extras:
         e2e_ms, roof = ms, None
@@ -408,11 +440,14 @@ def run_boot(args, rank, world, dist):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic (seeded uniform slot values in [-1,1]^2, symmetric encryption, random keys)",
         "config": {"workload": ("boot: shared-a S2C-first bootstrap of a batch of ciphertexts per GPU per step"
-                                if S else "boot: S2C-first bootstrap of a batch of ciphertexts per GPU per step"),
+                                if S else "boot: original C2S-first bootstrap (bootstrap_3 form), eager, of a batch of "
+                                "ciphertexts per GPU per step" if c2s else
+                                "boot: S2C-first bootstrap of a batch of ciphertexts per GPU per step"),
                    "batch_per_gpu": B, "shared_a_group": S or None, "N": h.n, "slots": n,
                    "input_primes": BOOT["input_level"], "output_primes": out_level, "Q": "[51]+20x[46]+14x[51]",
                    "P": "5x[51]", "dnum": h.nq // h.np,
-                   "path": "C++ host library over the C ABI: shm_boot_capture once, shm_host_graph_launch per step",
+                   "path": ("C++ host library over the C ABI: shm_boot_run_c2s_first per step (eager)" if c2s else
+                            "C++ host library over the C ABI: shm_boot_capture once, shm_host_graph_launch per step"),
                    "graph_kernels_per_step": int(graph_kernels),
                    "eager_ms_per_step": round(eager_ms, 3),
                    "autotune": {r["knob"]: r["candidates"][r["chosen"]] for r in bs.tuning} or None,
@@ -1046,7 +1081,7 @@ def run_gelu(args, rank, world, dist):
     def e2e_step():
         ct.write_from_ptr(h_in.data_ptr())
         graph.launch()
-        out.to_ptr(h_out.data_ptr())
+        (graph.out if c2s else out).to_ptr(h_out.data_ptr())
 
     e2e_ms = timed_steps(torch, e2e_step, args.steps, dist, None)
     clocks = clk.summary()
@@ -1170,6 +1205,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="boot: skip the autotuner (default tiles and BSGS split)")
     ap.add_argument("--g1", type=int, default=0, help="boot: baby steps of every slot-transform layer (0 = tuned)")
+    ap.add_argument("--form", default="s2c", choices=["s2c", "c2s"],
+                    help="boot: S2C-first (default) or the original per-ciphertext C2S-first form (with --shared 0)")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the step only (no e2e, roofline or CPU legs): used for ncu launch lists")
     ap.add_argument("--small", action="store_true",

@@ -451,6 +451,9 @@ Ciphertext batch_broadcast(const Evaluator &ev, const Ciphertext &one, uint32_t 
 // gamma, so no level is added (the reference's guess line suits variances of about 10..1000)
 Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &gamma,
                      const std::vector<double> &beta, int d_newt = 4, int d_gold = 2, double var_scale = 1.0);
+// the same, releasing x once its centred columns are formed (x is left empty)
+Ciphertext layernorm(const Evaluator &ev, Ciphertext &&x, const std::vector<double> &gamma,
+                     const std::vector<double> &beta, int d_newt = 4, int d_gold = 2, double var_scale = 1.0);
 // attention's ciphertext-ciphertext product in the column packing (ct_ct_matrix_mul_colpacking,
 // Ct_ct_matrix_mul.cuh:10-120): X and W batches of the same count; output batch of `rows`,
 // out_i = sum_j X_j * rot(W_j, i * num_batch) relinearised and rescaled (1 level); needs the

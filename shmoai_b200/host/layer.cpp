@@ -275,11 +275,12 @@ Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot,
     stage("1st Bootstrapping");
 
     // ---- LayerNorm1 on SelfOutput + X
-    Ciphertext ln1 = layernorm(ev, ev.add(b1, ev.mod_switch_to(X, b1.L)), w.ln1_gamma, w.ln1_beta, cfg.ln_newt,
-                               cfg.ln_gold, cfg.ln_var_scale);
+    Ciphertext res1 = ev.add(b1, ev.mod_switch_to(X, b1.L));
     b1 = Ciphertext();
+    Ciphertext ln1 = layernorm(ev, std::move(res1), w.ln1_gamma, w.ln1_beta, cfg.ln_newt, cfg.ln_gold,
+                               cfg.ln_var_scale);
     stage("LayerNorm1");
-    const Ciphertext H1 = bootstrap_segment(ev, boot, ln1, cfg.members, cfg.boot_batch);
+    Ciphertext H1 = bootstrap_segment(ev, boot, ln1, cfg.members, cfg.boot_batch);
     ln1 = Ciphertext();
     stage("2nd Bootstrapping");
 
@@ -322,9 +323,11 @@ Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot,
     stage("3rd Bootstrapping");
 
     // ---- LayerNorm2 on Final + H1
-    Ciphertext ln2 = layernorm(ev, ev.add(b3, ev.mod_switch_to(H1, b3.L)), w.ln2_gamma, w.ln2_beta, cfg.ln_newt,
-                               cfg.ln_gold, cfg.ln_var_scale);
+    Ciphertext res2 = ev.add(b3, ev.mod_switch_to(H1, b3.L));
     b3 = Ciphertext();
+    H1 = Ciphertext();
+    Ciphertext ln2 = layernorm(ev, std::move(res2), w.ln2_gamma, w.ln2_beta, cfg.ln_newt, cfg.ln_gold,
+                               cfg.ln_var_scale);
     stage("LayerNorm2");
     Ciphertext out = bootstrap_segment(ev, boot, ln2, cfg.members, cfg.boot_batch);
     stage("4th Bootstrapping");

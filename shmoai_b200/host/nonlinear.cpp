@@ -191,8 +191,11 @@ Ciphertext batch_gather(const Evaluator &ev, std::vector<Ciphertext> &&parts) {
 // LayerNorm over hidden columns packed one per ciphertext (layernorm, layernorm.cuh:899-):
 // mean and variance are sums over the batch, the inverse square root is inv_sqrt_approx, and
 // column i gets gamma_i (x_i - mean) / sqrt(var) + beta_i; 2 (d_newt + d_gold) + 8 levels
-Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &gamma,
-                     const std::vector<double> &beta, int d_newt, int d_gold, double var_scale) {
+namespace {
+
+// layernorm of x; with owned == &x's owner, x is released once the centred columns are formed
+Ciphertext layernorm_impl(const Evaluator &ev, const Ciphertext &x, Ciphertext *owned, const std::vector<double> &gamma,
+                          const std::vector<double> &beta, int d_newt, int d_gold, double var_scale) {
     need_ordinary(x, "layernorm");
     if (!(var_scale > 0)) throw Error("layernorm: var_scale must be positive");
     const uint32_t d = x.count;
@@ -201,31 +204,49 @@ Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector
     if (x.L < need) throw Error("layernorm needs " + std::to_string(need) + " primes");
     const Context &c = ev.context();
     const double S = x.scale_;
-    auto broadcast = [&](const Ciphertext &one, uint32_t k) {
-        return gather_ptrs(ev, std::vector<const Ciphertext *>(k, &one));
-    };
-    // columns are squared and normalised in chunks so that at most a chunk's temporaries sit beside the
-    // centred batch (at full width a whole-batch temporary is ~15 GB); the modular sums are the same
+    // columns are centred, squared and normalised in chunks, and the centred columns are kept as
+    // chunks, so that at most a chunk's temporaries (and no broadcast of a whole batch) sit beside
+    // them (at full width a whole-batch temporary is ~18 GB); the modular sums are the same
     const uint32_t chunk = std::min<uint32_t>(d, 128);
     const Ciphertext mean = ev.multiply_const(batch_sum(ev, x), 1.0 / d, S);
-    const Ciphertext xc = ev.sub(ev.mod_switch_to(x, mean.L), broadcast(mean, d));
-    Ciphertext sq_sum;
+    std::vector<Ciphertext> xc;
     for (uint32_t lo = 0; lo < d; lo += chunk) {
-        Ciphertext part = batch_sum(ev, square(ev, ev.slice(xc, lo, std::min(chunk, d - lo))));
-        sq_sum = sq_sum.count ? ev.add(sq_sum, part) : std::move(part);
+        const uint32_t k = std::min(chunk, d - lo);
+        xc.push_back(ev.sub(ev.mod_switch_to(ev.slice(x, lo, k), mean.L), batch_broadcast(ev, mean, k)));
+    }
+    if (owned) *owned = Ciphertext();
+    Ciphertext sq_sum;
+    for (const Ciphertext &part : xc) {
+        Ciphertext s = batch_sum(ev, square(ev, part));
+        sq_sum = sq_sum.count ? ev.add(sq_sum, s) : std::move(s);
     }
     const Ciphertext var = ev.multiply_const(sq_sum, var_scale / d, (double)c.primes[sq_sum.L - 2]);
     const Ciphertext inv = inv_sqrt_approx(ev, var, d_newt, d_gold);
     const double rs = std::sqrt(var_scale);
     std::vector<Ciphertext> cols;
     cols.reserve(d);
-    for (uint32_t lo = 0; lo < d; lo += chunk) {
-        const uint32_t k = std::min(chunk, d - lo);
-        const Ciphertext y = product(ev, ev.slice(xc, lo, k), broadcast(inv, k));
+    uint32_t lo = 0;
+    for (Ciphertext &part : xc) {
+        const uint32_t k = part.count;
+        const Ciphertext y = product(ev, part, batch_broadcast(ev, inv, k));
+        part = Ciphertext();
         for (uint32_t i = 0; i < k; i++)
             cols.push_back(ev.add_const(ev.multiply_const(ev.slice(y, i, 1), gamma[lo + i] * rs, S), beta[lo + i]));
+        lo += k;
     }
-    return batch_gather(ev, cols);
+    return batch_gather(ev, std::move(cols));
+}
+
+}  // namespace
+
+Ciphertext layernorm(const Evaluator &ev, const Ciphertext &x, const std::vector<double> &gamma,
+                     const std::vector<double> &beta, int d_newt, int d_gold, double var_scale) {
+    return layernorm_impl(ev, x, nullptr, gamma, beta, d_newt, d_gold, var_scale);
+}
+
+Ciphertext layernorm(const Evaluator &ev, Ciphertext &&x, const std::vector<double> &gamma,
+                     const std::vector<double> &beta, int d_newt, int d_gold, double var_scale) {
+    return layernorm_impl(ev, x, &x, gamma, beta, d_newt, d_gold, var_scale);
 }
 
 // softmax over the members of a batch (softmax.cuh:119-, without the attention layout's
