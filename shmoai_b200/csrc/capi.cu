@@ -35,7 +35,7 @@ void push4(std::vector<uint64_t> &v, uint64_t c, uint64_t psi_half_inv, uint64_t
 Context::~Context() {
     cudaSetDevice(device);
     release_encode_tables(*this);
-    for (void *p : {(void *)pc, (void *)tw, (void *)inv_scale_plain, (void *)moddown_scale, (void *)moddown_conv,
+    for (void *p : {(void *)pc, (void *)tw, (void *)twq, (void *)inv_scale_plain, (void *)moddown_scale, (void *)moddown_conv,
                     (void *)p_inv, (void *)p_mod, (void *)rescale_inv, arena})
         if (p) cudaFree(p);
     for (auto &l : ks)
@@ -135,6 +135,22 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
     }
     c->pc = upload(c->h_pc);
     c->tw = upload(tw);
+    {
+        // w / q rounded to the nearest double (w and q are exact doubles below 2^53) for the
+        // FP64-quotient butterflies of the primes below kF64GrowLimit; other primes never read it
+        std::vector<double> twq((size_t)QP * 2 * n, 0.0);
+        for (uint32_t i = 0; i < QP; i++) {
+            if (primes[i] >= kF64GrowLimit) continue;
+            const double qd = (double)primes[i];
+            const uint64_t *t = tw.data() + (size_t)i * 4 * n;
+            double *d = twq.data() + (size_t)i * 2 * n;
+            for (uint32_t k = 0; k < n; k++) {
+                d[k] = (double)t[k] / qd;
+                d[n + k] = (double)t[2 * n + k] / qd;
+            }
+        }
+        c->twq = upload(twq);
+    }
     c->inv_scale_plain = upload(sc_plain);
 
     // rescale: row L-1 holds q_{L-1}^-1 mod q_j

@@ -34,6 +34,7 @@ __device__ __forceinline__ uint32_t limb_major_row(uint32_t t, uint32_t slots, u
 template <int R, int S, int MINB, int IOK = kIoPlain>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
+                                                            const double *__restrict__ twq,
                                                             const PrimeConst *__restrict__ pc, NttIO io) {
     using G = Geo<R, S>;
     __shared__ uint64_t sm[G::M * S];
@@ -62,9 +63,10 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN), *ws = w + G::N;
+    const double *wq = twq + ((size_t)pidx * 2 << G::LOGN);
     uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * S;
 
-    const bool grow = q < kGrowPrimeLimit;  // uniform per CTA (one limb)
+    const int mode = bf_mode_of(q);  // uniform per CTA (one limb)
     uint64_t a[G::E];
     if constexpr (IOK == kIoModUp) {
         const ModUpIO &mu = io.mu;
@@ -123,19 +125,13 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 #pragma unroll
         for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane + m * G::E)];
     }
-    if (grow)
-        fwd_pass<R, true>(a, w, ws, 1, 0, 0, q);
-    else
-        fwd_pass<R>(a, w, ws, 1, 0, 0, q);
+    fwd_pass_any<R>(mode, a, w, ws, wq, 1, 0, 0, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) sm[(lane + m * G::E) * S + sig] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = sm[(lane * G::E + m) * S + sig];
-    if (grow)
-        fwd_pass<R, true>(a, w, ws, 1, R, lane, q);
-    else
-        fwd_pass<R>(a, w, ws, 1, R, lane, q);
+    fwd_pass_any<R>(mode, a, w, ws, wq, 1, R, lane, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane * G::E + m)] = a[m];
 }
@@ -146,6 +142,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 template <int R, int S, int MINB, int IOK = kIoPlain>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
+                                                            const double *__restrict__ twq,
                                                             const PrimeConst *__restrict__ pc, NttIO io) {
     using G = Geo<R, S>;
     __shared__ uint64_t sm[S * G::PAD_M];
@@ -155,32 +152,30 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN), *ws = w + G::N;
+    const double *wq = twq + ((size_t)pidx * 2 << G::LOGN);
     uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * S * G::M;
     const uint32_t sig = threadIdx.x / G::E, lane = threadIdx.x % G::E;
     const uint32_t b = chunk * S + sig;
     uint64_t *x = xc + (size_t)sig * G::M;
     uint64_t *s = sm + sig * G::PAD_M;
 
-    const bool grow = q < kGrowPrimeLimit;  // the same choice fwd_col made for this limb
+    const int mode = bf_mode_of(q);  // the same choice fwd_col made for this limb
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = x[lane + m * G::E];
-    if (grow)
-        fwd_pass<R, true>(a, w, ws, G::M + b, 0, 0, q);
-    else
-        fwd_pass<R>(a, w, ws, G::M + b, 0, 0, q);
+    fwd_pass_any<R>(mode, a, w, ws, wq, G::M + b, 0, 0, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) s[padded(lane + m * G::E)] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
-    if (grow) {
-        fwd_pass<R, true>(a, w, ws, G::M + b, R, lane, q);
+    if (mode != kBfHarvey) {
+        fwd_pass_any<R>(mode, a, w, ws, wq, G::M + b, R, lane, q);
         const PrimeConst p = pc[pidx];
 #pragma unroll
         for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = reduce_small(a[m], p);  // < 68q -> [0, q)
     } else {
-        fwd_pass<R>(a, w, ws, G::M + b, R, lane, q);
+        fwd_pass<R, kBfHarvey>(a, w, ws, wq, G::M + b, R, lane, q);
         const uint64_t q2 = 2 * q;
 #pragma unroll
         for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = csub(csub(a[m], q2), q);
@@ -240,6 +235,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
 template <int R, int S, int MINB>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
+                                                            const double *__restrict__ twq,
                                                             const PrimeConst *__restrict__ pc) {
     using G = Geo<R, S>;
     __shared__ uint64_t sm[S * G::PAD_M];
@@ -249,6 +245,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_blk(uint64_t *__
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN) + 2 * G::N, *ws = w + G::N;
+    const double *wq = twq + ((size_t)pidx * 2 << G::LOGN) + G::N;
     uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * S * G::M;
     const uint32_t sig = threadIdx.x / G::E, lane = threadIdx.x % G::E;
     const uint32_t b = chunk * S + sig;
@@ -263,20 +260,14 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_blk(uint64_t *__
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
-    const bool grow = q < kGrowPrimeLimit;  // uniform per CTA (one limb)
-    if (grow)
-        inv_pass<R, true>(a, w, ws, G::M + b, R, lane, q, 0);
-    else
-        inv_pass<R>(a, w, ws, G::M + b, R, lane, q, 0);
+    const int mode = bf_mode_of(q);  // uniform per CTA (one limb)
+    inv_pass_any<R>(mode, a, w, ws, wq, G::M + b, R, lane, q, 0);
 #pragma unroll
     for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane + m * G::E)];
-    if (grow)
-        inv_pass<R, true>(a, w, ws, G::M + b, 0, 0, q, 0);
-    else
-        inv_pass<R>(a, w, ws, G::M + b, 0, 0, q, 0);
+    inv_pass_any<R>(mode, a, w, ws, wq, G::M + b, 0, 0, q, 0);
     uint64_t *x = xc + (size_t)sig * G::M;
 #pragma unroll
     for (int m = 0; m < G::E; m++) x[lane + m * G::E] = a[m];
@@ -286,6 +277,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_blk(uint64_t *__
 template <int R, int S, int MINB>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
+                                                            const double *__restrict__ twq,
                                                             const PrimeConst *__restrict__ pc,
                                                             const uint64_t *__restrict__ scale, int scale_by_prime,
                                                             uint32_t scale_base) {
@@ -298,6 +290,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN) + 2 * G::N, *ws = w + G::N;
+    const double *wq = twq + ((size_t)pidx * 2 << G::LOGN) + G::N;
     const uint64_t *sc = scale + 4 * (scale_by_prime ? pidx : slot - scale_base);
     uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * S;
     const uint32_t sig = threadIdx.x % S, lane = threadIdx.x / S;
@@ -305,22 +298,16 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane * G::E + m)];
-    const bool grow = q < kGrowPrimeLimit;  // the same choice inv_blk made for this limb
-    if (grow)
-        inv_pass<R, true>(a, w, ws, 1, R, lane, q, 0);
-    else
-        inv_pass<R>(a, w, ws, 1, R, lane, q, 0);
+    const int mode = bf_mode_of(q);  // the same choice inv_blk made for this limb
+    inv_pass_any<R>(mode, a, w, ws, wq, 1, R, lane, q, 0);
 #pragma unroll
     for (int m = 0; m < G::E; m++) sm[(lane * G::E + m) * S + sig] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = sm[(lane + m * G::E) * S + sig];
-    if (grow)
-        inv_pass<R, true>(a, w, ws, 1, 0, 0, q, 1);
-    else
-        inv_pass<R>(a, w, ws, 1, 0, 0, q, 1);
-    // values in [0, 4q) (grow) or [0, 2q)
-    const uint64_t c0 = sc[0], c0s = sc[1], c1 = sc[2], c1s = sc[3], q2 = (grow ? 4 : 2) * q;
+    inv_pass_any<R>(mode, a, w, ws, wq, 1, 0, 0, q, 1);
+    // values in [0, 4q) (grow, FP64) or [0, 2q) (Harvey)
+    const uint64_t c0 = sc[0], c0s = sc[1], c1 = sc[2], c1s = sc[3], q2 = (mode != kBfHarvey ? 4 : 2) * q;
 #pragma unroll
     for (int m = 0; m < G::E / 2; m++) {
         uint64_t u = a[m], v = a[m + G::E / 2];
@@ -338,9 +325,9 @@ void launch_fwd_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slot
     dim3 grid(rows * G::CHUNKS);
     constexpr int BLK = IOK == kIoModUp ? kIoPlain : IOK;  // ModUp's block phase is a plain one
     SHM_LAUNCHED(1);
-    fwd_col<R, S, MINB, IOK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
+    fwd_col<R, S, MINB, IOK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc, io);
     SHM_LAUNCHED(1);
-    fwd_blk<R, S, MINB, BLK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc, io);
+    fwd_blk<R, S, MINB, BLK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc, io);
 }
 
 template <int R, int S, int MINB>
@@ -349,9 +336,9 @@ void launch_inv_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slot
     using G = Geo<R, S>;
     dim3 grid(rows * G::CHUNKS);
     SHM_LAUNCHED(1);
-    inv_blk<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc);
+    inv_blk<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc);
     SHM_LAUNCHED(1);
-    inv_col<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.pc,
+    inv_col<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc,
                                                      scale ? scale : c.inv_scale_plain, scale ? 0 : 1, scale_base);
 }
 

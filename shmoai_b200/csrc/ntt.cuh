@@ -115,6 +115,38 @@ __device__ __forceinline__ void ct_bf_grow(uint64_t &x, uint64_t &y, uint64_t w,
     y = a - t + 4 * q;
 }
 
+// Primes below kF64GrowLimit take the twiddle product's quotient from the FP64 pipe instead of the
+// integer multipliers (the quotient estimate of Shoup's NTL MulMod, with the product's remainder
+// formed by the 64-bit low products): with wq = w / q rounded to the nearest double and y < 2^52,
+// y is exact as a double (its bits under the exponent of 2^52, minus 2^52), and
+// Q = round(y wq) comes from the mantissa of fma(y, wq, 2^52).  |Q - y w / q| <= 1/2 + y 2^-54 < 3/4,
+// so Q is floor(y w / q) or one more and r = y w - Q q lies in [-q, q) (as a wrapped 64-bit value);
+// the butterflies add q to it.  The integer pipe keeps the two low products only.
+constexpr uint64_t kF64GrowLimit = (1ull << 52) / 36;
+
+__device__ __forceinline__ uint64_t mulmod_f64_centred(uint64_t y, uint64_t w, double wq, uint64_t q) {
+    const double two52 = 4503599627370496.0;
+    const double yd = __dsub_rn(__longlong_as_double((long long)(0x4330000000000000ull | y)), two52);
+    const uint64_t Q = (uint64_t)__double_as_longlong(__fma_rn(yd, wq, two52)) & 0x000FFFFFFFFFFFFFull;
+    return y * w - Q * q;
+}
+
+// Cooley-Tukey butterfly with the FP64 quotient, values growing by less than 2q per stage: from
+// inputs below 4q, 16 stages stay below 36q < 2^52 (q < kF64GrowLimit), the multiplicands too
+__device__ __forceinline__ void ct_bf_f64(uint64_t &x, uint64_t &y, uint64_t w, double wq, uint64_t q) {
+    const uint64_t a = x + q, t = mulmod_f64_centred(y, w, wq, q);
+    x = a + t;
+    y = a - t;
+}
+
+// Gentleman-Sande butterfly on [0, 4q) with the FP64 quotient: x - y + 4q < 8q < 2^52
+__device__ __forceinline__ void gs_bf_f64(uint64_t &x, uint64_t &y, uint64_t w, double wq, uint64_t q) {
+    const uint64_t q4 = 4 * q;
+    const uint64_t a = x + y, d = x - y + q4;
+    x = csub(a, q4);
+    y = mulmod_f64_centred(d, w, wq, q) + q;
+}
+
 __device__ __forceinline__ void gs_bf(uint64_t &x, uint64_t &y, uint64_t w, uint64_t ws, uint64_t q) {
     uint64_t q2 = 2 * q;
     uint64_t a = x + y;
@@ -134,12 +166,20 @@ __device__ __forceinline__ void gs_bf4(uint64_t &x, uint64_t &y, uint64_t w, uin
 
 // R forward stages on E = 2^R registers.  Stage r of the pass is global stage
 // s0 + r; the twiddle of the pair starting at m is tw[(tb << (s0 + r)) + (g << r) + (m >> (R - r))].
-// GROW: use ct_bf_grow (primes below kGrowPrimeLimit), else the Harvey butterfly that
-// keeps values in [0, 4q).
-template <int R, bool GROW = false>
+// MODE kBfHarvey: Harvey butterflies that keep values in [0, 4q) (any prime); kBfGrow: ct_bf_grow
+// (primes below kGrowPrimeLimit); kBfF64: ct_bf_f64 (primes below kF64GrowLimit), whose second
+// twiddle array is wq (w / q as doubles) instead of the Shoup companions.
+constexpr int kBfHarvey = 0, kBfGrow = 1, kBfF64 = 2;
+
+// the butterfly family of a limb's prime
+__device__ __forceinline__ int bf_mode_of(uint64_t q) {
+    return q < kF64GrowLimit ? kBfF64 : q < kGrowPrimeLimit ? kBfGrow : kBfHarvey;
+}
+
+template <int R, int MODE = kBfHarvey>
 __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
-                                         const uint64_t *__restrict__ ws, uint32_t tb, uint32_t s0, uint32_t g,
-                                         uint64_t q) {
+                                         const uint64_t *__restrict__ ws, const double *__restrict__ wq, uint32_t tb,
+                                         uint32_t s0, uint32_t g, uint64_t q) {
 #pragma unroll
     for (int r = 0; r < R; r++) {
         const int half = (1 << R) >> (r + 1);
@@ -148,7 +188,9 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
         for (int m = 0; m < (1 << R); m++) {
             if (m & half) continue;
             uint32_t idx = base + (m >> (R - r));
-            if (GROW)
+            if (MODE == kBfF64)
+                ct_bf_f64(a[m], a[m + half], __ldg(w + idx), __ldg(wq + idx), q);
+            else if (MODE == kBfGrow)
                 ct_bf_grow(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
             else
                 ct_bf(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
@@ -156,11 +198,25 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
     }
 }
 
-// GROW: gs_bf4 on [0, 4q) (primes below kGrowPrimeLimit), else gs_bf on [0, 2q)
-template <int R, bool GROW = false>
+// fwd_pass in the butterfly family `mode` (uniform per CTA: one limb)
+template <int R>
+__device__ __forceinline__ void fwd_pass_any(int mode, uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
+                                             const uint64_t *__restrict__ ws, const double *__restrict__ wq,
+                                             uint32_t tb, uint32_t s0, uint32_t g, uint64_t q) {
+    if (mode == kBfF64)
+        fwd_pass<R, kBfF64>(a, w, ws, wq, tb, s0, g, q);
+    else if (mode == kBfGrow)
+        fwd_pass<R, kBfGrow>(a, w, ws, wq, tb, s0, g, q);
+    else
+        fwd_pass<R, kBfHarvey>(a, w, ws, wq, tb, s0, g, q);
+}
+
+// MODE kBfGrow: gs_bf4 on [0, 4q) (primes below kGrowPrimeLimit); kBfF64: gs_bf_f64 on [0, 4q);
+// kBfHarvey: gs_bf on [0, 2q)
+template <int R, int MODE = kBfHarvey>
 __device__ __forceinline__ void inv_pass(uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
-                                         const uint64_t *__restrict__ ws, uint32_t tb, uint32_t s0, uint32_t g,
-                                         uint64_t q, int skip_stage0) {
+                                         const uint64_t *__restrict__ ws, const double *__restrict__ wq, uint32_t tb,
+                                         uint32_t s0, uint32_t g, uint64_t q, int skip_stage0) {
 #pragma unroll
     for (int r = R - 1; r >= 0; r--) {
         if (r == 0 && skip_stage0) break;
@@ -170,12 +226,26 @@ __device__ __forceinline__ void inv_pass(uint64_t (&a)[1 << R], const uint64_t *
         for (int m = 0; m < (1 << R); m++) {
             if (m & half) continue;
             uint32_t idx = base + (m >> (R - r));
-            if (GROW)
+            if (MODE == kBfF64)
+                gs_bf_f64(a[m], a[m + half], __ldg(w + idx), __ldg(wq + idx), q);
+            else if (MODE == kBfGrow)
                 gs_bf4(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
             else
                 gs_bf(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
         }
     }
+}
+
+template <int R>
+__device__ __forceinline__ void inv_pass_any(int mode, uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
+                                             const uint64_t *__restrict__ ws, const double *__restrict__ wq,
+                                             uint32_t tb, uint32_t s0, uint32_t g, uint64_t q, int skip_stage0) {
+    if (mode == kBfF64)
+        inv_pass<R, kBfF64>(a, w, ws, wq, tb, s0, g, q, skip_stage0);
+    else if (mode == kBfGrow)
+        inv_pass<R, kBfGrow>(a, w, ws, wq, tb, s0, g, q, skip_stage0);
+    else
+        inv_pass<R, kBfHarvey>(a, w, ws, wq, tb, s0, g, q, skip_stage0);
 }
 
 }  // namespace shm
