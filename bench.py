@@ -862,7 +862,7 @@ def run_layer(args, rank, world, dist):
     torch.cuda.set_device(dev)
     lib = shmoai_b200.lib()
     S = args.shared
-    cfg = dict(LAYER, members=S, boot_batch=LAYER["boot_batch"] if S else 1)
+    cfg = dict(LAYER, members=S, boot_batch=(args.batch or LAYER["boot_batch"]) if S else 1)
     t_setup = time.perf_counter()
     h = Host(16, bits=LAYER_BITS, n_special=5, hamming_weight=BOOT["h"], seed=0x5EED + rank, device=dev)
     h.gen_relin_key()
@@ -1216,7 +1216,7 @@ def main():
     if args.small:
         CTPT.update(L=1)
     if args.batch is None:
-        args.batch = {"boot": 32, "gelu": 64}.get(args.workload, 1)
+        args.batch = {"boot": 32, "gelu": 64, "layer": 0}.get(args.workload, 1)  # layer: 0 = LAYER's boot_batch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -199,7 +199,7 @@ class KeyGenerator {
     uint64_t next_seed();
     std::vector<int64_t> ternary(uint32_t hamming_weight);
     DeviceBuffer ntt_qp(const std::vector<int64_t> &coeffs) const;  // [QP][N]
-    DeviceBuffer automorph(const std::vector<int64_t> &coeffs, uint32_t elt) const;
+    DeviceBuffer automorph_ntt(const DeviceBuffer &s_ntt, uint32_t elt) const;  // s(X^elt), [QP][N] NTT form
     // B_{d,row} += unit * s (unit: residues over QP)
     struct KeyTerm {
         uint32_t row;
@@ -351,6 +351,15 @@ class Evaluator {
     // (two levels, output scale X.scale * w_scale / q exactly as ctpt_matmul's).  mask: N/2 slots.
     Ciphertext ctpt_matmul_masked(const Ciphertext &X, const std::vector<int64_t> &W, uint32_t n_out,
                                   double w_scale, const std::vector<double> &mask, bool tensor_cores = true) const;
+
+    // out[c] = sum_t A[t][c] x B[t][c] as size-3 ciphertexts, the products summed before one
+    // reduction (shm_multiply_accumulate); every B[t] of one member is broadcast over the batch.
+    // Equal to multiply_lazy of every pair followed by add.  Terms at different levels are
+    // brought to the lowest.
+    Ciphertext multiply_accumulate(const std::vector<const Ciphertext *> &A,
+                                   const std::vector<const Ciphertext *> &B) const;
+    // sum over the members j of X_j x W_j: one size-3 ciphertext
+    Ciphertext sum_of_products(const Ciphertext &X, const Ciphertext &W) const;
 
     // frees the scratch buffer that key switches, rescales and matmuls share (it grows to the
     // largest request and is kept); the next such call allocates it again
@@ -595,6 +604,10 @@ Ciphertext add_column_bias(const Evaluator &ev, const Ciphertext &Y, const std::
 // ciphertexts (shared-a groups of `members`, a short last group padded; 0 = ordinary)
 Ciphertext bootstrap_segment(const Evaluator &ev, const BatchBootstrapper &boot, const Ciphertext &x,
                              uint32_t members, uint32_t batch);
+// the same, releasing x once it is at the input level (x is left empty): the segment's own
+// working set then sits beside the small input batch instead of the whole-level one
+Ciphertext bootstrap_segment(const Evaluator &ev, const BatchBootstrapper &boot, Ciphertext &&x, uint32_t members,
+                             uint32_t batch);
 // One layer on X (hidden columns at the bootstrap's output level and scale); the output has X's
 // level and scale.  ev needs the relinearisation key, the Galois keys of the bootstrap (ordinary)
 // or the shared-a keys of `members`, and the Galois keys of bert_layer_rotation_steps: either in

@@ -89,6 +89,14 @@ int shm_multiply_plain(const shm_context *ctx, const uint64_t *ct, const uint64_
 int shm_multiply(const shm_context *ctx, const uint64_t *a, const uint64_t *b, uint64_t *out, uint32_t n_cts,
                  uint32_t L, void *stream);
 
+/* Sum of k size-3 tensor products: out[c] = sum_t A[t][c] x B[t][b_broadcast ? 0 : c] for n_cts
+ * output ciphertexts [n_cts][3][L][N] (A[t]: [n_cts][2][L][N]; B[t]: one ciphertext when b_broadcast,
+ * else [n_cts][2][L][N]); accumulate: add into out.  Equal to shm_multiply of every pair followed by
+ * additions mod q.  Replaces the multiply + add_inplace loops of the attention's ct-ct products
+ * (src/include/source/matrix_mul/Ct_ct_matrix_mul.cuh:10-120, :182-).  */
+int shm_multiply_accumulate(const shm_context *ctx, const uint64_t *const *A, const uint64_t *const *B, uint32_t k,
+                            int b_broadcast, uint64_t *out, uint32_t n_cts, uint32_t L, int accumulate, void *stream);
+
 /* Rescale (floor division by the last prime) of n_polys polynomials, L -> L-1 limbs.
  * Replaces rescale_to_next / divide_and_round_q_last_ntt (evaluate.cu:1392-1443,
  * src/rns.cu:1157-1181). */
@@ -141,6 +149,13 @@ int shm_relinearize_rescale(const shm_context *ctx, const uint64_t *ct3, const u
 int shm_apply_galois(const shm_context *ctx, const uint64_t *ct, uint32_t galois_elt, const uint64_t *galois_key,
                      uint64_t *out, uint32_t n_cts, uint32_t L, void *workspace, size_t workspace_bytes,
                      void *stream);
+/* The automorphism X -> X^galois_elt of n_rows NTT-form polynomials of N words each, without key
+ * switching (a permutation of the evaluation points; any prime per row): used on secrets to form
+ * Galois keys on the device (generate_one_kswitch_key's s(X^elt), secretkey.cu:328-373, computed
+ * there from the coefficients).  out must not overlap in. */
+int shm_permute_galois(const shm_context *ctx, const uint64_t *in, uint32_t galois_elt, uint64_t *out,
+                       uint32_t n_rows, void *stream);
+
 /* Hoisted automorphisms of the same n_cts ciphertexts: ModUp of c1 once, then for
  * each of n_elts Galois elements the permuted inner product with keys[e] and
  * ModDown: outs[e] = (sigma(c0) + cx0, cx1).  keys / outs are host arrays of

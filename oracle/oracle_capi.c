@@ -467,6 +467,41 @@ int shm_multiply(const shm_context *ctx, const uint64_t *a, const uint64_t *b, u
     return SHM_OK;
 }
 
+int shm_permute_galois(const shm_context *ctx, const uint64_t *in, uint32_t galois_elt, uint64_t *out,
+                       uint32_t n_rows, void *stream) {
+    (void)stream;
+    if (!ctx) return fail("null context");
+    if (!(galois_elt & 1) || galois_elt >= 2 * ctx->c->n) return fail("Galois element must be odd and < 2N");
+    if ((!in || !out) && n_rows) return fail("null pointer");
+    if (in == out && n_rows) return fail("permute_galois cannot work in place");
+    orc_apply_galois(ctx->c, in, out, n_rows, 1, galois_elt);
+    return SHM_OK;
+}
+
+int shm_multiply_accumulate(const shm_context *ctx, const uint64_t *const *A, const uint64_t *const *B, uint32_t k,
+                            int b_broadcast, uint64_t *out, uint32_t n_cts, uint32_t L, int accumulate, void *stream) {
+    (void)stream;
+    if (!lvl_ok(ctx, L)) return fail("level out of range");
+    if (((!A || !B) && k) || (!out && n_cts)) return fail("null argument");
+    size_t n = ctx->c->n, ln = (size_t)L * n;
+    uint64_t *t3 = (uint64_t *)malloc(3 * ln * sizeof(uint64_t));
+    if (!t3) return fail("out of host memory");
+    for (uint32_t c = 0; c < n_cts; c++) {
+        uint64_t *o = out + (size_t)c * 3 * ln;
+        if (!accumulate) memset(o, 0, 3 * ln * sizeof(uint64_t));
+        for (uint32_t t = 0; t < k; t++) {
+            orc_tensor(ctx->c, A[t] + (size_t)c * 2 * ln, B[t] + (b_broadcast ? 0 : (size_t)c * 2 * ln), t3, L);
+            for (uint32_t h = 0; h < 3; h++)
+                for (uint32_t l = 0; l < L; l++) {
+                    uint64_t q = ctx->c->primes[l], *oo = o + (h * L + l) * n, *tt = t3 + (h * L + l) * n;
+                    for (size_t j = 0; j < n; j++) oo[j] = addmod(oo[j], tt[j], q);
+                }
+        }
+    }
+    free(t3);
+    return SHM_OK;
+}
+
 int shm_multiply_scalar(const shm_context *ctx, const uint64_t *a, const uint64_t *scalars, uint64_t *out,
                         uint32_t n_polys, uint32_t L, void *stream) {
     (void)stream;

@@ -55,6 +55,9 @@ __global__ void mul_plain_acc_kernel(PtrTab X, PtrTab P, uint32_t k, uint64_t *_
     const size_t off = ((size_t)row << log_n) + blockIdx.x * kT + threadIdx.x;
     const size_t poff = ((size_t)limb << log_n) + blockIdx.x * kT + threadIdx.x;
     u128 acc = {0, 0};
+    // unrolled so that a group of terms' loads is in flight together (the loads, not the
+    // multiplies, bound this kernel)
+#pragma unroll 8
     for (uint32_t t = 0; t < k; t++) mac(acc, X.p[t][off], P.p[t][poff]);
     uint64_t r = barrett(acc, p);
     if (accumulate) r = add_mod(r, out[off], p.q);

@@ -1,5 +1,7 @@
 // Context construction and the extern "C" entry points of include/shmoai_ckks.h.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -66,6 +68,11 @@ cudaMemPool_t Context::mempool() {
     return pool;
 }
 
+__global__ void perm_table_kernel(uint32_t *p, uint32_t elt, uint32_t log_n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    p[k] = galois_index(k, elt, log_n);
+}
+
 const uint32_t *Context::perm(uint32_t elt) {
     std::lock_guard<std::mutex> g(mu);
     auto it = galois_perm.find(elt);
@@ -74,12 +81,12 @@ const uint32_t *Context::perm(uint32_t elt) {
     // NTT-domain automorphism (src/galois.cu:8-21, include/galois.cuh:44-60):
     // slot k holds a(psi^(2*brv(k)+1)); X -> X^elt moves slot perm[k] to k with
     // 2*brv(perm[k]) + 1 = (2*brv(k) + 1) * elt mod 2N.
-    std::vector<uint32_t> p(n);
-    for (uint32_t k = 0; k < n; k++) {
-        uint64_t e = ((uint64_t)(2 * host::bitrev(k, log_n) + 1) * elt) & (2ull * n - 1);
-        p[k] = host::bitrev((uint32_t)((e - 1) >> 1), log_n);
-    }
-    uint32_t *d = upload(p);
+    // built on the device (the table of galois_index), then waited for once: every stream may use it
+    uint32_t *d = nullptr;
+    SHM_CUDA(cudaMalloc(&d, (size_t)n * sizeof(uint32_t)));
+    perm_table_kernel<<<n / 256, 256>>>(d, elt, log_n);
+    SHM_CUDA(cudaGetLastError());
+    SHM_CUDA(cudaStreamSynchronize(0));
     galois_perm[elt] = d;
     return d;
 }
@@ -114,6 +121,11 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
             throw std::invalid_argument("alpha * q must stay below 2^63 for the lazy base conversion");
     }
     c->s52 = *std::max_element(primes.begin(), primes.end()) < kS52PrimeLimit;
+    {
+        int fam = 0;
+        for (uint64_t q : primes) fam |= 1 << bf_mode_of(q);
+        c->ntt_families = (fam & ~kFamSmall) == 0 ? kFamSmall : (fam & ~kFamLarge) == 0 ? kFamLarge : kFamAll;
+    }
     // per-prime constants and twiddles
     std::vector<uint64_t> tw((size_t)QP * 4 * n), psi_half_inv(QP), sc_plain;
     for (uint32_t i = 0; i < QP; i++) {
@@ -435,6 +447,50 @@ int shm_multiply(const shm_context *ctx, const uint64_t *a, const uint64_t *b, u
         check_level(c, L);
         set_device(c);
         shm::tensor(c, a, b, out, n_cts, L, S(stream));
+    });
+}
+
+int shm_permute_galois(const shm_context *ctx, const uint64_t *in, uint32_t galois_elt, uint64_t *out,
+                       uint32_t n_rows, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        if (!(galois_elt & 1) || galois_elt >= 2 * c.n) throw std::invalid_argument("Galois element must be odd and < 2N");
+        if ((!in || !out) && n_rows) throw std::invalid_argument("null pointer");
+        if (in == out && n_rows) throw std::invalid_argument("permute_galois cannot work in place");
+        set_device(c);
+        shm::apply_galois(c, in, out, n_rows, galois_elt, S(stream));
+    });
+}
+
+int shm_multiply_accumulate(const shm_context *ctx, const uint64_t *const *A, const uint64_t *const *B, uint32_t k,
+                            int b_broadcast, uint64_t *out, uint32_t n_cts, uint32_t L, int accumulate, void *stream) {
+    return guard([&] {
+        auto &c = ctx_of(ctx);
+        check_level(c, L);
+        if ((!A || !B) && k) throw std::invalid_argument("null term arrays");
+        if (!out && n_cts) throw std::invalid_argument("null output");
+        set_device(c);
+        // 2 * chunk products (the middle term) must stay below the Barrett bound 2^(63 + bits(q))
+        uint32_t chunk = shm::kMaxAccTerms;
+        for (uint32_t i = 0; i < L; i++) {
+            const int b = shm::host::bit_length(c.primes[i]);
+            const int room = 63 + b - 2 * b;  // log2 of the products one sum may hold
+            const uint32_t lim = room >= 6 ? 64u : (1u << room);
+            chunk = std::min(chunk, std::max(1u, lim / 2));
+        }
+        for (uint32_t t0 = 0; t0 < k; t0 += chunk) {
+            const uint32_t kk = std::min(chunk, k - t0);
+            shm::PtrTab a{}, b{};
+            for (uint32_t t = 0; t < kk; t++) {
+                if (!A[t0 + t] || !B[t0 + t]) throw std::invalid_argument("null term");
+                a.p[t] = A[t0 + t];
+                b.p[t] = B[t0 + t];
+            }
+            shm::tensor_accumulate(c, a, b, kk, 1, b_broadcast ? 0 : 1, out, n_cts, L, accumulate || t0 > 0,
+                                   S(stream));
+        }
+        if (k == 0 && !accumulate && n_cts)
+            SHM_CUDA(cudaMemsetAsync(out, 0, (size_t)n_cts * 3 * L * c.n * 8, S(stream)));
     });
 }
 
@@ -898,6 +954,8 @@ int shm_malloc(const shm_context *ctx, size_t bytes, void **out, void *stream) {
             // blocks freed on other streams become reusable once their work is done: wait for
             // the device once and retry before reporting out of memory
             cudaGetLastError();
+            if (std::getenv("SHMOAI_POOL_TRACE"))
+                std::fprintf(stderr, "shm_malloc: %.2f GB found no room: waiting for the device\n", bytes / 1e9);
             SHM_CUDA(cudaDeviceSynchronize());
             e = cudaMallocFromPoolAsync(out, bytes, pool, S(stream));
         }
@@ -905,6 +963,13 @@ int shm_malloc(const shm_context *ctx, size_t bytes, void **out, void *stream) {
             // the free blocks may be scattered over the pool's chunks with none large enough:
             // give every wholly free chunk back to the device and try once more
             cudaGetLastError();
+            if (std::getenv("SHMOAI_POOL_TRACE")) {
+                uint64_t reserved = 0, used = 0;
+                cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+                cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+                std::fprintf(stderr, "shm_malloc: %.2f GB found no room (pool %.2f GB used, %.2f GB reserved): trimming\n",
+                             bytes / 1e9, used / 1e9, reserved / 1e9);
+            }
             SHM_CUDA(cudaMemPoolTrimTo(pool, 0));
             e = cudaMallocFromPoolAsync(out, bytes, pool, S(stream));
         }

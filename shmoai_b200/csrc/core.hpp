@@ -46,12 +46,33 @@ struct LevelKS {
     double *rr_inv_s = nullptr;    // [np + 1]: 1 / s_k rounded to double
 };
 
+// the slot that an NTT-domain automorphism X -> X^elt moves to slot k (N = 2^log_n):
+// 2 brv(perm) + 1 = (2 brv(k) + 1) elt mod 2N, brv the log_n-bit reversal
+__host__ __device__ __forceinline__ uint32_t galois_index(uint32_t k, uint32_t elt, uint32_t log_n) {
+#ifdef __CUDA_ARCH__
+    const uint32_t bk = __brev(k) >> (32 - log_n);
+#else
+    uint32_t bk = 0;
+    for (uint32_t i = 0; i < log_n; i++) bk |= ((k >> i) & 1u) << (log_n - 1 - i);
+#endif
+    const uint32_t e = (uint32_t)(((uint64_t)(2 * bk + 1) * elt) & ((2ull << log_n) - 1));
+    const uint32_t h = (e - 1) >> 1;
+#ifdef __CUDA_ARCH__
+    return __brev(h) >> (32 - log_n);
+#else
+    uint32_t r = 0;
+    for (uint32_t i = 0; i < log_n; i++) r |= ((h >> i) & 1u) << (log_n - 1 - i);
+    return r;
+#endif
+}
+
 struct Context {
     int device = 0;
     uint32_t log_n = 0, n = 0, nq = 0, np = 0, dnum = 0;
     std::vector<uint64_t> primes;       // nq + np
     bool s52 = false;                   // every prime below kS52PrimeLimit (Acc<true> kernels)
     int ntt_variant = 0;                // index into kNttVariants (set by the autotuner)
+    int ntt_families = 0;               // the NTT instantiation for the primes' butterfly families (kFam*)
     uint32_t ip_chunk_bytes = 32768;    // shared memory per Sh-Rot inner-product block (autotuned)
     std::vector<PrimeConst> h_pc;       // host copy
     PrimeConst *pc = nullptr;           // [QP]
@@ -153,6 +174,10 @@ constexpr int kMaxAccTerms = 32;
 struct PtrTab {
     const uint64_t *p[kMaxAccTerms];
 };
+// out[ct] (+)= sum_{t < k} A_t[ct a_step] x B_t[ct b_step] (size-3 tensor products; k <= kMaxAccTerms,
+// bounded by the caller so that 2k products stay below every limb's Barrett bound)
+void tensor_accumulate(const Context &c, const PtrTab &A, const PtrTab &B, uint32_t k, uint32_t a_step,
+                       uint32_t b_step, uint64_t *out, uint32_t n_cts, uint32_t L, bool accumulate, cudaStream_t st);
 void mul_scalar(const Context &c, const uint64_t *a, uint64_t *out, const ScalarTab &s, uint32_t n_polys, uint32_t L,
                 cudaStream_t st);
 void add_scalar(const Context &c, const uint64_t *a, uint64_t *out, const ScalarTab &s, uint32_t n_cts, uint32_t L,

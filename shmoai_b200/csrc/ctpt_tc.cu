@@ -45,7 +45,7 @@ constexpr long long kSpinLimit = 1ll << 24;
 // write it write the same bytes; each kernel takes its T as an argument.
 struct ModTab {
     uint32_t m[kMaxMods];
-    uint32_t fracx[kMaxMods + 1][kMaxMods];  // [T][t]: [(M/m_t)^-1]_{m_t} / m_t, 32-bit fixed point
+    double fracd[kMaxMods + 1][kMaxMods];  // [T][t]: [(M/m_t)^-1]_{m_t} / m_t rounded to a double
     uint32_t c24[kMaxMods];  // 2^20 mod m_t
     uint32_t c48[kMaxMods];  // 2^40 mod m_t
     uint32_t magic[kMaxMods];  // ceil(2^32 / m_t)
@@ -88,7 +88,9 @@ __device__ __forceinline__ uint32_t mod_acc(int a, uint32_t t) {
     return mod_small(x, t);
 }
 
-// X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via a 64 x 64 shared-memory transpose
+// X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via a 64 x 64 shared-memory transpose.  Each
+// thread writes four consecutive inputs' residues of one column as one 32-bit word, so a warp's
+// store covers 64 contiguous bytes of each of two columns for every modulus.
 __global__ void __launch_bounds__(256, 4) xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__ XP, uint32_t n_in, uint32_t Kp,
                             uint64_t R, uint64_t r0, uint32_t T) {
     __shared__ uint64_t tile[64][65];
@@ -101,10 +103,19 @@ __global__ void __launch_bounds__(256, 4) xres_kernel(const uint64_t *__restrict
     }
     __syncthreads();
     const uint64_t chunk = (uint64_t)gridDim.x * 64;
-    for (uint32_t rr = ty; rr < 64; rr += 4) {
-        uint64_t x = tile[tx][rr];
-        for (uint32_t t = 0; t < T; t++)
-            XP[((uint64_t)t * chunk + rb + rr) * Kp + i0 + tx] = balanced(mod_small(x, t), c_mods.m[t]);
+    const uint32_t kq = threadIdx.x & 15, cg = threadIdx.x >> 4;  // inputs 4 kq .. 4 kq + 3, columns 4 cg .. 4 cg + 3
+#pragma unroll
+    for (uint32_t c = 0; c < 4; c++) {
+        const uint32_t col = 4 * cg + c;
+        uint64_t x[4];
+#pragma unroll
+        for (uint32_t j = 0; j < 4; j++) x[j] = tile[4 * kq + j][col];
+        for (uint32_t t = 0; t < T; t++) {
+            uint32_t w = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) w |= (uint32_t)(uint8_t)balanced(mod_small(x[j], t), c_mods.m[t]) << (8 * j);
+            *reinterpret_cast<uint32_t *>(XP + ((uint64_t)t * chunk + rb + col) * Kp + i0 + 4 * kq) = w;
+        }
     }
 }
 
@@ -313,9 +324,217 @@ __global__ void __launch_bounds__(kThreads, 2) mma_kernel(const int8_t *__restri
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kBN));
 }
 
+// ---------------------------------------------------------------- persistent GEMM
+// For K <= kResKp the 256-column X tile of one modulus stays resident in shared memory (Kp / 64
+// blocks of 16 KB in the MMA's core-matrix layout) while the CTA runs every output tile of it:
+// the weight tiles (A, 128 outputs x 64 K bytes) stream through a kAStages ring, and the
+// accumulators alternate between two 256-column TMEM buffers so that the epilogue of one output
+// tile overlaps the MMAs of the next.  One CTA per SM (all 512 TMEM columns), persistent over
+// the (modulus, column tile) pairs.  Roles: warps 0-3 copy (cp.async; the X tile, then the A
+// stages, each group's barrier arrived once the next group is issued), one thread of warp 4
+// issues the MMAs, warps 5-12 read the accumulators back (two warps per 32-lane quarter, one
+// per half of the columns).  Every wait is bounded; after a timeout a role waits no more and
+// carries on without its work, still arriving on its barriers, so the other roles finish too,
+// and the call reports the failure through *err.
+constexpr uint32_t kResKp = 768;
+constexpr int kAStages = 3;
+constexpr uint32_t kXBlock = kBN * kKB;  // 16 KB
+constexpr uint32_t kSmemP = (kResKp / kKB) * kXBlock + kAStages * kStageA + 1024;
+constexpr uint32_t kEpiWarp0 = 5;
+constexpr uint32_t kThreadsP = (kEpiWarp0 + 8) * 32;
+
+__global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8_t *__restrict__ XP,
+                                                                      const int8_t *__restrict__ WP,
+                                                                      uint8_t *__restrict__ RES, uint32_t Kp,
+                                                                      uint32_t Np, uint32_t n_out, uint64_t chunk,
+                                                                      uint32_t T, int *__restrict__ err, int acc24) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t full[kAStages], empty[kAStages], x_full, x_empty, acc_full[2], acc_empty[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ int failed;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint8_t *sX = smem, *sA = smem + (kResKp / kKB) * kXBlock;
+    const uint32_t nkb = Kp / kKB, n_ot = Np / kBM;
+    const uint64_t n_ct = chunk / kBN, n_tiles = (uint64_t)T * n_ct;
+    constexpr uint32_t kProducers = 128, kEpi = 256;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base)),
+                     "r"(2 * kBN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kAStages; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full[s])), "r"(kProducers));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&x_full)), "r"(kProducers));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&x_empty)));
+        for (int b = 0; b < 2; b++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&acc_full[b])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&acc_empty[b])), "r"(kEpi));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n");
+        failed = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n");
+    const uint32_t tmem = tmem_base;
+    const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((kBN >> 3) << 17) | ((kBM >> 4) << 24);
+    auto arrive = [](uint32_t bar) { asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar)); };
+
+    if (tid < kProducers) {
+        bool ok = true;
+        uint64_t g = 0;         // A stages issued so far (ring position)
+        uint32_t ti = 0;        // column tiles of this CTA so far
+        uint32_t pending = 0;   // barrier of the last committed group, arrived once the next is issued
+        const uint32_t kx16 = Kp / 16;
+        for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ti++) {
+            const uint32_t t = (uint32_t)(tile / n_ct);
+            const uint64_t rbase = (tile % n_ct) * kBN;
+            // every MMA of the previous column tile must have read the X tile: settle the last
+            // A stage first (the MMA thread waits for it), then wait
+            if (pending) {
+                asm volatile("cp.async.wait_group 0;\n");
+                asm volatile("fence.proxy.async.shared::cta;\n");
+                arrive(pending);
+                pending = 0;
+            }
+            if (ok && ti > 0 && !mbar_wait(smem_u32(&x_empty), (ti - 1) & 1)) ok = false;
+            const int8_t *B = XP + ((uint64_t)t * chunk + rbase) * Kp;
+            if (ok)
+                for (uint32_t c = tid; c < kBN * kx16; c += kProducers) {
+                    const uint32_t row = c / kx16, k16 = c % kx16;
+                    cp_async16(smem_u32(sX + (k16 >> 2) * kXBlock) + core_off(row, k16 & 3),
+                               B + (uint64_t)row * Kp + k16 * 16);
+                }
+            asm volatile("cp.async.commit_group;\n");
+            pending = smem_u32(&x_full);
+            for (uint32_t o = 0; o < n_ot; o++) {
+                const int8_t *A = WP + ((uint64_t)t * Np + o * kBM) * Kp;
+                for (uint32_t kb = 0; kb < nkb; kb++, g++) {
+                    const uint32_t s = (uint32_t)(g % kAStages);
+                    if (ok && g >= (uint64_t)kAStages && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((g / kAStages) - 1) & 1))
+                        ok = false;
+                    if (ok)
+                        for (uint32_t c = tid; c < kBM * (kKB / 16); c += kProducers) {
+                            const uint32_t row = c / (kKB / 16), kc = c % (kKB / 16);
+                            cp_async16(smem_u32(sA + s * kStageA) + core_off(row, kc),
+                                       A + (uint64_t)row * Kp + (uint64_t)kb * kKB + kc * 16);
+                        }
+                    asm volatile("cp.async.commit_group;\n");
+                    asm volatile("cp.async.wait_group 1;\n");  // the previous group has landed
+                    asm volatile("fence.proxy.async.shared::cta;\n");
+                    arrive(pending);
+                    pending = smem_u32(&full[s]);
+                }
+            }
+        }
+        if (pending) {
+            asm volatile("cp.async.wait_group 0;\n");
+            asm volatile("fence.proxy.async.shared::cta;\n");
+            arrive(pending);
+        }
+        if (!ok) failed = 1;
+    } else if (tid == kProducers) {
+        bool ok = true;
+        uint64_t g = 0;
+        uint32_t ti = 0, ai = 0;  // column tiles, accumulator tiles
+        for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ti++) {
+            if (ok && !mbar_wait(smem_u32(&x_full), ti & 1)) ok = false;
+            asm volatile("tcgen05.fence::after_thread_sync;\n");
+            for (uint32_t o = 0; o < n_ot; o++, ai++) {
+                const uint32_t buf = ai & 1;
+                if (ok && ai >= 2 && !mbar_wait(smem_u32(&acc_empty[buf]), ((ai >> 1) - 1) & 1)) ok = false;
+                asm volatile("tcgen05.fence::after_thread_sync;\n");
+                for (uint32_t kb = 0; kb < nkb; kb++, g++) {
+                    const uint32_t s = (uint32_t)(g % kAStages);
+                    if (ok && !mbar_wait(smem_u32(&full[s]), (uint32_t)(g / kAStages) & 1)) ok = false;
+                    asm volatile("tcgen05.fence::after_thread_sync;\n");
+                    if (ok) {
+                        const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sX + kb * kXBlock);
+#pragma unroll
+                        for (uint32_t k = 0; k < kKB / 32; k++) {
+                            const uint64_t ad = smem_desc(a0 + k * 256), bd = smem_desc(b0 + k * 256);
+                            const uint32_t accum = (kb | k) ? 1u : 0u;
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + buf * kBN),
+                                "l"(ad), "l"(bd), "r"(idesc), "r"(accum));
+                        }
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                        smem_u32(&empty[s])));
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                    smem_u32(&acc_full[buf])));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                smem_u32(&x_empty)));
+        }
+        if (!ok) failed = 1;
+    } else if (warp >= kEpiWarp0) {
+        bool ok = true;
+        const uint32_t quarter = warp & 3, half = (warp - kEpiWarp0) >> 2;
+        uint32_t ai = 0;
+        for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+            const uint32_t t = (uint32_t)(tile / n_ct);
+            const uint64_t rbase = (tile % n_ct) * kBN;
+            for (uint32_t o = 0; o < n_ot; o++, ai++) {
+                const uint32_t buf = ai & 1;
+                if (ok && !mbar_wait(smem_u32(&acc_full[buf]), (ai >> 1) & 1)) ok = false;
+                asm volatile("tcgen05.fence::after_thread_sync;\n");
+                const uint32_t out = o * kBM + quarter * 32 + lane;
+                if (ok) {
+                    for (uint32_t c0 = half * (kBN / 2); c0 < (half + 1) * (kBN / 2); c0 += 32) {
+                        uint32_t v[32];
+                        const uint32_t taddr = tmem + ((quarter * 32) << 16) + buf * kBN + c0;
+                        asm volatile(
+                            "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+                            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                              "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+                              "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+                              "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                            : "r"(taddr));
+                        asm volatile("tcgen05.wait::ld.sync.aligned;\n");
+                        if (out < n_out) {
+                            uint32_t pk[8];
+#pragma unroll
+                            for (int j = 0; j < 8; j++) {
+                                uint32_t w = 0;
+#pragma unroll
+                                for (int b = 0; b < 4; b++)
+                                    w |= (acc24 ? mod_acc24((int)v[4 * j + b], t) : mod_acc((int)v[4 * j + b], t))
+                                         << (8 * b);
+                                pk[j] = w;
+                            }
+                            uint4 *dst = reinterpret_cast<uint4 *>(RES + ((uint64_t)t * n_out + out) * chunk + rbase + c0);
+                            dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                            dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                        }
+                    }
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;\n");
+                arrive(smem_u32(&acc_empty[buf]));
+            }
+        }
+        if (!ok) failed = 1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n");
+    __syncthreads();
+    if (tid == 0 && failed) atomicExch(err, 1);
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(2 * kBN));
+}
+
 // ---------------------------------------------------------------- CRT fold
 struct CrtLimb {
     uint64_t c[kMaxMods];  // c_t mod q_l
+    double chd[kMaxMods];  // c_t >> 32 as a double (exact: below 2^29 for any prime below 2^61)
     uint64_t M;            // M mod q_l
 };
 
@@ -336,24 +555,31 @@ __global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict
         res[t] = t < T ? *reinterpret_cast<const uint32_t *>(RES + ((uint64_t)t * n_out + o) * chunk + r) : 0u;
     const PrimeConst p = pc[limb];
     uint64_t y[4];
+    const double two52 = 4503599627370496.0;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-        // sum_t r_t c_t as two 64-bit partial sums over the 32-bit halves of c_t (r_t < 2^8)
-        // v = round(sum_t r_t frac_t) in 32-bit fixed point: each frac_t is within 2^-33 of the
-        // exact fraction, so v is off by < 20 * 255 * 2^-33 while the CRT margin is 1/8
-        uint64_t lo = 0, hi = 0, vx = 0;
+        // sum_t r_t c_t from the 32-bit halves of c_t (r_t < 2^8): the low products on the integer
+        // pipe (64-bit sum below 2^45), the high ones on the FP64 pipe (each below 2^37, their sum
+        // below 2^42: exact in a double); v = round(sum_t r_t frac_t) on the FP64 pipe, off by far
+        // less than the CRT margin of 1/8.  The FP64 values are read back from their mantissas
+        // (2^52 added: exact integers below 2^52).
+        uint64_t lo = 0;
+        double hi = 0.0, v = 0.0;
 #pragma unroll
         for (uint32_t t = 0; t < kMaxMods; t++) {
             if (t < T) {
                 const uint32_t rt = (res[t] >> (8 * e)) & 0xFF;
-                const uint64_t c = cl.c[t];
-                lo += (uint64_t)rt * (uint32_t)c;
-                hi += (uint64_t)rt * (uint32_t)(c >> 32);
-                vx += (uint64_t)rt * c_mods.fracx[T][t];
+                lo += (uint64_t)rt * (uint32_t)cl.c[t];
+                const double rd = __dsub_rn(__hiloint2double(0x43300000, (int)rt), two52);
+                hi = __fma_rn(rd, cl.chd[t], hi);
+                v = __fma_rn(rd, c_mods.fracd[T][t], v);
             }
         }
-        u128 pos = {lo + (hi << 32), (hi >> 32) + ((lo + (hi << 32)) < lo ? 1ull : 0ull)};
-        const uint64_t vi = (vx + (1ull << 31)) >> 32;
+        const uint64_t mant = 0x000FFFFFFFFFFFFFull;
+        const uint64_t hii = (uint64_t)__double_as_longlong(__dadd_rn(hi, two52)) & mant;
+        const uint64_t vi = (uint64_t)__double_as_longlong(__dadd_rn(v, two52)) & mant;
+        const uint64_t plo = lo + (hii << 32);
+        const u128 pos = {plo, (hii >> 32) + (plo < lo ? 1ull : 0ull)};
         y[e] = sub_mod(barrett(pos, p), barrett(mul_wide(vi, cl.M), p), p.q);
     }
     ulonglong2 *out = reinterpret_cast<ulonglong2 *>(Y + (uint64_t)o * R + rg);
@@ -406,7 +632,7 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
             for (uint32_t u = 0; u < n; u++)
                 if (u != t) Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (cand[u] % m) % m);
             const uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);  // m prime
-            p.mods.fracx[n][t] = (uint32_t)std::llround((double)inv / (double)m * 4294967296.0);
+            p.mods.fracd[n][t] = (double)inv / (double)m;
         }
     // CRT constants of the chosen T: c_t = (M/m_t) * [(M/m_t)^-1 mod m_t] mod q_l
     p.limbs.resize(L);
@@ -424,6 +650,7 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
                 }
             uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);
             p.limbs[l].c[t] = host::mulmod(Mt, inv, q);
+            p.limbs[l].chd[t] = (double)(p.limbs[l].c[t] >> 32);
         }
     }
     return p;
@@ -469,7 +696,13 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     SHM_LAUNCHED(1);
     wres_kernel<<<dim3((Kp + 255) / 256, Np), 256, 0, st>>>(W, WP, n_in, n_out, Kp, Np, T);
     SHM_CUDA(cudaGetLastError());
-    SHM_CUDA(cudaFuncSetAttribute(mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    const bool resident = Kp <= kResKp;  // the X tile fits in shared memory: the persistent kernel
+    if (resident)
+        SHM_CUDA(cudaFuncSetAttribute(mma_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemP));
+    else
+        SHM_CUDA(cudaFuncSetAttribute(mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    int sms = 0;
+    SHM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
     const int acc24 = (uint64_t)Kp * 125 * 125 < (1ull << 24) ? 1 : 0;  // accumulators exact in float
     for (uint64_t r0 = 0; r0 < R; r0 += chunk) {
         // a shorter last pass (2 L N not a multiple of the chunk, e.g. at N = 2^12) lays its planes out
@@ -479,8 +712,14 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
         xres_kernel<<<dim3((uint32_t)(cur / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0, T);
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
-        mma_kernel<<<dim3(Np / kBM, (uint32_t)(cur / kBN), T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
-                                                                                     cur, err, acc24);
+        if (resident) {
+            const uint64_t tiles = (uint64_t)T * (cur / kBN);
+            const uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sms);
+            mma_persistent_kernel<<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24);
+        } else {
+            mma_kernel<<<dim3(Np / kBM, (uint32_t)(cur / kBN), T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
+                                                                                         cur, err, acc24);
+        }
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
         crt_kernel<<<dim3((uint32_t)((cur / 4 + 255) / 256), n_out), 256, 0, st>>>(RES, Y, tab, n_out, cur, r0, R, L,

@@ -76,11 +76,46 @@ __global__ void tensor_kernel(const uint64_t *__restrict__ a, const uint64_t *__
     O[2 * ln + k] = mul_mod(a1, b1, p);
 }
 
-__global__ void galois_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ out,
-                              const uint32_t *__restrict__ perm, uint32_t log_n) {
+// out[ct] (+)= sum_{t < k} A_t[ct a_step] x B_t[ct b_step]: the size-3 tensor products of k
+// ciphertext pairs summed before one reduction (step 0 broadcasts one ciphertext over the batch).
+// The host bounds k so that each sum (2k products for the middle term) stays below the Barrett
+// bound; S52: the products' 32-bit partials summed in three 64-bit words (every prime < 2^52).
+template <bool S52>
+__global__ void tensor_acc_kernel(PtrTab A, PtrTab B, uint32_t k, uint32_t a_step, uint32_t b_step,
+                                  uint64_t *__restrict__ out, uint32_t L, uint32_t log_n,
+                                  const PrimeConst *__restrict__ pc, int accumulate) {
+    const uint32_t limb = blockIdx.y, ct = blockIdx.z;
+    const PrimeConst p = pc[limb];
+    const size_t ln = (size_t)L << log_n;
+    const size_t kk = ((size_t)limb << log_n) + blockIdx.x * kEwThreads + threadIdx.x;
+    Acc<S52> s0, s1, s2;
+    for (uint32_t t = 0; t < k; t++) {
+        const uint64_t *a = A.p[t] + (size_t)ct * a_step * 2 * ln, *b = B.p[t] + (size_t)ct * b_step * 2 * ln;
+        const uint64_t a0 = a[kk], a1 = a[ln + kk], b0 = b[kk], b1 = b[ln + kk];
+        s0.add(a0, b0);
+        s1.add(a0, b1);
+        s1.add(a1, b0);
+        s2.add(a1, b1);
+    }
+    uint64_t *O = out + (size_t)ct * 3 * ln;
+    uint64_t r0 = barrett(s0.get(), p), r1 = barrett(s1.get(), p), r2 = barrett(s2.get(), p);
+    if (accumulate) {
+        r0 = add_mod(r0, O[kk], p.q);
+        r1 = add_mod(r1, O[ln + kk], p.q);
+        r2 = add_mod(r2, O[2 * ln + kk], p.q);
+    }
+    O[kk] = r0;
+    O[ln + kk] = r1;
+    O[2 * ln + kk] = r2;
+}
+
+// NTT-domain automorphism computed per element: slot k takes slot perm(k) with
+// 2 brv(perm(k)) + 1 = (2 brv(k) + 1) elt mod 2N (the table of Context::perm, without the table)
+__global__ void galois_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ out, uint32_t elt,
+                              uint32_t log_n) {
     const size_t row = blockIdx.y;
     const uint32_t k = blockIdx.x * kEwThreads + threadIdx.x;
-    out[(row << log_n) + k] = in[(row << log_n) + __ldg(perm + k)];
+    out[(row << log_n) + k] = in[(row << log_n) + galois_index(k, elt, log_n)];
 }
 
 // copy the last limb of every polynomial into a contiguous buffer
@@ -128,10 +163,23 @@ void tensor(const Context &c, const uint64_t *a, const uint64_t *b, uint64_t *ou
     SHM_CUDA(cudaGetLastError());
 }
 
+void tensor_accumulate(const Context &c, const PtrTab &A, const PtrTab &B, uint32_t k, uint32_t a_step,
+                       uint32_t b_step, uint64_t *out, uint32_t n_cts, uint32_t L, bool accumulate, cudaStream_t st) {
+    if (n_cts == 0 || k == 0) return;
+    const dim3 grid(c.n / kEwThreads, L, n_cts);
+    SHM_LAUNCHED(1);
+    if (c.s52)
+        tensor_acc_kernel<true><<<grid, kEwThreads, 0, st>>>(A, B, k, a_step, b_step, out, L, c.log_n, c.pc,
+                                                             accumulate ? 1 : 0);
+    else
+        tensor_acc_kernel<false><<<grid, kEwThreads, 0, st>>>(A, B, k, a_step, b_step, out, L, c.log_n, c.pc,
+                                                              accumulate ? 1 : 0);
+    SHM_CUDA(cudaGetLastError());
+}
+
 void apply_galois(const Context &c, const uint64_t *in, uint64_t *out, uint32_t rows, uint32_t elt, cudaStream_t st) {
     if (rows == 0) return;
-    const uint32_t *perm = const_cast<Context &>(c).perm(elt);
-    SHM_LAUNCHED(1); galois_kernel<<<dim3(c.n / kEwThreads, rows), kEwThreads, 0, st>>>(in, out, perm, c.log_n);
+    SHM_LAUNCHED(1); galois_kernel<<<dim3(c.n / kEwThreads, rows), kEwThreads, 0, st>>>(in, out, elt, c.log_n);
     SHM_CUDA(cudaGetLastError());
 }
 

@@ -19,6 +19,24 @@ struct Geo {
 
 __device__ __forceinline__ uint32_t padded(uint32_t p) { return p + (p >> 4); }
 
+// sum_{i < n} x[i << log_n] c[i] mod p (a base conversion's term for one coefficient; n <= 16).  The
+// first eight terms' loads are issued together before any product, so one load latency is exposed
+// per coefficient instead of one per term.
+template <bool S52>
+__device__ __forceinline__ uint64_t conv_sum(const uint64_t *__restrict__ x, const uint64_t *c, uint32_t n,
+                                             int log_n, const PrimeConst &p) {
+    constexpr uint32_t kBatch = 8;
+    uint64_t v[kBatch];
+#pragma unroll
+    for (uint32_t i = 0; i < kBatch; i++) v[i] = i < n ? x[(size_t)i << log_n] : 0;
+    Acc<S52> acc;
+#pragma unroll
+    for (uint32_t i = 0; i < kBatch; i++)
+        if (i < n) acc.add(v[i], c[i]);
+    for (uint32_t i = kBatch; i < n; i++) acc.add(x[(size_t)i << log_n], c[i]);
+    return barrett(acc.get(), p);
+}
+
 // CTAs are issued limb-major: consecutive CTAs work on the same limb slot (one prime) of
 // successive polynomials, so the CTAs in flight share one prime's twiddle table in L2.
 // rows = polys * slots; CTA index t -> (poly = t % polys, slot = t / polys).
@@ -31,7 +49,7 @@ __device__ __forceinline__ uint32_t limb_major_row(uint32_t t, uint32_t slots, u
 // IOK = kIoRescale: row (poly, j) is read as c_last[poly] mod q_j from the coefficient-form
 // last limbs; kIoModDown: as the base conversion of the special-prime limbs (ModDownIO);
 // kIoPlain: from `data`
-template <int R, int S, int MINB, int IOK = kIoPlain>
+template <int R, int S, int MINB, int IOK, int FAM>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const double *__restrict__ twq,
@@ -80,15 +98,8 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 #pragma unroll
         for (int m = 0; m < G::E; m++) {
             const size_t pos = sig + (size_t)G::M * (lane + m * G::E);
-            if (mu.s52) {
-                Acc<true> acc;
-                for (uint32_t i = 0; i < na; i++) acc.add(y[((size_t)i << G::LOGN) + pos], sconv[i]);
-                a[m] = barrett(acc.get(), p);
-            } else {
-                Acc<false> acc;
-                for (uint32_t i = 0; i < na; i++) acc.add(y[((size_t)i << G::LOGN) + pos], sconv[i]);
-                a[m] = barrett(acc.get(), p);
-            }
+            a[m] = mu.s52 ? conv_sum<true>(y + pos, sconv, na, G::LOGN, p)
+                          : conv_sum<false>(y + pos, sconv, na, G::LOGN, p);
         }
     } else if constexpr (IOK == kIoRescale) {
         const PrimeConst p = pc[pidx];
@@ -106,15 +117,8 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 #pragma unroll
         for (int m = 0; m < G::E; m++) {
             const size_t pos = sig + (size_t)G::M * (lane + m * G::E);
-            if (io.md.s52) {
-                Acc<true> acc;
-                for (uint32_t k = 0; k < np; k++) acc.add(z[((size_t)k << G::LOGN) + pos], sconv[k]);
-                a[m] = barrett(acc.get(), p);
-            } else {
-                Acc<false> acc;
-                for (uint32_t k = 0; k < np; k++) acc.add(z[((size_t)k << G::LOGN) + pos], sconv[k]);
-                a[m] = barrett(acc.get(), p);
-            }
+            a[m] = io.md.s52 ? conv_sum<true>(z + pos, sconv, np, G::LOGN, p)
+                             : conv_sum<false>(z + pos, sconv, np, G::LOGN, p);
         }
         if (io.md.vrow) {
             const uint8_t *vr = io.md.vrow + ((size_t)(row / slots) << G::LOGN) + chunk * S;
@@ -125,13 +129,13 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 #pragma unroll
         for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane + m * G::E)];
     }
-    fwd_pass_any<R>(mode, a, w, ws, wq, 1, 0, 0, q);
+    fwd_pass_any<R, FAM>(mode, a, w, ws, wq, 1, 0, 0, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) sm[(lane + m * G::E) * S + sig] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = sm[(lane * G::E + m) * S + sig];
-    fwd_pass_any<R>(mode, a, w, ws, wq, 1, R, lane, q);
+    fwd_pass_any<R, FAM>(mode, a, w, ws, wq, 1, R, lane, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane * G::E + m)] = a[m];
 }
@@ -139,7 +143,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 // ---------------- forward, phase 2: blocks (global stages LOGM .. 2*LOGM-1), fully reduced output
 // IOK = kIoRescale: instead of storing t = NTT(...) of row (poly, j), write (c_j - t) q_last^-1
 // to io.rs.out; kIoModDown: write (acc_j - t) P^-1 (+ add) to io.md.out
-template <int R, int S, int MINB, int IOK = kIoPlain>
+template <int R, int S, int MINB, int IOK, int FAM>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const double *__restrict__ twq,
@@ -163,14 +167,14 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = x[lane + m * G::E];
-    fwd_pass_any<R>(mode, a, w, ws, wq, G::M + b, 0, 0, q);
+    fwd_pass_any<R, FAM>(mode, a, w, ws, wq, G::M + b, 0, 0, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) s[padded(lane + m * G::E)] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
-    if (mode != kBfHarvey) {
-        fwd_pass_any<R>(mode, a, w, ws, wq, G::M + b, R, lane, q);
+    if (!(FAM & (1 << kBfHarvey)) || mode != kBfHarvey) {
+        fwd_pass_any<R, FAM>(mode, a, w, ws, wq, G::M + b, R, lane, q);
         const PrimeConst p = pc[pidx];
 #pragma unroll
         for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = reduce_small(a[m], p);  // < 68q -> [0, q)
@@ -232,7 +236,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
 }
 
 // ---------------- inverse, phase 1: blocks (global stages 2*LOGM-1 .. LOGM)
-template <int R, int S, int MINB>
+template <int R, int S, int MINB, int FAM>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_blk(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const double *__restrict__ twq,
@@ -261,20 +265,20 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_blk(uint64_t *__
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
     const int mode = bf_mode_of(q);  // uniform per CTA (one limb)
-    inv_pass_any<R>(mode, a, w, ws, wq, G::M + b, R, lane, q, 0);
+    inv_pass_any<R, FAM>(mode, a, w, ws, wq, G::M + b, R, lane, q, 0);
 #pragma unroll
     for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane + m * G::E)];
-    inv_pass_any<R>(mode, a, w, ws, wq, G::M + b, 0, 0, q, 0);
+    inv_pass_any<R, FAM>(mode, a, w, ws, wq, G::M + b, 0, 0, q, 0);
     uint64_t *x = xc + (size_t)sig * G::M;
 #pragma unroll
     for (int m = 0; m < G::E; m++) x[lane + m * G::E] = a[m];
 }
 
 // ---------------- inverse, phase 2: columns (global stages LOGM-1 .. 0) with the folded scale
-template <int R, int S, int MINB>
+template <int R, int S, int MINB, int FAM>
 __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__restrict__ data, uint32_t slots, LimbMap map,
                                                             const uint64_t *__restrict__ tw,
                                                             const double *__restrict__ twq,
@@ -299,13 +303,13 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane * G::E + m)];
     const int mode = bf_mode_of(q);  // the same choice inv_blk made for this limb
-    inv_pass_any<R>(mode, a, w, ws, wq, 1, R, lane, q, 0);
+    inv_pass_any<R, FAM>(mode, a, w, ws, wq, 1, R, lane, q, 0);
 #pragma unroll
     for (int m = 0; m < G::E; m++) sm[(lane * G::E + m) * S + sig] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = sm[(lane + m * G::E) * S + sig];
-    inv_pass_any<R>(mode, a, w, ws, wq, 1, 0, 0, q, 1);
+    inv_pass_any<R, FAM>(mode, a, w, ws, wq, 1, 0, 0, q, 1);
     // values in [0, 4q) (grow, FP64) or [0, 2q) (Harvey)
     const uint64_t c0 = sc[0], c0s = sc[1], c1 = sc[2], c1s = sc[3], q2 = (mode != kBfHarvey ? 4 : 2) * q;
 #pragma unroll
@@ -318,50 +322,71 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__
     for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane + m * G::E)] = a[m];
 }
 
-template <int R, int S, int MINB, int IOK = kIoPlain>
+template <int R, int S, int MINB, int IOK, int FAM>
 void launch_fwd_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
-                  cudaStream_t st, const NttIO &io = NttIO{}) {
+                  cudaStream_t st, const NttIO &io) {
     using G = Geo<R, S>;
     dim3 grid(rows * G::CHUNKS);
     constexpr int BLK = IOK == kIoModUp ? kIoPlain : IOK;  // ModUp's block phase is a plain one
     SHM_LAUNCHED(1);
-    fwd_col<R, S, MINB, IOK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc, io);
+    fwd_col<R, S, MINB, IOK, FAM><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc, io);
     SHM_LAUNCHED(1);
-    fwd_blk<R, S, MINB, BLK><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc, io);
+    fwd_blk<R, S, MINB, BLK, FAM><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc, io);
 }
 
-template <int R, int S, int MINB>
+template <int R, int S, int MINB, int FAM>
 void launch_inv_v(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
                   const uint64_t *scale, uint32_t scale_base, cudaStream_t st) {
     using G = Geo<R, S>;
     dim3 grid(rows * G::CHUNKS);
     SHM_LAUNCHED(1);
-    inv_blk<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc);
+    inv_blk<R, S, MINB, FAM><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc);
     SHM_LAUNCHED(1);
-    inv_col<R, S, MINB><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc,
-                                                     scale ? scale : c.inv_scale_plain, scale ? 0 : 1, scale_base);
+    inv_col<R, S, MINB, FAM><<<grid, G::THREADS, 0, st>>>(data, slots, map, c.tw, c.twq, c.pc,
+                                                          scale ? scale : c.inv_scale_plain, scale ? 0 : 1, scale_base);
 }
 
-// the tile variants of kNttVariants (ntt.cuh), selected per context by c.ntt_variant
+// the tile variants of kNttVariants (ntt.cuh), selected per context by c.ntt_variant, in the
+// butterfly families of the context's primes (c.ntt_families)
+template <int R, int IOK, int FAM>
+void launch_fwd_f(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                  cudaStream_t st, const NttIO &io) {
+    switch (c.ntt_variant) {
+        case 1: launch_fwd_v<R, 16, 3, IOK, FAM>(c, data, rows, slots, map, st, io); break;
+        case 2: launch_fwd_v<R, 8, 8, IOK, FAM>(c, data, rows, slots, map, st, io); break;
+        case 3: launch_fwd_v<R, 8, 6, IOK, FAM>(c, data, rows, slots, map, st, io); break;
+        default: launch_fwd_v<R, 16, 4, IOK, FAM>(c, data, rows, slots, map, st, io); break;
+    }
+}
+
 template <int R, int IOK = kIoPlain>
 void launch_fwd(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
                 cudaStream_t st, const NttIO &io = NttIO{}) {
+    switch (c.ntt_families) {
+        case kFamSmall: launch_fwd_f<R, IOK, kFamSmall>(c, data, rows, slots, map, st, io); break;
+        case kFamLarge: launch_fwd_f<R, IOK, kFamLarge>(c, data, rows, slots, map, st, io); break;
+        default: launch_fwd_f<R, IOK, kFamAll>(c, data, rows, slots, map, st, io); break;
+    }
+}
+
+template <int R, int FAM>
+void launch_inv_f(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
+                  const uint64_t *scale, uint32_t scale_base, cudaStream_t st) {
     switch (c.ntt_variant) {
-        case 1: launch_fwd_v<R, 16, 3, IOK>(c, data, rows, slots, map, st, io); break;
-        case 2: launch_fwd_v<R, 8, 8, IOK>(c, data, rows, slots, map, st, io); break;
-        case 3: launch_fwd_v<R, 8, 6, IOK>(c, data, rows, slots, map, st, io); break;
-        default: launch_fwd_v<R, 16, 4, IOK>(c, data, rows, slots, map, st, io); break;
+        case 1: launch_inv_v<R, 16, 3, FAM>(c, data, rows, slots, map, scale, scale_base, st); break;
+        case 2: launch_inv_v<R, 8, 8, FAM>(c, data, rows, slots, map, scale, scale_base, st); break;
+        case 3: launch_inv_v<R, 8, 6, FAM>(c, data, rows, slots, map, scale, scale_base, st); break;
+        default: launch_inv_v<R, 16, 4, FAM>(c, data, rows, slots, map, scale, scale_base, st); break;
     }
 }
 
 template <int R>
 void launch_inv(const Context &c, uint64_t *data, uint32_t rows, uint32_t slots, const LimbMap &map,
                 const uint64_t *scale, uint32_t scale_base, cudaStream_t st) {
-    switch (c.ntt_variant) {
-        case 1: launch_inv_v<R, 16, 3>(c, data, rows, slots, map, scale, scale_base, st); break;
-        case 2: launch_inv_v<R, 8, 8>(c, data, rows, slots, map, scale, scale_base, st); break;
-        case 3: launch_inv_v<R, 8, 6>(c, data, rows, slots, map, scale, scale_base, st); break;
-        default: launch_inv_v<R, 16, 4>(c, data, rows, slots, map, scale, scale_base, st); break;
+    switch (c.ntt_families) {
+        case kFamSmall: launch_inv_f<R, kFamSmall>(c, data, rows, slots, map, scale, scale_base, st); break;
+        case kFamLarge: launch_inv_f<R, kFamLarge>(c, data, rows, slots, map, scale, scale_base, st); break;
+        default: launch_inv_f<R, kFamAll>(c, data, rows, slots, map, scale, scale_base, st); break;
     }
 }
 

@@ -172,9 +172,16 @@ __device__ __forceinline__ void gs_bf4(uint64_t &x, uint64_t &y, uint64_t w, uin
 constexpr int kBfHarvey = 0, kBfGrow = 1, kBfF64 = 2;
 
 // the butterfly family of a limb's prime
-__device__ __forceinline__ int bf_mode_of(uint64_t q) {
+__host__ __device__ __forceinline__ int bf_mode_of(uint64_t q) {
     return q < kF64GrowLimit ? kBfF64 : q < kGrowPrimeLimit ? kBfGrow : kBfHarvey;
 }
+
+// The families a kernel instantiation carries (a bit per family).  Every unrolled family adds a
+// full copy of the transform's butterflies to the kernel, so a context's launches use the
+// instantiation with just the families its primes need: kFamSmall (every prime below 2^57: the
+// bootstrapping chains), kFamLarge (none below kF64GrowLimit), kFamAll otherwise.
+constexpr int kFamSmall = (1 << kBfF64) | (1 << kBfGrow), kFamLarge = (1 << kBfGrow) | (1 << kBfHarvey),
+              kFamAll = kFamSmall | kFamLarge;
 
 template <int R, int MODE = kBfHarvey>
 __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
@@ -198,14 +205,14 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
     }
 }
 
-// fwd_pass in the butterfly family `mode` (uniform per CTA: one limb)
-template <int R>
+// fwd_pass in the butterfly family `mode` (uniform per CTA: one limb), one of the families FAM carries
+template <int R, int FAM>
 __device__ __forceinline__ void fwd_pass_any(int mode, uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
                                              const uint64_t *__restrict__ ws, const double *__restrict__ wq,
                                              uint32_t tb, uint32_t s0, uint32_t g, uint64_t q) {
-    if (mode == kBfF64)
+    if ((FAM & (1 << kBfF64)) && mode == kBfF64)
         fwd_pass<R, kBfF64>(a, w, ws, wq, tb, s0, g, q);
-    else if (mode == kBfGrow)
+    else if (!(FAM & (1 << kBfHarvey)) || mode == kBfGrow)
         fwd_pass<R, kBfGrow>(a, w, ws, wq, tb, s0, g, q);
     else
         fwd_pass<R, kBfHarvey>(a, w, ws, wq, tb, s0, g, q);
@@ -236,13 +243,13 @@ __device__ __forceinline__ void inv_pass(uint64_t (&a)[1 << R], const uint64_t *
     }
 }
 
-template <int R>
+template <int R, int FAM>
 __device__ __forceinline__ void inv_pass_any(int mode, uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
                                              const uint64_t *__restrict__ ws, const double *__restrict__ wq,
                                              uint32_t tb, uint32_t s0, uint32_t g, uint64_t q, int skip_stage0) {
-    if (mode == kBfF64)
+    if ((FAM & (1 << kBfF64)) && mode == kBfF64)
         inv_pass<R, kBfF64>(a, w, ws, wq, tb, s0, g, q, skip_stage0);
-    else if (mode == kBfGrow)
+    else if (!(FAM & (1 << kBfHarvey)) || mode == kBfGrow)
         inv_pass<R, kBfGrow>(a, w, ws, wq, tb, s0, g, q, skip_stage0);
     else
         inv_pass<R, kBfHarvey>(a, w, ws, wq, tb, s0, g, q, skip_stage0);

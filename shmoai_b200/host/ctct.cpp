@@ -2,28 +2,14 @@
 // (ct_ct_matrix_mul_colpacking, src/include/source/matrix_mul/Ct_ct_matrix_mul.cuh:10-120):
 // out_i = sum_j X_j * rot(W_j, i * num_batch), one relinearisation and rescale per output.
 // The rotations of W are hoisted (one ModUp of the whole W batch for every step) and the
-// products are summed unrelinearised (size 3), as the reference sums before relinearising.
+// products are summed unrelinearised (size 3) in one pass, as the reference sums before
+// relinearising.
 #include <algorithm>
 #include <cmath>
 
 #include "internal.hpp"
 
 namespace shmoai {
-
-namespace {
-
-// sum over a batch of ordinary ciphertexts of any size (2 or 3): halves added pairwise
-Ciphertext sum_members(const Evaluator &ev, Ciphertext cur) {
-    while (cur.count > 1) {
-        const uint32_t h = cur.count / 2;
-        Ciphertext s = ev.add(ev.slice(cur, 0, h), ev.slice(cur, h, h));
-        if (cur.count & 1) s = ev.concat(s, ev.slice(cur, 2 * h, 1));
-        cur = std::move(s);
-    }
-    return cur;
-}
-
-}  // namespace
 
 Ciphertext ct_ct_matmul_colpacking(const Evaluator &ev, const Ciphertext &X, const Ciphertext &W, uint32_t rows,
                                    uint32_t num_batch, KeyGenerator *keys) {
@@ -53,14 +39,18 @@ Ciphertext ct_ct_matmul_colpacking(const Evaluator &ev, const Ciphertext &X, con
                 if (!chunk_keys.count(e)) chunk_keys.emplace(e, keys->galois_key(e));
             }
         const std::map<int, Ciphertext> rot = (keys ? kev : ev).rotate_many(W, steps);
+        // each row's products summed in one pass (no size-3 batch of the products), and the chunk's
+        // rows relinearised and rescaled as one batch
+        std::vector<Ciphertext> sums;
         for (uint32_t i = lo; i < hi; i++) {
             const int step = (int)(i * num_batch);
             auto it = rot.find(step);
             const Ciphertext &Wi = (i == 0 || it == rot.end()) ? W : it->second;  // a full turn is W itself
-            outs.push_back(ev.relinearize_rescale(sum_members(ev, ev.multiply_lazy(X, Wi))));
+            sums.push_back(ev.sum_of_products(X, Wi));
         }
+        outs.push_back(ev.relinearize_rescale(batch_gather(ev, std::move(sums))));
     }
-    return batch_gather(ev, outs);
+    return batch_gather(ev, std::move(outs));
 }
 
 Ciphertext ct_ct_matmul_diagpacking(const Evaluator &ev, const Ciphertext &X, const Ciphertext &W,
@@ -98,13 +88,15 @@ Ciphertext ct_ct_matmul_diagpacking(const Evaluator &ev, const Ciphertext &X, co
     };
     Ciphertext total;
     for (uint32_t i = 0; i < b; i++) {
-        Ciphertext acc;
-        for (uint32_t k = 0; k < g && i * g + k < col; k++) {
-            const Ciphertext xk = ev.slice(rx[i], k, 1);
-            Ciphertext p = ev.multiply_lazy(baby(k), batch_broadcast(ev, xk, cw));
-            acc = acc.count ? ev.add(acc, p) : std::move(p);
+        // sum_k baby(k) x X's member k of the group, X's member broadcast over W's batch, summed in one pass
+        std::vector<Ciphertext> xs;
+        std::vector<const Ciphertext *> As, Bs;
+        for (uint32_t k = 0; k < g && i * g + k < col; k++) xs.push_back(ev.slice(rx[i], k, 1));
+        for (uint32_t k = 0; k < xs.size(); k++) {
+            As.push_back(&baby(k));
+            Bs.push_back(&xs[k]);
         }
-        Ciphertext o = ev.relinearize_rescale(acc);
+        Ciphertext o = ev.relinearize_rescale(ev.multiply_accumulate(As, Bs));
         const int gs = norm((int64_t)i * g * num_batch);
         if (i > 0 && gs != 0) o = std::move(ev.rotate_many(o, {gs}).at(gs));
         total = total.count ? ev.add(total, o) : std::move(o);

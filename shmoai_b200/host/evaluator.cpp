@@ -237,6 +237,71 @@ Ciphertext Evaluator::multiply_lazy(const Ciphertext &a, const Ciphertext &b) co
     return r;
 }
 
+Ciphertext Evaluator::multiply_accumulate(const std::vector<const Ciphertext *> &A,
+                                          const std::vector<const Ciphertext *> &B) const {
+    if (A.empty() || A.size() != B.size()) throw Error("multiply_accumulate: bad term lists");
+    const uint32_t count = A[0]->count;
+    uint32_t L = A[0]->L;
+    const bool bcast = B[0]->count == 1 && count > 1;
+    for (size_t t = 0; t < A.size(); t++) {
+        const Ciphertext &a = *A[t], &b = *B[t];
+        if (a.shared || b.shared || a.size != 2 || b.size != 2) throw Error("multiply needs ordinary ciphertexts");
+        if (a.count != count || b.count != (bcast ? 1 : count)) throw Error("multiply_accumulate: batch sizes differ");
+        if (!same_scale(a.scale_ * b.scale_, A[0]->scale_ * B[0]->scale_)) throw Error("scale mismatch in add");
+        L = std::min(L, std::min(a.L, b.L));
+    }
+    // terms above the common level are dropped to it (kept alive here for the call)
+    std::vector<Ciphertext> dropped;
+    dropped.reserve(2 * A.size());
+    std::vector<const uint64_t *> pa(A.size()), pb(B.size());
+    for (size_t t = 0; t < A.size(); t++) {
+        const Ciphertext *a = A[t], *b = B[t];
+        if (a->L != L) {
+            dropped.push_back(mod_switch_to(*a, L));
+            a = &dropped.back();
+        }
+        if (b->L != L) {
+            dropped.push_back(mod_switch_to(*b, L));
+            b = &dropped.back();
+        }
+        pa[t] = a->data.data();
+        pb[t] = b->data.data();
+    }
+    Ciphertext r;
+    r.data = DeviceBuffer(c_, (size_t)count * 3 * L * c_.n);
+    r.count = count;
+    r.size = 3;
+    r.L = L;
+    r.scale_ = A[0]->scale_ * B[0]->scale_;
+    c_.check(shm_multiply_accumulate(c_.handle(), pa.data(), pb.data(), (uint32_t)A.size(), bcast ? 1 : 0,
+                                     r.data.data(), count, L, 0, c_.stream()));
+    return r;
+}
+
+Ciphertext Evaluator::sum_of_products(const Ciphertext &X, const Ciphertext &W) const {
+    if (X.shared || W.shared || X.size != 2 || W.size != 2) throw Error("multiply needs ordinary ciphertexts");
+    if (X.count != W.count || X.count == 0) throw Error("sum_of_products: batches of different sizes");
+    if (X.L != W.L) {
+        const uint32_t L = std::min(X.L, W.L);
+        return X.L > L ? sum_of_products(mod_switch_to(X, L), W) : sum_of_products(X, mod_switch_to(W, L));
+    }
+    const size_t per = (size_t)2 * X.L * c_.n;
+    std::vector<const uint64_t *> pa(X.count), pb(X.count);
+    for (uint32_t j = 0; j < X.count; j++) {
+        pa[j] = X.data.data() + j * per;
+        pb[j] = W.data.data() + j * per;
+    }
+    Ciphertext r;
+    r.data = DeviceBuffer(c_, (size_t)3 * X.L * c_.n);
+    r.count = 1;
+    r.size = 3;
+    r.L = X.L;
+    r.scale_ = X.scale_ * W.scale_;
+    c_.check(shm_multiply_accumulate(c_.handle(), pa.data(), pb.data(), X.count, 0, r.data.data(), 1, X.L, 0,
+                                     c_.stream()));
+    return r;
+}
+
 Ciphertext Evaluator::relinearize(const Ciphertext &a) const {
     if (a.shared || a.size != 3) throw Error("relinearize takes size-3 ciphertexts");
     if (!relin_key) throw Error("no relinearisation key");

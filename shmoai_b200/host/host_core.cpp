@@ -311,18 +311,6 @@ DeviceBuffer KeyGenerator::ntt_qp(const std::vector<int64_t> &coeffs) const {
     return d;
 }
 
-// s(X^elt) in NTT form: coefficient j moves to j * elt mod 2N, negated past N
-DeviceBuffer KeyGenerator::automorph(const std::vector<int64_t> &s, uint32_t elt) const {
-    const uint64_t N = c_.n, M = 2 * N;
-    std::vector<int64_t> out(N, 0);
-    for (uint64_t j = 0; j < N; j++) {
-        const uint64_t t = (j * elt) % M;
-        if (t < N) out[t] += s[j];
-        else out[t - N] -= s[j];
-    }
-    return ntt_qp(out);
-}
-
 std::vector<uint64_t> KeyGenerator::p_units(int digit) const {
     std::vector<uint64_t> unit(c_.nq + c_.np, 0);
     uint32_t lo = 0, hi = c_.nq;
@@ -453,7 +441,15 @@ Ciphertext PublicEncryptor::encrypt(const Plaintext &pt) {
     return ct;
 }
 
-DeviceBuffer KeyGenerator::galois_key(uint32_t elt) { return switching_key(automorph(s_coeffs_, elt)); }
+// s(X^elt) in NTT form, permuted on the device from the NTT form of s (equal to the NTT of the
+// permuted coefficients: the automorphism only reorders the evaluation points)
+DeviceBuffer KeyGenerator::automorph_ntt(const DeviceBuffer &s_ntt, uint32_t elt) const {
+    DeviceBuffer out(c_, (size_t)(c_.nq + c_.np) * c_.n);
+    c_.check(shm_permute_galois(c_.handle(), s_ntt.data(), elt, out.data(), c_.nq + c_.np, c_.stream()));
+    return out;
+}
+
+DeviceBuffer KeyGenerator::galois_key(uint32_t elt) { return switching_key(automorph_ntt(s_, elt)); }
 
 std::map<uint32_t, DeviceBuffer> KeyGenerator::galois_keys(const std::vector<uint32_t> &elts) {
     std::map<uint32_t, DeviceBuffer> out;
@@ -474,7 +470,7 @@ void KeyGenerator::gen_aux_secrets(uint32_t members, uint32_t hamming_weight) {
 DeviceBuffer KeyGenerator::shared_galois_key(uint32_t elt) {
     if (aux_.empty()) throw Error("no auxiliary secrets: call gen_aux_secrets first");
     std::vector<DeviceBuffer> news;
-    for (auto &s : aux_coeffs_) news.push_back(automorph(s, elt));
+    for (auto &s : aux_) news.push_back(automorph_ntt(s, elt));
     std::vector<const DeviceBuffer *> olds;
     for (auto &a : aux_) olds.push_back(&a);
     std::vector<std::vector<KeyTerm>> adds(c_.dnum);

@@ -86,10 +86,13 @@ Ciphertext add_column_bias(const Evaluator &ev, const Ciphertext &Y, const std::
     return o;
 }
 
-Ciphertext bootstrap_segment(const Evaluator &ev, const BatchBootstrapper &boot, const Ciphertext &x,
-                             uint32_t members, uint32_t batch) {
+namespace {
+
+Ciphertext bootstrap_segment_impl(const Evaluator &ev, const BatchBootstrapper &boot, const Ciphertext &x,
+                                  Ciphertext *owned, uint32_t members, uint32_t batch) {
     const BootstrapParams &p = boot.params();
     const Ciphertext in = ev.adjust(x, p.input_level, p.scale);
+    if (owned) *owned = Ciphertext();
     const uint32_t unit = members ? members : 1;
     uint32_t step = std::max(unit, batch - batch % unit);
     std::vector<Ciphertext> parts;
@@ -106,6 +109,18 @@ Ciphertext bootstrap_segment(const Evaluator &ev, const BatchBootstrapper &boot,
         }
     }
     return batch_gather(ev, std::move(parts));
+}
+
+}  // namespace
+
+Ciphertext bootstrap_segment(const Evaluator &ev, const BatchBootstrapper &boot, const Ciphertext &x,
+                             uint32_t members, uint32_t batch) {
+    return bootstrap_segment_impl(ev, boot, x, nullptr, members, batch);
+}
+
+Ciphertext bootstrap_segment(const Evaluator &ev, const BatchBootstrapper &boot, Ciphertext &&x, uint32_t members,
+                             uint32_t batch) {
+    return bootstrap_segment_impl(ev, boot, x, &x, members, batch);
 }
 
 namespace {
@@ -270,8 +285,7 @@ Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot,
     Ciphertext so = add_column_bias(ev, ev.ctpt_matmul(att, int_weights(w.Wo, d, d, 0, d, ws), d, ws), w.bo, bias_vec);
     att = Ciphertext();
     stage("SelfOutput");
-    Ciphertext b1 = bootstrap_segment(ev, boot, so, cfg.members, cfg.boot_batch);
-    so = Ciphertext();
+    Ciphertext b1 = bootstrap_segment(ev, boot, std::move(so), cfg.members, cfg.boot_batch);
     stage("1st Bootstrapping");
 
     // ---- LayerNorm1 on SelfOutput + X
@@ -280,8 +294,7 @@ Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot,
     Ciphertext ln1 = layernorm(ev, std::move(res1), w.ln1_gamma, w.ln1_beta, cfg.ln_newt, cfg.ln_gold,
                                cfg.ln_var_scale);
     stage("LayerNorm1");
-    Ciphertext H1 = bootstrap_segment(ev, boot, ln1, cfg.members, cfg.boot_batch);
-    ln1 = Ciphertext();
+    Ciphertext H1 = bootstrap_segment(ev, boot, std::move(ln1), cfg.members, cfg.boot_batch);
     stage("2nd Bootstrapping");
 
     // ---- Intermediate + GELU in column chunks (each chunk's GELU working set stays bounded)
@@ -318,8 +331,7 @@ Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot,
                                      w.bf, bias_vec);
     G = Ciphertext();
     stage("Final Linear");
-    Ciphertext b3 = bootstrap_segment(ev, boot, fin, cfg.members, cfg.boot_batch);
-    fin = Ciphertext();
+    Ciphertext b3 = bootstrap_segment(ev, boot, std::move(fin), cfg.members, cfg.boot_batch);
     stage("3rd Bootstrapping");
 
     // ---- LayerNorm2 on Final + H1
@@ -329,7 +341,7 @@ Ciphertext bert_layer_stages(const Evaluator &ev, const BatchBootstrapper &boot,
     Ciphertext ln2 = layernorm(ev, std::move(res2), w.ln2_gamma, w.ln2_beta, cfg.ln_newt, cfg.ln_gold,
                                cfg.ln_var_scale);
     stage("LayerNorm2");
-    Ciphertext out = bootstrap_segment(ev, boot, ln2, cfg.members, cfg.boot_batch);
+    Ciphertext out = bootstrap_segment(ev, boot, std::move(ln2), cfg.members, cfg.boot_batch);
     stage("4th Bootstrapping");
     (void)top;
     return out;

@@ -10,7 +10,10 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n_in,n_out,wbits", [(8, 4, 36), (200, 300, 39), (64, 256, 20), (130, 17, 39)])
+# K up to 768 runs the persistent kernel (X tile resident in shared memory); 800 inputs (K padded
+# to 832) the tile-per-CTA kernel
+@pytest.mark.parametrize("n_in,n_out,wbits", [(8, 4, 36), (200, 300, 39), (64, 256, 20), (130, 17, 39),
+                                              (768, 130, 30), (800, 40, 30)])
 def test_tc_matches_cuda_core_and_oracle(n_in, n_out, wbits):
     import ctypes
 
