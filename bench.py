@@ -842,7 +842,7 @@ def cpu_gelu_sample():
 # primes where the bootstrap region starts, so every rescale after a bootstrap is by a 46-bit prime
 LAYER_BITS = [51] + [46] * 23 + [51] * 11 + [51] * 5
 LAYER = dict(hidden=768, heads=12, ffn=3072, num_X=256, tokens=128, input_num=128, softmax_iter=13, ln_newt=3,
-             ln_gold=2, gelu_input_level=13, ffn_chunk=128, boot_batch=8, w_scale=2.0 ** 40, ln_var_scale=64.0)
+             ln_gold=2, gelu_input_level=13, ffn_chunk=128, boot_batch=16, w_scale=2.0 ** 40, ln_var_scale=64.0)
 LAYER_METRIC = "BERT-base layer amortized seconds per input (256 inputs x 128 tokens, hidden 768, 12 heads, FFN 3072)"
 
 
@@ -928,6 +928,7 @@ def run_layer(args, rank, world, dist):
                                + ("shared-a bootstrap segments, groups of %d" % S if S else
                                   "one ordinary bootstrap per ciphertext") + ")",
                    "form": "sham" if S else "orig", "N": h.n, "Q": "[51]+23x[46]+11x[51]", "P": "5x[51]",
+                   "bootstrap_call_batch": cfg["boot_batch"],
                    "inputs": n_in, "tokens": cfg["tokens"], "hidden": cfg["hidden"], "heads": cfg["heads"],
                    "ffn": cfg["ffn"], "stage_seconds": stages, "total_seconds": round(ms / 1000.0, 2),
                    "setup_seconds": round(setup_s, 1),

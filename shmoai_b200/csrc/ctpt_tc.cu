@@ -330,14 +330,15 @@ __global__ void __launch_bounds__(kThreads, 2) mma_kernel(const int8_t *__restri
 // the weight tiles (A, 128 outputs x 64 K bytes) stream through a kAStages ring, and the
 // accumulators alternate between two 256-column TMEM buffers so that the epilogue of one output
 // tile overlaps the MMAs of the next.  One CTA per SM (all 512 TMEM columns), persistent over
-// the (modulus, column tile) pairs.  Roles: warps 0-3 copy (cp.async; the X tile, then the A
-// stages, each group's barrier arrived once the next group is issued), one thread of warp 4
+// the (modulus, column tile) pairs.  Roles: warps 0-3 copy (cp.async; the X tile together, then
+// the A stages, warp w filling ring slot w and arriving on its barrier once its copies land, the
+// next X tile prefetched into L2 meanwhile), one thread of warp 4
 // issues the MMAs, warps 5-12 read the accumulators back (two warps per 32-lane quarter, one
 // per half of the columns).  Every wait is bounded; after a timeout a role waits no more and
 // carries on without its work, still arriving on its barriers, so the other roles finish too,
 // and the call reports the failure through *err.
 constexpr uint32_t kResKp = 768;
-constexpr int kAStages = 3;
+constexpr int kAStages = 4;  // one ring slot per producer warp
 constexpr uint32_t kXBlock = kBN * kKB;  // 16 KB
 constexpr uint32_t kSmemP = (kResKp / kKB) * kXBlock + kAStages * kStageA + 1024;
 constexpr uint32_t kEpiWarp0 = 5;
@@ -365,7 +366,7 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
     }
     if (tid == 0) {
         for (int s = 0; s < kAStages; s++) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full[s])), "r"(kProducers));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;\n" ::"r"(smem_u32(&full[s])));  // its producer warp
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
         }
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&x_full)), "r"(kProducers));
@@ -385,22 +386,16 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
     auto arrive = [](uint32_t bar) { asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar)); };
 
     if (tid < kProducers) {
+        // producer warp w fills ring slot w (A stages w, w + 4, ...): each warp waits for its own
+        // copies only, so four stages are in flight; all four copy the X tile together
         bool ok = true;
-        uint64_t g = 0;         // A stages issued so far (ring position)
-        uint32_t ti = 0;        // column tiles of this CTA so far
-        uint32_t pending = 0;   // barrier of the last committed group, arrived once the next is issued
+        uint64_t g = 0;   // A stages so far (ring position)
+        uint32_t ti = 0;  // column tiles of this CTA so far
         const uint32_t kx16 = Kp / 16;
         for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ti++) {
             const uint32_t t = (uint32_t)(tile / n_ct);
             const uint64_t rbase = (tile % n_ct) * kBN;
-            // every MMA of the previous column tile must have read the X tile: settle the last
-            // A stage first (the MMA thread waits for it), then wait
-            if (pending) {
-                asm volatile("cp.async.wait_group 0;\n");
-                asm volatile("fence.proxy.async.shared::cta;\n");
-                arrive(pending);
-                pending = 0;
-            }
+            // every MMA of the previous column tile must have read the X tile
             if (ok && ti > 0 && !mbar_wait(smem_u32(&x_empty), (ti - 1) & 1)) ok = false;
             const int8_t *B = XP + ((uint64_t)t * chunk + rbase) * Kp;
             if (ok)
@@ -410,31 +405,35 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
                                B + (uint64_t)row * Kp + k16 * 16);
                 }
             asm volatile("cp.async.commit_group;\n");
-            pending = smem_u32(&x_full);
+            asm volatile("cp.async.wait_group 0;\n");
+            asm volatile("fence.proxy.async.shared::cta;\n");
+            arrive(smem_u32(&x_full));
+            // the next column tile's X into L2 while this one's MMAs run
+            const uint64_t next = tile + gridDim.x;
+            if (next < n_tiles) {
+                const int8_t *Bn = XP + ((uint64_t)(next / n_ct) * chunk + (next % n_ct) * kBN) * Kp;
+                for (uint32_t off = tid * 128; off < kBN * Kp; off += kProducers * 128)
+                    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(Bn + off));
+            }
             for (uint32_t o = 0; o < n_ot; o++) {
                 const int8_t *A = WP + ((uint64_t)t * Np + o * kBM) * Kp;
                 for (uint32_t kb = 0; kb < nkb; kb++, g++) {
                     const uint32_t s = (uint32_t)(g % kAStages);
+                    if (s != warp) continue;
                     if (ok && g >= (uint64_t)kAStages && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((g / kAStages) - 1) & 1))
                         ok = false;
                     if (ok)
-                        for (uint32_t c = tid; c < kBM * (kKB / 16); c += kProducers) {
+                        for (uint32_t c = lane; c < kBM * (kKB / 16); c += 32) {
                             const uint32_t row = c / (kKB / 16), kc = c % (kKB / 16);
                             cp_async16(smem_u32(sA + s * kStageA) + core_off(row, kc),
                                        A + (uint64_t)row * Kp + (uint64_t)kb * kKB + kc * 16);
                         }
                     asm volatile("cp.async.commit_group;\n");
-                    asm volatile("cp.async.wait_group 1;\n");  // the previous group has landed
+                    asm volatile("cp.async.wait_group 0;\n");
                     asm volatile("fence.proxy.async.shared::cta;\n");
-                    arrive(pending);
-                    pending = smem_u32(&full[s]);
+                    arrive(smem_u32(&full[s]));
                 }
             }
-        }
-        if (pending) {
-            asm volatile("cp.async.wait_group 0;\n");
-            asm volatile("fence.proxy.async.shared::cta;\n");
-            arrive(pending);
         }
         if (!ok) failed = 1;
     } else if (tid == kProducers) {
@@ -540,7 +539,7 @@ struct CrtLimb {
 
 // one thread folds 4 consecutive columns r (one limb, 4 | N): 4-byte residue loads and
 // two 16-byte stores instead of byte loads and 8-byte stores
-__global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict__ Y, const CrtLimb *__restrict__ tab,
+__global__ void __launch_bounds__(256, 4) crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict__ Y, const CrtLimb *__restrict__ tab,
                            uint32_t n_out, uint64_t chunk, uint64_t r0, uint64_t R, uint32_t L, uint32_t log_n,
                            const PrimeConst *__restrict__ pc, uint32_t T) {
     const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
@@ -549,37 +548,40 @@ __global__ void crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict
     const uint64_t rg = r0 + r;
     const uint32_t limb = (uint32_t)((rg >> log_n) % L);
     const CrtLimb &cl = tab[limb];
-    uint32_t res[kMaxMods];
-#pragma unroll
-    for (uint32_t t = 0; t < kMaxMods; t++)  // all loads in flight before any use
-        res[t] = t < T ? *reinterpret_cast<const uint32_t *>(RES + ((uint64_t)t * n_out + o) * chunk + r) : 0u;
     const PrimeConst p = pc[limb];
-    uint64_t y[4];
     const double two52 = 4503599627370496.0;
+    // sum_t r_t c_t from the 32-bit halves of c_t (r_t < 2^8): the low products on the integer
+    // pipe (64-bit sums below 2^45), the high ones on the FP64 pipe (each below 2^37, their sum
+    // below 2^42: exact in a double); v = round(sum_t r_t frac_t) on the FP64 pipe, off by far less
+    // than the CRT margin of 1/8.  The FP64 values are read back from their mantissas (2^52 added:
+    // exact integers below 2^52).  Moduli outer, the four columns inner: one 4-byte residue load
+    // per modulus.
+    uint64_t lo[4] = {0, 0, 0, 0};
+    double hi[4] = {0.0, 0.0, 0.0, 0.0}, v[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-        // sum_t r_t c_t from the 32-bit halves of c_t (r_t < 2^8): the low products on the integer
-        // pipe (64-bit sum below 2^45), the high ones on the FP64 pipe (each below 2^37, their sum
-        // below 2^42: exact in a double); v = round(sum_t r_t frac_t) on the FP64 pipe, off by far
-        // less than the CRT margin of 1/8.  The FP64 values are read back from their mantissas
-        // (2^52 added: exact integers below 2^52).
-        uint64_t lo = 0;
-        double hi = 0.0, v = 0.0;
+    for (uint32_t t = 0; t < kMaxMods; t++) {
+        if (t < T) {
+            const uint32_t r4 = *reinterpret_cast<const uint32_t *>(RES + ((uint64_t)t * n_out + o) * chunk + r);
+            const uint32_t c32 = (uint32_t)cl.c[t];
+            const double ch = cl.chd[t], fr = c_mods.fracd[T][t];
 #pragma unroll
-        for (uint32_t t = 0; t < kMaxMods; t++) {
-            if (t < T) {
-                const uint32_t rt = (res[t] >> (8 * e)) & 0xFF;
-                lo += (uint64_t)rt * (uint32_t)cl.c[t];
+            for (int e = 0; e < 4; e++) {
+                const uint32_t rt = (r4 >> (8 * e)) & 0xFF;
+                lo[e] += (uint64_t)rt * c32;
                 const double rd = __dsub_rn(__hiloint2double(0x43300000, (int)rt), two52);
-                hi = __fma_rn(rd, cl.chd[t], hi);
-                v = __fma_rn(rd, c_mods.fracd[T][t], v);
+                hi[e] = __fma_rn(rd, ch, hi[e]);
+                v[e] = __fma_rn(rd, fr, v[e]);
             }
         }
+    }
+    uint64_t y[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
         const uint64_t mant = 0x000FFFFFFFFFFFFFull;
-        const uint64_t hii = (uint64_t)__double_as_longlong(__dadd_rn(hi, two52)) & mant;
-        const uint64_t vi = (uint64_t)__double_as_longlong(__dadd_rn(v, two52)) & mant;
-        const uint64_t plo = lo + (hii << 32);
-        const u128 pos = {plo, (hii >> 32) + (plo < lo ? 1ull : 0ull)};
+        const uint64_t hii = (uint64_t)__double_as_longlong(__dadd_rn(hi[e], two52)) & mant;
+        const uint64_t vi = (uint64_t)__double_as_longlong(__dadd_rn(v[e], two52)) & mant;
+        const uint64_t plo = lo[e] + (hii << 32);
+        const u128 pos = {plo, (hii >> 32) + (plo < lo[e] ? 1ull : 0ull)};
         y[e] = sub_mod(barrett(pos, p), barrett(mul_wide(vi, cl.M), p), p.q);
     }
     ulonglong2 *out = reinterpret_cast<ulonglong2 *>(Y + (uint64_t)o * R + rg);
