@@ -19,7 +19,11 @@
 // K in 64-byte stages (4-stage cp.async ring, one mbarrier per stage), s32
 // accumulator in TMEM (256 columns) -> epilogue tcgen05.ld, acc mod m_t -> uint8
 // residue planes -> CRT kernel.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "core.hpp"
@@ -88,9 +92,24 @@ __device__ __forceinline__ uint32_t mod_acc(int a, uint32_t t) {
     return mod_small(x, t);
 }
 
+// The balanced residue of x mod m_t (in (-m/2, m/2), m odd) on the FP64 pipe, for x < 2^51 given
+// as the exact double xd: q = round(x / m) from fma(xd, 1/m, 1.5 2^52) (the pre-rounding value is
+// within (x / m) 2^-53 < 0.25 / m of x / m, and x / m lies at least 0.5 / m from a half-integer,
+// so q is the nearest integer), then x - q m exactly by a second fma.  The result is returned as
+// the low byte of the mantissa of r + 1.5 2^52 (|r| < 2^51: two's complement of r mod 256).
+__device__ __forceinline__ uint32_t balanced_f64(double xd, uint32_t t) {
+    const double magic = 6755399441055744.0;  // 1.5 * 2^52
+    const double q = __dsub_rn(__fma_rn(xd, c_mods.inv[t], magic), magic);
+    const double r = __fma_rn(-q, (double)c_mods.m[t], xd);
+    return (uint32_t)__double2loint(__dadd_rn(r, magic)) & 0xFF;
+}
+
 // X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via a 64 x 64 shared-memory transpose.  Each
 // thread writes four consecutive inputs' residues of one column as one 32-bit word, so a warp's
-// store covers 64 contiguous bytes of each of two columns for every modulus.
+// store covers 64 contiguous bytes of each of two columns for every modulus.  F64 (every limb
+// prime below 2^51): the residues on the FP64 pipe (balanced_f64), else in 32-bit integer
+// arithmetic (mod_small).
+template <bool F64>
 __global__ void __launch_bounds__(256, 4) xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__ XP, uint32_t n_in, uint32_t Kp,
                             uint64_t R, uint64_t r0, uint32_t T) {
     __shared__ uint64_t tile[64][65];
@@ -110,11 +129,26 @@ __global__ void __launch_bounds__(256, 4) xres_kernel(const uint64_t *__restrict
         uint64_t x[4];
 #pragma unroll
         for (uint32_t j = 0; j < 4; j++) x[j] = tile[4 * kq + j][col];
-        for (uint32_t t = 0; t < T; t++) {
-            uint32_t w = 0;
+        if constexpr (F64) {
+            const double two52 = 4503599627370496.0;
+            double xd[4];
 #pragma unroll
-            for (uint32_t j = 0; j < 4; j++) w |= (uint32_t)(uint8_t)balanced(mod_small(x[j], t), c_mods.m[t]) << (8 * j);
-            *reinterpret_cast<uint32_t *>(XP + ((uint64_t)t * chunk + rb + col) * Kp + i0 + 4 * kq) = w;
+            for (uint32_t j = 0; j < 4; j++)  // exact: x < 2^51
+                xd[j] = __dsub_rn(__longlong_as_double((long long)(0x4330000000000000ull | x[j])), two52);
+            for (uint32_t t = 0; t < T; t++) {
+                uint32_t w = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < 4; j++) w |= balanced_f64(xd[j], t) << (8 * j);
+                *reinterpret_cast<uint32_t *>(XP + ((uint64_t)t * chunk + rb + col) * Kp + i0 + 4 * kq) = w;
+            }
+        } else {
+            for (uint32_t t = 0; t < T; t++) {
+                uint32_t w = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < 4; j++)
+                    w |= (uint32_t)(uint8_t)balanced(mod_small(x[j], t), c_mods.m[t]) << (8 * j);
+                *reinterpret_cast<uint32_t *>(XP + ((uint64_t)t * chunk + rb + col) * Kp + i0 + 4 * kq) = w;
+            }
         }
     }
 }
@@ -146,6 +180,18 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     d |= (uint64_t)((kKB / 16 * 128) >> 4) << 32;  // stride byte offset (M/N direction)
     d |= (uint64_t)1 << 46;                      // descriptor version for sm_100
     return d;                                    // base offset 0, lbo mode 0, layout SWIZZLE_NONE
+}
+
+// K-major operand written by TMA with the 64-byte swizzle (rows of kKB = 64 bytes, 8-row groups
+// 512 bytes apart); the MMA over K bytes [32 k, 32 k + 32) starts 32 k bytes into the atom
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;           // leading byte offset: unused within one swizzle atom
+    d |= (uint64_t)(512 >> 4) << 32;  // stride byte offset: 8 rows x 64 bytes
+    d |= (uint64_t)1 << 46;           // descriptor version for sm_100
+    d |= (uint64_t)4 << 61;           // layout: SWIZZLE_64B
+    return d;
 }
 
 // byte offset of (row, k-chunk) inside one stage operand of `rows` x kKB bytes
@@ -344,12 +390,17 @@ constexpr uint32_t kSmemP = (kResKp / kKB) * kXBlock + kAStages * kStageA + 1024
 constexpr uint32_t kEpiWarp0 = 5;
 constexpr uint32_t kThreadsP = (kEpiWarp0 + 8) * 32;
 
+// TMA_A: the weight tiles come by TMA (one thread, 64-byte swizzle, completion on the stage's
+// mbarrier) instead of the producer warps' cp.async
+template <bool TMA_A>
 __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8_t *__restrict__ XP,
                                                                       const int8_t *__restrict__ WP,
                                                                       uint8_t *__restrict__ RES, uint32_t Kp,
                                                                       uint32_t Np, uint32_t n_out, uint64_t chunk,
-                                                                      uint32_t T, int *__restrict__ err, int acc24) {
-    extern __shared__ __align__(1024) uint8_t smem[];
+                                                                      uint32_t T, int *__restrict__ err, int acc24,
+                                                                      const __grid_constant__ CUtensorMap tmA) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // swizzle atoms need 1 KB alignment
     __shared__ __align__(8) uint64_t full[kAStages], empty[kAStages], x_full, x_empty, acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_base;
     __shared__ int failed;
@@ -366,7 +417,8 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
     }
     if (tid == 0) {
         for (int s = 0; s < kAStages; s++) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;\n" ::"r"(smem_u32(&full[s])));  // its producer warp
+            // the TMA issuer's expect-tx arrival, or the 32 threads of the slot's producer warp
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full[s])), "r"(TMA_A ? 1 : 32));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
         }
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&x_full)), "r"(kProducers));
@@ -419,6 +471,26 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
                 const int8_t *A = WP + ((uint64_t)t * Np + o * kBM) * Kp;
                 for (uint32_t kb = 0; kb < nkb; kb++, g++) {
                     const uint32_t s = (uint32_t)(g % kAStages);
+                    if constexpr (TMA_A) {
+                        if (tid != 0) continue;
+                        if (ok && g >= (uint64_t)kAStages && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((g / kAStages) - 1) & 1))
+                            ok = false;
+                        const uint32_t bar = smem_u32(&full[s]);
+                        if (ok) {
+                            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
+                                         "r"(kStageA));
+                            // x = kb * 64 bytes: 16-byte aligned as a tiled TMA load requires
+                            asm volatile(
+                                "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                                "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(smem_u32(sA + s * kStageA)),
+                                "l"(reinterpret_cast<uint64_t>(&tmA)), "r"((int)(kb * kKB)),
+                                "r"((int)(t * Np + o * kBM)), "r"(bar)
+                                : "memory");
+                        } else {
+                            arrive(bar);  // no copy: the barrier still completes
+                        }
+                        continue;
+                    }
                     if (s != warp) continue;
                     if (ok && g >= (uint64_t)kAStages && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((g / kAStages) - 1) & 1))
                         ok = false;
@@ -455,7 +527,8 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
                         const uint32_t a0 = smem_u32(sA + s * kStageA), b0 = smem_u32(sX + kb * kXBlock);
 #pragma unroll
                         for (uint32_t k = 0; k < kKB / 32; k++) {
-                            const uint64_t ad = smem_desc(a0 + k * 256), bd = smem_desc(b0 + k * 256);
+                            const uint64_t ad = TMA_A ? smem_desc_sw64(a0 + k * 32) : smem_desc(a0 + k * 256);
+                            const uint64_t bd = smem_desc(b0 + k * 256);
                             const uint32_t accum = (kb | k) ? 1u : 0u;
                             asm volatile(
                                 "{\n\t.reg .pred p;\n\t"
@@ -539,7 +612,7 @@ struct CrtLimb {
 
 // one thread folds 4 consecutive columns r (one limb, 4 | N): 4-byte residue loads and
 // two 16-byte stores instead of byte loads and 8-byte stores
-__global__ void __launch_bounds__(256, 4) crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict__ Y, const CrtLimb *__restrict__ tab,
+__global__ void __launch_bounds__(256, 3) crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict__ Y, const CrtLimb *__restrict__ tab,
                            uint32_t n_out, uint64_t chunk, uint64_t r0, uint64_t R, uint32_t L, uint32_t log_n,
                            const PrimeConst *__restrict__ pc, uint32_t T) {
     const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
@@ -554,14 +627,21 @@ __global__ void __launch_bounds__(256, 4) crt_kernel(const uint8_t *__restrict__
     // pipe (64-bit sums below 2^45), the high ones on the FP64 pipe (each below 2^37, their sum
     // below 2^42: exact in a double); v = round(sum_t r_t frac_t) on the FP64 pipe, off by far less
     // than the CRT margin of 1/8.  The FP64 values are read back from their mantissas (2^52 added:
-    // exact integers below 2^52).  Moduli outer, the four columns inner: one 4-byte residue load
-    // per modulus.
+    // exact integers below 2^52).  Moduli outer, the four columns inner; the residues (one 4-byte
+    // word per modulus, read once: streaming loads) requested before the fold.
+    constexpr uint32_t kAhead = 14;  // residue words requested before the fold (T <= 14 at the usual weight sizes)
+    uint32_t res[kAhead];
+#pragma unroll
+    for (uint32_t t = 0; t < kAhead; t++)
+        res[t] = t < T ? __ldcs(reinterpret_cast<const uint32_t *>(RES + ((uint64_t)t * n_out + o) * chunk + r)) : 0u;
     uint64_t lo[4] = {0, 0, 0, 0};
     double hi[4] = {0.0, 0.0, 0.0, 0.0}, v[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (uint32_t t = 0; t < kMaxMods; t++) {
         if (t < T) {
-            const uint32_t r4 = *reinterpret_cast<const uint32_t *>(RES + ((uint64_t)t * n_out + o) * chunk + r);
+            const uint32_t r4 =
+                t < kAhead ? res[t]
+                           : __ldcs(reinterpret_cast<const uint32_t *>(RES + ((uint64_t)t * n_out + o) * chunk + r));
             const uint32_t c32 = (uint32_t)cl.c[t];
             const double ch = cl.chd[t], fr = c_mods.fracd[T][t];
 #pragma unroll
@@ -660,6 +740,30 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
 
 }  // namespace
 
+// The weight planes WP [T * Np][Kp] as a 2D tensor map for TMA: 64-byte K boxes of 128 rows with the
+// 64-byte swizzle.  False when the driver's encoder is unavailable or refuses, or when the
+// environment sets SHMOAI_CTPT_TMA=0 (then the producer warps copy the weight tiles with cp.async).
+bool weight_tensor_map(CUtensorMap *map, const int8_t *WP, uint32_t Kp, uint64_t rows) {
+    static PFN_cuTensorMapEncodeTiled encode = [] {
+        const char *off = std::getenv("SHMOAI_CTPT_TMA");
+        if (off && off[0] == '0') return (PFN_cuTensorMapEncodeTiled) nullptr;
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        cudaGetLastError();
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+    }();
+    if (!encode) return false;
+    const cuuint64_t dims[2] = {Kp, rows}, strides[1] = {Kp};
+    const cuuint32_t box[2] = {kKB, kBM}, estr[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t *>(WP), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // columns of X processed per pass (bounds the residue workspaces)
 constexpr uint64_t kChunkCols = 131072;
 
@@ -699,25 +803,39 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     wres_kernel<<<dim3((Kp + 255) / 256, Np), 256, 0, st>>>(W, WP, n_in, n_out, Kp, Np, T);
     SHM_CUDA(cudaGetLastError());
     const bool resident = Kp <= kResKp;  // the X tile fits in shared memory: the persistent kernel
+    CUtensorMap tmA;
+    std::memset(&tmA, 0, sizeof tmA);
+    const bool tma_a = resident && weight_tensor_map(&tmA, WP, Kp, (uint64_t)T * Np);
     if (resident)
-        SHM_CUDA(cudaFuncSetAttribute(mma_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemP));
+        SHM_CUDA(cudaFuncSetAttribute(tma_a ? mma_persistent_kernel<true> : mma_persistent_kernel<false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemP));
     else
         SHM_CUDA(cudaFuncSetAttribute(mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
     int sms = 0;
     SHM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
     const int acc24 = (uint64_t)Kp * 125 * 125 < (1ull << 24) ? 1 : 0;  // accumulators exact in float
+    bool f64_res = true;  // every limb prime below 2^51: the X residues on the FP64 pipe
+    for (uint32_t l = 0; l < L; l++) f64_res = f64_res && c.primes[l] < (1ull << 51);
     for (uint64_t r0 = 0; r0 < R; r0 += chunk) {
         // a shorter last pass (2 L N not a multiple of the chunk, e.g. at N = 2^12) lays its planes out
         // with its own column count; every count here is a multiple of 256
         const uint64_t cur = std::min<uint64_t>(chunk, R - r0);
         SHM_LAUNCHED(1);
-        xres_kernel<<<dim3((uint32_t)(cur / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0, T);
+        if (f64_res)
+            xres_kernel<true><<<dim3((uint32_t)(cur / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0, T);
+        else
+            xres_kernel<false><<<dim3((uint32_t)(cur / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0, T);
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
         if (resident) {
             const uint64_t tiles = (uint64_t)T * (cur / kBN);
             const uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sms);
-            mma_persistent_kernel<<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24);
+            if (tma_a)
+                mma_persistent_kernel<true>
+                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24, tmA);
+            else
+                mma_persistent_kernel<false>
+                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24, tmA);
         } else {
             mma_kernel<<<dim3(Np / kBM, (uint32_t)(cur / kBN), T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
                                                                                          cur, err, acc24);
