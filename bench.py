@@ -517,7 +517,7 @@ def cpu_boot_sample(shared: int = 0):
 # the same jobs executed one after the other on the plain per-ciphertext path
 
 SERVE = dict(n_jobs=200, rate=3.0, seed=5, p_rot=0.65, p_mm=0.15, members=8, boot_batch=32, mm_n=192, mm_L=13,
-             rot_steps=(1, 2, 4, 8), rot_max=32, rot_levels=(4, 24), slots=3, budget_gb=64)
+             rot_steps=(1, 2, 4, 8), rot_max=32, rot_levels=(4, 24), slots=3, budget_gb=72)
 
 
 def serve_jobs(rng):
