@@ -390,15 +390,16 @@ constexpr uint32_t kSmemP = (kResKp / kKB) * kXBlock + kAStages * kStageA + 1024
 constexpr uint32_t kEpiWarp0 = 5;
 constexpr uint32_t kThreadsP = (kEpiWarp0 + 8) * 32;
 
-// TMA_A: the weight tiles come by TMA (one thread, 64-byte swizzle, completion on the stage's
-// mbarrier) instead of the producer warps' cp.async
+// TMA_A: both operands come by TMA (one thread issues the X tile's and the weight stages' loads,
+// 64-byte swizzle, completion on their mbarriers) instead of the producer warps' cp.async
 template <bool TMA_A>
 __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8_t *__restrict__ XP,
                                                                       const int8_t *__restrict__ WP,
                                                                       uint8_t *__restrict__ RES, uint32_t Kp,
                                                                       uint32_t Np, uint32_t n_out, uint64_t chunk,
                                                                       uint32_t T, int *__restrict__ err, int acc24,
-                                                                      const __grid_constant__ CUtensorMap tmA) {
+                                                                      const __grid_constant__ CUtensorMap tmA,
+                                                                      const __grid_constant__ CUtensorMap tmX) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // swizzle atoms need 1 KB alignment
     __shared__ __align__(8) uint64_t full[kAStages], empty[kAStages], x_full, x_empty, acc_full[2], acc_empty[2];
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full[s])), "r"(TMA_A ? 1 : 32));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
         }
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&x_full)), "r"(kProducers));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&x_full)), "r"(TMA_A ? 1 : kProducers));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&x_empty)));
         for (int b = 0; b < 2; b++) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&acc_full[b])));
@@ -437,9 +438,11 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
     const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((kBN >> 3) << 17) | ((kBM >> 4) << 24);
     auto arrive = [](uint32_t bar) { asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar)); };
 
-    if (tid < kProducers) {
-        // producer warp w fills ring slot w (A stages w, w + 4, ...): each warp waits for its own
-        // copies only, so four stages are in flight; all four copy the X tile together
+    if (tid < kProducers && !(TMA_A && warp > 0)) {
+        // cp.async: producer warp w fills ring slot w (A stages w, w + 4, ...): each warp waits for
+        // its own copies only, so four stages are in flight; all four copy the X tile together.
+        // TMA: thread 0 issues every load (the X tile as Kp / 64 boxes of 256 rows, then the A
+        // stages), its warp prefetches the next X tile into L2
         bool ok = true;
         uint64_t g = 0;   // A stages so far (ring position)
         uint32_t ti = 0;  // column tiles of this CTA so far
@@ -447,24 +450,47 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
         for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ti++) {
             const uint32_t t = (uint32_t)(tile / n_ct);
             const uint64_t rbase = (tile % n_ct) * kBN;
-            // every MMA of the previous column tile must have read the X tile
-            if (ok && ti > 0 && !mbar_wait(smem_u32(&x_empty), (ti - 1) & 1)) ok = false;
-            const int8_t *B = XP + ((uint64_t)t * chunk + rbase) * Kp;
-            if (ok)
-                for (uint32_t c = tid; c < kBN * kx16; c += kProducers) {
-                    const uint32_t row = c / kx16, k16 = c % kx16;
-                    cp_async16(smem_u32(sX + (k16 >> 2) * kXBlock) + core_off(row, k16 & 3),
-                               B + (uint64_t)row * Kp + k16 * 16);
+            if constexpr (TMA_A) {
+                if (tid == 0) {
+                    // every MMA of the previous column tile must have read the X tile
+                    if (ok && ti > 0 && !mbar_wait(smem_u32(&x_empty), (ti - 1) & 1)) ok = false;
+                    const uint32_t bar = smem_u32(&x_full);
+                    if (ok) {
+                        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
+                                     "r"(kBN * Kp));
+                        for (uint32_t kb = 0; kb < nkb; kb++)  // x = kb * 64 bytes: 16-byte aligned
+                            asm volatile(
+                                "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                                "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(smem_u32(sX + kb * kXBlock)),
+                                "l"(reinterpret_cast<uint64_t>(&tmX)), "r"((int)(kb * kKB)),
+                                "r"((int)((uint64_t)t * chunk + rbase)), "r"(bar)
+                                : "memory");
+                    } else {
+                        arrive(bar);
+                    }
                 }
-            asm volatile("cp.async.commit_group;\n");
-            asm volatile("cp.async.wait_group 0;\n");
-            asm volatile("fence.proxy.async.shared::cta;\n");
-            arrive(smem_u32(&x_full));
+                __syncwarp();
+            } else {
+                // every MMA of the previous column tile must have read the X tile
+                if (ok && ti > 0 && !mbar_wait(smem_u32(&x_empty), (ti - 1) & 1)) ok = false;
+                const int8_t *B = XP + ((uint64_t)t * chunk + rbase) * Kp;
+                if (ok)
+                    for (uint32_t c = tid; c < kBN * kx16; c += kProducers) {
+                        const uint32_t row = c / kx16, k16 = c % kx16;
+                        cp_async16(smem_u32(sX + (k16 >> 2) * kXBlock) + core_off(row, k16 & 3),
+                                   B + (uint64_t)row * Kp + k16 * 16);
+                    }
+                asm volatile("cp.async.commit_group;\n");
+                asm volatile("cp.async.wait_group 0;\n");
+                asm volatile("fence.proxy.async.shared::cta;\n");
+                arrive(smem_u32(&x_full));
+            }
             // the next column tile's X into L2 while this one's MMAs run
             const uint64_t next = tile + gridDim.x;
             if (next < n_tiles) {
                 const int8_t *Bn = XP + ((uint64_t)(next / n_ct) * chunk + (next % n_ct) * kBN) * Kp;
-                for (uint32_t off = tid * 128; off < kBN * Kp; off += kProducers * 128)
+                const uint32_t nthr = TMA_A ? 32 : kProducers;
+                for (uint32_t off = tid * 128; off < kBN * Kp; off += nthr * 128)
                     asm volatile("prefetch.global.L2 [%0];\n" ::"l"(Bn + off));
             }
             for (uint32_t o = 0; o < n_ot; o++) {
@@ -528,7 +554,7 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
 #pragma unroll
                         for (uint32_t k = 0; k < kKB / 32; k++) {
                             const uint64_t ad = TMA_A ? smem_desc_sw64(a0 + k * 32) : smem_desc(a0 + k * 256);
-                            const uint64_t bd = smem_desc(b0 + k * 256);
+                            const uint64_t bd = TMA_A ? smem_desc_sw64(b0 + k * 32) : smem_desc(b0 + k * 256);
                             const uint32_t accum = (kb | k) ? 1u : 0u;
                             asm volatile(
                                 "{\n\t.reg .pred p;\n\t"
@@ -740,10 +766,11 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
 
 }  // namespace
 
-// The weight planes WP [T * Np][Kp] as a 2D tensor map for TMA: 64-byte K boxes of 128 rows with the
-// 64-byte swizzle.  False when the driver's encoder is unavailable or refuses, or when the
-// environment sets SHMOAI_CTPT_TMA=0 (then the producer warps copy the weight tiles with cp.async).
-bool weight_tensor_map(CUtensorMap *map, const int8_t *WP, uint32_t Kp, uint64_t rows) {
+// Residue planes [rows][Kp] (the weights' or X's) as a 2D tensor map for TMA: 64-byte K boxes of
+// box_rows rows with the 64-byte swizzle.  False when the driver's encoder is unavailable or
+// refuses, or when the environment sets SHMOAI_CTPT_TMA=0 (then the producer warps copy the
+// operand tiles with cp.async).
+bool operand_tensor_map(CUtensorMap *map, const int8_t *P, uint32_t Kp, uint64_t rows, uint32_t box_rows) {
     static PFN_cuTensorMapEncodeTiled encode = [] {
         const char *off = std::getenv("SHMOAI_CTPT_TMA");
         if (off && off[0] == '0') return (PFN_cuTensorMapEncodeTiled) nullptr;
@@ -758,8 +785,8 @@ bool weight_tensor_map(CUtensorMap *map, const int8_t *WP, uint32_t Kp, uint64_t
     }();
     if (!encode) return false;
     const cuuint64_t dims[2] = {Kp, rows}, strides[1] = {Kp};
-    const cuuint32_t box[2] = {kKB, kBM}, estr[2] = {1, 1};
-    return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t *>(WP), dims, strides, box, estr,
+    const cuuint32_t box[2] = {kKB, box_rows}, estr[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t *>(P), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -803,9 +830,10 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     wres_kernel<<<dim3((Kp + 255) / 256, Np), 256, 0, st>>>(W, WP, n_in, n_out, Kp, Np, T);
     SHM_CUDA(cudaGetLastError());
     const bool resident = Kp <= kResKp;  // the X tile fits in shared memory: the persistent kernel
-    CUtensorMap tmA;
+    CUtensorMap tmA, tmX;
     std::memset(&tmA, 0, sizeof tmA);
-    const bool tma_a = resident && weight_tensor_map(&tmA, WP, Kp, (uint64_t)T * Np);
+    std::memset(&tmX, 0, sizeof tmX);
+    const bool tma_a = resident && operand_tensor_map(&tmA, WP, Kp, (uint64_t)T * Np, kBM);
     if (resident)
         SHM_CUDA(cudaFuncSetAttribute(tma_a ? mma_persistent_kernel<true> : mma_persistent_kernel<false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemP));
@@ -830,12 +858,15 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
         if (resident) {
             const uint64_t tiles = (uint64_t)T * (cur / kBN);
             const uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sms);
-            if (tma_a)
+            // the X planes of this pass, [T * cur][Kp], as 256-row boxes (a pass's planes have its own
+            // column count)
+            const bool tma = tma_a && operand_tensor_map(&tmX, XP, Kp, (uint64_t)T * cur, kBN);
+            if (tma)
                 mma_persistent_kernel<true>
-                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24, tmA);
+                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24, tmA, tmX);
             else
                 mma_persistent_kernel<false>
-                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24, tmA);
+                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24, tmA, tmX);
         } else {
             mma_kernel<<<dim3(Np / kBM, (uint32_t)(cur / kBN), T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
                                                                                          cur, err, acc24);
