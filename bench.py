@@ -38,6 +38,7 @@ library's kernels on the same calls ("reference_gpu", "ours_same_calls").
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import math
 import os
@@ -517,7 +518,7 @@ def cpu_boot_sample(shared: int = 0):
 # the same jobs executed one after the other on the plain per-ciphertext path
 
 SERVE = dict(n_jobs=200, rate=3.0, seed=5, p_rot=0.65, p_mm=0.15, members=8, boot_batch=32, mm_n=192, mm_L=13,
-             rot_steps=(1, 2, 4, 8), rot_max=32, rot_levels=(4, 24), slots=3, budget_gb=72)
+             rot_steps=(1, 2, 4, 8), rot_max=32, rot_levels=(4, 24), slots=3, budget_gb=72, outstanding=24)
 
 
 def serve_jobs(rng):
@@ -585,62 +586,95 @@ def run_serve(args, rank, world, dist):
             return srv.submit_matmul(ct, W, w_scale)
         return srv.submit_bootstrap(ct, arg)
 
+    def digest(arr):
+        return hashlib.blake2b(np.ascontiguousarray(arr).tobytes(), digest_size=16).hexdigest()
+
+    def run_stream(srv, t0=None):
+        """Submit every job (at its Poisson arrival time when t0 is given, else at once) with at most
+        `outstanding` jobs submitted and not yet collected, and collect them in order on another
+        thread: each output is reduced to a digest (rotations, matmuls) or a decryption error
+        (bootstraps) and released at once, so device memory holds only the outstanding jobs."""
+        n = len(jobs)
+        ids, ready = [None] * n, [threading.Event() for _ in range(n)]
+        times, digests, errs, fail = [None] * n, [None] * n, [], []
+        late = [0.0] * n  # how long after its arrival time each job was submitted
+        slots = threading.Semaphore(S["outstanding"])
+
+        def feeder():
+            try:
+                for i, j in enumerate(jobs):
+                    if t0 is not None:
+                        delay = t0 + j[4] - time.perf_counter()
+                        if delay > 0:
+                            time.sleep(delay)
+                    slots.acquire()
+                    if t0 is not None:
+                        late[i] = max(0.0, time.perf_counter() - (t0 + j[4]))
+                    ids[i] = submit(srv, i)
+                    ready[i].set()
+            except Exception as e:  # reported by the main thread
+                fail.append(e)
+                for ev in ready:
+                    ev.set()
+
+        def collector():
+            try:
+                for i in range(n):
+                    ready[i].wait()
+                    if fail:
+                        return
+                    out, t, _ = srv.wait(ids[i])
+                    times[i] = t
+                    if jobs[i][0] == "boot":
+                        errs.append(float(np.abs(h.decrypt(out) - inputs[i][0]).mean()))
+                    else:
+                        digests[i] = digest(out.to_host())
+                    out.close()
+                    slots.release()
+            except Exception as e:
+                fail.append(e)
+
+        th = [threading.Thread(target=feeder), threading.Thread(target=collector)]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        if fail:
+            raise fail[0]
+        return times, digests, errs, late
+
     # warm-up: one job of each kind through a server, then the timed stream
     srv = Server(h, bs, hbm_budget=S["budget_gb"] << 30, slots=S["slots"])
     for kind in ("rot", "mm", "boot"):
         i = next((k for k, j in enumerate(jobs) if j[0] == kind), None)
         if i is not None:
-            srv.wait(submit(srv, i))
+            out, _, _ = srv.wait(submit(srv, i))
+            out.close()
     srv.close()
     srv = Server(h, bs, hbm_budget=S["budget_gb"] << 30, slots=S["slots"])
     resident, _ = h.device_memory(reset_peak=True)
     clk = ClockSampler(dev).start()
-    ids = [None] * len(jobs)
     l0 = lib.shm_kernel_launches()
     t0 = time.perf_counter()
-
-    def feeder():
-        for i, j in enumerate(jobs):
-            delay = t0 + j[4] - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            ids[i] = submit(srv, i)
-
-    th = threading.Thread(target=feeder)
-    th.start()
-    th.join()
-    served = [srv.wait(j) for j in ids]
+    times, results, boot_err, late = run_stream(srv, t0)
     launches = lib.shm_kernel_launches() - l0
     _, peak = h.device_memory()
     stats = srv.stats()
     clocks = clk.summary()
     srv.close()
-    lat = np.array([t[2] - t[0] for _, t, _ in served])
-    span = max(t[2] for _, t, _ in served) - min(t[0] for _, t, _ in served)
-    # results to the host (device memory back for the plain run); bootstraps judged by decryption
-    boot_err, results = [], []
-    for i, (out, _, _) in enumerate(served):
-        if jobs[i][0] == "boot":
-            boot_err.append(float(np.abs(h.decrypt(out) - inputs[i][0]).mean()))
-            results.append(None)
-        else:
-            results.append(out.to_host())
-        out.close()
-    del served
+    # latency from the job's arrival (its scheduled submission) to its completion: the server's own
+    # submit-to-end time plus any delay of the submission past the arrival
+    lat = np.array([t[2] - t[0] + d for t, d in zip(times, late)])
+    span = max(t[2] for t in times) - min(t[0] for t in times)
 
-    # capacity: the same jobs all queued at once (throughput with the slots saturated)
+    # capacity: the same jobs queued as fast as the outstanding limit allows (slots saturated)
     srv = Server(h, bs, hbm_budget=S["budget_gb"] << 30, slots=S["slots"])
-    srv.pause()
-    cap_ids = [submit(srv, i) for i in range(len(jobs))]
-    srv.resume()
-    cap = [srv.wait(j) for j in cap_ids]
-    cap_span = max(t[2] for _, t, _ in cap) - min(t[0] for _, t, _ in cap)
+    cap_times, cap_results, _, _ = run_stream(srv)
+    cap_span = max(t[2] for t in cap_times) - min(t[0] for t in cap_times)
     cap_stats = srv.stats()
-    for i, (out, _, _) in enumerate(cap):
-        if results[i] is not None and not np.array_equal(out.to_host(), results[i]):
+    for i in range(len(jobs)):
+        if results[i] is not None and cap_results[i] != results[i]:
             raise AssertionError(f"serving job {i} differs between the two runs")
-        out.close()
-    del cap
     srv.close()
 
     # serial plain execution on the same GPU: jobs in arrival order, one ciphertext per call,
@@ -659,8 +693,10 @@ def run_serve(args, rank, world, dist):
                 outs.append(h.rotate(one, arg) if kind == "rot" else bs.run(one, 0))
         h.synchronize()
         service.append(time.perf_counter() - t)
-        plain.append(None if kind == "boot" else np.concatenate([o.to_host() for o in outs]))
-        del outs
+        plain.append(None if kind == "boot" else digest(np.concatenate([o.to_host() for o in outs])))
+        for o in outs:
+            o.close()
+        x.close()
     finish, plat = 0.0, []
     for (kind, _, _, _, arr), s in zip(jobs, service):
         finish = max(finish, arr) + s
@@ -670,7 +706,7 @@ def run_serve(args, rank, world, dist):
     same = {"rot": True, "mm": True}
     for i, (kind, *_rest) in enumerate(jobs):
         if kind != "boot":
-            same[kind] = same[kind] and bool(np.array_equal(results[i], plain[i]))
+            same[kind] = same[kind] and results[i] == plain[i]
     n_cts = sum(j[1] for j in jobs)
     kinds = {k: sum(1 for j in jobs if j[0] == k) for k in ("rot", "mm", "boot")}
     ms = lambda a, q: round(float(np.percentile(a, q)) * 1000.0, 2)  # noqa: E731
@@ -688,7 +724,7 @@ def run_serve(args, rank, world, dist):
         "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform slot values, random keys)",
         "config": {"workload": "serve: Poisson arrivals at N=2^16 with resident keys, HBM-budget admission",
                    "rate_jobs_per_s": S["rate"], "jobs": kinds, "ciphertexts": n_cts, "slots": S["slots"],
-                   "budget_gb": S["budget_gb"], "rotation_batches": f"1-{S['rot_max']} cts at {S['rot_levels']} limbs",
+                   "budget_gb": S["budget_gb"], "outstanding_jobs": S["outstanding"], "rotation_batches": f"1-{S['rot_max']} cts at {S['rot_levels']} limbs",
                    "matmul": f"{S['mm_n']}x{S['mm_n']} at {S['mm_L']} limbs",
                    "bootstrap": f"{S['boot_batch']} cts, shared-a n={S['members']}"},
         "serving": {"p50_ms": ms(lat, 50), "p99_ms": ms(lat, 99), "by_kind": by_kind,
