@@ -634,6 +634,7 @@ struct CrtLimb {
     uint64_t c[kMaxMods];  // c_t mod q_l
     double chd[kMaxMods];  // c_t >> 32 as a double (exact: below 2^29 for any prime below 2^61)
     uint64_t M;            // M mod q_l
+    uint64_t Mneg;         // q_l - (M mod q_l), below q_l
 };
 
 // one thread folds 4 consecutive columns r (one limb, 4 | N): 4-byte residue loads and
@@ -686,9 +687,12 @@ __global__ void __launch_bounds__(256, 3) crt_kernel(const uint8_t *__restrict__
         const uint64_t mant = 0x000FFFFFFFFFFFFFull;
         const uint64_t hii = (uint64_t)__double_as_longlong(__dadd_rn(hi[e], two52)) & mant;
         const uint64_t vi = (uint64_t)__double_as_longlong(__dadd_rn(v[e], two52)) & mant;
+        // S = sum_t r_t c_t - v M = sum_t r_t c_t + v (q - M mod q) mod q: one reduction of the sum
+        // (v < 2^13, so v (q - M mod q) < 2^74 and the whole sum stays far below the Barrett bound)
         const uint64_t plo = lo[e] + (hii << 32);
-        const u128 pos = {plo, (hii >> 32) + (plo < lo[e] ? 1ull : 0ull)};
-        y[e] = sub_mod(barrett(pos, p), barrett(mul_wide(vi, cl.M), p), p.q);
+        u128 pos = {plo, (hii >> 32) + (plo < lo[e] ? 1ull : 0ull)};
+        mac(pos, vi, cl.Mneg);
+        y[e] = barrett(pos, p);
     }
     ulonglong2 *out = reinterpret_cast<ulonglong2 *>(Y + (uint64_t)o * R + rg);
     out[0] = make_ulonglong2(y[0], y[1]);
@@ -748,6 +752,7 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
         uint64_t q = c.primes[l], M = 1;
         for (uint32_t u = 0; u < T; u++) M = host::mulmod(M, cand[u], q);
         p.limbs[l].M = M;
+        p.limbs[l].Mneg = (q - M) % q;
         for (uint32_t t = 0; t < T; t++) {
             uint32_t m = cand[t], Mt_mod_m = 1;
             uint64_t Mt = 1;
