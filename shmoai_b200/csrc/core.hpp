@@ -236,8 +236,9 @@ void fmt_forward(const Context &c, const uint64_t *cts, uint32_t n_groups, uint3
 size_t fmt_backward_ws_words(const Context &c, uint32_t n_groups, uint32_t n, uint32_t L);
 void fmt_backward(const Context &c, const uint64_t *sh, uint32_t n_groups, uint32_t n, uint32_t L,
                   const uint64_t *const *keys, uint64_t *out, uint64_t *ws, cudaStream_t st);
+// max_l1 = max over outputs o of sum_i |W_io| (it sizes the residue system)
 void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
-                    uint32_t L, void *ws, uint64_t max_abs_w, cudaStream_t st);
+                    uint32_t L, void *ws, uint64_t max_l1, cudaStream_t st);
 int ctpt_tc_error(void *ws, cudaStream_t st);
 size_t ctpt_ws_words(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L);
 // ---- the extended basis QlP: a polynomial at level L has L + np limbs, the Q limbs 0..L-1

@@ -8,6 +8,8 @@
 // The signed weights are small (|W| < 2^40), so each thread accumulates the
 // positive and the negative part of sum_i x_i * |W_io| exactly in two 128-bit
 // registers and reduces once at the end.
+#include <algorithm>
+
 #include "core.hpp"
 
 namespace shm {
@@ -80,14 +82,23 @@ void ctpt_matmul(const Context &c, const uint64_t *X, const int64_t *W, uint64_t
                  uint32_t L, uint64_t *ws, cudaStream_t st) {
     if (n_in == 0 || n_out == 0) return;
     if (L < 1 || L > c.nq) throw std::invalid_argument("level out of range");
-    // the residue system is sized from max|W| (one small device-to-host copy of the weights)
+    // the residue system is sized from the largest column sum of |W| (one small device-to-host copy
+    // of the weights); every |W| must be below 2^40
     std::vector<int64_t> hw((size_t)n_in * n_out);
     SHM_CUDA(cudaMemcpyAsync(hw.data(), W, hw.size() * 8, cudaMemcpyDeviceToHost, st));
     SHM_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint64_t> l1(n_out, 0);
     uint64_t mx = 0;
-    for (int64_t w : hw) mx = std::max<uint64_t>(mx, w < 0 ? (uint64_t)(-(w + 1)) + 1 : (uint64_t)w);
+    for (uint32_t i = 0; i < n_in; i++)
+        for (uint32_t o = 0; o < n_out; o++) {
+            const int64_t w = hw[(size_t)i * n_out + o];
+            const uint64_t a = w < 0 ? (uint64_t)(-(w + 1)) + 1 : (uint64_t)w;
+            mx = std::max(mx, a);
+            l1[o] += a;  // below n_in 2^40: no overflow for n_in < 2^24
+        }
     if (mx >= (1ull << 40)) throw std::invalid_argument("ct-pt matmul: |W| must be below 2^40");
-    ctpt_matmul_tc(c, X, W, Y, n_in, n_out, L, ws, mx, st);
+    if (n_in >= (1u << 24)) throw std::invalid_argument("ct-pt matmul: too many inputs");
+    ctpt_matmul_tc(c, X, W, Y, n_in, n_out, L, ws, *std::max_element(l1.begin(), l1.end()), st);
     if (ctpt_tc_error(ws, st)) throw CudaError("ct-pt matmul: tensor-core pipeline wait timed out");
 }
 

@@ -7,24 +7,25 @@
 // dense contraction.
 //
 // Exactness by a small-modulus residue system: the integer S = sum_i x_i w_i
-// (|S| < n_in * max q * max|W|) is computed modulo T pairwise-coprime moduli
-// m_t <= 251 whose product exceeds 8|S|, each as an int8 GEMM with balanced
+// (|S| <= (q_l - 1) max_o sum_i |w_io|) is computed modulo T pairwise-coprime moduli
+// m_t <= 251 whose product exceeds 2.02 |S|, each as an int8 GEMM with balanced
 // residues in [-125, 125] (|acc| < n_in * 125^2 < 2^31), then rebuilt by the CRT:
 //   S = sum_t r_t c_t - v M,  c_t = (M/m_t) [(M/m_t)^-1]_{m_t},  v = round(sum_t r_t inv_t / m_t),
 // and reduced mod q_l with per-limb constants.  T GEMMs replace the 35 byte-slice
-// products of a positional split.
+// products of a positional split; T is chosen per limb (a smaller prime needs fewer moduli)
+// and each pass of columns runs with the largest T of its limbs.
 //
-// Pipeline per modulus: X residue planes [R][K] and W residue planes [N][K]
-// (both K-major) -> tcgen05 GEMM tile M = 128 columns of X x N = 256 outputs,
-// K in 64-byte stages (4-stage cp.async ring, one mbarrier per stage), s32
-// accumulator in TMEM (256 columns) -> epilogue tcgen05.ld, acc mod m_t -> uint8
-// residue planes -> CRT kernel.
+// Pipeline per pass of columns: X residue planes [T][R][K] and W residue planes [T][N][K]
+// (both K-major) -> tcgen05 GEMMs (weights as the M = 128 side, 256 X columns as N, s32
+// accumulators in TMEM; operands by TMA where the X tile fits in shared memory) ->
+// epilogue tcgen05.ld, acc mod m_t -> uint8 residue planes -> CRT kernel.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 #include "core.hpp"
 #include "host_math.hpp"
@@ -49,7 +50,7 @@ constexpr long long kSpinLimit = 1ll << 24;
 // write it write the same bytes; each kernel takes its T as an argument.
 struct ModTab {
     uint32_t m[kMaxMods];
-    double fracd[kMaxMods + 1][kMaxMods];  // [T][t]: [(M/m_t)^-1]_{m_t} / m_t rounded to a double
+    uint32_t fracq[kMaxMods + 1][kMaxMods];  // [T][t]: round(2^19 [(M/m_t)^-1]_{m_t} / m_t)
     uint32_t c24[kMaxMods];  // 2^20 mod m_t
     uint32_t c48[kMaxMods];  // 2^40 mod m_t
     uint32_t magic[kMaxMods];  // ceil(2^32 / m_t)
@@ -58,6 +59,8 @@ struct ModTab {
 };
 
 __constant__ ModTab c_mods;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 // ---------------------------------------------------------------- residues
 __device__ __forceinline__ int8_t balanced(uint32_t r, uint32_t m) { return (int8_t)(r > m / 2 ? (int)r - (int)m : (int)r); }
@@ -92,64 +95,98 @@ __device__ __forceinline__ uint32_t mod_acc(int a, uint32_t t) {
     return mod_small(x, t);
 }
 
-// The balanced residue of x mod m_t (in (-m/2, m/2), m odd) on the FP64 pipe, for x < 2^51 given
-// as the exact double xd: q = round(x / m) from fma(xd, 1/m, 1.5 2^52) (the pre-rounding value is
+// The balanced residue of x mod m_t (in (-m/2, m/2), m odd) for x < 2^51 given as the exact double
+// xd and its low word xlo: q = round(x / m) from fma(xd, 1/m, 1.5 2^52) (the pre-rounding value is
 // within (x / m) 2^-53 < 0.25 / m of x / m, and x / m lies at least 0.5 / m from a half-integer,
-// so q is the nearest integer), then x - q m exactly by a second fma.  The result is returned as
-// the low byte of the mantissa of r + 1.5 2^52 (|r| < 2^51: two's complement of r mod 256).
-__device__ __forceinline__ uint32_t balanced_f64(double xd, uint32_t t) {
+// so q is the nearest integer).  The fma's result 1.5 2^52 + q carries q in the low bits of its
+// mantissa (2^51 is a multiple of 2^32), so (x - q m) mod 2^32 = xlo - q_lo m, whose low byte is
+// the two's complement of the residue: one FP64 multiply-add and one integer multiply-add.
+__device__ __forceinline__ uint32_t balanced_f64(double xd, uint32_t xlo, uint32_t t) {
     const double magic = 6755399441055744.0;  // 1.5 * 2^52
-    const double q = __dsub_rn(__fma_rn(xd, c_mods.inv[t], magic), magic);
-    const double r = __fma_rn(-q, (double)c_mods.m[t], xd);
-    return (uint32_t)__double2loint(__dadd_rn(r, magic)) & 0xFF;
+    const uint32_t q = (uint32_t)__double2loint(__fma_rn(xd, c_mods.inv[t], magic));
+    return xlo - q * c_mods.m[t];
 }
 
-// X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via a 64 x 64 shared-memory transpose.  Each
-// thread writes four consecutive inputs' residues of one column as one 32-bit word, so a warp's
-// store covers 64 contiguous bytes of each of two columns for every modulus.  F64 (every limb
-// prime below 2^51): the residues on the FP64 pipe (balanced_f64), else in 32-bit integer
-// arithmetic (mod_small).
+// the low bytes of four words as one word
+__device__ __forceinline__ uint32_t pack_low_bytes(uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3) {
+    return __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
+}
+
+// X [n_in][R] (uint64) -> XP [t][R][Kp] (int8), via 64 x 64 shared-memory transposes.  A block
+// converts kXresTiles column tiles of one 64-input group: the next tile's rows are copied by
+// cp.async (8-byte pieces; rows past n_in filled with zeros) while the current one is converted.
+// Each thread writes four consecutive inputs' residues of one column as one 32-bit word, so a
+// warp's store covers 64 contiguous bytes of each of two columns for every modulus.  F64 (every
+// limb prime below 2^51): each residue from one FP64 and one integer multiply-add (balanced_f64),
+// else in 32-bit integer arithmetic (mod_small).
+constexpr uint32_t kXresTiles = 2;
+constexpr uint32_t kXresSmem = 2 * 64 * 65 * 8;
+
 template <bool F64>
-__global__ void __launch_bounds__(256, 4) xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__ XP, uint32_t n_in, uint32_t Kp,
-                            uint64_t R, uint64_t r0, uint32_t T) {
-    __shared__ uint64_t tile[64][65];
+__global__ void __launch_bounds__(256, 3) xres_kernel(const uint64_t *__restrict__ X, int8_t *__restrict__ XP,
+                                                      uint32_t n_in, uint32_t Kp, uint64_t R, uint64_t r0,
+                                                      uint64_t chunk, uint32_t T) {
+    extern __shared__ uint64_t xres_smem[];
+    uint64_t(*tile)[64][65] = reinterpret_cast<uint64_t(*)[64][65]>(xres_smem);
     const uint32_t i0 = blockIdx.y * 64;
-    const uint64_t rb = (uint64_t)blockIdx.x * 64;
     const uint32_t tx = threadIdx.x & 63, ty = threadIdx.x >> 6;  // 256 threads: 64 x 4
-    for (uint32_t i = ty; i < 64; i += 4) {
-        uint32_t ii = i0 + i;
-        tile[i][tx] = ii < n_in ? X[(uint64_t)ii * R + r0 + rb + tx] : 0;
-    }
-    __syncthreads();
-    const uint64_t chunk = (uint64_t)gridDim.x * 64;
+    const uint64_t rb0 = (uint64_t)blockIdx.x * kXresTiles * 64;
+    auto fetch = [&](uint32_t buf, uint64_t rb) {
+        for (uint32_t i = ty; i < 64; i += 4) {
+            const uint32_t ii = i0 + i;
+            const uint64_t *src = X + (uint64_t)(ii < n_in ? ii : 0) * R + r0 + rb + tx;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(&tile[buf][i][tx])), "l"(src),
+                         "r"(ii < n_in ? 8 : 0));
+        }
+        asm volatile("cp.async.commit_group;\n");
+    };
+    fetch(0, rb0);
     const uint32_t kq = threadIdx.x & 15, cg = threadIdx.x >> 4;  // inputs 4 kq .. 4 kq + 3, columns 4 cg .. 4 cg + 3
-#pragma unroll
-    for (uint32_t c = 0; c < 4; c++) {
-        const uint32_t col = 4 * cg + c;
-        uint64_t x[4];
-#pragma unroll
-        for (uint32_t j = 0; j < 4; j++) x[j] = tile[4 * kq + j][col];
-        if constexpr (F64) {
-            const double two52 = 4503599627370496.0;
-            double xd[4];
-#pragma unroll
-            for (uint32_t j = 0; j < 4; j++)  // exact: x < 2^51
-                xd[j] = __dsub_rn(__longlong_as_double((long long)(0x4330000000000000ull | x[j])), two52);
-            for (uint32_t t = 0; t < T; t++) {
-                uint32_t w = 0;
-#pragma unroll
-                for (uint32_t j = 0; j < 4; j++) w |= balanced_f64(xd[j], t) << (8 * j);
-                *reinterpret_cast<uint32_t *>(XP + ((uint64_t)t * chunk + rb + col) * Kp + i0 + 4 * kq) = w;
-            }
+    for (uint32_t k = 0; k < kXresTiles; k++) {
+        const uint32_t buf = k & 1;
+        const uint64_t rb = rb0 + (uint64_t)k * 64;
+        if (k + 1 < kXresTiles) {
+            fetch(buf ^ 1, rb + 64);
+            asm volatile("cp.async.wait_group 1;\n");
         } else {
-            for (uint32_t t = 0; t < T; t++) {
-                uint32_t w = 0;
+            asm volatile("cp.async.wait_group 0;\n");
+        }
+        __syncthreads();
 #pragma unroll
-                for (uint32_t j = 0; j < 4; j++)
-                    w |= (uint32_t)(uint8_t)balanced(mod_small(x[j], t), c_mods.m[t]) << (8 * j);
-                *reinterpret_cast<uint32_t *>(XP + ((uint64_t)t * chunk + rb + col) * Kp + i0 + 4 * kq) = w;
+        for (uint32_t c = 0; c < 4; c++) {
+            const uint32_t col = 4 * cg + c;
+            uint64_t x[4];
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) x[j] = tile[buf][4 * kq + j][col];
+            int8_t *dst = XP + (rb + col) * Kp + i0 + 4 * kq;
+            if constexpr (F64) {
+                const double two52 = 4503599627370496.0;
+                double xd[4];
+                uint32_t xl[4];
+#pragma unroll
+                for (uint32_t j = 0; j < 4; j++) {  // exact: x < 2^51
+                    xd[j] = __dsub_rn(__longlong_as_double((long long)(0x4330000000000000ull | x[j])), two52);
+                    xl[j] = (uint32_t)x[j];
+                }
+                // unrolled over every candidate modulus (a uniform guard): the constants become operands
+#pragma unroll
+                for (uint32_t t = 0; t < (uint32_t)kMaxMods; t++) {
+                    if (t < T)
+                        *reinterpret_cast<uint32_t *>(dst + (uint64_t)t * chunk * Kp) =
+                            pack_low_bytes(balanced_f64(xd[0], xl[0], t), balanced_f64(xd[1], xl[1], t),
+                                           balanced_f64(xd[2], xl[2], t), balanced_f64(xd[3], xl[3], t));
+                }
+            } else {
+                for (uint32_t t = 0; t < T; t++) {
+                    uint32_t w = 0;
+#pragma unroll
+                    for (uint32_t j = 0; j < 4; j++)
+                        w |= (uint32_t)(uint8_t)balanced(mod_small(x[j], t), c_mods.m[t]) << (8 * j);
+                    *reinterpret_cast<uint32_t *>(dst + (uint64_t)t * chunk * Kp) = w;
+                }
             }
         }
+        __syncthreads();  // the buffer is refilled by the tile after next
     }
 }
 
@@ -169,7 +206,6 @@ __global__ void wres_kernel(const int64_t *__restrict__ W, int8_t *__restrict__ 
 }
 
 // ---------------------------------------------------------------- tcgen05 GEMM
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 // K-major, no-swizzle ("interleaved") operand: core matrices of 8 rows x 16 bytes,
 // K-adjacent core matrices 128 B apart (LBO), 8-row groups (KB / 16) * 128 B apart (SBO).
@@ -632,66 +668,87 @@ __global__ void __launch_bounds__(kThreadsP, 1) mma_persistent_kernel(const int8
 // ---------------------------------------------------------------- CRT fold
 struct CrtLimb {
     uint64_t c[kMaxMods];  // c_t mod q_l
-    double chd[kMaxMods];  // c_t >> 32 as a double (exact: below 2^29 for any prime below 2^61)
     uint64_t M;            // M mod q_l
     uint64_t Mneg;         // q_l - (M mod q_l), below q_l
 };
 
-// one thread folds 4 consecutive columns r (one limb, 4 | N): 4-byte residue loads and
-// two 16-byte stores instead of byte loads and 8-byte stores
-__global__ void __launch_bounds__(256, 3) crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict__ Y, const CrtLimb *__restrict__ tab,
-                           uint32_t n_out, uint64_t chunk, uint64_t r0, uint64_t R, uint32_t L, uint32_t log_n,
-                           const PrimeConst *__restrict__ pc, uint32_t T) {
-    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+// Fraction bits of the fixed-point CRT fractions F_t = round(2^19 [(M/m_t)^-1]_{m_t} / m_t): with
+// r_t < 251 and T <= 20, sum_t r_t F_t + 2^18 < 2^32, and the sum's rounding error
+// T 251 2^-20 < 0.005 keeps v = round(sum_t r_t frac_t) exact (the CRT margin leaves the true sum
+// within 1/8 of an integer).
+constexpr uint32_t kCrtFracBits = 19;
+
+// workspace bytes before the residue planes: the error flag, then the CRT tables for every
+// moduli count in use (at most kMaxMods counts of up to 64 limbs)
+constexpr size_t kCrtTabBytes = 256 + sizeof(CrtLimb) * 64 * kMaxMods;
+
+// One thread folds 4 consecutive columns r of one output (4-byte residue loads, two 16-byte
+// stores).  The host sizes the block so that its 4 blockDim.x columns lie in one limb: the limb's
+// constants (the 32-bit halves of c_t and the fixed-point fractions) are staged in shared memory
+// once per block.  Per residue and column three integer multiply-adds:
+//   lo += r_t (c_t mod 2^32),  hi += r_t (c_t >> 32)   (exact sums),
+//   v  += r_t F_t                                        (32-bit fixed point),
+// then S = lo + hi 2^32 - v M = lo + hi 2^32 + v (q - M mod q) mod q, one Barrett reduction
+// (the sum is below 20 251 2^61 + 2^13 2^61 < 2^75).  HI32: the host has checked that
+// T 250 max(c_t >> 32) < 2^32, so hi is summed in 32 bits.  The residue words (one per modulus,
+// read once: streaming loads) are requested before the fold.
+template <bool HI32>
+__global__ void __launch_bounds__(256) crt_kernel(const uint8_t *__restrict__ RES, uint64_t *__restrict__ Y,
+                                                  const CrtLimb *__restrict__ tab, uint32_t n_out, uint64_t chunk,
+                                                  uint64_t r0, uint64_t R, uint32_t L, uint32_t log_n,
+                                                  const PrimeConst *__restrict__ pc, uint32_t T) {
+    __shared__ uint32_t s_lo[kMaxMods], s_hi[kMaxMods], s_f[kMaxMods];
+    const uint64_t rb = (uint64_t)blockIdx.x * blockDim.x * 4;
     const uint32_t o = blockIdx.y;
+    const uint32_t row = (uint32_t)((r0 + rb) >> log_n);  // h L + limb, below 2 L
+    const uint32_t limb = row >= L ? row - L : row;
+    if (threadIdx.x < (uint32_t)kMaxMods) {
+        const uint32_t t = threadIdx.x;
+        const uint64_t c = t < T ? tab[limb].c[t] : 0;
+        s_lo[t] = (uint32_t)c;
+        s_hi[t] = (uint32_t)(c >> 32);
+        s_f[t] = t < T ? c_mods.fracq[T][t] : 0u;
+    }
+    __syncthreads();
+    const uint64_t r = rb + (uint64_t)threadIdx.x * 4;
     if (r >= chunk) return;
     const uint64_t rg = r0 + r;
-    const uint32_t limb = (uint32_t)((rg >> log_n) % L);
-    const CrtLimb &cl = tab[limb];
     const PrimeConst p = pc[limb];
-    const double two52 = 4503599627370496.0;
-    // sum_t r_t c_t from the 32-bit halves of c_t (r_t < 2^8): the low products on the integer
-    // pipe (64-bit sums below 2^45), the high ones on the FP64 pipe (each below 2^37, their sum
-    // below 2^42: exact in a double); v = round(sum_t r_t frac_t) on the FP64 pipe, off by far less
-    // than the CRT margin of 1/8.  The FP64 values are read back from their mantissas (2^52 added:
-    // exact integers below 2^52).  Moduli outer, the four columns inner; the residues (one 4-byte
-    // word per modulus, read once: streaming loads) requested before the fold.
-    constexpr uint32_t kAhead = 14;  // residue words requested before the fold (T <= 14 at the usual weight sizes)
+    const uint64_t Mneg = tab[limb].Mneg;
+    constexpr uint32_t kAhead = 16;  // residue words requested before the fold
     uint32_t res[kAhead];
 #pragma unroll
     for (uint32_t t = 0; t < kAhead; t++)
         res[t] = t < T ? __ldcs(reinterpret_cast<const uint32_t *>(RES + ((uint64_t)t * n_out + o) * chunk + r)) : 0u;
+    using HiT = typename std::conditional<HI32, uint32_t, uint64_t>::type;
     uint64_t lo[4] = {0, 0, 0, 0};
-    double hi[4] = {0.0, 0.0, 0.0, 0.0}, v[4] = {0.0, 0.0, 0.0, 0.0};
+    HiT hi[4] = {0, 0, 0, 0};
+    uint32_t v[4];
 #pragma unroll
-    for (uint32_t t = 0; t < kMaxMods; t++) {
+    for (int e = 0; e < 4; e++) v[e] = 1u << (kCrtFracBits - 1);
+#pragma unroll
+    for (uint32_t t = 0; t < (uint32_t)kMaxMods; t++) {
         if (t < T) {
             const uint32_t r4 =
                 t < kAhead ? res[t]
                            : __ldcs(reinterpret_cast<const uint32_t *>(RES + ((uint64_t)t * n_out + o) * chunk + r));
-            const uint32_t c32 = (uint32_t)cl.c[t];
-            const double ch = cl.chd[t], fr = c_mods.fracd[T][t];
+            const uint32_t cl = s_lo[t], ch = s_hi[t], f = s_f[t];
 #pragma unroll
             for (int e = 0; e < 4; e++) {
                 const uint32_t rt = (r4 >> (8 * e)) & 0xFF;
-                lo[e] += (uint64_t)rt * c32;
-                const double rd = __dsub_rn(__hiloint2double(0x43300000, (int)rt), two52);
-                hi[e] = __fma_rn(rd, ch, hi[e]);
-                v[e] = __fma_rn(rd, fr, v[e]);
+                lo[e] += (uint64_t)rt * cl;
+                hi[e] += (HiT)rt * ch;
+                v[e] += rt * f;
             }
         }
     }
     uint64_t y[4];
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-        const uint64_t mant = 0x000FFFFFFFFFFFFFull;
-        const uint64_t hii = (uint64_t)__double_as_longlong(__dadd_rn(hi[e], two52)) & mant;
-        const uint64_t vi = (uint64_t)__double_as_longlong(__dadd_rn(v[e], two52)) & mant;
-        // S = sum_t r_t c_t - v M = sum_t r_t c_t + v (q - M mod q) mod q: one reduction of the sum
-        // (v < 2^13, so v (q - M mod q) < 2^74 and the whole sum stays far below the Barrett bound)
-        const uint64_t plo = lo[e] + (hii << 32);
-        u128 pos = {plo, (hii >> 32) + (plo < lo[e] ? 1ull : 0ull)};
-        mac(pos, vi, cl.Mneg);
+        const uint64_t h = hi[e];
+        const uint64_t plo = lo[e] + (h << 32);
+        u128 pos = {plo, (h >> 32) + (plo < lo[e] ? 1ull : 0ull)};
+        mac(pos, v[e] >> kCrtFracBits, Mneg);
         y[e] = barrett(pos, p);
     }
     ulonglong2 *out = reinterpret_cast<ulonglong2 *>(Y + (uint64_t)o * R + rg);
@@ -707,26 +764,38 @@ namespace {
 
 struct Plan {
     ModTab mods;
-    uint32_t T = 0;
-    std::vector<CrtLimb> limbs;
+    uint32_t T_min = 0, T_max = 0;   // the moduli counts the limbs need
+    std::vector<uint32_t> limb_T;    // per limb
+    std::vector<CrtLimb> limbs;      // [T - T_min][L]: the CRT constants for each count in use
+    bool hi32 = false;               // T_max 250 max(c_t >> 32) < 2^32: the CRT's high sums in 32 bits
 };
 
-Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) {
-    // |S| < n_in * max q * max|W|; the moduli product must exceed 8 |S| (CRT margin)
+// The moduli count of each limb: |S| = |sum_i x_i w_io| <= (q_l - 1) max_o sum_i |w_io| = B_l, and
+// the CRT with the fixed-point v (error below 0.005) is exact while M > 2 B_l / (1 - 0.01); the
+// product of the first T candidates must exceed that (log2 M >= log2 B_l + 1.05).
+Plan make_plan(const Context &c, uint32_t L, uint64_t max_l1) {
     static const uint32_t cand[kMaxMods] = {251, 241, 239, 233, 229, 227, 223, 211, 199, 197,
                                             193, 191, 181, 179, 173, 167, 163, 157, 151, 149};
-    uint64_t maxq = 0;
-    for (uint32_t l = 0; l < L; l++) maxq = std::max(maxq, c.primes[l]);
-    const double need = std::log2((double)n_in) + std::log2((double)maxq) + std::log2((double)std::max<uint64_t>(max_abs_w, 1)) + 4.0;
     Plan p{};
-    double have = 0;
-    uint32_t T = 0;
-    while (have < need) {
-        if (T >= (uint32_t)kMaxMods) throw std::invalid_argument("ct-pt matmul: weights or inputs too large");
-        have += std::log2((double)cand[T]);
-        T++;
+    p.limb_T.resize(L);
+    p.T_min = kMaxMods;
+    uint64_t max_hi = 0;
+    for (uint32_t l = 0; l < L; l++) {
+        const uint64_t q = c.primes[l];
+        const double need = std::log2((double)(q - 1)) + std::log2((double)std::max<uint64_t>(max_l1, 1)) + 1.05;
+        double have = 0;
+        uint32_t T = 0;
+        while (have < need) {
+            if (T >= (uint32_t)kMaxMods) throw std::invalid_argument("ct-pt matmul: weights or inputs too large");
+            have += std::log2((double)cand[T]);
+            T++;
+        }
+        p.limb_T[l] = T;
+        p.T_min = std::min(p.T_min, T);
+        p.T_max = std::max(p.T_max, T);
+        max_hi = std::max(max_hi, (q - 1) >> 32);
     }
-    p.T = T;
+    p.hi32 = (uint64_t)p.T_max * 250 * max_hi < (1ull << 32);
     for (uint32_t t = 0; t < (uint32_t)kMaxMods; t++) {
         const uint32_t m = cand[t];
         p.mods.m[t] = m;
@@ -736,7 +805,7 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
         p.mods.inv[t] = 1.0 / m;
         p.mods.invf[t] = 1.0f / (float)m;
     }
-    // CRT fractions [(M/m_t)^-1 mod m_t] / m_t for every modulus count
+    // CRT fractions [(M/m_t)^-1 mod m_t] / m_t in fixed point, for every modulus count
     for (uint32_t n = 1; n <= (uint32_t)kMaxMods; n++)
         for (uint32_t t = 0; t < n; t++) {
             const uint32_t m = cand[t];
@@ -744,28 +813,29 @@ Plan make_plan(const Context &c, uint32_t n_in, uint32_t L, uint64_t max_abs_w) 
             for (uint32_t u = 0; u < n; u++)
                 if (u != t) Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (cand[u] % m) % m);
             const uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);  // m prime
-            p.mods.fracd[n][t] = (double)inv / (double)m;
+            p.mods.fracq[n][t] = (uint32_t)((((uint64_t)inv << kCrtFracBits) + m / 2) / m);
         }
-    // CRT constants of the chosen T: c_t = (M/m_t) * [(M/m_t)^-1 mod m_t] mod q_l
-    p.limbs.resize(L);
-    for (uint32_t l = 0; l < L; l++) {
-        uint64_t q = c.primes[l], M = 1;
-        for (uint32_t u = 0; u < T; u++) M = host::mulmod(M, cand[u], q);
-        p.limbs[l].M = M;
-        p.limbs[l].Mneg = (q - M) % q;
-        for (uint32_t t = 0; t < T; t++) {
-            uint32_t m = cand[t], Mt_mod_m = 1;
-            uint64_t Mt = 1;
-            for (uint32_t u = 0; u < T; u++)
-                if (u != t) {
-                    Mt = host::mulmod(Mt, cand[u], q);
-                    Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (cand[u] % m) % m);
-                }
-            uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);
-            p.limbs[l].c[t] = host::mulmod(Mt, inv, q);
-            p.limbs[l].chd[t] = (double)(p.limbs[l].c[t] >> 32);
+    // CRT constants for each count T in use: c_t = (M/m_t) * [(M/m_t)^-1 mod m_t] mod q_l
+    p.limbs.resize((size_t)(p.T_max - p.T_min + 1) * L);
+    for (uint32_t T = p.T_min; T <= p.T_max; T++)
+        for (uint32_t l = 0; l < L; l++) {
+            CrtLimb &cl = p.limbs[(size_t)(T - p.T_min) * L + l];
+            uint64_t q = c.primes[l], M = 1;
+            for (uint32_t u = 0; u < T; u++) M = host::mulmod(M, cand[u], q);
+            cl.M = M;
+            cl.Mneg = (q - M) % q;
+            for (uint32_t t = 0; t < T; t++) {
+                uint32_t m = cand[t], Mt_mod_m = 1;
+                uint64_t Mt = 1;
+                for (uint32_t u = 0; u < T; u++)
+                    if (u != t) {
+                        Mt = host::mulmod(Mt, cand[u], q);
+                        Mt_mod_m = (uint32_t)((uint64_t)Mt_mod_m * (cand[u] % m) % m);
+                    }
+                uint32_t inv = (uint32_t)host::powmod(Mt_mod_m, m - 2, m);
+                cl.c[t] = host::mulmod(Mt, inv, q);
+            }
         }
-    }
     return p;
 }
 
@@ -796,38 +866,48 @@ bool operand_tensor_map(CUtensorMap *map, const int8_t *P, uint32_t Kp, uint64_t
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// columns of X processed per pass (bounds the residue workspaces)
+// columns of X processed per pass (bounds the residue workspaces); the environment variable
+// SHMOAI_CTPT_CHUNK (a multiple of 256) replaces the default, read once per process
 constexpr uint64_t kChunkCols = 131072;
+
+static uint64_t chunk_cols() {
+    static const uint64_t v = [] {
+        const char *s = std::getenv("SHMOAI_CTPT_CHUNK");
+        const uint64_t c = s ? std::strtoull(s, nullptr, 10) : 0;
+        return (c >= kBN && c % kBN == 0) ? c : kChunkCols;
+    }();
+    return v;
+}
 
 size_t ctpt_tc_ws_bytes(const Context &c, uint32_t n_in, uint32_t n_out, uint32_t L) {
     const uint64_t R = 2ull * L * c.n;
-    const uint64_t chunk = std::min<uint64_t>(R, kChunkCols);
+    const uint64_t chunk = std::min<uint64_t>(R, chunk_cols());
     const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBM - 1) / kBM * kBM;
-    return (size_t)kMaxMods * (chunk * Kp + (uint64_t)Np * Kp + (uint64_t)n_out * chunk) + 4096 +
-           sizeof(CrtLimb) * 64;
+    return (size_t)kMaxMods * (chunk * Kp + (uint64_t)Np * Kp + (uint64_t)n_out * chunk) + kCrtTabBytes;
 }
 
 // Chunks of 131,072 columns run one after the other on `st`.  (Alternating them over two
 // streams, so that one chunk's residue and CRT kernels could run beside the other's GEMM,
 // measured no faster: the GEMM's grid fills every SM.)
 void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint64_t *Y, uint32_t n_in, uint32_t n_out,
-                    uint32_t L, void *ws, uint64_t max_abs_w, cudaStream_t st) {
+                    uint32_t L, void *ws, uint64_t max_l1, cudaStream_t st) {
     if (n_in == 0 || n_out == 0) return;
     const uint64_t R = 2ull * L * c.n;
     if (R % kBN) throw std::invalid_argument("ct-pt matmul: 2 L N must be a multiple of 256");
-    const uint64_t chunk = std::min<uint64_t>(R, kChunkCols);
+    const uint64_t chunk = std::min<uint64_t>(R, chunk_cols());
     const uint32_t Kp = (n_in + kKB - 1) / kKB * kKB, Np = (n_out + kBM - 1) / kBM * kBM;
-    Plan plan = make_plan(c, n_in, L, max_abs_w);
-    const uint32_t T = plan.T;
+    Plan plan = make_plan(c, L, max_l1);
+    const uint32_t T = plan.T_max;  // the weight planes and the workspaces hold T_max moduli
     SHM_CUDA(cudaMemcpyToSymbolAsync(c_mods, &plan.mods, sizeof(ModTab), 0, cudaMemcpyHostToDevice, st));
     // workspace carve-up
     uint8_t *base = static_cast<uint8_t *>(ws);
     int *err = reinterpret_cast<int *>(base);
     CrtLimb *tab = reinterpret_cast<CrtLimb *>(base + 256);
-    int8_t *XP = reinterpret_cast<int8_t *>(base + 4096 + sizeof(CrtLimb) * 64);
+    int8_t *XP = reinterpret_cast<int8_t *>(base + kCrtTabBytes);
     int8_t *WP = XP + (size_t)T * chunk * Kp;
     uint8_t *RES = reinterpret_cast<uint8_t *>(WP + (size_t)T * Np * Kp);
-    SHM_CUDA(cudaMemcpyAsync(tab, plan.limbs.data(), sizeof(CrtLimb) * L, cudaMemcpyHostToDevice, st));
+    if (plan.limbs.size() > (size_t)64 * kMaxMods) throw std::invalid_argument("ct-pt matmul: too many limbs");
+    SHM_CUDA(cudaMemcpyAsync(tab, plan.limbs.data(), sizeof(CrtLimb) * plan.limbs.size(), cudaMemcpyHostToDevice, st));
     SHM_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
     // zero-padded K tail of the X planes stays zero: clear once per call
     if (Kp != n_in) SHM_CUDA(cudaMemsetAsync(XP, 0, (size_t)T * chunk * Kp, st));
@@ -849,37 +929,50 @@ void ctpt_matmul_tc(const Context &c, const uint64_t *X, const int64_t *W, uint6
     const int acc24 = (uint64_t)Kp * 125 * 125 < (1ull << 24) ? 1 : 0;  // accumulators exact in float
     bool f64_res = true;  // every limb prime below 2^51: the X residues on the FP64 pipe
     for (uint32_t l = 0; l < L; l++) f64_res = f64_res && c.primes[l] < (1ull << 51);
+    SHM_CUDA(cudaFuncSetAttribute(f64_res ? xres_kernel<true> : xres_kernel<false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kXresSmem));
     for (uint64_t r0 = 0; r0 < R; r0 += chunk) {
         // a shorter last pass (2 L N not a multiple of the chunk, e.g. at N = 2^12) lays its planes out
         // with its own column count; every count here is a multiple of 256
         const uint64_t cur = std::min<uint64_t>(chunk, R - r0);
+        // the pass's moduli count: the largest its limbs (rows h L + l, h = 0, 1) need
+        uint32_t Tc = 0;
+        for (uint64_t row = r0 >> c.log_n; row <= (r0 + cur - 1) >> c.log_n; row++)
+            Tc = std::max(Tc, plan.limb_T[row % L]);
+        const CrtLimb *tab_c = tab + (size_t)(Tc - plan.T_min) * L;
         SHM_LAUNCHED(1);
+        const dim3 xgrid((uint32_t)(cur / (64 * kXresTiles)), (n_in + 63) / 64);
         if (f64_res)
-            xres_kernel<true><<<dim3((uint32_t)(cur / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0, T);
+            xres_kernel<true><<<xgrid, 256, kXresSmem, st>>>(X, XP, n_in, Kp, R, r0, cur, Tc);
         else
-            xres_kernel<false><<<dim3((uint32_t)(cur / 64), (n_in + 63) / 64), 256, 0, st>>>(X, XP, n_in, Kp, R, r0, T);
+            xres_kernel<false><<<xgrid, 256, kXresSmem, st>>>(X, XP, n_in, Kp, R, r0, cur, Tc);
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
         if (resident) {
-            const uint64_t tiles = (uint64_t)T * (cur / kBN);
+            const uint64_t tiles = (uint64_t)Tc * (cur / kBN);
             const uint32_t grid = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)sms);
             // the X planes of this pass, [T * cur][Kp], as 256-row boxes (a pass's planes have its own
             // column count)
-            const bool tma = tma_a && operand_tensor_map(&tmX, XP, Kp, (uint64_t)T * cur, kBN);
+            const bool tma = tma_a && operand_tensor_map(&tmX, XP, Kp, (uint64_t)Tc * cur, kBN);
             if (tma)
                 mma_persistent_kernel<true>
-                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24, tmA, tmX);
+                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, Tc, err, acc24, tmA, tmX);
             else
                 mma_persistent_kernel<false>
-                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, T, err, acc24, tmA, tmX);
+                    <<<grid, kThreadsP, kSmemP, st>>>(XP, WP, RES, Kp, Np, n_out, cur, Tc, err, acc24, tmA, tmX);
         } else {
-            mma_kernel<<<dim3(Np / kBM, (uint32_t)(cur / kBN), T), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
-                                                                                         cur, err, acc24);
+            mma_kernel<<<dim3(Np / kBM, (uint32_t)(cur / kBN), Tc), kThreads, kSmem, st>>>(XP, WP, RES, Kp, Np, n_out,
+                                                                                          cur, err, acc24);
         }
         SHM_CUDA(cudaGetLastError());
         SHM_LAUNCHED(1);
-        crt_kernel<<<dim3((uint32_t)((cur / 4 + 255) / 256), n_out), 256, 0, st>>>(RES, Y, tab, n_out, cur, r0, R, L,
-                                                                                  c.log_n, c.pc, T);
+        // 4 columns a thread; a block's columns within one limb (N and r0 are multiples of the block's)
+        const uint32_t crt_threads = chunk % 1024 == 0 ? 256 : 64;
+        const dim3 cgrid((uint32_t)((cur / 4 + crt_threads - 1) / crt_threads), n_out);
+        if (plan.hi32)
+            crt_kernel<true><<<cgrid, crt_threads, 0, st>>>(RES, Y, tab_c, n_out, cur, r0, R, L, c.log_n, c.pc, Tc);
+        else
+            crt_kernel<false><<<cgrid, crt_threads, 0, st>>>(RES, Y, tab_c, n_out, cur, r0, R, L, c.log_n, c.pc, Tc);
         SHM_CUDA(cudaGetLastError());
     }
 }
