@@ -148,17 +148,19 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
     c->pc = upload(c->h_pc);
     c->tw = upload(tw);
     {
-        // w / q rounded to the nearest double (w and q are exact doubles below 2^53) for the
-        // FP64-quotient butterflies of the primes below kF64GrowLimit; other primes never read it
-        std::vector<double> twq((size_t)QP * 2 * n, 0.0);
+        // for the FP64 butterflies of the primes below kF64GrowLimit (other primes never read it):
+        // the forward and inverse w / q rounded to the nearest double (w and q are exact doubles
+        // below 2^53), then the forward w itself as a double
+        std::vector<double> twq((size_t)QP * 3 * n, 0.0);
         for (uint32_t i = 0; i < QP; i++) {
             if (primes[i] >= kF64GrowLimit) continue;
             const double qd = (double)primes[i];
             const uint64_t *t = tw.data() + (size_t)i * 4 * n;
-            double *d = twq.data() + (size_t)i * 2 * n;
+            double *d = twq.data() + (size_t)i * 3 * n;
             for (uint32_t k = 0; k < n; k++) {
                 d[k] = (double)t[k] / qd;
                 d[n + k] = (double)t[2 * n + k] / qd;
+                d[2 * n + k] = (double)t[k];
             }
         }
         c->twq = upload(twq);

@@ -77,7 +77,7 @@ struct Context {
     std::vector<PrimeConst> h_pc;       // host copy
     PrimeConst *pc = nullptr;           // [QP]
     uint64_t *tw = nullptr;             // [QP][4][N]
-    double *twq = nullptr;              // [QP][2][N]: the forward and inverse twiddles over q, as doubles
+    double *twq = nullptr;              // [QP][3][N]: the forward and inverse twiddles over q, and the forward twiddles, as doubles
     uint64_t *inv_scale_plain = nullptr;  // [QP][4]: N^-1 for a plain INTT, indexed by prime
     uint64_t *moddown_scale = nullptr;  // [np][4]: N^-1 * phat_k^-1
     uint64_t *moddown_conv = nullptr;   // [nq][np]: phat_k mod q_j

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN), *ws = w + G::N;
-    const double *wq = twq + ((size_t)pidx * 2 << G::LOGN);
+    const double *wq = twq + ((size_t)pidx * 3 << G::LOGN), *wd = wq + 2 * G::N;
     uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * S;
 
     const int mode = bf_mode_of(q);  // uniform per CTA (one limb)
@@ -129,13 +129,17 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
 #pragma unroll
         for (int m = 0; m < G::E; m++) a[m] = x[sig + (size_t)G::M * (lane + m * G::E)];
     }
-    fwd_pass_any<R, FAM>(mode, a, w, ws, wq, 1, 0, 0, q);
+    if ((FAM & (1 << kBfF64)) && mode == kBfF64) {  // [0, q) -> doubles for the FP64 butterflies
+#pragma unroll
+        for (int m = 0; m < G::E; m++) a[m] = to_dbl_bits(a[m]);
+    }
+    fwd_pass_any<R, FAM>(mode, a, w, ws, wq, wd, 1, 0, 0, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) sm[(lane + m * G::E) * S + sig] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = sm[(lane * G::E + m) * S + sig];
-    fwd_pass_any<R, FAM>(mode, a, w, ws, wq, 1, R, lane, q);
+    fwd_pass_any<R, FAM>(mode, a, w, ws, wq, wd, 1, R, lane, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) x[sig + (size_t)G::M * (lane * G::E + m)] = a[m];
 }
@@ -156,7 +160,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN), *ws = w + G::N;
-    const double *wq = twq + ((size_t)pidx * 2 << G::LOGN);
+    const double *wq = twq + ((size_t)pidx * 3 << G::LOGN), *wd = wq + 2 * G::N;
     uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * S * G::M;
     const uint32_t sig = threadIdx.x / G::E, lane = threadIdx.x % G::E;
     const uint32_t b = chunk * S + sig;
@@ -167,19 +171,24 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = x[lane + m * G::E];
-    fwd_pass_any<R, FAM>(mode, a, w, ws, wq, G::M + b, 0, 0, q);
+    fwd_pass_any<R, FAM>(mode, a, w, ws, wq, wd, G::M + b, 0, 0, q);
 #pragma unroll
     for (int m = 0; m < G::E; m++) s[padded(lane + m * G::E)] = a[m];
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
-    if (!(FAM & (1 << kBfHarvey)) || mode != kBfHarvey) {
-        fwd_pass_any<R, FAM>(mode, a, w, ws, wq, G::M + b, R, lane, q);
+    if ((FAM & (1 << kBfF64)) && mode == kBfF64) {
+        fwd_pass<R, kBfF64>(a, w, ws, wq, wd, G::M + b, R, lane, q);
+        const double qd = (double)q, qinv = 1.0 / qd;
+#pragma unroll
+        for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = dbl_bits_mod(a[m], qd, qinv);  // |v| < 13q -> [0, q)
+    } else if (!(FAM & (1 << kBfHarvey)) || mode != kBfHarvey) {
+        fwd_pass<R, kBfGrow>(a, w, ws, wq, wd, G::M + b, R, lane, q);
         const PrimeConst p = pc[pidx];
 #pragma unroll
         for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = reduce_small(a[m], p);  // < 68q -> [0, q)
     } else {
-        fwd_pass<R, kBfHarvey>(a, w, ws, wq, G::M + b, R, lane, q);
+        fwd_pass<R, kBfHarvey>(a, w, ws, wq, wd, G::M + b, R, lane, q);
         const uint64_t q2 = 2 * q;
 #pragma unroll
         for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = csub(csub(a[m], q2), q);
@@ -249,7 +258,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_blk(uint64_t *__
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN) + 2 * G::N, *ws = w + G::N;
-    const double *wq = twq + ((size_t)pidx * 2 << G::LOGN) + G::N;
+    const double *wq = twq + ((size_t)pidx * 3 << G::LOGN) + G::N;
     uint64_t *xc = data + ((size_t)row << G::LOGN) + (size_t)chunk * S * G::M;
     const uint32_t sig = threadIdx.x / G::E, lane = threadIdx.x % G::E;
     const uint32_t b = chunk * S + sig;
@@ -294,7 +303,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) inv_col(uint64_t *__
     if (pidx == 255) return;
     const uint64_t q = pc[pidx].q;
     const uint64_t *w = tw + ((size_t)pidx * 4 << G::LOGN) + 2 * G::N, *ws = w + G::N;
-    const double *wq = twq + ((size_t)pidx * 2 << G::LOGN) + G::N;
+    const double *wq = twq + ((size_t)pidx * 3 << G::LOGN) + G::N;
     const uint64_t *sc = scale + 4 * (scale_by_prime ? pidx : slot - scale_base);
     uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * S;
     const uint32_t sig = threadIdx.x % S, lane = threadIdx.x / S;

@@ -12,7 +12,8 @@
 // variant); a thread owns 2^R elements and runs R radix-2 stages in registers, twice, with
 // one shared-memory exchange in between.  Global loads and stores move S consecutive words
 // per column row / per block segment (128 bytes at S = 16).  Values between the two
-// phases are lazy: below 36q (grow butterflies, q < 2^57) or in [0, 4q) (Harvey).
+// phases are lazy: below 36q (grow butterflies, q < 2^57), in [0, 4q) (Harvey), or signed
+// doubles below 7q in magnitude (the forward's FP64 butterflies, q < 2^52 / 36).
 //
 // The inverse's last stage folds a per-limb scale c (N^-1, or N^-1 times the
 // ModUp digit factor) into both outputs: (X+Y)*c and (X-Y)*psi^-(N/2)*c.
@@ -121,7 +122,7 @@ __device__ __forceinline__ void ct_bf_grow(uint64_t &x, uint64_t &y, uint64_t w,
 // y is exact as a double (its bits under the exponent of 2^52, minus 2^52), and
 // Q = round(y wq) comes from the mantissa of fma(y, wq, 2^52).  |Q - y w / q| <= 1/2 + y 2^-54 < 3/4,
 // so Q is floor(y w / q) or one more and r = y w - Q q lies in [-q, q) (as a wrapped 64-bit value);
-// the butterflies add q to it.  The integer pipe keeps the two low products only.
+// the inverse's butterflies add q to it.  The integer pipe keeps the two low products only.
 constexpr uint64_t kF64GrowLimit = (1ull << 52) / 36;
 
 __device__ __forceinline__ uint64_t mulmod_f64_centred(uint64_t y, uint64_t w, double wq, uint64_t q) {
@@ -131,12 +132,40 @@ __device__ __forceinline__ uint64_t mulmod_f64_centred(uint64_t y, uint64_t w, d
     return y * w - Q * q;
 }
 
-// Cooley-Tukey butterfly with the FP64 quotient, values growing by less than 2q per stage: from
-// inputs below 4q, 16 stages stay below 36q < 2^52 (q < kF64GrowLimit), the multiplicands too
-__device__ __forceinline__ void ct_bf_f64(uint64_t &x, uint64_t &y, uint64_t w, double wq, uint64_t q) {
-    const uint64_t a = x + q, t = mulmod_f64_centred(y, w, wq, q);
-    x = a + t;
-    y = a - t;
+// The forward transform of the primes below kF64GrowLimit runs entirely on the FP64 pipe, on values
+// held as doubles (signed exact integers, stored in the uint64_t registers as their bit patterns;
+// the column phase's output keeps that form in memory for the block phase).  Cooley-Tukey:
+// t = y w - Q q with Q = round(y wq), |Q - y w / q| < 3/4 (|y| < 16q, so |y| 2^-53 < 1/4), hence
+// |t| < q; y w = hi + lo exactly (hi = y w rounded, lo from an fma), hi - Q q is exact by a second
+// fma (an integer below 2^47 in magnitude), and t = (hi - Q q) + lo exactly.  From inputs below q in
+// magnitude, values grow by less than 3q/4 per stage: below 13q < 2^51 after 16 stages.  Eight FP64
+// operations and no integer multiply per butterfly.
+__device__ __forceinline__ void ct_bf_dbl(uint64_t &xb, uint64_t &yb, double w, double wq, double q) {
+    const double magic = 6755399441055744.0;  // 1.5 2^52
+    const double x = __longlong_as_double((long long)xb), y = __longlong_as_double((long long)yb);
+    const double Q = __dsub_rn(__fma_rn(y, wq, magic), magic);
+    const double hi = __dmul_rn(y, w);
+    const double lo = __fma_rn(y, w, -hi);
+    const double t = __dadd_rn(__fma_rn(-Q, q, hi), lo);
+    xb = (uint64_t)__double_as_longlong(__dadd_rn(x, t));
+    yb = (uint64_t)__double_as_longlong(__dsub_rn(x, t));
+}
+
+// x < 2^52 as the bit pattern of the double x
+__device__ __forceinline__ uint64_t to_dbl_bits(uint64_t x) {
+    const double two52 = 4503599627370496.0;
+    return (uint64_t)__double_as_longlong(__dsub_rn(__longlong_as_double((long long)(0x4330000000000000ull | x)), two52));
+}
+
+// a double holding a signed integer v (|v| < 2^51) -> v mod q in [0, q): v - round(v / q) q is exact
+// and within q/2 + 1 of zero, one conditional addition of q finishes it
+__device__ __forceinline__ uint64_t dbl_bits_mod(uint64_t vb, double q, double qinv) {
+    const double magic = 6755399441055744.0, two52 = 4503599627370496.0;
+    const double v = __longlong_as_double((long long)vb);
+    const double Q = __dsub_rn(__fma_rn(v, qinv, magic), magic);
+    double r = __fma_rn(-Q, q, v);
+    r = r < 0.0 ? __dadd_rn(r, q) : r;
+    return (uint64_t)__double_as_longlong(__dadd_rn(r, two52)) & 0x000FFFFFFFFFFFFFull;
 }
 
 // Gentleman-Sande butterfly on [0, 4q) with the FP64 quotient: x - y + 4q < 8q < 2^52
@@ -167,8 +196,8 @@ __device__ __forceinline__ void gs_bf4(uint64_t &x, uint64_t &y, uint64_t w, uin
 // R forward stages on E = 2^R registers.  Stage r of the pass is global stage
 // s0 + r; the twiddle of the pair starting at m is tw[(tb << (s0 + r)) + (g << r) + (m >> (R - r))].
 // MODE kBfHarvey: Harvey butterflies that keep values in [0, 4q) (any prime); kBfGrow: ct_bf_grow
-// (primes below kGrowPrimeLimit); kBfF64: ct_bf_f64 (primes below kF64GrowLimit), whose second
-// twiddle array is wq (w / q as doubles) instead of the Shoup companions.
+// (primes below kGrowPrimeLimit); kBfF64: ct_bf_dbl (primes below kF64GrowLimit) on values held as
+// doubles, with the twiddles wd (w as doubles) and wq (w / q as doubles).
 constexpr int kBfHarvey = 0, kBfGrow = 1, kBfF64 = 2;
 
 // the butterfly family of a limb's prime
@@ -185,8 +214,10 @@ constexpr int kFamSmall = (1 << kBfF64) | (1 << kBfGrow), kFamLarge = (1 << kBfG
 
 template <int R, int MODE = kBfHarvey>
 __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
-                                         const uint64_t *__restrict__ ws, const double *__restrict__ wq, uint32_t tb,
-                                         uint32_t s0, uint32_t g, uint64_t q) {
+                                         const uint64_t *__restrict__ ws, const double *__restrict__ wq,
+                                         const double *__restrict__ wd, uint32_t tb, uint32_t s0, uint32_t g,
+                                         uint64_t q) {
+    const double qd = (double)q;
 #pragma unroll
     for (int r = 0; r < R; r++) {
         const int half = (1 << R) >> (r + 1);
@@ -196,7 +227,7 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
             if (m & half) continue;
             uint32_t idx = base + (m >> (R - r));
             if (MODE == kBfF64)
-                ct_bf_f64(a[m], a[m + half], __ldg(w + idx), __ldg(wq + idx), q);
+                ct_bf_dbl(a[m], a[m + half], __ldg(wd + idx), __ldg(wq + idx), qd);
             else if (MODE == kBfGrow)
                 ct_bf_grow(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
             else
@@ -209,13 +240,14 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
 template <int R, int FAM>
 __device__ __forceinline__ void fwd_pass_any(int mode, uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
                                              const uint64_t *__restrict__ ws, const double *__restrict__ wq,
-                                             uint32_t tb, uint32_t s0, uint32_t g, uint64_t q) {
+                                             const double *__restrict__ wd, uint32_t tb, uint32_t s0, uint32_t g,
+                                             uint64_t q) {
     if ((FAM & (1 << kBfF64)) && mode == kBfF64)
-        fwd_pass<R, kBfF64>(a, w, ws, wq, tb, s0, g, q);
+        fwd_pass<R, kBfF64>(a, w, ws, wq, wd, tb, s0, g, q);
     else if (!(FAM & (1 << kBfHarvey)) || mode == kBfGrow)
-        fwd_pass<R, kBfGrow>(a, w, ws, wq, tb, s0, g, q);
+        fwd_pass<R, kBfGrow>(a, w, ws, wq, wd, tb, s0, g, q);
     else
-        fwd_pass<R, kBfHarvey>(a, w, ws, wq, tb, s0, g, q);
+        fwd_pass<R, kBfHarvey>(a, w, ws, wq, wd, tb, s0, g, q);
 }
 
 // MODE kBfGrow: gs_bf4 on [0, 4q) (primes below kGrowPrimeLimit); kBfF64: gs_bf_f64 on [0, 4q);
