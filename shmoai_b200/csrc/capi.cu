@@ -123,7 +123,7 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
     c->s52 = *std::max_element(primes.begin(), primes.end()) < kS52PrimeLimit;
     {
         int fam = 0;
-        for (uint64_t q : primes) fam |= 1 << bf_mode_of(q);
+        for (uint64_t q : primes) fam |= (1 << bf_mode_of(q)) | (1 << fwd_mode_of(q));
         c->ntt_families = (fam & ~kFamSmall) == 0 ? kFamSmall : (fam & ~kFamLarge) == 0 ? kFamLarge : kFamAll;
     }
     // per-prime constants and twiddles
@@ -148,12 +148,12 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
     c->pc = upload(c->h_pc);
     c->tw = upload(tw);
     {
-        // for the FP64 butterflies of the primes below kF64GrowLimit (other primes never read it):
+        // for the FP64 butterflies of the primes below kF64CentreLimit (other primes never read it):
         // the forward and inverse w / q rounded to the nearest double (w and q are exact doubles
         // below 2^53), then the forward w itself as a double
         std::vector<double> twq((size_t)QP * 3 * n, 0.0);
         for (uint32_t i = 0; i < QP; i++) {
-            if (primes[i] >= kF64GrowLimit) continue;
+            if (primes[i] >= kF64CentreLimit) continue;
             const double qd = (double)primes[i];
             const uint64_t *t = tw.data() + (size_t)i * 4 * n;
             double *d = twq.data() + (size_t)i * 3 * n;

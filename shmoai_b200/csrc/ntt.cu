@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
     const double *wq = twq + ((size_t)pidx * 3 << G::LOGN), *wd = wq + 2 * G::N;
     uint64_t *x = data + ((size_t)row << G::LOGN) + chunk * S;
 
-    const int mode = bf_mode_of(q);  // uniform per CTA (one limb)
+    const int mode = fwd_mode_of(q);  // uniform per CTA (one limb)
     uint64_t a[G::E];
     if constexpr (IOK == kIoModUp) {
         const ModUpIO &mu = io.mu;
@@ -132,6 +132,10 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_col(uint64_t *__
     if ((FAM & (1 << kBfF64)) && mode == kBfF64) {  // [0, q) -> doubles for the FP64 butterflies
 #pragma unroll
         for (int m = 0; m < G::E; m++) a[m] = to_dbl_bits(a[m]);
+    } else if ((FAM & (1 << kBfF64R)) && mode == kBfF64R) {  // [0, q) -> doubles within q/2 of zero
+        const double qd = (double)q, qinv = __ldg(wq);
+#pragma unroll
+        for (int m = 0; m < G::E; m++) a[m] = dbl_centre(to_dbl_bits(a[m]), qd, qinv);
     }
     fwd_pass_any<R, FAM>(mode, a, w, ws, wq, wd, 1, 0, 0, q);
 #pragma unroll
@@ -167,7 +171,7 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
     uint64_t *x = xc + (size_t)sig * G::M;
     uint64_t *s = sm + sig * G::PAD_M;
 
-    const int mode = bf_mode_of(q);  // the same choice fwd_col made for this limb
+    const int mode = fwd_mode_of(q);  // the same choice fwd_col made for this limb
     uint64_t a[G::E];
 #pragma unroll
     for (int m = 0; m < G::E; m++) a[m] = x[lane + m * G::E];
@@ -179,9 +183,14 @@ __global__ void __launch_bounds__(Geo<R, S>::THREADS, MINB) fwd_blk(uint64_t *__
     for (int m = 0; m < G::E; m++) a[m] = s[padded(lane * G::E + m)];
     if ((FAM & (1 << kBfF64)) && mode == kBfF64) {
         fwd_pass<R, kBfF64>(a, w, ws, wq, wd, G::M + b, R, lane, q);
-        const double qd = (double)q, qinv = 1.0 / qd;
+        const double qd = (double)q, qinv = __ldg(wq);  // wq[0] = 1 / q
 #pragma unroll
         for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = dbl_bits_mod(a[m], qd, qinv);  // |v| < 13q -> [0, q)
+    } else if ((FAM & (1 << kBfF64R)) && mode == kBfF64R) {
+        fwd_pass<R, kBfF64R>(a, w, ws, wq, wd, G::M + b, R, lane, q);  // centred by the pass
+        const double qd = (double)q;
+#pragma unroll
+        for (int m = 0; m < G::E; m++) s[padded(lane * G::E + m)] = dbl_bits_canon(a[m], qd);
     } else if (!(FAM & (1 << kBfHarvey)) || mode != kBfHarvey) {
         fwd_pass<R, kBfGrow>(a, w, ws, wq, wd, G::M + b, R, lane, q);
         const PrimeConst p = pc[pidx];

@@ -157,6 +157,30 @@ __device__ __forceinline__ uint64_t to_dbl_bits(uint64_t x) {
     return (uint64_t)__double_as_longlong(__dsub_rn(__longlong_as_double((long long)(0x4330000000000000ull | x)), two52));
 }
 
+// Primes in [kF64GrowLimit, 2^51) run the same butterfly with its multiplicand first brought within
+// q/2 + 1 of zero (dbl_centre), so that |y wq| < 2^50 and the rounding through 1.5 2^52 gives Q
+// exactly: |Q - y w / q| <= 1/2 + |y| 2^-54 < 0.57, |t| < 0.57q; y w < 2^102, so |lo| <= 2^48
+// and hi - Q q stays below 2^51.  All values are centred again after every pass of four stages, so
+// the other operand, growing by less than 0.57q per stage, stays below 2.75q < 2^53: exact.
+constexpr uint64_t kF64CentreLimit = 1ull << 51;
+
+// v (|v| < 2^52, a signed integer) -> v - round(v / q) q, within q/2 + 1 of zero (exact: an integer
+// below q); qinv = 1 / q rounded
+__device__ __forceinline__ uint64_t dbl_centre(uint64_t vb, double q, double qinv) {
+    const double magic = 6755399441055744.0;
+    const double v = __longlong_as_double((long long)vb);
+    const double Q = __dsub_rn(__fma_rn(v, qinv, magic), magic);
+    return (uint64_t)__double_as_longlong(__fma_rn(-Q, q, v));
+}
+
+// a centred double (|v| <= q/2 + 1) -> v mod q in [0, q) as an integer
+__device__ __forceinline__ uint64_t dbl_bits_canon(uint64_t vb, double q) {
+    const double two52 = 4503599627370496.0;
+    double v = __longlong_as_double((long long)vb);
+    v = v < 0.0 ? __dadd_rn(v, q) : v;
+    return (uint64_t)__double_as_longlong(__dadd_rn(v, two52)) & 0x000FFFFFFFFFFFFFull;
+}
+
 // a double holding a signed integer v (|v| < 2^51) -> v mod q in [0, q): v - round(v / q) q is exact
 // and within q/2 + 1 of zero, one conditional addition of q finishes it
 __device__ __forceinline__ uint64_t dbl_bits_mod(uint64_t vb, double q, double qinv) {
@@ -196,21 +220,30 @@ __device__ __forceinline__ void gs_bf4(uint64_t &x, uint64_t &y, uint64_t w, uin
 // R forward stages on E = 2^R registers.  Stage r of the pass is global stage
 // s0 + r; the twiddle of the pair starting at m is tw[(tb << (s0 + r)) + (g << r) + (m >> (R - r))].
 // MODE kBfHarvey: Harvey butterflies that keep values in [0, 4q) (any prime); kBfGrow: ct_bf_grow
-// (primes below kGrowPrimeLimit); kBfF64: ct_bf_dbl (primes below kF64GrowLimit) on values held as
-// doubles, with the twiddles wd (w as doubles) and wq (w / q as doubles).
-constexpr int kBfHarvey = 0, kBfGrow = 1, kBfF64 = 2;
+// (primes below kGrowPrimeLimit); kBfF64: ct_bf_dbl (forward, primes below kF64GrowLimit) on values
+// held as doubles, with the twiddles wd (w as doubles) and wq (w / q as doubles); kBfF64R: the same
+// with each multiplicand centred before its product and every value centred after the pass
+// (forward, primes below kF64CentreLimit).  The inverse's kBfF64 is gs_bf_f64 (integer values,
+// FP64 quotient).
+constexpr int kBfHarvey = 0, kBfGrow = 1, kBfF64 = 2, kBfF64R = 3;
 
-// the butterfly family of a limb's prime
+// the inverse's butterfly family of a limb's prime
 __host__ __device__ __forceinline__ int bf_mode_of(uint64_t q) {
     return q < kF64GrowLimit ? kBfF64 : q < kGrowPrimeLimit ? kBfGrow : kBfHarvey;
 }
 
-// The families a kernel instantiation carries (a bit per family).  Every unrolled family adds a
-// full copy of the transform's butterflies to the kernel, so a context's launches use the
-// instantiation with just the families its primes need: kFamSmall (every prime below 2^57: the
-// bootstrapping chains), kFamLarge (none below kF64GrowLimit), kFamAll otherwise.
-constexpr int kFamSmall = (1 << kBfF64) | (1 << kBfGrow), kFamLarge = (1 << kBfGrow) | (1 << kBfHarvey),
-              kFamAll = kFamSmall | kFamLarge;
+// the forward's butterfly family of a limb's prime
+__host__ __device__ __forceinline__ int fwd_mode_of(uint64_t q) {
+    return q < kF64GrowLimit ? kBfF64 : q < kF64CentreLimit ? kBfF64R : q < kGrowPrimeLimit ? kBfGrow : kBfHarvey;
+}
+
+// The families a kernel instantiation carries (a bit per family, forward and inverse together).
+// Every unrolled family adds a full copy of the transform's butterflies to the kernel, so a
+// context's launches use the instantiation with just the families its primes need: kFamSmall
+// (every prime below 2^57: the bootstrapping chains), kFamLarge (none below kF64GrowLimit),
+// kFamAll otherwise.
+constexpr int kFamSmall = (1 << kBfF64) | (1 << kBfF64R) | (1 << kBfGrow),
+              kFamLarge = (1 << kBfF64R) | (1 << kBfGrow) | (1 << kBfHarvey), kFamAll = kFamSmall | kFamLarge;
 
 template <int R, int MODE = kBfHarvey>
 __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *__restrict__ w,
@@ -218,6 +251,7 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
                                          const double *__restrict__ wd, uint32_t tb, uint32_t s0, uint32_t g,
                                          uint64_t q) {
     const double qd = (double)q;
+    const double qinv = MODE == kBfF64R ? __ldg(wq) : 0.0;  // wq[0] = 1 / q (the twiddle at index 0 is 1)
 #pragma unroll
     for (int r = 0; r < R; r++) {
         const int half = (1 << R) >> (r + 1);
@@ -228,11 +262,19 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
             uint32_t idx = base + (m >> (R - r));
             if (MODE == kBfF64)
                 ct_bf_dbl(a[m], a[m + half], __ldg(wd + idx), __ldg(wq + idx), qd);
+            else if (MODE == kBfF64R) {
+                a[m + half] = dbl_centre(a[m + half], qd, qinv);
+                ct_bf_dbl(a[m], a[m + half], __ldg(wd + idx), __ldg(wq + idx), qd);
+            }
             else if (MODE == kBfGrow)
                 ct_bf_grow(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
             else
                 ct_bf(a[m], a[m + half], __ldg(w + idx), __ldg(ws + idx), q);
         }
+    }
+    if (MODE == kBfF64R) {
+#pragma unroll
+        for (int m = 0; m < (1 << R); m++) a[m] = dbl_centre(a[m], qd, qinv);
     }
 }
 
@@ -244,6 +286,8 @@ __device__ __forceinline__ void fwd_pass_any(int mode, uint64_t (&a)[1 << R], co
                                              uint64_t q) {
     if ((FAM & (1 << kBfF64)) && mode == kBfF64)
         fwd_pass<R, kBfF64>(a, w, ws, wq, wd, tb, s0, g, q);
+    else if ((FAM & (1 << kBfF64R)) && mode == kBfF64R)
+        fwd_pass<R, kBfF64R>(a, w, ws, wq, wd, tb, s0, g, q);
     else if (!(FAM & (1 << kBfHarvey)) || mode == kBfGrow)
         fwd_pass<R, kBfGrow>(a, w, ws, wq, wd, tb, s0, g, q);
     else
