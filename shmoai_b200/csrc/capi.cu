@@ -150,17 +150,22 @@ Context *create_context(uint32_t log_n, const std::vector<uint64_t> &primes, uin
     {
         // for the FP64 butterflies of the primes below kF64CentreLimit (other primes never read it):
         // the forward and inverse w / q rounded to the nearest double (w and q are exact doubles
-        // below 2^53), then the forward w itself as a double
+        // below 2^53), then the forward w itself as a double.  The forward twiddles of the primes
+        // at or above kF64GrowLimit (the centred family) are kept within q/2 of zero (w - q for
+        // w > q/2), so that |w / q| <= 1/2.
         std::vector<double> twq((size_t)QP * 3 * n, 0.0);
         for (uint32_t i = 0; i < QP; i++) {
             if (primes[i] >= kF64CentreLimit) continue;
-            const double qd = (double)primes[i];
+            const uint64_t q = primes[i];
+            const double qd = (double)q;
+            const bool centre = q >= kF64GrowLimit;
             const uint64_t *t = tw.data() + (size_t)i * 4 * n;
             double *d = twq.data() + (size_t)i * 3 * n;
             for (uint32_t k = 0; k < n; k++) {
-                d[k] = (double)t[k] / qd;
+                const double w = centre && t[k] > q / 2 ? (double)t[k] - qd : (double)t[k];
+                d[k] = w / qd;
                 d[n + k] = (double)t[2 * n + k] / qd;
-                d[2 * n + k] = (double)t[k];
+                d[2 * n + k] = w;
             }
         }
         c->twq = upload(twq);

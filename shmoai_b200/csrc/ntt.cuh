@@ -157,11 +157,13 @@ __device__ __forceinline__ uint64_t to_dbl_bits(uint64_t x) {
     return (uint64_t)__double_as_longlong(__dsub_rn(__longlong_as_double((long long)(0x4330000000000000ull | x)), two52));
 }
 
-// Primes in [kF64GrowLimit, 2^51) run the same butterfly with its multiplicand first brought within
-// q/2 + 1 of zero (dbl_centre), so that |y wq| < 2^50 and the rounding through 1.5 2^52 gives Q
-// exactly: |Q - y w / q| <= 1/2 + |y| 2^-54 < 0.57, |t| < 0.57q; y w < 2^102, so |lo| <= 2^48
-// and hi - Q q stays below 2^51.  All values are centred again after every pass of four stages, so
-// the other operand, growing by less than 0.57q per stage, stays below 2.75q < 2^53: exact.
+// Primes in [kF64GrowLimit, 2^51) run the same butterfly on twiddles kept within q/2 of zero
+// (|wq| <= 1/2, |wq - w / q| <= 2^-55), with every value centred (dbl_centre) at the start and
+// after every pass of four stages, and the multiplicands of a pass's fourth stage centred before
+// their products.  |Q - y w / q| <= 1/2 + |y| 2^-55, so from |v| <= q/2 the multiplicands of the
+// first three stages stay below q/2, 1.03q and 1.6q (|y wq| < 2^51: the rounding through
+// 1.5 2^52 is exact), |t| below 0.53q, 0.57q and 0.6q, the fourth stage's below 0.53q, and every
+// value below 2.73q < 2^53: exact; |y w| < 2^102, so |lo| <= 2^48 and hi - Q q stays below 2^52.
 constexpr uint64_t kF64CentreLimit = 1ull << 51;
 
 // v (|v| < 2^52, a signed integer) -> v - round(v / q) q, within q/2 + 1 of zero (exact: an integer
@@ -222,8 +224,8 @@ __device__ __forceinline__ void gs_bf4(uint64_t &x, uint64_t &y, uint64_t w, uin
 // MODE kBfHarvey: Harvey butterflies that keep values in [0, 4q) (any prime); kBfGrow: ct_bf_grow
 // (primes below kGrowPrimeLimit); kBfF64: ct_bf_dbl (forward, primes below kF64GrowLimit) on values
 // held as doubles, with the twiddles wd (w as doubles) and wq (w / q as doubles); kBfF64R: the same
-// with each multiplicand centred before its product and every value centred after the pass
-// (forward, primes below kF64CentreLimit).  The inverse's kBfF64 is gs_bf_f64 (integer values,
+// on centred twiddles, with the last stage's multiplicands centred before their products and
+// every value centred after the pass (forward, primes below kF64CentreLimit).  The inverse's kBfF64 is gs_bf_f64 (integer values,
 // FP64 quotient).
 constexpr int kBfHarvey = 0, kBfGrow = 1, kBfF64 = 2, kBfF64R = 3;
 
@@ -263,7 +265,7 @@ __device__ __forceinline__ void fwd_pass(uint64_t (&a)[1 << R], const uint64_t *
             if (MODE == kBfF64)
                 ct_bf_dbl(a[m], a[m + half], __ldg(wd + idx), __ldg(wq + idx), qd);
             else if (MODE == kBfF64R) {
-                a[m + half] = dbl_centre(a[m + half], qd, qinv);
+                if (r == R - 1) a[m + half] = dbl_centre(a[m + half], qd, qinv);
                 ct_bf_dbl(a[m], a[m + half], __ldg(wd + idx), __ldg(wq + idx), qd);
             }
             else if (MODE == kBfGrow)

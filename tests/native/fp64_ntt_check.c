@@ -39,7 +39,14 @@ int run(uint64_t q, int centred) {
     static uint64_t a[N], w[N];
     static double d[N], wd[N], wq[N];
     const double qd = (double)q, qinv = 1.0 / qd;
-    for (int i = 0; i < N; i++) { a[i] = xs() % q; w[i] = xs() % q; d[i] = (double)a[i]; wd[i] = (double)w[i]; wq[i] = (double)w[i] / qd; }
+    for (int i = 0; i < N; i++) {
+        a[i] = xs() % q;
+        w[i] = xs() % q;
+        d[i] = (double)a[i];
+        // the centred family keeps its twiddles within q/2 of zero
+        wd[i] = centred && w[i] > q / 2 ? (double)w[i] - qd : (double)w[i];
+        wq[i] = wd[i] / qd;
+    }
     if (centred) for (int i = 0; i < N; i++) d[i] = centre(d[i], qd, qinv);
     double maxabs = 0;
     for (int s = 0; s < 16; s++) {
@@ -51,7 +58,7 @@ int run(uint64_t q, int centred) {
                 uint64_t x = a[j], y = (uint64_t)(((u128)a[j + t] * W) % q);
                 a[j] = (x + y) % q;
                 a[j + t] = (x + q - y) % q;
-                if (centred) d[j + t] = centre(d[j + t], qd, qinv);
+                if (centred && (s & 3) == 3) d[j + t] = centre(d[j + t], qd, qinv);  // a pass's fourth stage
                 bf_dbl(&d[j], &d[j + t], Wd, Wq, qd);
                 if (fabs(d[j]) > maxabs) maxabs = fabs(d[j]);
                 if (fabs(d[j + t]) > maxabs) maxabs = fabs(d[j + t]);
