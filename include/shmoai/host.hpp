@@ -538,8 +538,11 @@ class BatchBootstrapper {
     Ciphertext evalmod(const Ciphertext &x, const Evaluator *ev = nullptr) const;
     // Autotuning for batches of `count` ciphertexts (members per shared-a group, 0 =
     // ordinary): the NTT tile and, for shared-a, the Sh-Rot inner-product chunk (timed on
-    // scratch data), then each slot-transform layer's BSGS split, modelled from a hoisted
-    // ModUp and a per-step key switch timed at the layer's level; re-prepares the layers.
+    // scratch data), the NTT tile again by a hoisted rotation of the batch at the top level
+    // under each tile (record "ntt_tile (hoisted rotation, top level)", the tile kept; only
+    // where the knobs time real kernels), then each slot-transform layer's BSGS split,
+    // modelled from a hoisted ModUp and a per-step key switch timed at the layer's level;
+    // re-prepares the layers.
     // The split decides the rotation steps, so call it before generating Galois keys.
     std::vector<TuneRecord> tune(uint32_t count, uint32_t members);
     // a stored split (BootstrapParams::bsgs_g1 layout); re-prepares the layers
