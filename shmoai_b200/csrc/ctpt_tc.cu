@@ -674,8 +674,8 @@ struct CrtLimb {
 
 // Fraction bits of the fixed-point CRT fractions F_t = round(2^19 [(M/m_t)^-1]_{m_t} / m_t): with
 // r_t < 251 and T <= 20, sum_t r_t F_t + 2^18 < 2^32, and the sum's rounding error
-// T 251 2^-20 < 0.005 keeps v = round(sum_t r_t frac_t) exact (the CRT margin leaves the true sum
-// within 1/8 of an integer).
+// T 251 2^-20 < 0.005 keeps v = round(sum_t r_t frac_t) exact (M > 2.02 |S| leaves the true sum
+// within 0.495 of an integer).
 constexpr uint32_t kCrtFracBits = 19;
 
 // workspace bytes before the residue planes: the error flag, then the CRT tables for every
